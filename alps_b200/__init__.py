@@ -1,0 +1,361 @@
+"""B200 exact-diagonalisation engine for the ALPS sparsediag Lanczos path.
+
+Python face of libaed.so (C ABI in include/aed.h).  The engine keeps ALPS's
+parameter surface (LATTICE, MODEL, J/J1, CONSERVED_QUANTUMNUMBERS, Sz_total,
+NUMBER_EIGENVALUES) and the ietl vector-space / mult() operations; every call
+goes to the CUDA library.  There is no CPU fallback: importing the engine
+without a built libaed.so raises, and calls without a GPU fail with the
+library's error message.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "AEDError", "Hamiltonian", "DeviceVector", "parse_parameters", "model_from_parameters", "lib",
+    "FP64", "FP32",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libaed.so")
+
+FP64 = 0
+FP32 = 1
+MAX_NEV = 16
+MAX_BONDS = 128
+
+OK = 0
+ERR_INVALID = -1
+ERR_NOMEM = -2
+ERR_ADMISSION = -3
+ERR_CUDA = -4
+ERR_TIMEOUT = -5
+ERR_NOT_CONVERGED = -6
+ERR_TRIDIAG = -7
+ERR_MISMATCH = -8
+ERR_CANCELLED = -9
+PENDING = 1
+
+
+class AEDError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"aed error {code}: {msg}")
+        self.code = code
+
+
+class ModelDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_sites", ctypes.c_int32), ("n_up", ctypes.c_int32), ("n_bonds", ctypes.c_int32),
+        ("bond_s1", ctypes.POINTER(ctypes.c_int32)), ("bond_s2", ctypes.POINTER(ctypes.c_int32)),
+        ("bond_jz", ctypes.POINTER(ctypes.c_double)), ("bond_jxy", ctypes.POINTER(ctypes.c_double)),
+        ("bond_k", ctypes.POINTER(ctypes.c_double)), ("site_h", ctypes.POINTER(ctypes.c_double)),
+        ("site_d", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class ParamInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_sites", ctypes.c_int32), ("n_up", ctypes.c_int32), ("n_bonds", ctypes.c_int32),
+        ("number_eigenvalues", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
+        ("has_site_terms", ctypes.c_int32),
+    ]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [
+        ("nev", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("rtol", ctypes.c_double),
+        ("atol", ctypes.c_double), ("seed", ctypes.c_uint64), ("start", ctypes.POINTER(ctypes.c_double)),
+        ("refine", ctypes.c_int32), ("profile", ctypes.c_int32),
+    ]
+
+
+class SolveResult(ctypes.Structure):
+    _fields_ = [
+        ("n_evals", ctypes.c_int32), ("iterations", ctypes.c_int32), ("iterations_low", ctypes.c_int32),
+        ("converged", ctypes.c_int32), ("evals", ctypes.c_double * MAX_NEV),
+        ("errors", ctypes.c_double * MAX_NEV), ("evals_low", ctypes.c_double * MAX_NEV),
+        ("seconds", ctypes.c_double), ("apply_ms", ctypes.c_double),
+    ]
+
+
+_lib = None
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_I64P = ctypes.POINTER(ctypes.c_int64)
+_U32P = ctypes.POINTER(ctypes.c_uint32)
+
+
+def lib():
+    """The loaded libaed.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libaed.so not found at {LIB_PATH}: run `python -m alps_b200.build` "
+                              "(the engine has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "aed_last_error": (ctypes.c_char_p, []),
+            "aed_parse_parameters": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ParamInfo), _I32P, _I32P, _DP,
+                                                    _DP, _DP, _DP, _DP, _I32, _I32]),
+            "aed_create": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(_P)]),
+            "aed_destroy": (ctypes.c_int, [_P]),
+            "aed_dimension": (ctypes.c_int, [_P, _I64P]),
+            "aed_basis_copy": (ctypes.c_int, [_P, _U32P, _I64, _I64]),
+            "aed_index": (ctypes.c_int, [_P, _U32P, _I64, _I64P]),
+            "aed_vec_alloc": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+            "aed_vec_free": (ctypes.c_int, [_P, _P]),
+            "aed_vec_upload": (ctypes.c_int, [_P, _P, _DP]),
+            "aed_vec_download": (ctypes.c_int, [_P, _P, _DP]),
+            "aed_vec_copy": (ctypes.c_int, [_P, _P, _P]),
+            "aed_vec_clear": (ctypes.c_int, [_P, _P]),
+            "aed_vec_fill_random": (ctypes.c_int, [_P, _P, ctypes.c_uint64]),
+            "aed_mult": (ctypes.c_int, [_P, _P, _P]),
+            "aed_dot": (ctypes.c_int, [_P, _P, _P, _DP]),
+            "aed_nrm2": (ctypes.c_int, [_P, _P, _DP]),
+            "aed_axpy": (ctypes.c_int, [_P, _D, _P, _P]),
+            "aed_scal": (ctypes.c_int, [_P, _D, _P]),
+            "aed_div": (ctypes.c_int, [_P, _D, _P]),
+            "aed_lanczos_step": (ctypes.c_int, [_P, _P, _P, _P, _D, _DP, _DP]),
+            "aed_solve": (ctypes.c_int, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),
+            "aed_last_tmatrix": (ctypes.c_int, [_P, _DP, _DP, _I32, _I32P]),
+            "aed_time_mult": (ctypes.c_int, [_P, _P, _P, _I32, _DP]),
+            "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+            "aed_launch_count": (ctypes.c_int, [_I64P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc not in (OK, PENDING):
+        msg = lib().aed_last_error()
+        raise AEDError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP) if a is not None else None
+
+
+def launch_count() -> int:
+    """Engine kernel launches made by this process so far."""
+    c = ctypes.c_int64(0)
+    _check(lib().aed_launch_count(ctypes.byref(c)))
+    return c.value
+
+
+def parse_parameters(text: str):
+    """ALPS parameter text -> dict(n_sites, n_up, bonds=[(s1, s2, Jz, Jxy, K)], nev, max_iter, site_h, site_d)."""
+    info = ParamInfo()
+    _check(lib().aed_parse_parameters(text.encode(), ctypes.byref(info), None, None, None, None, None, None, None,
+                                      0, 0))
+    nb, ns = info.n_bonds, info.n_sites
+    s1 = np.zeros(max(nb, 1), np.int32)
+    s2 = np.zeros(max(nb, 1), np.int32)
+    jz = np.zeros(max(nb, 1))
+    jxy = np.zeros(max(nb, 1))
+    kq = np.zeros(max(nb, 1))
+    sh = np.zeros(ns)
+    sd = np.zeros(ns)
+    _check(lib().aed_parse_parameters(text.encode(), ctypes.byref(info), s1.ctypes.data_as(_I32P),
+                                      s2.ctypes.data_as(_I32P), _dp(jz), _dp(jxy), _dp(kq), _dp(sh), _dp(sd), nb, ns))
+    bonds = [(int(s1[b]), int(s2[b]), float(jz[b]), float(jxy[b]), float(kq[b])) for b in range(nb)]
+    return {"n_sites": ns, "n_up": info.n_up, "bonds": bonds, "nev": info.number_eigenvalues,
+            "max_iter": info.max_iterations,
+            "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
+
+
+def model_from_parameters(params) -> dict:
+    """dict or text of ALPS parameters -> parse_parameters() result."""
+    if isinstance(params, dict):
+        lines = []
+        for k, v in params.items():
+            if isinstance(v, str) and not v.replace(".", "", 1).replace("-", "", 1).isdigit():
+                lines.append(f'{k} = "{v}"')
+            else:
+                lines.append(f"{k} = {v}")
+        params = "\n".join(lines)
+    return parse_parameters(params)
+
+
+class DeviceVector:
+    """A device vector of the handle's precision (ietl vector_type)."""
+
+    def __init__(self, ham: "Hamiltonian"):
+        self.ham = ham
+        p = _P()
+        _check(lib().aed_vec_alloc(ham._h, ctypes.byref(p)))
+        self.ptr = p
+
+    def free(self):
+        if self.ptr is not None and self.ptr.value:
+            lib().aed_vec_free(self.ham._h, self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            if self.ham._h:
+                self.free()
+        except Exception:
+            pass
+
+    def upload(self, host):
+        host = np.ascontiguousarray(host, dtype=np.float64)
+        assert host.size == self.ham.dim
+        _check(lib().aed_vec_upload(self.ham._h, self.ptr, _dp(host)))
+        return self
+
+    def download(self):
+        out = np.empty(self.ham.dim)
+        _check(lib().aed_vec_download(self.ham._h, self.ptr, _dp(out)))
+        return out
+
+
+class Hamiltonian:
+    """One Sz sector of a spin-1/2 model on one GPU (an aed_handle)."""
+
+    def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None):
+        self.n_sites, self.n_up = int(n_sites), int(n_up)
+        self.bonds = [tuple(b) for b in bonds]
+        self.precision = precision
+        nb = len(self.bonds)
+        self._s1 = np.array([b[0] for b in self.bonds] or [0], np.int32)
+        self._s2 = np.array([b[1] for b in self.bonds] or [0], np.int32)
+        self._jz = np.array([b[2] for b in self.bonds] or [0.0])
+        self._jxy = np.array([b[3] for b in self.bonds] or [0.0])
+        self._k = np.array([(b[4] if len(b) > 4 else 0.0) for b in self.bonds] or [0.0])
+        self._sh = None if site_h is None else np.ascontiguousarray(site_h, dtype=np.float64)
+        self._sd = None if site_d is None else np.ascontiguousarray(site_d, dtype=np.float64)
+        desc = ModelDesc(self.n_sites, self.n_up, nb, self._s1.ctypes.data_as(_I32P), self._s2.ctypes.data_as(_I32P),
+                         _dp(self._jz), _dp(self._jxy), _dp(self._k), _dp(self._sh), _dp(self._sd))
+        h = _P()
+        self._h = None
+        _check(lib().aed_create(ctypes.byref(desc), precision, device, ctypes.byref(h)))
+        self._h = h
+        d = ctypes.c_int64(0)
+        _check(lib().aed_dimension(self._h, ctypes.byref(d)))
+        self.dim = d.value
+
+    @classmethod
+    def from_parameters(cls, params, precision=FP64, device=0):
+        m = model_from_parameters(params)
+        ham = cls(m["n_sites"], m["n_up"], m["bonds"], precision, device, m["site_h"], m["site_d"])
+        ham.params = m
+        return ham
+
+    def close(self):
+        if self._h:
+            lib().aed_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- basis ---------------------------------------------------------------
+    def basis(self, offset=0, count=None):
+        count = self.dim - offset if count is None else count
+        out = np.empty(count, np.uint32)
+        _check(lib().aed_basis_copy(self._h, out.ctypes.data_as(_U32P), offset, count))
+        return out
+
+    def index(self, states):
+        st = np.ascontiguousarray(states, dtype=np.uint32)
+        out = np.empty(st.size, np.int64)
+        _check(lib().aed_index(self._h, st.ctypes.data_as(_U32P), st.size, out.ctypes.data_as(_I64P)))
+        return out
+
+    # -- ietl vector space ------------------------------------------------------
+    def new_vector(self):
+        return DeviceVector(self)
+
+    def mult(self, x: DeviceVector, y: DeviceVector):
+        _check(lib().aed_mult(self._h, x.ptr, y.ptr))
+
+    def apply(self, xh):
+        """Host convenience: y = H x for a host vector (uploads, applies, downloads)."""
+        x = self.new_vector().upload(xh)
+        y = self.new_vector()
+        self.mult(x, y)
+        out = y.download()
+        x.free()
+        y.free()
+        return out
+
+    def dot(self, x, y):
+        out = ctypes.c_double(0)
+        _check(lib().aed_dot(self._h, x.ptr, y.ptr, ctypes.byref(out)))
+        return out.value
+
+    def two_norm(self, x):
+        out = ctypes.c_double(0)
+        _check(lib().aed_nrm2(self._h, x.ptr, ctypes.byref(out)))
+        return out.value
+
+    def axpy(self, a, x, y):
+        _check(lib().aed_axpy(self._h, a, x.ptr, y.ptr))
+
+    def scal(self, a, x):
+        _check(lib().aed_scal(self._h, a, x.ptr))
+
+    def div(self, a, x):
+        _check(lib().aed_div(self._h, a, x.ptr))
+
+    def fill_random(self, x, seed):
+        _check(lib().aed_vec_fill_random(self._h, x.ptr, seed))
+
+    def copy(self, x, y):
+        _check(lib().aed_vec_copy(self._h, x.ptr, y.ptr))
+
+    def lanczos_step(self, v_prev, v_cur, v_next, beta_prev):
+        a = ctypes.c_double(0)
+        b = ctypes.c_double(0)
+        _check(lib().aed_lanczos_step(self._h, v_prev.ptr if v_prev is not None else None, v_cur.ptr, v_next.ptr,
+                                      beta_prev, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def time_mult(self, x, y, reps=10):
+        ms = ctypes.c_double(0)
+        _check(lib().aed_time_mult(self._h, x.ptr, y.ptr, reps, ctypes.byref(ms)))
+        return ms.value
+
+    # -- solves ---------------------------------------------------------------------
+    def solve(self, nev=1, max_iter=0, seed=0, start=None, rtol=0.0, atol=0.0, refine=0, profile=False):
+        st = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
+        opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0)
+        res = SolveResult()
+        _check(lib().aed_solve(self._h, ctypes.byref(opts), ctypes.byref(res)))
+        n = res.n_evals
+        return {"evals": np.array(res.evals[:n]), "errors": np.array(res.errors[:n]),
+                "iterations": res.iterations, "iterations_low": res.iterations_low,
+                "evals_low": np.array(res.evals_low[:n]), "converged": bool(res.converged),
+                "seconds": res.seconds, "apply_ms": res.apply_ms}
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        p = _P()
+        _check(lib().aed_get_stream(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    def last_tmatrix(self):
+        n = ctypes.c_int32(0)
+        _check(lib().aed_last_tmatrix(self._h, None, None, 0, ctypes.byref(n)))
+        a = np.zeros(max(n.value, 1))
+        b = np.zeros(max(n.value, 1))
+        _check(lib().aed_last_tmatrix(self._h, _dp(a), _dp(b), n.value, ctypes.byref(n)))
+        return a[: n.value], b[: n.value]

@@ -1,0 +1,106 @@
+// aed_internal.h -- shared declarations of the engine's host and device code.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/aed.h"
+
+namespace aed {
+
+// ---- errors ----------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define AED_CUDA_TRY(expr)                                                                  \
+  do {                                                                                      \
+    cudaError_t aed_e_ = (expr);                                                            \
+    if (aed_e_ != cudaSuccess)                                                              \
+      return ::aed::fail(AED_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(aed_e_)); \
+  } while (0)
+
+constexpr int kMaxBonds = AED_MAX_BONDS;
+constexpr int kMaxDiag = AED_MAX_BONDS + 32;
+
+// ---- host model ------------------------------------------------------------
+struct Model {
+  int N = 0, n_up = 0;
+  std::vector<int> s1, s2;
+  std::vector<double> jz, jxy, kq;
+  std::vector<double> site_h, site_d;  // empty when absent
+};
+
+int model_from_desc(const aed_model_desc* d, Model& m);
+
+// ---- device-facing coupling tables -------------------------------------------
+// A spin-flip pair: bits mhi > mlo (masks), merged coefficient of all bonds
+// joining the two sites, summed in bond order.
+struct PairTerm {
+  uint32_t mhi, mlo;
+  double c;
+  float chi, clo;  // c split into two floats (c ~= chi + clo) for the FP32 kernels
+};
+
+// One diagonal contribution, in the reference's accumulation order (site
+// terms, then bonds): v = ((s & m1) != 0) == ((s & m2) != 0) ? veq : vne.
+// A site term uses m2 = 0, so veq is its Sz = -1/2 value and vne its +1/2 value.
+struct DiagTerm {
+  uint32_t m1, m2;
+  double veq, vne;
+};
+
+struct HvParams {
+  int N, Nlo, n_up;
+  int n_pairs;  // entries in low[] and rise[]
+  int n_diag;
+  uint32_t lomask;
+  // pairs in ascending-column order for a row: "low" flips (target < source)
+  // sorted by (hi desc, lo asc); "rise" flips (target > source) by (hi asc, lo desc)
+  PairTerm low[kMaxBonds];
+  PairTerm rise[kMaxBonds];
+  DiagTerm diag[kMaxDiag];
+};
+
+int build_hv_params(const Model& m, int Nlo, HvParams& P);
+
+// ---- basis tables ----------------------------------------------------------
+// Lin two-table ranking: rank(s) = thi[s >> Nlo] + tlo[s & lomask].
+struct BasisTables {
+  int N = 0, n_up = 0, Nlo = 0, Nhi = 0;
+  int64_t D = 0;
+  std::vector<uint32_t> thi;     // 2^Nhi: states before hi block h
+  std::vector<uint16_t> tlo;     // 2^Nlo: rank of l among same-popcount lo values
+  std::vector<uint16_t> lolist;  // 2^Nlo: lo values grouped by popcount, ascending
+  std::vector<uint32_t> looff;   // Nlo+2 offsets into lolist per popcount
+};
+
+int build_tables(int N, int n_up, BasisTables& t);
+
+// Work tiles over the sector: (hi block h, first row r0 within the block).
+void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr);
+
+// ---- tridiagonal / Tmatrix (host) ---------------------------------------------
+int tridiag_eigen(int n, double* d, double* e, double* zlast, double* zfull = nullptr);
+
+struct TmatInfo {
+  std::vector<double> evals, errs;  // distinct, non-ghost
+  std::vector<int> mults;
+  std::vector<int> first;           // index of each value in the sorted T spectrum
+  double thold = 0, multol = 0;
+};
+int tmatrix_analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
+                    TmatInfo& out);
+bool nlowest_converged(const TmatInfo& t, int nev, double rtol, double atol);
+
+// ---- parameters / lattices ----------------------------------------------------
+struct ParsedParams {
+  aed_param_info info;
+  std::vector<int> s1, s2;
+  std::vector<double> jz, jxy, kq, site_h, site_d;
+};
+int parse_parameters(const char* text, ParsedParams& out);
+
+}  // namespace aed

@@ -1,0 +1,501 @@
+// api.cpp -- the C ABI of libaed.so (declared in include/aed.h).
+
+#include <cstring>
+
+#include "handle.h"
+
+namespace aed {
+const char* last_error_cstr();
+
+namespace {
+
+template <typename T>
+int dev_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  const cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(AED_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return AED_OK;
+}
+
+void release(aed_handle* h) {
+  if (!h) return;
+  handle_release_workspace(h);
+  cudaFree(h->d_thi);
+  cudaFree(h->d_tlo);
+  cudaFree(h->d_lolist);
+  cudaFree(h->d_looff);
+  cudaFree(h->d_tile_h);
+  cudaFree(h->d_tile_r);
+  cudaFree(h->d_partA);
+  cudaFree(h->d_partB);
+  cudaFree(h->d_scal);
+  if (h->h_scal) cudaFreeHost(h->h_scal);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int check_vec(const aed_handle* h, const void* p, const char* name) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  if (!p) return fail(AED_ERR_INVALID, std::string(name) + " is NULL");
+  return AED_OK;
+}
+
+}  // namespace
+
+int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out) {
+  if (bytes > h->ws_bytes[slot]) {
+    if (h->ws[slot]) {
+      cudaStreamSynchronize(h->stream);
+      cudaFree(h->ws[slot]);
+    }
+    h->ws[slot] = nullptr;
+    h->ws_bytes[slot] = 0;
+    const cudaError_t e = cudaMalloc(&h->ws[slot], bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      h->ws[slot] = nullptr;
+      return fail(AED_ERR_NOMEM, std::string("workspace of ") + std::to_string(bytes) +
+                                     " bytes: " + cudaGetErrorString(e));
+    }
+    h->ws_bytes[slot] = bytes;
+  }
+  *out = h->ws[slot];
+  return AED_OK;
+}
+
+int handle_pinned(aed_handle* h, size_t n, double** out) {
+  if (n > h->h_ab_n) {
+    if (h->h_ab) cudaFreeHost(h->h_ab);
+    h->h_ab = nullptr;
+    h->h_ab_n = 0;
+    if (cudaMallocHost((void**)&h->h_ab, n * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      h->h_ab = nullptr;
+      return fail(AED_ERR_NOMEM, "pinned host allocation failed");
+    }
+    h->h_ab_n = n;
+  }
+  *out = h->h_ab;
+  return AED_OK;
+}
+
+void handle_release_workspace(aed_handle* h) {
+  for (int k = 0; k < 2; ++k) {
+    if (h->ws[k]) cudaFree(h->ws[k]);
+    h->ws[k] = nullptr;
+    h->ws_bytes[k] = 0;
+  }
+  if (h->h_ab) cudaFreeHost(h->h_ab);
+  h->h_ab = nullptr;
+  h->h_ab_n = 0;
+}
+
+int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+  if (f32)
+    return launch_hv_f32(h->P, h->dt, (const float*)x, (float*)y, alpha_part, h->hv_grid32, h->stream);
+  return launch_hv_f64(h->P, h->dt, (const double*)x, (double*)y, alpha_part, h->hv_grid64, h->stream);
+}
+
+}  // namespace aed
+
+using namespace aed;
+
+extern "C" {
+
+const char* aed_last_error(void) { return last_error_cstr(); }
+
+int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy,
+                         double* kq, double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity) {
+  if (!info) return fail(AED_ERR_INVALID, "info is NULL");
+  ParsedParams pp;
+  const int rc = parse_parameters(text, pp);
+  if (rc) return rc;
+  *info = pp.info;
+  const int nb = pp.info.n_bonds;
+  if (s1 || s2 || jz || jxy || kq) {
+    if (bond_capacity < nb) return fail(AED_ERR_INVALID, "bond_capacity too small");
+    for (int b = 0; b < nb; ++b) {
+      if (s1) s1[b] = pp.s1[b];
+      if (s2) s2[b] = pp.s2[b];
+      if (jz) jz[b] = pp.jz[b];
+      if (jxy) jxy[b] = pp.jxy[b];
+      if (kq) kq[b] = pp.kq[b];
+    }
+  }
+  if (site_h || site_d) {
+    if (site_capacity < pp.info.n_sites) return fail(AED_ERR_INVALID, "site_capacity too small");
+    for (int s = 0; s < pp.info.n_sites; ++s) {
+      if (site_h) site_h[s] = pp.site_h.empty() ? 0.0 : pp.site_h[s];
+      if (site_d) site_d[s] = pp.site_d.empty() ? 0.0 : pp.site_d[s];
+    }
+  }
+  return AED_OK;
+}
+
+int aed_create(const aed_model_desc* model, int precision, int device, aed_handle** out) {
+  if (!out) return fail(AED_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (precision != AED_FP64 && precision != AED_FP32) return fail(AED_ERR_INVALID, "precision must be AED_FP64 or AED_FP32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AED_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(AED_ERR_INVALID, "device index out of range");
+  DeviceGuard g(device);
+  aed_handle* h = new aed_handle;
+  h->device = device;
+  h->precision = precision;
+  int rc = model_from_desc(model, h->model);
+  if (!rc) rc = build_tables(h->model.N, h->model.n_up, h->tab);
+  if (!rc) rc = build_hv_params(h->model, h->tab.Nlo, h->P);
+  if (rc) {
+    release(h);
+    return rc;
+  }
+  std::vector<uint32_t> th, tr;
+  build_tiles(h->tab, kHvThreads, th, tr);
+  const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
+  if ((rc = dev_alloc(&h->d_thi, nhi)) || (rc = dev_alloc(&h->d_tlo, nlo)) || (rc = dev_alloc(&h->d_lolist, nlo)) ||
+      (rc = dev_alloc(&h->d_looff, h->tab.looff.size())) || (rc = dev_alloc(&h->d_tile_h, th.size())) ||
+      (rc = dev_alloc(&h->d_tile_r, tr.size())) || (rc = dev_alloc(&h->d_scal, 8))) {
+    release(h);
+    return rc;
+  }
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost((void**)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    release(h);
+    return fail(AED_ERR_CUDA, "stream / pinned memory creation failed");
+  }
+  h->hv_grid64 = hv_grid_size(false, 1);
+  h->hv_grid32 = hv_grid_size(true, 1);
+  h->red_grid = red_grid_size();
+  const int ga = h->hv_grid64 > h->hv_grid32 ? h->hv_grid64 : h->hv_grid32;
+  if ((rc = dev_alloc(&h->d_partA, ga)) || (rc = dev_alloc(&h->d_partB, h->red_grid))) {
+    release(h);
+    return rc;
+  }
+  cudaMemcpyAsync(h->d_thi, h->tab.thi.data(), nhi * 4, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_tlo, h->tab.tlo.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_lolist, h->tab.lolist.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_looff, h->tab.looff.data(), h->tab.looff.size() * 4, cudaMemcpyHostToDevice, h->stream);
+  if (!th.empty()) {
+    cudaMemcpyAsync(h->d_tile_h, th.data(), th.size() * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_tile_r, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice, h->stream);
+  }
+  const cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    release(h);
+    return fail(AED_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
+  }
+  DevTables& t = h->dt;
+  t.thi = h->d_thi;
+  t.tlo = h->d_tlo;
+  t.lolist = h->d_lolist;
+  t.looff = h->d_looff;
+  t.tile_h = h->d_tile_h;
+  t.tile_r = h->d_tile_r;
+  t.n_tiles = (int64_t)th.size();
+  t.D = h->tab.D;
+  t.Nlo = h->tab.Nlo;
+  t.Nhi = h->tab.Nhi;
+  t.n_up = h->tab.n_up;
+  *out = h;
+  return AED_OK;
+}
+
+int aed_destroy(aed_handle* h) {
+  if (!h) return AED_OK;
+  DeviceGuard g(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  release(h);
+  return AED_OK;
+}
+
+int aed_dimension(const aed_handle* h, int64_t* dim) {
+  if (!h || !dim) return fail(AED_ERR_INVALID, "NULL argument");
+  *dim = h->tab.D;
+  return AED_OK;
+}
+
+int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t count) {
+  if (!h || (!host_out && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
+  if (offset < 0 || count < 0 || offset + count > h->tab.D) return fail(AED_ERR_INVALID, "range outside the basis");
+  if (count == 0) return AED_OK;
+  DeviceGuard g(h->device);
+  uint32_t* d = nullptr;
+  int rc = dev_alloc(&d, (size_t)count);
+  if (rc) return rc;
+  rc = launch_basis_copy(h->dt, d, offset, count, h->stream);
+  if (!rc) {
+    cudaMemcpyAsync(host_out, d, count * 4, cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(AED_ERR_CUDA, std::string("basis copy: ") + cudaGetErrorString(e));
+  }
+  cudaFree(d);
+  return rc;
+}
+
+int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t* host_idx) {
+  if (!h || ((!host_states || !host_idx) && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
+  if (count <= 0) return AED_OK;
+  DeviceGuard g(h->device);
+  uint32_t* ds = nullptr;
+  int64_t* di = nullptr;
+  int rc = dev_alloc(&ds, (size_t)count);
+  if (!rc) rc = dev_alloc(&di, (size_t)count);
+  if (!rc) {
+    cudaMemcpyAsync(ds, host_states, count * 4, cudaMemcpyHostToDevice, h->stream);
+    rc = launch_rank(h->dt, h->model.N, ds, count, di, h->stream);
+    if (!rc) {
+      cudaMemcpyAsync(host_idx, di, count * 8, cudaMemcpyDeviceToHost, h->stream);
+      const cudaError_t e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess) rc = fail(AED_ERR_CUDA, std::string("index: ") + cudaGetErrorString(e));
+    }
+  }
+  cudaFree(ds);
+  cudaFree(di);
+  return rc;
+}
+
+int aed_vec_alloc(aed_handle* h, void** v) {
+  if (!h || !v) return fail(AED_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  const size_t bytes = (size_t)h->tab.D * h->elem_size();
+  const cudaError_t e = cudaMalloc(v, bytes ? bytes : 8);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *v = nullptr;
+    return fail(AED_ERR_NOMEM, std::string("vector allocation: ") + cudaGetErrorString(e));
+  }
+  AED_CUDA_TRY(cudaMemsetAsync(*v, 0, bytes, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
+int aed_vec_free(aed_handle* h, void* v) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  AED_CUDA_TRY(cudaFree(v));
+  return AED_OK;
+}
+
+int aed_vec_upload(aed_handle* h, void* v, const double* host) {
+  int rc = check_vec(h, v, "vector");
+  if (rc) return rc;
+  if (!host) return fail(AED_ERR_INVALID, "host is NULL");
+  DeviceGuard g(h->device);
+  const int64_t D = h->tab.D;
+  if (h->precision == AED_FP64) {
+    AED_CUDA_TRY(cudaMemcpyAsync(v, host, D * 8, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    std::vector<float> tmp(D);
+    for (int64_t i = 0; i < D; ++i) tmp[i] = (float)host[i];
+    AED_CUDA_TRY(cudaMemcpyAsync(v, tmp.data(), D * 4, cudaMemcpyHostToDevice, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
+int aed_vec_download(aed_handle* h, const void* v, double* host) {
+  int rc = check_vec(h, v, "vector");
+  if (rc) return rc;
+  if (!host) return fail(AED_ERR_INVALID, "host is NULL");
+  DeviceGuard g(h->device);
+  const int64_t D = h->tab.D;
+  if (h->precision == AED_FP64) {
+    AED_CUDA_TRY(cudaMemcpyAsync(host, v, D * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> tmp(D);
+    AED_CUDA_TRY(cudaMemcpyAsync(tmp.data(), v, D * 4, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t i = 0; i < D; ++i) host[i] = tmp[i];
+  }
+  return AED_OK;
+}
+
+int aed_vec_copy(aed_handle* h, const void* x, void* y) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  AED_CUDA_TRY(cudaMemcpyAsync(y, x, h->tab.D * h->elem_size(), cudaMemcpyDeviceToDevice, h->stream));
+  return AED_OK;
+}
+
+int aed_vec_clear(aed_handle* h, void* x) {
+  int rc = check_vec(h, x, "x");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  AED_CUDA_TRY(cudaMemsetAsync(x, 0, h->tab.D * h->elem_size(), h->stream));
+  return AED_OK;
+}
+
+int aed_vec_fill_random(aed_handle* h, void* x, uint64_t seed) {
+  int rc = check_vec(h, x, "x");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (h->precision == AED_FP64) return launch_fill_random((double*)x, h->tab.D, seed, h->stream);
+  return launch_fill_random((float*)x, h->tab.D, seed, h->stream);
+}
+
+int aed_mult(aed_handle* h, const void* x, void* y) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  if (x == y) return fail(AED_ERR_INVALID, "x and y must not alias");
+  DeviceGuard g(h->device);
+  return handle_hv(h, h->precision == AED_FP32, x, y, nullptr);
+}
+
+static int reduce_to_host(aed_handle* h, const void* x, const void* y, bool sq, bool take_sqrt, double* out) {
+  int rc;
+  if (h->precision == AED_FP64)
+    rc = launch_dot_partials((const double*)x, (const double*)y, h->tab.D, h->d_partB, h->red_grid, sq, h->stream);
+  else
+    rc = launch_dot_partials((const float*)x, (const float*)y, h->tab.D, h->d_partB, h->red_grid, sq, h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, h->red_grid, h->d_scal, take_sqrt, h->stream);
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->d_scal, 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = h->h_scal[0];
+  return AED_OK;
+}
+
+int aed_dot(aed_handle* h, const void* x, const void* y, double* out) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  if (!out) return fail(AED_ERR_INVALID, "out is NULL");
+  DeviceGuard g(h->device);
+  return reduce_to_host(h, x, y, false, false, out);
+}
+
+int aed_nrm2(aed_handle* h, const void* x, double* out) {
+  int rc = check_vec(h, x, "x");
+  if (rc) return rc;
+  if (!out) return fail(AED_ERR_INVALID, "out is NULL");
+  DeviceGuard g(h->device);
+  return reduce_to_host(h, x, x, true, true, out);
+}
+
+int aed_axpy(aed_handle* h, double a, const void* x, void* y) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (h->precision == AED_FP64) return launch_axpy(a, (const double*)x, (double*)y, h->tab.D, h->stream);
+  return launch_axpy(a, (const float*)x, (float*)y, h->tab.D, h->stream);
+}
+
+int aed_scal(aed_handle* h, double a, void* x) {
+  int rc = check_vec(h, x, "x");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->tab.D, false, h->stream);
+  return launch_scal(a, (float*)x, h->tab.D, false, h->stream);
+}
+
+int aed_div(aed_handle* h, double a, void* x) {
+  int rc = check_vec(h, x, "x");
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->tab.D, true, h->stream);
+  return launch_scal(a, (float*)x, h->tab.D, true, h->stream);
+}
+
+int aed_lanczos_step(aed_handle* h, const void* v_prev, const void* v_cur, void* v_next, double beta_prev,
+                     double* alpha, double* beta) {
+  int rc = check_vec(h, v_cur, "v_cur");
+  if (!rc) rc = check_vec(h, v_next, "v_next");
+  if (rc) return rc;
+  if (v_cur == v_next || (v_prev && (v_prev == v_cur || v_prev == v_next)))
+    return fail(AED_ERR_INVALID, "Lanczos vectors must not alias");
+  DeviceGuard g(h->device);
+  const bool f32 = h->precision == AED_FP32;
+  const int nA = f32 ? h->hv_grid32 : h->hv_grid64;
+  h->h_scal[4] = beta_prev;
+  AED_CUDA_TRY(cudaMemcpyAsync(h->d_scal + 4, h->h_scal + 4, 8, cudaMemcpyHostToDevice, h->stream));
+  rc = handle_hv(h, f32, v_cur, v_next, h->d_partA);
+  if (rc) return rc;
+  if (f32) {
+    rc = launch_lanczos_update((const double*)h->d_partA, nA, (const float*)v_cur, (const float*)v_prev,
+                               h->d_scal + 4, (float*)v_next, h->tab.D, h->d_partB, h->red_grid, h->d_scal + 0,
+                               h->stream);
+    if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (float*)v_next, h->tab.D, h->d_scal + 1,
+                                           h->red_grid, h->stream);
+  } else {
+    rc = launch_lanczos_update((const double*)h->d_partA, nA, (const double*)v_cur, (const double*)v_prev,
+                               h->d_scal + 4, (double*)v_next, h->tab.D, h->d_partB, h->red_grid, h->d_scal + 0,
+                               h->stream);
+    if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (double*)v_next, h->tab.D, h->d_scal + 1,
+                                           h->red_grid, h->stream);
+  }
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->d_scal, 16, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (alpha) *alpha = h->h_scal[0];
+  if (beta) *beta = h->h_scal[1];
+  return AED_OK;
+}
+
+int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res) {
+  if (!h || !opts || !res) return fail(AED_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  return solve(h, opts, res);
+}
+
+int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n) {
+  if (!h || !n) return fail(AED_ERR_INVALID, "NULL argument");
+  *n = (int32_t)h->last_alpha.size();
+  for (int32_t i = 0; i < *n && i < cap; ++i) {
+    if (alpha) alpha[i] = h->last_alpha[i];
+    if (beta) beta[i] = h->last_beta[i];
+  }
+  return AED_OK;
+}
+
+int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  if (reps < 1 || !ms) return fail(AED_ERR_INVALID, "reps must be >= 1 and ms non-NULL");
+  DeviceGuard g(h->device);
+  cudaEvent_t e0, e1;
+  AED_CUDA_TRY(cudaEventCreate(&e0));
+  AED_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEventRecord(e0, h->stream);
+  for (int r = 0; r < reps && !rc; ++r) rc = handle_hv(h, h->precision == AED_FP32, x, y, nullptr);
+  cudaEventRecord(e1, h->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  *ms = (double)t / reps;
+  return AED_OK;
+}
+
+int aed_get_stream(aed_handle* h, void** stream) {
+  if (!h || !stream) return fail(AED_ERR_INVALID, "NULL argument");
+  *stream = (void*)h->stream;
+  return AED_OK;
+}
+
+int aed_launch_count(int64_t* count) {
+  if (!count) return fail(AED_ERR_INVALID, "NULL argument");
+  *count = launch_count();
+  return AED_OK;
+}
+
+}  // extern "C"

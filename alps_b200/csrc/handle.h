@@ -1,0 +1,65 @@
+// handle.h -- the engine handle behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "aed_internal.h"
+#include "kernels.cuh"
+
+struct aed_handle {
+  int device = 0;
+  int precision = AED_FP64;
+  cudaStream_t stream = nullptr;
+  aed::Model model;
+  aed::HvParams P;
+  aed::BasisTables tab;
+  aed::DevTables dt;
+  // device memory
+  uint32_t* d_thi = nullptr;
+  uint16_t* d_tlo = nullptr;
+  uint16_t* d_lolist = nullptr;
+  uint32_t* d_looff = nullptr;
+  uint32_t* d_tile_h = nullptr;
+  uint32_t* d_tile_r = nullptr;
+  double* d_partA = nullptr;  // hv_grid partial sums
+  double* d_partB = nullptr;  // red_grid partial sums
+  double* d_scal = nullptr;   // 8 device scalars
+  double* h_scal = nullptr;   // 8 pinned host scalars
+  int hv_grid32 = 0, hv_grid64 = 0, red_grid = 0;
+  size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }
+  // solve workspaces, kept between solves (grown on demand): slot 0 = FP64
+  // recurrence, slot 1 = FP32 Lanczos basis store of the mixed path
+  void* ws[2] = {nullptr, nullptr};
+  size_t ws_bytes[2] = {0, 0};
+  double* h_ab = nullptr;  // pinned alpha/beta staging
+  size_t h_ab_n = 0;
+  // last solve
+  std::vector<double> last_alpha, last_beta;
+};
+
+namespace aed {
+
+// RAII device switch for an API call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
+// Workspace of at least `bytes` device bytes / `n` pinned doubles, reused across solves.
+int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out);
+int handle_pinned(aed_handle* h, size_t n, double** out);
+void handle_release_workspace(aed_handle* h);
+int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r);
+
+}  // namespace aed

@@ -1,0 +1,464 @@
+// kernels.cu -- sm_100a kernels of the exact-diagonalisation engine.
+//
+// The apply y = H x is matrix-free: each thread owns one row (one basis
+// state s), walks the coupling tables held in the kernel's parameter space and
+// gathers x at the rank of every reachable state s' = s ^ (bit pair).  Ranks
+// come from the two-table (Lin) scheme rank(s) = thi[s >> Nlo] + tlo[s & lomask].
+// No tensor cores: the apply is a bandwidth-bound gather.
+//
+// Reference paths are relative to the ALPS source tree.
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "kernels.cuh"
+
+namespace aed {
+namespace {
+
+__device__ __forceinline__ uint32_t rank_of(uint32_t s, int Nlo, uint32_t lomask, const uint32_t* __restrict__ thi,
+                                            const uint16_t* __restrict__ tlo) {
+  return __ldg(thi + (s >> Nlo)) + (uint32_t)__ldg(tlo + (s & lomask));
+}
+
+// Fixed-shape block reduction: warp shuffles, then warp 0 over the warp sums.
+// Same order on every call, so the result is bitwise reproducible.  The
+// total is returned to every thread.
+template <int NT>
+__device__ __forceinline__ double block_sum_all(double v, double* sm) {
+  static_assert(NT % 32 == 0 && NT <= 1024, "block size");
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sm[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double r = (l < NT / 32) ? sm[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    if (l == 0) sm[32] = r;
+  }
+  __syncthreads();
+  const double r = sm[32];
+  __syncthreads();
+  return r;
+}
+
+// Sum of n partials in a fixed order (thread-strided, then block_sum_all).
+template <int NT>
+__device__ __forceinline__ double sum_partials(const double* __restrict__ p, int n, double* sm) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += NT) v += p[i];
+  return block_sum_all<NT>(v, sm);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 row: bit-identical to y = prod(M, x) over the reference's explicit
+// matrix (src/ietl/interface/ublas.h:57-63 over hamiltonian_matrix.hpp:307-345).
+// A row of M holds the flips to smaller states (ascending column = hi bit
+// descending, then lo bit ascending), the diagonal M(i,i), then the flips to
+// larger states (hi ascending, lo descending).  Products and sums round
+// separately (__dmul_rn/__dadd_rn: no FMA contraction), as on the reference's
+// x86-64 build.  M(i,i) is accumulated in the reference's term order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double row_f64(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* __restrict__ thi,
+                                          const uint16_t* __restrict__ tlo, const double* __restrict__ x) {
+  const int Nlo = P.Nlo;
+  const uint32_t lm = P.lomask;
+  double acc = 0.0;
+  for (int q = 0; q < P.n_pairs; ++q) {
+    const uint32_t mh = P.low[q].mhi, ml = P.low[q].mlo;
+    if ((s & (mh | ml)) == mh) {
+      const double xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
+      acc = __dadd_rn(acc, __dmul_rn(P.low[q].c, xv));
+    }
+  }
+  double d = 0.0;
+  for (int q = 0; q < P.n_diag; ++q) {
+    const bool eq = ((s & P.diag[q].m1) != 0u) == ((s & P.diag[q].m2) != 0u);
+    d = __dadd_rn(d, eq ? P.diag[q].veq : P.diag[q].vne);
+  }
+  acc = __dadd_rn(acc, __dmul_rn(d, __ldg(x + i)));
+  for (int q = 0; q < P.n_pairs; ++q) {
+    const uint32_t mh = P.rise[q].mhi, ml = P.rise[q].mlo;
+    if ((s & (mh | ml)) == ml) {
+      const double xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
+      acc = __dadd_rn(acc, __dmul_rn(P.rise[q].c, xv));
+    }
+  }
+  return acc;
+}
+
+// Error-free transformations: TwoSum (Knuth, TAOCP Vol. 2, 4.2.2) and the
+// FMA-based exact product error.  Compensated row sum in the style of
+// Ogita, Rump & Oishi (SIAM J. Sci. Comput. 26 (2005)) "Dot2".
+struct Comp32 {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add_prod(float a_hi, float a_lo, float xv) {
+    const float p = __fmul_rn(a_hi, xv);
+    const float pe = __fmaf_rn(a_hi, xv, -p);  // exact: a_hi*xv - p
+    const float t = __fadd_rn(s, p);
+    const float bb = __fsub_rn(t, s);
+    const float se = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(p, bb));
+    s = t;
+    c = __fadd_rn(c, __fadd_rn(se, __fmaf_rn(a_lo, xv, pe)));
+  }
+  __device__ __forceinline__ float value() const { return __fadd_rn(s, c); }
+};
+
+// FP32 row with compensated accumulation; order of terms is free here.
+__device__ __forceinline__ float row_f32(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* __restrict__ thi,
+                                         const uint16_t* __restrict__ tlo, const float* __restrict__ x) {
+  const int Nlo = P.Nlo;
+  const uint32_t lm = P.lomask;
+  Comp32 acc;
+  double d = 0.0;
+  for (int q = 0; q < P.n_diag; ++q) {
+    const bool eq = ((s & P.diag[q].m1) != 0u) == ((s & P.diag[q].m2) != 0u);
+    d += eq ? P.diag[q].veq : P.diag[q].vne;
+  }
+  {
+    const float dh = (float)d, dl = (float)(d - (double)dh);
+    acc.add_prod(dh, dl, __ldg(x + i));
+  }
+  for (int q = 0; q < P.n_pairs; ++q) {
+    const uint32_t mh = P.low[q].mhi, ml = P.low[q].mlo;
+    const uint32_t b = s & (mh | ml);
+    if (b == mh || b == ml) {
+      const float xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
+      acc.add_prod(P.low[q].chi, P.low[q].clo, xv);
+    }
+  }
+  return acc.value();
+}
+
+template <typename T>
+__device__ __forceinline__ T row_value(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
+                                       const uint16_t* tlo, const T* x);
+template <>
+__device__ __forceinline__ double row_value<double>(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
+                                                    const uint16_t* tlo, const double* x) {
+  return row_f64(P, s, i, thi, tlo, x);
+}
+template <>
+__device__ __forceinline__ float row_value<float>(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
+                                                  const uint16_t* tlo, const float* x) {
+  return row_f32(P, s, i, thi, tlo, x);
+}
+
+// y = H x over tiles (hi block h, rows r0 .. r0+kHvThreads-1).  CTAs take
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ...: a static assignment, so the
+// per-CTA partial sums of x_i*y_i (for the fused Lanczos step) are
+// reproducible bit for bit.
+template <typename T>
+__global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ HvParams P, const DevTables t,
+                                                        const T* __restrict__ x, T* __restrict__ y,
+                                                        double* __restrict__ alpha_part) {
+  __shared__ double sm[33];
+  double dotacc = 0.0;
+  for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
+    const uint32_t h = __ldg(t.tile_h + it);
+    const uint32_t r = __ldg(t.tile_r + it) + threadIdx.x;
+    const int k = P.n_up - __popc(h);
+    const uint32_t base = __ldg(t.looff + k);
+    const uint32_t rows = __ldg(t.looff + k + 1) - base;
+    if (r < rows) {
+      const uint32_t l = __ldg(t.lolist + base + r);
+      const uint32_t s = (h << P.Nlo) | l;
+      const uint32_t i = __ldg(t.thi + h) + r;
+      const T v = row_value<T>(P, s, i, t.thi, t.tlo, x);
+      y[i] = v;
+      if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
+    }
+  }
+  if (alpha_part) {
+    const double tot = block_sum_all<kHvThreads>(dotacc, sm);
+    if (threadIdx.x == 0) alpha_part[blockIdx.x] = tot;
+  }
+}
+
+// basis_states order (basisstates.h:175-278) from the tables: row idx lies in
+// the hi block h with the largest thi[h] <= idx.
+__global__ void basis_copy_kernel(const DevTables t, uint32_t* __restrict__ out, int64_t offset, int64_t count) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= count) return;
+  const uint32_t idx = (uint32_t)(offset + n);
+  uint32_t lo = 0, hi = (1u << t.Nhi) - 1u;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    if (t.thi[mid] <= idx)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const uint32_t h = lo;
+  const uint32_t r = idx - t.thi[h];
+  const int k = t.n_up - __popc(h);
+  out[n] = (h << t.Nlo) | t.lolist[t.looff[k] + r];
+}
+
+// basis_states::index (basisstates.h:68-74): D when the state is not in the sector.
+__global__ void rank_kernel(const DevTables t, int N, const uint32_t* __restrict__ st, int64_t count,
+                            int64_t* __restrict__ out) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= count) return;
+  const uint32_t s = st[n];
+  const bool outside = (N < 32 && (s >> N) != 0u) || __popc(s) != t.n_up;
+  out[n] = outside ? t.D : (int64_t)(t.thi[s >> t.Nlo] + t.tlo[s & ((1u << t.Nlo) - 1u)]);
+}
+
+// splitmix64 (Steele, Lea & Flood, OOPSLA 2014)
+__device__ __forceinline__ uint64_t splitmix64(uint64_t seed, uint64_t i) {
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void fill_random_kernel(T* __restrict__ x, int64_t n, uint64_t seed) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t z = splitmix64(seed, (uint64_t)i);
+    if constexpr (sizeof(T) == 8)
+      x[i] = (double)(z >> 11) * 0x1.0p-53;
+    else
+      x[i] = (float)((double)(z >> 40) * 0x1.0p-24);
+  }
+}
+
+template <typename T>
+__global__ void copy_kernel(const T* __restrict__ x, T* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+
+// y += a*x, as ublas evaluates v += s*w: the product rounds, then the sum.
+template <typename T>
+__global__ void axpy_kernel(double a, const T* __restrict__ x, T* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (T)__dadd_rn((double)y[i], __dmul_rn(a, (double)x[i]));
+}
+
+template <typename T>
+__global__ void scal_kernel(double a, T* __restrict__ x, int64_t n, bool divide) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (T)(divide ? __ddiv_rn((double)x[i], a) : __dmul_rn((double)x[i], a));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) dot_partials_kernel(const T* __restrict__ x, const T* __restrict__ y,
+                                                                  int64_t n, double* __restrict__ part, bool sq) {
+  __shared__ double sm[33];
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
+    const double a = (double)x[i];
+    acc = fma(a, sq ? a : (double)y[i], acc);
+  }
+  const double tot = block_sum_all<kRedThreads>(acc, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kRedThreads) finish_sum_kernel(const double* __restrict__ part, int n,
+                                                                 double* __restrict__ out, bool take_sqrt) {
+  __shared__ double sm[33];
+  const double tot = sum_partials<kRedThreads>(part, n, sm);
+  if (threadIdx.x == 0) *out = take_sqrt ? sqrt(tot) : tot;
+}
+
+// make_step middle part (lanczos.h:398-401): a = dot(v, Hv); w -= a v; w -= b v_prev; |w|^2
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const double* __restrict__ partA, int nA,
+                                                                    const T* __restrict__ x,
+                                                                    const T* __restrict__ vprev,
+                                                                    const double* __restrict__ beta_prev,
+                                                                    T* __restrict__ y, int64_t n,
+                                                                    double* __restrict__ partB,
+                                                                    double* __restrict__ alpha_out) {
+  __shared__ double sm[33];
+  const double alpha = sum_partials<kRedThreads>(partA, nA, sm);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *alpha_out = alpha;
+  const double b = vprev ? *beta_prev : 0.0;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
+    double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
+    if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
+    const T wt = (T)w;
+    y[i] = wt;
+    acc = fma((double)wt, (double)wt, acc);
+  }
+  const double tot = block_sum_all<kRedThreads>(acc, sm);
+  if (threadIdx.x == 0) partB[blockIdx.x] = tot;
+}
+
+// make_step tail (lanczos.h:401-402): b = |w|; w /= b
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const double* __restrict__ partB, int nB,
+                                                                       T* __restrict__ y, int64_t n,
+                                                                       double* __restrict__ beta_out) {
+  __shared__ double sm[33];
+  const double beta = sqrt(sum_partials<kRedThreads>(partB, nB, sm));
+  if (blockIdx.x == 0 && threadIdx.x == 0 && beta_out) *beta_out = beta;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    y[i] = (T)__ddiv_rn((double)y[i], beta);
+}
+
+// Ritz vector from the stored FP32 Lanczos basis, accumulated in FP64.
+// Each thread owns elements i (coalesced across the warp) and walks the m
+// stored vectors; coefficients are staged in shared memory in chunks.
+__global__ void __launch_bounds__(256) ritz_combine_kernel(const float* __restrict__ V, int64_t ld, int m,
+                                                          const double* __restrict__ coef, double* __restrict__ out,
+                                                          int64_t n) {
+  __shared__ double cs[512];
+  const int64_t stride = (int64_t)gridDim.x * 256;
+  for (int64_t base = (int64_t)blockIdx.x * 256; base < n; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    double acc = 0.0;
+    for (int j0 = 0; j0 < m; j0 += 512) {
+      const int cnt = min(512, m - j0);
+      __syncthreads();
+      for (int q = threadIdx.x; q < cnt; q += 256) cs[q] = coef[j0 + q];
+      __syncthreads();
+      if (i < n)
+        for (int q = 0; q < cnt; ++q) acc = fma(cs[q], (double)__ldg(V + (int64_t)(j0 + q) * ld + i), acc);
+    }
+    if (i < n) out[i] = acc;
+  }
+}
+
+int g_num_sms = 0;
+std::atomic<int64_t> g_launches{0};
+
+int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+inline int elem_grid(int64_t n) {
+  const int64_t want = (n + 255) / 256;
+  const int64_t cap = (int64_t)num_sms() * 8;
+  return (int)(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+inline int check_launch(const char* what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(AED_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return AED_OK;
+}
+
+}  // namespace
+
+int red_grid_size() { return num_sms() * 4; }
+
+int64_t launch_count() { return g_launches.load(); }
+
+int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
+                        cudaStream_t st) {
+  if (m < 1 || m > kMaxRitzTerms) return fail(AED_ERR_INVALID, "ritz_combine: bad number of terms");
+  ritz_combine_kernel<<<elem_grid(n), 256, 0, st>>>(V, ld, m, coef, out, n);
+  return check_launch("ritz_combine_kernel");
+}
+
+int hv_grid_size(bool f32, int) {
+  int per_sm = 0;
+  if (f32)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<float>, kHvThreads, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<double>, kHvThreads, 0);
+  if (per_sm < 1) per_sm = 1;
+  return num_sms() * per_sm;
+}
+
+int launch_hv_f64(const HvParams& P, const DevTables& t, const double* x, double* y, double* alpha_part, int grid,
+                  cudaStream_t st) {
+  if (t.n_tiles == 0) return AED_OK;
+  hv_kernel<double><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
+  return check_launch("hv_kernel<double>");
+}
+
+int launch_hv_f32(const HvParams& P, const DevTables& t, const float* x, float* y, double* alpha_part, int grid,
+                  cudaStream_t st) {
+  if (t.n_tiles == 0) return AED_OK;
+  hv_kernel<float><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
+  return check_launch("hv_kernel<float>");
+}
+
+int launch_basis_copy(const DevTables& t, uint32_t* out, int64_t offset, int64_t count, cudaStream_t st) {
+  if (count <= 0) return AED_OK;
+  basis_copy_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(t, out, offset, count);
+  return check_launch("basis_copy_kernel");
+}
+
+int launch_rank(const DevTables& t, int N, const uint32_t* states, int64_t count, int64_t* out, cudaStream_t st) {
+  if (count <= 0) return AED_OK;
+  rank_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(t, N, states, count, out);
+  return check_launch("rank_kernel");
+}
+
+template <typename T>
+int launch_fill_random(T* x, int64_t n, uint64_t seed, cudaStream_t st) {
+  fill_random_kernel<T><<<elem_grid(n), 256, 0, st>>>(x, n, seed);
+  return check_launch("fill_random_kernel");
+}
+
+template <typename T>
+int launch_copy(const T* x, T* y, int64_t n, cudaStream_t st) {
+  copy_kernel<T><<<elem_grid(n), 256, 0, st>>>(x, y, n);
+  return check_launch("copy_kernel");
+}
+
+template <typename T>
+int launch_axpy(double a, const T* x, T* y, int64_t n, cudaStream_t st) {
+  axpy_kernel<T><<<elem_grid(n), 256, 0, st>>>(a, x, y, n);
+  return check_launch("axpy_kernel");
+}
+
+template <typename T>
+int launch_scal(double a, T* x, int64_t n, bool divide, cudaStream_t st) {
+  scal_kernel<T><<<elem_grid(n), 256, 0, st>>>(a, x, n, divide);
+  return check_launch("scal_kernel");
+}
+
+template <typename T>
+int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, int grid, bool sq, cudaStream_t st) {
+  dot_partials_kernel<T><<<grid, kRedThreads, 0, st>>>(x, y, n, part, sq);
+  return check_launch("dot_partials_kernel");
+}
+
+int launch_finish_sum(const double* part, int n, double* out, bool take_sqrt, cudaStream_t st) {
+  finish_sum_kernel<<<1, kRedThreads, 0, st>>>(part, n, out, take_sqrt);
+  return check_launch("finish_sum_kernel");
+}
+
+template <typename T>
+int launch_lanczos_update(const double* partA, int nA, const T* x, const T* vprev, const double* beta_prev, T* y,
+                          int64_t n, double* partB, int gridB, double* alpha_out, cudaStream_t st) {
+  lanczos_update_kernel<T><<<gridB, kRedThreads, 0, st>>>(partA, nA, x, vprev, beta_prev, y, n, partB, alpha_out);
+  return check_launch("lanczos_update_kernel");
+}
+
+template <typename T>
+int launch_lanczos_normalize(const double* partB, int nB, T* y, int64_t n, double* beta_out, int grid,
+                             cudaStream_t st) {
+  lanczos_normalize_kernel<T><<<grid, kRedThreads, 0, st>>>(partB, nB, y, n, beta_out);
+  return check_launch("lanczos_normalize_kernel");
+}
+
+#define AED_INST(T)                                                                                          \
+  template int launch_fill_random<T>(T*, int64_t, uint64_t, cudaStream_t);                                   \
+  template int launch_copy<T>(const T*, T*, int64_t, cudaStream_t);                                          \
+  template int launch_axpy<T>(double, const T*, T*, int64_t, cudaStream_t);                                  \
+  template int launch_scal<T>(double, T*, int64_t, bool, cudaStream_t);                                      \
+  template int launch_dot_partials<T>(const T*, const T*, int64_t, double*, int, bool, cudaStream_t);        \
+  template int launch_lanczos_update<T>(const double*, int, const T*, const T*, const double*, T*, int64_t, \
+                                        double*, int, double*, cudaStream_t);                               \
+  template int launch_lanczos_normalize<T>(const double*, int, T*, int64_t, double*, int, cudaStream_t);
+AED_INST(double)
+AED_INST(float)
+#undef AED_INST
+
+}  // namespace aed

@@ -1,0 +1,546 @@
+// model.cpp -- model description, coupling tables, basis tables, parameter surface.
+//
+// Reference paths are relative to the ALPS source tree.
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+
+#include "aed_internal.h"
+
+namespace aed {
+
+// ---- errors ------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+// ---- model ---------------------------------------------------------------------
+int model_from_desc(const aed_model_desc* d, Model& m) {
+  if (!d) return fail(AED_ERR_INVALID, "model is NULL");
+  if (d->n_sites < 2 || d->n_sites > 32) return fail(AED_ERR_INVALID, "n_sites must be in 2..32");
+  if (d->n_up < 0 || d->n_up > d->n_sites) return fail(AED_ERR_INVALID, "n_up out of range");
+  if (d->n_bonds < 0 || d->n_bonds > kMaxBonds) return fail(AED_ERR_INVALID, "n_bonds must be in 0..128");
+  if (d->n_bonds > 0 && (!d->bond_s1 || !d->bond_s2 || !d->bond_jz || !d->bond_jxy))
+    return fail(AED_ERR_INVALID, "bond arrays are NULL");
+  m = Model();
+  m.N = d->n_sites;
+  m.n_up = d->n_up;
+  for (int b = 0; b < d->n_bonds; ++b) {
+    const int a = d->bond_s1[b], c = d->bond_s2[b];
+    if (a < 0 || a >= m.N || c < 0 || c >= m.N || a == c)
+      return fail(AED_ERR_INVALID, "bond " + std::to_string(b) + " has invalid sites");
+    const double jz = d->bond_jz[b], jxy = d->bond_jxy[b], k = d->bond_k ? d->bond_k[b] : 0.0;
+    if (!std::isfinite(jz) || !std::isfinite(jxy) || !std::isfinite(k))
+      return fail(AED_ERR_INVALID, "bond " + std::to_string(b) + " has a non-finite coupling");
+    m.s1.push_back(a);
+    m.s2.push_back(c);
+    m.jz.push_back(jz);
+    m.jxy.push_back(jxy);
+    m.kq.push_back(k);
+  }
+  if (d->site_h || d->site_d) {
+    m.site_h.assign(m.N, 0.0);
+    m.site_d.assign(m.N, 0.0);
+    for (int s = 0; s < m.N; ++s) {
+      if (d->site_h) m.site_h[s] = d->site_h[s];
+      if (d->site_d) m.site_d[s] = d->site_d[s];
+      if (!std::isfinite(m.site_h[s]) || !std::isfinite(m.site_d[s]))
+        return fail(AED_ERR_INVALID, "non-finite site term");
+    }
+  }
+  return AED_OK;
+}
+
+// Matrix elements of the spin-1/2 "spin" HAMILTONIAN (lib/xml/models.xml.in:342-373)
+// as the reference's model library evaluates them (test/model/example3.output):
+// site  Sz=-1/2: 0.25*D + 0.5*h;   Sz=+1/2: 0.25*D - 0.5*h
+// bond  parallel: 0.25*Jz + 0.0625*K;  antiparallel: -0.25*Jz + 0.3125*K;
+//       flip: 0.5*Jxy - 0.25*K
+int build_hv_params(const Model& m, int Nlo, HvParams& P) {
+  std::memset(&P, 0, sizeof P);
+  P.N = m.N;
+  P.Nlo = Nlo;
+  P.n_up = m.n_up;
+  P.lomask = (Nlo >= 32) ? 0xffffffffu : ((1u << Nlo) - 1u);
+  const int nb = (int)m.s1.size();
+  // diagonal terms in the reference's order: sites, then bonds
+  // (hamiltonian_matrix.hpp:387-397); zero elements are skipped by
+  // numeric::is_nonzero (hamiltonian_matrix.hpp:277,317) and adding +0.0 to
+  // the accumulator is exact, so zero terms are simply dropped.
+  int nd = 0;
+  if (!m.site_h.empty()) {
+    for (int s = 0; s < m.N; ++s) {
+      const double vdown = 0.25 * m.site_d[s] + 0.5 * m.site_h[s];
+      const double vup = 0.25 * m.site_d[s] - 0.5 * m.site_h[s];
+      if (vdown == 0.0 && vup == 0.0) continue;
+      if (nd >= kMaxDiag) return fail(AED_ERR_INVALID, "too many diagonal terms");
+      P.diag[nd++] = {1u << (m.N - 1 - s), 0u, vdown, vup};
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    const double par = 0.25 * m.jz[b] + 0.0625 * m.kq[b];
+    const double anti = -0.25 * m.jz[b] + 0.3125 * m.kq[b];
+    if (par == 0.0 && anti == 0.0) continue;
+    if (nd >= kMaxDiag) return fail(AED_ERR_INVALID, "too many diagonal terms");
+    P.diag[nd++] = {1u << (m.N - 1 - m.s1[b]), 1u << (m.N - 1 - m.s2[b]), par, anti};
+  }
+  P.n_diag = nd;
+  // flip pairs, merged over bonds joining the same two sites in bond order
+  // (matrix_as_vector.hpp:72-73 accumulates M(i,j) += v starting from 0)
+  std::vector<PairTerm> pairs;
+  for (int b = 0; b < nb; ++b) {
+    const double flip = 0.5 * m.jxy[b] - 0.25 * m.kq[b];
+    if (flip == 0.0) continue;
+    uint32_t ma = 1u << (m.N - 1 - m.s1[b]), mb = 1u << (m.N - 1 - m.s2[b]);
+    const uint32_t mhi = std::max(ma, mb), mlo = std::min(ma, mb);
+    bool merged = false;
+    for (auto& p : pairs)
+      if (p.mhi == mhi && p.mlo == mlo) {
+        p.c += flip;
+        merged = true;
+        break;
+      }
+    if (!merged) pairs.push_back({mhi, mlo, 0.0 + flip, 0.f, 0.f});
+  }
+  for (auto& p : pairs) {
+    p.chi = (float)p.c;
+    p.clo = (float)(p.c - (double)p.chi);
+  }
+  P.n_pairs = (int)pairs.size();
+  std::vector<PairTerm> low = pairs, rise = pairs;
+  // target < source (hi bit 1 -> 0): s' = s - 2^hi + 2^lo, ascending in
+  // s' means hi descending, then lo ascending
+  std::sort(low.begin(), low.end(), [](const PairTerm& a, const PairTerm& b) {
+    return a.mhi != b.mhi ? a.mhi > b.mhi : a.mlo < b.mlo;
+  });
+  // target > source: s' = s + 2^hi - 2^lo, ascending means hi ascending, then lo descending
+  std::sort(rise.begin(), rise.end(), [](const PairTerm& a, const PairTerm& b) {
+    return a.mhi != b.mhi ? a.mhi < b.mhi : a.mlo > b.mlo;
+  });
+  for (int i = 0; i < P.n_pairs; ++i) {
+    P.low[i] = low[i];
+    P.rise[i] = rise[i];
+  }
+  return AED_OK;
+}
+
+// ---- basis tables (Lin 1990 two-table ranking) -----------------------------------
+static inline int popc32(uint32_t v) { return __builtin_popcount(v); }
+
+int build_tables(int N, int n_up, BasisTables& t) {
+  if (N < 2 || N > 32 || n_up < 0 || n_up > N) return fail(AED_ERR_INVALID, "bad sector");
+  t = BasisTables();
+  t.N = N;
+  t.n_up = n_up;
+  t.Nlo = (N + 1) / 2;
+  t.Nhi = N - t.Nlo;
+  if (t.Nlo > 16) return fail(AED_ERR_INVALID, "N too large for 16-bit lo tables");
+  const uint32_t nlo = 1u << t.Nlo, nhi = 1u << t.Nhi;
+  std::vector<uint32_t> cnt(t.Nlo + 2, 0);
+  for (uint32_t l = 0; l < nlo; ++l) cnt[popc32(l)]++;
+  t.looff.assign(t.Nlo + 2, 0);
+  for (int k = 0; k <= t.Nlo; ++k) t.looff[k + 1] = t.looff[k] + cnt[k];
+  t.tlo.assign(nlo, 0);
+  t.lolist.assign(nlo, 0);
+  std::vector<uint32_t> fill(t.Nlo + 1, 0);
+  for (uint32_t l = 0; l < nlo; ++l) {
+    const int k = popc32(l);
+    t.tlo[l] = (uint16_t)fill[k];
+    t.lolist[t.looff[k] + fill[k]] = (uint16_t)l;
+    fill[k]++;
+  }
+  t.thi.assign(nhi, 0);
+  int64_t acc = 0;
+  for (uint32_t h = 0; h < nhi; ++h) {
+    t.thi[h] = (uint32_t)acc;
+    const int k = n_up - popc32(h);
+    if (k >= 0 && k <= t.Nlo) acc += cnt[k];
+  }
+  t.D = acc;
+  if (acc > 0xffffffffll) return fail(AED_ERR_INVALID, "sector too large");
+  return AED_OK;
+}
+
+void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr) {
+  th.clear();
+  tr.clear();
+  const uint32_t nhi = 1u << t.Nhi;
+  for (uint32_t h = 0; h < nhi; ++h) {
+    const int k = t.n_up - popc32(h);
+    if (k < 0 || k > t.Nlo) continue;
+    const uint32_t rows = t.looff[k + 1] - t.looff[k];
+    for (uint32_t r = 0; r < rows; r += tile_rows) {
+      th.push_back(h);
+      tr.push_back(r);
+    }
+  }
+}
+
+// ---- parameter surface -------------------------------------------------------------
+namespace {
+
+struct Params {
+  std::map<std::string, std::string> kv;
+  bool has(const std::string& k) const { return kv.count(k) != 0; }
+};
+
+std::string trim(const std::string& s) {
+  size_t a = 0, b = s.size();
+  while (a < b && std::isspace((unsigned char)s[a])) ++a;
+  while (b > a && std::isspace((unsigned char)s[b - 1])) --b;
+  return s.substr(a, b - a);
+}
+
+// "KEY = value" statements separated by newlines, ';' or ','; '{' '}' task
+// blocks are flattened (later assignments win); '//' starts a comment.
+int parse_kv(const char* text, Params& p) {
+  std::string s(text ? text : "");
+  std::string cur;
+  std::vector<std::string> stmts;
+  bool inq = false;
+  for (size_t i = 0; i < s.size(); ++i) {
+    const char c = s[i];
+    if (c == '"') inq = !inq;
+    if (!inq && c == '/' && i + 1 < s.size() && s[i + 1] == '/') {
+      while (i < s.size() && s[i] != '\n') ++i;
+      stmts.push_back(cur);
+      cur.clear();
+      continue;
+    }
+    if (!inq && (c == '\n' || c == ';' || c == ',' || c == '{' || c == '}')) {
+      stmts.push_back(cur);
+      cur.clear();
+    } else {
+      cur += c;
+    }
+  }
+  stmts.push_back(cur);
+  for (auto& st : stmts) {
+    const std::string t = trim(st);
+    if (t.empty()) continue;
+    const size_t eq = t.find('=');
+    if (eq == std::string::npos) return fail(AED_ERR_INVALID, "parameter statement without '=': " + t);
+    std::string key = trim(t.substr(0, eq)), val = trim(t.substr(eq + 1));
+    if (val.size() >= 2 && val.front() == '"' && val.back() == '"') val = val.substr(1, val.size() - 2);
+    p.kv[key] = val;
+  }
+  return AED_OK;
+}
+
+// Small expression evaluator: numbers, + - * / ^, parentheses, sqrt(), and
+// parameter names (resolved recursively through the model defaults).
+struct Eval {
+  const std::map<std::string, std::string>& kv;
+  const std::map<std::string, std::string>& defaults;
+  int depth = 0;
+
+  double name(const std::string& n) {
+    if (++depth > 64) throw std::runtime_error("parameter recursion too deep at " + n);
+    double v;
+    auto it = kv.find(n);
+    if (it != kv.end()) {
+      v = expr_str(it->second);
+    } else {
+      auto d = defaults.find(n);
+      if (d == defaults.end()) throw std::runtime_error("undefined parameter " + n);
+      v = expr_str(d->second);
+    }
+    --depth;
+    return v;
+  }
+  double expr_str(const std::string& s) {
+    size_t pos = 0;
+    double v = sum(s, pos);
+    skip(s, pos);
+    if (pos != s.size()) throw std::runtime_error("cannot evaluate '" + s + "'");
+    return v;
+  }
+  static void skip(const std::string& s, size_t& p) {
+    while (p < s.size() && std::isspace((unsigned char)s[p])) ++p;
+  }
+  double sum(const std::string& s, size_t& p) {
+    double v = prod(s, p);
+    while (true) {
+      skip(s, p);
+      if (p < s.size() && (s[p] == '+' || s[p] == '-')) {
+        const char op = s[p++];
+        const double r = prod(s, p);
+        v = op == '+' ? v + r : v - r;
+      } else {
+        return v;
+      }
+    }
+  }
+  double prod(const std::string& s, size_t& p) {
+    double v = power(s, p);
+    while (true) {
+      skip(s, p);
+      if (p < s.size() && (s[p] == '*' || s[p] == '/')) {
+        const char op = s[p++];
+        const double r = power(s, p);
+        v = op == '*' ? v * r : v / r;
+      } else {
+        return v;
+      }
+    }
+  }
+  double power(const std::string& s, size_t& p) {
+    double v = unary(s, p);
+    skip(s, p);
+    if (p < s.size() && s[p] == '^') {
+      ++p;
+      v = std::pow(v, power(s, p));
+    }
+    return v;
+  }
+  double unary(const std::string& s, size_t& p) {
+    skip(s, p);
+    if (p < s.size() && s[p] == '-') {
+      ++p;
+      return -unary(s, p);
+    }
+    if (p < s.size() && s[p] == '+') {
+      ++p;
+      return unary(s, p);
+    }
+    return atom(s, p);
+  }
+  double atom(const std::string& s, size_t& p) {
+    skip(s, p);
+    if (p >= s.size()) throw std::runtime_error("unexpected end of expression");
+    if (s[p] == '(') {
+      ++p;
+      const double v = sum(s, p);
+      skip(s, p);
+      if (p >= s.size() || s[p] != ')') throw std::runtime_error("missing ')'");
+      ++p;
+      return v;
+    }
+    if (std::isdigit((unsigned char)s[p]) || s[p] == '.') {
+      size_t q = p;
+      while (q < s.size() && (std::isdigit((unsigned char)s[q]) || s[q] == '.')) ++q;
+      if (q < s.size() && (s[q] == 'e' || s[q] == 'E')) {
+        size_t r = q + 1;
+        if (r < s.size() && (s[r] == '+' || s[r] == '-')) ++r;
+        if (r < s.size() && std::isdigit((unsigned char)s[r])) {
+          q = r;
+          while (q < s.size() && std::isdigit((unsigned char)s[q])) ++q;
+        }
+      }
+      const double v = std::stod(s.substr(p, q - p));
+      p = q;
+      return v;
+    }
+    if (std::isalpha((unsigned char)s[p]) || s[p] == '_') {
+      size_t q = p;
+      while (q < s.size() && (std::isalnum((unsigned char)s[q]) || s[q] == '_' || s[q] == '\'' || s[q] == '#')) ++q;
+      const std::string id = s.substr(p, q - p);
+      p = q;
+      skip(s, p);
+      if (p < s.size() && s[p] == '(') {
+        ++p;
+        skip(s, p);
+        if (id == "random") throw std::runtime_error("random() disorder is not supported; pass per-bond couplings");
+        const double a = sum(s, p);
+        skip(s, p);
+        if (p >= s.size() || s[p] != ')') throw std::runtime_error("missing ')' after " + id);
+        ++p;
+        if (id == "sqrt") return std::sqrt(a);
+        if (id == "abs") return std::fabs(a);
+        throw std::runtime_error("unsupported function " + id);
+      }
+      return name(id);
+    }
+    throw std::runtime_error(std::string("unexpected character '") + s[p] + "'");
+  }
+};
+
+// spin HAMILTONIAN defaults (lib/xml/models.xml.in:343-358) and BONDTERM /
+// SITETERM parameter defaults (models.xml.in:360-371).
+const std::map<std::string, std::string>& spin_defaults() {
+  static const std::map<std::string, std::string> d = {
+      {"J0", "0"},    {"J", "J0"},     {"Jz", "J"},      {"Jxy", "J"},     {"Jz0", "Jz"},
+      {"Jxy0", "Jxy"}, {"J1", "0"},    {"J'", "J1"},     {"Jz'", "J'"},    {"Jxy'", "J'"},
+      {"Jz1", "Jz'"}, {"Jxy1", "Jxy'"}, {"h", "0"},      {"Gamma", "0"},   {"D", "0"},
+      {"K", "0"},     {"local_S", "1/2"}, {"Sz_total", "0"}};
+  return d;
+}
+
+struct LatticeSpec {
+  int dim;
+  const char* ext_w_default;  // W default: "L" or "2" (2D only)
+  bool periodic[2];
+  int n_edges;
+  int off_src[2][2], off_tgt[2][2], etype[2];
+};
+
+// Unit cells and finite lattices of lib/xml/lattices.xml.in (simple1d 174-177,
+// complex1d 179-183, simple2d 185-189, anisotropic2d 205-209; chain 416-423,
+// nnn chain 434-450, square 326-346, anisotropic square 470-479, ladder 494-516).
+bool lattice_spec(const std::string& name, LatticeSpec& L) {
+  std::memset(&L, 0, sizeof L);
+  auto set1d = [&](bool per, int ne) {
+    L.dim = 1;
+    L.periodic[0] = per;
+    L.n_edges = ne;
+    L.off_src[0][0] = 0;
+    L.off_tgt[0][0] = 1;
+    L.etype[0] = 0;
+    if (ne == 2) {
+      L.off_src[1][0] = 0;
+      L.off_tgt[1][0] = 2;
+      L.etype[1] = 1;
+    }
+  };
+  auto set2d = [&](bool p0, bool p1, bool aniso, const char* wdef) {
+    L.dim = 2;
+    L.periodic[0] = p0;
+    L.periodic[1] = p1;
+    L.ext_w_default = wdef;
+    L.n_edges = 2;
+    if (!aniso) {  // simple2d: (0,0)->(0,1), then (0,0)->(1,0), both type 0
+      L.off_tgt[0][0] = 0; L.off_tgt[0][1] = 1; L.etype[0] = 0;
+      L.off_tgt[1][0] = 1; L.off_tgt[1][1] = 0; L.etype[1] = 0;
+    } else {  // anisotropic2d: type 0 (0,0)->(1,0), type 1 (0,0)->(0,1)
+      L.off_tgt[0][0] = 1; L.off_tgt[0][1] = 0; L.etype[0] = 0;
+      L.off_tgt[1][0] = 0; L.off_tgt[1][1] = 1; L.etype[1] = 1;
+    }
+  };
+  if (name == "chain lattice") set1d(true, 1);
+  else if (name == "open chain lattice") set1d(false, 1);
+  else if (name == "nnn chain lattice") set1d(true, 2);
+  else if (name == "nnn open chain lattice") set1d(false, 2);
+  else if (name == "square lattice") set2d(true, true, false, "L");
+  else if (name == "open square lattice") set2d(false, false, false, "L");
+  else if (name == "anisotropic square lattice") set2d(true, true, true, "L");
+  else if (name == "ladder") set2d(true, false, true, "2");
+  else if (name == "open ladder") set2d(false, false, true, "2");
+  else return false;
+  return true;
+}
+
+}  // namespace
+
+int parse_parameters(const char* text, ParsedParams& out) {
+  Params p;
+  int rc = parse_kv(text, p);
+  if (rc) return rc;
+  out = ParsedParams();
+  std::memset(&out.info, 0, sizeof out.info);
+  Eval ev{p.kv, spin_defaults()};
+  try {
+    auto str = [&](const std::string& k, const std::string& dflt) {
+      auto it = p.kv.find(k);
+      return it == p.kv.end() ? dflt : it->second;
+    };
+    const std::string model = str("MODEL", "");
+    if (model != "spin") return fail(AED_ERR_INVALID, "MODEL must be \"spin\" (got \"" + model + "\")");
+    if (std::fabs(ev.name("local_S") - 0.5) > 1e-12) return fail(AED_ERR_INVALID, "only local_S=1/2 is supported");
+    const std::string latname = str("LATTICE", "");
+    LatticeSpec L;
+    if (!lattice_spec(latname, L)) return fail(AED_ERR_INVALID, "unsupported LATTICE \"" + latname + "\"");
+    const std::string cq = str("CONSERVED_QUANTUMNUMBERS", "");
+    if (cq.find("Sz") == std::string::npos)
+      return fail(AED_ERR_INVALID, "CONSERVED_QUANTUMNUMBERS must contain Sz (full Hilbert space not supported)");
+    const std::string ts = str("TRANSLATION_SYMMETRY", "true");
+    if (!(ts == "false" || ts == "0" || ts == "False" || ts == "FALSE"))
+      return fail(AED_ERR_INVALID,
+                  "TRANSLATION_SYMMETRY must be false: momentum sectors are not supported (factory.C:17-30)");
+    if (!p.has("Sz_total"))
+      return fail(AED_ERR_INVALID, "Sz_total must be given (the loop over all Sz sectors is not supported)");
+    const int Lx = (int)std::lround(ev.name("L"));
+    int Wy = 1;
+    if (L.dim == 2) Wy = p.has("W") ? (int)std::lround(ev.name("W")) : (int)std::lround(ev.expr_str(L.ext_w_default));
+    if (Lx < 1 || Wy < 1) return fail(AED_ERR_INVALID, "lattice extents must be positive");
+    const int N = Lx * Wy;
+    if (N < 2 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 2..32");
+    const double szt = ev.name("Sz_total");
+    const double nup_d = N / 2.0 + szt;
+    const int n_up = (int)std::lround(nup_d);
+    if (std::fabs(nup_d - n_up) > 1e-9 || n_up < 0 || n_up > N)
+      return fail(AED_ERR_INVALID, "Sz_total incompatible with the number of sites");
+    // edges: cell by cell (last coordinate fastest), unit-cell edge order,
+    // open boundaries drop edges, self-loops are dropped (latticegraph.h:98-136)
+    const int ext[2] = {Lx, Wy};
+    for (int c = 0; c < N; ++c) {
+      int cc[2];
+      if (L.dim == 1) {
+        cc[0] = c;
+        cc[1] = 0;
+      } else {
+        cc[0] = c / Wy;
+        cc[1] = c % Wy;
+      }
+      for (int e = 0; e < L.n_edges; ++e) {
+        int src[2], tgt[2];
+        bool ok = true;
+        for (int d = 0; d < L.dim; ++d) {
+          src[d] = cc[d] + L.off_src[e][d];
+          tgt[d] = cc[d] + L.off_tgt[e][d];
+          for (int* v : {&src[d], &tgt[d]}) {
+            if (*v < 0 || *v >= ext[d]) {
+              if (!L.periodic[d]) ok = false;
+              *v = ((*v % ext[d]) + ext[d]) % ext[d];
+            }
+          }
+        }
+        if (!ok) continue;
+        const int si = L.dim == 1 ? src[0] : src[0] * Wy + src[1];
+        const int ti = L.dim == 1 ? tgt[0] : tgt[0] * Wy + tgt[1];
+        if (si == ti) continue;
+        const std::string t = std::to_string(L.etype[e]);
+        // Jz# / Jxy# / K#: HAMILTONIAN parameters first, then BONDTERM default J#
+        auto coupling = [&](const std::string& base) {
+          const std::string n = base + t;
+          if (p.has(n) || spin_defaults().count(n)) return ev.name(n);
+          const std::string j = "J" + t;
+          if (p.has(j) || spin_defaults().count(j)) return ev.name(j);
+          return 0.0;
+        };
+        const double jz = coupling("Jz"), jxy = coupling("Jxy");
+        // K# has BONDTERM default 0 (models.xml.in:370); the HAMILTONIAN-level K
+        // is not substituted into it
+        const std::string kn = "K" + t;
+        const double kq = p.has(kn) ? ev.name(kn) : 0.0;
+        if ((int)out.s1.size() >= kMaxBonds) return fail(AED_ERR_INVALID, "too many bonds");
+        out.s1.push_back(si);
+        out.s2.push_back(ti);
+        out.jz.push_back(jz);
+        out.jxy.push_back(jxy);
+        out.kq.push_back(kq);
+      }
+    }
+    // site terms (site type 0): h0 = h, D0 = D, Gamma0 = Gamma
+    const double h0 = p.has("h0") ? ev.name("h0") : ev.name("h");
+    const double d0 = p.has("D0") ? ev.name("D0") : ev.name("D");
+    const double g0 = p.has("Gamma0") ? ev.name("Gamma0") : ev.name("Gamma");
+    if (g0 != 0.0) return fail(AED_ERR_INVALID, "Gamma (transverse field) breaks Sz conservation");
+    if (h0 != 0.0 || d0 != 0.0) {
+      out.site_h.assign(N, h0);
+      out.site_d.assign(N, d0);
+      out.info.has_site_terms = 1;
+    }
+    out.info.n_sites = N;
+    out.info.n_up = n_up;
+    out.info.n_bonds = (int)out.s1.size();
+    out.info.number_eigenvalues = p.has("NUMBER_EIGENVALUES") ? (int)std::lround(ev.name("NUMBER_EIGENVALUES")) : 1;
+    out.info.max_iterations = p.has("MAX_ITERATIONS") ? (int)std::lround(ev.name("MAX_ITERATIONS")) : 0;
+    if (out.info.number_eigenvalues < 1) return fail(AED_ERR_INVALID, "NUMBER_EIGENVALUES must be >= 1");
+  } catch (const std::exception& e) {
+    return fail(AED_ERR_INVALID, std::string("parameter error: ") + e.what());
+  }
+  return AED_OK;
+}
+
+}  // namespace aed

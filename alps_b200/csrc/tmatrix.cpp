@@ -1,0 +1,176 @@
+// tmatrix.cpp -- host-side Lanczos T-matrix analysis.
+//
+// Tmatrix::compute(do_err = true) of src/ietl/tmatrix.h:121-228 with the LAPACK
+// dstev call (src/ietl/ietl2lapack.h:84-99) replaced by an implicit QL
+// eigensolver for symmetric tridiagonal matrices (Bowdler, Martin, Reinsch &
+// Wilkinson, Numer. Math. 11 (1968) 293-306).  Only the last row of the
+// eigenvector matrix is formed: it is the only part the error estimates
+// |beta_m z_{m,i}| use, so each analysis costs O(m^2) instead of O(m^3).
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "aed_internal.h"
+
+namespace aed {
+
+// d[0..n): diagonal -> eigenvalues ascending.  e[0..n): sub-diagonal in
+// e[0..n-2] (destroyed).  zlast (optional, n entries): last row of Z.
+// zfull (optional, n*n, column-major): all eigenvectors (column k <-> d[k]).
+int tridiag_eigen(int n, double* d, double* e, double* zlast, double* zfull) {
+  if (n <= 0) return 0;
+  if (zlast) {
+    std::fill(zlast, zlast + n, 0.0);
+    zlast[n - 1] = 1.0;
+  }
+  if (zfull) {
+    std::fill(zfull, zfull + (size_t)n * n, 0.0);
+    for (int k = 0; k < n; ++k) zfull[(size_t)k * n + k] = 1.0;
+  }
+  e[n - 1] = 0.0;
+  for (int l = 0; l < n; ++l) {
+    for (int sweep = 0;; ++sweep) {
+      // smallest m >= l where the matrix splits
+      int m = l;
+      while (m < n - 1 && std::fabs(e[m]) > DBL_EPSILON * (std::fabs(d[m]) + std::fabs(d[m + 1]))) ++m;
+      if (m == l) break;
+      if (sweep >= 90) return l + 1;
+      // shift: eigenvalue of the leading 2x2 block closer to d[l]
+      const double theta = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      const double rho = std::hypot(theta, 1.0);
+      double g = d[m] - d[l] + e[l] / (theta + std::copysign(rho, theta));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool split = false;
+      for (; i >= l; --i) {
+        const double f = s * e[i], b = c * e[i];
+        const double r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {  // underflow: the matrix splits at i+1
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          split = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        const double gg = d[i + 1] - p;
+        const double t = (d[i] - gg) * s + 2.0 * c * b;
+        p = s * t;
+        d[i + 1] = gg + p;
+        g = c * t - b;
+        if (zlast) {
+          const double z1 = zlast[i + 1];
+          zlast[i + 1] = s * zlast[i] + c * z1;
+          zlast[i] = c * zlast[i] - s * z1;
+        }
+        if (zfull) {
+          double* ci = zfull + (size_t)i * n;
+          double* cj = zfull + (size_t)(i + 1) * n;
+          for (int k = 0; k < n; ++k) {
+            const double z1 = cj[k];
+            cj[k] = s * ci[k] + c * z1;
+            ci[k] = c * ci[k] - s * z1;
+          }
+        }
+      }
+      if (split) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  // ascending order (stable), carrying zlast / zfull columns
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return d[a] < d[b]; });
+  std::vector<double> tmp(d, d + n);
+  for (int i = 0; i < n; ++i) d[i] = tmp[ord[i]];
+  if (zlast) {
+    tmp.assign(zlast, zlast + n);
+    for (int i = 0; i < n; ++i) zlast[i] = tmp[ord[i]];
+  }
+  if (zfull) {
+    std::vector<double> zt(zfull, zfull + (size_t)n * n);
+    for (int i = 0; i < n; ++i)
+      std::copy(zt.begin() + (size_t)ord[i] * n, zt.begin() + (size_t)(ord[i] + 1) * n, zfull + (size_t)i * n);
+  }
+  return 0;
+}
+
+int tmatrix_analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
+                    TmatInfo& out) {
+  out = TmatInfo();
+  if (n < 1) return AED_OK;
+  std::vector<double> ev(alpha, alpha + n), e(n + 1, 0.0), zl(n);
+  for (int i = 0; i + 1 < n; ++i) e[i] = beta[i];
+  if (tridiag_eigen(n, ev.data(), e.data(), zl.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  const double eps = DBL_EPSILON;
+  const double error_tol = std::pow(eps, 2.0 / 3.0);  // tmatrix.h:32
+  out.multol = std::max(alpha_max, beta_max) * 2 * eps * (10000 + n);
+  out.thold = std::max(error_tol * std::max(ev[0], ev[n - 1]), 5 * out.multol);
+  const double bl = beta[n - 1];  // beta_{m+1}
+  std::vector<double> dist, err;
+  std::vector<int> mult, first;
+  double temp = ev[0];
+  dist.push_back(ev[0]);
+  first.push_back(0);
+  int multiple = 1;
+  for (int i = 1; i < n; ++i) {
+    if ((ev[i] - temp) > out.thold) {
+      dist.push_back(ev[i]);
+      first.push_back(i);
+      temp = ev[i];
+      mult.push_back(multiple);
+      err.push_back(multiple > 1 ? 0.0 : std::fabs(bl * zl[i - 1]));
+      multiple = 1;
+    } else {
+      ++multiple;
+    }
+  }
+  mult.push_back(multiple);
+  err.push_back(multiple > 1 ? 0.0 : std::fabs(bl * zl[n - 1]));
+  // spurious ("ghost") values: eigenvalues of T without its first row and
+  // column that coincide within multol with a simple eigenvalue of T
+  std::vector<double> evg;
+  if (n > 1) {
+    evg.assign(alpha + 1, alpha + n);
+    std::vector<double> eg(n, 0.0);
+    for (int i = 1; i + 1 < n; ++i) eg[i - 1] = beta[i];
+    if (tridiag_eigen(n - 1, evg.data(), eg.data(), nullptr))
+      return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  }
+  int t2 = 0;
+  for (size_t i = 0; i < dist.size(); ++i) {
+    if (mult[i] != 1) continue;
+    for (int j = t2; j < n - 2; ++j, ++t2) {
+      if ((evg[j] - dist[i]) >= out.multol) break;
+      if (std::fabs(dist[i] - evg[j]) < out.multol) {
+        mult[i] = 0;
+        err[i] = 0.0;
+        ++t2;
+        break;
+      }
+    }
+  }
+  for (size_t i = 0; i < dist.size(); ++i)
+    if (mult[i] != 0) {
+      out.evals.push_back(dist[i]);
+      out.errs.push_back(err[i]);
+      out.mults.push_back(mult[i]);
+      out.first.push_back(first[i]);
+    }
+  return AED_OK;
+}
+
+// lanczos_iteration_nlowest::converged (src/ietl/iteration.h:115-130)
+bool nlowest_converged(const TmatInfo& t, int nev, double rtol, double atol) {
+  if ((int)t.evals.size() < nev) return false;
+  for (int i = 0; i < nev; ++i)
+    if (t.errs[i] > std::max(atol, rtol * std::fabs(t.evals[i]))) return false;
+  return true;
+}
+
+}  // namespace aed

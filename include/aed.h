@@ -1,0 +1,198 @@
+/* aed.h -- C ABI of the B200 exact-diagonalisation engine (libaed.so).
+ *
+ * The engine replaces the hot path of ALPS `sparsediag`: the Sz-sector basis,
+ * the Hamiltonian apply y = H*x and the ietl Lanczos iteration, for the spin-1/2
+ * "spin" model on one GPU.  Every function returns an int status (AED_OK = 0,
+ * negative on error); aed_last_error() describes the most recent failure on the
+ * calling thread.  Vectors are plain device pointers to D elements of the
+ * handle's precision (double for AED_FP64, float for AED_FP32).  All calls on a
+ * handle are ordered on that handle's CUDA stream; calls that return host
+ * scalars synchronise that stream.  One handle per host thread at a time.
+ *
+ * Reference paths are relative to the ALPS source tree.
+ */
+#ifndef AED_H
+#define AED_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define AED_OK 0
+#define AED_ERR_INVALID (-1)        /* bad argument / unsupported model        */
+#define AED_ERR_NOMEM (-2)          /* device or host allocation failed        */
+#define AED_ERR_ADMISSION (-3)      /* request refused: HBM budget exceeded    */
+#define AED_ERR_CUDA (-4)           /* CUDA runtime error                      */
+#define AED_ERR_TIMEOUT (-5)        /* bounded device wait gave up             */
+#define AED_ERR_NOT_CONVERGED (-6)  /* MAX_ITERATIONS reached (iteration.h:80) */
+#define AED_ERR_TRIDIAG (-7)        /* tridiagonal solver failed (tmatrix.h:144-145) */
+#define AED_ERR_MISMATCH (-8)       /* replayed alpha/beta differ (lanczos.h:249-250,267-268) */
+#define AED_ERR_CANCELLED (-9)      /* request cancelled before completion     */
+#define AED_PENDING 1               /* aed_poll: request not finished yet      */
+
+/* vector precision of a handle */
+#define AED_FP64 0
+#define AED_FP32 1
+
+/* ---- model description ---------------------------------------------------
+ * Replaces the model/lattice surface that hamiltonian_matrix reads
+ * (src/alps/model/hamiltonian_matrix.hpp:224-231, 387-397): N spin-1/2 sites,
+ * the Sz_total constraint (CONSERVED_QUANTUMNUMBERS="Sz") and the bond list in
+ * graph order with per-bond couplings of the "spin" HAMILTONIAN
+ * (lib/xml/models.xml.in:342-373):
+ *   H = sum_s [-h_s Sz_s + D_s Sz_s^2]
+ *     + sum_b [Jz_b Sz_i Sz_j + Jxy_b (S+_i S-_j + S-_i S+_j)/2 + K_b (S_i.S_j)^2]
+ * All arrays are host memory and are copied by aed_create. */
+typedef struct {
+  int32_t n_sites;        /* N, 2..32                                          */
+  int32_t n_up;           /* number of up spins: Sz_total = n_up - N/2          */
+  int32_t n_bonds;        /* 0..AED_MAX_BONDS                                   */
+  const int32_t* bond_s1; /* source site of each bond                           */
+  const int32_t* bond_s2; /* target site of each bond (!= source)               */
+  const double* bond_jz;  /* Jz of each bond                                    */
+  const double* bond_jxy; /* Jxy of each bond                                   */
+  const double* bond_k;   /* biquadratic K of each bond, or NULL for 0          */
+  const double* site_h;   /* longitudinal field h per site, or NULL for 0       */
+  const double* site_d;   /* single-ion D per site, or NULL for 0               */
+} aed_model_desc;
+
+#define AED_MAX_BONDS 128
+
+/* Parameters read from an ALPS parameter file (the subset of the sparsediag
+ * surface this engine supports; see aed_parse_parameters). */
+typedef struct {
+  int32_t n_sites;
+  int32_t n_up;
+  int32_t n_bonds;
+  int32_t number_eigenvalues; /* NUMBER_EIGENVALUES, default 1 (sparsediag.h:110)        */
+  int32_t max_iterations;     /* MAX_ITERATIONS, 0 = default min(10 D, 1000) (sparsediag.h:109) */
+  int32_t has_site_terms;     /* h or D present                                         */
+} aed_param_info;
+
+/* Parse an ALPS parameter file ("KEY = value" lines, ';' or newline separated,
+ * quoted strings, simple numeric expressions) into a bond list in ALPS graph
+ * order.  Supported: MODEL="spin", local_S=1/2, LATTICE in {chain lattice,
+ * open chain lattice, nnn chain lattice, nnn open chain lattice, square
+ * lattice, open square lattice, anisotropic square lattice, ladder, open
+ * ladder} with L/W, couplings J, J0, J1, J', Jz, Jxy, Jz<n>, Jxy<n>, J<n>, K<n>,
+ * h, D with the model library's defaults, CONSERVED_QUANTUMNUMBERS containing Sz, Sz_total,
+ * NUMBER_EIGENVALUES, MAX_ITERATIONS, TRANSLATION_SYMMETRY=false.
+ * Replaces the parameter path of SparseDiagFactory/DiagMatrix
+ * (applications/diag/sparsediag/factory.C:17-30, applications/diag/diag.h:85-175,
+ * src/alps/lattice/latticegraph.h:98-136, lib/xml/lattices.xml.in).
+ * Call once with NULL arrays to get info->n_bonds, then with arrays of at least
+ * that many entries (site arrays: n_sites entries). */
+int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* bond_s1, int32_t* bond_s2,
+                         double* bond_jz, double* bond_jxy, double* bond_k, double* site_h,
+                         double* site_d, int32_t bond_capacity, int32_t site_capacity);
+
+/* ---- handles -------------------------------------------------------------- */
+typedef struct aed_handle aed_handle;
+
+/* Build the sector basis tables and the coupling tables on `device`.
+ * Replaces hamiltonian_matrix::build_basis + build
+ * (src/alps/model/hamiltonian_matrix.hpp:402-450; basis_states::build,
+ * src/alps/model/basisstates.h:175-278).  No explicit matrix is stored: the
+ * apply is matrix-free. */
+int aed_create(const aed_model_desc* model, int precision, int device, aed_handle** out);
+int aed_destroy(aed_handle* h);
+
+/* Sector dimension D (hamiltonian_matrix::dimension). */
+int aed_dimension(const aed_handle* h, int64_t* dim);
+
+/* Most recent error message of the calling thread ("" if none). */
+const char* aed_last_error(void);
+
+/* Basis states [offset, offset+count) as bit strings (site s <-> bit N-1-s,
+ * up = 1), in the reference's order (basisstates.h:175-278).  host_out is host memory. */
+int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t count);
+
+/* Ranks of `count` host bit strings through the device tables: the row index
+ * of each state, or D when the state is outside the sector
+ * (basis_states::index, basisstates.h:68-74). */
+int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t* host_idx);
+
+/* ---- vectors (ietl vectorspace / free functions, src/ietl/vectorspace.h:23-46,
+ *      src/ietl/interface/ublas.h:27-55) ------------------------------------ */
+int aed_vec_alloc(aed_handle* h, void** dev_vec);          /* zeroed (new_vector)  */
+int aed_vec_free(aed_handle* h, void* dev_vec);
+int aed_vec_upload(aed_handle* h, void* dev_vec, const double* host);   /* D doubles */
+int aed_vec_download(aed_handle* h, const void* dev_vec, double* host); /* D doubles */
+int aed_vec_copy(aed_handle* h, const void* x, void* y);               /* ietl::copy  */
+int aed_vec_clear(aed_handle* h, void* x);                             /* ietl::clear */
+/* ietl::generate with the engine's generator: x[i] = uniform[0,1) from
+ * splitmix64(seed, i), bit-identical on host and device. */
+int aed_vec_fill_random(aed_handle* h, void* x, uint64_t seed);
+
+/* y = H x (ietl::mult, src/ietl/interface/ublas.h:57-63).  In FP64 every row
+ * is summed in ascending column order without FMA contraction, exactly as
+ * y = prod(M, x) over the explicit matrix: results are bit-identical to it. */
+int aed_mult(aed_handle* h, const void* x, void* y);
+
+int aed_dot(aed_handle* h, const void* x, const void* y, double* out); /* ietl::dot      */
+int aed_nrm2(aed_handle* h, const void* x, double* out);               /* ietl::two_norm */
+int aed_axpy(aed_handle* h, double a, const void* x, void* y);         /* y += a*x       */
+int aed_scal(aed_handle* h, double a, void* x);                        /* x *= a         */
+int aed_div(aed_handle* h, double a, void* x);                         /* x /= a         */
+
+/* One fused Lanczos step, lanczos::make_step (src/ietl/lanczos.h:392-406):
+ *   w = H v_cur;  alpha = <v_cur, w>;  w -= alpha v_cur;  w -= beta_prev v_prev;
+ *   beta = ||w||;  v_next = w / beta.
+ * v_prev may be NULL for the first step (lanczos.h:377-390). */
+int aed_lanczos_step(aed_handle* h, const void* v_prev, const void* v_cur, void* v_next,
+                     double beta_prev, double* alpha, double* beta);
+
+/* ---- whole solves ----------------------------------------------------------- */
+typedef struct {
+  int32_t nev;          /* NUMBER_EIGENVALUES (>= 1)                                  */
+  int32_t max_iter;     /* MAX_ITERATIONS, 0 = min(10 D, 1000)                         */
+  double rtol, atol;    /* lanczos_iteration_nlowest tolerances, 0 = 100 eps (iteration.h:110-113) */
+  uint64_t seed;        /* start-vector seed                                           */
+  const double* start;  /* optional HOST start vector (D doubles), else seeded          */
+  int32_t refine;       /* AED_FP32 handles: 0 = mixed FP32 + FP64 refinement (default),
+                           -1 = plain FP64 Lanczos on the same handle                  */
+  int32_t profile;      /* 1: time every apply with CUDA events (res->apply_ms)         */
+} aed_solve_opts;
+
+#define AED_MAX_NEV 16
+typedef struct {
+  int32_t n_evals;              /* min(nev, #distinct non-ghost values) (sparsediag.h:115-118) */
+  int32_t iterations;           /* T-matrix size at convergence (FP64 phase for FP32 handles)   */
+  int32_t iterations_low;       /* FP32 phase iterations (0 for FP64 handles)                    */
+  int32_t converged;            /* 1 when all nev errors met the tolerance                       */
+  double evals[AED_MAX_NEV];    /* lowest distinct eigenvalues, ascending                        */
+  double errors[AED_MAX_NEV];   /* |beta_m z_{m,i}| error estimates (tmatrix.h:159-183)          */
+  double evals_low[AED_MAX_NEV];/* FP32-phase eigenvalues before refinement (FP32 handles)       */
+  double seconds;               /* wall time of the solve                                        */
+  double apply_ms;              /* mean device time of one H*x inside the solve                  */
+} aed_solve_result;
+
+/* Lanczos eigenvalues: SparseDiagMatrix::do_subspace's Lanczos part
+ * (applications/diag/sparsediag/sparsediag.h:104-118) with ietl::lanczos
+ * (src/ietl/lanczos.h:341-406), lanczos_iteration_nlowest (src/ietl/iteration.h:106-130)
+ * and Tmatrix::compute's distinct/ghost rules (src/ietl/tmatrix.h:121-228). */
+int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res);
+
+/* Copy the alpha/beta recurrence of the last aed_solve (FP64 phase) to host;
+ * *n receives its length (at most cap entries are written). */
+int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n);
+
+/* Time `reps` back-to-back applies y = H x on the handle's stream with CUDA
+ * events; *ms = mean milliseconds per apply. */
+int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own
+ * work or record timing events on it.  Engine addition, no reference counterpart. */
+int aed_get_stream(aed_handle* h, void** stream);
+
+/* Number of engine kernel launches made by this process so far. */
+int aed_launch_count(int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AED_H */

@@ -1,0 +1,136 @@
+"""Generate the golden fixtures in this folder from the reference's own test outputs.
+
+Run in a checkout where the ALPS sources are available:
+
+    python tests/golden/make_golden.py /path/to/alps
+
+Reads (paths relative to the ALPS source tree) and writes JSON beside this script:
+  test/model/example10.output   -> basis_example10.json  (2x2 square, all 16 states)
+  test/model/example12.output   -> basis_example12.json  (2x2 square, Sz_total = 0)
+  test/model/example3.output    -> spin_terms_example3.json (HSpinSite, HSpinBond)
+  test/model/example4.output    -> spin_half_example4.json  (two-site HSpinHalf)
+  test/lattice/example5.output  -> lattice_example5.json (anisotropic square 10x4 sites)
+  test/lattice/example6.output  -> lattice_example6.json (anisotropic square 10x4 bonds)
+The fixtures are committed; the tests never read the ALPS tree.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _states(text):
+    """Parse '[ |1/2 -1/2 > |1/2 1/2 > ... ]' rows into lists of Sz (as +1/-1)."""
+    rows = []
+    for line in text.splitlines():
+        line = line.strip()
+        if not line.startswith("["):
+            continue
+        kets = re.findall(r"\|\s*(\S+)\s+(\S+)\s*>", line)
+        rows.append([1 if sz == "1/2" else -1 for _s, sz in kets])
+    return rows
+
+
+def _block(text, name):
+    """Return the brace expression following 'name =' in an example output."""
+    start = text.index(name)
+    start = text.index("{", start)
+    depth = 0
+    for i in range(start, len(text)):
+        if text[i] == "{":
+            depth += 1
+        elif text[i] == "}":
+            depth -= 1
+            if depth == 0:
+                return text[start: i + 1]
+    raise ValueError(name)
+
+
+def _nested(expr):
+    """'{{a, b}, {c, d}}' -> nested python lists of expression strings."""
+    pos = 0
+
+    def parse():
+        nonlocal pos
+        assert expr[pos] == "{"
+        pos += 1
+        items = []
+        cur = ""
+        while True:
+            ch = expr[pos]
+            if ch == "{":
+                items.append(parse())
+                cur = ""
+            elif ch == ",":
+                if cur.strip():
+                    items.append(cur.strip())
+                cur = ""
+                pos += 1
+            elif ch == "}":
+                if cur.strip():
+                    items.append(cur.strip())
+                pos += 1
+                return items
+            else:
+                cur += ch
+                pos += 1
+
+    return parse()
+
+
+def main(alps):
+    out = {}
+    t = open(os.path.join(alps, "test/model/example10.output")).read()
+    out["basis_example10.json"] = {
+        "source": "test/model/example10.output",
+        "lattice": "square lattice", "L": 2, "constraint": None,
+        "states_sz": _states(t),
+    }
+    t = open(os.path.join(alps, "test/model/example12.output")).read()
+    out["basis_example12.json"] = {
+        "source": "test/model/example12.output",
+        "lattice": "square lattice", "L": 2, "constraint": {"Sz_total": 0},
+        "states_sz": _states(t),
+    }
+    t = open(os.path.join(alps, "test/model/example3.output")).read()
+    out["spin_terms_example3.json"] = {
+        "source": "test/model/example3.output",
+        "HSpinSite": _nested(_block(t, "HSpinSite")),
+        "HSpinBond": _nested(_block(t, "HSpinBond")),
+    }
+    t = open(os.path.join(alps, "test/model/example4.output")).read()
+    out["spin_half_example4.json"] = {
+        "source": "test/model/example4.output",
+        "HSpinHalf": _nested(_block(t, "HSpinHalf")),
+    }
+    t = open(os.path.join(alps, "test/lattice/example5.output")).read()
+    sites = []
+    for m in re.finditer(r"Site (\d+) has type (\d+) and has coordinates ([\d\s\.\-]+)", t):
+        sites.append({"site": int(m.group(1)), "type": int(m.group(2)),
+                      "coords": [float(v) for v in m.group(3).split()]})
+    out["lattice_example5.json"] = {
+        "source": "test/lattice/example5.output",
+        "params": {"LATTICE": "anisotropic square lattice", "L": 10, "W": 4},
+        "sites": sites,
+    }
+    t = open(os.path.join(alps, "test/lattice/example6.output")).read()
+    bonds = [[int(a), int(b), int(c)] for a, b, c in
+             re.findall(r"The bond between site (\d+) and site (\d+) has type (\d+)", t)]
+    out["lattice_example6.json"] = {
+        "source": "test/lattice/example6.output",
+        "params": {"LATTICE": "anisotropic square lattice", "L": 10, "W": 4},
+        "bonds": bonds,
+    }
+    for name, obj in out.items():
+        with open(os.path.join(HERE, name), "w") as f:
+            json.dump(obj, f, indent=1)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,142 @@
+"""Host-side checks of libaed.so without a GPU: exports, parameter surface, error paths."""
+
+import ctypes
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import alps_b200 as ed
+import oracle
+from oracle import lattice
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\**\s+(aed_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ed.lib()
+    names = header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+PARAM_CASES = [
+    {"LATTICE": "chain lattice", "L": 16, "J": 1},
+    {"LATTICE": "open chain lattice", "L": 10, "J": 0.7},
+    {"LATTICE": "nnn chain lattice", "L": 28, "J": 1, "J1": 0.31},
+    {"LATTICE": "nnn open chain lattice", "L": 10, "J": 1, "J1": 0.5},
+    {"LATTICE": "square lattice", "L": 6, "W": 5, "J": 1},
+    {"LATTICE": "square lattice", "L": 4, "J": 1.5},
+    {"LATTICE": "open square lattice", "L": 3, "W": 4, "J": 1.0},
+    {"LATTICE": "anisotropic square lattice", "L": 10, "W": 3, "J0": 1, "J1": 0.4},
+    {"LATTICE": "ladder", "L": 12, "J0": 1.2, "J1": 0.8},
+    {"LATTICE": "open ladder", "L": 6, "J0": 1, "J1": 2},
+    {"LATTICE": "chain lattice", "L": 2, "J": 1},
+    {"LATTICE": "nnn chain lattice", "L": 4, "J": 1, "J1": 1},
+    {"LATTICE": "chain lattice", "L": 8, "Jz": 1.3, "Jxy": 0.6},
+    {"LATTICE": "nnn chain lattice", "L": 8, "J": 1, "Jz1": 0.2, "Jxy1": 0.9},
+]
+
+
+@pytest.mark.parametrize("p", PARAM_CASES)
+def test_parameter_surface_matches_oracle(p):
+    p = dict(p, MODEL="spin", CONSERVED_QUANTUMNUMBERS="Sz", Sz_total=0, TRANSLATION_SYMMETRY="false")
+    m = ed.model_from_parameters(p)
+    N, nu, bonds = lattice.spin_model(p)
+    assert m["n_sites"] == N and m["n_up"] == nu
+    assert len(m["bonds"]) == len(bonds)
+    for a, b in zip(m["bonds"], bonds):
+        assert a[0] == b[0] and a[1] == b[1]
+        assert a[2] == pytest.approx(b[2], abs=0) and a[3] == pytest.approx(b[3], abs=0)
+
+
+def test_parameter_surface_matches_golden_example6():
+    """The reference's example6 (anisotropic square 10x4) has 40 sites, beyond the
+    engine's 32; the oracle lattice is pinned to it (tests/test_oracle.py) and the
+    engine is checked against the oracle on 10x3 with the same edge rules."""
+    with open(os.path.join(ROOT, "tests", "golden", "lattice_example6.json")) as f:
+        g = json.load(f)
+    _, _, ob = lattice.lattice_graph("anisotropic square lattice", {"L": 10, "W": 4})
+    assert [list(b) for b in ob] == g["bonds"]
+    txt = ('MODEL="spin"\nLATTICE="anisotropic square lattice"\nL=10\nW=3\nJ0=1\nJ1=2\n'
+           'CONSERVED_QUANTUMNUMBERS="Sz"\nSz_total=0\nTRANSLATION_SYMMETRY=false\n')
+    m = ed.parse_parameters(txt)
+    _, _, ob3 = lattice.lattice_graph("anisotropic square lattice", {"L": 10, "W": 3})
+    assert [[b[0], b[1]] for b in m["bonds"]] == [[s, t] for s, t, _ in ob3]
+    # J per bond type: type 0 -> J0, type 1 -> J1
+    assert [b[2] for b in m["bonds"]] == [1.0 if t == 0 else 2.0 for _, _, t in ob3]
+
+
+def test_parameter_file_syntax_and_defaults():
+    txt = """// sparsediag job
+    MODEL = "spin"; LATTICE = "nnn chain lattice"
+    L = 2*7, J = 1
+    J1 = 1/4
+    local_S = 1/2
+    CONSERVED_QUANTUMNUMBERS = "Sz"
+    Sz_total = 1
+    TRANSLATION_SYMMETRY = false
+    NUMBER_EIGENVALUES = 3
+    MAX_ITERATIONS = 200
+    h = 0.1
+    """
+    m = ed.parse_parameters(txt)
+    assert m["n_sites"] == 14 and m["n_up"] == 8
+    assert m["nev"] == 3 and m["max_iter"] == 200
+    assert m["bonds"][1][2] == 0.25 and m["bonds"][0][2] == 1.0
+    assert np.allclose(m["site_h"], 0.1)
+
+
+@pytest.mark.parametrize("bad,msg", [
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n', "TRANSLATION"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nTRANSLATION_SYMMETRY=false\nCONSERVED_QUANTUMNUMBERS="Sz"\n',
+     "Sz_total"),
+    ('MODEL="boson Hubbard"\nLATTICE="chain lattice"\nL=8\n', "MODEL"),
+    ('MODEL="spin"\nLATTICE="kagome lattice"\nL=8\n', "LATTICE"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nlocal_S=1\n', "local_S"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=40\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n'
+     'TRANSLATION_SYMMETRY=false\n', "sites"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n'
+     'TRANSLATION_SYMMETRY=false\nJ="0.8+0.4*random()"\n', "random"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nCONSERVED_QUANTUMNUMBERS="N"\n', "Sz"),
+])
+def test_parameter_errors(bad, msg):
+    with pytest.raises(ed.AEDError) as e:
+        ed.parse_parameters(bad)
+    assert e.value.code == ed.ERR_INVALID
+    assert msg in str(e.value)
+
+
+def test_create_reports_invalid_models_before_touching_a_device():
+    with pytest.raises(ed.AEDError) as e:
+        ed.Hamiltonian(40, 20, [])
+    assert e.value.code in (ed.ERR_INVALID, ed.ERR_CUDA)
+    with pytest.raises(ed.AEDError):
+        ed.Hamiltonian(4, 2, [(0, 0, 1.0, 1.0)])
+
+
+def test_create_without_gpu_fails_loudly():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except Exception:
+        pass
+    with pytest.raises(ed.AEDError) as e:
+        ed.Hamiltonian(4, 2, [(0, 1, 1.0, 1.0), (1, 2, 1.0, 1.0)])
+    assert e.value.code == ed.ERR_CUDA

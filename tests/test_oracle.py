@@ -1,0 +1,209 @@
+"""The oracle pinned against the reference's own golden outputs, LAPACK and closed forms (CPU)."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import lattice
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def gold(name):
+    with open(os.path.join(GOLD, name)) as f:
+        return json.load(f)
+
+
+def sz_rows_to_bits(rows):
+    """[+1/-1 per site] -> bit strings, site 0 most significant (up = 1)."""
+    n = len(rows[0])
+    out = []
+    for r in rows:
+        v = 0
+        for s, sz in enumerate(r):
+            if sz > 0:
+                v |= 1 << (n - 1 - s)
+        out.append(v)
+    return np.array(out, dtype=np.uint32)
+
+
+def test_basis_example10_full_space_order():
+    g = gold("basis_example10.json")
+    bits = sz_rows_to_bits(g["states_sz"])
+    # no constraint: all 16 states, lexicographic with site 0 most significant
+    assert list(bits) == list(range(16))
+    # the union of the Sz sectors of the oracle, in order, is the same list
+    union = np.sort(np.concatenate([oracle.basis(4, k) for k in range(5)]))
+    assert list(union) == list(bits)
+
+
+def test_basis_example12_sz0_order():
+    g = gold("basis_example12.json")
+    bits = sz_rows_to_bits(g["states_sz"])
+    assert list(oracle.basis(4, 2)) == list(bits)
+
+
+@pytest.mark.parametrize("N,k", [(1, 0), (5, 2), (8, 4), (12, 5), (16, 8), (10, 0), (10, 10)])
+def test_basis_is_ascending_popcount_sector(N, k):
+    from math import comb
+
+    b = oracle.basis(N, k)
+    assert b.size == comb(N, k)
+    assert np.all(np.diff(b.astype(np.int64)) > 0)
+    assert all(bin(int(v)).count("1") == k for v in b)
+    # lower_bound index and "absent" -> D
+    for i in [0, b.size // 2, b.size - 1]:
+        assert oracle.index(b, int(b[i])) == i
+    if k < N:
+        absent = (1 << N) - 1
+        assert oracle.index(b, absent) == b.size
+
+
+def test_lattice_example5_sites():
+    g = gold("lattice_example5.json")
+    n, coords, _ = lattice.lattice_graph(g["params"]["LATTICE"], g["params"])
+    assert n == len(g["sites"])
+    for s in g["sites"]:
+        assert [float(c) for c in coords[s["site"]]] == s["coords"]
+
+
+def test_lattice_example6_bonds():
+    g = gold("lattice_example6.json")
+    _, _, bonds = lattice.lattice_graph(g["params"]["LATTICE"], g["params"])
+    assert [list(b) for b in bonds] == g["bonds"]
+
+
+def _eval_matrix_expr(expr, vals):
+    e = expr.replace(" ", "")
+    for k, v in vals.items():
+        e = e.replace(k, f"({v!r})")
+    return eval(e) if e else 0.0
+
+
+def _nested_eval(obj, vals):
+    if isinstance(obj, list):
+        return [_nested_eval(o, vals) for o in obj]
+    return _eval_matrix_expr(obj, vals)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_spin_bond_and_site_terms_example3_example4(seed):
+    rng = np.random.default_rng(seed)
+    jz, jxy, k, h, d = rng.uniform(-2, 2, 5)
+    vals = {"Jz0": jz, "Jxy0": jxy, "K0": k, "h0": h, "D0": d, "Gamma0": 0.0}
+    # two sites, one bond, both site terms: the reference's HSpinHalf (example4)
+    g4 = np.array(_nested_eval(gold("spin_half_example4.json")["HSpinHalf"], vals), dtype=float)
+    full = np.zeros((4, 4))
+    for nup in range(3):
+        m = oracle.Matrix(2, nup, [(0, 1, jz, jxy, k)], site_h=[h, h], site_d=[d, d])
+        st = m.states()
+        dm = m.dense()
+        for a in range(m.D):
+            for b in range(m.D):
+                full[st[a], st[b]] = dm[a, b]
+    # HSpinHalf rows/cols are the two-site product states in order (0,0),(0,1),(1,0),(1,1)
+    # of the site-basis index, i.e. bit strings 00,01,10,11
+    np.testing.assert_allclose(full, g4, rtol=0, atol=1e-13)
+    # bond tensor alone (example3 HSpinBond): [is1][is2][js1][js2]
+    g3 = np.array(_nested_eval(gold("spin_terms_example3.json")["HSpinBond"], vals), dtype=float)
+    full_b = np.zeros((4, 4))
+    for nup in range(3):
+        m = oracle.Matrix(2, nup, [(0, 1, jz, jxy, k)])
+        st = m.states()
+        dm = m.dense()
+        for a in range(m.D):
+            for b in range(m.D):
+                full_b[st[a], st[b]] = dm[a, b]
+    for is1 in range(2):
+        for is2 in range(2):
+            for js1 in range(2):
+                for js2 in range(2):
+                    # M(i,j) with i = source (is1,is2), j = target (js1,js2)
+                    assert abs(full_b[(is1 << 1) | is2, (js1 << 1) | js2] - g3[is1][is2][js1][js2]) < 1e-13
+
+
+def test_stev_matches_lapack():
+    from scipy.linalg import lapack
+
+    rng = np.random.default_rng(5)
+    for n in [1, 2, 3, 10, 57, 200]:
+        d = rng.normal(size=n)
+        e = rng.uniform(0.1, 1, size=max(n - 1, 0))
+        w, zl, zf = oracle.stev(d, e, want_last=True, want_full=True)
+        if n > 1:
+            wl, zz, info = lapack.dstev(d.copy(), e.copy(), compute_v=1)[:3]
+        else:
+            wl, zz = d.copy(), np.ones((1, 1))
+        np.testing.assert_allclose(w, wl, rtol=0, atol=1e-13 * max(1, np.abs(wl).max()))
+        np.testing.assert_allclose(np.abs(zl), np.abs(zz[-1]), atol=1e-10)
+        T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+        np.testing.assert_allclose(T @ zf, zf * w, atol=1e-11)
+
+
+def test_tmatrix_rules_match_lapack_restatement():
+    p = {"LATTICE": "chain lattice", "L": 14, "J": 1, "Sz_total": 0}
+    N, nu, bonds = lattice.spin_model(p)
+    M = oracle.Matrix(N, nu, bonds)
+    r = M.lanczos(nev=4, seed=11)
+    a, b = r["alpha"], r["beta"]
+    for m in [2, 5, 20, len(a) // 2, len(a)]:
+        t1 = oracle.tmatrix(a[:m], b[:m])
+        t2 = oracle.tmatrix_lapack(a[:m], b[:m])
+        assert len(t1["evals"]) == len(t2["evals"])
+        np.testing.assert_allclose(t1["evals"], t2["evals"], rtol=1e-12, atol=1e-12)
+        assert list(t1["mults"]) == list(t2["mults"])
+        np.testing.assert_allclose(t1["errors"], t2["errors"], rtol=1e-5, atol=1e-14)
+
+
+def test_closed_forms():
+    eps = 1e-12
+    # two-site dimer: singlet -3J/4
+    m = oracle.Matrix(2, 1, [(0, 1, 1.0, 1.0, 0.0)])
+    assert abs(np.linalg.eigvalsh(m.dense())[0] + 0.75) < eps
+    # 4-site ring: -2J
+    p = {"LATTICE": "chain lattice", "L": 4, "J": 1, "Sz_total": 0}
+    N, nu, bonds = lattice.spin_model(p)
+    m = oracle.Matrix(N, nu, bonds)
+    assert abs(np.linalg.eigvalsh(m.dense())[0] + 2.0) < eps
+    # Majumdar-Ghosh point of the J1-J2 chain (J2 = J1/2, periodic even L): -3 L / 8
+    for L in (8, 10, 12):
+        p = {"LATTICE": "nnn chain lattice", "L": L, "J": 1, "J1": 0.5, "Sz_total": 0}
+        N, nu, bonds = lattice.spin_model(p)
+        m = oracle.Matrix(N, nu, bonds)
+        r = m.lanczos(nev=1, seed=3)
+        assert abs(r["evals"][0] + 3 * L / 8) < 1e-11
+
+
+@pytest.mark.parametrize("params,nev", [
+    ({"LATTICE": "chain lattice", "L": 12, "J": 1, "Sz_total": 0}, 4),
+    ({"LATTICE": "nnn chain lattice", "L": 12, "J": 1, "J1": 0.37, "Sz_total": 0}, 2),
+    ({"LATTICE": "ladder", "L": 5, "J0": 1.1, "J1": 0.7, "Sz_total": 0}, 3),
+    ({"LATTICE": "square lattice", "L": 3, "W": 4, "J": 1, "Sz_total": 1}, 2),
+    ({"LATTICE": "open chain lattice", "L": 11, "J": 1, "Sz_total": 0.5}, 2),
+])
+def test_oracle_lanczos_matches_dense(params, nev):
+    N, nu, bonds = lattice.spin_model(params)
+    m = oracle.Matrix(N, nu, bonds)
+    w = np.linalg.eigvalsh(m.dense())
+    distinct = [w[0]]
+    for v in w[1:]:
+        if v - distinct[-1] > 1e-8:
+            distinct.append(v)
+    r = m.lanczos(nev=nev, seed=7)
+    np.testing.assert_allclose(r["evals"], distinct[:nev], rtol=1e-12, atol=1e-12)
+    assert r["fail"] == 0
+
+
+def test_csr_is_symmetric_and_matches_matfree():
+    p = {"LATTICE": "nnn chain lattice", "L": 12, "J": 1, "J1": 0.3, "Sz_total": 0}
+    N, nu, bonds = lattice.spin_model(p)
+    m = oracle.Matrix(N, nu, bonds)
+    H = m.dense()
+    assert np.array_equal(H, H.T)
+    x = np.random.default_rng(0).normal(size=m.D)
+    y1 = m.mult(x)
+    y2 = oracle.hv_matfree(N, m.states(), bonds, x)
+    assert np.array_equal(y1, y2)
