@@ -84,7 +84,30 @@ int handle_pinned(aed_handle* h, size_t n, double** out) {
   return AED_OK;
 }
 
+void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes) {
+  if (chunk_bytes != h->store_chunk_bytes) {
+    cudaStreamSynchronize(h->stream);
+    for (void* p : h->store_chunks) cudaFree(p);
+    h->store_chunks.clear();
+    h->store_chunk_bytes = chunk_bytes;
+  }
+  while ((int)h->store_chunks.size() <= c) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, chunk_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      fail(AED_ERR_NOMEM, "device memory exhausted by the FP32 Lanczos basis (" +
+                              std::to_string(h->store_chunks.size() * kStoreChunk) + " vectors)");
+      return nullptr;
+    }
+    h->store_chunks.push_back(p);
+  }
+  return h->store_chunks[c];
+}
+
 void handle_release_workspace(aed_handle* h) {
+  for (void* p : h->store_chunks) cudaFree(p);
+  h->store_chunks.clear();
+  h->store_chunk_bytes = 0;
   for (int k = 0; k < 2; ++k) {
     if (h->ws[k]) cudaFree(h->ws[k]);
     h->ws[k] = nullptr;
@@ -159,7 +182,7 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     return rc;
   }
   std::vector<uint32_t> th, tr;
-  build_tiles(h->tab, kHvThreads, th, tr);
+  build_tiles(h->tab, kHvTileRows, th, tr);
   const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
   if ((rc = dev_alloc(&h->d_thi, nhi)) || (rc = dev_alloc(&h->d_tlo, nlo)) || (rc = dev_alloc(&h->d_lolist, nlo)) ||
       (rc = dev_alloc(&h->d_looff, h->tab.looff.size())) || (rc = dev_alloc(&h->d_tile_h, th.size())) ||

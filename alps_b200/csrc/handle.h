@@ -33,6 +33,8 @@ struct aed_handle {
   // recurrence, slot 1 = FP32 Lanczos basis store of the mixed path
   void* ws[2] = {nullptr, nullptr};
   size_t ws_bytes[2] = {0, 0};
+  std::vector<void*> store_chunks;  // FP32 Lanczos basis of the mixed path, kStoreChunk vectors each
+  size_t store_chunk_bytes = 0;
   double* h_ab = nullptr;  // pinned alpha/beta staging
   size_t h_ab_n = 0;
   // last solve
@@ -60,6 +62,9 @@ int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_par
 int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out);
 int handle_pinned(aed_handle* h, size_t n, double** out);
 void handle_release_workspace(aed_handle* h);
+constexpr int kStoreChunk = 16;
+// Pointer to chunk `c` of the FP32 basis store (allocated on first use), or nullptr.
+void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes);
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r);
 
 }  // namespace aed

@@ -17,11 +17,6 @@
 namespace aed {
 namespace {
 
-__device__ __forceinline__ uint32_t rank_of(uint32_t s, int Nlo, uint32_t lomask, const uint32_t* __restrict__ thi,
-                                            const uint16_t* __restrict__ tlo) {
-  return __ldg(thi + (s >> Nlo)) + (uint32_t)__ldg(tlo + (s & lomask));
-}
-
 // Fixed-shape block reduction: warp shuffles, then warp 0 over the warp sums.
 // Same order on every call, so the result is bitwise reproducible.  The
 // total is returned to every thread.
@@ -52,40 +47,48 @@ __device__ __forceinline__ double sum_partials(const double* __restrict__ p, int
 }
 
 // ---------------------------------------------------------------------------
-// FP64 row: bit-identical to y = prod(M, x) over the reference's explicit
-// matrix (src/ietl/interface/ublas.h:57-63 over hamiltonian_matrix.hpp:307-345).
-// A row of M holds the flips to smaller states (ascending column = hi bit
+// The apply.  A tile is up to kHvThreads*kRowsPerThread consecutive rows of one
+// hi block h (all its states share the high Nhi bits), so for every flip pair
+// the target's hi block h' = h ^ (flip >> Nlo) is the same for the whole tile:
+// its base row thi[h'] is looked up once per tile into shared memory.  The
+// target's row is then base + tlo[l'] (l' = l ^ lo part of the flip), or
+// base + r when the flip leaves the lo bits alone.  The coupling tables are
+// staged in shared memory once per CTA (reading them with a loop index from
+// parameter space serialises on the constant-load path), and each thread
+// carries kRowsPerThread rows through every table entry.
+//
+// FP64 rows are bit-identical to y = prod(M, x) over the reference's explicit
+// matrix (src/ietl/interface/ublas.h:57-63 over hamiltonian_matrix.hpp:307-345):
+// a row of M holds the flips to smaller states (ascending column = hi bit
 // descending, then lo bit ascending), the diagonal M(i,i), then the flips to
-// larger states (hi ascending, lo descending).  Products and sums round
-// separately (__dmul_rn/__dadd_rn: no FMA contraction), as on the reference's
-// x86-64 build.  M(i,i) is accumulated in the reference's term order.
+// larger states (hi ascending, lo descending), summed left to right from 0.
+// Products and sums round separately (__dmul_rn/__dadd_rn: no FMA
+// contraction), as on the reference's x86-64 build; M(i,i) is accumulated in
+// the reference's term order (sites, then bonds).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double row_f64(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* __restrict__ thi,
-                                          const uint16_t* __restrict__ tlo, const double* __restrict__ x) {
-  const int Nlo = P.Nlo;
-  const uint32_t lm = P.lomask;
-  double acc = 0.0;
-  for (int q = 0; q < P.n_pairs; ++q) {
-    const uint32_t mh = P.low[q].mhi, ml = P.low[q].mlo;
-    if ((s & (mh | ml)) == mh) {
-      const double xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
-      acc = __dadd_rn(acc, __dmul_rn(P.low[q].c, xv));
-    }
-  }
-  double d = 0.0;
-  for (int q = 0; q < P.n_diag; ++q) {
-    const bool eq = ((s & P.diag[q].m1) != 0u) == ((s & P.diag[q].m2) != 0u);
-    d = __dadd_rn(d, eq ? P.diag[q].veq : P.diag[q].vne);
-  }
-  acc = __dadd_rn(acc, __dmul_rn(d, __ldg(x + i)));
-  for (int q = 0; q < P.n_pairs; ++q) {
-    const uint32_t mh = P.rise[q].mhi, ml = P.rise[q].mlo;
-    if ((s & (mh | ml)) == ml) {
-      const double xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
-      acc = __dadd_rn(acc, __dmul_rn(P.rise[q].c, xv));
-    }
-  }
-  return acc;
+constexpr int kRowsPerThread = 4;
+constexpr int kTileRows = kHvThreads * kRowsPerThread;
+static_assert(kTileRows == kHvTileRows, "tile size");
+
+enum : uint32_t { kLoLo = 0, kHiHi = 1, kCross = 2 };
+
+struct SPair {
+  uint32_t flip;    // both bits
+  uint32_t cond;    // (s & flip) == cond selects the rows this entry applies to
+  uint32_t loflip;  // flip & lomask
+  uint32_t cat;     // kLoLo / kHiHi / kCross
+  double c;
+  float chi, clo;
+};
+
+struct SDiag {
+  uint32_t m1, m2;
+  double veq, vne;
+};
+
+__device__ __forceinline__ uint32_t pair_cat(uint32_t flip, uint32_t lomask) {
+  const uint32_t lo = flip & lomask, hi = flip & ~lomask;
+  return hi == 0u ? kLoLo : (lo == 0u ? kHiHi : kCross);
 }
 
 // Error-free transformations: TwoSum (Knuth, TAOCP Vol. 2, 4.2.2) and the
@@ -105,69 +108,134 @@ struct Comp32 {
   __device__ __forceinline__ float value() const { return __fadd_rn(s, c); }
 };
 
-// FP32 row with compensated accumulation; order of terms is free here.
-__device__ __forceinline__ float row_f32(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* __restrict__ thi,
-                                         const uint16_t* __restrict__ tlo, const float* __restrict__ x) {
-  const int Nlo = P.Nlo;
-  const uint32_t lm = P.lomask;
-  Comp32 acc;
-  double d = 0.0;
-  for (int q = 0; q < P.n_diag; ++q) {
-    const bool eq = ((s & P.diag[q].m1) != 0u) == ((s & P.diag[q].m2) != 0u);
-    d += eq ? P.diag[q].veq : P.diag[q].vne;
-  }
-  {
-    const float dh = (float)d, dl = (float)(d - (double)dh);
-    acc.add_prod(dh, dl, __ldg(x + i));
-  }
-  for (int q = 0; q < P.n_pairs; ++q) {
-    const uint32_t mh = P.low[q].mhi, ml = P.low[q].mlo;
-    const uint32_t b = s & (mh | ml);
-    if (b == mh || b == ml) {
-      const float xv = __ldg(x + rank_of(s ^ (mh | ml), Nlo, lm, thi, tlo));
-      acc.add_prod(P.low[q].chi, P.low[q].clo, xv);
-    }
-  }
-  return acc.value();
-}
-
-template <typename T>
-__device__ __forceinline__ T row_value(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
-                                       const uint16_t* tlo, const T* x);
-template <>
-__device__ __forceinline__ double row_value<double>(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
-                                                    const uint16_t* tlo, const double* x) {
-  return row_f64(P, s, i, thi, tlo, x);
-}
-template <>
-__device__ __forceinline__ float row_value<float>(const HvParams& P, uint32_t s, uint32_t i, const uint32_t* thi,
-                                                  const uint16_t* tlo, const float* x) {
-  return row_f32(P, s, i, thi, tlo, x);
-}
-
-// y = H x over tiles (hi block h, rows r0 .. r0+kHvThreads-1).  CTAs take
-// tiles blockIdx.x, blockIdx.x + gridDim.x, ...: a static assignment, so the
-// per-CTA partial sums of x_i*y_i (for the fused Lanczos step) are
-// reproducible bit for bit.
 template <typename T>
 __global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ HvParams P, const DevTables t,
                                                         const T* __restrict__ x, T* __restrict__ y,
                                                         double* __restrict__ alpha_part) {
+  constexpr bool kF64 = sizeof(T) == 8;
+  constexpr int R = kRowsPerThread;
+  __shared__ SPair s_low[kMaxBonds];
+  __shared__ SPair s_rise[kMaxBonds];
+  __shared__ SDiag s_diag[kMaxDiag];
+  __shared__ uint32_t s_nb_low[kMaxBonds];
+  __shared__ uint32_t s_nb_rise[kMaxBonds];
   __shared__ double sm[33];
+  const int np = P.n_pairs, nd = P.n_diag, Nlo = P.Nlo;
+  const uint32_t lm = P.lomask;
+  for (int q = threadIdx.x; q < np; q += kHvThreads) {
+    const PairTerm a = P.low[q], b = P.rise[q];
+    const uint32_t fa = a.mhi | a.mlo, fb = b.mhi | b.mlo;
+    // FP64: "low" entries take rows with the hi bit set (target < source),
+    // "rise" entries rows with the lo bit set.  FP32 uses s_low for both
+    // directions (cond is tested as "exactly one bit set" there).
+    s_low[q] = {fa, a.mhi, fa & lm, pair_cat(fa, lm), a.c, a.chi, a.clo};
+    s_rise[q] = {fb, b.mlo, fb & lm, pair_cat(fb, lm), b.c, b.chi, b.clo};
+  }
+  for (int q = threadIdx.x; q < nd; q += kHvThreads) s_diag[q] = {P.diag[q].m1, P.diag[q].m2, P.diag[q].veq, P.diag[q].vne};
   double dotacc = 0.0;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
     const uint32_t h = __ldg(t.tile_h + it);
-    const uint32_t r = __ldg(t.tile_r + it) + threadIdx.x;
+    const uint32_t r0 = __ldg(t.tile_r + it);
     const int k = P.n_up - __popc(h);
-    const uint32_t base = __ldg(t.looff + k);
-    const uint32_t rows = __ldg(t.looff + k + 1) - base;
-    if (r < rows) {
-      const uint32_t l = __ldg(t.lolist + base + r);
-      const uint32_t s = (h << P.Nlo) | l;
-      const uint32_t i = __ldg(t.thi + h) + r;
-      const T v = row_value<T>(P, s, i, t.thi, t.tlo, x);
-      y[i] = v;
-      if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
+    const uint32_t lbase = __ldg(t.looff + k);
+    const uint32_t rows = __ldg(t.looff + k + 1) - lbase;
+    const uint32_t base = __ldg(t.thi + h);
+    __syncthreads();  // previous tile done with s_nb_*; tables staged
+    for (int q = threadIdx.x; q < np; q += kHvThreads) {
+      s_nb_low[q] = __ldg(t.thi + (h ^ (s_low[q].flip >> Nlo)));
+      if (kF64) s_nb_rise[q] = __ldg(t.thi + (h ^ (s_rise[q].flip >> Nlo)));
+    }
+    __syncthreads();
+    uint32_t rr[R], sv[R], lv[R];
+    bool ok[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      rr[u] = r0 + threadIdx.x + u * kHvThreads;
+      ok[u] = rr[u] < rows && rr[u] < r0 + kTileRows;
+      lv[u] = ok[u] ? (uint32_t)__ldg(t.lolist + lbase + rr[u]) : 0u;
+      sv[u] = (h << Nlo) | lv[u];
+    }
+    T out[R];
+    if constexpr (kF64) {
+      double acc[R], d[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) acc[u] = 0.0, d[u] = 0.0;
+      for (int q = 0; q < np; ++q) {
+        const SPair e = s_low[q];
+        const uint32_t nb = s_nb_low[q];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (ok[u] && (sv[u] & e.flip) == e.cond) {
+            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
+            acc[u] = __dadd_rn(acc[u], __dmul_rn(e.c, __ldg(x + j)));
+          }
+        }
+      }
+      for (int q = 0; q < nd; ++q) {
+        const SDiag e = s_diag[q];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          const bool eq = ((sv[u] & e.m1) != 0u) == ((sv[u] & e.m2) != 0u);
+          d[u] = __dadd_rn(d[u], eq ? e.veq : e.vne);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (ok[u]) acc[u] = __dadd_rn(acc[u], __dmul_rn(d[u], __ldg(x + base + rr[u])));
+      for (int q = 0; q < np; ++q) {
+        const SPair e = s_rise[q];
+        const uint32_t nb = s_nb_rise[q];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (ok[u] && (sv[u] & e.flip) == e.cond) {
+            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
+            acc[u] = __dadd_rn(acc[u], __dmul_rn(e.c, __ldg(x + j)));
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) out[u] = acc[u];
+    } else {
+      Comp32 acc[R];
+      double d[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) d[u] = 0.0;
+      for (int q = 0; q < nd; ++q) {
+        const SDiag e = s_diag[q];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          const bool eq = ((sv[u] & e.m1) != 0u) == ((sv[u] & e.m2) != 0u);
+          d[u] += eq ? e.veq : e.vne;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        if (ok[u]) {
+          const float dh = (float)d[u], dl = (float)(d[u] - (double)dh);
+          acc[u].add_prod(dh, dl, __ldg(x + base + rr[u]));
+        }
+      }
+      for (int q = 0; q < np; ++q) {
+        const SPair e = s_low[q];
+        const uint32_t nb = s_nb_low[q];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          const uint32_t bsel = sv[u] & e.flip;
+          if (ok[u] && bsel != 0u && bsel != e.flip) {
+            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
+            acc[u].add_prod(e.chi, e.clo, __ldg(x + j));
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) out[u] = acc[u].value();
+    }
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      if (ok[u]) {
+        y[base + rr[u]] = out[u];
+        if (alpha_part) dotacc += (double)__ldg(x + base + rr[u]) * (double)out[u];
+      }
     }
   }
   if (alpha_part) {
@@ -306,7 +374,7 @@ __global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const do
 // stored vectors; coefficients are staged in shared memory in chunks.
 __global__ void __launch_bounds__(256) ritz_combine_kernel(const float* __restrict__ V, int64_t ld, int m,
                                                           const double* __restrict__ coef, double* __restrict__ out,
-                                                          int64_t n) {
+                                                          int64_t n, bool accumulate) {
   __shared__ double cs[512];
   const int64_t stride = (int64_t)gridDim.x * 256;
   for (int64_t base = (int64_t)blockIdx.x * 256; base < n; base += stride) {
@@ -320,7 +388,7 @@ __global__ void __launch_bounds__(256) ritz_combine_kernel(const float* __restri
       if (i < n)
         for (int q = 0; q < cnt; ++q) acc = fma(cs[q], (double)__ldg(V + (int64_t)(j0 + q) * ld + i), acc);
     }
-    if (i < n) out[i] = acc;
+    if (i < n) out[i] = accumulate ? out[i] + acc : acc;
   }
 }
 
@@ -357,9 +425,9 @@ int red_grid_size() { return num_sms() * 4; }
 int64_t launch_count() { return g_launches.load(); }
 
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
-                        cudaStream_t st) {
+                        bool accumulate, cudaStream_t st) {
   if (m < 1 || m > kMaxRitzTerms) return fail(AED_ERR_INVALID, "ritz_combine: bad number of terms");
-  ritz_combine_kernel<<<elem_grid(n), 256, 0, st>>>(V, ld, m, coef, out, n);
+  ritz_combine_kernel<<<elem_grid(n), 256, 0, st>>>(V, ld, m, coef, out, n, accumulate);
   return check_launch("ritz_combine_kernel");
 }
 

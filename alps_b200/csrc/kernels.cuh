@@ -23,6 +23,7 @@ struct DevTables {
 };
 
 constexpr int kHvThreads = 256;
+constexpr int kHvTileRows = 1024;  // rows per work tile (kHvThreads x rows per thread)
 constexpr int kRedThreads = 256;
 
 // y = H x.  alpha_part (optional): per-CTA partial sums of x_i * y_i.
@@ -69,7 +70,7 @@ int launch_lanczos_normalize(const double* partB, int nB, T* y, int64_t n, doubl
 // coef in device memory (m <= kMaxRitzTerms).
 constexpr int kMaxRitzTerms = 4096;
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
-                        cudaStream_t st);
+                        bool accumulate, cudaStream_t st);
 
 int red_grid_size();
 int64_t launch_count();

@@ -200,13 +200,20 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters,
   int launched = 0;
   int m = 1;
   *failed = 0;
-  int rc = R.launch_step(0, nullptr, slot(0), slot(1));
+  void* s0 = slot(0);
+  void* s1 = slot(1);
+  if (!s0 || !s1) return AED_ERR_NOMEM;
+  int rc = R.launch_step(0, nullptr, s0, s1);
   if (rc) return rc;
   launched = 1;
   while (true) {
     // keep the device one step ahead of the host analysis
     while (launched < m + 1 && launched < R.max_iter) {
-      rc = R.launch_step(launched, slot(launched - 1), slot(launched), slot(launched + 1));
+      void* a = slot(launched - 1);
+      void* b = slot(launched);
+      void* c = slot(launched + 1);
+      if (!a || !b || !c) return AED_ERR_NOMEM;
+      rc = R.launch_step(launched, a, b, c);
       if (rc) return rc;
       ++launched;
     }
@@ -279,62 +286,60 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
 int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev, int max_iter, double rtol,
                 double atol, bool profile, aed_solve_result* r) {
   const int64_t D = h->tab.D;
-  // Lanczos basis store: as many FP32 vectors as fit (bounded by max_iter+1)
-  size_t free_b = 0, total_b = 0;
-  AED_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  // Lanczos basis store: chunks of kStoreChunk FP32 vectors, grown as the
+  // recurrence advances and kept by the handle for later solves
   const size_t vbytes = (((size_t)D * 4 + 255) & ~(size_t)255);
-  const size_t s64 = (((size_t)D * 8 + 255) & ~(size_t)255);
-  // keep room for the FP64 refinement's three vectors and some slack
-  const size_t reserve = (h->ws_bytes[0] >= 3 * s64 ? 0 : 3 * s64) + s64 + ((size_t)256 << 20);
-  int cap = max_iter + 1;
-  const size_t have = free_b + h->ws_bytes[1];
-  if (have > reserve) {
-    const size_t fit = (have - reserve) / vbytes;
-    if ((size_t)cap > fit) cap = (int)fit;
-  } else {
-    cap = 0;
-  }
-  if (cap > kMaxRitzTerms) cap = kMaxRitzTerms;
-  if (cap < 8) return fail(AED_ERR_NOMEM, "not enough device memory for the FP32 Lanczos basis");
+  const int64_t ldv = (int64_t)(vbytes / 4);  // stride of the stored vectors (256-byte aligned)
+  const size_t chunk_bytes = vbytes * kStoreChunk;
+  const int cap = std::min(max_iter + 1, kMaxRitzTerms);
   HostPinned hab;
   EventRing ring;
+  DevMem small;  // start64 | alpha/beta pairs | Ritz coefficients
   int rc;
-  void* ws1 = nullptr;
+  const size_t s64 = (((size_t)D * 8 + 255) & ~(size_t)255);
   const size_t ab_bytes = (((size_t)2 * (cap + 2) * 8 + 255) & ~(size_t)255);
-  const size_t coef_bytes = (((size_t)cap * 8 + 255) & ~(size_t)255);
-  if ((rc = handle_workspace(h, 1, vbytes * cap + s64 + ab_bytes + coef_bytes, &ws1)) ||
-      (rc = hab.alloc((size_t)2 * (cap + 2))) || (rc = ring.init()))
+  if ((rc = small.alloc(s64 + ab_bytes + (size_t)kStoreChunk * 8)) || (rc = hab.alloc((size_t)2 * (cap + 2))) ||
+      (rc = ring.init()))
     return rc;
-  struct {
-    void* p;
-  } store{ws1}, start64{(char*)ws1 + vbytes * cap}, ab{(char*)ws1 + vbytes * cap + s64},
-      coef{(char*)ws1 + vbytes * cap + s64 + ab_bytes};
-  float* V = (float*)store.p;
-  const int64_t ldv = (int64_t)(vbytes / 4);  // stride of the stored vectors (256-byte aligned)
+  double* start64 = (double*)small.p;
+  double* d_ab = (double*)((char*)small.p + s64);
+  double* coef = (double*)((char*)small.p + s64 + ab_bytes);
+  bool oom = false;
+  auto slot = [&](int j) -> void* {
+    char* c = (char*)handle_store_chunk(h, j / kStoreChunk, chunk_bytes);
+    if (!c) {
+      oom = true;
+      return nullptr;
+    }
+    return c + (size_t)(j % kStoreChunk) * vbytes;
+  };
+  float* V0 = (float*)slot(0);
+  if (!V0) return AED_ERR_NOMEM;
   if (start_host) {
     std::vector<float> tmp(D);
     for (int64_t i = 0; i < D; ++i) tmp[i] = (float)start_host[i];
-    AED_CUDA_TRY(cudaMemcpyAsync(V, tmp.data(), (size_t)D * 4, cudaMemcpyHostToDevice, h->stream));
+    AED_CUDA_TRY(cudaMemcpyAsync(V0, tmp.data(), (size_t)D * 4, cudaMemcpyHostToDevice, h->stream));
     AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  } else if ((rc = launch_fill_random(V, D, seed, h->stream))) {
+  } else if ((rc = launch_fill_random(V0, D, seed, h->stream))) {
     return rc;
   }
-  if ((rc = normalize(h, V, D))) return rc;
+  if ((rc = normalize(h, V0, D))) return rc;
   // phase 1: FP32 vectors, stop at FP32-level residual estimates
-  const int max1 = cap - 1;
-  Recurrence R{h, true, D, max1, (double*)ab.p, hab.p, &ring, {}, {}, 0, 0, profile, {}};
+  Recurrence R{h, true, D, cap - 1, d_ab, hab.p, &ring, {}, {}, 0, 0, profile, {}};
   const double tol32 = 2e-6;
   StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
   int it1 = 0, failed1 = 0;
-  rc = run_recurrence(R, stop1, [&](int j) { return (void*)(V + (int64_t)j * ldv); }, &it1, &failed1, T1);
+  rc = run_recurrence(R, stop1, slot, &it1, &failed1, T1);
+  if (oom) return AED_ERR_NOMEM;
   if (rc) return rc;
   const int m1 = it1;
   const int n1 = std::min(nev, (int)T1.evals.size());
   for (int i = 0; i < n1; ++i) r->evals_low[i] = T1.evals[i];
   r->iterations_low = m1;
   const double apply32_ms = profile ? R.apply_ms() : 0.0;
-  // Ritz vectors: eigenvectors of T(m1), combined with equal weights
+  // Ritz vectors: eigenvectors of T(m1), combined with equal weights, accumulated
+  // in FP64 chunk by chunk from the stored basis
   std::vector<double> ev(R.alpha.begin(), R.alpha.begin() + m1), e(m1 + 1, 0.0), Z((size_t)m1 * m1);
   for (int i = 0; i + 1 < m1; ++i) e[i] = R.beta[i];
   if (tridiag_eigen(m1, ev.data(), e.data(), nullptr, Z.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
@@ -343,14 +348,17 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
     const int k = T1.first[i];
     for (int j = 0; j < m1; ++j) c[j] += Z[(size_t)k * m1 + j];
   }
-  AED_CUDA_TRY(cudaMemcpyAsync(coef.p, c.data(), m1 * 8, cudaMemcpyHostToDevice, h->stream));
-  if ((rc = launch_ritz_combine(V, ldv, m1, (const double*)coef.p, (double*)start64.p, D, h->stream))) return rc;
-  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
+    const int cnt = std::min(kStoreChunk, m1 - j0);
+    AED_CUDA_TRY(cudaMemcpyAsync(coef, c.data() + j0, cnt * 8, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = launch_ritz_combine((const float*)slot(j0), ldv, cnt, coef, start64, D, j0 > 0, h->stream))) return rc;
+    // the coefficient buffer is reused by the next chunk: order the host copy after this kernel
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
   // phase 2: FP64 refinement from the Ritz combination
   TmatInfo T2;
   const int max2 = std::max(max_iter, nev + 4);
-  rc = solve_fp64(h, nullptr, (const double*)start64.p, seed, nev, max2, rtol, atol, true, 1e-12, nev + 2, false, r,
-                  T2);
+  rc = solve_fp64(h, nullptr, start64, seed, nev, max2, rtol, atol, true, 1e-12, nev + 2, false, r, T2);
   // apply_ms of a mixed solve: the FP32 applies (the bulk of the work)
   if (profile) r->apply_ms = apply32_ms;
   return rc;

@@ -289,6 +289,8 @@ def run_ours(args):
         e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
         e2e = {"value": total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                "path": "aed_create + aed_solve(host start vector) + aed_destroy"}
+    print(f"[bench] fp64: {value:.3f} solves/s, iterations {iters}, apply {t_apply*1e3:.3f} ms "
+          f"({achieved:.0f} GB/s)", file=sys.stderr)
     # mixed precision on the same inputs: FP32 Lanczos basis + FP64 refinement
     mixed = None
     if not args.no_mixed:
@@ -312,6 +314,7 @@ def run_ours(args):
                  "hv_fp32_gbs": b32 / (float(np.mean(m32ms)) / 1e3) / 1e9}
         for h in h32:
             h.close()
+        print(f"[bench] mixed: {mixed}", file=sys.stderr)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(float(j2s[W]), int(round(np.mean(iters))))
