@@ -31,6 +31,7 @@ void release(aed_handle* h) {
   cudaFree(h->d_looff);
   cudaFree(h->d_tile_h);
   cudaFree(h->d_tile_r);
+  cudaFree(h->d_dg);
   cudaFree(h->d_partA);
   cudaFree(h->d_partB);
   cudaFree(h->d_scal);
@@ -186,7 +187,8 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
   if ((rc = dev_alloc(&h->d_thi, nhi)) || (rc = dev_alloc(&h->d_tlo, nlo)) || (rc = dev_alloc(&h->d_lolist, nlo)) ||
       (rc = dev_alloc(&h->d_looff, h->tab.looff.size())) || (rc = dev_alloc(&h->d_tile_h, th.size())) ||
-      (rc = dev_alloc(&h->d_tile_r, tr.size())) || (rc = dev_alloc(&h->d_scal, 8))) {
+      (rc = dev_alloc(&h->d_tile_r, tr.size())) || (rc = dev_alloc(&h->d_scal, 8)) ||
+      (rc = dev_alloc(&h->d_dg, (size_t)h->tab.D))) {
     release(h);
     return rc;
   }
@@ -229,6 +231,13 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   t.Nlo = h->tab.Nlo;
   t.Nhi = h->tab.Nhi;
   t.n_up = h->tab.n_up;
+  t.dg = h->d_dg;
+  rc = launch_diag_table(h->P, t, h->d_dg, h->stream);
+  const cudaError_t e2 = rc ? cudaSuccess : cudaStreamSynchronize(h->stream);
+  if (rc || e2 != cudaSuccess) {
+    release(h);
+    return rc ? rc : fail(AED_ERR_CUDA, std::string("diagonal table: ") + cudaGetErrorString(e2));
+  }
   *out = h;
   return AED_OK;
 }

@@ -23,6 +23,7 @@ struct aed_handle {
   uint32_t* d_looff = nullptr;
   uint32_t* d_tile_h = nullptr;
   uint32_t* d_tile_r = nullptr;
+  double* d_dg = nullptr;     // per-row diagonal
   double* d_partA = nullptr;  // hv_grid partial sums
   double* d_partB = nullptr;  // red_grid partial sums
   double* d_scal = nullptr;   // 8 device scalars

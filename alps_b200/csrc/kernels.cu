@@ -47,15 +47,23 @@ __device__ __forceinline__ double sum_partials(const double* __restrict__ p, int
 }
 
 // ---------------------------------------------------------------------------
-// The apply.  A tile is up to kHvThreads*kRowsPerThread consecutive rows of one
-// hi block h (all its states share the high Nhi bits), so for every flip pair
-// the target's hi block h' = h ^ (flip >> Nlo) is the same for the whole tile:
-// its base row thi[h'] is looked up once per tile into shared memory.  The
-// target's row is then base + tlo[l'] (l' = l ^ lo part of the flip), or
-// base + r when the flip leaves the lo bits alone.  The coupling tables are
-// staged in shared memory once per CTA (reading them with a loop index from
-// parameter space serialises on the constant-load path), and each thread
-// carries kRowsPerThread rows through every table entry.
+// The apply.  A tile is up to kTileRows consecutive rows of one hi block h: all
+// its states share the high Nhi bits.  For such a tile every flip pair falls
+// into one of three cases, decided once per tile:
+//   * both bits in the hi part: the flip applies to all rows of the tile or to
+//     none (it depends on h only); its target is row thi[h'] + r of the hi
+//     block h' = h ^ flip (same lo state, so the same offset r): a coalesced
+//     stream of x;
+//   * one bit in each part: applies iff the lo state has one given bit value;
+//     target thi[h'] + tlo[l ^ bit];
+//   * both bits in the lo part: applies iff the lo state has the two bits in
+//     a given order; target thi[h] + tlo[l ^ flip].
+// Warp 0 compiles the tile's "program": the list of flips that can apply,
+// with their target block base already looked up, in the reference's column
+// order, plus one diagonal entry.  All threads then run the program on
+// kRowsPerThread rows each.  The coupling tables are staged in shared memory
+// once per CTA (indexing them from parameter space with a loop counter
+// serialises on the constant-load path).
 //
 // FP64 rows are bit-identical to y = prod(M, x) over the reference's explicit
 // matrix (src/ietl/interface/ublas.h:57-63 over hamiltonian_matrix.hpp:307-345):
@@ -63,33 +71,35 @@ __device__ __forceinline__ double sum_partials(const double* __restrict__ p, int
 // descending, then lo bit ascending), the diagonal M(i,i), then the flips to
 // larger states (hi ascending, lo descending), summed left to right from 0.
 // Products and sums round separately (__dmul_rn/__dadd_rn: no FMA
-// contraction), as on the reference's x86-64 build; M(i,i) is accumulated in
-// the reference's term order (sites, then bonds).
+// contraction), as on the reference's x86-64 build.  M(i,i) comes from a
+// per-row table filled once per handle in the reference's term order.
 // ---------------------------------------------------------------------------
 constexpr int kRowsPerThread = 4;
 constexpr int kTileRows = kHvThreads * kRowsPerThread;
 static_assert(kTileRows == kHvTileRows, "tile size");
-
-enum : uint32_t { kLoLo = 0, kHiHi = 1, kCross = 2 };
+constexpr uint32_t kDiagOp = 0xffffffffu;
+constexpr int kMaxOps = 2 * kMaxBonds + 1;
 
 struct SPair {
-  uint32_t flip;    // both bits
-  uint32_t cond;    // (s & flip) == cond selects the rows this entry applies to
-  uint32_t loflip;  // flip & lomask
-  uint32_t cat;     // kLoLo / kHiHi / kCross
+  uint32_t flip, cond;
   double c;
   float chi, clo;
 };
 
-struct SDiag {
-  uint32_t m1, m2;
-  double veq, vne;
+// One program entry: mc = lo-part flip | (lo-part condition << 16) (or
+// kDiagOp); nb = base row of the target hi block; c = coupling.
+template <typename T>
+struct TileOp;
+template <>
+struct TileOp<double> {
+  uint32_t mc, nb;
+  double c;
 };
-
-__device__ __forceinline__ uint32_t pair_cat(uint32_t flip, uint32_t lomask) {
-  const uint32_t lo = flip & lomask, hi = flip & ~lomask;
-  return hi == 0u ? kLoLo : (lo == 0u ? kHiHi : kCross);
-}
+template <>
+struct TileOp<float> {
+  uint32_t mc, nb;
+  float chi, clo;
+};
 
 // Error-free transformations: TwoSum (Knuth, TAOCP Vol. 2, 4.2.2) and the
 // FMA-based exact product error.  Compensated row sum in the style of
@@ -109,29 +119,78 @@ struct Comp32 {
 };
 
 template <typename T>
+struct RowAcc;
+template <>
+struct RowAcc<double> {
+  double a = 0.0;
+  __device__ __forceinline__ void add(const TileOp<double>& e, double xv) { a = __dadd_rn(a, __dmul_rn(e.c, xv)); }
+  __device__ __forceinline__ void add_diag(double d, double xv) { a = __dadd_rn(a, __dmul_rn(d, xv)); }
+  __device__ __forceinline__ double value() const { return a; }
+};
+template <>
+struct RowAcc<float> {
+  Comp32 a;
+  __device__ __forceinline__ void add(const TileOp<float>& e, float xv) { a.add_prod(e.chi, e.clo, xv); }
+  __device__ __forceinline__ void add_diag(double d, float xv) {
+    const float dh = (float)d, dl = (float)(d - (double)dh);
+    a.add_prod(dh, dl, xv);
+  }
+  __device__ __forceinline__ float value() const { return a.value(); }
+};
+
+template <typename T>
+__device__ __forceinline__ TileOp<T> make_op(uint32_t mc, uint32_t nb, const SPair& e);
+template <>
+__device__ __forceinline__ TileOp<double> make_op<double>(uint32_t mc, uint32_t nb, const SPair& e) {
+  return {mc, nb, e.c};
+}
+template <>
+__device__ __forceinline__ TileOp<float> make_op<float>(uint32_t mc, uint32_t nb, const SPair& e) {
+  return {mc, nb, e.chi, e.clo};
+}
+
+// Warp 0: append the entries of `list` that can apply in hi block h to prog.
+template <typename T>
+__device__ __forceinline__ int compile_list(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
+                                            const uint32_t* __restrict__ thi, TileOp<T>* prog, int cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int q0 = 0; q0 < np; q0 += 32) {
+    const int q = q0 + lane;
+    bool emit = false;
+    TileOp<T> op;
+    if (q < np) {
+      const SPair e = list[q];
+      const uint32_t fhi = e.flip >> Nlo, chi = e.cond >> Nlo;
+      if ((h & fhi) == chi) {
+        emit = true;
+        op = make_op<T>((e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e);
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, emit);
+    if (emit) prog[cnt + __popc(m & ((1u << lane) - 1u))] = op;
+    cnt += __popc(m);
+  }
+  return cnt;
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ HvParams P, const DevTables t,
                                                         const T* __restrict__ x, T* __restrict__ y,
                                                         double* __restrict__ alpha_part) {
-  constexpr bool kF64 = sizeof(T) == 8;
   constexpr int R = kRowsPerThread;
   __shared__ SPair s_low[kMaxBonds];
   __shared__ SPair s_rise[kMaxBonds];
-  __shared__ SDiag s_diag[kMaxDiag];
-  __shared__ uint32_t s_nb_low[kMaxBonds];
-  __shared__ uint32_t s_nb_rise[kMaxBonds];
+  __shared__ TileOp<T> prog[kMaxOps];
+  __shared__ int s_nops;
   __shared__ double sm[33];
-  const int np = P.n_pairs, nd = P.n_diag, Nlo = P.Nlo;
+  const int np = P.n_pairs, Nlo = P.Nlo;
   const uint32_t lm = P.lomask;
+  // flips to smaller states need the higher bit set, flips to larger states the lower one
   for (int q = threadIdx.x; q < np; q += kHvThreads) {
     const PairTerm a = P.low[q], b = P.rise[q];
-    const uint32_t fa = a.mhi | a.mlo, fb = b.mhi | b.mlo;
-    // FP64: "low" entries take rows with the hi bit set (target < source),
-    // "rise" entries rows with the lo bit set.  FP32 uses s_low for both
-    // directions (cond is tested as "exactly one bit set" there).
-    s_low[q] = {fa, a.mhi, fa & lm, pair_cat(fa, lm), a.c, a.chi, a.clo};
-    s_rise[q] = {fb, b.mlo, fb & lm, pair_cat(fb, lm), b.c, b.chi, b.clo};
+    s_low[q] = {a.mhi | a.mlo, a.mhi, a.c, a.chi, a.clo};
+    s_rise[q] = {b.mhi | b.mlo, b.mlo, b.c, b.chi, b.clo};
   }
-  for (int q = threadIdx.x; q < nd; q += kHvThreads) s_diag[q] = {P.diag[q].m1, P.diag[q].m2, P.diag[q].veq, P.diag[q].vne};
   double dotacc = 0.0;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
     const uint32_t h = __ldg(t.tile_h + it);
@@ -140,107 +199,83 @@ __global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ 
     const uint32_t lbase = __ldg(t.looff + k);
     const uint32_t rows = __ldg(t.looff + k + 1) - lbase;
     const uint32_t base = __ldg(t.thi + h);
-    __syncthreads();  // previous tile done with s_nb_*; tables staged
-    for (int q = threadIdx.x; q < np; q += kHvThreads) {
-      s_nb_low[q] = __ldg(t.thi + (h ^ (s_low[q].flip >> Nlo)));
-      if (kF64) s_nb_rise[q] = __ldg(t.thi + (h ^ (s_rise[q].flip >> Nlo)));
+    __syncthreads();  // tables staged; previous tile done with prog
+    if (threadIdx.x < 32) {
+      int cnt = compile_list<T>(s_low, np, h, Nlo, lm, t.thi, prog, 0);
+      if (threadIdx.x == 0) prog[cnt].mc = kDiagOp;
+      cnt = compile_list<T>(s_rise, np, h, Nlo, lm, t.thi, prog, cnt + 1);
+      if (threadIdx.x == 0) s_nops = cnt;
     }
     __syncthreads();
-    uint32_t rr[R], sv[R], lv[R];
-    bool ok[R];
+    const int nops = s_nops;
+    uint32_t lv[R];
+    uint32_t nrow = 0;  // rows of this thread that exist
 #pragma unroll
     for (int u = 0; u < R; ++u) {
-      rr[u] = r0 + threadIdx.x + u * kHvThreads;
-      ok[u] = rr[u] < rows && rr[u] < r0 + kTileRows;
-      lv[u] = ok[u] ? (uint32_t)__ldg(t.lolist + lbase + rr[u]) : 0u;
-      sv[u] = (h << Nlo) | lv[u];
+      const uint32_t r = r0 + threadIdx.x + u * kHvThreads;
+      const bool ok = r < rows && r < r0 + kTileRows;
+      nrow += ok ? 1u : 0u;
+      lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
     }
-    T out[R];
-    if constexpr (kF64) {
-      double acc[R], d[R];
+    RowAcc<T> acc[R];
+    const uint32_t rt = r0 + threadIdx.x;  // row offset of u = 0
+    for (int o = 0; o < nops; ++o) {
+      const TileOp<T> e = prog[o];
+      const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
+      if (e.mc == kDiagOp) {
 #pragma unroll
-      for (int u = 0; u < R; ++u) acc[u] = 0.0, d[u] = 0.0;
-      for (int q = 0; q < np; ++q) {
-        const SPair e = s_low[q];
-        const uint32_t nb = s_nb_low[q];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          if (ok[u] && (sv[u] & e.flip) == e.cond) {
-            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
-            acc[u] = __dadd_rn(acc[u], __dmul_rn(e.c, __ldg(x + j)));
+        for (int u = 0; u < R; ++u)
+          if ((uint32_t)u < nrow) {
+            const uint32_t i = base + rt + u * kHvThreads;
+            acc[u].add_diag(__ldg(t.dg + i), __ldg(x + i));
           }
-        }
+      } else if (fl == 0u) {
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if ((uint32_t)u < nrow) acc[u].add(e, __ldg(x + e.nb + rt + u * kHvThreads));
+      } else {
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if ((uint32_t)u < nrow && (lv[u] & fl) == cd)
+            acc[u].add(e, __ldg(x + e.nb + __ldg(t.tlo + (lv[u] ^ fl))));
       }
-      for (int q = 0; q < nd; ++q) {
-        const SDiag e = s_diag[q];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const bool eq = ((sv[u] & e.m1) != 0u) == ((sv[u] & e.m2) != 0u);
-          d[u] = __dadd_rn(d[u], eq ? e.veq : e.vne);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u)
-        if (ok[u]) acc[u] = __dadd_rn(acc[u], __dmul_rn(d[u], __ldg(x + base + rr[u])));
-      for (int q = 0; q < np; ++q) {
-        const SPair e = s_rise[q];
-        const uint32_t nb = s_nb_rise[q];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          if (ok[u] && (sv[u] & e.flip) == e.cond) {
-            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
-            acc[u] = __dadd_rn(acc[u], __dmul_rn(e.c, __ldg(x + j)));
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) out[u] = acc[u];
-    } else {
-      Comp32 acc[R];
-      double d[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) d[u] = 0.0;
-      for (int q = 0; q < nd; ++q) {
-        const SDiag e = s_diag[q];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const bool eq = ((sv[u] & e.m1) != 0u) == ((sv[u] & e.m2) != 0u);
-          d[u] += eq ? e.veq : e.vne;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        if (ok[u]) {
-          const float dh = (float)d[u], dl = (float)(d[u] - (double)dh);
-          acc[u].add_prod(dh, dl, __ldg(x + base + rr[u]));
-        }
-      }
-      for (int q = 0; q < np; ++q) {
-        const SPair e = s_low[q];
-        const uint32_t nb = s_nb_low[q];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const uint32_t bsel = sv[u] & e.flip;
-          if (ok[u] && bsel != 0u && bsel != e.flip) {
-            const uint32_t j = nb + (e.cat == kHiHi ? rr[u] : (uint32_t)__ldg(t.tlo + (lv[u] ^ e.loflip)));
-            acc[u].add_prod(e.chi, e.clo, __ldg(x + j));
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) out[u] = acc[u].value();
     }
 #pragma unroll
     for (int u = 0; u < R; ++u) {
-      if (ok[u]) {
-        y[base + rr[u]] = out[u];
-        if (alpha_part) dotacc += (double)__ldg(x + base + rr[u]) * (double)out[u];
+      if ((uint32_t)u < nrow) {
+        const uint32_t i = base + rt + u * kHvThreads;
+        const T v = acc[u].value();
+        y[i] = v;
+        if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
       }
     }
   }
   if (alpha_part) {
     const double tot = block_sum_all<kHvThreads>(dotacc, sm);
     if (threadIdx.x == 0) alpha_part[blockIdx.x] = tot;
+  }
+}
+
+// Diagonal M(i,i) of every row, accumulated in the reference's term order
+// (site terms, then bonds; hamiltonian_matrix.hpp:387-397 starting from the
+// 0 of initialized_matrix, :53-56).  Run once per handle.
+__global__ void __launch_bounds__(256) diag_table_kernel(const __grid_constant__ HvParams P, const DevTables t,
+                                                         double* __restrict__ dg) {
+  for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
+    const uint32_t h = t.tile_h[it];
+    const int k = P.n_up - __popc(h);
+    const uint32_t lbase = t.looff[k];
+    const uint32_t rows = t.looff[k + 1] - lbase;
+    const uint32_t r0 = t.tile_r[it];
+    for (uint32_t r = r0 + threadIdx.x; r < rows && r < r0 + kTileRows; r += 256) {
+      const uint32_t s = (h << P.Nlo) | t.lolist[lbase + r];
+      double d = 0.0;
+      for (int q = 0; q < P.n_diag; ++q) {
+        const bool eq = ((s & P.diag[q].m1) != 0u) == ((s & P.diag[q].m2) != 0u);
+        d = __dadd_rn(d, eq ? P.diag[q].veq : P.diag[q].vne);
+      }
+      dg[t.thi[h] + r] = d;
+    }
   }
 }
 
@@ -453,6 +488,12 @@ int launch_hv_f32(const HvParams& P, const DevTables& t, const float* x, float* 
   if (t.n_tiles == 0) return AED_OK;
   hv_kernel<float><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
   return check_launch("hv_kernel<float>");
+}
+
+int launch_diag_table(const HvParams& P, const DevTables& t, double* dg, cudaStream_t st) {
+  if (t.n_tiles == 0) return AED_OK;
+  diag_table_kernel<<<num_sms() * 8, 256, 0, st>>>(P, t, dg);
+  return check_launch("diag_table_kernel");
 }
 
 int launch_basis_copy(const DevTables& t, uint32_t* out, int64_t offset, int64_t count, cudaStream_t st) {

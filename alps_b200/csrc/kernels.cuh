@@ -17,6 +17,7 @@ struct DevTables {
   const uint32_t* looff;   // Nlo+2
   const uint32_t* tile_h;  // n_tiles
   const uint32_t* tile_r;  // n_tiles
+  const double* dg;        // D: diagonal M(i,i) of every row
   int64_t n_tiles;
   int64_t D;
   int Nlo, Nhi, n_up;
@@ -33,6 +34,9 @@ int launch_hv_f64(const HvParams& P, const DevTables& t, const double* x, double
 int launch_hv_f32(const HvParams& P, const DevTables& t, const float* x, float* y, double* alpha_part,
                   int grid, cudaStream_t st);
 int hv_grid_size(bool f32, int rows_per_thread_unused);
+
+// per-row diagonal table (once per handle)
+int launch_diag_table(const HvParams& P, const DevTables& t, double* dg, cudaStream_t st);
 
 // basis / rank
 int launch_basis_copy(const DevTables& t, uint32_t* out, int64_t offset, int64_t count, cudaStream_t st);
