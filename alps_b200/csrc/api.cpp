@@ -1,6 +1,10 @@
 // api.cpp -- the C ABI of libaed.so (declared in include/aed.h).
 
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "handle.h"
 
@@ -119,10 +123,84 @@ void handle_release_workspace(aed_handle* h) {
   h->h_ab_n = 0;
 }
 
+namespace {
+
+int launch_variant(aed_handle* h, bool f32, int v, const void* x, void* y, double* alpha_part) {
+  if (f32) return launch_hv_f32(v, h->P, h->dt, (const float*)x, (float*)y, alpha_part, h->stream);
+  return launch_hv_f64(v, h->P, h->dt, (const double*)x, (double*)y, alpha_part, h->stream);
+}
+
+// Autotuner: the apply variant (rows per thread, ops per group, CTAs per SM)
+// is picked by timing every variant on the first apply of a handle, once per
+// (precision, size bucket, number of flip pairs); later handles in the same
+// bucket reuse the choice.  Results do not depend on the variant (each row
+// adds its terms in the same order).  AED_HV_VARIANT=<index> forces one.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tune;
+
+int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
+  if (const char* env = std::getenv("AED_HV_VARIANT")) {
+    const int v = std::atoi(env);
+    if (v >= 0 && v < hv_num_variants()) {
+      *out = v;
+      return AED_OK;
+    }
+  }
+  const int64_t D = h->tab.D;
+  int bucket = 0;
+  while ((1ll << (bucket + 1)) <= D) ++bucket;
+  const auto key = std::make_tuple(f32 ? 1 : 0, bucket, h->P.n_pairs);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      *out = it->second;
+      return AED_OK;
+    }
+  }
+  if (D < (1 << 18)) {  // small sectors: launch-bound, not worth timing
+    *out = 0;
+    return AED_OK;
+  }
+  cudaEvent_t e0, e1;
+  AED_CUDA_TRY(cudaEventCreate(&e0));
+  AED_CUDA_TRY(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  int rc = AED_OK;
+  for (int v = 0; v < hv_num_variants() && !rc; ++v) {
+    rc = launch_variant(h, f32, v, x, y, nullptr);  // warm-up
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < 2 && !rc; ++r) rc = launch_variant(h, f32, v, x, y, nullptr);
+    cudaEventRecord(e1, h->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+  }
+  *out = best;
+  return AED_OK;
+}
+
+}  // namespace
+
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
-  if (f32)
-    return launch_hv_f32(h->P, h->dt, (const float*)x, (float*)y, alpha_part, h->hv_grid32, h->stream);
-  return launch_hv_f64(h->P, h->dt, (const double*)x, (double*)y, alpha_part, h->hv_grid64, h->stream);
+  int& v = h->hv_var[f32 ? 1 : 0];
+  if (v < 0) {
+    const int rc = pick_variant(h, f32, x, y, &v);
+    if (rc) return rc;
+  }
+  return launch_variant(h, f32, v, x, y, alpha_part);
 }
 
 }  // namespace aed
@@ -198,11 +276,7 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     release(h);
     return fail(AED_ERR_CUDA, "stream / pinned memory creation failed");
   }
-  h->hv_grid64 = hv_grid_size(false, 1);
-  h->hv_grid32 = hv_grid_size(true, 1);
-  h->red_grid = red_grid_size();
-  const int ga = h->hv_grid64 > h->hv_grid32 ? h->hv_grid64 : h->hv_grid32;
-  if ((rc = dev_alloc(&h->d_partA, ga)) || (rc = dev_alloc(&h->d_partB, h->red_grid))) {
+  if ((rc = dev_alloc(&h->d_partA, th.size() + 1)) || (rc = dev_alloc(&h->d_partB, (size_t)red_chunks(h->tab.D) + 1))) {
     release(h);
     return rc;
   }
@@ -392,10 +466,10 @@ int aed_mult(aed_handle* h, const void* x, void* y) {
 static int reduce_to_host(aed_handle* h, const void* x, const void* y, bool sq, bool take_sqrt, double* out) {
   int rc;
   if (h->precision == AED_FP64)
-    rc = launch_dot_partials((const double*)x, (const double*)y, h->tab.D, h->d_partB, h->red_grid, sq, h->stream);
+    rc = launch_dot_partials((const double*)x, (const double*)y, h->tab.D, h->d_partB, sq, h->stream);
   else
-    rc = launch_dot_partials((const float*)x, (const float*)y, h->tab.D, h->d_partB, h->red_grid, sq, h->stream);
-  if (!rc) rc = launch_finish_sum(h->d_partB, h->red_grid, h->d_scal, take_sqrt, h->stream);
+    rc = launch_dot_partials((const float*)x, (const float*)y, h->tab.D, h->d_partB, sq, h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(h->tab.D), h->d_scal, take_sqrt, h->stream);
   if (rc) return rc;
   AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->d_scal, 8, cudaMemcpyDeviceToHost, h->stream));
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -454,24 +528,9 @@ int aed_lanczos_step(aed_handle* h, const void* v_prev, const void* v_cur, void*
     return fail(AED_ERR_INVALID, "Lanczos vectors must not alias");
   DeviceGuard g(h->device);
   const bool f32 = h->precision == AED_FP32;
-  const int nA = f32 ? h->hv_grid32 : h->hv_grid64;
   h->h_scal[4] = beta_prev;
   AED_CUDA_TRY(cudaMemcpyAsync(h->d_scal + 4, h->h_scal + 4, 8, cudaMemcpyHostToDevice, h->stream));
-  rc = handle_hv(h, f32, v_cur, v_next, h->d_partA);
-  if (rc) return rc;
-  if (f32) {
-    rc = launch_lanczos_update((const double*)h->d_partA, nA, (const float*)v_cur, (const float*)v_prev,
-                               h->d_scal + 4, (float*)v_next, h->tab.D, h->d_partB, h->red_grid, h->d_scal + 0,
-                               h->stream);
-    if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (float*)v_next, h->tab.D, h->d_scal + 1,
-                                           h->red_grid, h->stream);
-  } else {
-    rc = launch_lanczos_update((const double*)h->d_partA, nA, (const double*)v_cur, (const double*)v_prev,
-                               h->d_scal + 4, (double*)v_next, h->tab.D, h->d_partB, h->red_grid, h->d_scal + 0,
-                               h->stream);
-    if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (double*)v_next, h->tab.D, h->d_scal + 1,
-                                           h->red_grid, h->stream);
-  }
+  rc = lanczos_step_kernels(h, f32, v_prev, v_cur, v_next, h->d_scal + 4, h->d_scal + 0, h->d_scal + 1);
   if (rc) return rc;
   AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->d_scal, 16, cudaMemcpyDeviceToHost, h->stream));
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));

@@ -24,11 +24,11 @@ struct aed_handle {
   uint32_t* d_tile_h = nullptr;
   uint32_t* d_tile_r = nullptr;
   double* d_dg = nullptr;     // per-row diagonal
-  double* d_partA = nullptr;  // hv_grid partial sums
-  double* d_partB = nullptr;  // red_grid partial sums
+  double* d_partA = nullptr;  // per-tile partial sums (n_tiles)
+  double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
   double* d_scal = nullptr;   // 8 device scalars
   double* h_scal = nullptr;   // 8 pinned host scalars
-  int hv_grid32 = 0, hv_grid64 = 0, red_grid = 0;
+  int hv_var[2] = {-1, -1};  // apply variant per precision (FP64, FP32), -1 = not tuned yet
   size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }
   // solve workspaces, kept between solves (grown on demand): slot 0 = FP64
   // recurrence, slot 1 = FP32 Lanczos basis store of the mixed path
@@ -67,5 +67,9 @@ constexpr int kStoreChunk = 16;
 // Pointer to chunk `c` of the FP32 basis store (allocated on first use), or nullptr.
 void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes);
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r);
+// One make_step on device vectors: apply, alpha, update, beta, normalise.
+// beta_prev / alpha / beta are device scalars; v_prev may be NULL.
+int lanczos_step_kernels(aed_handle* h, bool f32, const void* v_prev, const void* v_cur, void* v_next,
+                         const double* beta_prev, double* alpha, double* beta);
 
 }  // namespace aed

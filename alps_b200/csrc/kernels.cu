@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdlib>
+#include <string>
 
 #include "kernels.cuh"
 
@@ -56,12 +58,11 @@ __device__ __forceinline__ double sum_partials(const double* __restrict__ p, int
 //     stream of x;
 //   * one bit in each part: applies iff the lo state has one given bit value;
 //     target thi[h'] + tlo[l ^ bit];
-//   * both bits in the lo part: applies iff the lo state has the two bits in
-//     a given order; target thi[h] + tlo[l ^ flip].
-// Warp 0 compiles the tile's "program": the list of flips that can apply,
-// with their target block base already looked up, in the reference's column
-// order, plus one diagonal entry.  All threads then run the program on
-// kRowsPerThread rows each.  The coupling tables are staged in shared memory
+//   * both bits in the lo part: applies iff the two lo bits differ (in a given
+//     order for the FP64 row order); target thi[h] + tlo[l ^ flip].
+// Warp 0 compiles the tile's "program": the flips that can apply, with their
+// target block base already looked up, plus the diagonal.  All threads then
+// run it on R rows each.  The coupling tables are staged in shared memory
 // once per CTA (indexing them from parameter space with a loop counter
 // serialises on the constant-load path).
 //
@@ -72,98 +73,76 @@ __device__ __forceinline__ double sum_partials(const double* __restrict__ p, int
 // larger states (hi ascending, lo descending), summed left to right from 0.
 // Products and sums round separately (__dmul_rn/__dadd_rn: no FMA
 // contraction), as on the reference's x86-64 build.  M(i,i) comes from a
-// per-row table filled once per handle in the reference's term order.
+// per-row table filled once per handle in the reference's term order; the
+// program for FP64 holds the "smaller" flips, the diagonal, then the "larger"
+// flips, in that column order.
+//
+// FP32 rows (mixed path) take each flip once in any order and accumulate the
+// terms c * x_j in FP64 (c is FP64, x_j FP32: every product carries a 53-bit
+// significand), rounding to FP32 once at the end; the alternative TwoSum
+// (Knuth) + FMA-product-error accumulation in FP32 (Ogita, Rump & Oishi,
+// "Dot2") is kept as AccTwoSum.
 // ---------------------------------------------------------------------------
-constexpr int kRowsPerThread = 4;
-constexpr int kTileRows = kHvThreads * kRowsPerThread;
-static_assert(kTileRows == kHvTileRows, "tile size");
+constexpr int kTileRows = kHvTileRows;
 constexpr uint32_t kDiagOp = 0xffffffffu;
+constexpr uint32_t kXorCond = 0xffffu;  // lo-part condition: the two bits differ
 constexpr int kMaxOps = 2 * kMaxBonds + 1;
 
 struct SPair {
   uint32_t flip, cond;
   double c;
-  float chi, clo;
 };
 
-// One program entry: mc = lo-part flip | (lo-part condition << 16) (or
-// kDiagOp); nb = base row of the target hi block; c = coupling.
-template <typename T>
-struct TileOp;
-template <>
-struct TileOp<double> {
+// One program entry: mc = lo-part flip | (lo-part condition << 16), or
+// kDiagOp; nb = base row of the target hi block; c = coupling.
+struct TileOp {
   uint32_t mc, nb;
   double c;
 };
-template <>
-struct TileOp<float> {
-  uint32_t mc, nb;
-  float chi, clo;
+
+// ---- row accumulators ----
+struct AccExact64 {  // FP64 vectors, the reference's rounding
+  double a = 0.0;
+  __device__ __forceinline__ void add(double c, double xv) { a = __dadd_rn(a, __dmul_rn(c, xv)); }
+  __device__ __forceinline__ double value() const { return a; }
 };
 
-// Error-free transformations: TwoSum (Knuth, TAOCP Vol. 2, 4.2.2) and the
-// FMA-based exact product error.  Compensated row sum in the style of
-// Ogita, Rump & Oishi (SIAM J. Sci. Comput. 26 (2005)) "Dot2".
-struct Comp32 {
-  float s = 0.f, c = 0.f;
-  __device__ __forceinline__ void add_prod(float a_hi, float a_lo, float xv) {
-    const float p = __fmul_rn(a_hi, xv);
-    const float pe = __fmaf_rn(a_hi, xv, -p);  // exact: a_hi*xv - p
+struct AccWide32 {  // FP32 vectors, FP64 accumulator
+  double a = 0.0;
+  __device__ __forceinline__ void add(double c, float xv) { a = fma(c, (double)xv, a); }
+  __device__ __forceinline__ float value() const { return (float)a; }
+};
+
+struct AccTwoSum32 {  // FP32 vectors, TwoSum + exact product error in FP32
+  float s = 0.f, e = 0.f;
+  __device__ __forceinline__ void add(double c, float xv) {
+    const float ch = (float)c, cl = (float)(c - (double)ch);
+    const float p = __fmul_rn(ch, xv);
+    const float pe = __fmaf_rn(ch, xv, -p);  // exact: ch*xv - p
     const float t = __fadd_rn(s, p);
     const float bb = __fsub_rn(t, s);
     const float se = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(p, bb));
     s = t;
-    c = __fadd_rn(c, __fadd_rn(se, __fmaf_rn(a_lo, xv, pe)));
+    e = __fadd_rn(e, __fadd_rn(se, __fmaf_rn(cl, xv, pe)));
   }
-  __device__ __forceinline__ float value() const { return __fadd_rn(s, c); }
+  __device__ __forceinline__ float value() const { return __fadd_rn(s, e); }
 };
 
-template <typename T>
-struct RowAcc;
-template <>
-struct RowAcc<double> {
-  double a = 0.0;
-  __device__ __forceinline__ void add(const TileOp<double>& e, double xv) { a = __dadd_rn(a, __dmul_rn(e.c, xv)); }
-  __device__ __forceinline__ void add_diag(double d, double xv) { a = __dadd_rn(a, __dmul_rn(d, xv)); }
-  __device__ __forceinline__ double value() const { return a; }
-};
-template <>
-struct RowAcc<float> {
-  Comp32 a;
-  __device__ __forceinline__ void add(const TileOp<float>& e, float xv) { a.add_prod(e.chi, e.clo, xv); }
-  __device__ __forceinline__ void add_diag(double d, float xv) {
-    const float dh = (float)d, dl = (float)(d - (double)dh);
-    a.add_prod(dh, dl, xv);
-  }
-  __device__ __forceinline__ float value() const { return a.value(); }
-};
-
-template <typename T>
-__device__ __forceinline__ TileOp<T> make_op(uint32_t mc, uint32_t nb, const SPair& e);
-template <>
-__device__ __forceinline__ TileOp<double> make_op<double>(uint32_t mc, uint32_t nb, const SPair& e) {
-  return {mc, nb, e.c};
-}
-template <>
-__device__ __forceinline__ TileOp<float> make_op<float>(uint32_t mc, uint32_t nb, const SPair& e) {
-  return {mc, nb, e.chi, e.clo};
-}
-
-// Warp 0: append the entries of `list` that can apply in hi block h to prog.
-template <typename T>
-__device__ __forceinline__ int compile_list(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
-                                            const uint32_t* __restrict__ thi, TileOp<T>* prog, int cnt) {
+// Warp 0: append to prog the entries of `list` that can apply in hi block h
+// (FP64 order: cond fixes which of the two bits must be set).
+__device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
+                                               const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
   const int lane = threadIdx.x & 31;
   for (int q0 = 0; q0 < np; q0 += 32) {
     const int q = q0 + lane;
     bool emit = false;
-    TileOp<T> op;
+    TileOp op;
     if (q < np) {
       const SPair e = list[q];
       const uint32_t fhi = e.flip >> Nlo, chi = e.cond >> Nlo;
       if ((h & fhi) == chi) {
         emit = true;
-        op = make_op<T>((e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e);
+        op = {(e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e.c};
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, emit);
@@ -173,14 +152,81 @@ __device__ __forceinline__ int compile_list(const SPair* list, int np, uint32_t 
   return cnt;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ HvParams P, const DevTables t,
-                                                        const T* __restrict__ x, T* __restrict__ y,
-                                                        double* __restrict__ alpha_part) {
-  constexpr int R = kRowsPerThread;
+// Warp 0: every flip once, either direction (FP32 rows: order is free).
+__device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
+                                          const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int q0 = 0; q0 < np; q0 += 32) {
+    const int q = q0 + lane;
+    bool emit = false;
+    TileOp op;
+    if (q < np) {
+      const SPair e = list[q];
+      const uint32_t fhi = e.flip >> Nlo, flo = e.flip & lm;
+      const uint32_t hb = h & fhi;
+      if (flo == 0u) {  // hi part only: applies to the whole tile iff the two bits differ
+        emit = __popc(hb) == 1;
+        op = {0u, __ldg(thi + (h ^ fhi)), e.c};
+      } else if (fhi == 0u) {  // lo part only
+        emit = true;
+        op = {flo | (kXorCond << 16), __ldg(thi + h), e.c};
+      } else {  // crossing: the lo bit must differ from the hi bit
+        emit = true;
+        op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, emit);
+    if (emit) prog[cnt + __popc(m & ((1u << lane) - 1u))] = op;
+    cnt += __popc(m);
+  }
+  return cnt;
+}
+
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void run_ops(const TileOp* prog, int o0, int o1, const uint32_t* lv, uint32_t nrow,
+                                        uint32_t rt, const double* __restrict__ dg, uint32_t base,
+                                        const uint16_t* __restrict__ tlo, const T* __restrict__ x, Acc* acc) {
+  for (int o = o0; o < o1; ++o) {
+    const TileOp e = prog[o];
+    const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
+    if (e.mc == kDiagOp) {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          acc[u].add(__ldg(dg + i), __ldg(x + i));
+        }
+    } else if (fl == 0u) {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow) acc[u].add(e.c, __ldg(x + e.nb + rt + u * kHvThreads));
+    } else if (cd == kXorCond) {
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const uint32_t b = lv[u] & fl;
+        if ((uint32_t)u < nrow && b != 0u && b != fl) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow && (lv[u] & fl) == cd) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+    }
+  }
+}
+
+// y = H x.  Tiles are taken in a static round robin; alpha_part (optional)
+// receives one partial sum of x_i * y_i per tile, so the reduction does not
+// depend on the grid.  R rows per thread per pass, MINB CTAs per SM.
+template <typename T, typename Acc, int R, int MINB>
+__global__ void __launch_bounds__(kHvThreads, MINB) hv_kernel(const __grid_constant__ HvParams P, const DevTables t,
+                                                              const T* __restrict__ x, T* __restrict__ y,
+                                                              double* __restrict__ alpha_part) {
+  static_assert(kTileRows % (kHvThreads * R) == 0, "rows per thread must divide the tile");
+  constexpr bool kOrdered = sizeof(T) == 8;
+  constexpr int kPasses = kTileRows / (kHvThreads * R);
   __shared__ SPair s_low[kMaxBonds];
   __shared__ SPair s_rise[kMaxBonds];
-  __shared__ TileOp<T> prog[kMaxOps];
+  __shared__ TileOp prog[kMaxOps];
   __shared__ int s_nops;
   __shared__ double sm[33];
   const int np = P.n_pairs, Nlo = P.Nlo;
@@ -188,10 +234,9 @@ __global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ 
   // flips to smaller states need the higher bit set, flips to larger states the lower one
   for (int q = threadIdx.x; q < np; q += kHvThreads) {
     const PairTerm a = P.low[q], b = P.rise[q];
-    s_low[q] = {a.mhi | a.mlo, a.mhi, a.c, a.chi, a.clo};
-    s_rise[q] = {b.mhi | b.mlo, b.mlo, b.c, b.chi, b.clo};
+    s_low[q] = {a.mhi | a.mlo, a.mhi, a.c};
+    s_rise[q] = {b.mhi | b.mlo, b.mlo, b.c};
   }
-  double dotacc = 0.0;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
     const uint32_t h = __ldg(t.tile_h + it);
     const uint32_t r0 = __ldg(t.tile_r + it);
@@ -201,58 +246,48 @@ __global__ void __launch_bounds__(kHvThreads) hv_kernel(const __grid_constant__ 
     const uint32_t base = __ldg(t.thi + h);
     __syncthreads();  // tables staged; previous tile done with prog
     if (threadIdx.x < 32) {
-      int cnt = compile_list<T>(s_low, np, h, Nlo, lm, t.thi, prog, 0);
-      if (threadIdx.x == 0) prog[cnt].mc = kDiagOp;
-      cnt = compile_list<T>(s_rise, np, h, Nlo, lm, t.thi, prog, cnt + 1);
+      int cnt;
+      if (kOrdered) {
+        const int nl = compile_ordered(s_low, np, h, Nlo, lm, t.thi, prog, 0);
+        if (threadIdx.x == 0) prog[nl].mc = kDiagOp;
+        cnt = compile_ordered(s_rise, np, h, Nlo, lm, t.thi, prog, nl + 1);
+      } else {
+        if (threadIdx.x == 0) prog[0].mc = kDiagOp;
+        cnt = compile_any(s_low, np, h, Nlo, lm, t.thi, prog, 1);
+      }
       if (threadIdx.x == 0) s_nops = cnt;
     }
     __syncthreads();
     const int nops = s_nops;
-    uint32_t lv[R];
-    uint32_t nrow = 0;  // rows of this thread that exist
+    double dotacc = 0.0;
+#pragma unroll 1
+    for (int pass = 0; pass < kPasses; ++pass) {
+      const uint32_t rt = r0 + pass * (kHvThreads * R) + threadIdx.x;  // row offset of u = 0
+      uint32_t lv[R];
+      uint32_t nrow = 0;  // rows of this thread that exist (a prefix of u)
 #pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const uint32_t r = r0 + threadIdx.x + u * kHvThreads;
-      const bool ok = r < rows && r < r0 + kTileRows;
-      nrow += ok ? 1u : 0u;
-      lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
-    }
-    RowAcc<T> acc[R];
-    const uint32_t rt = r0 + threadIdx.x;  // row offset of u = 0
-    for (int o = 0; o < nops; ++o) {
-      const TileOp<T> e = prog[o];
-      const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
-      if (e.mc == kDiagOp) {
+      for (int u = 0; u < R; ++u) {
+        const uint32_t r = rt + u * kHvThreads;
+        const bool ok = r < rows && r < r0 + kTileRows;
+        nrow += ok ? 1u : 0u;
+        lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
+      }
+      Acc acc[R];
+      run_ops<T, Acc, R>(prog, 0, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
 #pragma unroll
-        for (int u = 0; u < R; ++u)
-          if ((uint32_t)u < nrow) {
-            const uint32_t i = base + rt + u * kHvThreads;
-            acc[u].add_diag(__ldg(t.dg + i), __ldg(x + i));
-          }
-      } else if (fl == 0u) {
-#pragma unroll
-        for (int u = 0; u < R; ++u)
-          if ((uint32_t)u < nrow) acc[u].add(e, __ldg(x + e.nb + rt + u * kHvThreads));
-      } else {
-#pragma unroll
-        for (int u = 0; u < R; ++u)
-          if ((uint32_t)u < nrow && (lv[u] & fl) == cd)
-            acc[u].add(e, __ldg(x + e.nb + __ldg(t.tlo + (lv[u] ^ fl))));
+      for (int u = 0; u < R; ++u) {
+        if ((uint32_t)u < nrow) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          const T v = acc[u].value();
+          y[i] = v;
+          if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
+        }
       }
     }
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      if ((uint32_t)u < nrow) {
-        const uint32_t i = base + rt + u * kHvThreads;
-        const T v = acc[u].value();
-        y[i] = v;
-        if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
-      }
+    if (alpha_part) {
+      const double tot = block_sum_all<kHvThreads>(dotacc, sm);
+      if (threadIdx.x == 0) alpha_part[it] = tot;
     }
-  }
-  if (alpha_part) {
-    const double tot = block_sum_all<kHvThreads>(dotacc, sm);
-    if (threadIdx.x == 0) alpha_part[blockIdx.x] = tot;
   }
 }
 
@@ -347,59 +382,69 @@ __global__ void scal_kernel(double a, T* __restrict__ x, int64_t n, bool divide)
     x[i] = (T)(divide ? __ddiv_rn((double)x[i], a) : __dmul_rn((double)x[i], a));
 }
 
+// Deterministic reductions over fixed chunks of kRedChunk elements: chunk c
+// is always summed by one CTA in the same thread order and tree, whatever the
+// grid, so partial[c] and every total built from the partials are
+// reproducible bit for bit on any GPU.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) dot_partials_kernel(const T* __restrict__ x, const T* __restrict__ y,
                                                                   int64_t n, double* __restrict__ part, bool sq) {
   __shared__ double sm[33];
-  double acc = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
-    const double a = (double)x[i];
-    acc = fma(a, sq ? a : (double)y[i], acc);
+  const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
+    double acc = 0.0;
+    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+      const double a = (double)x[i];
+      acc = fma(a, sq ? a : (double)y[i], acc);
+    }
+    const double tot = block_sum_all<kRedThreads>(acc, sm);
+    if (threadIdx.x == 0) part[c] = tot;
   }
-  const double tot = block_sum_all<kRedThreads>(acc, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(kRedThreads) finish_sum_kernel(const double* __restrict__ part, int n,
-                                                                 double* __restrict__ out, bool take_sqrt) {
+// *out = sum of n partials (sqrt if asked), one CTA, fixed order.
+__global__ void __launch_bounds__(1024) finish_sum_kernel(const double* __restrict__ part, int64_t n,
+                                                          double* __restrict__ out, bool take_sqrt) {
   __shared__ double sm[33];
-  const double tot = sum_partials<kRedThreads>(part, n, sm);
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += 1024) v += part[i];
+  const double tot = block_sum_all<1024>(v, sm);
   if (threadIdx.x == 0) *out = take_sqrt ? sqrt(tot) : tot;
 }
 
-// make_step middle part (lanczos.h:398-401): a = dot(v, Hv); w -= a v; w -= b v_prev; |w|^2
+// make_step middle part (lanczos.h:398-401): w -= a v; w -= b v_prev; chunk partials of |w|^2
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const double* __restrict__ partA, int nA,
+__global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const double* __restrict__ alpha_p,
                                                                     const T* __restrict__ x,
                                                                     const T* __restrict__ vprev,
                                                                     const double* __restrict__ beta_prev,
                                                                     T* __restrict__ y, int64_t n,
-                                                                    double* __restrict__ partB,
-                                                                    double* __restrict__ alpha_out) {
+                                                                    double* __restrict__ partB) {
   __shared__ double sm[33];
-  const double alpha = sum_partials<kRedThreads>(partA, nA, sm);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *alpha_out = alpha;
+  const double alpha = *alpha_p;
   const double b = vprev ? *beta_prev : 0.0;
-  double acc = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads) {
-    double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
-    if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
-    const T wt = (T)w;
-    y[i] = wt;
-    acc = fma((double)wt, (double)wt, acc);
+  const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
+    double acc = 0.0;
+    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+      double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
+      if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
+      const T wt = (T)w;
+      y[i] = wt;
+      acc = fma((double)wt, (double)wt, acc);
+    }
+    const double tot = block_sum_all<kRedThreads>(acc, sm);
+    if (threadIdx.x == 0) partB[c] = tot;
   }
-  const double tot = block_sum_all<kRedThreads>(acc, sm);
-  if (threadIdx.x == 0) partB[blockIdx.x] = tot;
 }
 
-// make_step tail (lanczos.h:401-402): b = |w|; w /= b
+// make_step tail (lanczos.h:402): w /= b
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const double* __restrict__ partB, int nB,
-                                                                       T* __restrict__ y, int64_t n,
-                                                                       double* __restrict__ beta_out) {
-  __shared__ double sm[33];
-  const double beta = sqrt(sum_partials<kRedThreads>(partB, nB, sm));
-  if (blockIdx.x == 0 && threadIdx.x == 0 && beta_out) *beta_out = beta;
+__global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const double* __restrict__ beta_p,
+                                                                       T* __restrict__ y, int64_t n) {
+  const double beta = *beta_p;
   for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
     y[i] = (T)__ddiv_rn((double)y[i], beta);
 }
@@ -455,8 +500,6 @@ inline int check_launch(const char* what) {
 
 }  // namespace
 
-int red_grid_size() { return num_sms() * 4; }
-
 int64_t launch_count() { return g_launches.load(); }
 
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
@@ -466,28 +509,62 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
   return check_launch("ritz_combine_kernel");
 }
 
-int hv_grid_size(bool f32, int) {
-  int per_sm = 0;
-  if (f32)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<float>, kHvThreads, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<double>, kHvThreads, 0);
-  if (per_sm < 1) per_sm = 1;
-  return num_sms() * per_sm;
+// ---- apply variants (rows per thread, CTAs per SM) ------------------------------
+struct HvVariant {
+  int R, minb;
+  const char* name;
+};
+constexpr HvVariant kVariants[] = {
+    {4, 6, "r4b6"}, {4, 5, "r4b5"}, {4, 4, "r4b4"}, {2, 8, "r2b8"}, {2, 6, "r2b6"}, {8, 3, "r8b3"},
+};
+constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+
+template <typename T, typename Acc, int R, int B>
+int launch_one(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st,
+               int* grid_cache) {
+  if (*grid_cache <= 0) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<T, Acc, R, B>, kHvThreads, 0);
+    *grid_cache = num_sms() * (per_sm < 1 ? 1 : per_sm);
+  }
+  int grid = *grid_cache;
+  if (grid > t.n_tiles) grid = (int)t.n_tiles;
+  hv_kernel<T, Acc, R, B><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
+  return check_launch("hv_kernel");
 }
 
-int launch_hv_f64(const HvParams& P, const DevTables& t, const double* x, double* y, double* alpha_part, int grid,
-                  cudaStream_t st) {
+template <typename T, typename Acc>
+int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
+                cudaStream_t st) {
+  static int grids[kNumVariants] = {};
   if (t.n_tiles == 0) return AED_OK;
-  hv_kernel<double><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
-  return check_launch("hv_kernel<double>");
+  switch (v) {
+    case 0: return launch_one<T, Acc, 4, 6>(P, t, x, y, alpha_part, st, &grids[0]);
+    case 1: return launch_one<T, Acc, 4, 5>(P, t, x, y, alpha_part, st, &grids[1]);
+    case 2: return launch_one<T, Acc, 4, 4>(P, t, x, y, alpha_part, st, &grids[2]);
+    case 3: return launch_one<T, Acc, 2, 8>(P, t, x, y, alpha_part, st, &grids[3]);
+    case 4: return launch_one<T, Acc, 2, 6>(P, t, x, y, alpha_part, st, &grids[4]);
+    case 5: return launch_one<T, Acc, 8, 3>(P, t, x, y, alpha_part, st, &grids[5]);
+    default: return fail(AED_ERR_INVALID, "unknown apply variant");
+  }
 }
 
-int launch_hv_f32(const HvParams& P, const DevTables& t, const float* x, float* y, double* alpha_part, int grid,
-                  cudaStream_t st) {
-  if (t.n_tiles == 0) return AED_OK;
-  hv_kernel<float><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
-  return check_launch("hv_kernel<float>");
+int hv_num_variants() { return kNumVariants; }
+const char* hv_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
+
+int launch_hv_f64(int variant, const HvParams& P, const DevTables& t, const double* x, double* y,
+                  double* alpha_part, cudaStream_t st) {
+  return launch_hv_t<double, AccExact64>(variant, P, t, x, y, alpha_part, st);
+}
+
+int launch_hv_f32(int variant, const HvParams& P, const DevTables& t, const float* x, float* y,
+                  double* alpha_part, cudaStream_t st) {
+  static const bool twosum = [] {
+    const char* e = std::getenv("AED_FP32_ACCUM");
+    return e && std::string(e) == "twosum";
+  }();
+  if (twosum) return launch_hv_t<float, AccTwoSum32>(variant, P, t, x, y, alpha_part, st);
+  return launch_hv_t<float, AccWide32>(variant, P, t, x, y, alpha_part, st);
 }
 
 int launch_diag_table(const HvParams& P, const DevTables& t, double* dg, cudaStream_t st) {
@@ -532,28 +609,33 @@ int launch_scal(double a, T* x, int64_t n, bool divide, cudaStream_t st) {
   return check_launch("scal_kernel");
 }
 
+int64_t red_chunks(int64_t n) { return (n + kRedChunk - 1) / kRedChunk; }
+
 template <typename T>
-int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, int grid, bool sq, cudaStream_t st) {
-  dot_partials_kernel<T><<<grid, kRedThreads, 0, st>>>(x, y, n, part, sq);
+int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, bool sq, cudaStream_t st) {
+  const int64_t nch = red_chunks(n);
+  const int grid = (int)(nch < (int64_t)num_sms() * 8 ? nch : (int64_t)num_sms() * 8);
+  dot_partials_kernel<T><<<grid < 1 ? 1 : grid, kRedThreads, 0, st>>>(x, y, n, part, sq);
   return check_launch("dot_partials_kernel");
 }
 
-int launch_finish_sum(const double* part, int n, double* out, bool take_sqrt, cudaStream_t st) {
-  finish_sum_kernel<<<1, kRedThreads, 0, st>>>(part, n, out, take_sqrt);
+int launch_finish_sum(const double* part, int64_t n, double* out, bool take_sqrt, cudaStream_t st) {
+  finish_sum_kernel<<<1, 1024, 0, st>>>(part, n, out, take_sqrt);
   return check_launch("finish_sum_kernel");
 }
 
 template <typename T>
-int launch_lanczos_update(const double* partA, int nA, const T* x, const T* vprev, const double* beta_prev, T* y,
-                          int64_t n, double* partB, int gridB, double* alpha_out, cudaStream_t st) {
-  lanczos_update_kernel<T><<<gridB, kRedThreads, 0, st>>>(partA, nA, x, vprev, beta_prev, y, n, partB, alpha_out);
+int launch_lanczos_update(const double* alpha, const T* x, const T* vprev, const double* beta_prev, T* y,
+                          int64_t n, double* partB, cudaStream_t st) {
+  const int64_t nch = red_chunks(n);
+  const int grid = (int)(nch < (int64_t)num_sms() * 8 ? nch : (int64_t)num_sms() * 8);
+  lanczos_update_kernel<T><<<grid < 1 ? 1 : grid, kRedThreads, 0, st>>>(alpha, x, vprev, beta_prev, y, n, partB);
   return check_launch("lanczos_update_kernel");
 }
 
 template <typename T>
-int launch_lanczos_normalize(const double* partB, int nB, T* y, int64_t n, double* beta_out, int grid,
-                             cudaStream_t st) {
-  lanczos_normalize_kernel<T><<<grid, kRedThreads, 0, st>>>(partB, nB, y, n, beta_out);
+int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t st) {
+  lanczos_normalize_kernel<T><<<elem_grid(n), kRedThreads, 0, st>>>(beta, y, n);
   return check_launch("lanczos_normalize_kernel");
 }
 
@@ -562,10 +644,10 @@ int launch_lanczos_normalize(const double* partB, int nB, T* y, int64_t n, doubl
   template int launch_copy<T>(const T*, T*, int64_t, cudaStream_t);                                          \
   template int launch_axpy<T>(double, const T*, T*, int64_t, cudaStream_t);                                  \
   template int launch_scal<T>(double, T*, int64_t, bool, cudaStream_t);                                      \
-  template int launch_dot_partials<T>(const T*, const T*, int64_t, double*, int, bool, cudaStream_t);        \
-  template int launch_lanczos_update<T>(const double*, int, const T*, const T*, const double*, T*, int64_t, \
-                                        double*, int, double*, cudaStream_t);                               \
-  template int launch_lanczos_normalize<T>(const double*, int, T*, int64_t, double*, int, cudaStream_t);
+  template int launch_dot_partials<T>(const T*, const T*, int64_t, double*, bool, cudaStream_t);             \
+  template int launch_lanczos_update<T>(const double*, const T*, const T*, const double*, T*, int64_t,      \
+                                        double*, cudaStream_t);                                              \
+  template int launch_lanczos_normalize<T>(const double*, T*, int64_t, cudaStream_t);
 AED_INST(double)
 AED_INST(float)
 #undef AED_INST

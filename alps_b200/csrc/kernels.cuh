@@ -24,16 +24,17 @@ struct DevTables {
 };
 
 constexpr int kHvThreads = 256;
-constexpr int kHvTileRows = 1024;  // rows per work tile (kHvThreads x rows per thread)
+constexpr int kHvTileRows = 2048;  // rows per work tile (a multiple of kHvThreads x rows per thread)
 constexpr int kRedThreads = 256;
 
-// y = H x.  alpha_part (optional): per-CTA partial sums of x_i * y_i.
-// grid = number of CTAs (fixed per handle so partial sums are deterministic).
-int launch_hv_f64(const HvParams& P, const DevTables& t, const double* x, double* y, double* alpha_part,
-                  int grid, cudaStream_t st);
-int launch_hv_f32(const HvParams& P, const DevTables& t, const float* x, float* y, double* alpha_part,
-                  int grid, cudaStream_t st);
-int hv_grid_size(bool f32, int rows_per_thread_unused);
+// y = H x with apply variant `variant` (0 .. hv_num_variants()-1).
+// alpha_part (optional): one partial sum of x_i * y_i per tile (n_tiles entries).
+int launch_hv_f64(int variant, const HvParams& P, const DevTables& t, const double* x, double* y,
+                  double* alpha_part, cudaStream_t st);
+int launch_hv_f32(int variant, const HvParams& P, const DevTables& t, const float* x, float* y,
+                  double* alpha_part, cudaStream_t st);
+int hv_num_variants();
+const char* hv_variant_name(int v);
 
 // per-row diagonal table (once per handle)
 int launch_diag_table(const HvParams& P, const DevTables& t, double* dg, cudaStream_t st);
@@ -52,23 +53,25 @@ int launch_axpy(double a, const T* x, T* y, int64_t n, cudaStream_t st);
 template <typename T>
 int launch_scal(double a, T* x, int64_t n, bool divide, cudaStream_t st);
 
-// deterministic reductions: partials over a fixed grid, then one fixed-order
-// final sum into *out (device).  sq: sum of squares of x (y ignored).
+// Deterministic reductions: one partial per fixed chunk of kRedChunk elements
+// (red_chunks(n) of them), then one fixed-order sum.  sq: sum of squares of x.
+constexpr int64_t kRedChunk = 4096;
+int64_t red_chunks(int64_t n);
 template <typename T>
-int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, int grid, bool sq, cudaStream_t st);
-int launch_finish_sum(const double* part, int n, double* out, bool take_sqrt, cudaStream_t st);
+int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, bool sq, cudaStream_t st);
+int launch_finish_sum(const double* part, int64_t n, double* out, bool take_sqrt, cudaStream_t st);
 
-// fused Lanczos step (make_step, src/ietl/lanczos.h:392-406), after
-// launch_hv_*(x -> y, alpha partials):
-//   update:    alpha = sum(partA); y = (y - alpha x) - beta_prev v_prev; partB = |y|^2
-//   normalize: beta = sqrt(sum(partB)); y /= beta
-// beta_prev is read from device memory (NULL: first step, no v_prev term).
+// Fused Lanczos step (make_step, src/ietl/lanczos.h:392-406), after the apply
+// x -> y with per-tile partials and launch_finish_sum(partials -> *alpha):
+//   update:    y = (y - alpha x) - beta_prev v_prev; chunk partials of |y|^2
+//   (launch_finish_sum(partB -> *beta, sqrt))
+//   normalize: y /= beta
+// alpha, beta, beta_prev are device scalars (vprev == NULL: first step).
 template <typename T>
-int launch_lanczos_update(const double* partA, int nA, const T* x, const T* vprev, const double* beta_prev, T* y,
-                          int64_t n, double* partB, int gridB, double* alpha_out, cudaStream_t st);
+int launch_lanczos_update(const double* alpha, const T* x, const T* vprev, const double* beta_prev, T* y,
+                          int64_t n, double* partB, cudaStream_t st);
 template <typename T>
-int launch_lanczos_normalize(const double* partB, int nB, T* y, int64_t n, double* beta_out, int grid,
-                             cudaStream_t st);
+int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t st);
 
 // out[i] = sum_j coef[j] * V[j*ld + i] (FP32 Lanczos store -> FP64 vector),
 // coef in device memory (m <= kMaxRitzTerms).
@@ -76,7 +79,6 @@ constexpr int kMaxRitzTerms = 4096;
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
                         bool accumulate, cudaStream_t st);
 
-int red_grid_size();
 int64_t launch_count();
 
 }  // namespace aed

@@ -85,6 +85,25 @@ double diag_of_state(const HvParams& P, uint32_t s) {
   return d;
 }
 
+// After the apply x -> y (per-tile partials in h->d_partA): alpha, update,
+// beta, normalise (lanczos.h:398-402).
+int lanczos_step_tail(aed_handle* h, bool f32, const void* vprev, const void* x, void* y, const double* beta_prev,
+                      double* alpha, double* beta) {
+  const int64_t D = h->tab.D;
+  int rc = launch_finish_sum(h->d_partA, h->dt.n_tiles, alpha, false, h->stream);
+  if (rc) return rc;
+  if (f32)
+    rc = launch_lanczos_update(alpha, (const float*)x, (const float*)vprev, beta_prev, (float*)y, D, h->d_partB,
+                               h->stream);
+  else
+    rc = launch_lanczos_update(alpha, (const double*)x, (const double*)vprev, beta_prev, (double*)y, D, h->d_partB,
+                               h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(D), beta, true, h->stream);
+  if (rc) return rc;
+  if (f32) return launch_lanczos_normalize(beta, (float*)y, D, h->stream);
+  return launch_lanczos_normalize(beta, (double*)y, D, h->stream);
+}
+
 // One Lanczos recurrence on device vectors of type T.  Vectors rotate through
 // `slot(j)`, the buffer that receives v_j.  Returns T-matrix and convergence.
 struct Recurrence {
@@ -118,7 +137,6 @@ struct Recurrence {
 
   // launch step j: x = v_j -> y = v_{j+1}; vprev = v_{j-1} (NULL for j = 0)
   int launch_step(int j, const void* vprev, const void* x, void* y) {
-    const int nA = f32 ? h->hv_grid32 : h->hv_grid64;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (profile) {
       AED_CUDA_TRY(cudaEventCreate(&e0));
@@ -131,17 +149,7 @@ struct Recurrence {
     if (rc) return rc;
     if (profile) AED_CUDA_TRY(cudaEventRecord(e1, h->stream));
     const double* bprev = j > 0 ? d_ab + 2 * (j - 1) + 1 : nullptr;
-    if (f32) {
-      rc = launch_lanczos_update((const double*)h->d_partA, nA, (const float*)x, (const float*)vprev, bprev,
-                                 (float*)y, D, h->d_partB, h->red_grid, d_ab + 2 * j, h->stream);
-      if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (float*)y, D, d_ab + 2 * j + 1, h->red_grid,
-                                             h->stream);
-    } else {
-      rc = launch_lanczos_update((const double*)h->d_partA, nA, (const double*)x, (const double*)vprev, bprev,
-                                 (double*)y, D, h->d_partB, h->red_grid, d_ab + 2 * j, h->stream);
-      if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, (double*)y, D, d_ab + 2 * j + 1,
-                                             h->red_grid, h->stream);
-    }
+    rc = lanczos_step_tail(h, f32, vprev, x, y, bprev, d_ab + 2 * j, d_ab + 2 * j + 1);
     if (rc) return rc;
     AED_CUDA_TRY(cudaMemcpyAsync(h_ab + 2 * j, d_ab + 2 * j, 16, cudaMemcpyDeviceToHost, h->stream));
     AED_CUDA_TRY(cudaEventRecord(ring->ev[j % EventRing::kN], h->stream));
@@ -167,8 +175,9 @@ struct Recurrence {
 // normalise v in place (lanczos.h:383): v /= |v|
 template <typename T>
 int normalize(aed_handle* h, T* v, int64_t D) {
-  int rc = launch_dot_partials(v, v, D, h->d_partB, h->red_grid, true, h->stream);
-  if (!rc) rc = launch_lanczos_normalize(h->d_partB, h->red_grid, v, D, h->d_scal + 7, h->red_grid, h->stream);
+  int rc = launch_dot_partials(v, v, D, h->d_partB, true, h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(D), h->d_scal + 7, true, h->stream);
+  if (!rc) rc = launch_lanczos_normalize(h->d_scal + 7, v, D, h->stream);
   return rc;
 }
 
@@ -365,6 +374,13 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
 }
 
 }  // namespace
+
+int lanczos_step_kernels(aed_handle* h, bool f32, const void* v_prev, const void* v_cur, void* v_next,
+                         const double* beta_prev, double* alpha, double* beta) {
+  int rc = handle_hv(h, f32, v_cur, v_next, h->d_partA);
+  if (rc) return rc;
+  return lanczos_step_tail(h, f32, v_prev, v_cur, v_next, v_prev ? beta_prev : nullptr, alpha, beta);
+}
 
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
   std::memset(r, 0, sizeof *r);
