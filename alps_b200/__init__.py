@@ -130,6 +130,7 @@ def lib():
             "aed_time_mult": (ctypes.c_int, [_P, _P, _P, _I32, _DP]),
             "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
             "aed_launch_count": (ctypes.c_int, [_I64P]),
+            "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

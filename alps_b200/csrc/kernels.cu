@@ -15,38 +15,10 @@
 #include <string>
 
 #include "kernels.cuh"
+#include "reduce.cuh"
 
 namespace aed {
 namespace {
-
-// Fixed-shape block reduction: warp shuffles, then warp 0 over the warp sums.
-// Same order on every call, so the result is bitwise reproducible.  The
-// total is returned to every thread.
-template <int NT>
-__device__ __forceinline__ double block_sum_all(double v, double* sm) {
-  static_assert(NT % 32 == 0 && NT <= 1024, "block size");
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sm[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    double r = (l < NT / 32) ? sm[l] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-    if (l == 0) sm[32] = r;
-  }
-  __syncthreads();
-  const double r = sm[32];
-  __syncthreads();
-  return r;
-}
-
-// Sum of n partials in a fixed order (thread-strided, then block_sum_all).
-template <int NT>
-__device__ __forceinline__ double sum_partials(const double* __restrict__ p, int n, double* sm) {
-  double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += NT) v += p[i];
-  return block_sum_all<NT>(v, sm);
-}
 
 // ---------------------------------------------------------------------------
 // The apply.  A tile is up to kTileRows consecutive rows of one hi block h: all
@@ -382,35 +354,15 @@ __global__ void scal_kernel(double a, T* __restrict__ x, int64_t n, bool divide)
     x[i] = (T)(divide ? __ddiv_rn((double)x[i], a) : __dmul_rn((double)x[i], a));
 }
 
-// Deterministic reductions over fixed chunks of kRedChunk elements: chunk c
-// is always summed by one CTA in the same thread order and tree, whatever the
-// grid, so partial[c] and every total built from the partials are
-// reproducible bit for bit on any GPU.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) dot_partials_kernel(const T* __restrict__ x, const T* __restrict__ y,
                                                                   int64_t n, double* __restrict__ part, bool sq) {
-  __shared__ double sm[33];
-  const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
-  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
-    const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
-    double acc = 0.0;
-    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
-      const double a = (double)x[i];
-      acc = fma(a, sq ? a : (double)y[i], acc);
-    }
-    const double tot = block_sum_all<kRedThreads>(acc, sm);
-    if (threadIdx.x == 0) part[c] = tot;
-  }
+  chunk_dot_partials<T>(x, y, n, part, sq);
 }
 
-// *out = sum of n partials (sqrt if asked), one CTA, fixed order.
-__global__ void __launch_bounds__(1024) finish_sum_kernel(const double* __restrict__ part, int64_t n,
-                                                          double* __restrict__ out, bool take_sqrt) {
-  __shared__ double sm[33];
-  double v = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += 1024) v += part[i];
-  const double tot = block_sum_all<1024>(v, sm);
-  if (threadIdx.x == 0) *out = take_sqrt ? sqrt(tot) : tot;
+__global__ void __launch_bounds__(kFinishThreads) finish_sum_kernel(const double* __restrict__ part, int64_t n,
+                                                                    double* __restrict__ out, bool take_sqrt) {
+  finish_sum(part, n, out, take_sqrt);
 }
 
 // make_step middle part (lanczos.h:398-401): w -= a v; w -= b v_prev; chunk partials of |w|^2
@@ -620,7 +572,7 @@ int launch_dot_partials(const T* x, const T* y, int64_t n, double* part, bool sq
 }
 
 int launch_finish_sum(const double* part, int64_t n, double* out, bool take_sqrt, cudaStream_t st) {
-  finish_sum_kernel<<<1, 1024, 0, st>>>(part, n, out, take_sqrt);
+  finish_sum_kernel<<<1, kFinishThreads, 0, st>>>(part, n, out, take_sqrt);
   return check_launch("finish_sum_kernel");
 }
 

@@ -192,6 +192,30 @@ int aed_get_stream(aed_handle* h, void** stream);
 /* Number of engine kernel launches made by this process so far. */
 int aed_launch_count(int64_t* count);
 
+/* Dot product that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot let a library allocate device memory: applications
+ * whose device memory belongs to another allocator (a framework's caching
+ * allocator, a fixed arena given to a simulation code at start-up), and
+ * latency-critical loops that cannot pay for cudaMalloc/cudaFree (cudaFree
+ * synchronises the whole device).
+ *
+ * *out (a device double) = sum_i x[i] * y[i] over n device elements (double for
+ * AED_FP64, float for AED_FP32, accumulated in double), with the same chunking
+ * and summation order as aed_dot, so both return the same bits.  Work is
+ * queued on `stream` (a cudaStream_t; NULL = the legacy default stream) and the
+ * call returns without waiting.  The caller passes the inputs and the output;
+ * the scratch (the per-chunk partial sums) is a fixed 512 KiB device array
+ * inside libaed.so that every GPU loading the library keeps until the process
+ * exits, so n is limited to 268,435,456 elements (larger n: AED_ERR_INVALID,
+ * nothing launched).  The first call on a device looks up that array's device
+ * address; make that first call before any stream capture.  Every call
+ * overwrites the partials it then reads, so nothing needs clearing, but all
+ * calls share the one array: calls that overlap on the GPU (different
+ * streams, different host threads) race and can return wrong sums; order
+ * them on one stream. */
+int aed_dot_noalloc(const void* x, const void* y, int64_t n, int precision, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
