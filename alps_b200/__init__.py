@@ -108,6 +108,7 @@ def lib():
             "aed_create": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(_P)]),
             "aed_destroy": (ctypes.c_int, [_P]),
+            "aed_set_couplings": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc)]),
             "aed_dimension": (ctypes.c_int, [_P, _I64P]),
             "aed_basis_copy": (ctypes.c_int, [_P, _U32P, _I64, _I64]),
             "aed_index": (ctypes.c_int, [_P, _U32P, _I64, _I64P]),
@@ -249,6 +250,21 @@ class Hamiltonian:
         d = ctypes.c_int64(0)
         _check(lib().aed_dimension(self._h, ctypes.byref(d)))
         self.dim = d.value
+
+    def set_couplings(self, bonds, site_h=None, site_d=None):
+        """Re-target this handle to a new bond list on the same sector."""
+        nb = len(bonds)
+        self.bonds = [tuple(b) for b in bonds]
+        self._s1 = np.array([b[0] for b in self.bonds] or [0], np.int32)
+        self._s2 = np.array([b[1] for b in self.bonds] or [0], np.int32)
+        self._jz = np.array([b[2] for b in self.bonds] or [0.0])
+        self._jxy = np.array([b[3] for b in self.bonds] or [0.0])
+        self._k = np.array([(b[4] if len(b) > 4 else 0.0) for b in self.bonds] or [0.0])
+        self._sh = None if site_h is None else np.ascontiguousarray(site_h, dtype=np.float64)
+        self._sd = None if site_d is None else np.ascontiguousarray(site_d, dtype=np.float64)
+        desc = ModelDesc(self.n_sites, self.n_up, nb, self._s1.ctypes.data_as(_I32P), self._s2.ctypes.data_as(_I32P),
+                         _dp(self._jz), _dp(self._jxy), _dp(self._k), _dp(self._sh), _dp(self._sd))
+        _check(lib().aed_set_couplings(self._h, ctypes.byref(desc)))
 
     @classmethod
     def from_parameters(cls, params, precision=FP64, device=0):

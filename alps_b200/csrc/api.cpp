@@ -316,6 +316,25 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   return AED_OK;
 }
 
+int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
+  if (!h || !model) return fail(AED_ERR_INVALID, "NULL argument");
+  if (model->n_sites != h->model.N || model->n_up != h->model.n_up)
+    return fail(AED_ERR_INVALID, "aed_set_couplings: the sector (n_sites, n_up) must stay the same");
+  Model m;
+  int rc = model_from_desc(model, m);
+  if (rc) return rc;
+  HvParams P;
+  if ((rc = build_hv_params(m, h->tab.Nlo, P))) return rc;
+  DeviceGuard g(h->device);
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // no apply of the old couplings in flight
+  h->model = m;
+  h->P = P;
+  rc = launch_diag_table(h->P, h->dt, h->d_dg, h->stream);
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
 int aed_destroy(aed_handle* h) {
   if (!h) return AED_OK;
   DeviceGuard g(h->device);

@@ -51,6 +51,11 @@ NEV = 2
 # CPU, scales its per-iteration sample by these counts.
 FP64_ITERATIONS_FALLBACK = 160
 
+# DRAM bytes (read + write) of one launch of the FP64 apply on this workload,
+# from ncu (dram__bytes_read.sum + dram__bytes_write.sum), summarised in
+# profiles/hv_kernel_l28_fp64.md.  None until captured.
+HV_TRAFFIC_L28_FP64 = None
+
 
 def j2_stream(n):
     return np.random.default_rng(SEED_J2).uniform(0.0, 0.5, n)
@@ -227,13 +232,14 @@ def run_ours(args):
     K, W = args.steps, args.warmup
     N, n_up = L28, L28 // 2
     j2s = j2_stream((W + K) * world)[rank::world]
-    # inputs resident before the timed region: one handle per input
-    hams = [ed.Hamiltonian(N, n_up, chain_bonds(L28, j2), precision=ed.FP64, device=local) for j2 in j2s]
-    D = hams[0].dim
-    for h in hams[:W]:
-        h.solve(nev=NEV, seed=1)
-    barrier(pg)
-    stream = torch.cuda.ExternalStream(hams[0].stream())
+    # the sector tables are resident before the timed region; each step sets
+    # that step's couplings (coupling tables + diagonal, ~ms) and solves
+    ham = ed.Hamiltonian(N, n_up, chain_bonds(L28, j2s[0]), precision=ed.FP64, device=local)
+    D = ham.dim
+    for j2 in j2s[:W]:
+        ham.set_couplings(chain_bonds(L28, j2))
+        ham.solve(nev=NEV, seed=1)
+    stream = torch.cuda.ExternalStream(ham.stream())
     launches0 = ed.launch_count()
     clocks = ClockSampler(local)
     iters, apply_ms, evals = [], [], []
@@ -241,16 +247,14 @@ def run_ours(args):
         barrier(pg)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        # all handles record on their own streams; bracket with events on the
-        # first handle's stream and a device-wide synchronize before the end event
         e0.record(stream)
         t0 = time.perf_counter()
-        for h in hams[W:]:
-            r = h.solve(nev=NEV, seed=1, profile=True)
+        for j2 in j2s[W:]:
+            ham.set_couplings(chain_bonds(L28, j2))
+            r = ham.solve(nev=NEV, seed=1, profile=True)
             iters.append(r["iterations"])
             apply_ms.append(r["apply_ms"])
             evals.append(r["evals"].tolist())
-        torch.cuda.synchronize()
         e1.record(stream)
         e1.synchronize()
         wall = time.perf_counter() - t0
@@ -268,67 +272,73 @@ def run_ours(args):
     achieved = b_apply / t_apply / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "kernel": "hv_kernel<double>", "apply_ms": t_apply * 1e3,
-            "algorithmic_bytes_per_apply": b_apply, "traffic": read_traffic("hv_kernel<double>@L28")}
-    # end-to-end through the public API with host buffers: create (tables H2D),
-    # solve from a pinned host start vector (H2D), eigenvalues back (D2H)
-    e2e = None
-    if rank == 0 or True:
-        start = torch.empty(D, dtype=torch.float64, pin_memory=True)
-        start.numpy()[:] = np.random.default_rng(7).uniform(0, 1, D)
-        h2d = d2h = 0
-        barrier(pg)
-        t0 = time.perf_counter()
-        for j2 in j2s[W:]:
-            bonds = chain_bonds(L28, j2)
-            h = ed.Hamiltonian(N, n_up, bonds, precision=ed.FP64, device=local)
-            r = h.solve(nev=NEV, start=start.numpy())
-            h.close()
-            h2d += D * 8 + (2 ** 14) * 4 + (2 ** 14) * 4 + len(bonds) * 32 + (D // 256 + 2 ** 14) * 8
-            d2h += 16 * (r["iterations"] + 1)
-        torch.cuda.synchronize()
-        e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
-        e2e = {"value": total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
-               "path": "aed_create + aed_solve(host start vector) + aed_destroy"}
+            "algorithmic_bytes_per_apply": b_apply, "traffic": HV_TRAFFIC_L28_FP64,
+            "traffic_source": "profiles/hv_kernel_l28_fp64.md (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                              "one launch)"}
     print(f"[bench] fp64: {value:.3f} solves/s, iterations {iters}, apply {t_apply*1e3:.3f} ms "
           f"({achieved:.0f} GB/s)", file=sys.stderr)
+    # end-to-end through the public API with host buffers, every step:
+    # aed_create (tables H2D) + aed_solve from a pinned host start vector (H2D)
+    # + eigenvalues and the alpha/beta stream (D2H) + aed_destroy
+    start = torch.empty(D, dtype=torch.float64, pin_memory=True)
+    start.numpy()[:] = np.random.default_rng(7).uniform(0, 1, D)
+    nlo = (N + 1) // 2
+    table_bytes = (1 << (N - nlo)) * 4 + 2 * (1 << nlo) * 2 + (nlo + 2) * 4 + 8 * ((D + 2047) // 2048 + (1 << (N - nlo)))
+    h2d = d2h = 0
+    barrier(pg)
+    t0 = time.perf_counter()
+    for j2 in j2s[W:]:
+        bonds = chain_bonds(L28, j2)
+        h = ed.Hamiltonian(N, n_up, bonds, precision=ed.FP64, device=local)
+        r = h.solve(nev=NEV, start=start.numpy())
+        h.close()
+        h2d += D * 8 + table_bytes + len(bonds) * 32
+        d2h += 16 * (r["iterations"] + 1) + 32 * NEV
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    e2e = {"value": total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
+           "path": "aed_create + aed_solve(pinned host start vector) + aed_destroy, wall clock"}
     # mixed precision on the same inputs: FP32 Lanczos basis + FP64 refinement
     mixed = None
     if not args.no_mixed:
-        h32 = [ed.Hamiltonian(N, n_up, chain_bonds(L28, j2), precision=ed.FP32, device=local) for j2 in j2s[W:]]
-        h32[0].solve(nev=NEV, seed=1)
+        h32 = ed.Hamiltonian(N, n_up, chain_bonds(L28, j2s[0]), precision=ed.FP32, device=local)
+        h32.solve(nev=NEV, seed=1)  # grows the FP32 basis store once
         barrier(pg)
-        t0 = time.perf_counter()
+        s32 = torch.cuda.ExternalStream(h32.stream())
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
         mev, mit, m32ms = [], [], []
-        for h in h32:
-            r = h.solve(nev=NEV, seed=1, profile=True)
+        m0.record(s32)
+        for j2 in j2s[W:]:
+            h32.set_couplings(chain_bonds(L28, j2))
+            r = h32.solve(nev=NEV, seed=1, profile=True)
             mev.append(r["evals"].tolist())
             mit.append((r["iterations_low"], r["iterations"]))
             m32ms.append(r["apply_ms"])
-        torch.cuda.synchronize()
-        mixed_s = max_over_ranks(pg, time.perf_counter() - t0)
+        m1.record(s32)
+        m1.synchronize()
+        mixed_s = max_over_ranks(pg, m0.elapsed_time(m1) / 1e3)
         rel = max(abs(a - b) / abs(b) for ea, eb in zip(mev, evals) for a, b in zip(ea, eb))
         b32 = D * ((1 + nbar) * 4 + 4)
         mixed = {"solves_per_s": total / mixed_s, "speedup_vs_fp64": (total / mixed_s) / value,
                  "max_rel_energy_err_vs_fp64": rel, "iterations_fp32_fp64": mit,
                  "apply_ms_fp32": float(np.mean(m32ms)),
                  "hv_fp32_gbs": b32 / (float(np.mean(m32ms)) / 1e3) / 1e9}
-        for h in h32:
-            h.close()
+        h32.close()
         print(f"[bench] mixed: {mixed}", file=sys.stderr)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(float(j2s[W]), int(round(np.mean(iters))))
-    for h in hams:
-        h.close()
+    ham.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": t_max / K * 1e3 if world == 1 else t_max / (K) * 1e3,
+            "ms_per_step": t_max / K * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "J1-J2 chain L=28 periodic, Sz=0, D=40116600, J1=1, J2~U[0,0.5] seed 2802, "
                                    "lowest 2 eigenvalues, FP64 Lanczos (ietl rule 100 eps)",
                        "dimension": D, "nev": NEV, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (each vector 321 MB)"},
+                       "l2": "inputs larger than L2 (each vector 321 MB); no flush"},
             "iterations": iters, "evals": evals, "wall_s": wall,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(), "mixed": mixed,

@@ -101,6 +101,13 @@ typedef struct aed_handle aed_handle;
 int aed_create(const aed_model_desc* model, int precision, int device, aed_handle** out);
 int aed_destroy(aed_handle* h);
 
+/* Replace the couplings of a handle (same N, n_up; any bond list), keeping its
+ * basis tables, workspaces and apply tuning: the parameter sweeps sparsediag
+ * jobs run (one task per coupling set, applications/diag/diag.h:85-138)
+ * without rebuilding the sector.  Rebuilds the coupling tables and the
+ * diagonal M(i,i) (hamiltonian_matrix.hpp:422-450). */
+int aed_set_couplings(aed_handle* h, const aed_model_desc* model);
+
 /* Sector dimension D (hamiltonian_matrix::dimension). */
 int aed_dimension(const aed_handle* h, int64_t* dim);
 

@@ -303,3 +303,17 @@ def test_mixed_precision_within_1e9_of_fp64(name, p, nev):
     rel = np.abs(r32["evals"] - r64["evals"]) / np.abs(r64["evals"])
     assert np.all(rel <= 1e-9), rel
     assert r32["iterations_low"] > 0
+
+
+def test_set_couplings_matches_fresh_handle():
+    """aed_set_couplings re-targets a handle: same results as a handle built from scratch."""
+    p1 = spin_params(LATTICE="nnn chain lattice", L=14, J=1, J1=0.2)
+    p2 = spin_params(LATTICE="nnn chain lattice", L=14, J=1, J1=0.45, h=0.1)
+    ham = ed.Hamiltonian.from_parameters(p1)
+    m2 = ed.model_from_parameters(p2)
+    ham.set_couplings(m2["bonds"], m2["site_h"], m2["site_d"])
+    ref = _oracle_for(m2)
+    x = np.random.default_rng(2).normal(size=ham.dim)
+    assert np.array_equal(ham.apply(x), ref.mult(x))
+    with pytest.raises(ed.AEDError):
+        ham.set_couplings([(0, 1, 1.0, 1.0)] * 3 + [(0, 15, 1.0, 1.0)])
