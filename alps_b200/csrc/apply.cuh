@@ -1,0 +1,272 @@
+// apply.cuh -- the tile apply y = H x shared by the single-instance and the
+// batched kernels.
+//
+// Reference paths are relative to the ALPS source tree.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "reduce.cuh"
+
+namespace aed {
+namespace apply {
+
+// ---------------------------------------------------------------------------
+// The apply.  A tile is up to kTileRows consecutive rows of one hi block h: all
+// its states share the high Nhi bits.  For such a tile every flip pair falls
+// into one of three cases, decided once per tile:
+//   * both bits in the hi part: the flip applies to all rows of the tile or to
+//     none (it depends on h only); its target is row thi[h'] + r of the hi
+//     block h' = h ^ flip (same lo state, so the same offset r): a coalesced
+//     stream of x;
+//   * one bit in each part: applies iff the lo state has one given bit value;
+//     target thi[h'] + tlo[l ^ bit];
+//   * both bits in the lo part: applies iff the two lo bits differ (in a given
+//     order for the FP64 row order); target thi[h] + tlo[l ^ flip].
+// Warp 0 compiles the tile's "program": the flips that can apply, with their
+// target block base already looked up, plus the diagonal.  All threads then
+// run it on R rows each.  The coupling tables are staged in shared memory
+// once per CTA (indexing them from parameter space with a loop counter
+// serialises on the constant-load path).
+//
+// FP64 rows are bit-identical to y = prod(M, x) over the reference's explicit
+// matrix (src/ietl/interface/ublas.h:57-63 over hamiltonian_matrix.hpp:307-345):
+// a row of M holds the flips to smaller states (ascending column = hi bit
+// descending, then lo bit ascending), the diagonal M(i,i), then the flips to
+// larger states (hi ascending, lo descending), summed left to right from 0.
+// Products and sums round separately (__dmul_rn/__dadd_rn: no FMA
+// contraction), as on the reference's x86-64 build.  M(i,i) comes from a
+// per-row table filled once per handle in the reference's term order; the
+// program for FP64 holds the "smaller" flips, the diagonal, then the "larger"
+// flips, in that column order.
+//
+// FP32 rows (mixed path) take each flip once in any order and accumulate the
+// terms c * x_j in FP64 (c is FP64, x_j FP32: every product carries a 53-bit
+// significand), rounding to FP32 once at the end; the alternative TwoSum
+// (Knuth) + FMA-product-error accumulation in FP32 (Ogita, Rump & Oishi,
+// "Dot2") is kept as AccTwoSum.
+// ---------------------------------------------------------------------------
+constexpr int kTileRows = kHvTileRows;
+constexpr uint32_t kDiagOp = 0xffffffffu;
+constexpr uint32_t kXorCond = 0xffffu;  // lo-part condition: the two bits differ
+constexpr int kMaxOps = 2 * kMaxBonds + 1;
+
+struct SPair {
+  uint32_t flip, cond;
+  double c;
+};
+
+// One program entry: mc = lo-part flip | (lo-part condition << 16), or
+// kDiagOp; nb = base row of the target hi block; c = coupling.
+struct TileOp {
+  uint32_t mc, nb;
+  double c;
+};
+
+// ---- row accumulators ----
+struct AccExact64 {  // FP64 vectors, the reference's rounding
+  double a = 0.0;
+  __device__ __forceinline__ void add(double c, double xv) { a = __dadd_rn(a, __dmul_rn(c, xv)); }
+  __device__ __forceinline__ double value() const { return a; }
+};
+
+struct AccWide32 {  // FP32 vectors, FP64 accumulator
+  double a = 0.0;
+  __device__ __forceinline__ void add(double c, float xv) { a = fma(c, (double)xv, a); }
+  __device__ __forceinline__ float value() const { return (float)a; }
+};
+
+struct AccTwoSum32 {  // FP32 vectors, TwoSum + exact product error in FP32
+  float s = 0.f, e = 0.f;
+  __device__ __forceinline__ void add(double c, float xv) {
+    const float ch = (float)c, cl = (float)(c - (double)ch);
+    const float p = __fmul_rn(ch, xv);
+    const float pe = __fmaf_rn(ch, xv, -p);  // exact: ch*xv - p
+    const float t = __fadd_rn(s, p);
+    const float bb = __fsub_rn(t, s);
+    const float se = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(p, bb));
+    s = t;
+    e = __fadd_rn(e, __fadd_rn(se, __fmaf_rn(cl, xv, pe)));
+  }
+  __device__ __forceinline__ float value() const { return __fadd_rn(s, e); }
+};
+
+// Warp 0: append to prog the entries of `list` that can apply in hi block h
+// (FP64 order: cond fixes which of the two bits must be set).
+__device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
+                                               const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int q0 = 0; q0 < np; q0 += 32) {
+    const int q = q0 + lane;
+    bool emit = false;
+    TileOp op;
+    if (q < np) {
+      const SPair e = list[q];
+      const uint32_t fhi = e.flip >> Nlo, chi = e.cond >> Nlo;
+      if ((h & fhi) == chi) {
+        emit = true;
+        op = {(e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e.c};
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, emit);
+    if (emit) prog[cnt + __popc(m & ((1u << lane) - 1u))] = op;
+    cnt += __popc(m);
+  }
+  return cnt;
+}
+
+// Warp 0: every flip once, either direction (FP32 rows: order is free).
+__device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
+                                          const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int q0 = 0; q0 < np; q0 += 32) {
+    const int q = q0 + lane;
+    bool emit = false;
+    TileOp op;
+    if (q < np) {
+      const SPair e = list[q];
+      const uint32_t fhi = e.flip >> Nlo, flo = e.flip & lm;
+      const uint32_t hb = h & fhi;
+      if (flo == 0u) {  // hi part only: applies to the whole tile iff the two bits differ
+        emit = __popc(hb) == 1;
+        op = {0u, __ldg(thi + (h ^ fhi)), e.c};
+      } else if (fhi == 0u) {  // lo part only
+        emit = true;
+        op = {flo | (kXorCond << 16), __ldg(thi + h), e.c};
+      } else {  // crossing: the lo bit must differ from the hi bit
+        emit = true;
+        op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, emit);
+    if (emit) prog[cnt + __popc(m & ((1u << lane) - 1u))] = op;
+    cnt += __popc(m);
+  }
+  return cnt;
+}
+
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void run_ops(const TileOp* prog, int o0, int o1, const uint32_t* lv, uint32_t nrow,
+                                        uint32_t rt, const double* __restrict__ dg, uint32_t base,
+                                        const uint16_t* __restrict__ tlo, const T* __restrict__ x, Acc* acc) {
+  for (int o = o0; o < o1; ++o) {
+    const TileOp e = prog[o];
+    const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
+    if (e.mc == kDiagOp) {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          acc[u].add(__ldg(dg + i), __ldg(x + i));
+        }
+    } else if (fl == 0u) {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow) acc[u].add(e.c, __ldg(x + e.nb + rt + u * kHvThreads));
+    } else if (cd == kXorCond) {
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const uint32_t b = lv[u] & fl;
+        if ((uint32_t)u < nrow && b != 0u && b != fl) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow && (lv[u] & fl) == cd) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+    }
+  }
+}
+
+struct ApplyCtx {
+  int np, Nlo, n_up;
+  uint32_t lm;
+};
+
+// Shared memory of one CTA running tiles.
+struct ApplySmem {
+  SPair low[kMaxBonds];
+  SPair rise[kMaxBonds];
+  TileOp prog[kMaxOps];
+  int nops;
+  double red[33];
+};
+
+__device__ __forceinline__ ApplyCtx ctx_of(const HvParams& P) { return {P.n_pairs, P.Nlo, P.n_up, P.lomask}; }
+
+// Stage the flip pairs of P in shared memory (all threads; the next
+// apply_tile starts with a barrier).  Flips to smaller states need the higher
+// bit set, flips to larger states the lower one.
+__device__ __forceinline__ void stage_pairs(const HvParams& P, ApplySmem& sm) {
+  for (int q = threadIdx.x; q < P.n_pairs; q += kHvThreads) {
+    const PairTerm a = P.low[q], b = P.rise[q];
+    sm.low[q] = {a.mhi | a.mlo, a.mhi, a.c};
+    sm.rise[q] = {b.mhi | b.mlo, b.mlo, b.c};
+  }
+}
+
+// Tile `it` of y = H x.  alpha_part (optional) receives the tile's partial sum
+// of x_i * y_i at index it.  All threads of the CTA call it together.
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t, int64_t it,
+                                           const T* __restrict__ x, T* __restrict__ y,
+                                           double* __restrict__ alpha_part, ApplySmem& sm) {
+  static_assert(kTileRows % (kHvThreads * R) == 0, "rows per thread must divide the tile");
+  constexpr bool kOrdered = sizeof(T) == 8;
+  constexpr int kPasses = kTileRows / (kHvThreads * R);
+  const uint32_t h = __ldg(t.tile_h + it);
+  const uint32_t r0 = __ldg(t.tile_r + it);
+  const int k = c.n_up - __popc(h);
+  const uint32_t lbase = __ldg(t.looff + k);
+  const uint32_t rows = __ldg(t.looff + k + 1) - lbase;
+  const uint32_t base = __ldg(t.thi + h);
+  __syncthreads();  // tables staged; previous tile done with prog
+  if (threadIdx.x < 32) {
+    int cnt;
+    if (kOrdered) {
+      const int nl = compile_ordered(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
+      if (threadIdx.x == 0) sm.prog[nl].mc = kDiagOp;
+      cnt = compile_ordered(sm.rise, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, nl + 1);
+    } else {
+      if (threadIdx.x == 0) sm.prog[0].mc = kDiagOp;
+      cnt = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 1);
+    }
+    if (threadIdx.x == 0) sm.nops = cnt;
+  }
+  __syncthreads();
+  const int nops = sm.nops;
+  double dotacc = 0.0;
+#pragma unroll 1
+  for (int pass = 0; pass < kPasses; ++pass) {
+    const uint32_t rt = r0 + pass * (kHvThreads * R) + threadIdx.x;  // row offset of u = 0
+    uint32_t lv[R];
+    uint32_t nrow = 0;  // rows of this thread that exist (a prefix of u)
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const uint32_t r = rt + u * kHvThreads;
+      const bool ok = r < rows && r < r0 + kTileRows;
+      nrow += ok ? 1u : 0u;
+      lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
+    }
+    Acc acc[R];
+    run_ops<T, Acc, R>(sm.prog, 0, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      if ((uint32_t)u < nrow) {
+        const uint32_t i = base + rt + u * kHvThreads;
+        const T v = acc[u].value();
+        y[i] = v;
+        if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
+      }
+    }
+  }
+  if (alpha_part) {
+    const double tot = block_sum_all<kHvThreads>(dotacc, sm.red);
+    if (threadIdx.x == 0) alpha_part[it] = tot;
+  }
+}
+
+}  // namespace apply
+}  // namespace aed
