@@ -132,6 +132,7 @@ def lib():
             "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
             "aed_launch_count": (ctypes.c_int, [_I64P]),
             "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
+            "aed_tmatrix": (ctypes.c_int, [_I32, _DP, _DP, _I32, _DP, _DP, _I32P, _I32P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -150,6 +151,19 @@ def _check(rc):
 
 def _dp(a):
     return a.ctypes.data_as(_DP) if a is not None else None
+
+
+def tmatrix(alpha, beta):
+    """The engine's Tmatrix::compute(true): distinct non-ghost values, errors, multiplicities."""
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    b = np.ascontiguousarray(beta, dtype=np.float64)
+    n = a.size
+    ev, er = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+    mu = np.zeros(max(n, 1), np.int32)
+    cnt = ctypes.c_int32(0)
+    _check(lib().aed_tmatrix(n, _dp(a), _dp(b), n, _dp(ev), _dp(er), mu.ctypes.data_as(_I32P), ctypes.byref(cnt)))
+    c = cnt.value
+    return {"evals": ev[:c], "errors": er[:c], "mults": mu[:c]}
 
 
 def launch_count() -> int:

@@ -27,7 +27,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-para
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
 CPP_SOURCES = ["model.cpp", "tmatrix.cpp", "api.cpp", "lanczos.cpp"]
-HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh"]
+HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "tmatrix_core.h"]
 
 
 def _newer(src, dst, deps):

@@ -1,5 +1,6 @@
 // api.cpp -- the C ABI of libaed.so (declared in include/aed.h).
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -593,6 +594,29 @@ int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* m
   cudaEventDestroy(e1);
   if (rc) return rc;
   *ms = (double)t / reps;
+  return AED_OK;
+}
+
+int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap, double* evals, double* errors,
+                int32_t* mults, int32_t* count) {
+  if (n < 0 || (n > 0 && (!alpha || !beta)) || !count) return fail(AED_ERR_INVALID, "NULL argument");
+  *count = 0;
+  if (n == 0) return AED_OK;
+  double amax = alpha[0], bmax = beta[0];
+  for (int i = 1; i < n; ++i) {
+    amax = std::max(amax, alpha[i]);
+    bmax = std::max(bmax, beta[i]);
+  }
+  TmatInfo t;
+  const int rc = tmatrix_analyze(n, alpha, beta, amax, bmax, t);
+  if (rc) return rc;
+  const int c = (int)t.evals.size();
+  for (int i = 0; i < c && i < cap; ++i) {
+    if (evals) evals[i] = t.evals[i];
+    if (errors) errors[i] = t.errs[i];
+    if (mults) mults[i] = t.mults[i];
+  }
+  *count = c;
   return AED_OK;
 }
 

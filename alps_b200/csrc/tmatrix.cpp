@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "aed_internal.h"
+#include "tmatrix_core.h"
 
 namespace aed {
 
@@ -104,64 +105,18 @@ int tmatrix_analyze(int n, const double* alpha, const double* beta, double alpha
                     TmatInfo& out) {
   out = TmatInfo();
   if (n < 1) return AED_OK;
-  std::vector<double> ev(alpha, alpha + n), e(n + 1, 0.0), zl(n);
-  for (int i = 0; i + 1 < n; ++i) e[i] = beta[i];
-  if (tridiag_eigen(n, ev.data(), e.data(), zl.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
-  const double eps = DBL_EPSILON;
-  const double error_tol = std::pow(eps, 2.0 / 3.0);  // tmatrix.h:32
-  out.multol = std::max(alpha_max, beta_max) * 2 * eps * (10000 + n);
-  out.thold = std::max(error_tol * std::max(ev[0], ev[n - 1]), 5 * out.multol);
-  const double bl = beta[n - 1];  // beta_{m+1}
-  std::vector<double> dist, err;
-  std::vector<int> mult, first;
-  double temp = ev[0];
-  dist.push_back(ev[0]);
-  first.push_back(0);
-  int multiple = 1;
-  for (int i = 1; i < n; ++i) {
-    if ((ev[i] - temp) > out.thold) {
-      dist.push_back(ev[i]);
-      first.push_back(i);
-      temp = ev[i];
-      mult.push_back(multiple);
-      err.push_back(multiple > 1 ? 0.0 : std::fabs(bl * zl[i - 1]));
-      multiple = 1;
-    } else {
-      ++multiple;
-    }
-  }
-  mult.push_back(multiple);
-  err.push_back(multiple > 1 ? 0.0 : std::fabs(bl * zl[n - 1]));
-  // spurious ("ghost") values: eigenvalues of T without its first row and
-  // column that coincide within multol with a simple eigenvalue of T
-  std::vector<double> evg;
-  if (n > 1) {
-    evg.assign(alpha + 1, alpha + n);
-    std::vector<double> eg(n, 0.0);
-    for (int i = 1; i + 1 < n; ++i) eg[i - 1] = beta[i];
-    if (tridiag_eigen(n - 1, evg.data(), eg.data(), nullptr))
-      return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
-  }
-  int t2 = 0;
-  for (size_t i = 0; i < dist.size(); ++i) {
-    if (mult[i] != 1) continue;
-    for (int j = t2; j < n - 2; ++j, ++t2) {
-      if ((evg[j] - dist[i]) >= out.multol) break;
-      if (std::fabs(dist[i] - evg[j]) < out.multol) {
-        mult[i] = 0;
-        err[i] = 0.0;
-        ++t2;
-        break;
-      }
-    }
-  }
-  for (size_t i = 0; i < dist.size(); ++i)
-    if (mult[i] != 0) {
-      out.evals.push_back(dist[i]);
-      out.errs.push_back(err[i]);
-      out.mults.push_back(mult[i]);
-      out.first.push_back(first[i]);
-    }
+  std::vector<double> scratch(5 * (size_t)n + 2), ev(n), er(n);
+  std::vector<int> mu(n), fi(n);
+  tcore::TResult res;
+  if (tcore::analyze(n, alpha, beta, alpha_max, beta_max, scratch.data(), n, ev.data(), er.data(), mu.data(),
+                     fi.data(), &res))
+    return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  out.thold = res.thold;
+  out.multol = res.multol;
+  out.evals.assign(ev.begin(), ev.begin() + res.count);
+  out.errs.assign(er.begin(), er.begin() + res.count);
+  out.mults.assign(mu.begin(), mu.begin() + res.count);
+  out.first.assign(fi.begin(), fi.begin() + res.count);
   return AED_OK;
 }
 

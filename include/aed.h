@@ -188,6 +188,13 @@ int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res);
  * *n receives its length (at most cap entries are written). */
 int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n);
 
+/* Tmatrix::compute(true) on a host recurrence (src/ietl/tmatrix.h:121-228):
+ * distinct non-ghost eigenvalues of T (alpha[0..n), beta[0..n-1) off-diagonal,
+ * beta[n-1] = beta_{m+1}), their error estimates |beta_{m+1} z_{m,i}| and
+ * multiplicities; at most cap written, *count = how many.  Host-only. */
+int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap, double* evals, double* errors,
+                int32_t* mults, int32_t* count);
+
 /* Time `reps` back-to-back applies y = H x on the handle's stream with CUDA
  * events; *ms = mean milliseconds per apply. */
 int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms);

@@ -140,3 +140,21 @@ def test_create_without_gpu_fails_loudly():
     with pytest.raises(ed.AEDError) as e:
         ed.Hamiltonian(4, 2, [(0, 1, 1.0, 1.0), (1, 2, 1.0, 1.0)])
     assert e.value.code == ed.ERR_CUDA
+
+
+@pytest.mark.parametrize("L,nev,seed", [(12, 4, 1), (14, 4, 11), (14, 2, 3)])
+def test_engine_tmatrix_matches_oracle_and_lapack(L, nev, seed):
+    """The engine's T-matrix analysis (shared by the host driver and the batched
+    device check) against the oracle's and the LAPACK-based restatement."""
+    N, nu, bonds = lattice.spin_model({"LATTICE": "chain lattice", "L": L, "J": 1, "Sz_total": 0})
+    r = oracle.Matrix(N, nu, bonds).lanczos(nev=nev, seed=seed)
+    a, b = r["alpha"], r["beta"]
+    for m in sorted({2, 3, 7, 20, len(a) // 2, len(a)}):
+        t = ed.tmatrix(a[:m], b[:m])
+        o = oracle.tmatrix(a[:m], b[:m])
+        lp = oracle.tmatrix_lapack(a[:m], b[:m])
+        assert len(t["evals"]) == len(o["evals"]) == len(lp["evals"])
+        np.testing.assert_allclose(t["evals"], lp["evals"], rtol=1e-12, atol=1e-12)
+        assert list(t["mults"]) == list(lp["mults"])
+        # error estimates are |beta z_last|; below ~eps*|T| they are rounding noise
+        np.testing.assert_allclose(t["errors"], lp["errors"], rtol=1e-5, atol=1e-13)
