@@ -16,7 +16,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "AEDError", "Hamiltonian", "DeviceVector", "parse_parameters", "model_from_parameters", "lib",
+    "AEDError", "Hamiltonian", "DeviceVector", "Server", "parse_parameters", "model_from_parameters", "lib",
     "FP64", "FP32",
 ]
 
@@ -82,6 +82,20 @@ class SolveResult(ctypes.Structure):
     ]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32), ("max_slots", ctypes.c_int32), ("steps_per_launch", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("hbm_fraction", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_int64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("resident", ctypes.c_int32), ("queued", ctypes.c_int32), ("bytes_used", ctypes.c_int64),
+        ("bytes_budget", ctypes.c_int64), ("graph_launches", ctypes.c_int64),
+    ]
+
+
 _lib = None
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -133,6 +147,13 @@ def lib():
             "aed_launch_count": (ctypes.c_int, [_I64P]),
             "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
             "aed_tmatrix": (ctypes.c_int, [_I32, _DP, _DP, _I32, _DP, _DP, _I32P, _I32P]),
+            "aed_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
+            "aed_server_destroy": (ctypes.c_int, [_P]),
+            "aed_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc), ctypes.POINTER(SolveOpts), _I64P]),
+            "aed_server_step": (ctypes.c_int, [_P, _I32P]),
+            "aed_server_poll": (ctypes.c_int, [_P, _I64, ctypes.POINTER(SolveResult)]),
+            "aed_server_cancel": (ctypes.c_int, [_P, _I64]),
+            "aed_server_get_stats": (ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -390,3 +411,89 @@ class Hamiltonian:
         b = np.zeros(max(n.value, 1))
         _check(lib().aed_last_tmatrix(self._h, _dp(a), _dp(b), n.value, ctypes.byref(n)))
         return a[: n.value], b[: n.value]
+
+
+def _result_dict(res):
+    n = res.n_evals
+    return {"evals": np.array(res.evals[:n]), "errors": np.array(res.errors[:n]), "iterations": res.iterations,
+            "iterations_low": res.iterations_low, "evals_low": np.array(res.evals_low[:n]),
+            "converged": bool(res.converged), "seconds": res.seconds}
+
+
+class Server:
+    """Batched / served Lanczos solves on one GPU (aed_server_*): requests are
+    admitted by HBM footprint and advance together, S Lanczos steps per CUDA
+    graph launch; new requests join at the next step."""
+
+    def __init__(self, precision=FP32, device=0, max_slots=512, steps=8, hbm_fraction=0.0, hbm_budget=0):
+        o = ServerOpts(device, max_slots, steps, precision, hbm_fraction, hbm_budget)
+        h = _P()
+        self._h = None
+        _check(lib().aed_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if self._h:
+            lib().aed_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, n_sites, n_up, bonds, nev=1, seed=0, max_iter=0, site_h=None, site_d=None):
+        nb = len(bonds)
+        s1 = np.array([b[0] for b in bonds] or [0], np.int32)
+        s2 = np.array([b[1] for b in bonds] or [0], np.int32)
+        jz = np.array([b[2] for b in bonds] or [0.0])
+        jxy = np.array([b[3] for b in bonds] or [0.0])
+        kq = np.array([(b[4] if len(b) > 4 else 0.0) for b in bonds] or [0.0])
+        sh = None if site_h is None else np.ascontiguousarray(site_h, dtype=np.float64)
+        sd = None if site_d is None else np.ascontiguousarray(site_d, dtype=np.float64)
+        desc = ModelDesc(n_sites, n_up, nb, s1.ctypes.data_as(_I32P), s2.ctypes.data_as(_I32P), _dp(jz), _dp(jxy),
+                         _dp(kq), _dp(sh), _dp(sd))
+        opts = SolveOpts(nev, max_iter, 0.0, 0.0, seed, None, 0, 0)
+        t = ctypes.c_int64(0)
+        _check(lib().aed_server_submit(self._h, ctypes.byref(desc), ctypes.byref(opts), ctypes.byref(t)))
+        return t.value
+
+    def step(self):
+        n = ctypes.c_int32(0)
+        _check(lib().aed_server_step(self._h, ctypes.byref(n)))
+        return n.value
+
+    def poll(self, ticket):
+        res = SolveResult()
+        rc = lib().aed_server_poll(self._h, ticket, ctypes.byref(res))
+        if rc == PENDING:
+            return None
+        _check(rc)
+        return _result_dict(res)
+
+    def cancel(self, ticket):
+        _check(lib().aed_server_cancel(self._h, ticket))
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().aed_server_get_stats(self._h, ctypes.byref(st)))
+        return {"resident": st.resident, "queued": st.queued, "bytes_used": st.bytes_used,
+                "bytes_budget": st.bytes_budget, "graph_launches": st.graph_launches}
+
+    def run(self, tickets, max_steps=100000):
+        """Step until every ticket finished; returns {ticket: result}."""
+        out, left = {}, set(tickets)
+        for _ in range(max_steps):
+            if not left:
+                break
+            self.step()
+            for t in list(left):
+                r = self.poll(t)
+                if r is not None:
+                    out[t] = r
+                    left.discard(t)
+        if left:
+            raise AEDError(ERR_NOT_CONVERGED, f"{len(left)} requests unfinished after {max_steps} steps")
+        return out

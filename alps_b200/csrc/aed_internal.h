@@ -92,7 +92,9 @@ struct TmatInfo {
   double thold = 0, multol = 0;
 };
 int tmatrix_analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
-                    TmatInfo& out);
+                    TmatInfo& out, double thold_rel = 0.0);
+// merge threshold (relative) of T-matrix analyses of FP32 recurrences
+constexpr double kFp32MergeRel = 2e-6;
 bool nlowest_converged(const TmatInfo& t, int nev, double rtol, double atol);
 
 // ---- parameters / lattices ----------------------------------------------------

@@ -1,0 +1,351 @@
+// batch.cu -- kernels of the batched / served Lanczos engine.
+//
+// One engine step advances every resident instance by one Lanczos step
+// (lanczos::make_step, src/ietl/lanczos.h:392-406):
+//   b_hv       y = H x over the (instance, tile) queue, per-tile <x,y> partials
+//   b_alpha    alpha_j = sum of the instance's tile partials (one CTA each)
+//   b_update   y = (y - alpha x) - beta_{j-1} v_{j-1} over (instance, chunk), chunk partials of |y|^2
+//   b_beta     beta_j = sqrt(sum of the chunk partials)
+//   b_norm     y /= beta_j
+//   b_advance  j += 1
+// After S steps the graph runs b_check (one thread per instance: the
+// T-matrix analysis of tmatrix_core.h and the phase rules), then the FP32 ->
+// FP64 hand-over (b_ritz, b_ritz_norm, b_ritz_scale, b_ritz_commit).
+// Every sum is formed per instance in a fixed order, so an instance's result
+// does not depend on which other instances share the batch.
+
+#include <cuda_runtime.h>
+
+#include "apply.cuh"
+#include "batch.cuh"
+#include "reduce.cuh"
+#include "tmatrix_core.h"
+
+namespace aed {
+namespace {
+
+using apply::AccExact64;
+using apply::AccWide32;
+using apply::ApplyCtx;
+using apply::ApplySmem;
+
+constexpr int kBR = 4;     // rows per thread of the batched apply
+constexpr int kBMinB = 4;  // CTAs per SM of the batched apply
+
+__device__ __forceinline__ bool stepping(const BInst& I) {
+  if (I.phase == kPhLow) return I.j + 1 < I.n_store && I.j < I.cap;
+  if (I.phase == kPhHigh) return I.j < I.cap;
+  return false;
+}
+
+__device__ __forceinline__ float* low_vec(const BInst& I, int j) {
+  return I.chunk[j / kStoreChunkB] + (int64_t)(j % kStoreChunkB) * I.ldv;
+}
+__device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v64[j % 3]; }
+
+__global__ void __launch_bounds__(kHvThreads, kBMinB) b_hv(BatchArgs a) {
+  __shared__ ApplySmem sm;
+  const int n = *a.n_tiles;
+  int cur = -1;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.tiles[it];
+    const BInst& I = a.inst[w.inst];
+    if (!stepping(I)) continue;  // same for every thread of the CTA
+    const int j = I.j;
+    if (w.inst != cur) {
+      __syncthreads();  // the previous tile is done with the staged pairs
+      apply::stage_pairs(*I.P, sm);
+      cur = w.inst;
+    }
+    const ApplyCtx c = apply::ctx_of(*I.P);
+    if (I.phase == kPhLow)
+      apply::apply_tile<float, AccWide32, kBR>(c, I.t, w.idx, low_vec(I, j), low_vec(I, j + 1), I.partA, sm);
+    else
+      apply::apply_tile<double, AccExact64, kBR>(c, I.t, w.idx, high_vec(I, j), high_vec(I, j + 1), I.partA, sm);
+  }
+}
+
+__global__ void __launch_bounds__(256) b_alpha(BatchArgs a) {
+  __shared__ double red[33];
+  if ((int)blockIdx.x >= *a.n_inst) return;
+  BInst& I = a.inst[blockIdx.x];
+  if (!stepping(I)) return;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < I.n_tiles; i += 256) v += I.partA[i];
+  const double tot = block_sum_all<256>(v, red);
+  if (threadIdx.x == 0) I.ab[2 * I.j] = tot;
+}
+
+template <typename T>
+__device__ __forceinline__ double update_chunk(const T* x, const T* vp, T* y, int64_t e0, int64_t e1, double alpha,
+                                               double b) {
+  double acc = 0.0;
+  for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+    double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
+    if (vp) w = __dsub_rn(w, __dmul_rn(b, (double)vp[i]));
+    const T wt = (T)w;
+    y[i] = wt;
+    acc = fma((double)wt, (double)wt, acc);
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kRedThreads) b_update(BatchArgs a) {
+  __shared__ double red[33];
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    BInst& I = a.inst[w.inst];
+    if (!stepping(I)) continue;
+    const int j = I.j;
+    const double alpha = I.ab[2 * j];
+    const double b = j > 0 ? I.ab[2 * (j - 1) + 1] : 0.0;
+    const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+    double acc;
+    if (I.phase == kPhLow)
+      acc = update_chunk<float>(low_vec(I, j), j > 0 ? low_vec(I, j - 1) : nullptr, low_vec(I, j + 1), e0, e1, alpha, b);
+    else
+      acc = update_chunk<double>(high_vec(I, j), j > 0 ? high_vec(I, j - 1) : nullptr, high_vec(I, j + 1), e0, e1,
+                                 alpha, b);
+    const double tot = block_sum_all<kRedThreads>(acc, red);
+    if (threadIdx.x == 0) I.partB[w.idx] = tot;
+  }
+}
+
+__global__ void __launch_bounds__(256) b_beta(BatchArgs a) {
+  __shared__ double red[33];
+  if ((int)blockIdx.x >= *a.n_inst) return;
+  BInst& I = a.inst[blockIdx.x];
+  if (!stepping(I)) return;
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < I.n_chunks; i += 256) v += I.partB[i];
+  const double tot = block_sum_all<256>(v, red);
+  if (threadIdx.x == 0) I.ab[2 * I.j + 1] = sqrt(tot);
+}
+
+__global__ void __launch_bounds__(kRedThreads) b_norm(BatchArgs a) {
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    const BInst& I = a.inst[w.inst];
+    if (!stepping(I)) continue;
+    const int j = I.j;
+    const double beta = I.ab[2 * j + 1];
+    const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+    if (I.phase == kPhLow) {
+      float* y = low_vec(I, j + 1);
+      for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) y[i] = (float)__ddiv_rn((double)y[i], beta);
+    } else {
+      double* y = high_vec(I, j + 1);
+      for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) y[i] = __ddiv_rn(y[i], beta);
+    }
+  }
+}
+
+__global__ void b_advance(BatchArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *a.n_inst) return;
+  BInst& I = a.inst[s];
+  if (stepping(I)) I.j += 1;
+}
+
+// End of a graph launch: T-matrix analysis of every stepping instance and the
+// phase rules.  One thread per instance.
+__global__ void __launch_bounds__(32) b_check(BatchArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *a.n_inst) return;
+  BInst& I = a.inst[s];
+  if (I.phase != kPhLow && I.phase != kPhHigh) return;
+  const int m = I.j;  // alpha_0 .. alpha_{j-1} are final
+  if (m < 2) return;
+  const int cap = I.cap;
+  double* al = I.scratch;
+  double* be = al + cap;
+  double* work = be + cap;      // 5 cap + 2
+  double* z = work + 5 * cap + 2;  // cap
+  double* inv = z + cap;         // 6 cap
+  double amax = I.ab[0], bmax = I.ab[1];
+  for (int q = 0; q < m; ++q) {
+    al[q] = I.ab[2 * q];
+    be[q] = I.ab[2 * q + 1];
+    amax = tcore::dmax(amax, al[q]);
+    bmax = tcore::dmax(bmax, be[q]);
+  }
+  const int nev = I.nev;
+  double ev[AED_MAX_NEV + 1], er[AED_MAX_NEV + 1];
+  int first[AED_MAX_NEV + 1];
+  tcore::TResult res;
+  const int want = nev + 1;
+  const bool bad = tcore::analyze(m, al, be, amax, bmax, work, want, ev, er, nullptr, first, &res,
+                                  I.phase == kPhLow ? kFp32MergeRel : 0.0) != 0;
+  const int cnt = res.count;
+  bool conv = !bad && cnt >= nev;
+  if (I.phase == kPhLow) {
+    for (int i = 0; conv && i < nev; ++i)
+      if (!(er[i] <= tcore::dmax(I.tol32 * 1e-3, I.tol32 * fabs(ev[i])))) conv = false;
+    const bool full = !stepping(I);
+    if (!(conv || full || bad)) return;
+    // Ritz coefficients: sum of the unit eigenvectors of T(m) of the nev
+    // lowest distinct values
+    const int n1 = cnt < nev ? cnt : nev;
+    for (int q = 0; q < m; ++q) I.coef[q] = 0.0;
+    for (int i = 0; i < n1; ++i) {
+      tcore::inverse_iteration(m, al, be, ev[i], z, inv);
+      for (int q = 0; q < m; ++q) I.coef[q] += z[q];
+    }
+    if (n1 == 0) I.coef[0] = 1.0;
+    for (int i = 0; i < n1; ++i) I.evals_low[i] = ev[i];
+    I.m_low = m;
+    I.phase = kPhRitz;
+  } else {
+    if (m < nev + 2) conv = false;
+    bool ietl = conv;
+    for (int i = 0; ietl && i < nev; ++i)
+      if (er[i] > tcore::dmax(I.atol, I.rtol * fabs(ev[i]))) ietl = false;
+    bool energy = conv && I.etol > 0.0 && cnt >= nev + 1;
+    for (int i = 0; energy && i < nev; ++i) {
+      const double gap = ev[i + 1] - ev[i];
+      if (!(gap > 0.0) || !(er[i] * er[i] / gap <= I.etol * fabs(ev[i]))) energy = false;
+    }
+    const bool full = !stepping(I);
+    if (!(ietl || energy || full || bad)) return;
+    const int n = cnt < nev ? cnt : nev;
+    for (int i = 0; i < n; ++i) {
+      I.evals[i] = ev[i];
+      I.errs[i] = er[i];
+    }
+    I.n_evals = n;
+    I.iters = m;
+    I.converged = (ietl || energy) ? 1 : 0;
+    I.phase = kPhDone;
+  }
+}
+
+// FP64 start of the refinement: v = sum_q coef[q] v_q (stored FP32 basis),
+// chunk partials of |v|^2.
+__global__ void __launch_bounds__(kRedThreads) b_ritz(BatchArgs a) {
+  __shared__ double red[33];
+  __shared__ double cs[kStoreChunkB];
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRitz) continue;
+    const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+    double* out = I.v64[0];
+    double acc[kRedChunk / kRedThreads];
+#pragma unroll
+    for (int u = 0; u < kRedChunk / kRedThreads; ++u) acc[u] = 0.0;
+    for (int q0 = 0; q0 < I.m_low; q0 += kStoreChunkB) {
+      const int cnt = I.m_low - q0 < kStoreChunkB ? I.m_low - q0 : kStoreChunkB;
+      __syncthreads();
+      if (threadIdx.x < cnt) cs[threadIdx.x] = I.coef[q0 + threadIdx.x];
+      __syncthreads();
+      for (int q = 0; q < cnt; ++q) {
+        const float* v = low_vec(I, q0 + q);
+#pragma unroll
+        for (int u = 0; u < kRedChunk / kRedThreads; ++u) {
+          const int64_t i = e0 + threadIdx.x + u * kRedThreads;
+          if (i < e1) acc[u] = fma(cs[q], (double)v[i], acc[u]);
+        }
+      }
+    }
+    double sq = 0.0;
+#pragma unroll
+    for (int u = 0; u < kRedChunk / kRedThreads; ++u) {
+      const int64_t i = e0 + threadIdx.x + u * kRedThreads;
+      if (i < e1) {
+        out[i] = acc[u];
+        sq = fma(acc[u], acc[u], sq);
+      }
+    }
+    const double tot = block_sum_all<kRedThreads>(sq, red);
+    if (threadIdx.x == 0) I.partB[w.idx] = tot;
+  }
+}
+
+__global__ void __launch_bounds__(256) b_ritz_norm(BatchArgs a) {
+  __shared__ double red[33];
+  if ((int)blockIdx.x >= *a.n_inst) return;
+  BInst& I = a.inst[blockIdx.x];
+  if (I.phase != kPhRitz) return;
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < I.n_chunks; i += 256) v += I.partB[i];
+  const double tot = block_sum_all<256>(v, red);
+  if (threadIdx.x == 0) I.ritz_norm = sqrt(tot);
+}
+
+__global__ void __launch_bounds__(kRedThreads) b_ritz_scale(BatchArgs a) {
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRitz) continue;
+    const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+    double* v = I.v64[0];
+    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) v[i] = __ddiv_rn(v[i], I.ritz_norm);
+  }
+}
+
+__global__ void b_ritz_commit(BatchArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *a.n_inst) return;
+  BInst& I = a.inst[s];
+  if (I.phase != kPhRitz) return;
+  I.phase = kPhHigh;
+  I.j = 0;
+}
+
+int g_sms = 0;
+int sms() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+int hv_grid() {
+  static int g = 0;
+  if (!g) {
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, b_hv, kHvThreads, 0);
+    g = sms() * (per < 1 ? 1 : per);
+  }
+  return g;
+}
+
+int check(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(AED_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return AED_OK;
+}
+
+}  // namespace
+
+int batch_record_step(const BatchArgs& a, cudaStream_t st) {
+  const int ni = a.max_inst;
+  const int gchunk = sms() * 8;
+  b_hv<<<hv_grid(), kHvThreads, 0, st>>>(a);
+  b_alpha<<<ni, 256, 0, st>>>(a);
+  b_update<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_beta<<<ni, 256, 0, st>>>(a);
+  b_norm<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_advance<<<(ni + 127) / 128, 128, 0, st>>>(a);
+  return check("batched Lanczos step");
+}
+
+int batch_record_check(const BatchArgs& a, cudaStream_t st) {
+  const int ni = a.max_inst;
+  const int gchunk = sms() * 8;
+  b_check<<<(ni + 31) / 32, 32, 0, st>>>(a);
+  b_ritz<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_ritz_norm<<<ni, 256, 0, st>>>(a);
+  b_ritz_scale<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_ritz_commit<<<(ni + 127) / 128, 128, 0, st>>>(a);
+  return check("batched Lanczos check");
+}
+
+}  // namespace aed

@@ -1,0 +1,89 @@
+// batch.cuh -- device state of the batched / served Lanczos engine.
+//
+// Many independent Lanczos solves (one per request) advance together: every
+// step of the engine runs one Lanczos step for every resident instance, with
+// work queues of (instance, tile) and (instance, chunk) items, so instances of
+// very different dimension share the GPU without one kernel per instance.
+// A CUDA graph holds S such steps plus the convergence check and the hand-over
+// from the FP32 phase to the FP64 refinement; the host only admits and retires
+// requests between graph launches.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "aed_internal.h"
+#include "kernels.cuh"
+
+namespace aed {
+
+constexpr int kBatchMaxChunks = 64;  // FP32 basis store: chunks of kStoreChunkB vectors
+constexpr int kStoreChunkB = 16;
+
+// Instance phases
+enum : int32_t {
+  kPhIdle = 0,   // slot free
+  kPhLow = 1,    // FP32 Lanczos recurrence, basis kept in HBM
+  kPhRitz = 2,   // FP32 phase done: Ritz vectors being assembled into the FP64 start
+  kPhHigh = 3,   // FP64 Lanczos recurrence (refinement, or the whole solve in FP64 mode)
+  kPhDone = 4,   // results ready
+};
+
+struct BInst {
+  // set at admission
+  const HvParams* P;  // device copy of the coupling tables
+  DevTables t;        // sector tables (shared per sector), tiles, per-instance diagonal
+  int64_t D;
+  int32_t nev;
+  int32_t cap;        // alpha/beta capacity (steps) of each phase
+  int32_t n_store;    // FP32 basis capacity (vectors)
+  int32_t n_tiles;
+  int64_t n_chunks;   // reduction chunks (kRedChunk elements)
+  int64_t ldv;        // stride of stored FP32 vectors (elements)
+  double tol32;       // FP32 phase: residual estimate <= tol32 * |lambda|
+  double etol;        // FP64 phase: r^2 / gap <= etol * |lambda| (0: ietl rule only)
+  double rtol, atol;  // ietl rule
+  float* chunk[kBatchMaxChunks];
+  double* v64[3];     // FP64 vectors (rotating)
+  double* partA;      // n_tiles
+  double* partB;      // n_chunks
+  double* ab;         // 2 * cap: alpha_j, beta_j of the current phase
+  double* scratch;    // 12 * cap doubles for the T-matrix analysis
+  double* coef;       // cap: Ritz coefficients
+  // dynamic
+  int32_t phase;
+  int32_t j;          // index of the newest Lanczos vector of the current phase
+  int32_t m_low;      // FP32 phase length (T size) when it ended
+  int32_t n_evals;
+  int32_t iters;      // FP64 phase T size at the end
+  int32_t converged;
+  double ritz_norm;
+  double evals[AED_MAX_NEV];
+  double errs[AED_MAX_NEV];
+  double evals_low[AED_MAX_NEV];
+};
+
+struct BItem {
+  int32_t inst;
+  int32_t idx;  // tile or chunk index within the instance
+};
+
+// Kernels of one engine step and of the end-of-graph phase logic.  All take
+// the instance table, the item lists and their counts from device memory, so
+// a captured graph stays valid while the host changes them between launches.
+struct BatchArgs {
+  BInst* inst;
+  int32_t* n_inst;     // number of slots in use (device)
+  BItem* tiles;
+  int32_t* n_tiles;
+  BItem* chunks;
+  int32_t* n_chunks;
+  int max_inst;
+};
+
+int batch_record_step(const BatchArgs& a, cudaStream_t st);
+int batch_record_check(const BatchArgs& a, cudaStream_t st);
+int batch_max_inst_grid();
+
+}  // namespace aed

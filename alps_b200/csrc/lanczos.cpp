@@ -229,7 +229,7 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters,
     rc = R.wait_step(m - 1);
     if (rc) return rc;
     if (m > 1) {
-      rc = tmatrix_analyze(m, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T);
+      rc = tmatrix_analyze(m, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, R.f32 ? kFp32MergeRel : 0.0);
       if (rc) return rc;
       if (stop.done(T, m)) break;
     }
@@ -240,7 +240,7 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters,
     ++m;
   }
   if (m == 1) {
-    rc = tmatrix_analyze(1, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T);
+    rc = tmatrix_analyze(1, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, R.f32 ? kFp32MergeRel : 0.0);
     if (rc) return rc;
   }
   AED_CUDA_TRY(cudaStreamSynchronize(R.h->stream));

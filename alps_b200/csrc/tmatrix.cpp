@@ -102,14 +102,14 @@ int tridiag_eigen(int n, double* d, double* e, double* zlast, double* zfull) {
 }
 
 int tmatrix_analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
-                    TmatInfo& out) {
+                    TmatInfo& out, double thold_rel) {
   out = TmatInfo();
   if (n < 1) return AED_OK;
   std::vector<double> scratch(5 * (size_t)n + 2), ev(n), er(n);
   std::vector<int> mu(n), fi(n);
   tcore::TResult res;
   if (tcore::analyze(n, alpha, beta, alpha_max, beta_max, scratch.data(), n, ev.data(), er.data(), mu.data(),
-                     fi.data(), &res))
+                     fi.data(), &res, thold_rel))
     return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
   out.thold = res.thold;
   out.multol = res.multol;

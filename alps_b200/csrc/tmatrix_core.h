@@ -121,10 +121,13 @@ struct TResult {
 // Tmatrix::compute(true) on alpha[0..n), beta[0..n) (beta[n-1] = beta_{m+1}).
 // Writes up to `cap` distinct non-ghost eigenvalues (ascending) with their
 // error estimates, multiplicities and first index in the sorted spectrum.
-// scratch: 5*n + 2 doubles.  Returns 0 or the eigensolver's failure code.
+// scratch: 5*n + 2 doubles.  thold_rel > 0 raises the merge threshold to
+// thold_rel * max|eigenvalue| (recurrences run with FP32 vectors, whose copies
+// of a converged eigenvalue differ by FP32 rounding, far above the FP64
+// threshold).  Returns 0 or the eigensolver's failure code.
 AED_HD inline int analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
                           double* scratch, int cap, double* evals, double* errs, int* mults, int* first,
-                          TResult* res) {
+                          TResult* res, double thold_rel = 0.0) {
   res->count = 0;
   res->thold = res->multol = 0.0;
   if (n < 1) return 0;
@@ -141,7 +144,8 @@ AED_HD inline int analyze(int n, const double* alpha, const double* beta, double
   const double eps = DBL_EPSILON;
   const double error_tol = pow(eps, 2.0 / 3.0);  // tmatrix.h:32
   const double multol = dmax(alpha_max, beta_max) * 2 * eps * (10000 + n);
-  const double thold = dmax(error_tol * dmax(ev[0], ev[n - 1]), 5 * multol);
+  double thold = dmax(error_tol * dmax(ev[0], ev[n - 1]), 5 * multol);
+  if (thold_rel > 0.0) thold = dmax(thold, thold_rel * dmax(fabs(ev[0]), fabs(ev[n - 1])));
   res->thold = thold;
   res->multol = multol;
   const double bl = beta[n - 1];

@@ -348,6 +348,215 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def ladder_bonds(L, jl, jr):
+    """ladder lattice (anisotropic2d cell, periodic legs, open rungs) in ALPS order; site = 2x + y."""
+    out = []
+    for x in range(L):
+        for y in range(2):
+            s = 2 * x + y
+            out.append((s, 2 * ((x + 1) % L) + y, float(jl), float(jl), 0.0))
+            if y == 0:
+                out.append((s, s + 1, float(jr), float(jr), 0.0))
+    return out
+
+
+def square_bonds(Lx, Wy, seed):
+    """square lattice (simple2d cell, periodic) in ALPS order, per-bond J ~ U[0.8, 1.2]."""
+    raw = []
+    for x in range(Lx):
+        for y in range(Wy):
+            s = x * Wy + y
+            raw.append((s, x * Wy + (y + 1) % Wy))
+            raw.append((s, ((x + 1) % Lx) * Wy + y))
+    js = np.random.default_rng(seed).uniform(0.8, 1.2, len(raw))
+    return [(a, b, float(j), float(j), 0.0) for (a, b), j in zip(raw, js)]
+
+
+def batch_requests():
+    """Config 4: 512 J1-J2 chains, L uniform over {12,...,22} even, J2 ~ U[0,1], seed 5124, 2 eigenvalues."""
+    rng = np.random.default_rng(5124)
+    Ls = rng.choice([12, 14, 16, 18, 20, 22], size=512)
+    j2 = rng.uniform(0.0, 1.0, size=512)
+    return [(int(L), chain_bonds(int(L), j), 2, k) for k, (L, j) in enumerate(zip(Ls, j2))]
+
+
+def serve_requests(n):
+    """Config 5: Poisson arrivals at 200/s (seed 2000); chain L in {14..26} even or ladder 2x{7..12},
+    J_leg, J_rung ~ U[0.5, 1.5], k ~ U{1..4}."""
+    rng = np.random.default_rng(2000)
+    arr = np.cumsum(rng.exponential(1.0 / 200.0, n))
+    out = []
+    for k in range(n):
+        jl, jr = rng.uniform(0.5, 1.5, 2)
+        nev = int(rng.integers(1, 5))
+        if rng.random() < 0.5:
+            L = int(rng.choice(np.arange(14, 27, 2)))
+            out.append((float(arr[k]), L, chain_bonds_jl(L, jl), nev, k))
+        else:
+            L = int(rng.integers(7, 13))
+            out.append((float(arr[k]), 2 * L, ladder_bonds(L, jl, jr), nev, k))
+    return out
+
+
+def chain_bonds_jl(L, jl):
+    return [(i, (i + 1) % L, float(jl), float(jl), 0.0) for i in range(L)]
+
+
+def cpu_solve_estimate(N, bonds, nev, iterations, rows=200_000):
+    """Seconds of the reference-algorithm restatement for one solve on one core: a full
+    oracle solve when the sector is small, else a bounded row sample scaled to the sector."""
+    import oracle
+
+    D = comb(N, N // 2)
+    if D <= 60000:
+        t0 = time.perf_counter()
+        M = oracle.Matrix(N, N // 2, bonds)
+        M.lanczos(nev=nev, seed=1)
+        return time.perf_counter() - t0, "full"
+    states = oracle.basis_fast(N, N // 2)
+    r = min(rows, D)
+    tb, tp, tv = oracle.sample_times(N, states, bonds, 0, r)
+    return (tb + iterations * (tp + tv)) * D / r, f"sample {r} rows"
+
+
+def run_square(args):
+    """Config 3: 6x5 square lattice, per-bond J ~ U[0.8,1.2] (seed 3005): mixed vs plain FP64."""
+    import alps_b200 as ed
+
+    bonds = square_bonds(6, 5, 3005)
+    out = {}
+    for name, prec in (("fp64", ed.FP64), ("mixed", ed.FP32)):
+        ham = ed.Hamiltonian(30, 15, bonds, precision=prec)
+        t0 = time.perf_counter()
+        r = ham.solve(nev=1, seed=1, profile=True)
+        out[name] = {"seconds": time.perf_counter() - t0, "evals": r["evals"].tolist(), "iterations": r["iterations"],
+                     "iterations_low": r["iterations_low"], "apply_ms": r["apply_ms"]}
+        ham.close()
+    D = 155117520
+    nbar = 60 * 2 * comb(28, 14) / D
+    rel = abs(out["mixed"]["evals"][0] - out["fp64"]["evals"][0]) / abs(out["fp64"]["evals"][0])
+    peak, _ = read_peaks()
+    g64 = D * ((1 + nbar) * 8 + 8) / (out["fp64"]["apply_ms"] / 1e3) / 1e9
+    g32 = D * ((1 + nbar) * 4 + 4) / (out["mixed"]["apply_ms"] / 1e3) / 1e9
+    line = {"metric": "6x5 square lattice ground state: solves/s, mixed vs FP64", "value": 1.0 / out["mixed"]["seconds"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "square lattice 6x5 periodic, Sz=0, D=155117520, J_b~U[0.8,1.2] seed 3005, k=1"},
+            "fp64": out["fp64"], "mixed": out["mixed"], "speedup_mixed_vs_fp64": out["fp64"]["seconds"] / out["mixed"]["seconds"],
+            "rel_energy_err_mixed_vs_fp64": rel,
+            "hv_gbs": {"fp64": g64, "fp32": g32, "peak": peak, "frac_fp32": g32 / peak, "frac_fp64": g64 / peak}}
+    print(json.dumps(line))
+
+
+def run_batch(args):
+    """Config 4: 512 J1-J2 chains through the batched engine, mixed and FP64, and through the
+    single-instance FP64 drop-in one after the other."""
+    import alps_b200 as ed
+
+    reqs = batch_requests()
+    res = {}
+    for name, prec in (("mixed", ed.FP32), ("fp64", ed.FP64)):
+        srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch)
+        w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs[:8]]  # warm-up
+        srv.run(w)
+        t0 = time.perf_counter()
+        tickets = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+        out = srv.run(tickets)
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        res[name] = {"seconds": dt, "solves_per_s": len(reqs) / dt, "graph_launches": st["graph_launches"],
+                     "evals": [out[t]["evals"].tolist() for t in tickets],
+                     "converged": all(out[t]["converged"] for t in tickets)}
+    # the drop-in single-instance FP64 path, instance after instance
+    t0 = time.perf_counter()
+    single = []
+    hams = {}
+    for n, b, nev, sd in reqs:
+        h = hams.get(n)
+        if h is None:
+            h = hams[n] = ed.Hamiltonian(n, n // 2, b, precision=ed.FP64)
+        else:
+            h.set_couplings(b)
+        single.append(h.solve(nev=nev, seed=sd)["evals"].tolist())
+    t_single = time.perf_counter() - t0
+    for h in hams.values():
+        h.close()
+    rel = max(abs(a - c) / abs(c) for ea, ec in zip(res["mixed"]["evals"], single) for a, c in zip(ea, ec))
+    rel64 = max(abs(a - c) / abs(c) for ea, ec in zip(res["fp64"]["evals"], single) for a, c in zip(ea, ec))
+    line = {"metric": "batched Lanczos solves/s (512 J1-J2 chains, L 12..22), mixed vs plain FP64",
+            "value": res["mixed"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "512 J1-J2 chains, L~U{12..22} even, J2~U[0,1] seed 5124, Sz=0, k=2",
+                       "steps_per_graph": args.steps_per_launch},
+            "mixed_batched": {k: v for k, v in res["mixed"].items() if k != "evals"},
+            "fp64_batched": {k: v for k, v in res["fp64"].items() if k != "evals"},
+            "fp64_single_instance": {"seconds": t_single, "solves_per_s": len(reqs) / t_single},
+            "speedup_mixed_batched_vs_fp64_single": res["mixed"]["solves_per_s"] / (len(reqs) / t_single),
+            "speedup_mixed_batched_vs_fp64_batched": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
+            "max_rel_energy_err_mixed_vs_fp64": rel, "max_rel_energy_err_fp64_batched_vs_single": rel64}
+    if not args.no_cpu:
+        classes = {}
+        for n, b, nev, sd in reqs:
+            classes.setdefault(n, (b, nev))
+        tot, notes = 0.0, {}
+        counts = {}
+        for n, b, nev, sd in reqs:
+            counts[n] = counts.get(n, 0) + 1
+        for n, (b, nev) in sorted(classes.items()):
+            t, how = cpu_solve_estimate(n, b, nev, 120)
+            tot += t * counts[n]
+            notes[n] = f"{t:.3g} s ({how})"
+        line["cpu_baseline"] = {"value": len(reqs) / tot, "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": "one instance per chain length, explicit-matrix Lanczos on one core "
+                                          "(row sample x 120 iterations above 60000 states): " + json.dumps(notes)}
+    print(json.dumps(line))
+
+
+def run_serve(args):
+    """Config 5: Poisson stream of requests at 200/s through the served engine; latency from the
+    scheduled arrival to the harvest of the result."""
+    import alps_b200 as ed
+
+    reqs = serve_requests(args.requests)
+    prec = ed.FP32 if args.precision == "mixed" else ed.FP64
+    srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch)
+    w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for _, n, b, nev, sd in reqs[:16]]
+    srv.run(w)
+    pending = {}
+    lat = []
+    i = 0
+    t0 = time.perf_counter()
+    while i < len(reqs) or pending:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i][0] <= now:
+            arr, n, b, nev, sd = reqs[i]
+            pending[srv.submit(n, n // 2, b, nev=nev, seed=sd)] = arr
+            i += 1
+        if pending:
+            srv.step()
+            done_t = time.perf_counter() - t0
+            for t in list(pending):
+                r = srv.poll(t)
+                if r is not None:
+                    lat.append(done_t - pending.pop(t))
+        elif i < len(reqs):
+            time.sleep(max(0.0, min(0.002, reqs[i][0] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat)
+    line = {"metric": "served Lanczos: solves/s and latency (Poisson 200 req/s)", "value": len(reqs) / wall,
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64" if prec == ed.FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{len(reqs)} requests, Poisson 200/s seed 2000, chain L 14..26 or ladder 2x7..2x12, "
+                                   "J_leg,J_rung~U[0.5,1.5], k~U{1..4}", "precision": args.precision,
+                       "steps_per_graph": args.steps_per_launch},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "mean": float(lat.mean()), "max": float(lat.max())},
+            "offered_rate": 200.0, "graph_launches": st["graph_launches"], "wall_s": wall}
+    print(json.dumps(line))
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -386,11 +595,21 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="l28", choices=["l28", "square", "batch", "serve"])
+    ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="serve: engine precision")
+    ap.add_argument("--steps-per-launch", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "square":
+        run_square(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

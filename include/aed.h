@@ -199,6 +199,51 @@ int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap,
  * events; *ms = mean milliseconds per apply. */
 int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms);
 
+/* ---- batched / served solves ------------------------------------------------
+ * Many independent requests (a model and solve options each) advance together
+ * on one GPU: every engine step runs one Lanczos step of every resident
+ * request over work queues of (request, tile) and (request, chunk) items, and
+ * a CUDA graph holds S steps plus the convergence check.  Requests are
+ * admitted in arrival order while their HBM footprint fits the server's
+ * budget, and join the running batch at the next step (continuous batching).
+ * The analogue of the reference's task farm over independent parameter sets
+ * (src/alps/scheduler/mpp_scheduler.C:50) on one GPU.  AED_FP32 servers run
+ * the mixed path (FP32 Lanczos basis, FP64 refinement to r^2/gap <= 1e-11
+ * |lambda|); AED_FP64 servers the plain FP64 recurrence with the ietl rule,
+ * checked every S steps (results come from T at the first check after
+ * convergence).  A request's result does not depend on the other requests in
+ * the batch. */
+typedef struct aed_server aed_server;
+
+typedef struct {
+  int32_t device;
+  int32_t max_slots;         /* resident requests at most (default 512)                */
+  int32_t steps_per_launch;  /* S, Lanczos steps per graph launch (default 8)          */
+  int32_t precision;         /* AED_FP32 (mixed) or AED_FP64                           */
+  double hbm_fraction;       /* budget as a fraction of free memory (default 0.8)      */
+  int64_t hbm_budget_bytes;  /* explicit budget in bytes (overrides hbm_fraction)      */
+} aed_server_opts;
+
+typedef struct {
+  int32_t resident, queued;
+  int64_t bytes_used, bytes_budget;
+  int64_t graph_launches;
+} aed_server_stats;
+
+int aed_server_create(const aed_server_opts* opts, aed_server** out);
+int aed_server_destroy(aed_server* s);
+/* Queue a request.  AED_ERR_ADMISSION if its footprint alone exceeds the budget.
+ * opts->start is ignored (start vectors are drawn from opts->seed). */
+int aed_server_submit(aed_server* s, const aed_model_desc* model, const aed_solve_opts* opts, int64_t* ticket);
+/* Admit what fits, run one graph launch (S engine steps + check), harvest
+ * finished requests.  *n_pending = resident + queued requests afterwards. */
+int aed_server_step(aed_server* s, int32_t* n_pending);
+/* AED_PENDING while running; AED_OK with *out filled (out->seconds = latency
+ * from submission to completion) once, after which the ticket is forgotten. */
+int aed_server_poll(aed_server* s, int64_t ticket, aed_solve_result* out);
+int aed_server_cancel(aed_server* s, int64_t ticket);
+int aed_server_get_stats(aed_server* s, aed_server_stats* out);
+
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own
  * work or record timing events on it.  Engine addition, no reference counterpart. */
 int aed_get_stream(aed_handle* h, void** stream);

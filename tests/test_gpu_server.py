@@ -1,0 +1,136 @@
+"""The batched / served engine (aed_server_*): parity with single solves, batch
+independence, admission by HBM footprint, continuous batching (needs a B200)."""
+
+import numpy as np
+import pytest
+
+import alps_b200 as ed
+
+pytestmark = pytest.mark.gpu
+
+
+def j1j2(L, j2):
+    out = []
+    for i in range(L):
+        out.append((i, (i + 1) % L, 1.0, 1.0))
+        out.append((i, (i + 2) % L, float(j2), float(j2)))
+    return out
+
+
+def ladder(L, jl, jr):
+    # anisotropic2d cell order: leg (x,y)->(x+1,y) type 0, rung (x,0)->(x,1) type 1; site = 2x + y
+    out = []
+    for x in range(L):
+        for y in range(2):
+            s = 2 * x + y
+            out.append((s, 2 * ((x + 1) % L) + y, jl, jl))
+            if y == 0:
+                out.append((s, s + 1, jr, jr))
+    return out
+
+
+def reference(n, bonds, nev):
+    ham = ed.Hamiltonian(n, n // 2, bonds)
+    r = ham.solve(nev=nev, seed=3)
+    ham.close()
+    return r["evals"]
+
+
+def mixed_requests(seed, count):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(count):
+        if rng.random() < 0.6:
+            L = int(rng.choice([10, 12, 14, 16, 18]))
+            reqs.append((L, j1j2(L, rng.uniform(0, 1)), int(rng.integers(1, 4)), int(rng.integers(0, 1 << 30))))
+        else:
+            L = int(rng.choice([5, 6, 7, 8]))
+            reqs.append((2 * L, ladder(L, rng.uniform(0.5, 1.5), rng.uniform(0.5, 1.5)), int(rng.integers(1, 4)),
+                         int(rng.integers(0, 1 << 30))))
+    return reqs
+
+
+@pytest.mark.parametrize("prec,tol", [(ed.FP32, 1e-9), (ed.FP64, 1e-11)])
+def test_batch_matches_single_solves(prec, tol):
+    reqs = mixed_requests(5124, 24)
+    srv = ed.Server(precision=prec, max_slots=64, steps=8)
+    tickets = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+    res = srv.run(tickets)
+    for t, (n, b, nev, sd) in zip(tickets, reqs):
+        r = res[t]
+        ref = reference(n, b, nev)
+        assert r["converged"]
+        assert len(r["evals"]) == len(ref)
+        rel = np.abs(r["evals"] - ref) / np.abs(ref)
+        assert np.all(rel <= tol), (n, nev, rel)
+        if prec == ed.FP32:
+            assert r["iterations_low"] > 0
+    srv.close()
+
+
+@pytest.mark.parametrize("prec", [ed.FP32, ed.FP64])
+def test_result_is_the_same_alone_and_in_the_mix(prec):
+    probe = (16, j1j2(16, 0.37), 2, 77)
+    alone = ed.Server(precision=prec, max_slots=8, steps=4)
+    t = alone.submit(16, 8, probe[1], nev=2, seed=77)
+    r_alone = alone.run([t])[t]
+    alone.close()
+    srv = ed.Server(precision=prec, max_slots=32, steps=4)
+    others = mixed_requests(99, 12)
+    ts = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in others[:6]]
+    srv.step()  # the probe arrives while others are resident
+    tp = srv.submit(16, 8, probe[1], nev=2, seed=77)
+    srv.step()
+    ts += [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in others[6:]]
+    res = srv.run(ts + [tp])
+    r_mix = res[tp]
+    assert np.array_equal(r_mix["evals"], r_alone["evals"])
+    assert r_mix["iterations"] == r_alone["iterations"]
+    srv.close()
+
+
+def test_admission_by_hbm_footprint_queues_and_refuses():
+    rng = np.random.default_rng(7)
+    reqs = [(18, j1j2(18, rng.uniform(0, 1)), 1, k) for k in range(10)]
+    budget = 64 << 20  # an L=18 request holds ~30 MB: two resident at a time
+    srv = ed.Server(precision=ed.FP32, max_slots=64, hbm_budget=budget)
+    tickets = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+    srv.step()
+    st = srv.stats()
+    assert st["bytes_used"] <= budget
+    assert st["queued"] > 0 and st["resident"] >= 1
+    res = srv.run(tickets)
+    assert len(res) == len(tickets)
+    with pytest.raises(ed.AEDError) as e:
+        srv.submit(24, 12, j1j2(24, 0.2), nev=1)
+    assert e.value.code == ed.ERR_ADMISSION
+    srv.close()
+
+
+def test_cancel_and_continuous_batching():
+    srv = ed.Server(precision=ed.FP32, max_slots=16, steps=2)
+    a = srv.submit(18, 9, j1j2(18, 0.3), nev=1, seed=1)
+    c = srv.submit(14, 7, j1j2(14, 0.6), nev=1, seed=2)
+    srv.cancel(c)
+    srv.step()
+    b = srv.submit(12, 6, j1j2(12, 0.8), nev=1, seed=3)  # joins while a is resident
+    overlap = False
+    done = {}
+    for _ in range(2000):
+        srv.step()
+        st = srv.stats()
+        if st["resident"] >= 2:
+            overlap = True
+        for t in (a, b):
+            if t not in done:
+                r = srv.poll(t)
+                if r is not None:
+                    done[t] = r
+        if len(done) == 2:
+            break
+    assert overlap and len(done) == 2
+    with pytest.raises(ed.AEDError) as e:
+        srv.poll(c)
+    assert e.value.code == ed.ERR_CANCELLED
+    assert done[b]["seconds"] > 0
+    srv.close()
