@@ -62,6 +62,10 @@ struct HvParams {
   PairTerm low[kMaxBonds];
   PairTerm rise[kMaxBonds];
   DiagTerm diag[kMaxDiag];
+  // flips with both bits in the lo part, in the order of low[]: their
+  // coefficients, indexed by the lo-neighbour table
+  int n_lolo;
+  double lolo_c[kMaxBonds];
 };
 
 int build_hv_params(const Model& m, int Nlo, HvParams& P);
@@ -78,6 +82,14 @@ struct BasisTables {
 };
 
 int build_tables(int N, int n_up, BasisTables& t);
+
+// Lo-neighbour table: for every lo state l (rank r within its popcount class
+// k), the flips with both bits in the lo part that apply to l, as
+// (target rank r' = tlo[l ^ flip]) | (flip index << 16), sorted by r' and
+// padded with kEllPad to a common width W.  Entry e of row r of class k sits
+// at W * looff[k] + e * C(Nlo, k) + r (coalesced across consecutive rows).
+constexpr uint32_t kEllPad = 0xffffffffu;
+void build_lo_table(const BasisTables& t, const HvParams& P, std::vector<uint32_t>& ell, int* width);
 
 // Work tiles over the sector: (hi block h, first row r0 within the block).
 void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr);

@@ -37,12 +37,34 @@ void release(aed_handle* h) {
   cudaFree(h->d_tile_h);
   cudaFree(h->d_tile_r);
   cudaFree(h->d_dg);
+  cudaFree(h->d_ell);
   cudaFree(h->d_partA);
   cudaFree(h->d_partB);
   cudaFree(h->d_scal);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+// (Re)build the lo-neighbour table of the handle's couplings on the device.
+int upload_lo_table(aed_handle* h) {
+  std::vector<uint32_t> ell;
+  int W = 0;
+  build_lo_table(h->tab, h->P, ell, &W);
+  if (h->d_ell) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_ell);
+    h->d_ell = nullptr;
+  }
+  int rc = dev_alloc(&h->d_ell, ell.size() + 1);
+  if (rc) return rc;
+  if (!ell.empty()) {
+    AED_CUDA_TRY(cudaMemcpyAsync(h->d_ell, ell.data(), ell.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // host vector goes out of scope
+  }
+  h->dt.ell = h->d_ell;
+  h->dt.ell_w = W;
+  return AED_OK;
 }
 
 int check_vec(const aed_handle* h, const void* p, const char* name) {
@@ -169,17 +191,20 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
   int best = 0;
   float best_ms = 1e30f;
   int rc = AED_OK;
+  // as solves run them: with the per-tile <x,y> partials; best of three
   for (int v = 0; v < hv_num_variants() && !rc; ++v) {
-    rc = launch_variant(h, f32, v, x, y, nullptr);  // warm-up
-    cudaEventRecord(e0, h->stream);
-    for (int r = 0; r < 2 && !rc; ++r) rc = launch_variant(h, f32, v, x, y, nullptr);
-    cudaEventRecord(e1, h->stream);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = v;
+    rc = launch_variant(h, f32, v, x, y, h->d_partA);  // warm-up
+    for (int r = 0; r < 3 && !rc; ++r) {
+      cudaEventRecord(e0, h->stream);
+      rc = launch_variant(h, f32, v, x, y, h->d_partA);
+      cudaEventRecord(e1, h->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -307,6 +332,10 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   t.Nhi = h->tab.Nhi;
   t.n_up = h->tab.n_up;
   t.dg = h->d_dg;
+  if ((rc = upload_lo_table(h))) {
+    release(h);
+    return rc;
+  }
   rc = launch_diag_table(h->P, t, h->d_dg, h->stream);
   const cudaError_t e2 = rc ? cudaSuccess : cudaStreamSynchronize(h->stream);
   if (rc || e2 != cudaSuccess) {
@@ -330,6 +359,7 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // no apply of the old couplings in flight
   h->model = m;
   h->P = P;
+  if ((rc = upload_lo_table(h))) return rc;
   rc = launch_diag_table(h->P, h->dt, h->d_dg, h->stream);
   if (rc) return rc;
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));

@@ -106,7 +106,7 @@ __device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32
     if (q < np) {
       const SPair e = list[q];
       const uint32_t fhi = e.flip >> Nlo, chi = e.cond >> Nlo;
-      if ((h & fhi) == chi) {
+      if (fhi != 0u && (h & fhi) == chi) {  // lo-part flips come from the lo-neighbour table
         emit = true;
         op = {(e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e.c};
       }
@@ -133,9 +133,8 @@ __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h
       if (flo == 0u) {  // hi part only: applies to the whole tile iff the two bits differ
         emit = __popc(hb) == 1;
         op = {0u, __ldg(thi + (h ^ fhi)), e.c};
-      } else if (fhi == 0u) {  // lo part only
-        emit = true;
-        op = {flo | (kXorCond << 16), __ldg(thi + h), e.c};
+      } else if (fhi == 0u) {  // lo part only: from the lo-neighbour table
+        emit = false;
       } else {  // crossing: the lo bit must differ from the hi bit
         emit = true;
         op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
@@ -190,7 +189,8 @@ struct ApplySmem {
   SPair low[kMaxBonds];
   SPair rise[kMaxBonds];
   TileOp prog[kMaxOps];
-  int nops;
+  double lolo_c[kMaxBonds];
+  int nlow, nops;
   double red[33];
 };
 
@@ -204,6 +204,41 @@ __device__ __forceinline__ void stage_pairs(const HvParams& P, ApplySmem& sm) {
     const PairTerm a = P.low[q], b = P.rise[q];
     sm.low[q] = {a.mhi | a.mlo, a.mhi, a.c};
     sm.rise[q] = {b.mhi | b.mlo, b.mlo, b.c};
+  }
+  for (int q = threadIdx.x; q < P.n_lolo; q += kHvThreads) sm.lolo_c[q] = P.lolo_c[q];
+}
+
+// Flips inside the lo part, from the lo-neighbour table: entry e of the R rows
+// of this thread.  All targets lie in the thread's own hi block (base).  With
+// kOrdered the entries come in ascending target rank, so the diagonal is
+// added just before the first target above the row (the explicit matrix's
+// column order); `dd` records that it was added.
+template <typename T, typename Acc, int R, bool kOrdered>
+__device__ __forceinline__ void run_lo_table(const DevTables& t, uint32_t lbase, uint32_t nk, uint32_t base,
+                                             uint32_t rt, uint32_t nrow, const double* lolo_c,
+                                             const T* __restrict__ x, Acc* acc, bool* dd) {
+  const uint32_t* E = t.ell + (size_t)t.ell_w * lbase;
+  for (int e = 0; e < t.ell_w; ++e) {
+    uint32_t ent[R];
+    bool any = false;
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      ent[u] = (uint32_t)u < nrow ? __ldg(E + (size_t)e * nk + rt + u * kHvThreads) : kEllPad;
+      any |= ent[u] != kEllPad;
+    }
+    if (!__any_sync(0xffffffffu, any)) break;  // rows are padded at the end: nothing left in this warp
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      if (ent[u] != kEllPad) {
+        const uint32_t rp = ent[u] & 0xffffu;
+        if (kOrdered && !dd[u] && rp > rt + u * kHvThreads) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          acc[u].add(__ldg(t.dg + i), __ldg(x + i));
+          dd[u] = true;
+        }
+        acc[u].add(lolo_c[ent[u] >> 16], __ldg(x + base + rp));
+      }
+    }
   }
 }
 
@@ -224,19 +259,21 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
   const uint32_t base = __ldg(t.thi + h);
   __syncthreads();  // tables staged; previous tile done with prog
   if (threadIdx.x < 32) {
-    int cnt;
+    int nl, cnt;
     if (kOrdered) {
-      const int nl = compile_ordered(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
-      if (threadIdx.x == 0) sm.prog[nl].mc = kDiagOp;
-      cnt = compile_ordered(sm.rise, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, nl + 1);
+      nl = compile_ordered(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
+      cnt = compile_ordered(sm.rise, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, nl);
     } else {
-      if (threadIdx.x == 0) sm.prog[0].mc = kDiagOp;
-      cnt = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 1);
+      nl = 0;
+      cnt = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
     }
-    if (threadIdx.x == 0) sm.nops = cnt;
+    if (threadIdx.x == 0) {
+      sm.nlow = nl;
+      sm.nops = cnt;
+    }
   }
   __syncthreads();
-  const int nops = sm.nops;
+  const int nlow = sm.nlow, nops = sm.nops;
   double dotacc = 0.0;
 #pragma unroll 1
   for (int pass = 0; pass < kPasses; ++pass) {
@@ -251,7 +288,31 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
       lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
     }
     Acc acc[R];
-    run_ops<T, Acc, R>(sm.prog, 0, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+    bool dd[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) dd[u] = false;
+    if (kOrdered) {
+      // flips to smaller states outside the lo part, then the lo-part flips
+      // with the diagonal at its column, then the larger states outside
+      run_ops<T, Acc, R>(sm.prog, 0, nlow, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+      run_lo_table<T, Acc, R, true>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc, dd);
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow && !dd[u]) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          acc[u].add(__ldg(t.dg + i), __ldg(x + i));
+        }
+      run_ops<T, Acc, R>(sm.prog, nlow, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+    } else {
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if ((uint32_t)u < nrow) {
+          const uint32_t i = base + rt + u * kHvThreads;
+          acc[u].add(__ldg(t.dg + i), __ldg(x + i));
+        }
+      run_ops<T, Acc, R>(sm.prog, 0, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+      run_lo_table<T, Acc, R, false>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc, dd);
+    }
 #pragma unroll
     for (int u = 0; u < R; ++u) {
       if ((uint32_t)u < nrow) {

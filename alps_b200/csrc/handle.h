@@ -24,6 +24,7 @@ struct aed_handle {
   uint32_t* d_tile_h = nullptr;
   uint32_t* d_tile_r = nullptr;
   double* d_dg = nullptr;     // per-row diagonal
+  uint32_t* d_ell = nullptr;  // lo-neighbour table
   double* d_partA = nullptr;  // per-tile partial sums (n_tiles)
   double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
   double* d_scal = nullptr;   // 8 device scalars

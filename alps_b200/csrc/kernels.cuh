@@ -18,6 +18,8 @@ struct DevTables {
   const uint32_t* tile_h;  // n_tiles
   const uint32_t* tile_r;  // n_tiles
   const double* dg;        // D: diagonal M(i,i) of every row
+  const uint32_t* ell;     // lo-neighbour table (build_lo_table), ell_w entries per lo state
+  int ell_w;
   int64_t n_tiles;
   int64_t D;
   int Nlo, Nhi, n_up;

@@ -132,7 +132,44 @@ int build_hv_params(const Model& m, int Nlo, HvParams& P) {
     P.low[i] = low[i];
     P.rise[i] = rise[i];
   }
+  P.n_lolo = 0;
+  for (int i = 0; i < P.n_pairs; ++i)
+    if ((P.low[i].mhi >> Nlo) == 0u) P.lolo_c[P.n_lolo++] = P.low[i].c;
   return AED_OK;
+}
+
+void build_lo_table(const BasisTables& t, const HvParams& P, std::vector<uint32_t>& ell, int* width) {
+  std::vector<uint32_t> flips;
+  for (int i = 0; i < P.n_pairs; ++i)
+    if ((P.low[i].mhi >> t.Nlo) == 0u) flips.push_back(P.low[i].mhi | P.low[i].mlo);
+  const uint32_t nlo = 1u << t.Nlo;
+  // width: most flips applying to one lo state
+  int W = 0;
+  for (uint32_t l = 0; l < nlo; ++l) {
+    int c = 0;
+    for (uint32_t f : flips) {
+      const uint32_t b = l & f;
+      c += (b != 0u && b != f) ? 1 : 0;
+    }
+    W = std::max(W, c);
+  }
+  *width = W;
+  ell.assign((size_t)W * nlo, kEllPad);
+  std::vector<std::pair<uint32_t, uint32_t>> row;
+  for (int k = 0; k <= t.Nlo; ++k) {
+    const uint32_t base = t.looff[k], nk = t.looff[k + 1] - t.looff[k];
+    for (uint32_t r = 0; r < nk; ++r) {
+      const uint32_t l = t.lolist[base + r];
+      row.clear();
+      for (uint32_t q = 0; q < flips.size(); ++q) {
+        const uint32_t b = l & flips[q];
+        if (b != 0u && b != flips[q]) row.push_back({(uint32_t)t.tlo[l ^ flips[q]], q});
+      }
+      std::sort(row.begin(), row.end());
+      for (size_t e = 0; e < row.size(); ++e)
+        ell[(size_t)W * base + e * nk + r] = row[e].first | (row[e].second << 16);
+    }
+  }
 }
 
 // ---- basis tables (Lin 1990 two-table ranking) -----------------------------------

@@ -108,7 +108,7 @@ int dmalloc(aed_server* s, void** p, size_t bytes) {
 }
 
 // Bytes a request holds while resident (the admission footprint).
-size_t request_bytes(const aed_server* s, int64_t D, int nev, int cap, int n_store) {
+size_t request_bytes(const aed_server* s, int N, int64_t D, int nev, int cap, int n_store) {
   const size_t ldv = ((size_t)D * 4 + 255) & ~(size_t)255;
   size_t b = (size_t)D * 8;                      // diagonal
   b += 3 * (((size_t)D * 8 + 255) & ~(size_t)255);  // FP64 vectors
@@ -116,6 +116,7 @@ size_t request_bytes(const aed_server* s, int64_t D, int nev, int cap, int n_sto
   b += (size_t)sector_tiles_est(D) * 8 + (size_t)red_chunks(D) * 8;  // partials
   b += (size_t)cap * 8 * (2 + 16 + 1);                               // alpha/beta, scratch, coefficients
   b += sizeof(HvParams) + 4096;
+  b += (size_t)40 * ((size_t)1 << ((N + 1) / 2)) * 4;  // lo-neighbour table (width <= 40)
   (void)nev;
   return b;
 }
@@ -233,6 +234,19 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   t.Nhi = sec->tab.Nhi;
   t.n_up = sec->tab.n_up;
   t.dg = (const double*)pdg;
+  {
+    std::vector<uint32_t> ell;
+    int W = 0;
+    build_lo_table(sec->tab, P, ell, &W);
+    void* pe = nullptr;
+    if ((rc = take(&pe, ell.size() * 4 + 4))) return rc;
+    if (!ell.empty()) {
+      cudaMemcpyAsync(pe, ell.data(), ell.size() * 4, cudaMemcpyHostToDevice, s->stream);
+      AED_CUDA_TRY(cudaStreamSynchronize(s->stream));  // host vector goes out of scope
+    }
+    t.ell = (const uint32_t*)pe;
+    t.ell_w = W;
+  }
   if ((rc = launch_diag_table(P, t, (double*)pdg, s->stream))) return rc;
   I.D = D;
   I.nev = r->opts.nev;
@@ -468,7 +482,7 @@ int aed_server_submit(aed_server* s, const aed_model_desc* model, const aed_solv
   r->opts.start = nullptr;  // the server draws its own start vectors
   const int cap = cap_of(*r, t.D);
   const int n_store = s->precision == AED_FP32 ? std::min(kServerStore, cap + 1) : 0;
-  r->footprint = request_bytes(s, t.D, opts->nev, cap, n_store);
+  r->footprint = request_bytes(s, r->model.N, t.D, opts->nev, cap, n_store);
   if (r->footprint + sector_bytes(r->model.N, r->model.n_up) > s->budget)
     return fail(AED_ERR_ADMISSION, "request footprint (" + std::to_string(r->footprint) +
                                        " bytes) exceeds the server's HBM budget (" + std::to_string(s->budget) + ")");

@@ -179,24 +179,29 @@ def barrier(pg):
     torch.cuda.synchronize()
 
 
-def max_over_ranks(pg, v):
+def _reduce(pg, v, op):
     if pg is None:
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(pg, v):
+    return _reduce(pg, v, None if pg is None else pg.ReduceOp.MAX)
 
 
 def sum_over_ranks(pg, v):
-    if pg is None:
-        return v
-    import torch
+    return _reduce(pg, v, None if pg is None else pg.ReduceOp.SUM)
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+
+def rank_inputs(n_per_rank, world, rank):
+    """This rank's J2 values: the seed-2802 stream dealt round robin over the ranks
+    (replicas: every rank solves its own inputs, no data-path collective)."""
+    return j2_stream(n_per_rank * world)[rank::world]
 
 
 def cpu_sample(j2, iterations, threads_note="1 thread (the reference path is single-threaded)", rows=400_000):
@@ -231,7 +236,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     K, W = args.steps, args.warmup
     N, n_up = L28, L28 // 2
-    j2s = j2_stream((W + K) * world)[rank::world]
+    j2s = rank_inputs(W + K, world, rank)
     # the sector tables are resident before the timed region; each step sets
     # that step's couplings (coupling tables + diagonal, ~ms) and solves
     ham = ed.Hamiltonian(N, n_up, chain_bonds(L28, j2s[0]), precision=ed.FP64, device=local)
