@@ -143,6 +143,7 @@ def lib():
             "aed_solve": (ctypes.c_int, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),
             "aed_last_tmatrix": (ctypes.c_int, [_P, _DP, _DP, _I32, _I32P]),
             "aed_time_mult": (ctypes.c_int, [_P, _P, _P, _I32, _DP]),
+            "aed_time_apply": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _DP, _I32P]),
             "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
             "aed_launch_count": (ctypes.c_int, [_I64P]),
             "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
@@ -380,6 +381,14 @@ class Hamiltonian:
         _check(lib().aed_lanczos_step(self._h, v_prev.ptr if v_prev is not None else None, v_cur.ptr, v_next.ptr,
                                       beta_prev, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def time_apply(self, x, y, reps=5, variant=-1, with_alpha=False):
+        """(mean ms, variant) of the apply, optionally with the fused step's <x,y> partials."""
+        ms = ctypes.c_double(0)
+        v = ctypes.c_int32(0)
+        _check(lib().aed_time_apply(self._h, x.ptr, y.ptr, reps, variant, 1 if with_alpha else 0, ctypes.byref(ms),
+                                    ctypes.byref(v)))
+        return ms.value, v.value
 
     def time_mult(self, x, y, reps=10):
         ms = ctypes.c_double(0)

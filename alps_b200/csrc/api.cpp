@@ -1,6 +1,7 @@
 // api.cpp -- the C ABI of libaed.so (declared in include/aed.h).
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -214,6 +215,9 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
   }
+  if (std::getenv("AED_VERBOSE"))
+    std::fprintf(stderr, "[aed] apply %s D=%lld: variant %s (%.3f ms)\n", f32 ? "fp32" : "fp64", (long long)D,
+                 hv_variant_name(best), best_ms);
   *out = best;
   return AED_OK;
 }
@@ -602,6 +606,40 @@ int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, in
     if (alpha) alpha[i] = h->last_alpha[i];
     if (beta) beta[i] = h->last_beta[i];
   }
+  return AED_OK;
+}
+
+int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t variant, int32_t with_alpha,
+                   double* ms, int32_t* variant_used) {
+  int rc = check_vec(h, x, "x");
+  if (!rc) rc = check_vec(h, y, "y");
+  if (rc) return rc;
+  if (reps < 1 || !ms) return fail(AED_ERR_INVALID, "reps must be >= 1 and ms non-NULL");
+  if (variant >= hv_num_variants()) return fail(AED_ERR_INVALID, "unknown variant");
+  DeviceGuard g(h->device);
+  const bool f32 = h->precision == AED_FP32;
+  int v = variant;
+  if (v < 0) {
+    int& hv = h->hv_var[f32 ? 1 : 0];
+    if (hv < 0 && (rc = pick_variant(h, f32, x, y, &hv))) return rc;
+    v = hv;
+  }
+  double* part = with_alpha ? h->d_partA : nullptr;
+  if ((rc = launch_variant(h, f32, v, x, y, part))) return rc;  // warm-up
+  cudaEvent_t e0, e1;
+  AED_CUDA_TRY(cudaEventCreate(&e0));
+  AED_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEventRecord(e0, h->stream);
+  for (int r = 0; r < reps && !rc; ++r) rc = launch_variant(h, f32, v, x, y, part);
+  cudaEventRecord(e1, h->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  *ms = (double)t / reps;
+  if (variant_used) *variant_used = v;
   return AED_OK;
 }
 

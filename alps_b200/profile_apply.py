@@ -43,16 +43,25 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--variant", type=int, default=-1, help="apply variant (-1: autotuned)")
+    ap.add_argument("--alpha", action="store_true", help="with the fused step's <x,y> partials")
+    ap.add_argument("--sweep", action="store_true", help="time every variant with and without partials")
     a = ap.parse_args()
     N, n_up, bonds = workload_bonds(a.workload)
     prec = ed.FP64 if a.precision == "fp64" else ed.FP32
     ham = ed.Hamiltonian(N, n_up, bonds, precision=prec)
     x, y = ham.new_vector(), ham.new_vector()
     ham.fill_random(x, 1)
+    if a.sweep:
+        for v in range(6):
+            m0, _ = ham.time_apply(x, y, a.reps, v, False)
+            m1, _ = ham.time_apply(x, y, a.reps, v, True)
+            print(f"{a.workload} {a.precision} variant {v}: apply_ms={m0:.4f} with_alpha_ms={m1:.4f}")
+        return
     if a.warmup:
-        ham.time_mult(x, y, a.warmup)
-    ms = ham.time_mult(x, y, a.reps)
-    print(f"{a.workload} {a.precision} D={ham.dim} apply_ms={ms:.4f}")
+        ham.time_apply(x, y, a.warmup, a.variant, a.alpha)
+    ms, v = ham.time_apply(x, y, a.reps, a.variant, a.alpha)
+    print(f"{a.workload} {a.precision} D={ham.dim} variant={v} alpha={int(a.alpha)} apply_ms={ms:.4f}")
 
 
 if __name__ == "__main__":

@@ -199,6 +199,12 @@ int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap,
  * events; *ms = mean milliseconds per apply. */
 int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms);
 
+/* As aed_time_mult, for apply variant `variant` (-1: the handle's tuned one),
+ * with the per-tile <x, y> partials of the fused Lanczos step when
+ * with_alpha != 0.  *variant_used receives the variant timed. */
+int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t variant, int32_t with_alpha,
+                   double* ms, int32_t* variant_used);
+
 /* ---- batched / served solves ------------------------------------------------
  * Many independent requests (a model and solve options each) advance together
  * on one GPU: every engine step runs one Lanczos step of every resident
