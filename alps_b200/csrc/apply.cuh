@@ -119,8 +119,11 @@ __device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32
 }
 
 // Warp 0: every flip once, either direction (FP32 rows: order is free).
+// want_cross = false: the hi-part flips that apply to the tile (all rows);
+// true: the crossing flips (one lo-bit test per row).
 __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
-                                          const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
+                                          const uint32_t* __restrict__ thi, TileOp* prog, int cnt,
+                                          bool want_cross) {
   const int lane = threadIdx.x & 31;
   for (int q0 = 0; q0 < np; q0 += 32) {
     const int q = q0 + lane;
@@ -131,13 +134,13 @@ __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h
       const uint32_t fhi = e.flip >> Nlo, flo = e.flip & lm;
       const uint32_t hb = h & fhi;
       if (flo == 0u) {  // hi part only: applies to the whole tile iff the two bits differ
-        emit = __popc(hb) == 1;
-        op = {0u, __ldg(thi + (h ^ fhi)), e.c};
+        emit = !want_cross && __popc(hb) == 1;
+        if (emit) op = {0u, __ldg(thi + (h ^ fhi)), e.c};
       } else if (fhi == 0u) {  // lo part only: from the lo-neighbour table
         emit = false;
       } else {  // crossing: the lo bit must differ from the hi bit
-        emit = true;
-        op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
+        emit = want_cross;
+        if (emit) op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, emit);
@@ -208,6 +211,105 @@ __device__ __forceinline__ void stage_pairs(const HvParams& P, ApplySmem& sm) {
   for (int q = threadIdx.x; q < P.n_lolo; q += kHvThreads) sm.lolo_c[q] = P.lolo_c[q];
 }
 
+// FP32 rows, hi-part flips: every row of the tile takes them; four flips at a
+// time so that 4*R independent loads of x are in flight per thread.
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void run_hihi(const TileOp* prog, int o0, int o1, uint32_t nrow, uint32_t rt,
+                                         const T* __restrict__ x, Acc* acc) {
+  int o = o0;
+  for (; o + 4 <= o1; o += 4) {
+    TileOp e[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) e[v] = prog[o + v];
+    T xv[4][R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) xv[v][u] = (uint32_t)u < nrow ? __ldg(x + e[v].nb + rt + u * kHvThreads) : T(0);
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        if ((uint32_t)u < nrow) acc[u].add(e[v].c, xv[v][u]);
+  }
+  for (; o < o1; ++o) {
+    const TileOp e = prog[o];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if ((uint32_t)u < nrow) acc[u].add(e.c, __ldg(x + e.nb + rt + u * kHvThreads));
+  }
+}
+
+// FP32 rows, crossing flips: two at a time (rank lookups, then gathers).
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void run_cross(const TileOp* prog, int o0, int o1, const uint32_t* lv, uint32_t nrow,
+                                          const uint16_t* __restrict__ tlo, const T* __restrict__ x, Acc* acc) {
+  int o = o0;
+  for (; o + 2 <= o1; o += 2) {
+    TileOp e[2];
+    uint32_t j[2][R];
+    bool p[2][R];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      e[v] = prog[o + v];
+      const uint32_t fl = e[v].mc & 0xffffu, cd = e[v].mc >> 16;
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        p[v][u] = (uint32_t)u < nrow && (lv[u] & fl) == cd;
+        j[v][u] = p[v][u] ? e[v].nb + (uint32_t)__ldg(tlo + (lv[u] ^ fl)) : 0u;
+      }
+    }
+    T xv[2][R];
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u) xv[v][u] = p[v][u] ? __ldg(x + j[v][u]) : T(0);
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p[v][u]) acc[u].add(e[v].c, xv[v][u]);
+  }
+  for (; o < o1; ++o) {
+    const TileOp e = prog[o];
+    const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if ((uint32_t)u < nrow && (lv[u] & fl) == cd) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+  }
+}
+
+// FP32 rows, lo-part flips from the lo-neighbour table, two entries at a time.
+template <typename T, typename Acc, int R>
+__device__ __forceinline__ void run_lo_table_any(const DevTables& t, uint32_t lbase, uint32_t nk, uint32_t base,
+                                                 uint32_t rt, uint32_t nrow, const double* lolo_c,
+                                                 const T* __restrict__ x, Acc* acc) {
+  const uint32_t* E = t.ell + (size_t)t.ell_w * lbase;
+  for (int e = 0; e < t.ell_w; e += 2) {
+    uint32_t ent[2][R];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        ent[v][u] = ((uint32_t)u < nrow && e + v < t.ell_w) ? __ldg(E + (size_t)(e + v) * nk + rt + u * kHvThreads)
+                                                             : kEllPad;
+        any |= ent[v][u] != kEllPad;
+      }
+    if (!__any_sync(0xffffffffu, any)) break;
+    T xv[2][R];
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u) xv[v][u] = ent[v][u] != kEllPad ? __ldg(x + base + (ent[v][u] & 0xffffu)) : T(0);
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (ent[v][u] != kEllPad) acc[u].add(lolo_c[ent[v][u] >> 16], xv[v][u]);
+  }
+}
+
 // Flips inside the lo part, from the lo-neighbour table: entry e of the R rows
 // of this thread.  All targets lie in the thread's own hi block (base).  With
 // kOrdered the entries come in ascending target rank, so the diagonal is
@@ -264,8 +366,8 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
       nl = compile_ordered(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
       cnt = compile_ordered(sm.rise, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, nl);
     } else {
-      nl = 0;
-      cnt = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0);
+      nl = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, 0, false);  // hi-part flips
+      cnt = compile_any(sm.low, c.np, h, c.Nlo, c.lm, t.thi, sm.prog, nl, true);  // crossing flips
     }
     if (threadIdx.x == 0) {
       sm.nlow = nl;
@@ -310,8 +412,9 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
           const uint32_t i = base + rt + u * kHvThreads;
           acc[u].add(__ldg(t.dg + i), __ldg(x + i));
         }
-      run_ops<T, Acc, R>(sm.prog, 0, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
-      run_lo_table<T, Acc, R, false>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc, dd);
+      run_hihi<T, Acc, R>(sm.prog, 0, nlow, nrow, rt, x, acc);
+      run_cross<T, Acc, R>(sm.prog, nlow, nops, lv, nrow, t.tlo, x, acc);
+      run_lo_table_any<T, Acc, R>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc);
     }
 #pragma unroll
     for (int u = 0; u < R; ++u) {
