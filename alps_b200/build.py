@@ -27,7 +27,8 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-para
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "batch.cu"]
 CPP_SOURCES = ["model.cpp", "tmatrix.cpp", "api.cpp", "lanczos.cpp", "server.cpp"]
-HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "tmatrix_core.h", "batch.cuh"]
+HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "apply_blocks.cuh", "tmatrix_core.h",
+           "batch.cuh"]
 
 
 def _newer(src, dst, deps):

@@ -92,7 +92,19 @@ constexpr uint32_t kEllPad = 0xffffffffu;
 void build_lo_table(const BasisTables& t, const HvParams& P, std::vector<uint32_t>& ell, int* width);
 
 // Work tiles over the sector: (hi block h, first row r0 within the block).
-void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr);
+void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr,
+                 std::vector<uint32_t>* tfirst = nullptr);
+// Hi blocks grouped by lo popcount (largest blocks first, h ascending within a
+// group), each group padded with kNoBlockEntry to a multiple of kBundleMax, so
+// that bundles of 1, 2 or 4 consecutive entries never mix groups.  *maxrows:
+// rows of the largest block.
+// Crossing-flip table: entry b * 2^Nlo + looff[k] + r is the rank (within
+// its popcount class) of lo state lolist[looff[k] + r] with bit b flipped,
+// with bit 15 = the state's bit b (ranks are below 2^15 for Nlo <= 16).
+void build_cross_table(const BasisTables& t, std::vector<uint16_t>& xt);
+constexpr int kBundleMax = 4;
+constexpr uint32_t kNoBlockEntry = 0xffffffffu;
+void build_block_list(const BasisTables& t, std::vector<uint32_t>& blk, int* maxrows);
 
 // ---- tridiagonal / Tmatrix (host) ---------------------------------------------
 int tridiag_eigen(int n, double* d, double* e, double* zlast, double* zfull = nullptr);

@@ -37,8 +37,11 @@ void release(aed_handle* h) {
   cudaFree(h->d_looff);
   cudaFree(h->d_tile_h);
   cudaFree(h->d_tile_r);
+  cudaFree(h->d_blk_h);
+  cudaFree(h->d_tfirst);
   cudaFree(h->d_dg);
   cudaFree(h->d_ell);
+  cudaFree(h->d_xtab);
   cudaFree(h->d_partA);
   cudaFree(h->d_partB);
   cudaFree(h->d_scal);
@@ -149,9 +152,17 @@ void handle_release_workspace(aed_handle* h) {
 
 namespace {
 
+// Returns kVariantNotApplicable (nothing launched) for a variant that does not fit the sector.
 int launch_variant(aed_handle* h, bool f32, int v, const void* x, void* y, double* alpha_part) {
   if (f32) return launch_hv_f32(v, h->P, h->dt, (const float*)x, (float*)y, alpha_part, h->stream);
   return launch_hv_f64(v, h->P, h->dt, (const double*)x, (double*)y, alpha_part, h->stream);
+}
+
+int launch_checked(aed_handle* h, bool f32, int v, const void* x, void* y, double* alpha_part) {
+  const int rc = launch_variant(h, f32, v, x, y, alpha_part);
+  if (rc == kVariantNotApplicable)
+    return fail(AED_ERR_INVALID, std::string("apply variant ") + hv_variant_name(v) + " does not fit this sector");
+  return rc;
 }
 
 // Autotuner: the apply variant (rows per thread, ops per group, CTAs per SM)
@@ -195,6 +206,10 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
   // as solves run them: with the per-tile <x,y> partials; best of three
   for (int v = 0; v < hv_num_variants() && !rc; ++v) {
     rc = launch_variant(h, f32, v, x, y, h->d_partA);  // warm-up
+    if (rc == kVariantNotApplicable) {  // does not fit this sector
+      rc = AED_OK;
+      continue;
+    }
     for (int r = 0; r < 3 && !rc; ++r) {
       cudaEventRecord(e0, h->stream);
       rc = launch_variant(h, f32, v, x, y, h->d_partA);
@@ -224,13 +239,15 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
 
 }  // namespace
 
-int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+int handle_tune(aed_handle* h, bool f32, const void* x, void* y) {
   int& v = h->hv_var[f32 ? 1 : 0];
-  if (v < 0) {
-    const int rc = pick_variant(h, f32, x, y, &v);
-    if (rc) return rc;
-  }
-  return launch_variant(h, f32, v, x, y, alpha_part);
+  return v < 0 ? pick_variant(h, f32, x, y, &v) : AED_OK;
+}
+
+int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+  const int rc = handle_tune(h, f32, x, y);
+  if (rc) return rc;
+  return launch_checked(h, f32, h->hv_var[f32 ? 1 : 0], x, y, alpha_part);
 }
 
 }  // namespace aed
@@ -290,12 +307,18 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     release(h);
     return rc;
   }
-  std::vector<uint32_t> th, tr;
-  build_tiles(h->tab, kHvTileRows, th, tr);
+  std::vector<uint32_t> th, tr, tf, blk;
+  std::vector<uint16_t> xt;
+  int maxrows = 0;
+  build_tiles(h->tab, kHvTileRows, th, tr, &tf);
+  build_block_list(h->tab, blk, &maxrows);
+  build_cross_table(h->tab, xt);
   const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
   if ((rc = dev_alloc(&h->d_thi, nhi)) || (rc = dev_alloc(&h->d_tlo, nlo)) || (rc = dev_alloc(&h->d_lolist, nlo)) ||
       (rc = dev_alloc(&h->d_looff, h->tab.looff.size())) || (rc = dev_alloc(&h->d_tile_h, th.size())) ||
       (rc = dev_alloc(&h->d_tile_r, tr.size())) || (rc = dev_alloc(&h->d_scal, 8)) ||
+      (rc = dev_alloc(&h->d_blk_h, blk.size() + 1)) || (rc = dev_alloc(&h->d_tfirst, tf.size() + 1)) ||
+      (rc = dev_alloc(&h->d_xtab, xt.size() + 1)) ||
       (rc = dev_alloc(&h->d_dg, (size_t)h->tab.D))) {
     release(h);
     return rc;
@@ -318,6 +341,9 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     cudaMemcpyAsync(h->d_tile_h, th.data(), th.size() * 4, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_tile_r, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice, h->stream);
   }
+  if (!blk.empty()) cudaMemcpyAsync(h->d_blk_h, blk.data(), blk.size() * 4, cudaMemcpyHostToDevice, h->stream);
+  if (!tf.empty()) cudaMemcpyAsync(h->d_tfirst, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice, h->stream);
+  if (!xt.empty()) cudaMemcpyAsync(h->d_xtab, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, h->stream);
   const cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     release(h);
@@ -331,6 +357,11 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   t.tile_h = h->d_tile_h;
   t.tile_r = h->d_tile_r;
   t.n_tiles = (int64_t)th.size();
+  t.xtab = h->d_xtab;
+  t.blk_h = h->d_blk_h;
+  t.tfirst = h->d_tfirst;
+  t.n_blk = (int64_t)blk.size();
+  t.maxrows = maxrows;
   t.D = h->tab.D;
   t.Nlo = h->tab.Nlo;
   t.Nhi = h->tab.Nhi;
@@ -625,12 +656,12 @@ int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t 
     v = hv;
   }
   double* part = with_alpha ? h->d_partA : nullptr;
-  if ((rc = launch_variant(h, f32, v, x, y, part))) return rc;  // warm-up
+  if ((rc = launch_checked(h, f32, v, x, y, part))) return rc;  // warm-up
   cudaEvent_t e0, e1;
   AED_CUDA_TRY(cudaEventCreate(&e0));
   AED_CUDA_TRY(cudaEventCreate(&e1));
   cudaEventRecord(e0, h->stream);
-  for (int r = 0; r < reps && !rc; ++r) rc = launch_variant(h, f32, v, x, y, part);
+  for (int r = 0; r < reps && !rc; ++r) rc = launch_checked(h, f32, v, x, y, part);
   cudaEventRecord(e1, h->stream);
   cudaEventSynchronize(e1);
   float t = 0.f;

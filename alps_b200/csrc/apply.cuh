@@ -120,7 +120,10 @@ __device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32
 
 // Warp 0: every flip once, either direction (FP32 rows: order is free).
 // want_cross = false: the hi-part flips that apply to the tile (all rows);
-// true: the crossing flips (one lo-bit test per row).
+// true: the crossing flips.  A crossing entry names its lo bit b (mc >> 16)
+// and the lo-bit value v that the row must have (bit 15 of mc), for the
+// crossing-flip table: entry e = rank | (bit b << 15) applies iff bit 15 of
+// e equals v, and then its target row is nb + e with nb = base - (v << 15).
 __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
                                           const uint32_t* __restrict__ thi, TileOp* prog, int cnt,
                                           bool want_cross) {
@@ -140,7 +143,8 @@ __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h
         emit = false;
       } else {  // crossing: the lo bit must differ from the hi bit
         emit = want_cross;
-        if (emit) op = {flo | ((hb ? 0u : flo) << 16), __ldg(thi + (h ^ fhi)), e.c};
+        const uint32_t v = hb ? 0u : 1u;
+        if (emit) op = {((uint32_t)(__ffs(flo) - 1) << 16) | (v << 15), __ldg(thi + (h ^ fhi)) - (v << 15), e.c};
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, emit);
@@ -240,42 +244,48 @@ __device__ __forceinline__ void run_hihi(const TileOp* prog, int o0, int o1, uin
   }
 }
 
-// FP32 rows, crossing flips: two at a time (rank lookups, then gathers).
+// FP32 rows, crossing flips from the crossing-flip table (coalesced 16-bit
+// loads, no dependent rank lookup), four flips at a time.  xt: table entries
+// of this thread's u = 0 row for lo bit 0 (xtab + lbase + rt); nlo = 2^Nlo,
+// the table's stride per lo bit.
 template <typename T, typename Acc, int R>
-__device__ __forceinline__ void run_cross(const TileOp* prog, int o0, int o1, const uint32_t* lv, uint32_t nrow,
-                                          const uint16_t* __restrict__ tlo, const T* __restrict__ x, Acc* acc) {
+__device__ __forceinline__ void run_cross(const TileOp* prog, int o0, int o1, const uint16_t* __restrict__ xt,
+                                          uint32_t nlo, uint32_t nrow, const T* __restrict__ x, Acc* acc) {
+  constexpr int U = 4;
   int o = o0;
-  for (; o + 2 <= o1; o += 2) {
-    TileOp e[2];
-    uint32_t j[2][R];
-    bool p[2][R];
+  for (; o + U <= o1; o += U) {
+    TileOp e[U];
+    uint32_t ent[U][R];
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < U; ++v) {
       e[v] = prog[o + v];
-      const uint32_t fl = e[v].mc & 0xffffu, cd = e[v].mc >> 16;
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        p[v][u] = (uint32_t)u < nrow && (lv[u] & fl) == cd;
-        j[v][u] = p[v][u] ? e[v].nb + (uint32_t)__ldg(tlo + (lv[u] ^ fl)) : 0u;
-      }
-    }
-    T xv[2][R];
-#pragma unroll
-    for (int v = 0; v < 2; ++v)
-#pragma unroll
-      for (int u = 0; u < R; ++u) xv[v][u] = p[v][u] ? __ldg(x + j[v][u]) : T(0);
-#pragma unroll
-    for (int v = 0; v < 2; ++v)
+      const uint16_t* xb = xt + (size_t)(e[v].mc >> 16) * nlo;
 #pragma unroll
       for (int u = 0; u < R; ++u)
-        if (p[v][u]) acc[u].add(e[v].c, xv[v][u]);
+        ent[v][u] = (uint32_t)u < nrow ? (uint32_t)__ldg(xb + u * kHvThreads) : (~e[v].mc & 0x8000u);
+    }
+    T xv[U][R];
+#pragma unroll
+    for (int v = 0; v < U; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        xv[v][u] = ((ent[v][u] ^ e[v].mc) & 0x8000u) == 0u ? __ldg(x + (e[v].nb + ent[v][u])) : T(0);
+#pragma unroll
+    for (int v = 0; v < U; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (((ent[v][u] ^ e[v].mc) & 0x8000u) == 0u) acc[u].add(e[v].c, xv[v][u]);
   }
   for (; o < o1; ++o) {
     const TileOp e = prog[o];
-    const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
+    const uint16_t* xb = xt + (size_t)(e.mc >> 16) * nlo;
 #pragma unroll
-    for (int u = 0; u < R; ++u)
-      if ((uint32_t)u < nrow && (lv[u] & fl) == cd) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+    for (int u = 0; u < R; ++u) {
+      if ((uint32_t)u < nrow) {
+        const uint32_t ent = __ldg(xb + u * kHvThreads);
+        if (((ent ^ e.mc) & 0x8000u) == 0u) acc[u].add(e.c, __ldg(x + (e.nb + ent)));
+      }
+    }
   }
 }
 
@@ -387,7 +397,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
       const uint32_t r = rt + u * kHvThreads;
       const bool ok = r < rows && r < r0 + kTileRows;
       nrow += ok ? 1u : 0u;
-      lv[u] = ok ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;
+      lv[u] = (kOrdered && ok) ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;  // FP32 rows use the tables only
     }
     Acc acc[R];
     bool dd[R];
@@ -413,7 +423,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
           acc[u].add(__ldg(t.dg + i), __ldg(x + i));
         }
       run_hihi<T, Acc, R>(sm.prog, 0, nlow, nrow, rt, x, acc);
-      run_cross<T, Acc, R>(sm.prog, nlow, nops, lv, nrow, t.tlo, x, acc);
+      run_cross<T, Acc, R>(sm.prog, nlow, nops, t.xtab + lbase + rt, 1u << c.Nlo, nrow, x, acc);
       run_lo_table_any<T, Acc, R>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc);
     }
 #pragma unroll
@@ -422,7 +432,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
         const uint32_t i = base + rt + u * kHvThreads;
         const T v = acc[u].value();
         y[i] = v;
-        if (alpha_part) dotacc += (double)__ldg(x + i) * (double)v;
+        if (alpha_part) dotacc = fma((double)__ldg(x + i), (double)v, dotacc);
       }
     }
   }

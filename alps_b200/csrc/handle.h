@@ -23,8 +23,11 @@ struct aed_handle {
   uint32_t* d_looff = nullptr;
   uint32_t* d_tile_h = nullptr;
   uint32_t* d_tile_r = nullptr;
+  uint32_t* d_blk_h = nullptr;   // block list of the bundle apply
+  uint32_t* d_tfirst = nullptr;  // first tile of each hi block
   double* d_dg = nullptr;     // per-row diagonal
   uint32_t* d_ell = nullptr;  // lo-neighbour table
+  uint16_t* d_xtab = nullptr;  // crossing-flip table
   double* d_partA = nullptr;  // per-tile partial sums (n_tiles)
   double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
   double* d_scal = nullptr;   // 8 device scalars
@@ -60,6 +63,9 @@ struct DeviceGuard {
 };
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
+// Choose the apply variant for this precision now (timed launches on x, y)
+// unless already chosen; handle_hv does this on its first call otherwise.
+int handle_tune(aed_handle* h, bool f32, const void* x, void* y);
 // Workspace of at least `bytes` device bytes / `n` pinned doubles, reused across solves.
 int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out);
 int handle_pinned(aed_handle* h, size_t n, double** out);

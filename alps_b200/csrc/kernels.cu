@@ -15,6 +15,7 @@
 #include <string>
 
 #include "apply.cuh"
+#include "apply_blocks.cuh"
 #include "kernels.cuh"
 #include "reduce.cuh"
 
@@ -36,6 +37,24 @@ __global__ void __launch_bounds__(kHvThreads, MINB) hv_kernel(const __grid_const
   apply::stage_pairs(P, sm);
   const apply::ApplyCtx c = apply::ctx_of(P);
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) apply::apply_tile<T, Acc, R>(c, t, it, x, y, alpha_part, sm);
+}
+
+// y = H x over bundles of B hi blocks with x staged in shared memory (dynamic:
+// B * maxrows values).  Bundles are taken in a static round robin; the block
+// list puts the largest blocks first.
+template <typename T, typename Acc, int R, int B, int MINB>
+__global__ void __launch_bounds__(kHvThreads, MINB) hvb_kernel(const __grid_constant__ HvParams P, const DevTables t,
+                                                               const T* __restrict__ x, T* __restrict__ y,
+                                                               double* __restrict__ alpha_part) {
+  extern __shared__ __align__(16) unsigned char hvb_dyn[];
+  __shared__ bapply::BundleSmem<B> sm;
+  T* xs = bapply::carve<T, B>(P, t, hvb_dyn, sm);
+  bapply::stage_pairs<B>(P, sm);
+  const apply::ApplyCtx c = apply::ctx_of(P);
+  const int64_t nb = t.n_blk / B;
+  int rc = 0;
+  for (int64_t ub = blockIdx.x; ub < nb; ub += gridDim.x)
+    bapply::apply_bundle<T, Acc, R, B>(c, t, ub, x, y, alpha_part, sm, xs, rc);
 }
 
 // Diagonal M(i,i) of every row, accumulated in the reference's term order
@@ -236,13 +255,17 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
   return check_launch("ritz_combine_kernel");
 }
 
-// ---- apply variants (rows per thread, CTAs per SM) ------------------------------
+// ---- apply variants -------------------------------------------------------------
+// Tile apply (apply.cuh): R rows per thread, MINB CTAs per SM.  Bundle apply
+// (apply_blocks.cuh): B hi blocks per CTA with x in shared memory.
 struct HvVariant {
-  int R, minb;
+  int B, R, minb;  // B = 0: tile apply
   const char* name;
 };
 constexpr HvVariant kVariants[] = {
-    {4, 6, "r4b6"}, {4, 5, "r4b5"}, {4, 4, "r4b4"}, {2, 8, "r2b8"}, {2, 6, "r2b6"}, {8, 3, "r8b3"},
+    {0, 4, 6, "r4b6"},      {0, 4, 5, "r4b5"},      {0, 4, 4, "r4b4"},      {0, 2, 8, "r2b8"},
+    {0, 2, 6, "r2b6"},      {0, 8, 3, "r8b3"},      {1, 4, 3, "blk1r4b3"},  {2, 2, 4, "blk2r2b4"},
+    {2, 4, 2, "blk2r4b2"},  {4, 1, 2, "blk4r1b2"},  {4, 2, 2, "blk4r2b2"},  {1, 2, 4, "blk1r2b4"},
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -260,10 +283,52 @@ int launch_one(const HvParams& P, const DevTables& t, const T* x, T* y, double* 
   return check_launch("hv_kernel");
 }
 
+// Occupancy of a bundle kernel for `dyn` bytes of dynamic shared memory,
+// cached per kernel and size (sectors of one process share a few sizes).
+struct BundleGrid {
+  size_t dyn = 0;
+  int grid = 0;
+};
+
+template <typename T, typename Acc, int R, int B, int MINB>
+int launch_bundle(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st,
+                  BundleGrid* cache) {
+  if (!t.blk_h || t.maxrows <= 0) return kVariantNotApplicable;
+  const size_t dyn = bapply::bundle_smem_bytes<T>(B, t.maxrows, P.n_pairs, P.n_lolo);
+  auto kern = hvb_kernel<T, Acc, R, B, MINB>;
+  if (cache->dyn != dyn || cache->grid <= 0) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+      const cudaError_t e = cudaGetLastError();
+      return fail(AED_ERR_CUDA, std::string("hvb_kernel attributes: ") + cudaGetErrorString(e));
+    }
+    if (fa.sharedSizeBytes + dyn > (size_t)optin) return kVariantNotApplicable;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
+      const cudaError_t e = cudaGetLastError();
+      return fail(AED_ERR_CUDA, std::string("hvb_kernel shared memory: ") + cudaGetErrorString(e));
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHvThreads, dyn);
+    if (per_sm < 1) return kVariantNotApplicable;
+    cache->dyn = dyn;
+    cache->grid = num_sms() * per_sm;
+  }
+  int64_t grid = cache->grid;
+  const int64_t nb = t.n_blk / B;
+  if (grid > nb) grid = nb;
+  if (grid < 1) return AED_OK;
+  kern<<<(unsigned)grid, kHvThreads, dyn, st>>>(P, t, x, y, alpha_part);
+  return check_launch("hvb_kernel");
+}
+
 template <typename T, typename Acc>
 int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
                 cudaStream_t st) {
   static int grids[kNumVariants] = {};
+  static BundleGrid bgrid[kNumVariants];
   if (t.n_tiles == 0) return AED_OK;
   switch (v) {
     case 0: return launch_one<T, Acc, 4, 6>(P, t, x, y, alpha_part, st, &grids[0]);
@@ -272,6 +337,12 @@ int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, 
     case 3: return launch_one<T, Acc, 2, 8>(P, t, x, y, alpha_part, st, &grids[3]);
     case 4: return launch_one<T, Acc, 2, 6>(P, t, x, y, alpha_part, st, &grids[4]);
     case 5: return launch_one<T, Acc, 8, 3>(P, t, x, y, alpha_part, st, &grids[5]);
+    case 6: return launch_bundle<T, Acc, 4, 1, 3>(P, t, x, y, alpha_part, st, &bgrid[6]);
+    case 7: return launch_bundle<T, Acc, 2, 2, 4>(P, t, x, y, alpha_part, st, &bgrid[7]);
+    case 8: return launch_bundle<T, Acc, 4, 2, 2>(P, t, x, y, alpha_part, st, &bgrid[8]);
+    case 9: return launch_bundle<T, Acc, 1, 4, 2>(P, t, x, y, alpha_part, st, &bgrid[9]);
+    case 10: return launch_bundle<T, Acc, 2, 4, 2>(P, t, x, y, alpha_part, st, &bgrid[10]);
+    case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[11]);
     default: return fail(AED_ERR_INVALID, "unknown apply variant");
   }
 }

@@ -19,22 +19,32 @@ struct DevTables {
   const uint32_t* tile_r;  // n_tiles
   const double* dg;        // D: diagonal M(i,i) of every row
   const uint32_t* ell;     // lo-neighbour table (build_lo_table), ell_w entries per lo state
+  const uint16_t* xtab = nullptr;  // crossing-flip table (build_cross_table), Nlo x 2^Nlo
   int ell_w;
   int64_t n_tiles;
   int64_t D;
   int Nlo, Nhi, n_up;
+  // block list of the bundle apply (build_block_list): hi blocks grouped by
+  // lo popcount, each group padded with kNoBlock to a multiple of kBundleMax
+  const uint32_t* blk_h = nullptr;   // n_blk
+  const uint32_t* tfirst = nullptr;  // 2^Nhi: index of the first tile of each hi block
+  int64_t n_blk = 0;
+  int maxrows = 0;  // rows of the largest hi block
 };
 
 constexpr int kHvThreads = 256;
 constexpr int kHvTileRows = 2048;  // rows per work tile (a multiple of kHvThreads x rows per thread)
 constexpr int kRedThreads = 256;
 
-// y = H x with apply variant `variant` (0 .. hv_num_variants()-1).
+// y = H x with apply variant `variant` (0 .. hv_num_variants()-1).  A
+// variant that does not fit the sector (shared memory) returns
+// kVariantNotApplicable without launching.
 // alpha_part (optional): one partial sum of x_i * y_i per tile (n_tiles entries).
 int launch_hv_f64(int variant, const HvParams& P, const DevTables& t, const double* x, double* y,
                   double* alpha_part, cudaStream_t st);
 int launch_hv_f32(int variant, const HvParams& P, const DevTables& t, const float* x, float* y,
                   double* alpha_part, cudaStream_t st);
+constexpr int kVariantNotApplicable = 2;
 int hv_num_variants();
 const char* hv_variant_name(int v);
 

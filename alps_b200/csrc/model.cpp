@@ -172,6 +172,16 @@ void build_lo_table(const BasisTables& t, const HvParams& P, std::vector<uint32_
   }
 }
 
+void build_cross_table(const BasisTables& t, std::vector<uint16_t>& xt) {
+  const uint32_t nlo = 1u << t.Nlo;
+  xt.assign((size_t)t.Nlo * nlo, 0);
+  for (int b = 0; b < t.Nlo; ++b)
+    for (uint32_t i = 0; i < nlo; ++i) {
+      const uint32_t l = t.lolist[i];
+      xt[(size_t)b * nlo + i] = (uint16_t)(t.tlo[l ^ (1u << b)] | (((l >> b) & 1u) << 15));
+    }
+}
+
 // ---- basis tables (Lin 1990 two-table ranking) -----------------------------------
 static inline int popc32(uint32_t v) { return __builtin_popcount(v); }
 
@@ -209,18 +219,42 @@ int build_tables(int N, int n_up, BasisTables& t) {
   return AED_OK;
 }
 
-void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr) {
+void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr,
+                 std::vector<uint32_t>* tfirst) {
   th.clear();
   tr.clear();
   const uint32_t nhi = 1u << t.Nhi;
+  if (tfirst) tfirst->assign(nhi, 0u);
   for (uint32_t h = 0; h < nhi; ++h) {
     const int k = t.n_up - popc32(h);
     if (k < 0 || k > t.Nlo) continue;
+    if (tfirst) (*tfirst)[h] = (uint32_t)th.size();
     const uint32_t rows = t.looff[k + 1] - t.looff[k];
     for (uint32_t r = 0; r < rows; r += tile_rows) {
       th.push_back(h);
       tr.push_back(r);
     }
+  }
+}
+
+void build_block_list(const BasisTables& t, std::vector<uint32_t>& blk, int* maxrows) {
+  blk.clear();
+  *maxrows = 0;
+  const uint32_t nhi = 1u << t.Nhi;
+  std::vector<int> ks;
+  for (int k = 0; k <= t.Nlo; ++k) {
+    const int hk = t.n_up - k;  // popcount of the hi blocks with lo popcount k
+    if (hk < 0 || hk > t.Nhi) continue;
+    ks.push_back(k);
+    *maxrows = std::max(*maxrows, (int)(t.looff[k + 1] - t.looff[k]));
+  }
+  std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) {
+    return t.looff[a + 1] - t.looff[a] > t.looff[b + 1] - t.looff[b];
+  });
+  for (int k : ks) {
+    for (uint32_t h = 0; h < nhi; ++h)
+      if (t.n_up - popc32(h) == k) blk.push_back(h);
+    while (blk.size() % kBundleMax) blk.push_back(kNoBlockEntry);
   }
 }
 

@@ -32,6 +32,7 @@ using clk = std::chrono::steady_clock;
 struct Sector {
   BasisTables tab;
   uint32_t *thi = nullptr, *looff = nullptr, *tile_h = nullptr, *tile_r = nullptr;
+  uint16_t* xtab = nullptr;  // crossing-flip table
   uint16_t *tlo = nullptr, *lolist = nullptr;
   int64_t n_tiles = 0;
   size_t bytes = 0;
@@ -125,7 +126,7 @@ size_t sector_bytes(int N, int n_up) {
   BasisTables t;
   if (build_tables(N, n_up, t)) return 0;
   return t.thi.size() * 4 + t.tlo.size() * 2 + t.lolist.size() * 2 + t.looff.size() * 4 +
-         (size_t)sector_tiles_est(t.D) * 8 + 4096;
+         (size_t)t.Nlo * t.tlo.size() * 2 + (size_t)sector_tiles_est(t.D) * 8 + 4096;
 }
 
 int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
@@ -140,13 +141,16 @@ int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
   int rc = build_tables(N, n_up, sec.tab);
   if (rc) return rc;
   std::vector<uint32_t> th, tr;
+  std::vector<uint16_t> xt;
   build_tiles(sec.tab, kHvTileRows, th, tr);
+  build_cross_table(sec.tab, xt);
   sec.n_tiles = (int64_t)th.size();
   const size_t nhi = sec.tab.thi.size(), nlo = sec.tab.tlo.size(), nof = sec.tab.looff.size();
   if ((rc = dmalloc(s, (void**)&sec.thi, nhi * 4)) || (rc = dmalloc(s, (void**)&sec.tlo, nlo * 2)) ||
       (rc = dmalloc(s, (void**)&sec.lolist, nlo * 2)) || (rc = dmalloc(s, (void**)&sec.looff, nof * 4)) ||
       (rc = dmalloc(s, (void**)&sec.tile_h, th.size() * 4 + 4)) ||
-      (rc = dmalloc(s, (void**)&sec.tile_r, tr.size() * 4 + 4)))
+      (rc = dmalloc(s, (void**)&sec.tile_r, tr.size() * 4 + 4)) ||
+      (rc = dmalloc(s, (void**)&sec.xtab, xt.size() * 2 + 4)))
     return rc;
   cudaMemcpyAsync(sec.thi, sec.tab.thi.data(), nhi * 4, cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(sec.tlo, sec.tab.tlo.data(), nlo * 2, cudaMemcpyHostToDevice, s->stream);
@@ -156,7 +160,8 @@ int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
     cudaMemcpyAsync(sec.tile_h, th.data(), th.size() * 4, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(sec.tile_r, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice, s->stream);
   }
-  AED_CUDA_TRY(cudaStreamSynchronize(s->stream));  // host vectors th/tr go out of scope
+  if (!xt.empty()) cudaMemcpyAsync(sec.xtab, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, s->stream);
+  AED_CUDA_TRY(cudaStreamSynchronize(s->stream));  // host vectors th/tr/xt go out of scope
   sec.bytes = sector_bytes(N, n_up);
   sec.refs = 1;
   s->used += sec.bytes;
@@ -171,7 +176,7 @@ void sector_release(aed_server* s, std::pair<int, int> key) {
   if (--it->second.refs > 0) return;
   Sector& sec = it->second;
   for (void* p : {(void*)sec.thi, (void*)sec.tlo, (void*)sec.lolist, (void*)sec.looff, (void*)sec.tile_h,
-                  (void*)sec.tile_r})
+                  (void*)sec.tile_r, (void*)sec.xtab})
     if (p) cudaFreeAsync(p, s->stream);
   s->used -= std::min(s->used, sec.bytes);
   s->sectors.erase(it);
@@ -228,6 +233,7 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   t.looff = sec->looff;
   t.tile_h = sec->tile_h;
   t.tile_r = sec->tile_r;
+  t.xtab = sec->xtab;
   t.n_tiles = sec->n_tiles;
   t.D = D;
   t.Nlo = sec->tab.Nlo;
@@ -453,7 +459,7 @@ int aed_server_destroy(aed_server* s) {
   for (auto& kv : s->sectors) {
     Sector& sec = kv.second;
     for (void* p : {(void*)sec.thi, (void*)sec.tlo, (void*)sec.lolist, (void*)sec.looff, (void*)sec.tile_h,
-                    (void*)sec.tile_r})
+                    (void*)sec.tile_r, (void*)sec.xtab})
       if (p) cudaFreeAsync(p, s->stream);
   }
   cudaStreamSynchronize(s->stream);

@@ -53,10 +53,17 @@ def main():
     x, y = ham.new_vector(), ham.new_vector()
     ham.fill_random(x, 1)
     if a.sweep:
-        for v in range(6):
-            m0, _ = ham.time_apply(x, y, a.reps, v, False)
-            m1, _ = ham.time_apply(x, y, a.reps, v, True)
-            print(f"{a.workload} {a.precision} variant {v}: apply_ms={m0:.4f} with_alpha_ms={m1:.4f}")
+        v = 0
+        while True:
+            try:
+                m0, _ = ham.time_apply(x, y, a.reps, v, False)
+                m1, _ = ham.time_apply(x, y, a.reps, v, True)
+                print(f"{a.workload} {a.precision} variant {v}: apply_ms={m0:.4f} with_alpha_ms={m1:.4f}")
+            except ed.AEDError as e:
+                if "unknown" in str(e):
+                    break
+                print(f"{a.workload} {a.precision} variant {v}: {e}")
+            v += 1
         return
     if a.warmup:
         ham.time_apply(x, y, a.warmup, a.variant, a.alpha)

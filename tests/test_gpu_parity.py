@@ -106,6 +106,82 @@ def test_hv_fp64_bit_exact_random_bond_square_4x5(seed):
     assert np.array_equal(ham.apply(x), M.mult(x))
 
 
+def _apply_variants(ham):
+    """Indices of the apply variants that fit this sector (tile and bundle kernels)."""
+    x, y = ham.new_vector(), ham.new_vector()
+    ham.fill_random(x, 1)
+    out, v = [], 0
+    while True:
+        try:
+            ham.time_apply(x, y, 1, v)
+            out.append(v)
+        except ed.AEDError as e:
+            if "unknown" in str(e):
+                break
+        v += 1
+    return out
+
+
+VARIANT_CASES = [HV_CASES[0], HV_CASES[1], HV_CASES[4], HV_CASES[6], HV_CASES[7], HV_CASES[8], HV_CASES[9],
+                 ("square4x4_h", dict(LATTICE="square lattice", L=4, J=1, h=0.21))]
+
+
+@pytest.mark.parametrize("name,p", VARIANT_CASES, ids=[c[0] for c in VARIANT_CASES])
+def test_hv_every_variant_fp64_bit_exact(name, p):
+    """Every apply variant (tile and bundle kernels, forced) gives the explicit matrix's rows bit for bit."""
+    ham = ed.Hamiltonian.from_parameters(spin_params(**p))
+    M = _oracle_for(ham.params)
+    x = np.random.default_rng(11).normal(size=ham.dim)
+    ref = M.mult(x)
+    xd, yd = ham.new_vector().upload(x), ham.new_vector()
+    vs = _apply_variants(ham)
+    assert len(vs) >= 12
+    for v in vs:
+        yd.upload(np.full(ham.dim, np.nan))
+        ham.time_apply(xd, yd, 1, v)
+        assert np.array_equal(yd.download(), ref), (v, ed.lib().aed_last_error())
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_hv_every_variant_random_square_4x5(seed):
+    n, bonds = random_bonds("square lattice", {"L": 4, "W": 5}, seed, 0.8, 1.2)
+    for prec in (ed.FP64, ed.FP32):
+        ham = ed.Hamiltonian(n, n // 2, bonds, precision=prec)
+        x = np.random.default_rng(seed).normal(size=ham.dim)
+        xd, yd = ham.new_vector().upload(x), ham.new_vector()
+        outs = []
+        for v in _apply_variants(ham):
+            ham.time_apply(xd, yd, 1, v)
+            outs.append(yd.download())
+        for o in outs[1:]:
+            assert np.array_equal(o, outs[0])
+        if prec == ed.FP64:
+            assert np.array_equal(outs[0], oracle.Matrix(n, n // 2, bonds).mult(x))
+
+
+@pytest.mark.parametrize("prec", [ed.FP64, ed.FP32])
+def test_lanczos_step_alpha_identical_across_variants(prec, monkeypatch):
+    """The fused <x, y> partials and |w| are formed in a fixed order: alpha and beta agree bit for
+    bit whichever apply variant the autotuner picks."""
+    n, bonds = random_bonds("square lattice", {"L": 4, "W": 5}, 7, 0.8, 1.2)
+    rng = np.random.default_rng(8)
+    got = []
+    probe = ed.Hamiltonian(n, n // 2, bonds, precision=prec)
+    vs = _apply_variants(probe)
+    v0 = rng.normal(size=probe.dim)
+    v0 /= np.linalg.norm(v0)
+    probe.close()
+    for v in vs:
+        monkeypatch.setenv("AED_HV_VARIANT", str(v))
+        ham = ed.Hamiltonian(n, n // 2, bonds, precision=prec)
+        cur, nxt = ham.new_vector().upload(v0), ham.new_vector()
+        got.append((ham.lanczos_step(None, cur, nxt, 0.0), nxt.download()))
+        ham.close()
+    for (ab, w) in got[1:]:
+        assert ab == got[0][0]
+        assert np.array_equal(w, got[0][1])
+
+
 def _fp32_bound(M, x):
     rp, col, val = M.csr()
     absrow = np.add.reduceat(np.abs(val) * np.abs(x[col]), rp[:-1])
