@@ -50,8 +50,7 @@ namespace apply {
 // "Dot2") is kept as AccTwoSum.
 // ---------------------------------------------------------------------------
 constexpr int kTileRows = kHvTileRows;
-constexpr uint32_t kDiagOp = 0xffffffffu;
-constexpr uint32_t kXorCond = 0xffffu;  // lo-part condition: the two bits differ
+constexpr uint32_t kCrossOp = 1u << 14;  // program entry of a crossing flip (ordered programs)
 constexpr int kMaxOps = 2 * kMaxBonds + 1;
 
 struct SPair {
@@ -59,8 +58,11 @@ struct SPair {
   double c;
 };
 
-// One program entry: mc = lo-part flip | (lo-part condition << 16), or
-// kDiagOp; nb = base row of the target hi block; c = coupling.
+// One program entry.  Hi-part flip: mc = 0, nb = base row of the target hi
+// block (target row nb + r).  Crossing flip: mc = lo bit b << 16 | required
+// lo-bit value v << 15 (| kCrossOp in ordered programs), nb = target base -
+// (v << 15), so that the target row is nb + (crossing-flip table entry).
+// c = coupling.
 struct TileOp {
   uint32_t mc, nb;
   double c;
@@ -95,7 +97,8 @@ struct AccTwoSum32 {  // FP32 vectors, TwoSum + exact product error in FP32
 };
 
 // Warp 0: append to prog the entries of `list` that can apply in hi block h
-// (FP64 order: cond fixes which of the two bits must be set).
+// (FP64 order: cond fixes which of the two bits must be set).  Hi-part flips
+// get mc = 0; crossing flips get kCrossOp with the encoding of compile_any.
 __device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32_t h, int Nlo, uint32_t lm,
                                                const uint32_t* __restrict__ thi, TileOp* prog, int cnt) {
   const int lane = threadIdx.x & 31;
@@ -108,7 +111,13 @@ __device__ __forceinline__ int compile_ordered(const SPair* list, int np, uint32
       const uint32_t fhi = e.flip >> Nlo, chi = e.cond >> Nlo;
       if (fhi != 0u && (h & fhi) == chi) {  // lo-part flips come from the lo-neighbour table
         emit = true;
-        op = {(e.flip & lm) | ((e.cond & lm) << 16), __ldg(thi + (h ^ fhi)), e.c};
+        const uint32_t flo = e.flip & lm, nb = __ldg(thi + (h ^ fhi));
+        if (flo == 0u) {  // hi part only: every row of the tile, target row nb + r
+          op = {0u, nb, e.c};
+        } else {  // crossing: the row's lo bit must equal the condition's (crossing-flip table)
+          const uint32_t v = (e.cond & lm) != 0u ? 1u : 0u;
+          op = {kCrossOp | ((uint32_t)(__ffs(flo) - 1) << 16) | (v << 15), nb - (v << 15), e.c};
+        }
       }
     }
     const unsigned m = __ballot_sync(0xffffffffu, emit);
@@ -154,34 +163,58 @@ __device__ __forceinline__ int compile_any(const SPair* list, int np, uint32_t h
   return cnt;
 }
 
+// FP64 rows: the program's flips in program (column) order.  The x values of
+// four flips are loaded before their terms are added, in order.  xt: as for
+// run_cross.
 template <typename T, typename Acc, int R>
-__device__ __forceinline__ void run_ops(const TileOp* prog, int o0, int o1, const uint32_t* lv, uint32_t nrow,
-                                        uint32_t rt, const double* __restrict__ dg, uint32_t base,
-                                        const uint16_t* __restrict__ tlo, const T* __restrict__ x, Acc* acc) {
-  for (int o = o0; o < o1; ++o) {
+__device__ __forceinline__ void run_ordered(const TileOp* prog, int o0, int o1, const uint16_t* __restrict__ xt,
+                                            uint32_t nlo, uint32_t nrow, uint32_t rt, const T* __restrict__ x,
+                                            Acc* acc) {
+  constexpr int U = R >= 8 ? 1 : 8 / R;  // about eight loads in flight per thread
+  int o = o0;
+  for (; o + U <= o1; o += U) {
+    TileOp e[U];
+    bool p[U][R];
+    T xv[U][R];
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+      e[v] = prog[o + v];
+      if (e[v].mc & kCrossOp) {
+        const uint16_t* xb = xt + (size_t)((e[v].mc >> 16) & 0xffffu) * nlo;
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          const uint32_t ent = (uint32_t)u < nrow ? (uint32_t)__ldg(xb + u * kHvThreads) : (~e[v].mc & 0x8000u);
+          p[v][u] = ((ent ^ e[v].mc) & 0x8000u) == 0u;
+          xv[v][u] = p[v][u] ? __ldg(x + (e[v].nb + ent)) : T(0);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          p[v][u] = (uint32_t)u < nrow;
+          xv[v][u] = p[v][u] ? __ldg(x + e[v].nb + rt + u * kHvThreads) : T(0);
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < U; ++v)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p[v][u]) acc[u].add(e[v].c, xv[v][u]);
+  }
+  for (; o < o1; ++o) {
     const TileOp e = prog[o];
-    const uint32_t fl = e.mc & 0xffffu, cd = e.mc >> 16;
-    if (e.mc == kDiagOp) {
+    if (e.mc & kCrossOp) {
+      const uint16_t* xb = xt + (size_t)((e.mc >> 16) & 0xffffu) * nlo;
 #pragma unroll
       for (int u = 0; u < R; ++u)
         if ((uint32_t)u < nrow) {
-          const uint32_t i = base + rt + u * kHvThreads;
-          acc[u].add(__ldg(dg + i), __ldg(x + i));
+          const uint32_t ent = __ldg(xb + u * kHvThreads);
+          if (((ent ^ e.mc) & 0x8000u) == 0u) acc[u].add(e.c, __ldg(x + (e.nb + ent)));
         }
-    } else if (fl == 0u) {
-#pragma unroll
-      for (int u = 0; u < R; ++u)
-        if ((uint32_t)u < nrow) acc[u].add(e.c, __ldg(x + e.nb + rt + u * kHvThreads));
-    } else if (cd == kXorCond) {
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const uint32_t b = lv[u] & fl;
-        if ((uint32_t)u < nrow && b != 0u && b != fl) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
-      }
     } else {
 #pragma unroll
       for (int u = 0; u < R; ++u)
-        if ((uint32_t)u < nrow && (lv[u] & fl) == cd) acc[u].add(e.c, __ldg(x + e.nb + __ldg(tlo + (lv[u] ^ fl))));
+        if ((uint32_t)u < nrow) acc[u].add(e.c, __ldg(x + e.nb + rt + u * kHvThreads));
     }
   }
 }
@@ -390,14 +423,11 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
 #pragma unroll 1
   for (int pass = 0; pass < kPasses; ++pass) {
     const uint32_t rt = r0 + pass * (kHvThreads * R) + threadIdx.x;  // row offset of u = 0
-    uint32_t lv[R];
     uint32_t nrow = 0;  // rows of this thread that exist (a prefix of u)
 #pragma unroll
     for (int u = 0; u < R; ++u) {
       const uint32_t r = rt + u * kHvThreads;
-      const bool ok = r < rows && r < r0 + kTileRows;
-      nrow += ok ? 1u : 0u;
-      lv[u] = (kOrdered && ok) ? (uint32_t)__ldg(t.lolist + lbase + r) : 0u;  // FP32 rows use the tables only
+      nrow += (r < rows && r < r0 + kTileRows) ? 1u : 0u;
     }
     Acc acc[R];
     bool dd[R];
@@ -406,7 +436,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
     if (kOrdered) {
       // flips to smaller states outside the lo part, then the lo-part flips
       // with the diagonal at its column, then the larger states outside
-      run_ops<T, Acc, R>(sm.prog, 0, nlow, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+      run_ordered<T, Acc, R>(sm.prog, 0, nlow, t.xtab + lbase + rt, 1u << c.Nlo, nrow, rt, x, acc);
       run_lo_table<T, Acc, R, true>(t, lbase, rows, base, rt, nrow, sm.lolo_c, x, acc, dd);
 #pragma unroll
       for (int u = 0; u < R; ++u)
@@ -414,7 +444,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
           const uint32_t i = base + rt + u * kHvThreads;
           acc[u].add(__ldg(t.dg + i), __ldg(x + i));
         }
-      run_ops<T, Acc, R>(sm.prog, nlow, nops, lv, nrow, rt, t.dg, base, t.tlo, x, acc);
+      run_ordered<T, Acc, R>(sm.prog, nlow, nops, t.xtab + lbase + rt, 1u << c.Nlo, nrow, rt, x, acc);
     } else {
 #pragma unroll
       for (int u = 0; u < R; ++u)

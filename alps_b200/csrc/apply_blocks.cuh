@@ -137,14 +137,12 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
   }
   Acc acc[B][R];
   if (kOrdered) {
-    uint32_t lv[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) lv[u] = (uint32_t)u < nrow ? (uint32_t)__ldg(t.lolist + q.lbase + rt + u * kHvThreads) : 0u;
     // flips to smaller states outside the lo part; the lo part with the
     // diagonal at its column; the larger states outside the lo part
 #pragma unroll
     for (int j = 0; j < B; ++j)
-      if (j < nv) apply::run_ops<T, Acc, R>(sm.prog[j], 0, q.nlow[j], lv, nrow, rt, t.dg, q.bj[j], t.tlo, x, acc[j]);
+      if (j < nv)
+        apply::run_ordered<T, Acc, R>(sm.prog[j], 0, q.nlow[j], t.xtab + q.lbase + rt, 1u << c.Nlo, nrow, rt, x, acc[j]);
     bool dd[R];
 #pragma unroll
     for (int u = 0; u < R; ++u) dd[u] = false;
@@ -187,7 +185,8 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
 #pragma unroll
     for (int j = 0; j < B; ++j)
       if (j < nv)
-        apply::run_ops<T, Acc, R>(sm.prog[j], q.nlow[j], q.nops[j], lv, nrow, rt, t.dg, q.bj[j], t.tlo, x, acc[j]);
+        apply::run_ordered<T, Acc, R>(sm.prog[j], q.nlow[j], q.nops[j], t.xtab + q.lbase + rt, 1u << c.Nlo, nrow, rt,
+                                      x, acc[j]);
   } else {
 #pragma unroll
     for (int u = 0; u < R; ++u) {
