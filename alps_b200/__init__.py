@@ -144,6 +144,8 @@ def lib():
             "aed_last_tmatrix": (ctypes.c_int, [_P, _DP, _DP, _I32, _I32P]),
             "aed_time_mult": (ctypes.c_int, [_P, _P, _P, _I32, _DP]),
             "aed_time_apply": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _DP, _I32P]),
+            "aed_apply_variant_count": (_I32, []),
+            "aed_apply_variant_name": (ctypes.c_char_p, [_I32]),
             "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
             "aed_launch_count": (ctypes.c_int, [_I64P]),
             "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
@@ -186,6 +188,12 @@ def tmatrix(alpha, beta):
     _check(lib().aed_tmatrix(n, _dp(a), _dp(b), n, _dp(ev), _dp(er), mu.ctypes.data_as(_I32P), ctypes.byref(cnt)))
     c = cnt.value
     return {"evals": ev[:c], "errors": er[:c], "mults": mu[:c]}
+
+
+def apply_variants() -> list:
+    """Names of the apply variants (index = the `variant` of Hamiltonian.time_apply)."""
+    L = lib()
+    return [L.aed_apply_variant_name(v).decode() for v in range(L.aed_apply_variant_count())]
 
 
 def launch_count() -> int:

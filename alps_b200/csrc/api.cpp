@@ -674,6 +674,12 @@ int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t 
   return AED_OK;
 }
 
+int32_t aed_apply_variant_count(void) { return hv_num_variants(); }
+
+const char* aed_apply_variant_name(int32_t variant) {
+  return (variant >= 0 && variant < hv_num_variants()) ? hv_variant_name(variant) : nullptr;
+}
+
 int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* ms) {
   int rc = check_vec(h, x, "x");
   if (!rc) rc = check_vec(h, y, "y");

@@ -173,10 +173,10 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
   }
   const int nev = I.nev;
   double ev[AED_MAX_NEV + 1], er[AED_MAX_NEV + 1];
-  int first[AED_MAX_NEV + 1];
+  int first[AED_MAX_NEV + 1], mults[AED_MAX_NEV + 1];
   tcore::TResult res;
   const int want = nev + 1;
-  const bool bad = tcore::analyze(m, al, be, amax, bmax, work, want, ev, er, nullptr, first, &res,
+  const bool bad = tcore::analyze(m, al, be, amax, bmax, work, want, ev, er, mults, first, &res,
                                   I.phase == kPhLow ? kFp32MergeRel : 0.0) != 0;
   const int cnt = res.count;
   bool conv = !bad && cnt >= nev;
@@ -185,15 +185,19 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
       if (!(er[i] <= tcore::dmax(I.tol32 * 1e-3, I.tol32 * fabs(ev[i])))) conv = false;
     const bool full = !stepping(I);
     if (!(conv || full || bad)) return;
-    // Ritz coefficients: sum of the unit eigenvectors of T(m) of the nev
-    // lowest distinct values
+    // Ritz coefficients: the unit eigenvectors of T(m) with sorted indices
+    // [0, K) (the nev lowest distinct values and one guard, whole clusters:
+    // tcore::ritz_span) with seeded weights; work[0..m) holds the sorted
+    // eigenvalues of T after analyze
     const int n1 = cnt < nev ? cnt : nev;
     for (int q = 0; q < m; ++q) I.coef[q] = 0.0;
-    for (int i = 0; i < n1; ++i) {
-      tcore::inverse_iteration(m, al, be, ev[i], z, inv);
-      for (int q = 0; q < m; ++q) I.coef[q] += z[q];
+    const int K = bad ? 0 : tcore::ritz_span(cnt, nev, first, mults, m);
+    for (int k = 0; k < K; ++k) {
+      tcore::inverse_iteration(m, al, be, work[k], z, inv);
+      const double w = tcore::ritz_weight(I.seed, k);
+      for (int q = 0; q < m; ++q) I.coef[q] += w * z[q];
     }
-    if (n1 == 0) I.coef[0] = 1.0;
+    if (K == 0) I.coef[0] = 1.0;
     for (int i = 0; i < n1; ++i) I.evals_low[i] = ev[i];
     I.m_low = m;
     I.phase = kPhRitz;

@@ -44,6 +44,7 @@ struct BInst {
   double tol32;       // FP32 phase: residual estimate <= tol32 * |lambda|
   double etol;        // FP64 phase: r^2 / gap <= etol * |lambda| (0: ietl rule only)
   double rtol, atol;  // ietl rule
+  uint64_t seed;      // the request's seed (start vector, Ritz weights)
   float* chunk[kBatchMaxChunks];
   double* v64[3];     // FP64 vectors (rotating)
   double* partA;      // n_tiles

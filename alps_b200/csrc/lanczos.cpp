@@ -24,6 +24,7 @@
 #include <cstring>
 
 #include "handle.h"
+#include "tmatrix_core.h"
 
 namespace aed {
 namespace {
@@ -355,15 +356,17 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   for (int i = 0; i < n1; ++i) r->evals_low[i] = T1.evals[i];
   r->iterations_low = m1;
   const double apply32_ms = profile ? R.apply_ms() : 0.0;
-  // Ritz vectors: eigenvectors of T(m1), combined with equal weights, accumulated
-  // in FP64 chunk by chunk from the stored basis
+  // Ritz start: the eigenvectors of T(m1) up to the end of the (nev+1)-th
+  // distinct cluster with seeded weights (tcore::ritz_span / ritz_weight),
+  // accumulated in FP64 chunk by chunk from the stored basis
   std::vector<double> ev(R.alpha.begin(), R.alpha.begin() + m1), e(m1 + 1, 0.0), Z((size_t)m1 * m1);
   for (int i = 0; i + 1 < m1; ++i) e[i] = R.beta[i];
   if (tridiag_eigen(m1, ev.data(), e.data(), nullptr, Z.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  const int K = tcore::ritz_span((int)T1.evals.size(), nev, T1.first.data(), T1.mults.data(), m1);
   std::vector<double> c(m1, 0.0);
-  for (int i = 0; i < n1; ++i) {
-    const int k = T1.first[i];
-    for (int j = 0; j < m1; ++j) c[j] += Z[(size_t)k * m1 + j];
+  for (int k = 0; k < K; ++k) {
+    const double w = tcore::ritz_weight(seed, k);
+    for (int j = 0; j < m1; ++j) c[j] += w * Z[(size_t)k * m1 + j];
   }
   for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
     const int cnt = std::min(kStoreChunk, m1 - j0);

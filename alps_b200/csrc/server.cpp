@@ -261,6 +261,7 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   I.n_tiles = (int32_t)sec->n_tiles;
   I.n_chunks = red_chunks(D);
   const double eps = 2.220446049250313e-16;
+  I.seed = r->opts.seed;
   I.rtol = r->opts.rtol > 0 ? r->opts.rtol : 100 * eps;
   I.atol = r->opts.atol > 0 ? r->opts.atol : 100 * eps;
   I.tol32 = 2e-6;

@@ -192,6 +192,31 @@ AED_HD inline int analyze(int n, const double* alpha, const double* beta, double
   return 0;
 }
 
+// Start of the FP64 refinement of the mixed path: the eigenvectors of T with
+// sorted indices [0, K) are combined, where K ends the (nev+1)-th distinct
+// value's cluster (the nev wanted and one guard).  A cluster holds ghost copies
+// and any pair closer than the FP32 phase resolves, so the partner of a
+// near-degenerate pair is kept.  first / mults: analyze's output (count values).
+AED_HD inline int ritz_span(int count, int nev, const int* first, const int* mults, int n) {
+  const int c = count < nev + 1 ? count : nev + 1;
+  if (c <= 0) return n < 1 ? 0 : 1;
+  const int K = first[c - 1] + (mults[c - 1] > 0 ? mults[c - 1] : 1);
+  return K < n ? K : n;
+}
+
+// Weight of the k-th eigenvector in that combination: +-[0.5, 1.5) from the
+// splitmix64 sequence (Steele, Lea & Flood, OOPSLA 2014) of the solve's seed.
+// Unit weights could cancel two copies of one eigenvector; these cannot, and
+// the start stays reproducible.
+AED_HD inline double ritz_weight(unsigned long long seed, int k) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(k + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  return ((z >> 10) & 1ull ? -1.0 : 1.0) * (0.5 + u);
+}
+
 // Eigenvector z of the tridiagonal (alpha, beta[0..n-2]) for eigenvalue lam by
 // inverse iteration with a partially pivoted LU of T - lam I (two sweeps),
 // normalised.  scratch: 6*n doubles.

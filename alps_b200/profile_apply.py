@@ -52,23 +52,20 @@ def main():
     ham = ed.Hamiltonian(N, n_up, bonds, precision=prec)
     x, y = ham.new_vector(), ham.new_vector()
     ham.fill_random(x, 1)
+    names = ed.apply_variants()
     if a.sweep:
-        v = 0
-        while True:
+        for v, name in enumerate(names):
             try:
                 m0, _ = ham.time_apply(x, y, a.reps, v, False)
                 m1, _ = ham.time_apply(x, y, a.reps, v, True)
-                print(f"{a.workload} {a.precision} variant {v}: apply_ms={m0:.4f} with_alpha_ms={m1:.4f}")
+                print(f"{a.workload} {a.precision} variant {v} ({name}): apply_ms={m0:.4f} with_alpha_ms={m1:.4f}")
             except ed.AEDError as e:
-                if "unknown" in str(e):
-                    break
-                print(f"{a.workload} {a.precision} variant {v}: {e}")
-            v += 1
+                print(f"{a.workload} {a.precision} variant {v} ({name}): {e}")
         return
     if a.warmup:
         ham.time_apply(x, y, a.warmup, a.variant, a.alpha)
     ms, v = ham.time_apply(x, y, a.reps, a.variant, a.alpha)
-    print(f"{a.workload} {a.precision} D={ham.dim} variant={v} alpha={int(a.alpha)} apply_ms={ms:.4f}")
+    print(f"{a.workload} {a.precision} D={ham.dim} variant={v} ({names[v]}) alpha={int(a.alpha)} apply_ms={ms:.4f}")
 
 
 if __name__ == "__main__":

@@ -52,9 +52,9 @@ NEV = 2
 FP64_ITERATIONS_FALLBACK = 180  # mean of the first five inputs: 190, 142, 180, 182, 208
 
 # DRAM bytes (read + write) of one launch of the FP64 apply on this workload,
-# from ncu (dram__bytes_read.sum + dram__bytes_write.sum), summarised in
-# profiles/hv_kernel_l28_fp64.md.  None until captured.
-HV_TRAFFIC_L28_FP64 = 3.051806e9
+# per apply variant, from ncu (dram__bytes_read.sum + dram__bytes_write.sum),
+# summarised in profiles/hvb_kernel_l28_fp64.md; null for a variant not captured.
+HV_TRAFFIC_L28_FP64 = {"blk1r4b3": 2.238548e9}
 
 
 def j2_stream(n):
@@ -68,6 +68,28 @@ def chain_bonds(L, j2):
         out.append((i, (i + 1) % L, 1.0, 1.0, 0.0))
         out.append((i, (i + 2) % L, float(j2), float(j2), 0.0))
     return out
+
+
+def table_upload_bytes(N, n_up, bonds):
+    """Host->device bytes of the sector and coupling tables that aed_create copies: thi, tlo,
+    lolist, looff, tiles (h, r), bundle block list, first tile per hi block, crossing-flip table,
+    lo-neighbour table, per-step scalars."""
+    nlo = (N + 1) // 2
+    nhi = N - nlo
+    pc = [bin(v).count("1") for v in range(1 << nlo)]
+    cnt = [comb(nlo, k) for k in range(nlo + 1)]
+    ks = [k for k in range(nlo + 1) if 0 <= n_up - k <= nhi]
+    n_tiles = sum(comb(nhi, n_up - k) * -(-cnt[k] // 2048) for k in ks)
+    n_blk = sum(-(-comb(nhi, n_up - k) // 4) * 4 for k in ks)
+    lo_pairs = set()
+    for b in bonds:
+        s, t = sorted((b[0], b[1]))
+        if s >= nhi and b[3] != 0.0:
+            lo_pairs.add((N - 1 - s, N - 1 - t))
+    masks = [(1 << i) | (1 << j) for i, j in lo_pairs]
+    width = max((sum(1 for m in masks if pc[l & m] == 1) for l in range(1 << nlo)), default=0)
+    return ((1 << nhi) * 4 + 2 * (1 << nlo) * 2 + (nlo + 2) * 4 + n_tiles * 8 + n_blk * 4 + (1 << nhi) * 4
+            + nlo * (1 << nlo) * 2 + width * (1 << nlo) * 4)
 
 
 def pair_offdiag_mean(N, n_up, bonds):
@@ -86,15 +108,6 @@ def read_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def read_traffic(kernel_key):
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        with open(p) as f:
-            return json.load(f).get(kernel_key)
-    except Exception:
-        return None
 
 
 class ClockSampler:
@@ -275,10 +288,16 @@ def run_ours(args):
     t_apply = float(np.mean(apply_ms)) / 1e3
     peak, peak_kind = read_peaks()
     achieved = b_apply / t_apply / 1e9
+    xv, yv = ham.new_vector(), ham.new_vector()  # the tuned apply variant (no launch: already tuned)
+    ham.fill_random(xv, 1)
+    _, vused = ham.time_apply(xv, yv, 1)
+    xv.free()
+    yv.free()
+    vname = ed.apply_variants()[vused]
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "kernel": "hv_kernel<double>", "apply_ms": t_apply * 1e3,
-            "algorithmic_bytes_per_apply": b_apply, "traffic": HV_TRAFFIC_L28_FP64,
-            "traffic_source": "profiles/hv_kernel_l28_fp64.md (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+            "peak_kind": peak_kind, "kernel": f"apply variant {vname} (FP64)", "apply_ms": t_apply * 1e3,
+            "algorithmic_bytes_per_apply": b_apply, "traffic": HV_TRAFFIC_L28_FP64.get(vname),
+            "traffic_source": "profiles/hvb_kernel_l28_fp64.md (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                               "one launch)"}
     print(f"[bench] fp64: {value:.3f} solves/s, iterations {iters}, apply {t_apply*1e3:.3f} ms "
           f"({achieved:.0f} GB/s)", file=sys.stderr)
@@ -287,8 +306,6 @@ def run_ours(args):
     # + eigenvalues and the alpha/beta stream (D2H) + aed_destroy
     start = torch.empty(D, dtype=torch.float64, pin_memory=True)
     start.numpy()[:] = np.random.default_rng(7).uniform(0, 1, D)
-    nlo = (N + 1) // 2
-    table_bytes = (1 << (N - nlo)) * 4 + 2 * (1 << nlo) * 2 + (nlo + 2) * 4 + 8 * ((D + 2047) // 2048 + (1 << (N - nlo)))
     h2d = d2h = 0
     barrier(pg)
     t0 = time.perf_counter()
@@ -297,7 +314,7 @@ def run_ours(args):
         h = ed.Hamiltonian(N, n_up, bonds, precision=ed.FP64, device=local)
         r = h.solve(nev=NEV, start=start.numpy())
         h.close()
-        h2d += D * 8 + table_bytes + len(bonds) * 32
+        h2d += D * 8 + table_upload_bytes(N, n_up, bonds) + 16
         d2h += 16 * (r["iterations"] + 1) + 32 * NEV
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(pg, time.perf_counter() - t0)

@@ -205,6 +205,12 @@ int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* m
 int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t variant, int32_t with_alpha,
                    double* ms, int32_t* variant_used);
 
+/* Apply variants (the kernel shapes that the autotuner times on a handle's
+ * first apply): their number, and the name of variant `variant` (NULL when out
+ * of range).  Engine addition, no reference counterpart. */
+int32_t aed_apply_variant_count(void);
+const char* aed_apply_variant_name(int32_t variant);
+
 /* ---- batched / served solves ------------------------------------------------
  * Many independent requests (a model and solve options each) advance together
  * on one GPU: every engine step runs one Lanczos step of every resident

@@ -34,6 +34,13 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_apply_variant_names():
+    names = ed.apply_variants()
+    assert len(names) >= 12 and len(set(names)) == len(names)
+    assert ed.lib().aed_apply_variant_name(len(names)) is None
+    assert ed.lib().aed_apply_variant_name(-1) is None
+
+
 PARAM_CASES = [
     {"LATTICE": "chain lattice", "L": 16, "J": 1},
     {"LATTICE": "open chain lattice", "L": 10, "J": 0.7},
