@@ -69,7 +69,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [
         ("nev", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("rtol", ctypes.c_double),
         ("atol", ctypes.c_double), ("seed", ctypes.c_uint64), ("start", ctypes.POINTER(ctypes.c_double)),
-        ("refine", ctypes.c_int32), ("profile", ctypes.c_int32),
+        ("refine", ctypes.c_int32), ("profile", ctypes.c_int32), ("resume", ctypes.c_int32),
     ]
 
 
@@ -142,6 +142,10 @@ def lib():
             "aed_lanczos_step": (ctypes.c_int, [_P, _P, _P, _P, _D, _DP, _DP]),
             "aed_solve": (ctypes.c_int, [_P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult)]),
             "aed_last_tmatrix": (ctypes.c_int, [_P, _DP, _DP, _I32, _I32P]),
+            "aed_eigenvectors": (ctypes.c_int, [_P, ctypes.POINTER(SolveOpts), _I32, ctypes.POINTER(_P), _DP, _DP]),
+            "aed_lanczos_state_bytes": (ctypes.c_int, [_P, _I64P]),
+            "aed_lanczos_save": (ctypes.c_int, [_P, ctypes.c_void_p, _I64]),
+            "aed_lanczos_load": (ctypes.c_int, [_P, ctypes.c_char_p, _I64]),
             "aed_time_mult": (ctypes.c_int, [_P, _P, _P, _I32, _DP]),
             "aed_time_apply": (ctypes.c_int, [_P, _P, _P, _I32, _I32, _I32, _DP, _I32P]),
             "aed_apply_variant_count": (_I32, []),
@@ -404,9 +408,12 @@ class Hamiltonian:
         return ms.value
 
     # -- solves ---------------------------------------------------------------------
-    def solve(self, nev=1, max_iter=0, seed=0, start=None, rtol=0.0, atol=0.0, refine=0, profile=False):
+    def solve(self, nev=1, max_iter=0, seed=0, start=None, rtol=0.0, atol=0.0, refine=0, profile=False,
+              resume=False):
+        """Lanczos eigenvalues (aed_solve).  resume=True continues the live FP64 recurrence (the last
+        solve's, or one restored by lanczos_load) until nev values converge."""
         st = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
-        opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0)
+        opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0, 1 if resume else 0)
         res = SolveResult()
         _check(lib().aed_solve(self._h, ctypes.byref(opts), ctypes.byref(res)))
         n = res.n_evals
@@ -414,6 +421,32 @@ class Hamiltonian:
                 "iterations": res.iterations, "iterations_low": res.iterations_low,
                 "evals_low": np.array(res.evals_low[:n]), "converged": bool(res.converged),
                 "seconds": res.seconds, "apply_ms": res.apply_ms}
+
+    def eigenvectors(self, k=1, seed=0, start=None):
+        """Ritz vectors of the k lowest eigenvalues of the last solve (aed_eigenvectors): the solve's
+        seed / start must be given again.  Returns (vectors, evals, residuals)."""
+        st = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
+        opts = SolveOpts(k, 0, 0.0, 0.0, seed, _dp(st), 0, 0, 0)
+        vecs = [self.new_vector() for _ in range(k)]
+        arr = (_P * k)(*[v.ptr for v in vecs])
+        ev = np.zeros(k)
+        rs = np.zeros(k)
+        _check(lib().aed_eigenvectors(self._h, ctypes.byref(opts), k, arr, _dp(ev), _dp(rs)))
+        return vecs, ev, rs
+
+    def lanczos_save(self) -> bytes:
+        """Checkpoint of the live FP64 recurrence (aed_lanczos_save)."""
+        n = ctypes.c_int64(0)
+        _check(lib().aed_lanczos_state_bytes(self._h, ctypes.byref(n)))
+        if n.value == 0:
+            raise AEDError(ERR_INVALID, "no live Lanczos recurrence")
+        buf = ctypes.create_string_buffer(n.value)
+        _check(lib().aed_lanczos_save(self._h, buf, n.value))
+        return buf.raw
+
+    def lanczos_load(self, state: bytes):
+        """Restore a checkpoint into this handle (aed_lanczos_load); solve(resume=True) continues it."""
+        _check(lib().aed_lanczos_load(self._h, state, len(state)))
 
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

@@ -45,6 +45,7 @@ void release(aed_handle* h) {
   cudaFree(h->d_partA);
   cudaFree(h->d_partB);
   cudaFree(h->d_scal);
+  cudaFree(h->d_start64);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -137,6 +138,7 @@ void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes) {
 }
 
 void handle_release_workspace(aed_handle* h) {
+  h->rec_live = false;
   for (void* p : h->store_chunks) cudaFree(p);
   h->store_chunks.clear();
   h->store_chunk_bytes = 0;
@@ -394,6 +396,11 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // no apply of the old couplings in flight
   h->model = m;
   h->P = P;
+  // the recurrence of the last solve belongs to the old Hamiltonian
+  h->last_alpha.clear();
+  h->last_beta.clear();
+  h->rec_m = 0;
+  h->rec_live = false;
   if ((rc = upload_lo_table(h))) return rc;
   rc = launch_diag_table(h->P, h->dt, h->d_dg, h->stream);
   if (rc) return rc;
@@ -628,6 +635,31 @@ int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res) 
   if (!h || !opts || !res) return fail(AED_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
   return solve(h, opts, res);
+}
+
+int aed_eigenvectors(aed_handle* h, const aed_solve_opts* opts, int32_t k, void* const* vecs, double* evals,
+                     double* residuals) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  return eigenvectors(h, opts, k, vecs, evals, residuals);
+}
+
+int aed_lanczos_state_bytes(aed_handle* h, int64_t* bytes) {
+  if (!h || !bytes) return fail(AED_ERR_INVALID, "NULL argument");
+  *bytes = lanczos_state_bytes(h);
+  return AED_OK;
+}
+
+int aed_lanczos_save(aed_handle* h, void* buf, int64_t bytes) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  return lanczos_save(h, buf, bytes);
+}
+
+int aed_lanczos_load(aed_handle* h, const void* buf, int64_t bytes) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  return lanczos_load(h, buf, bytes);
 }
 
 int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n) {

@@ -42,8 +42,14 @@ struct aed_handle {
   size_t store_chunk_bytes = 0;
   double* h_ab = nullptr;  // pinned alpha/beta staging
   size_t h_ab_n = 0;
-  // last solve
+  // last solve: the alpha/beta recurrence of its FP64 phase.  v_{m-1} and v_m
+  // of that recurrence stay in workspace slot 0 (buffers (m-1) % 3 and m % 3)
+  // while rec_live, for aed_lanczos_save and resumed solves.
   std::vector<double> last_alpha, last_beta;
+  int rec_m = 0;
+  bool rec_live = false;
+  bool last_mixed = false;      // the last solve was the mixed path
+  double* d_start64 = nullptr;  // mixed path: start vector of its FP64 phase (D doubles)
 };
 
 namespace aed {
@@ -74,6 +80,12 @@ constexpr int kStoreChunk = 16;
 // Pointer to chunk `c` of the FP32 basis store (allocated on first use), or nullptr.
 void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes);
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r);
+// Ritz vectors of the last solve by replaying its FP64 recurrence (lanczos.cpp).
+int eigenvectors(aed_handle* h, const aed_solve_opts* o, int k, void* const* vecs, double* evals, double* resid);
+// Serialised FP64 recurrence of the last solve (lanczos.cpp).
+int64_t lanczos_state_bytes(const aed_handle* h);
+int lanczos_save(aed_handle* h, void* buf, int64_t bytes);
+int lanczos_load(aed_handle* h, const void* buf, int64_t bytes);
 // One make_step on device vectors: apply, alpha, update, beta, normalise.
 // beta_prev / alpha / beta are device scalars; v_prev may be NULL.
 int lanczos_step_kernels(aed_handle* h, bool f32, const void* v_prev, const void* v_cur, void* v_next,

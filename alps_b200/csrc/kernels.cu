@@ -129,6 +129,12 @@ __global__ void fill_random_kernel(T* __restrict__ x, int64_t n, uint64_t seed) 
   }
 }
 
+// y = (float) x, round to nearest
+__global__ void round_to_f32_kernel(const double* __restrict__ x, float* __restrict__ y, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = __double2float_rn(x[i]);
+}
+
 template <typename T>
 __global__ void copy_kernel(const T* __restrict__ x, T* __restrict__ y, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -387,6 +393,11 @@ template <typename T>
 int launch_fill_random(T* x, int64_t n, uint64_t seed, cudaStream_t st) {
   fill_random_kernel<T><<<elem_grid(n), 256, 0, st>>>(x, n, seed);
   return check_launch("fill_random_kernel");
+}
+
+int launch_round_to_f32(const double* x, float* y, int64_t n, cudaStream_t st) {
+  round_to_f32_kernel<<<elem_grid(n), 256, 0, st>>>(x, y, n);
+  return check_launch("round_to_f32_kernel");
 }
 
 template <typename T>

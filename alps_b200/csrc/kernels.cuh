@@ -60,6 +60,7 @@ template <typename T>
 int launch_fill_random(T* x, int64_t n, uint64_t seed, cudaStream_t st);
 template <typename T>
 int launch_copy(const T* x, T* y, int64_t n, cudaStream_t st);
+int launch_round_to_f32(const double* x, float* y, int64_t n, cudaStream_t st);
 template <typename T>
 int launch_axpy(double a, const T* x, T* y, int64_t n, cudaStream_t st);
 template <typename T>

@@ -207,18 +207,27 @@ struct StopRule {
 };
 
 // Run a recurrence over rotating vector slots.  `slots(j)` gives the buffer
-// of v_j (v_0 already holds the normalised start vector).
+// of v_j.  m0 = 0: v_0 holds the normalised start vector.  m0 > 0 (resumed
+// run): R.alpha / R.beta and the device pairs hold steps 0 .. m0-1 and the
+// slots of v_{m0-1} and v_{m0} hold those vectors; T(m0) is tested first.
 template <typename SlotFn>
-int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters, int* failed, TmatInfo& T) {
+int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int* iters, int* failed,
+                   TmatInfo& T) {
   int launched = 0;
   int m = 1;
   *failed = 0;
-  void* s0 = slot(0);
-  void* s1 = slot(1);
-  if (!s0 || !s1) return AED_ERR_NOMEM;
-  int rc = R.launch_step(0, nullptr, s0, s1);
-  if (rc) return rc;
-  launched = 1;
+  int rc = AED_OK;
+  if (m0 == 0) {
+    void* s0 = slot(0);
+    void* s1 = slot(1);
+    if (!s0 || !s1) return AED_ERR_NOMEM;
+    rc = R.launch_step(0, nullptr, s0, s1);
+    if (rc) return rc;
+    launched = 1;
+  } else {
+    launched = m0;
+    m = m0;
+  }
   while (true) {
     // keep the device one step ahead of the host analysis
     while (launched < m + 1 && launched < R.max_iter) {
@@ -230,8 +239,10 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters,
       if (rc) return rc;
       ++launched;
     }
-    rc = R.wait_step(m - 1);
-    if (rc) return rc;
+    if (m > m0) {
+      rc = R.wait_step(m - 1);
+      if (rc) return rc;
+    }
     if (m > 1) {
       rc = tmatrix_analyze(m, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, R.f32 ? kFp32MergeRel : 0.0);
       if (rc) return rc;
@@ -252,22 +263,20 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int* iters,
   return AED_OK;
 }
 
-int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, int nev,
-               int max_iter, double rtol, double atol, bool energy_bound, double etol, int min_steps, bool profile,
-               aed_solve_result* r, TmatInfo& T) {
-  const int64_t D = h->tab.D;
-  EventRing ring;
-  int rc;
-  // workspace: three rotating vectors + the alpha/beta pairs
-  const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
+// The three rotating FP64 vectors of the recurrence in workspace slot 0.
+int recurrence_buffers(aed_handle* h, void* buf[3]) {
+  const size_t vb = ((size_t)h->tab.D * 8 + 255) & ~(size_t)255;
   void* ws = nullptr;
-  double* hab = nullptr;
-  if ((rc = handle_workspace(h, 0, 3 * vb + (size_t)2 * (max_iter + 2) * 8, &ws)) ||
-      (rc = handle_pinned(h, (size_t)2 * (max_iter + 2), &hab)) || (rc = ring.init()))
-    return rc;
-  void* buf[3] = {ws, (char*)ws + vb, (char*)ws + 2 * vb};
-  double* d_ab = (double*)((char*)ws + 3 * vb);
-  double* v0 = (double*)buf[0];
+  const int rc = handle_workspace(h, 0, 3 * vb, &ws);
+  if (rc) return rc;
+  for (int q = 0; q < 3; ++q) buf[q] = (char*)ws + q * vb;
+  return AED_OK;
+}
+
+// v_0 of a recurrence: copied from the device or the host, else seeded; normalised.
+int start_vector(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, double* v0) {
+  const int64_t D = h->tab.D;
+  int rc;
   if (start_dev) {
     AED_CUDA_TRY(cudaMemcpyAsync(v0, start_dev, D * 8, cudaMemcpyDeviceToDevice, h->stream));
   } else if (start_host) {
@@ -275,11 +284,50 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
   } else if ((rc = launch_fill_random(v0, D, seed, h->stream))) {
     return rc;
   }
-  if ((rc = normalize(h, v0, D))) return rc;
+  return normalize(h, v0, D);
+}
+
+// FP64 Lanczos (lanczos.h:341-406 with lanczos_iteration_nlowest).  resume:
+// continue the handle's live recurrence (last_alpha / last_beta, v_{m-1}, v_m)
+// instead of starting from a vector, like ietl's more_eigenvalues
+// (lanczos.h:77-78) after a load (lanczos.h:86-98).
+int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, int nev,
+               int max_iter, double rtol, double atol, bool energy_bound, double etol, int min_steps, bool profile,
+               aed_solve_result* r, TmatInfo& T, bool resume = false) {
+  const int64_t D = h->tab.D;
+  EventRing ring;
+  int rc;
+  const int m0 = resume ? h->rec_m : 0;
+  if (resume && (!h->rec_live || m0 < 1 || (int)h->last_alpha.size() != m0))
+    return fail(AED_ERR_INVALID, "no live Lanczos recurrence to resume (solve or aed_lanczos_load first)");
+  if (m0 >= max_iter) max_iter = m0 + 1;
+  void* buf[3];
+  DevMem ab;  // alpha/beta pairs of the device
+  double* hab = nullptr;
+  if ((rc = recurrence_buffers(h, buf)) || (rc = ab.alloc((size_t)2 * (max_iter + 2) * 8)) ||
+      (rc = handle_pinned(h, (size_t)2 * (max_iter + 2), &hab)) || (rc = ring.init()))
+    return rc;
+  double* d_ab = (double*)ab.p;
+  h->rec_live = false;  // from here on the slots change
   Recurrence R{h, false, D, max_iter, d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
+  if (resume) {
+    R.alpha = h->last_alpha;
+    R.beta = h->last_beta;
+    R.amax = *std::max_element(R.alpha.begin(), R.alpha.end());
+    R.bmax = *std::max_element(R.beta.begin(), R.beta.end());
+    std::vector<double> pairs((size_t)2 * m0);
+    for (int j = 0; j < m0; ++j) {
+      pairs[2 * j] = R.alpha[j];
+      pairs[2 * j + 1] = R.beta[j];
+    }
+    AED_CUDA_TRY(cudaMemcpyAsync(d_ab, pairs.data(), pairs.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // host pairs go out of scope
+  } else if ((rc = start_vector(h, start_host, start_dev, seed, (double*)buf[0]))) {
+    return rc;
+  }
   StopRule stop{nev, rtol, atol, energy_bound, etol, min_steps};
   int iters = 0, failed = 0;
-  rc = run_recurrence(R, stop, [&](int j) { return buf[j % 3]; }, &iters, &failed, T);
+  rc = run_recurrence(R, stop, [&](int j) { return buf[j % 3]; }, m0, &iters, &failed, T);
   if (rc) return rc;
   const int n = std::min(nev, (int)T.evals.size());
   r->n_evals = n;
@@ -290,8 +338,13 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
   r->iterations = iters;
   r->converged = failed ? 0 : 1;
   if (profile) r->apply_ms = R.apply_ms();
+  // the T of the stop (the extra step launched ahead of the analysis is discarded)
+  R.alpha.resize(iters);
+  R.beta.resize(iters);
   h->last_alpha = R.alpha;
   h->last_beta = R.beta;
+  h->rec_m = iters;
+  h->rec_live = true;
   return AED_OK;
 }
 
@@ -312,16 +365,24 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   const int cap = std::min(max_iter + 1, kMaxRitzTerms);
   HostPinned hab;
   EventRing ring;
-  DevMem small;  // start64 | alpha/beta pairs | Ritz coefficients
+  DevMem small;  // alpha/beta pairs | Ritz coefficients
   int rc;
-  const size_t s64 = (((size_t)D * 8 + 255) & ~(size_t)255);
   const size_t ab_bytes = (((size_t)2 * (cap + 2) * 8 + 255) & ~(size_t)255);
-  if ((rc = small.alloc(s64 + ab_bytes + (size_t)kStoreChunk * 8)) || (rc = hab.alloc((size_t)2 * (cap + 2))) ||
+  if ((rc = small.alloc(ab_bytes + (size_t)kStoreChunk * 8)) || (rc = hab.alloc((size_t)2 * (cap + 2))) ||
       (rc = ring.init()))
     return rc;
-  double* start64 = (double*)small.p;
-  double* d_ab = (double*)((char*)small.p + s64);
-  double* coef = (double*)((char*)small.p + s64 + ab_bytes);
+  // the FP64 phase's start stays with the handle (eigenvector replay)
+  if (!h->d_start64) {
+    const cudaError_t e = cudaMalloc((void**)&h->d_start64, (size_t)D * 8);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      h->d_start64 = nullptr;
+      return fail(AED_ERR_NOMEM, "device memory for the refinement start vector");
+    }
+  }
+  double* start64 = h->d_start64;
+  double* d_ab = (double*)small.p;
+  double* coef = (double*)((char*)small.p + ab_bytes);
   bool oom = false;
   auto slot = [&](int j) -> void* {
     char* c = (char*)handle_store_chunk(h, j / kStoreChunk, chunk_bytes);
@@ -348,7 +409,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
   int it1 = 0, failed1 = 0;
-  rc = run_recurrence(R, stop1, slot, &it1, &failed1, T1);
+  rc = run_recurrence(R, stop1, slot, 0, &it1, &failed1, T1);
   if (oom) return AED_ERR_NOMEM;
   if (rc) return rc;
   const int m1 = it1;
@@ -379,6 +440,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   TmatInfo T2;
   const int max2 = std::max(max_iter, nev + 4);
   rc = solve_fp64(h, nullptr, start64, seed, nev, max2, rtol, atol, true, kRefineEnergyTol, nev + 2, false, r, T2);
+  h->last_mixed = true;
   // apply_ms of a mixed solve: the FP32 applies (the bulk of the work)
   if (profile) r->apply_ms = apply32_ms;
   return rc;
@@ -419,15 +481,215 @@ int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
     const double eps = 2.220446049250313e-16;
     const double rtol = o->rtol > 0 ? o->rtol : 100 * eps;
     const double atol = o->atol > 0 ? o->atol : 100 * eps;
-    if (h->precision == AED_FP32 && o->refine != -1) {
+    if (o->resume) {  // continue the live FP64 recurrence (any handle precision)
+      TmatInfo T;
+      rc = solve_fp64(h, nullptr, nullptr, 0, nev, max_iter, rtol, atol, false, 0.0, 0, o->profile != 0, r, T, true);
+    } else if (h->precision == AED_FP32 && o->refine != -1) {
       rc = solve_mixed(h, o->start, o->seed, nev, max_iter, rtol, atol, o->profile != 0, r);
     } else {
       TmatInfo T;
       rc = solve_fp64(h, o->start, nullptr, o->seed, nev, max_iter, rtol, atol, false, 0.0, 0, o->profile != 0, r, T);
+      h->last_mixed = false;
     }
   }
   r->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return rc;
+}
+
+namespace {
+
+// |v| on the host (deterministic reduction, FP64 vector).
+int host_norm(aed_handle* h, const double* v, double* out) {
+  const int64_t D = h->tab.D;
+  int rc = launch_dot_partials(v, v, D, h->d_partB, true, h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(D), h->d_scal + 6, true, h->stream);
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal + 6, h->d_scal + 6, 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *out = h->h_scal[6];
+  return AED_OK;
+}
+
+// FNV-1a of the model (sector and couplings): a saved recurrence only loads
+// into a handle of the same Hamiltonian.
+uint64_t model_hash(const Model& m) {
+  uint64_t x = 1469598103934665603ull;
+  auto mix = [&](const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) x = (x ^ b[i]) * 1099511628211ull;
+  };
+  mix(&m.N, sizeof m.N);
+  mix(&m.n_up, sizeof m.n_up);
+  for (size_t b = 0; b < m.s1.size(); ++b) {
+    mix(&m.s1[b], sizeof(int));
+    mix(&m.s2[b], sizeof(int));
+    mix(&m.jz[b], 8);
+    mix(&m.jxy[b], 8);
+    mix(&m.kq[b], 8);
+  }
+  for (double v : m.site_h) mix(&v, 8);
+  for (double v : m.site_d) mix(&v, 8);
+  return x;
+}
+
+struct StateHeader {
+  char magic[8];
+  int64_t D;
+  int32_t N, n_up;
+  int32_t m, reserved;
+  uint64_t model;
+};
+constexpr char kStateMagic[8] = {'A', 'E', 'D', 'L', 'N', 'C', 'Z', '1'};
+
+}  // namespace
+
+// lanczos::eigenvectors (src/ietl/lanczos.h:134-336): the Lanczos vectors are
+// not stored, so the recurrence of the last solve is run again from its start
+// (the seeded or given vector of `o`; for a mixed solve the kept start of its
+// FP64 phase) and psi_i = sum_j z_i[j] v_j accumulates step by step, z_i the
+// eigenvector of T(m) of the i-th lowest distinct eigenvalue.  The replayed
+// alpha/beta must equal the stored ones bit for bit (lanczos.h:248-250,
+// 266-268), else AED_ERR_MISMATCH.  Then psi_i /= |psi_i| and the residual
+// |H psi_i - lambda_i psi_i| (lanczos.h:284-295).
+int eigenvectors(aed_handle* h, const aed_solve_opts* o, int k, void* const* vecs, double* evals, double* resid) {
+  if (!o || !vecs || k < 1) return fail(AED_ERR_INVALID, "eigenvectors: NULL argument or k < 1");
+  const int m = (int)h->last_alpha.size();
+  if (m < 1) return fail(AED_ERR_INVALID, "eigenvectors: no solve to take eigenvectors from");
+  for (int i = 0; i < k; ++i)
+    if (!vecs[i]) return fail(AED_ERR_INVALID, "eigenvectors: NULL output vector");
+  const int64_t D = h->tab.D;
+  const bool f32 = h->precision == AED_FP32;
+  const std::vector<double>& al = h->last_alpha;
+  const std::vector<double>& be = h->last_beta;
+  TmatInfo T;
+  int rc = tmatrix_analyze(m, al.data(), be.data(), *std::max_element(al.begin(), al.end()),
+                           *std::max_element(be.begin(), be.end()), T, 0.0);
+  if (rc) return rc;
+  if (k > (int)T.evals.size()) return fail(AED_ERR_INVALID, "eigenvectors: k exceeds the distinct eigenvalues found");
+  std::vector<double> ev(al), e(m + 1, 0.0), Z((size_t)m * m);
+  for (int i = 0; i + 1 < m; ++i) e[i] = be[i];
+  if (tridiag_eigen(m, ev.data(), e.data(), nullptr, Z.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
+  DevMem rb, dab;
+  if ((rc = rb.alloc((3 + (f32 ? k : 0)) * vb)) || (rc = dab.alloc((size_t)2 * m * 8))) return rc;
+  double* buf[3] = {(double*)rb.p, (double*)((char*)rb.p + vb), (double*)((char*)rb.p + 2 * vb)};
+  std::vector<double*> acc(k);
+  for (int i = 0; i < k; ++i) {
+    acc[i] = f32 ? (double*)((char*)rb.p + (3 + i) * vb) : (double*)vecs[i];
+    AED_CUDA_TRY(cudaMemsetAsync(acc[i], 0, (size_t)D * 8, h->stream));
+  }
+  if (h->last_mixed) {
+    if (!h->d_start64) return fail(AED_ERR_INVALID, "eigenvectors: the mixed solve's start is gone");
+    rc = start_vector(h, nullptr, h->d_start64, 0, buf[0]);
+  } else {
+    rc = start_vector(h, o->start, nullptr, o->seed, buf[0]);
+  }
+  if (rc) return rc;
+  double* d_ab = (double*)dab.p;
+  for (int j = 0; j < m; ++j) {
+    double* vj = buf[j % 3];
+    for (int i = 0; i < k; ++i)
+      if ((rc = launch_axpy<double>(Z[(size_t)T.first[i] * m + j], vj, acc[i], D, h->stream))) return rc;
+    if (j + 1 < m) {
+      double* w = buf[(j + 1) % 3];
+      const double* vp = j > 0 ? buf[(j + 2) % 3] : nullptr;
+      if ((rc = handle_hv(h, false, vj, w, h->d_partA))) return rc;
+      if ((rc = lanczos_step_tail(h, false, vp, vj, w, j > 0 ? d_ab + 2 * (j - 1) + 1 : nullptr, d_ab + 2 * j,
+                                  d_ab + 2 * j + 1)))
+        return rc;
+    }
+  }
+  if (m > 1) {
+    std::vector<double> rep((size_t)2 * (m - 1));
+    AED_CUDA_TRY(cudaMemcpyAsync(rep.data(), d_ab, rep.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int j = 0; j + 1 < m; ++j)
+      if (std::memcmp(&rep[2 * j], &al[j], 8) != 0 || std::memcmp(&rep[2 * j + 1], &be[j], 8) != 0)
+        return fail(AED_ERR_MISMATCH, "eigenvectors: the replayed recurrence differs from the solve's at step " +
+                                          std::to_string(j) + " (different start vector?)");
+  }
+  for (int i = 0; i < k; ++i) {
+    double nrm = 0.0;
+    if ((rc = host_norm(h, acc[i], &nrm))) return rc;
+    if (!(nrm > 0.0)) return fail(AED_ERR_INVALID, "eigenvectors: zero Ritz vector");
+    if ((rc = launch_scal<double>(nrm, acc[i], D, true, h->stream))) return rc;
+    double* w = buf[0];
+    if ((rc = handle_hv(h, false, acc[i], w, nullptr))) return rc;
+    if ((rc = launch_axpy<double>(-T.evals[i], acc[i], w, D, h->stream))) return rc;
+    double rn = 0.0;
+    if ((rc = host_norm(h, w, &rn))) return rc;
+    if (resid) resid[i] = rn;
+    if (evals) evals[i] = T.evals[i];
+    if (f32 && (rc = launch_round_to_f32(acc[i], (float*)vecs[i], D, h->stream))) return rc;
+  }
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
+int64_t lanczos_state_bytes(const aed_handle* h) {
+  if (!h->rec_live) return 0;
+  return (int64_t)sizeof(StateHeader) + (int64_t)16 * h->rec_m + (int64_t)16 * h->tab.D;
+}
+
+// Tmatrix::save + lanczos::save (src/ietl/tmatrix.h:66-77, lanczos.h:86-98):
+// the recurrence (alpha, beta) and the two live vectors v_{m-1}, v_m.
+int lanczos_save(aed_handle* h, void* buf, int64_t bytes) {
+  if (!buf) return fail(AED_ERR_INVALID, "lanczos_save: NULL buffer");
+  if (!h->rec_live) return fail(AED_ERR_INVALID, "lanczos_save: no live Lanczos recurrence (solve first)");
+  if (bytes < lanczos_state_bytes(h)) return fail(AED_ERR_INVALID, "lanczos_save: buffer too small");
+  const int m = h->rec_m;
+  const int64_t D = h->tab.D;
+  StateHeader hd{};
+  std::memcpy(hd.magic, kStateMagic, 8);
+  hd.D = D;
+  hd.N = h->model.N;
+  hd.n_up = h->model.n_up;
+  hd.m = m;
+  hd.model = model_hash(h->model);
+  char* p = (char*)buf;
+  std::memcpy(p, &hd, sizeof hd);
+  p += sizeof hd;
+  std::memcpy(p, h->last_alpha.data(), (size_t)m * 8);
+  p += (size_t)m * 8;
+  std::memcpy(p, h->last_beta.data(), (size_t)m * 8);
+  p += (size_t)m * 8;
+  void* slots[3];
+  int rc = recurrence_buffers(h, slots);
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(p, slots[(m - 1) % 3], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(p + (size_t)D * 8, slots[m % 3], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
+int lanczos_load(aed_handle* h, const void* buf, int64_t bytes) {
+  if (!buf || bytes < (int64_t)sizeof(StateHeader)) return fail(AED_ERR_INVALID, "lanczos_load: no state");
+  StateHeader hd;
+  std::memcpy(&hd, buf, sizeof hd);
+  if (std::memcmp(hd.magic, kStateMagic, 8) != 0) return fail(AED_ERR_INVALID, "lanczos_load: not a saved recurrence");
+  if (hd.D != h->tab.D || hd.N != h->model.N || hd.n_up != h->model.n_up || hd.model != model_hash(h->model))
+    return fail(AED_ERR_INVALID, "lanczos_load: the state belongs to a different Hamiltonian");
+  const int m = hd.m;
+  const int64_t D = hd.D;
+  if (m < 1 || bytes < (int64_t)sizeof hd + (int64_t)16 * m + (int64_t)16 * D)
+    return fail(AED_ERR_INVALID, "lanczos_load: truncated state");
+  const char* p = (const char*)buf + sizeof hd;
+  std::vector<double> al(m), be(m);
+  std::memcpy(al.data(), p, (size_t)m * 8);
+  std::memcpy(be.data(), p + (size_t)m * 8, (size_t)m * 8);
+  p += (size_t)16 * m;
+  void* slots[3];
+  int rc = recurrence_buffers(h, slots);
+  if (rc) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(slots[(m - 1) % 3], p, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(slots[m % 3], p + (size_t)D * 8, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->last_alpha = al;
+  h->last_beta = be;
+  h->rec_m = m;
+  h->rec_live = true;
+  h->last_mixed = false;
+  return AED_OK;
 }
 
 }  // namespace aed

@@ -163,6 +163,10 @@ typedef struct {
   int32_t refine;       /* AED_FP32 handles: 0 = mixed FP32 + FP64 refinement (default),
                            -1 = plain FP64 Lanczos on the same handle                  */
   int32_t profile;      /* 1: time every apply with CUDA events (res->apply_ms)         */
+  int32_t resume;       /* 1: continue the handle's live FP64 recurrence (the last solve's
+                           or one aed_lanczos_load restored) until the stop rule holds
+                           for nev values: ietl's more_eigenvalues (lanczos.h:77-78);
+                           start / seed / refine are then ignored                      */
 } aed_solve_opts;
 
 #define AED_MAX_NEV 16
@@ -183,6 +187,29 @@ typedef struct {
  * (src/ietl/lanczos.h:341-406), lanczos_iteration_nlowest (src/ietl/iteration.h:106-130)
  * and Tmatrix::compute's distinct/ghost rules (src/ietl/tmatrix.h:121-228). */
 int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res);
+
+/* Ritz vectors (lanczos::eigenvectors, src/ietl/lanczos.h:134-336) of the k
+ * lowest distinct eigenvalues of the last aed_solve (or resumed solve): its
+ * FP64 recurrence is run again from the same start -- `opts` must give the
+ * solve's seed or start vector; a mixed solve's FP64 phase restarts from the
+ * vector the handle kept -- and psi_i = sum_j z_i[j] v_j accumulates in FP64.
+ * The replayed alpha/beta must equal the solve's bit for bit
+ * (lanczos.h:248-250,266-268; AED_ERR_MISMATCH otherwise).  vecs[i]: device
+ * vectors of the handle (FP32 handles receive psi rounded to FP32); evals[i]
+ * and residuals[i] = |H psi_i - lambda_i psi_i| (lanczos.h:284-295), both
+ * optional.  The FP64 apply is used for AED_FP32 handles as well. */
+int aed_eigenvectors(aed_handle* h, const aed_solve_opts* opts, int32_t k, void* const* vecs, double* evals,
+                     double* residuals);
+
+/* Checkpoint of the live FP64 Lanczos recurrence: Tmatrix::save and
+ * lanczos::save (src/ietl/tmatrix.h:66-77, src/ietl/lanczos.h:86-98) -- alpha,
+ * beta, v_{m-1}, v_m and the step count -- into a host buffer of
+ * aed_lanczos_state_bytes bytes (0 when no recurrence is live).  A load
+ * checks that the state belongs to the same Hamiltonian (sector and
+ * couplings); an aed_solve with opts.resume = 1 then continues it. */
+int aed_lanczos_state_bytes(aed_handle* h, int64_t* bytes);
+int aed_lanczos_save(aed_handle* h, void* buf, int64_t bytes);
+int aed_lanczos_load(aed_handle* h, const void* buf, int64_t bytes);
 
 /* Copy the alpha/beta recurrence of the last aed_solve (FP64 phase) to host;
  * *n receives its length (at most cap entries are written). */
