@@ -56,13 +56,15 @@ int upload_lo_table(aed_handle* h) {
   std::vector<uint32_t> ell;
   int W = 0;
   build_lo_table(h->tab, h->P, ell, &W);
-  if (h->d_ell) {
-    cudaStreamSynchronize(h->stream);
+  cudaStreamSynchronize(h->stream);  // no apply reads the old table any more
+  if (ell.size() + 1 > h->d_ell_n) {  // grow only: new couplings usually keep the width
     cudaFree(h->d_ell);
     h->d_ell = nullptr;
+    h->d_ell_n = 0;
+    const int rc = dev_alloc(&h->d_ell, ell.size() + 1);
+    if (rc) return rc;
+    h->d_ell_n = ell.size() + 1;
   }
-  int rc = dev_alloc(&h->d_ell, ell.size() + 1);
-  if (rc) return rc;
   if (!ell.empty()) {
     AED_CUDA_TRY(cudaMemcpyAsync(h->d_ell, ell.data(), ell.size() * 4, cudaMemcpyHostToDevice, h->stream));
     AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // host vector goes out of scope

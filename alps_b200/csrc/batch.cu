@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
     const bool full = !stepping(I);
     if (!(conv || full || bad)) return;
     // Ritz coefficients: the unit eigenvectors of T(m) with sorted indices
-    // [0, K) (the nev lowest distinct values and one guard, whole clusters:
+    // [0, K) (the nev lowest distinct values, whole clusters:
     // tcore::ritz_span) with seeded weights; work[0..m) holds the sorted
     // eigenvalues of T after analyze
     const int n1 = cnt < nev ? cnt : nev;

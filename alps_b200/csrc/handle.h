@@ -27,6 +27,7 @@ struct aed_handle {
   uint32_t* d_tfirst = nullptr;  // first tile of each hi block
   double* d_dg = nullptr;     // per-row diagonal
   uint32_t* d_ell = nullptr;  // lo-neighbour table
+  size_t d_ell_n = 0;         // its capacity (entries), kept across aed_set_couplings
   uint16_t* d_xtab = nullptr;  // crossing-flip table
   double* d_partA = nullptr;  // per-tile partial sums (n_tiles)
   double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
@@ -34,8 +35,9 @@ struct aed_handle {
   double* h_scal = nullptr;   // 8 pinned host scalars
   int hv_var[2] = {-1, -1};  // apply variant per precision (FP64, FP32), -1 = not tuned yet
   size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }
-  // solve workspaces, kept between solves (grown on demand): slot 0 = FP64
-  // recurrence, slot 1 = FP32 Lanczos basis store of the mixed path
+  // solve workspaces, kept between solves (grown on demand, so that a solve
+  // makes no allocation once the handle is warm): slot 0 = the three FP64
+  // recurrence vectors, slot 1 = device alpha/beta pairs and Ritz coefficients
   void* ws[2] = {nullptr, nullptr};
   size_t ws_bytes[2] = {0, 0};
   std::vector<void*> store_chunks;  // FP32 Lanczos basis of the mixed path, kStoreChunk vectors each

@@ -302,12 +302,12 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
     return fail(AED_ERR_INVALID, "no live Lanczos recurrence to resume (solve or aed_lanczos_load first)");
   if (m0 >= max_iter) max_iter = m0 + 1;
   void* buf[3];
-  DevMem ab;  // alpha/beta pairs of the device
+  void* ab = nullptr;  // device alpha/beta pairs
   double* hab = nullptr;
-  if ((rc = recurrence_buffers(h, buf)) || (rc = ab.alloc((size_t)2 * (max_iter + 2) * 8)) ||
+  if ((rc = recurrence_buffers(h, buf)) || (rc = handle_workspace(h, 1, (size_t)2 * (max_iter + 2) * 8, &ab)) ||
       (rc = handle_pinned(h, (size_t)2 * (max_iter + 2), &hab)) || (rc = ring.init()))
     return rc;
-  double* d_ab = (double*)ab.p;
+  double* d_ab = (double*)ab;
   h->rec_live = false;  // from here on the slots change
   Recurrence R{h, false, D, max_iter, d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
   if (resume) {
@@ -363,13 +363,13 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   const int64_t ldv = (int64_t)(vbytes / 4);  // stride of the stored vectors (256-byte aligned)
   const size_t chunk_bytes = vbytes * kStoreChunk;
   const int cap = std::min(max_iter + 1, kMaxRitzTerms);
-  HostPinned hab;
   EventRing ring;
-  DevMem small;  // alpha/beta pairs | Ritz coefficients
+  void* small = nullptr;  // alpha/beta pairs | Ritz coefficients (workspace slot 1, reused by the FP64 phase after)
+  double* hab = nullptr;
   int rc;
   const size_t ab_bytes = (((size_t)2 * (cap + 2) * 8 + 255) & ~(size_t)255);
-  if ((rc = small.alloc(ab_bytes + (size_t)kStoreChunk * 8)) || (rc = hab.alloc((size_t)2 * (cap + 2))) ||
-      (rc = ring.init()))
+  if ((rc = handle_workspace(h, 1, ab_bytes + (size_t)kStoreChunk * 8, &small)) ||
+      (rc = handle_pinned(h, (size_t)2 * (cap + 2), &hab)) || (rc = ring.init()))
     return rc;
   // the FP64 phase's start stays with the handle (eigenvector replay)
   if (!h->d_start64) {
@@ -381,8 +381,8 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
     }
   }
   double* start64 = h->d_start64;
-  double* d_ab = (double*)small.p;
-  double* coef = (double*)((char*)small.p + ab_bytes);
+  double* d_ab = (double*)small;
+  double* coef = (double*)((char*)small + ab_bytes);
   bool oom = false;
   auto slot = [&](int j) -> void* {
     char* c = (char*)handle_store_chunk(h, j / kStoreChunk, chunk_bytes);
@@ -404,7 +404,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   }
   if ((rc = normalize(h, V0, D))) return rc;
   // phase 1: FP32 vectors, stop at FP32-level residual estimates
-  Recurrence R{h, true, D, cap - 1, d_ab, hab.p, &ring, {}, {}, 0, 0, profile, {}};
+  Recurrence R{h, true, D, cap - 1, d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
   const double tol32 = 2e-6;
   StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
@@ -417,7 +417,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   for (int i = 0; i < n1; ++i) r->evals_low[i] = T1.evals[i];
   r->iterations_low = m1;
   const double apply32_ms = profile ? R.apply_ms() : 0.0;
-  // Ritz start: the eigenvectors of T(m1) up to the end of the (nev+1)-th
+  // Ritz start: the eigenvectors of T(m1) up to the end of the nev-th
   // distinct cluster with seeded weights (tcore::ritz_span / ritz_weight),
   // accumulated in FP64 chunk by chunk from the stored basis
   std::vector<double> ev(R.alpha.begin(), R.alpha.begin() + m1), e(m1 + 1, 0.0), Z((size_t)m1 * m1);

@@ -201,7 +201,7 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   sl.has_sector = true;
   const int64_t D = sec->tab.D;
   BInst& I = sl.inst;
-  std::memset(&I, 0, sizeof I);
+  I = BInst{};
   HvParams P;
   if ((rc = build_hv_params(r->model, sec->tab.Nlo, P))) return rc;
   const int cap = cap_of(*r, D);
@@ -300,8 +300,7 @@ void release_slot(aed_server* s, int k) {
   sl.allocs.clear();
   if (sl.used) s->used -= std::min(s->used, sl.bytes);
   if (sl.has_sector) sector_release(s, sl.sector);
-  BInst idle;
-  std::memset(&idle, 0, sizeof idle);
+  BInst idle{};
   idle.phase = kPhIdle;
   s->h_inst[k] = idle;
   cudaMemcpyAsync(s->d_inst + k, &s->h_inst[k], sizeof(BInst), cudaMemcpyHostToDevice, s->stream);
@@ -428,7 +427,7 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
   cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thresh);
   s->slots.resize(s->max_slots);
   s->h_inst.resize(s->max_slots);
-  std::memset(s->h_inst.data(), 0, sizeof(BInst) * s->max_slots);
+  for (auto& b : s->h_inst) b = BInst{};
   if (cudaMalloc(&s->d_inst, sizeof(BInst) * s->max_slots) != cudaSuccess ||
       cudaMalloc(&s->d_counts, 4 * sizeof(int32_t)) != cudaSuccess ||
       cudaMallocHost(&s->h_counts, 4 * sizeof(int32_t)) != cudaSuccess) {

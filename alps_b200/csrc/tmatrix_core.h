@@ -193,12 +193,14 @@ AED_HD inline int analyze(int n, const double* alpha, const double* beta, double
 }
 
 // Start of the FP64 refinement of the mixed path: the eigenvectors of T with
-// sorted indices [0, K) are combined, where K ends the (nev+1)-th distinct
-// value's cluster (the nev wanted and one guard).  A cluster holds ghost copies
-// and any pair closer than the FP32 phase resolves, so the partner of a
-// near-degenerate pair is kept.  first / mults: analyze's output (count values).
+// sorted indices [0, K) are combined, where K ends the nev-th distinct value's
+// cluster.  A cluster holds ghost copies and any pair closer than the FP32
+// phase resolves, so the partner of a near-degenerate pair is kept (a guard
+// cluster beyond the nev-th made the refinement 1.5-3x longer on the J1-J2
+// chain, L=28, without changing a result).  first / mults: analyze's output
+// (count values).
 AED_HD inline int ritz_span(int count, int nev, const int* first, const int* mults, int n) {
-  const int c = count < nev + 1 ? count : nev + 1;
+  const int c = count < nev ? count : nev;
   if (c <= 0) return n < 1 ? 0 : 1;
   const int K = first[c - 1] + (mults[c - 1] > 0 ? mults[c - 1] : 1);
   return K < n ? K : n;

@@ -240,6 +240,43 @@ def cpu_sample(j2, iterations, threads_note="1 thread (the reference path is sin
     }
 
 
+def cpu_matfree_sample(j2, iterations, rows=4_000_000):
+    """Best-CPU baseline: the matrix-free restatement (no stored matrix, binary-search ranks) with
+    all host threads, timed on a bounded sample of rows and scaled to one solve."""
+    import oracle
+
+    N, n_up = L28, L28 // 2
+    states = oracle.basis_fast(N, n_up)
+    D = states.size
+    bonds = chain_bonds(L28, j2)
+    x = np.random.default_rng(5).uniform(0, 1, D)
+    r0 = D // 3
+    oracle.hv_matfree(N, states, bonds, x, r0, r0 + rows // 8)  # warm the threads and pages
+    t0 = time.perf_counter()
+    oracle.hv_matfree(N, states, bonds, x, r0, r0 + rows)
+    t = time.perf_counter() - t0
+    solve_s = iterations * t * D / rows
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": (f"matrix-free H*x (OpenMP, {oracle.num_threads()} threads) on rows [{r0}, {r0 + rows}) "
+                       f"({rows / D:.1%} of the sector) in {t:.2f} s, scaled to {iterations} applies per solve; "
+                       "vector passes not counted")}
+
+
+def compare_energies(got, ref):
+    """Relative differences of eigenvalue lists against a reference run (lists of per-solve lists).
+    gs: ground states only (the 1e-9 criterion).  An excited value of `got` below the reference's by
+    more than 1e-9 relative is a state the reference run missed (a Ritz value cannot lie below the
+    eigenvalue of its index): such solves are counted, not mixed into the maximum."""
+    gs = max(abs(a[0] - b[0]) / abs(b[0]) for a, b in zip(got, ref))
+    allv, missed = 0.0, 0
+    for a, b in zip(got, ref):
+        if any(x < y - 1e-9 * abs(y) for x, y in zip(a[1:], b[1:])):
+            missed += 1
+            continue
+        allv = max([allv] + [abs(x - y) / abs(y) for x, y in zip(a, b)])
+    return {"gs": gs, "all": allv, "ref_missed_states": missed}
+
+
 def run_ours(args):
     import torch
 
@@ -340,17 +377,18 @@ def run_ours(args):
         m1.record(s32)
         m1.synchronize()
         mixed_s = max_over_ranks(pg, m0.elapsed_time(m1) / 1e3)
-        rel = max(abs(a - b) / abs(b) for ea, eb in zip(mev, evals) for a, b in zip(ea, eb))
+        rel = compare_energies(mev, evals)
         b32 = D * ((1 + nbar) * 4 + 4)
         mixed = {"solves_per_s": total / mixed_s, "speedup_vs_fp64": (total / mixed_s) / value,
-                 "max_rel_energy_err_vs_fp64": rel, "iterations_fp32_fp64": mit,
+                 "rel_energy_err_vs_fp64": rel, "iterations_fp32_fp64": mit,
                  "apply_ms_fp32": float(np.mean(m32ms)),
                  "hv_fp32_gbs": b32 / (float(np.mean(m32ms)) / 1e3) / 1e9}
         h32.close()
         print(f"[bench] mixed: {mixed}", file=sys.stderr)
-    cpu = None
+    cpu = cpu_all = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(float(j2s[W]), int(round(np.mean(iters))))
+        cpu_all = cpu_matfree_sample(float(j2s[W]), int(round(np.mean(iters))))
     ham.close()
     if rank == 0:
         line = {
@@ -362,7 +400,7 @@ def run_ours(args):
                        "dimension": D, "nev": NEV, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (each vector 321 MB); no flush"},
             "iterations": iters, "evals": evals, "wall_s": wall,
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roof, "cpu_baseline": cpu, "cpu_baseline_all_cores": cpu_all, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(), "mixed": mixed,
         }
         print(json.dumps(line))
@@ -508,8 +546,8 @@ def run_batch(args):
     t_single = time.perf_counter() - t0
     for h in hams.values():
         h.close()
-    rel = max(abs(a - c) / abs(c) for ea, ec in zip(res["mixed"]["evals"], single) for a, c in zip(ea, ec))
-    rel64 = max(abs(a - c) / abs(c) for ea, ec in zip(res["fp64"]["evals"], single) for a, c in zip(ea, ec))
+    rel = compare_energies(res["mixed"]["evals"], single)
+    rel64 = compare_energies(res["fp64"]["evals"], single)
     line = {"metric": "batched Lanczos solves/s (512 J1-J2 chains, L 12..22), mixed vs plain FP64",
             "value": res["mixed"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f32+f64", "data": "synthetic",
@@ -520,7 +558,7 @@ def run_batch(args):
             "fp64_single_instance": {"seconds": t_single, "solves_per_s": len(reqs) / t_single},
             "speedup_mixed_batched_vs_fp64_single": res["mixed"]["solves_per_s"] / (len(reqs) / t_single),
             "speedup_mixed_batched_vs_fp64_batched": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
-            "max_rel_energy_err_mixed_vs_fp64": rel, "max_rel_energy_err_fp64_batched_vs_single": rel64}
+            "rel_energy_err_mixed_vs_fp64_single": rel, "rel_energy_err_fp64_batched_vs_single": rel64}
     if not args.no_cpu:
         classes = {}
         for n, b, nev, sd in reqs:
