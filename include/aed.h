@@ -272,7 +272,8 @@ typedef struct {
 int aed_server_create(const aed_server_opts* opts, aed_server** out);
 int aed_server_destroy(aed_server* s);
 /* Queue a request.  AED_ERR_ADMISSION if its footprint alone exceeds the budget.
- * opts->start is ignored (start vectors are drawn from opts->seed). */
+ * opts->start and opts->resume are ignored (start vectors are drawn from
+ * opts->seed). */
 int aed_server_submit(aed_server* s, const aed_model_desc* model, const aed_solve_opts* opts, int64_t* ticket);
 /* Admit what fits, run one graph launch (S engine steps + check), harvest
  * finished requests.  *n_pending = resident + queued requests afterwards. */
