@@ -109,6 +109,56 @@ __device__ __forceinline__ void tile_partials(double (&dot)[B], int nv, const ui
 }
 
 template <typename T, int B>
+struct BundlePass;
+
+// FP32 rows, crossing flips of all B blocks: every block has one entry per
+// crossing pair, in pair order, so entry o of each block's crossing segment
+// names the same lo bit and one crossing-flip table load per row serves all
+// blocks (their targets and required bit values differ).
+template <typename T, typename Acc, int R, int B>
+__device__ __forceinline__ void run_cross_shared(const BundleSmem<B>& sm, const BundlePass<T, B>& q, int nv,
+                                                 const uint16_t* __restrict__ xt, uint32_t nlo, uint32_t nrow,
+                                                 const T* __restrict__ x, Acc (*acc)[R]) {
+  constexpr int U = 2;
+  const int nc = q.nops[0] - q.nlow[0];  // crossing entries per block (equal for all blocks)
+  int o = 0;
+  for (; o < nc; o += U) {
+    uint32_t ent[U][R];
+#pragma unroll
+    for (int v = 0; v < U; ++v) {
+      const bool live = o + v < nc;
+      const uint32_t mc0 = live ? sm.prog[0][q.nlow[0] + o + v].mc : 0u;
+      const uint16_t* xb = xt + (size_t)(mc0 >> 16) * nlo;
+#pragma unroll
+      for (int u = 0; u < R; ++u) ent[v][u] = (live && (uint32_t)u < nrow) ? (uint32_t)__ldg(xb + u * kHvThreads) : 0u;
+    }
+    T xv[U][B][R];
+    bool p[U][B][R];
+    double cc[U][B];
+#pragma unroll
+    for (int v = 0; v < U; ++v)
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        const bool live = o + v < nc && j < nv;
+        const TileOp e = live ? sm.prog[j][q.nlow[j] + o + v] : TileOp{0u, 0u, 0.0};
+        cc[v][j] = e.c;
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          p[v][j][u] = live && (uint32_t)u < nrow && ((ent[v][u] ^ e.mc) & 0x8000u) == 0u;
+          xv[v][j][u] = p[v][j][u] ? __ldg(x + (e.nb + ent[v][u])) : T(0);
+        }
+      }
+#pragma unroll
+    for (int v = 0; v < U; ++v)
+#pragma unroll
+      for (int j = 0; j < B; ++j)
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p[v][j][u]) acc[j][u].add(cc[v][j], xv[v][j][u]);
+  }
+}
+
+template <typename T, int B>
 struct BundlePass {
   int nv;                   // blocks in the bundle
   const uint32_t* bj;       // [B] base row of each block
@@ -199,11 +249,13 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
     }
 #pragma unroll
     for (int j = 0; j < B; ++j)
-      if (j < nv) {
-        apply::run_hihi<T, Acc, R>(sm.prog[j], 0, q.nlow[j], nrow, rt, x, acc[j]);
-        apply::run_cross<T, Acc, R>(sm.prog[j], q.nlow[j], q.nops[j], t.xtab + q.lbase + rt, 1u << c.Nlo, nrow, x,
-                                    acc[j]);
-      }
+      if (j < nv) apply::run_hihi<T, Acc, R>(sm.prog[j], 0, q.nlow[j], nrow, rt, x, acc[j]);
+    if (B == 1) {
+      apply::run_cross<T, Acc, R>(sm.prog[0], q.nlow[0], q.nops[0], t.xtab + q.lbase + rt, 1u << c.Nlo, nrow, x,
+                                  acc[0]);
+    } else {
+      run_cross_shared<T, Acc, R, B>(sm, q, nv, t.xtab + q.lbase + rt, 1u << c.Nlo, nrow, x, acc);
+    }
     // lo-part flips: four table entries at a time, x from shared memory
     constexpr int U = 4;
     for (int e = 0; e < t.ell_w; e += U) {
