@@ -2,7 +2,7 @@
 //
 // One engine step advances every resident instance by one Lanczos step
 // (lanczos::make_step, src/ietl/lanczos.h:392-406):
-//   b_hv       y = H x over the (instance, tile) queue, per-tile <x,y> partials
+//   b_hv32/64  y = H x over the (instance, bundle) queue, per-tile <x,y> partials
 //   b_alpha    alpha_j = sum of the instance's tile partials (one CTA each)
 //   b_update   y = (y - alpha x) - beta_{j-1} v_{j-1} over (instance, chunk), chunk partials of |y|^2
 //   b_beta     beta_j = sqrt(sum of the chunk partials)
@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "apply.cuh"
+#include "apply_blocks.cuh"
 #include "batch.cuh"
 #include "reduce.cuh"
 #include "tmatrix_core.h"
@@ -29,8 +30,6 @@ using apply::AccWide32;
 using apply::ApplyCtx;
 using apply::ApplySmem;
 
-constexpr int kBR = 4;     // rows per thread of the batched apply
-constexpr int kBMinB = 4;  // CTAs per SM of the batched apply
 
 __device__ __forceinline__ bool stepping(const BInst& I) {
   if (I.phase == kPhLow) return I.j + 1 < I.n_store && I.j < I.cap;
@@ -43,25 +42,60 @@ __device__ __forceinline__ float* low_vec(const BInst& I, int j) {
 }
 __device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v64[j % 3]; }
 
-__global__ void __launch_bounds__(kHvThreads, kBMinB) b_hv(BatchArgs a) {
-  __shared__ ApplySmem sm;
+// The apply of every stepping instance over its (instance, bundle) items: the
+// bundle apply (apply_blocks.cuh, one hi block at a time) with the
+// instance's tables; the staged pairs and the shared-memory layout change
+// with the instance.  One kernel per phase, so that each has the registers of
+// its own path: FP32 vectors (b_hv32: 1 row per thread, 6 CTAs per SM) and
+// FP64 vectors (b_hv64: 4 rows per thread, 3 CTAs per SM).  Blocks of the
+// batched sectors are small (L = 12..26 chains: up to 1716 rows), and the
+// narrow FP32 pass measured 1.45x the solves/s of two blocks at 2 rows per
+// thread on the 512-chain batch.
+__global__ void __launch_bounds__(kHvThreads, 6) b_hv32(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char b_dyn[];
+  __shared__ bapply::BundleSmem<1> sm;
   const int n = *a.n_tiles;
-  int cur = -1;
+  int cur = -1, rc = 0;
+  float* xs = nullptr;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const BItem w = a.tiles[it];
     const BInst& I = a.inst[w.inst];
-    if (!stepping(I)) continue;  // same for every thread of the CTA
+    if (I.phase != kPhLow || !stepping(I)) continue;  // same for every thread of the CTA
     const int j = I.j;
     if (w.inst != cur) {
-      __syncthreads();  // the previous tile is done with the staged pairs
-      apply::stage_pairs(*I.P, sm);
+      __syncthreads();  // the previous block is done with the staged pairs
+      xs = bapply::carve<float, 1>(*I.P, I.t, b_dyn, sm);
+      bapply::stage_pairs<1>(*I.P, sm);
       cur = w.inst;
     }
     const ApplyCtx c = apply::ctx_of(*I.P);
-    if (I.phase == kPhLow)
-      apply::apply_tile<float, AccWide32, kBR>(c, I.t, w.idx, low_vec(I, j), low_vec(I, j + 1), I.partA, sm);
-    else
-      apply::apply_tile<double, AccExact64, kBR>(c, I.t, w.idx, high_vec(I, j), high_vec(I, j + 1), I.partA, sm);
+    for (int q = 0; q < kBatchBundle; ++q)  // the item's blocks one at a time (block-list entries)
+      bapply::apply_bundle<float, AccWide32, 1, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, low_vec(I, j),
+                                                   low_vec(I, j + 1), I.partA, sm, xs, rc);
+  }
+}
+
+__global__ void __launch_bounds__(kHvThreads, 3) b_hv64(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char b_dyn[];
+  __shared__ bapply::BundleSmem<1> sm;
+  const int n = *a.n_tiles;
+  int cur = -1, rc = 0;
+  double* xs = nullptr;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.tiles[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhHigh || !stepping(I)) continue;
+    const int j = I.j;
+    if (w.inst != cur) {
+      __syncthreads();
+      xs = bapply::carve<double, 1>(*I.P, I.t, b_dyn, sm);
+      bapply::stage_pairs<1>(*I.P, sm);
+      cur = w.inst;
+    }
+    const ApplyCtx c = apply::ctx_of(*I.P);
+    for (int q = 0; q < kBatchBundle; ++q)  // the item's blocks one at a time (block-list entries)
+      bapply::apply_bundle<double, AccExact64, 4, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, high_vec(I, j),
+                                                     high_vec(I, j + 1), I.partA, sm, xs, rc);
   }
 }
 
@@ -311,14 +345,19 @@ int sms() {
   return g_sms;
 }
 
-int hv_grid() {
-  static int g = 0;
-  if (!g) {
+int g_hv32 = 0, g_hv32_smem = -1, g_hv64 = 0, g_hv64_smem = -1;
+
+// Grid of an apply kernel for `smem` bytes of dynamic shared memory (cached per size).
+template <typename K>
+int hv_grid(K kern, int smem, int* g, int* g_smem) {
+  if (smem != *g_smem) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, b_hv, kHvThreads, 0);
-    g = sms() * (per < 1 ? 1 : per);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kHvThreads, smem);
+    *g = sms() * (per < 1 ? 1 : per);
+    *g_smem = smem;
   }
-  return g;
+  return *g;
 }
 
 int check(const char* what) {
@@ -329,10 +368,32 @@ int check(const char* what) {
 
 }  // namespace
 
+size_t batch_hv_smem_bytes(int maxrows, const HvParams& P) {
+  return bapply::bundle_smem_bytes<double>(1, maxrows, P.n_pairs, P.n_lolo);
+}
+
+size_t batch_hv_smem_limit() {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes f32{}, f64{};
+  cudaFuncGetAttributes(&f32, b_hv32);
+  cudaFuncGetAttributes(&f64, b_hv64);
+  const size_t st = f32.sharedSizeBytes > f64.sharedSizeBytes ? f32.sharedSizeBytes : f64.sharedSizeBytes;
+  return optin > (int)st ? (size_t)optin - st : 0;
+}
+
+int batch_prepare(const BatchArgs& a) {
+  hv_grid(b_hv32, a.hv_smem, &g_hv32, &g_hv32_smem);
+  hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem);
+  return check("batched apply attributes");
+}
+
 int batch_record_step(const BatchArgs& a, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
-  b_hv<<<hv_grid(), kHvThreads, 0, st>>>(a);
+  b_hv32<<<hv_grid(b_hv32, a.hv_smem, &g_hv32, &g_hv32_smem), kHvThreads, a.hv_smem, st>>>(a);
+  b_hv64<<<hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem), kHvThreads, a.hv_smem, st>>>(a);
   b_alpha<<<ni, 256, 0, st>>>(a);
   b_update<<<gchunk, kRedThreads, 0, st>>>(a);
   b_beta<<<ni, 256, 0, st>>>(a);

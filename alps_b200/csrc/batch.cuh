@@ -76,13 +76,24 @@ struct BItem {
 struct BatchArgs {
   BInst* inst;
   int32_t* n_inst;     // number of slots in use (device)
-  BItem* tiles;
+  BItem* tiles;        // apply items: (instance, bundle of kBatchBundle hi blocks)
   int32_t* n_tiles;
   BItem* chunks;
   int32_t* n_chunks;
   int max_inst;
+  int hv_smem;         // dynamic shared memory of the apply (batch_hv_smem_bytes, max over residents)
 };
 
+// Hi blocks per work item of the batched apply (entries ub * kBatchBundle ..
+// of a sector's block list, applied one block at a time).
+constexpr int kBatchBundle = 2;
+// Dynamic shared memory the batched apply needs for one instance (FP64 size,
+// which also covers its FP32 phase).
+size_t batch_hv_smem_bytes(int maxrows, const HvParams& P);
+// Largest dynamic shared memory a CTA of the batched apply may take on this device.
+size_t batch_hv_smem_limit();
+// Set the apply kernels' shared-memory limits for a.hv_smem; call before capturing.
+int batch_prepare(const BatchArgs& a);
 int batch_record_step(const BatchArgs& a, cudaStream_t st);
 int batch_record_check(const BatchArgs& a, cudaStream_t st);
 int batch_max_inst_grid();

@@ -33,6 +33,9 @@ struct Sector {
   BasisTables tab;
   uint32_t *thi = nullptr, *looff = nullptr, *tile_h = nullptr, *tile_r = nullptr;
   uint16_t* xtab = nullptr;  // crossing-flip table
+  uint32_t *blk_h = nullptr, *tfirst = nullptr;  // block list of the bundle apply, first tile per hi block
+  std::vector<uint32_t> blk;                     // host copy of the block list (work items)
+  int maxrows = 0;
   uint16_t *tlo = nullptr, *lolist = nullptr;
   int64_t n_tiles = 0;
   size_t bytes = 0;
@@ -88,6 +91,7 @@ struct aed_server {
   bool dirty = true;
   cudaGraphExec_t graph = nullptr;
   bool graph_stale = true;
+  int hv_smem = 0;  // dynamic shared memory of the apply in the graph
   int64_t launches = 0;
 };
 
@@ -126,7 +130,8 @@ size_t sector_bytes(int N, int n_up) {
   BasisTables t;
   if (build_tables(N, n_up, t)) return 0;
   return t.thi.size() * 4 + t.tlo.size() * 2 + t.lolist.size() * 2 + t.looff.size() * 4 +
-         (size_t)t.Nlo * t.tlo.size() * 2 + (size_t)sector_tiles_est(t.D) * 8 + 4096;
+         (size_t)t.Nlo * t.tlo.size() * 2 + (size_t)sector_tiles_est(t.D) * 8 + t.thi.size() * 8 + 4096 +
+         (size_t)4 * kBundleMax * (t.Nlo + 1);
 }
 
 int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
@@ -140,17 +145,20 @@ int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
   Sector sec;
   int rc = build_tables(N, n_up, sec.tab);
   if (rc) return rc;
-  std::vector<uint32_t> th, tr;
+  std::vector<uint32_t> th, tr, tf;
   std::vector<uint16_t> xt;
-  build_tiles(sec.tab, kHvTileRows, th, tr);
+  build_tiles(sec.tab, kHvTileRows, th, tr, &tf);
   build_cross_table(sec.tab, xt);
+  build_block_list(sec.tab, sec.blk, &sec.maxrows);
   sec.n_tiles = (int64_t)th.size();
   const size_t nhi = sec.tab.thi.size(), nlo = sec.tab.tlo.size(), nof = sec.tab.looff.size();
   if ((rc = dmalloc(s, (void**)&sec.thi, nhi * 4)) || (rc = dmalloc(s, (void**)&sec.tlo, nlo * 2)) ||
       (rc = dmalloc(s, (void**)&sec.lolist, nlo * 2)) || (rc = dmalloc(s, (void**)&sec.looff, nof * 4)) ||
       (rc = dmalloc(s, (void**)&sec.tile_h, th.size() * 4 + 4)) ||
       (rc = dmalloc(s, (void**)&sec.tile_r, tr.size() * 4 + 4)) ||
-      (rc = dmalloc(s, (void**)&sec.xtab, xt.size() * 2 + 4)))
+      (rc = dmalloc(s, (void**)&sec.xtab, xt.size() * 2 + 4)) ||
+      (rc = dmalloc(s, (void**)&sec.blk_h, sec.blk.size() * 4 + 4)) ||
+      (rc = dmalloc(s, (void**)&sec.tfirst, tf.size() * 4 + 4)))
     return rc;
   cudaMemcpyAsync(sec.thi, sec.tab.thi.data(), nhi * 4, cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(sec.tlo, sec.tab.tlo.data(), nlo * 2, cudaMemcpyHostToDevice, s->stream);
@@ -161,7 +169,10 @@ int sector_acquire(aed_server* s, int N, int n_up, Sector** out) {
     cudaMemcpyAsync(sec.tile_r, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice, s->stream);
   }
   if (!xt.empty()) cudaMemcpyAsync(sec.xtab, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, s->stream);
-  AED_CUDA_TRY(cudaStreamSynchronize(s->stream));  // host vectors th/tr/xt go out of scope
+  if (!sec.blk.empty())
+    cudaMemcpyAsync(sec.blk_h, sec.blk.data(), sec.blk.size() * 4, cudaMemcpyHostToDevice, s->stream);
+  if (!tf.empty()) cudaMemcpyAsync(sec.tfirst, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice, s->stream);
+  AED_CUDA_TRY(cudaStreamSynchronize(s->stream));  // host vectors th/tr/xt/tf go out of scope
   sec.bytes = sector_bytes(N, n_up);
   sec.refs = 1;
   s->used += sec.bytes;
@@ -176,7 +187,7 @@ void sector_release(aed_server* s, std::pair<int, int> key) {
   if (--it->second.refs > 0) return;
   Sector& sec = it->second;
   for (void* p : {(void*)sec.thi, (void*)sec.tlo, (void*)sec.lolist, (void*)sec.looff, (void*)sec.tile_h,
-                  (void*)sec.tile_r, (void*)sec.xtab})
+                  (void*)sec.tile_r, (void*)sec.xtab, (void*)sec.blk_h, (void*)sec.tfirst})
     if (p) cudaFreeAsync(p, s->stream);
   s->used -= std::min(s->used, sec.bytes);
   s->sectors.erase(it);
@@ -204,6 +215,13 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   I = BInst{};
   HvParams P;
   if ((rc = build_hv_params(r->model, sec->tab.Nlo, P))) return rc;
+  const size_t smem = batch_hv_smem_bytes(sec->maxrows, P);
+  if (smem > batch_hv_smem_limit())
+    return fail(AED_ERR_INVALID, "sector too large for the batched apply's shared memory");
+  if ((int)smem > s->hv_smem) {  // the graph's apply needs more shared memory: capture again
+    s->hv_smem = (int)((smem + 1023) & ~(size_t)1023);
+    s->graph_stale = true;
+  }
   const int cap = cap_of(*r, D);
   const int n_store = s->precision == AED_FP32 ? std::min(kServerStore, std::min(cap + 1, kBatchMaxChunks * kStoreChunkB)) : 0;
   auto take = [&](void** p, size_t bytes) -> int {
@@ -234,6 +252,10 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   t.tile_h = sec->tile_h;
   t.tile_r = sec->tile_r;
   t.xtab = sec->xtab;
+  t.blk_h = sec->blk_h;
+  t.tfirst = sec->tfirst;
+  t.n_blk = (int64_t)sec->blk.size();
+  t.maxrows = sec->maxrows;
   t.n_tiles = sec->n_tiles;
   t.D = D;
   t.Nlo = sec->tab.Nlo;
@@ -316,7 +338,9 @@ int rebuild_items(aed_server* s) {
     if (!s->slots[k].used) continue;
     n_inst = k + 1;
     const BInst& I = s->slots[k].inst;
-    for (int t = 0; t < I.n_tiles; ++t) tiles.push_back({k, t});
+    const std::vector<uint32_t>& blk = s->sectors.at(s->slots[k].sector).blk;
+    for (size_t ub = 0; ub * kBatchBundle < blk.size(); ++ub)  // bundles holding at least one block
+      if (blk[ub * kBatchBundle] != kNoBlockEntry) tiles.push_back({k, (int32_t)ub});
     for (int64_t c = 0; c < I.n_chunks; ++c) chunks.push_back({k, (int32_t)c});
   }
   if (tiles.size() > s->cap_tiles || chunks.size() > s->cap_chunks) {
@@ -355,8 +379,11 @@ int capture_graph(aed_server* s) {
     cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
   }
-  BatchArgs a{s->d_inst, s->d_counts, s->d_tiles, s->d_counts + 1, s->d_chunks, s->d_counts + 2, s->max_slots};
+  BatchArgs a{s->d_inst, s->d_counts, s->d_tiles, s->d_counts + 1, s->d_chunks, s->d_counts + 2, s->max_slots,
+              s->hv_smem};
   cudaGraph_t g = nullptr;
+  const int rp = batch_prepare(a);
+  if (rp) return rp;
   AED_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int rc = AED_OK;
   for (int k = 0; k < s->S && !rc; ++k) rc = batch_record_step(a, s->stream);
@@ -459,7 +486,7 @@ int aed_server_destroy(aed_server* s) {
   for (auto& kv : s->sectors) {
     Sector& sec = kv.second;
     for (void* p : {(void*)sec.thi, (void*)sec.tlo, (void*)sec.lolist, (void*)sec.looff, (void*)sec.tile_h,
-                    (void*)sec.tile_r, (void*)sec.xtab})
+                    (void*)sec.tile_r, (void*)sec.xtab, (void*)sec.blk_h, (void*)sec.tfirst})
       if (p) cudaFreeAsync(p, s->stream);
   }
   cudaStreamSynchronize(s->stream);
