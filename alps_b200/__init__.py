@@ -86,6 +86,7 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("max_slots", ctypes.c_int32), ("steps_per_launch", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("hbm_fraction", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_int64),
+        ("reserve_bytes", ctypes.c_int64),
     ]
 
 
@@ -475,8 +476,10 @@ class Server:
     admitted by HBM footprint and advance together, S Lanczos steps per CUDA
     graph launch; new requests join at the next step."""
 
-    def __init__(self, precision=FP32, device=0, max_slots=512, steps=8, hbm_fraction=0.0, hbm_budget=0):
-        o = ServerOpts(device, max_slots, steps, precision, hbm_fraction, hbm_budget)
+    def __init__(self, precision=FP32, device=0, max_slots=512, steps=8, hbm_fraction=0.0, hbm_budget=0,
+                 reserve=0):
+        """reserve: bytes of device memory to map into the server's pool up front (-1: the whole budget)."""
+        o = ServerOpts(device, max_slots, steps, precision, hbm_fraction, hbm_budget, reserve)
         h = _P()
         self._h = None
         _check(lib().aed_server_create(ctypes.byref(o), ctypes.byref(h)))

@@ -45,13 +45,16 @@ __device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v6
 // The apply of every stepping instance over its (instance, bundle) items: the
 // bundle apply (apply_blocks.cuh, one hi block at a time) with the
 // instance's tables; the staged pairs and the shared-memory layout change
-// with the instance.  One kernel per phase, so that each has the registers of
-// its own path: FP32 vectors (b_hv32: 1 row per thread, 6 CTAs per SM) and
-// FP64 vectors (b_hv64: 4 rows per thread, 3 CTAs per SM).  Blocks of the
-// batched sectors are small (L = 12..26 chains: up to 1716 rows), and the
-// narrow FP32 pass measured 1.45x the solves/s of two blocks at 2 rows per
-// thread on the 512-chain batch.
-__global__ void __launch_bounds__(kHvThreads, 6) b_hv32(BatchArgs a) {
+// with the instance.  One kernel per phase and block size, so that each has
+// the registers of its own path: FP32 vectors with small hi blocks
+// (maxrows <= kSmallBlock: 1 row per thread, 6 CTAs per SM -- 1.45x the
+// solves/s of 2 rows per thread on the 512-chain batch of L = 12..22) or
+// larger ones (2 rows per thread, 4 CTAs per SM), and FP64 vectors (b_hv64:
+// 4 rows per thread, 3 CTAs per SM).
+constexpr int kSmallBlock = 512;
+
+template <int R, int MINB, bool kSmall>
+__global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char b_dyn[];
   __shared__ bapply::BundleSmem<1> sm;
   const int n = *a.n_tiles;
@@ -60,7 +63,8 @@ __global__ void __launch_bounds__(kHvThreads, 6) b_hv32(BatchArgs a) {
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const BItem w = a.tiles[it];
     const BInst& I = a.inst[w.inst];
-    if (I.phase != kPhLow || !stepping(I)) continue;  // same for every thread of the CTA
+    if (I.phase != kPhLow || !stepping(I) || (I.t.maxrows <= kSmallBlock) != kSmall)
+      continue;  // same for every thread of the CTA
     const int j = I.j;
     if (w.inst != cur) {
       __syncthreads();  // the previous block is done with the staged pairs
@@ -70,7 +74,7 @@ __global__ void __launch_bounds__(kHvThreads, 6) b_hv32(BatchArgs a) {
     }
     const ApplyCtx c = apply::ctx_of(*I.P);
     for (int q = 0; q < kBatchBundle; ++q)  // the item's blocks one at a time (block-list entries)
-      bapply::apply_bundle<float, AccWide32, 1, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, low_vec(I, j),
+      bapply::apply_bundle<float, AccWide32, R, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, low_vec(I, j),
                                                    low_vec(I, j + 1), I.partA, sm, xs, rc);
   }
 }
@@ -345,7 +349,9 @@ int sms() {
   return g_sms;
 }
 
-int g_hv32 = 0, g_hv32_smem = -1, g_hv64 = 0, g_hv64_smem = -1;
+int g_hv32s = 0, g_hv32s_smem = -1, g_hv32l = 0, g_hv32l_smem = -1, g_hv64 = 0, g_hv64_smem = -1;
+#define B_HV32_SMALL b_hv32<1, 6, true>
+#define B_HV32_LARGE b_hv32<2, 4, false>
 
 // Grid of an apply kernel for `smem` bytes of dynamic shared memory (cached per size).
 template <typename K>
@@ -376,15 +382,18 @@ size_t batch_hv_smem_limit() {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncAttributes f32{}, f64{};
-  cudaFuncGetAttributes(&f32, b_hv32);
+  cudaFuncAttributes f32s{}, f32l{}, f64{};
+  cudaFuncGetAttributes(&f32s, B_HV32_SMALL);
+  cudaFuncGetAttributes(&f32l, B_HV32_LARGE);
   cudaFuncGetAttributes(&f64, b_hv64);
-  const size_t st = f32.sharedSizeBytes > f64.sharedSizeBytes ? f32.sharedSizeBytes : f64.sharedSizeBytes;
+  size_t st = f32s.sharedSizeBytes > f64.sharedSizeBytes ? f32s.sharedSizeBytes : f64.sharedSizeBytes;
+  if (f32l.sharedSizeBytes > st) st = f32l.sharedSizeBytes;
   return optin > (int)st ? (size_t)optin - st : 0;
 }
 
 int batch_prepare(const BatchArgs& a) {
-  hv_grid(b_hv32, a.hv_smem, &g_hv32, &g_hv32_smem);
+  hv_grid(B_HV32_SMALL, a.hv_smem, &g_hv32s, &g_hv32s_smem);
+  hv_grid(B_HV32_LARGE, a.hv_smem, &g_hv32l, &g_hv32l_smem);
   hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem);
   return check("batched apply attributes");
 }
@@ -392,7 +401,8 @@ int batch_prepare(const BatchArgs& a) {
 int batch_record_step(const BatchArgs& a, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
-  b_hv32<<<hv_grid(b_hv32, a.hv_smem, &g_hv32, &g_hv32_smem), kHvThreads, a.hv_smem, st>>>(a);
+  B_HV32_SMALL<<<hv_grid(B_HV32_SMALL, a.hv_smem, &g_hv32s, &g_hv32s_smem), kHvThreads, a.hv_smem, st>>>(a);
+  B_HV32_LARGE<<<hv_grid(B_HV32_LARGE, a.hv_smem, &g_hv32l, &g_hv32l_smem), kHvThreads, a.hv_smem, st>>>(a);
   b_hv64<<<hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem), kHvThreads, a.hv_smem, st>>>(a);
   b_alpha<<<ni, 256, 0, st>>>(a);
   b_update<<<gchunk, kRedThreads, 0, st>>>(a);

@@ -271,7 +271,7 @@ struct HvVariant {
 constexpr HvVariant kVariants[] = {
     {0, 4, 6, "r4b6"},      {0, 4, 5, "r4b5"},      {0, 4, 4, "r4b4"},      {0, 2, 8, "r2b8"},
     {0, 2, 6, "r2b6"},      {0, 8, 3, "r8b3"},      {1, 4, 3, "blk1r4b3"},  {2, 2, 4, "blk2r2b4"},
-    {2, 4, 2, "blk2r4b2"},  {4, 1, 2, "blk4r1b2"},  {4, 2, 2, "blk4r2b2"},  {1, 2, 4, "blk1r2b4"},
+    {2, 4, 2, "blk2r4b2"},  {2, 2, 3, "blk2r2b3"},  {1, 4, 4, "blk1r4b4"},  {1, 2, 4, "blk1r2b4"},
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -346,8 +346,8 @@ int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, 
     case 6: return launch_bundle<T, Acc, 4, 1, 3>(P, t, x, y, alpha_part, st, &bgrid[6]);
     case 7: return launch_bundle<T, Acc, 2, 2, 4>(P, t, x, y, alpha_part, st, &bgrid[7]);
     case 8: return launch_bundle<T, Acc, 4, 2, 2>(P, t, x, y, alpha_part, st, &bgrid[8]);
-    case 9: return launch_bundle<T, Acc, 1, 4, 2>(P, t, x, y, alpha_part, st, &bgrid[9]);
-    case 10: return launch_bundle<T, Acc, 2, 4, 2>(P, t, x, y, alpha_part, st, &bgrid[10]);
+    case 9: return launch_bundle<T, Acc, 2, 2, 3>(P, t, x, y, alpha_part, st, &bgrid[9]);
+    case 10: return launch_bundle<T, Acc, 4, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[10]);
     case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[11]);
     default: return fail(AED_ERR_INVALID, "unknown apply variant");
   }

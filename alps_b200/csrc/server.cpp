@@ -452,6 +452,16 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
   AED_CUDA_TRY(cudaDeviceGetDefaultMemPool(&s->pool, s->device));
   uint64_t thresh = UINT64_MAX;
   cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+  if (o->reserve_bytes != 0) {  // map memory into the pool now (best effort): later requests reuse it
+    const size_t want = o->reserve_bytes < 0 ? s->budget : std::min((size_t)o->reserve_bytes, s->budget);
+    void* p = nullptr;
+    if (want > 0 && cudaMallocAsync(&p, want, s->stream) == cudaSuccess) {
+      cudaFreeAsync(p, s->stream);
+      cudaStreamSynchronize(s->stream);
+    } else {
+      cudaGetLastError();
+    }
+  }
   s->slots.resize(s->max_slots);
   s->h_inst.resize(s->max_slots);
   for (auto& b : s->h_inst) b = BInst{};

@@ -520,7 +520,7 @@ def run_batch(args):
     reqs = batch_requests()
     res = {}
     for name, prec in (("mixed", ed.FP32), ("fp64", ed.FP64)):
-        srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch)
+        srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1)  # pool mapped up front
         w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs[:8]]  # warm-up
         srv.run(w)
         t0 = time.perf_counter()
@@ -584,7 +584,7 @@ def run_serve(args):
 
     reqs = serve_requests(args.requests)
     prec = ed.FP32 if args.precision == "mixed" else ed.FP64
-    srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch)
+    srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1)  # pool mapped up front
     w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for _, n, b, nev, sd in reqs[:16]]
     srv.run(w)
     pending = {}

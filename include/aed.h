@@ -261,6 +261,9 @@ typedef struct {
   int32_t precision;         /* AED_FP32 (mixed) or AED_FP64                           */
   double hbm_fraction;       /* budget as a fraction of free memory (default 0.8)      */
   int64_t hbm_budget_bytes;  /* explicit budget in bytes (overrides hbm_fraction)      */
+  int64_t reserve_bytes;     /* device memory mapped into the server's pool at creation
+                                (-1: the whole budget; 0: none), so that requests do not
+                                pay for mapping fresh memory on first use               */
 } aed_server_opts;
 
 typedef struct {

@@ -134,3 +134,15 @@ def test_cancel_and_continuous_batching():
     assert e.value.code == ed.ERR_CANCELLED
     assert done[b]["seconds"] > 0
     srv.close()
+
+
+def test_reserved_pool_serves_requests():
+    """A server that maps its budget into the memory pool at creation gives the same results."""
+    reqs = mixed_requests(77, 6)
+    srv = ed.Server(precision=ed.FP32, max_slots=16, steps=8, hbm_budget=1 << 30, reserve=-1)
+    tickets = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+    res = srv.run(tickets)
+    for t, (n, b, nev, sd) in zip(tickets, reqs):
+        ref = reference(n, b, nev)
+        assert np.all(np.abs(res[t]["evals"] - ref) / np.abs(ref) <= 1e-9)
+    srv.close()
