@@ -529,7 +529,7 @@ int parse_parameters(const char* text, ParsedParams& out) {
       return fail(AED_ERR_INVALID,
                   "TRANSLATION_SYMMETRY must be false: momentum sectors are not supported (factory.C:17-30)");
     if (!p.has("Sz_total"))
-      return fail(AED_ERR_INVALID, "Sz_total must be given (the loop over all Sz sectors is not supported)");
+      return fail(AED_ERR_INVALID, "Sz_total must be given (one sector per handle; alps_b200.sparsediag loops over them)");
     const int Lx = (int)std::lround(ev.name("L"));
     int Wy = 1;
     if (L.dim == 2) Wy = p.has("W") ? (int)std::lround(ev.name("W")) : (int)std::lround(ev.expr_str(L.ext_w_default));

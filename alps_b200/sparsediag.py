@@ -1,0 +1,114 @@
+"""The sparsediag task around the engine: the loop over Sz sectors and the results.
+
+Reference paths are relative to the ALPS source tree.
+
+`run(params)` follows DiagMatrix::dostep (applications/diag/diag.h:85-137) for
+the Sz-conserved spin-1/2 models the engine handles: when `Sz_total` is not
+given, every Sz_total from -N/2 to N/2 (step 1; diag.h:142-175 takes the range
+from the site bases) is a sector, each solved by SparseDiagMatrix::do_subspace
+(here `Hamiltonian.solve`, NUMBER_EIGENVALUES / MAX_ITERATIONS from the
+parameters); a fixed `Sz_total` gives one sector without quantum-number labels,
+as in the reference.  The ground-state energy and the gap are chosen as in
+SparseDiagMatrix::write_xml_body (sparsediag.h:59-90), and `write_xml` writes
+the EIGENVALUES and AVERAGES elements of DiagTask::write_xml_body
+(src/alps/scheduler/diag.hpp:127-140) and sparsediag.h:80-88.  (The HDF5
+archive, diag.hpp:112-124, needs h5py, which this image lacks.)
+"""
+
+from __future__ import annotations
+
+from fractions import Fraction
+from xml.sax.saxutils import escape
+
+import numpy as np
+
+from . import AEDError, FP64, Hamiltonian, model_from_parameters
+
+
+def half_integer_text(v: Fraction) -> str:
+    """alps::half_integer printing (src/alps/model/half_integer.h:243-253): "3", "-1/2"."""
+    twice = int(2 * v)
+    return str(twice // 2) if twice % 2 == 0 else f"{twice}/2"
+
+
+def _site_count(params: dict) -> int:
+    """Number of sites of the lattice (the parser needs a compatible Sz_total)."""
+    for trial in (0, 0.5):
+        try:
+            return model_from_parameters(dict(params, Sz_total=trial))["n_sites"]
+        except AEDError:
+            continue
+    raise AEDError(-1, "cannot read the lattice from the parameters")
+
+
+def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
+    """Eigenvalues of every sector: {"sectors": [{"quantumnumbers": [(name, value)], "energies": array,
+    "dimension": D, "iterations": m}], "ground_state_energy": E0, "energy_gap": gap}."""
+    params = dict(params)
+    qns = str(params.get("CONSERVED_QUANTUMNUMBERS", "")).replace(",", " ").split()
+    sectors = []
+    if "Sz_total" in params or "Sz" not in qns:
+        sz_values = [None]
+    else:
+        n = _site_count(params)
+        sz_values = [Fraction(k, 2) for k in range(-n, n + 1, 2)]
+    for sz in sz_values:
+        p = params if sz is None else dict(params, Sz_total=float(sz))
+        ham = Hamiltonian.from_parameters(p, precision=precision, device=device)
+        try:
+            if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
+                continue
+            r = ham.solve(nev=max(1, ham.params["nev"]), max_iter=ham.params["max_iter"], seed=seed)
+            sectors.append({"quantumnumbers": [] if sz is None else [("Sz", half_integer_text(sz))],
+                            "energies": np.array(r["evals"]), "dimension": ham.dim,
+                            "iterations": r["iterations"], "converged": r["converged"]})
+        finally:
+            ham.close()
+    e0, gap = ground_state_and_gap([s["energies"] for s in sectors])
+    return {"sectors": sectors, "ground_state_energy": e0, "energy_gap": gap}
+
+
+def ground_state_and_gap(energies):
+    """(ground-state energy, gap) over sectors as SparseDiagMatrix::write_xml_body picks them
+    (sparsediag.h:62-76): the lowest value, and the next one among each sector's lowest (and the
+    second of the sector holding the minimum when it is found); None where undefined."""
+    inf = float("inf")
+    min_val = exc_val = inf
+    for ev in energies:
+        ev = np.asarray(ev)
+        if ev.size >= 1:
+            if ev[0] < min_val:
+                exc_val = min_val
+                min_val = float(ev[0])
+                if ev.size >= 2 and ev[1] < exc_val:
+                    exc_val = float(ev[1])
+            elif ev[0] < exc_val:
+                exc_val = float(ev[0])
+    return (None if min_val == inf else min_val), (None if exc_val == inf else exc_val - min_val)
+
+
+def write_xml(result: dict, path: str, params: dict | None = None) -> None:
+    """The spectrum in the reference's XML elements (diag.hpp:127-140, sparsediag.h:80-88)."""
+    lines = ["<?xml version=\"1.0\" encoding=\"UTF-8\"?>", "<SIMULATION>"]
+    if params:
+        lines.append("  <PARAMETERS>")
+        for k, v in params.items():
+            lines.append(f"    <PARAMETER name=\"{escape(str(k))}\">{escape(str(v))}</PARAMETER>")
+        lines.append("  </PARAMETERS>")
+    lines.append("  <AVERAGES>")
+    if result["ground_state_energy"] is not None:
+        lines.append("    <SCALAR_AVERAGE name=\"Ground State Energy\"><MEAN>"
+                     f"{result['ground_state_energy']!r}</MEAN></SCALAR_AVERAGE>")
+    if result["energy_gap"] is not None:
+        lines.append(f"    <SCALAR_AVERAGE name=\"Energy Gap\"><MEAN>{result['energy_gap']!r}</MEAN></SCALAR_AVERAGE>")
+    lines.append("  </AVERAGES>")
+    for s in result["sectors"]:
+        ev = s["energies"]
+        lines.append(f"  <EIGENVALUES number=\"{ev.size}\">")
+        for name, value in s["quantumnumbers"]:
+            lines.append(f"    <QUANTUMNUMBER name=\"{escape(name)}\" value=\"{escape(value)}\"/>")
+        lines += [f"{float(e)!r}" for e in ev]
+        lines.append("  </EIGENVALUES>")
+    lines.append("</SIMULATION>")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

@@ -165,3 +165,26 @@ def test_engine_tmatrix_matches_oracle_and_lapack(L, nev, seed):
         assert list(t["mults"]) == list(lp["mults"])
         # error estimates are |beta z_last|; below ~eps*|T| they are rounding noise
         np.testing.assert_allclose(t["errors"], lp["errors"], rtol=1e-5, atol=1e-13)
+
+
+def test_sparsediag_gap_rule_and_labels(tmp_path):
+    """The ground state / gap choice of sparsediag.h:62-76 and the half-integer labels."""
+    from fractions import Fraction
+    import xml.etree.ElementTree as ET
+
+    from alps_b200 import sparsediag
+
+    e0, gap = sparsediag.ground_state_and_gap([[-1.0, -0.5], [-2.0, -1.2], [-1.5]])
+    assert e0 == -2.0 and gap == pytest.approx(0.5)  # -1.5 (another sector) lies below -1.2
+    e0, gap = sparsediag.ground_state_and_gap([[-2.0, -1.9], [-1.0]])
+    assert gap == pytest.approx(0.1)
+    assert sparsediag.ground_state_and_gap([[-3.0]]) == (-3.0, None)
+    assert [sparsediag.half_integer_text(Fraction(k, 2)) for k in (-3, -2, 0, 1, 4)] == ["-3/2", "-1", "0", "1/2", "2"]
+    res = {"sectors": [{"quantumnumbers": [("Sz", "1/2")], "energies": np.array([-1.25, -0.75])}],
+           "ground_state_energy": -1.25, "energy_gap": 0.5}
+    sparsediag.write_xml(res, str(tmp_path / "s.xml"), {"LATTICE": "chain lattice", "L": 5})
+    root = ET.parse(tmp_path / "s.xml").getroot()
+    ev = root.find("EIGENVALUES")
+    assert ev.get("number") == "2" and ev.find("QUANTUMNUMBER").get("value") == "1/2"
+    text = (ev.text or "") + "".join(c.tail or "" for c in ev)
+    assert [float(v) for v in text.split()] == [-1.25, -0.75]
