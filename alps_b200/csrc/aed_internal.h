@@ -94,8 +94,8 @@ void build_lo_table(const BasisTables& t, const HvParams& P, std::vector<uint32_
 // Work tiles over the sector: (hi block h, first row r0 within the block).
 void build_tiles(const BasisTables& t, int tile_rows, std::vector<uint32_t>& th, std::vector<uint32_t>& tr,
                  std::vector<uint32_t>* tfirst = nullptr);
-// Hi blocks grouped by lo popcount (largest blocks first, h ascending within a
-// group), each group padded with kNoBlockEntry to a multiple of kBundleMax, so
+// Hi blocks grouped by lo popcount (largest blocks first, bit-reversed h
+// ascending within a group), each group padded with kNoBlockEntry to a multiple of kBundleMax, so
 // that bundles of 1, 2 or 4 consecutive entries never mix groups.  *maxrows:
 // rows of the largest block.
 // Crossing-flip table: entry b * 2^Nlo + looff[k] + r is the rank (within

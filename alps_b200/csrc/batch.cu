@@ -47,16 +47,18 @@ __device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v6
 // instance's tables; the staged pairs and the shared-memory layout change
 // with the instance.  One kernel per phase and block size, so that each has
 // the registers of its own path: FP32 vectors with small hi blocks
-// (maxrows <= kSmallBlock: 1 row per thread, 6 CTAs per SM -- 1.45x the
-// solves/s of 2 rows per thread on the 512-chain batch of L = 12..22) or
-// larger ones (2 rows per thread, 4 CTAs per SM), and FP64 vectors (b_hv64:
+// (maxrows <= kSmallBlock: one block at a time, 1 row per thread, 6 CTAs per
+// SM -- 1.45x the solves/s of 2 rows per thread on the 512-chain batch of
+// L = 12..22) or larger ones (both blocks of an item at once, 2 rows per
+// thread, 4 CTAs per SM, as the single-instance blk2r2b4), and FP64 vectors (b_hv64:
 // 4 rows per thread, 3 CTAs per SM).
 constexpr int kSmallBlock = 512;
 
-template <int R, int MINB, bool kSmall>
+template <int R, int MINB, int B, bool kSmall>
 __global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a) {
+  static_assert(B == 1 || B == kBatchBundle, "an item is one bundle or its blocks one by one");
   extern __shared__ __align__(16) unsigned char b_dyn[];
-  __shared__ bapply::BundleSmem<1> sm;
+  __shared__ bapply::BundleSmem<B> sm;
   const int n = *a.n_tiles;
   int cur = -1, rc = 0;
   float* xs = nullptr;
@@ -68,14 +70,19 @@ __global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a) {
     const int j = I.j;
     if (w.inst != cur) {
       __syncthreads();  // the previous block is done with the staged pairs
-      xs = bapply::carve<float, 1>(*I.P, I.t, b_dyn, sm);
-      bapply::stage_pairs<1>(*I.P, sm);
+      xs = bapply::carve<float, B>(*I.P, I.t, b_dyn, sm);
+      bapply::stage_pairs<B>(*I.P, sm);
       cur = w.inst;
     }
     const ApplyCtx c = apply::ctx_of(*I.P);
-    for (int q = 0; q < kBatchBundle; ++q)  // the item's blocks one at a time (block-list entries)
-      bapply::apply_bundle<float, AccWide32, R, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, low_vec(I, j),
-                                                   low_vec(I, j + 1), I.partA, sm, xs, rc);
+    if (B == kBatchBundle) {  // both blocks of the item at once
+      bapply::apply_bundle<float, AccWide32, R, B>(c, I.t, w.idx, low_vec(I, j), low_vec(I, j + 1), I.partA, sm, xs,
+                                                   rc);
+    } else {
+      for (int q = 0; q < kBatchBundle; ++q)  // the item's blocks one at a time (block-list entries)
+        bapply::apply_bundle<float, AccWide32, R, B>(c, I.t, (int64_t)w.idx * kBatchBundle + q, low_vec(I, j),
+                                                     low_vec(I, j + 1), I.partA, sm, xs, rc);
+    }
   }
 }
 
@@ -350,8 +357,8 @@ int sms() {
 }
 
 int g_hv32s = 0, g_hv32s_smem = -1, g_hv32l = 0, g_hv32l_smem = -1, g_hv64 = 0, g_hv64_smem = -1;
-#define B_HV32_SMALL b_hv32<1, 6, true>
-#define B_HV32_LARGE b_hv32<2, 4, false>
+#define B_HV32_SMALL b_hv32<1, 6, 1, true>
+#define B_HV32_LARGE b_hv32<2, 4, kBatchBundle, false>
 
 // Grid of an apply kernel for `smem` bytes of dynamic shared memory (cached per size).
 template <typename K>
@@ -375,7 +382,9 @@ int check(const char* what) {
 }  // namespace
 
 size_t batch_hv_smem_bytes(int maxrows, const HvParams& P) {
-  return bapply::bundle_smem_bytes<double>(1, maxrows, P.n_pairs, P.n_lolo);
+  const size_t f64 = bapply::bundle_smem_bytes<double>(1, maxrows, P.n_pairs, P.n_lolo);
+  const size_t f32 = bapply::bundle_smem_bytes<float>(kBatchBundle, maxrows, P.n_pairs, P.n_lolo);
+  return f64 > f32 ? f64 : f32;
 }
 
 size_t batch_hv_smem_limit() {

@@ -87,8 +87,8 @@ struct BatchArgs {
 // Hi blocks per work item of the batched apply (entries ub * kBatchBundle ..
 // of a sector's block list, applied one block at a time).
 constexpr int kBatchBundle = 2;
-// Dynamic shared memory the batched apply needs for one instance (FP64 size,
-// which also covers its FP32 phase).
+// Dynamic shared memory the batched apply needs for one instance (the larger
+// of its FP64 layout, one block, and its FP32 layout, two blocks).
 size_t batch_hv_smem_bytes(int maxrows, const HvParams& P);
 // Largest dynamic shared memory a CTA of the batched apply may take on this device.
 size_t batch_hv_smem_limit();
