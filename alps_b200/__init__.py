@@ -123,6 +123,7 @@ def lib():
             "aed_create": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(_P)]),
             "aed_destroy": (ctypes.c_int, [_P]),
+            "aed_empty_cache": (ctypes.c_int, [ctypes.c_int]),
             "aed_set_couplings": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc)]),
             "aed_dimension": (ctypes.c_int, [_P, _I64P]),
             "aed_basis_copy": (ctypes.c_int, [_P, _U32P, _I64, _I64]),
@@ -199,6 +200,11 @@ def apply_variants() -> list:
     """Names of the apply variants (index = the `variant` of Hamiltonian.time_apply)."""
     L = lib()
     return [L.aed_apply_variant_name(v).decode() for v in range(L.aed_apply_variant_count())]
+
+
+def empty_cache(device: int = 0) -> None:
+    """Give the memory cached from destroyed handles back to the driver (aed_empty_cache)."""
+    _check(lib().aed_empty_cache(device))
 
 
 def launch_count() -> int:

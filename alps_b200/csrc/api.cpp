@@ -13,6 +13,114 @@
 namespace aed {
 const char* last_error_cstr();
 
+// ---- memory of handles ------------------------------------------------------------
+namespace {
+
+std::mutex g_mem_mu;
+// device blocks not in use, by (device, size); every cached device block's size
+std::multimap<std::pair<int, size_t>, void*> g_dev_free;
+std::map<void*, std::pair<int, size_t>> g_dev_block;
+std::multimap<size_t, void*> g_host_free;  // pinned blocks not in use, by size
+std::map<void*, size_t> g_host_size;       // every pinned block of the cache
+
+constexpr size_t kDevRound = (size_t)2 << 20;  // device blocks: multiples of 2 MiB (the driver's own granule)
+
+size_t dev_block_bytes(size_t bytes) {
+  if (bytes < kDevRound) return (bytes + 255) & ~(size_t)255;
+  return (bytes + kDevRound - 1) & ~(kDevRound - 1);
+}
+size_t host_block_bytes(size_t bytes) { return (bytes + 4095) & ~(size_t)4095; }
+
+void trim_device(int dev) {  // callers hold g_mem_mu
+  for (auto it = g_dev_free.begin(); it != g_dev_free.end();) {
+    if (it->first.first == dev) {
+      cudaFree(it->second);
+      g_dev_block.erase(it->second);
+      it = g_dev_free.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+}  // namespace
+
+int mem_dev_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  AED_CUDA_TRY(cudaGetDevice(&dev));
+  const size_t b = dev_block_bytes(bytes ? bytes : 8);
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  // the smallest cached block that fits and wastes at most half of itself
+  auto it = g_dev_free.lower_bound({dev, b});
+  if (it != g_dev_free.end() && it->first.first == dev && it->first.second <= 2 * b) {
+    *p = it->second;
+    g_dev_free.erase(it);
+    return AED_OK;
+  }
+  cudaError_t e = cudaMalloc(p, b);
+  if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and try once more
+    cudaGetLastError();
+    trim_device(dev);
+    e = cudaMalloc(p, b);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(AED_ERR_NOMEM, std::string("device allocation of ") + std::to_string(bytes) +
+                                   " bytes: " + cudaGetErrorString(e));
+  }
+  g_dev_block[*p] = {dev, b};
+  return AED_OK;
+}
+
+void mem_dev_free(void* p, cudaStream_t st) {
+  if (!p) return;
+  cudaStreamSynchronize(st);  // no work queued so far on st uses the block any more
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  auto it = g_dev_block.find(p);
+  if (it != g_dev_block.end()) g_dev_free.emplace(it->second, p);
+}
+
+int mem_host_alloc(void** p, size_t bytes) {
+  const size_t b = host_block_bytes(bytes ? bytes : 8);
+  {
+    std::lock_guard<std::mutex> lk(g_mem_mu);
+    auto it = g_host_free.find(b);
+    if (it != g_host_free.end()) {
+      *p = it->second;
+      g_host_free.erase(it);
+      return AED_OK;
+    }
+  }
+  if (cudaMallocHost(p, b) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(AED_ERR_NOMEM, "pinned host allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  g_host_size[*p] = b;
+  return AED_OK;
+}
+
+void mem_host_free(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  auto it = g_host_size.find(p);
+  if (it != g_host_size.end()) g_host_free.emplace(it->second, p);
+}
+
+void mem_empty_cache(int device) {
+  DeviceGuard g(device);
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  trim_device(device);
+  for (auto& f : g_host_free) {
+    cudaFreeHost(f.second);
+    g_host_size.erase(f.second);
+  }
+  g_host_free.clear();
+}
+
 namespace {
 
 template <typename T>
@@ -31,23 +139,15 @@ int dev_alloc(T** p, size_t count) {
 void release(aed_handle* h) {
   if (!h) return;
   handle_release_workspace(h);
-  cudaFree(h->d_thi);
-  cudaFree(h->d_tlo);
-  cudaFree(h->d_lolist);
-  cudaFree(h->d_looff);
-  cudaFree(h->d_tile_h);
-  cudaFree(h->d_tile_r);
-  cudaFree(h->d_blk_h);
-  cudaFree(h->d_tfirst);
-  cudaFree(h->d_dg);
-  cudaFree(h->d_ell);
-  cudaFree(h->d_xtab);
-  cudaFree(h->d_partA);
-  cudaFree(h->d_partB);
-  cudaFree(h->d_scal);
-  cudaFree(h->d_start64);
-  if (h->h_scal) cudaFreeHost(h->h_scal);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  for (void* p : {(void*)h->d_thi, (void*)h->d_tlo, (void*)h->d_lolist, (void*)h->d_looff, (void*)h->d_tile_h,
+                  (void*)h->d_tile_r, (void*)h->d_blk_h, (void*)h->d_tfirst, (void*)h->d_dg, (void*)h->d_ell,
+                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64})
+    mem_dev_free(p, h->stream);
+  mem_host_free(h->h_scal);
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);  // the frees are done: the memory is back in the pool
+    cudaStreamDestroy(h->stream);
+  }
   delete h;
 }
 
@@ -58,10 +158,10 @@ int upload_lo_table(aed_handle* h) {
   build_lo_table(h->tab, h->P, ell, &W);
   cudaStreamSynchronize(h->stream);  // no apply reads the old table any more
   if (ell.size() + 1 > h->d_ell_n) {  // grow only: new couplings usually keep the width
-    cudaFree(h->d_ell);
+    mem_dev_free(h->d_ell, h->stream);
     h->d_ell = nullptr;
     h->d_ell_n = 0;
-    const int rc = dev_alloc(&h->d_ell, ell.size() + 1);
+    const int rc = mem_dev_alloc_n(&h->d_ell, ell.size() + 1);
     if (rc) return rc;
     h->d_ell_n = ell.size() + 1;
   }
@@ -84,19 +184,11 @@ int check_vec(const aed_handle* h, const void* p, const char* name) {
 
 int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out) {
   if (bytes > h->ws_bytes[slot]) {
-    if (h->ws[slot]) {
-      cudaStreamSynchronize(h->stream);
-      cudaFree(h->ws[slot]);
-    }
+    mem_dev_free(h->ws[slot], h->stream);
     h->ws[slot] = nullptr;
     h->ws_bytes[slot] = 0;
-    const cudaError_t e = cudaMalloc(&h->ws[slot], bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      h->ws[slot] = nullptr;
-      return fail(AED_ERR_NOMEM, std::string("workspace of ") + std::to_string(bytes) +
-                                     " bytes: " + cudaGetErrorString(e));
-    }
+    const int rc = mem_dev_alloc(&h->ws[slot], bytes);
+    if (rc) return rc;
     h->ws_bytes[slot] = bytes;
   }
   *out = h->ws[slot];
@@ -105,14 +197,16 @@ int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out) {
 
 int handle_pinned(aed_handle* h, size_t n, double** out) {
   if (n > h->h_ab_n) {
-    if (h->h_ab) cudaFreeHost(h->h_ab);
+    if (h->h_ab) {
+      cudaStreamSynchronize(h->stream);  // no copy into the old buffer in flight
+      mem_host_free(h->h_ab);
+    }
     h->h_ab = nullptr;
     h->h_ab_n = 0;
-    if (cudaMallocHost((void**)&h->h_ab, n * sizeof(double)) != cudaSuccess) {
-      cudaGetLastError();
-      h->h_ab = nullptr;
-      return fail(AED_ERR_NOMEM, "pinned host allocation failed");
-    }
+    void* p = nullptr;
+    const int rc = mem_host_alloc(&p, n * sizeof(double));
+    if (rc) return rc;
+    h->h_ab = static_cast<double*>(p);
     h->h_ab_n = n;
   }
   *out = h->h_ab;
@@ -121,15 +215,13 @@ int handle_pinned(aed_handle* h, size_t n, double** out) {
 
 void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes) {
   if (chunk_bytes != h->store_chunk_bytes) {
-    cudaStreamSynchronize(h->stream);
-    for (void* p : h->store_chunks) cudaFree(p);
+    for (void* p : h->store_chunks) mem_dev_free(p, h->stream);
     h->store_chunks.clear();
     h->store_chunk_bytes = chunk_bytes;
   }
   while ((int)h->store_chunks.size() <= c) {
     void* p = nullptr;
-    if (cudaMalloc(&p, chunk_bytes) != cudaSuccess) {
-      cudaGetLastError();
+    if (mem_dev_alloc(&p, chunk_bytes)) {
       fail(AED_ERR_NOMEM, "device memory exhausted by the FP32 Lanczos basis (" +
                               std::to_string(h->store_chunks.size() * kStoreChunk) + " vectors)");
       return nullptr;
@@ -141,15 +233,18 @@ void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes) {
 
 void handle_release_workspace(aed_handle* h) {
   h->rec_live = false;
-  for (void* p : h->store_chunks) cudaFree(p);
+  for (void* p : h->store_chunks) mem_dev_free(p, h->stream);
   h->store_chunks.clear();
   h->store_chunk_bytes = 0;
   for (int k = 0; k < 2; ++k) {
-    if (h->ws[k]) cudaFree(h->ws[k]);
+    mem_dev_free(h->ws[k], h->stream);
     h->ws[k] = nullptr;
     h->ws_bytes[k] = 0;
   }
-  if (h->h_ab) cudaFreeHost(h->h_ab);
+  if (h->h_ab) {
+    cudaStreamSynchronize(h->stream);  // no copy into it in flight
+    mem_host_free(h->h_ab);
+  }
   h->h_ab = nullptr;
   h->h_ab_n = 0;
 }
@@ -318,25 +413,24 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   build_block_list(h->tab, blk, &maxrows);
   build_cross_table(h->tab, xt);
   const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
-  if ((rc = dev_alloc(&h->d_thi, nhi)) || (rc = dev_alloc(&h->d_tlo, nlo)) || (rc = dev_alloc(&h->d_lolist, nlo)) ||
-      (rc = dev_alloc(&h->d_looff, h->tab.looff.size())) || (rc = dev_alloc(&h->d_tile_h, th.size())) ||
-      (rc = dev_alloc(&h->d_tile_r, tr.size())) || (rc = dev_alloc(&h->d_scal, 8)) ||
-      (rc = dev_alloc(&h->d_blk_h, blk.size() + 1)) || (rc = dev_alloc(&h->d_tfirst, tf.size() + 1)) ||
-      (rc = dev_alloc(&h->d_xtab, xt.size() + 1)) ||
-      (rc = dev_alloc(&h->d_dg, (size_t)h->tab.D))) {
-    release(h);
-    return rc;
-  }
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMallocHost((void**)&h->h_scal, 8 * sizeof(double)) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     release(h);
-    return fail(AED_ERR_CUDA, "stream / pinned memory creation failed");
+    return fail(AED_ERR_CUDA, "stream creation failed");
   }
-  if ((rc = dev_alloc(&h->d_partA, th.size() + 1)) || (rc = dev_alloc(&h->d_partB, (size_t)red_chunks(h->tab.D) + 1))) {
+  void* hs = nullptr;
+  if ((rc = mem_dev_alloc_n(&h->d_thi, nhi)) || (rc = mem_dev_alloc_n(&h->d_tlo, nlo)) ||
+      (rc = mem_dev_alloc_n(&h->d_lolist, nlo)) || (rc = mem_dev_alloc_n(&h->d_looff, h->tab.looff.size())) ||
+      (rc = mem_dev_alloc_n(&h->d_tile_h, th.size())) || (rc = mem_dev_alloc_n(&h->d_tile_r, tr.size())) ||
+      (rc = mem_dev_alloc_n(&h->d_scal, 8)) || (rc = mem_dev_alloc_n(&h->d_blk_h, blk.size() + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_tfirst, tf.size() + 1)) || (rc = mem_dev_alloc_n(&h->d_xtab, xt.size() + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_dg, (size_t)h->tab.D)) || (rc = mem_dev_alloc_n(&h->d_partA, th.size() + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_partB, (size_t)red_chunks(h->tab.D) + 1)) ||
+      (rc = mem_host_alloc(&hs, 8 * sizeof(double)))) {
     release(h);
     return rc;
   }
+  h->h_scal = static_cast<double*>(hs);
   cudaMemcpyAsync(h->d_thi, h->tab.thi.data(), nhi * 4, cudaMemcpyHostToDevice, h->stream);
   cudaMemcpyAsync(h->d_tlo, h->tab.tlo.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
   cudaMemcpyAsync(h->d_lolist, h->tab.lolist.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
@@ -415,6 +509,16 @@ int aed_destroy(aed_handle* h) {
   DeviceGuard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   release(h);
+  return AED_OK;
+}
+
+int aed_empty_cache(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return fail(AED_ERR_INVALID, "device index out of range");
+  }
+  mem_empty_cache(device);
   return AED_OK;
 }
 

@@ -32,6 +32,9 @@ using apply::TileOp;
 constexpr uint32_t kNoBlock = 0xffffffffu;
 constexpr int kWarps = kHvThreads / 32;
 
+// Start moving the line holding p from HBM into L2 (no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Shared memory of a CTA.  The arrays sized by the sector live in dynamic
 // shared memory (bundle_smem_bytes), so that small flip lists leave room for
 // more CTAs per SM: x of the B blocks (B * maxrows values), the B compiled
@@ -187,6 +190,13 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
   }
   Acc acc[B][R];
   if (kOrdered) {
+    // M(i,i) is added in the middle of the row: start its fetch from HBM now,
+    // so that the load at its column finds it in L2
+#pragma unroll
+    for (int j = 0; j < B; ++j)
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (j < nv && (uint32_t)u < nrow) prefetch_l2(t.dg + q.bj[j] + rt + u * kHvThreads);
     // flips to smaller states outside the lo part; the lo part with the
     // diagonal at its column; the larger states outside the lo part
 #pragma unroll
@@ -196,32 +206,39 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
     bool dd[R];
 #pragma unroll
     for (int u = 0; u < R; ++u) dd[u] = false;
-    for (int e = 0; e < t.ell_w; ++e) {
-      uint32_t ent[R];
+    // two table entries per round trip (loaded together, added in order)
+    constexpr int UE = 2;
+    for (int e = 0; e < t.ell_w; e += UE) {
+      uint32_t ent[UE][R];
       bool any = false;
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        ent[u] = (uint32_t)u < nrow ? __ldg(q.E + (size_t)e * nk + rt + u * kHvThreads) : kEllPad;
-        any |= ent[u] != kEllPad;
-      }
+      for (int v = 0; v < UE; ++v)
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          ent[v][u] = ((uint32_t)u < nrow && e + v < t.ell_w) ? __ldg(q.E + (size_t)(e + v) * nk + rt + u * kHvThreads)
+                                                               : kEllPad;
+          any |= ent[v][u] != kEllPad;
+        }
       if (!__any_sync(0xffffffffu, any)) break;
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        if (ent[u] != kEllPad) {
-          const uint32_t r = rt + u * kHvThreads;
-          const uint32_t rp = ent[u] & 0xffffu;
-          if (!dd[u] && rp > r) {
+      for (int v = 0; v < UE; ++v)
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (ent[v][u] != kEllPad) {
+            const uint32_t r = rt + u * kHvThreads;
+            const uint32_t rp = ent[v][u] & 0xffffu;
+            if (!dd[u] && rp > r) {
+#pragma unroll
+              for (int j = 0; j < B; ++j)
+                if (j < nv) acc[j][u].add(__ldg(t.dg + q.bj[j] + r), q.xs[(size_t)j * q.maxrows + r]);
+              dd[u] = true;
+            }
+            const double cq = sm.lolo_c[ent[v][u] >> 16];
 #pragma unroll
             for (int j = 0; j < B; ++j)
-              if (j < nv) acc[j][u].add(__ldg(t.dg + q.bj[j] + r), q.xs[(size_t)j * q.maxrows + r]);
-            dd[u] = true;
+              if (j < nv) acc[j][u].add(cq, q.xs[(size_t)j * q.maxrows + rp]);
           }
-          const double cq = sm.lolo_c[ent[u] >> 16];
-#pragma unroll
-          for (int j = 0; j < B; ++j)
-            if (j < nv) acc[j][u].add(cq, q.xs[(size_t)j * q.maxrows + rp]);
         }
-      }
     }
 #pragma unroll
     for (int u = 0; u < R; ++u) {
@@ -339,12 +356,21 @@ __device__ __forceinline__ void apply_bundle(const ApplyCtx& c, const DevTables&
       sm.nops[warp] = cnt;
     }
   }
+  // x of the blocks into shared memory, four loads in flight per thread
+  constexpr int kStage = 4;
 #pragma unroll
   for (int j = 0; j < B; ++j) {
     if (j < nv) {
       const T* src = x + bj[j];
       T* dst = xs + (size_t)j * t.maxrows;
-      for (uint32_t i = threadIdx.x; i < nk; i += kHvThreads) dst[i] = __ldg(src + i);
+      for (uint32_t i0 = threadIdx.x; i0 < nk; i0 += kStage * kHvThreads) {
+        T v[kStage];
+#pragma unroll
+        for (int a = 0; a < kStage; ++a) v[a] = i0 + a * kHvThreads < nk ? __ldg(src + i0 + a * kHvThreads) : T(0);
+#pragma unroll
+        for (int a = 0; a < kStage; ++a)
+          if (i0 + a * kHvThreads < nk) dst[i0 + a * kHvThreads] = v[a];
+      }
     }
   }
   __syncthreads();

@@ -70,6 +70,27 @@ struct DeviceGuard {
   }
 };
 
+// Memory of handles.  Device and pinned host memory come from per-process
+// free lists that keep what handles give back, so that a loop of create /
+// solve / destroy allocates once instead of paying cudaFree (a device-wide
+// synchronisation) and cudaMallocHost / cudaFreeHost for every handle.
+// aed_empty_cache returns the blocks not in use; a failed cudaMalloc does so
+// for its device and tries again.
+// mem_dev_free(p, st): waits for the work queued on st so far, then caches p.
+int mem_dev_alloc(void** p, size_t bytes);
+void mem_dev_free(void* p, cudaStream_t st);
+int mem_host_alloc(void** p, size_t bytes);
+void mem_host_free(void* p);
+void mem_empty_cache(int device);
+
+template <typename T>
+int mem_dev_alloc_n(T** p, size_t count) {
+  void* v = nullptr;
+  const int rc = mem_dev_alloc(&v, (count ? count : 1) * sizeof(T));
+  *p = static_cast<T*>(v);
+  return rc;
+}
+
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
 // Choose the apply variant for this precision now (timed launches on x, y)
 // unless already chosen; handle_hv does this on its first call otherwise.

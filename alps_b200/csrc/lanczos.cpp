@@ -372,14 +372,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
       (rc = handle_pinned(h, (size_t)2 * (cap + 2), &hab)) || (rc = ring.init()))
     return rc;
   // the FP64 phase's start stays with the handle (eigenvector replay)
-  if (!h->d_start64) {
-    const cudaError_t e = cudaMalloc((void**)&h->d_start64, (size_t)D * 8);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      h->d_start64 = nullptr;
-      return fail(AED_ERR_NOMEM, "device memory for the refinement start vector");
-    }
-  }
+  if (!h->d_start64 && (rc = mem_dev_alloc_n(&h->d_start64, (size_t)D))) return rc;
   double* start64 = h->d_start64;
   double* d_ab = (double*)small;
   double* coef = (double*)((char*)small + ab_bytes);

@@ -99,7 +99,14 @@ typedef struct aed_handle aed_handle;
  * src/alps/model/basisstates.h:175-278).  No explicit matrix is stored: the
  * apply is matrix-free. */
 int aed_create(const aed_model_desc* model, int precision, int device, aed_handle** out);
+/* Device and pinned host memory of a destroyed handle goes back to a
+ * per-process cache that the next aed_create reuses (no cudaMalloc / cudaFree
+ * per handle in a create / solve / destroy loop). */
 int aed_destroy(aed_handle* h);
+/* Return the cached memory that no handle uses to the driver (device memory of
+ * `device`, all cached pinned host memory).  No reference counterpart: the
+ * reference's matrices are freed with their task. */
+int aed_empty_cache(int device);
 
 /* Replace the couplings of a handle (same N, n_up; any bond list), keeping its
  * basis tables, workspaces and apply tuning: the parameter sweeps sparsediag

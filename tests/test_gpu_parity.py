@@ -411,3 +411,21 @@ def test_set_couplings_matches_fresh_handle():
     assert np.array_equal(ham.apply(x), ref.mult(x))
     with pytest.raises(ed.AEDError):
         ham.set_couplings([(0, 1, 1.0, 1.0)] * 3 + [(0, 15, 1.0, 1.0)])
+
+
+@pytest.mark.parametrize("prec", [ed.FP64, ed.FP32])
+def test_handles_reuse_cached_memory(prec):
+    """Handles created after others were destroyed take their memory from the per-process cache: every
+    solve of the loop gives the same eigenvalues and recurrence length, before and after empty_cache."""
+    n, bonds = random_bonds("square lattice", {"L": 4, "W": 5}, 3, 0.8, 1.2)
+    got = []
+    for k in range(4):
+        if k == 2:
+            ed.empty_cache(0)
+        ham = ed.Hamiltonian(n, n // 2, bonds, precision=prec)
+        r = ham.solve(nev=2, seed=5)
+        ham.close()
+        got.append((list(r["evals"]), r["iterations"]))
+    assert all(g == got[0] for g in got[1:])
+    with pytest.raises(ed.AEDError):
+        ed.empty_cache(99)
