@@ -54,7 +54,7 @@ FP64_ITERATIONS_FALLBACK = 180  # mean of the first five inputs: 190, 142, 180, 
 # DRAM bytes (read + write) of one launch of the FP64 apply on this workload,
 # per apply variant, from ncu (dram__bytes_read.sum + dram__bytes_write.sum),
 # summarised in profiles/hvb_kernel_l28_fp64.md; null for a variant not captured.
-HV_TRAFFIC_L28_FP64 = {"blk1r4b4": 2.251629e9, "blk1r4b3": 2.235181e9}
+HV_TRAFFIC_L28_FP64 = {"blk1r4b4": 2.243246e9}
 
 
 def j2_stream(n):
