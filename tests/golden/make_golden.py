@@ -11,6 +11,9 @@ Reads (paths relative to the ALPS source tree) and writes JSON beside this scrip
   test/model/example4.output    -> spin_half_example4.json  (two-site HSpinHalf)
   test/lattice/example5.output  -> lattice_example5.json (anisotropic square 10x4 sites)
   test/lattice/example6.output  -> lattice_example6.json (anisotropic square 10x4 bonds)
+  test/model/example13.output   -> bloch_example13.json (4-site chain, Bloch bases at k = 2 pi m / 4)
+  test/model/example14.output   -> bloch_example14.json (2x2 square, k = (0, 0))
+  test/model/example15.output   -> bloch_example15.json (2x2 square, every translation momentum)
 The fixtures are committed; the tests never read the ALPS tree.
 """
 
@@ -83,6 +86,33 @@ def _nested(expr):
     return parse()
 
 
+def _bloch_sections(text):
+    """Split an example13-15 output into sections: translations (phase rounded to one digit, site
+    map) and the built states (normalisation printed with 6 digits, Sz per site)."""
+    sections = []
+    cur = None
+    for line in text.splitlines():
+        m = re.match(r"Momentum:\s*(.*)$", line)
+        if m:
+            cur = {"momentum": [float(v) for v in m.group(1).split()], "translations": [], "states": []}
+            sections.append(cur)
+            continue
+        m = re.match(r"Translation (\d+) with phase \(([-\d.e]+),([-\d.e]+)\) maps (.*)$", line)
+        if m:
+            if cur is None or (int(m.group(1)) == 0 and cur["states"]):
+                cur = {"momentum": None, "translations": [], "states": []}
+                sections.append(cur)
+            mp = [int(b) for a, b in re.findall(r"(\d+)->(\d+)", m.group(4))]
+            cur["translations"].append({"phase": [float(m.group(2)), float(m.group(3))], "map": mp})
+            continue
+        m = re.match(r"([-\d.e]+)\*\[(.*)\] \+ translations", line.strip())
+        if m and cur is not None:
+            kets = re.findall(r"\|\s*(\S+)\s+(\S+)\s*>", m.group(2))
+            cur["states"].append({"norm": float(m.group(1)),
+                                  "sz": [1 if sz == "1/2" else -1 for _s, sz in kets]})
+    return sections
+
+
 def main(alps):
     out = {}
     t = open(os.path.join(alps, "test/model/example10.output")).read()
@@ -126,6 +156,13 @@ def main(alps):
         "params": {"LATTICE": "anisotropic square lattice", "L": 10, "W": 4},
         "bonds": bonds,
     }
+    for ex, lat, L in (("13", "chain lattice", 4), ("14", "square lattice", 2), ("15", "square lattice", 2)):
+        t = open(os.path.join(alps, f"test/model/example{ex}.output")).read()
+        out[f"bloch_example{ex}.json"] = {
+            "source": f"test/model/example{ex}.output",
+            "lattice": lat, "L": L, "constraint": None,
+            "sections": _bloch_sections(t),
+        }
     for name, obj in out.items():
         with open(os.path.join(HERE, name), "w") as f:
             json.dump(obj, f, indent=1)

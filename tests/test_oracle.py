@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
-from oracle import lattice
+from oracle import bloch, lattice
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -207,3 +207,76 @@ def test_csr_is_symmetric_and_matches_matfree():
     y1 = m.mult(x)
     y2 = oracle.hv_matfree(N, m.states(), bonds, x)
     assert np.array_equal(y1, y2)
+
+
+# ---------------------------------------------------------------- momentum sectors
+def _bloch_cases():
+    out = []
+    for ex in ("13", "14", "15"):
+        g = json.load(open(os.path.join(GOLD, f"bloch_example{ex}.json")))
+        params = {"L": g["L"]}
+        n = g["L"] if g["lattice"] == "chain lattice" else g["L"] * g["L"]
+        for isec, sec in enumerate(g["sections"]):
+            if sec["momentum"] is not None:  # example15 prints k
+                k = sec["momentum"]
+                exact = [kk for kk in bloch.translation_momenta(g["lattice"], params)
+                         if np.allclose(kk, k, atol=1e-5)]
+                assert len(exact) == 1
+                k = exact[0]
+            elif ex == "13":  # k = 2 pi m / L, m = section index
+                k = (2.0 * isec * np.pi / n,)
+            else:  # example14: k = (0, 0)
+                k = (0.0, 0.0)
+            out.append((ex, g["lattice"], params, n, k, sec))
+    return out
+
+
+@pytest.mark.parametrize("case", _bloch_cases(), ids=lambda c: f"ex{c[0]}-k{','.join('%.2f' % v for v in c[4])}")
+def test_bloch_translations_and_basis_pinned(case):
+    """Translations (phases, site maps) and the Bloch basis (representatives in order, normalisations)
+    against the reference's test/model/example13-15 outputs."""
+    ex, lat, params, n, k, sec = case
+    tr = bloch.translations(lat, params, k)
+    assert len(tr) == len(sec["translations"])
+    for (phase, mp), g in zip(tr, sec["translations"]):
+        assert mp == g["map"]
+        assert abs(round(phase.real, 1) - g["phase"][0]) < 1e-9 and abs(round(phase.imag, 1) - g["phase"][1]) < 1e-9
+    b = bloch.bloch_basis(n, None, tr)
+    assert len(b["reps"]) == len(sec["states"])
+    for r, nm, g in zip(b["reps"], b["norm"], sec["states"]):
+        sz = [1 if (r >> (n - 1 - i)) & 1 else -1 for i in range(n)]
+        assert sz == g["sz"]
+        assert abs(nm - g["norm"]) <= 5e-6 * g["norm"]
+
+
+def test_bloch_spectra_union_is_the_sector_spectrum():
+    """The eigenvalues of all momentum sectors together are those of the Sz sector (J1-J2 chain and a
+    4x3 square lattice with random couplings per bond type)."""
+    cases = [("chain lattice", {"L": 10}, [(0, 1.0, 1.0), (1, 0.0, 0.0)]),
+             ("nnn chain lattice", {"L": 10}, [(0, 1.0, 1.0), (1, 0.4, 0.4)]),
+             ("square lattice", {"L": 4, "W": 3}, [(0, 1.0, 0.8)]),
+             ("ladder", {"L": 5}, [(0, 1.0, 1.0), (1, 0.7, 0.7)])]
+    for lat, params, types in cases:
+        n, _, graph = lattice.lattice_graph(lat, params)
+        coup = {t: (jz, jxy) for t, jz, jxy in types}
+        bonds = [(s, t, coup[ty][0], coup[ty][1], 0.0) for s, t, ty in graph]
+        for n_up in (n // 2, n // 2 - 1):
+            full = []
+            for k in bloch.translation_momenta(lat, params):
+                b = bloch.bloch_basis(n, n_up, bloch.translations(lat, params, k))
+                M = bloch.hamiltonian(n, bonds, b)
+                assert np.allclose(M, M.conj().T, atol=1e-12)
+                full += list(np.linalg.eigvalsh(M))
+            ref = np.linalg.eigvalsh(_dense_real(n, n_up, bonds, oracle.basis(n, n_up)))
+            assert np.allclose(np.sort(full), ref, atol=1e-10), lat
+
+
+def _dense_real(n, n_up, bonds, st):
+    M = oracle.Matrix(n, n_up, bonds)
+    D = len(st)
+    out = np.zeros((D, D))
+    for j in range(D):
+        e = np.zeros(D)
+        e[j] = 1.0
+        out[:, j] = M.mult(e)
+    return out
