@@ -57,6 +57,11 @@ class ModelDesc(ctypes.Structure):
     ]
 
 
+class Translations(ctypes.Structure):
+    _fields_ = [("n_trans", ctypes.c_int32), ("site_map", ctypes.POINTER(ctypes.c_int32)),
+                ("phase", ctypes.POINTER(ctypes.c_double))]
+
+
 class ParamInfo(ctypes.Structure):
     _fields_ = [
         ("n_sites", ctypes.c_int32), ("n_up", ctypes.c_int32), ("n_bonds", ctypes.c_int32),
@@ -124,6 +129,11 @@ def lib():
                                           ctypes.POINTER(_P)]),
             "aed_destroy": (ctypes.c_int, [_P]),
             "aed_empty_cache": (ctypes.c_int, [ctypes.c_int]),
+            "aed_create_momentum": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.POINTER(Translations),
+                                                   ctypes.c_int, ctypes.POINTER(_P)]),
+            "aed_momentum_basis": (ctypes.c_int, [_P, _U32P, _DP, _I64, _I64]),
+            "aed_lattice_momenta": (ctypes.c_int, [ctypes.c_char_p, _I32P, _I32P, _DP, _I32]),
+            "aed_lattice_translations": (ctypes.c_int, [ctypes.c_char_p, _DP, _I32, _I32P, _I32P, _I32P, _DP, _I32]),
             "aed_set_couplings": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc)]),
             "aed_dimension": (ctypes.c_int, [_P, _I64P]),
             "aed_basis_copy": (ctypes.c_int, [_P, _U32P, _I64, _I64]),
@@ -235,8 +245,7 @@ def parse_parameters(text: str):
             "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
 
 
-def model_from_parameters(params) -> dict:
-    """dict or text of ALPS parameters -> parse_parameters() result."""
+def _params_text(params) -> str:
     if isinstance(params, dict):
         lines = []
         for k, v in params.items():
@@ -244,8 +253,43 @@ def model_from_parameters(params) -> dict:
                 lines.append(f'{k} = "{v}"')
             else:
                 lines.append(f"{k} = {v}")
-        params = "\n".join(lines)
-    return parse_parameters(params)
+        return "\n".join(lines)
+    return params
+
+
+def model_from_parameters(params) -> dict:
+    """dict or text of ALPS parameters -> parse_parameters() result."""
+    return parse_parameters(_params_text(params))
+
+
+def lattice_momenta(params) -> list:
+    """Momenta of the sparsediag sector loop (aed_lattice_momenta): TOTAL_MOMENTUM when given, else every
+    translation momentum when TRANSLATION_SYMMETRY (default true), else []."""
+    txt = _params_text(params).encode()
+    n, nd = ctypes.c_int32(0), ctypes.c_int32(0)
+    _check(lib().aed_lattice_momenta(txt, ctypes.byref(n), ctypes.byref(nd), None, 0))
+    k = np.zeros(max(n.value * nd.value, 1))
+    _check(lib().aed_lattice_momenta(txt, ctypes.byref(n), ctypes.byref(nd), _dp(k), n.value))
+    return [tuple(k[m * nd.value:(m + 1) * nd.value]) for m in range(n.value)]
+
+
+def lattice_translations(params, k) -> list:
+    """[(phase, site map)] of the lattice at momentum k (aed_lattice_translations), the identity first."""
+    txt = _params_text(params).encode()
+    kk = np.ascontiguousarray(k, dtype=np.float64).reshape(-1)
+    nt, ns = ctypes.c_int32(0), ctypes.c_int32(0)
+    _check(lib().aed_lattice_translations(txt, _dp(kk), kk.size, ctypes.byref(nt), ctypes.byref(ns), None, None, 0))
+    mp = np.zeros(max(nt.value * ns.value, 1), np.int32)
+    ph = np.zeros(max(2 * nt.value, 1))
+    _check(lib().aed_lattice_translations(txt, _dp(kk), kk.size, ctypes.byref(nt), ctypes.byref(ns),
+                                          mp.ctypes.data_as(_I32P), _dp(ph), nt.value))
+    return [(complex(ph[2 * t], ph[2 * t + 1]), [int(v) for v in mp[t * ns.value:(t + 1) * ns.value]])
+            for t in range(nt.value)]
+
+
+def momentum_label(k) -> str:
+    """The TOTAL_MOMENTUM value of a sector: alps::write_vector(k), 20 significant digits."""
+    return " ".join("%.20g" % v for v in k)
 
 
 class DeviceVector:
@@ -270,21 +314,22 @@ class DeviceVector:
             pass
 
     def upload(self, host):
-        host = np.ascontiguousarray(host, dtype=np.float64)
-        assert host.size == self.ham.dim
+        host = self.ham._host_vector(host)
         _check(lib().aed_vec_upload(self.ham._h, self.ptr, _dp(host)))
         return self
 
     def download(self):
-        out = np.empty(self.ham.dim)
+        out = np.empty(self.ham.vlen)
         _check(lib().aed_vec_download(self.ham._h, self.ptr, _dp(out)))
-        return out
+        return out.view(np.complex128) if self.ham.momentum else out
 
 
 class Hamiltonian:
-    """One Sz sector of a spin-1/2 model on one GPU (an aed_handle)."""
+    """One Sz sector of a spin-1/2 model on one GPU (an aed_handle); with `translations` (a list of
+    (phase, site map), the identity first, as lattice_translations returns) one momentum sector of it,
+    whose vectors are complex."""
 
-    def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None):
+    def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None, translations=None):
         self.n_sites, self.n_up = int(n_sites), int(n_up)
         self.bonds = [tuple(b) for b in bonds]
         self.precision = precision
@@ -300,11 +345,31 @@ class Hamiltonian:
                          _dp(self._jz), _dp(self._jxy), _dp(self._k), _dp(self._sh), _dp(self._sd))
         h = _P()
         self._h = None
-        _check(lib().aed_create(ctypes.byref(desc), precision, device, ctypes.byref(h)))
+        self.momentum = translations is not None
+        if self.momentum:
+            if precision != FP64:
+                raise AEDError(ERR_INVALID, "momentum sectors are FP64")
+            self._tmap = np.ascontiguousarray([m for _, m in translations], dtype=np.int32).reshape(-1)
+            self._tph = np.ascontiguousarray([[p.real, p.imag] for p, _ in translations], dtype=np.float64)
+            tr = Translations(len(translations), self._tmap.ctypes.data_as(_I32P), _dp(self._tph))
+            _check(lib().aed_create_momentum(ctypes.byref(desc), ctypes.byref(tr), device, ctypes.byref(h)))
+        else:
+            _check(lib().aed_create(ctypes.byref(desc), precision, device, ctypes.byref(h)))
         self._h = h
         d = ctypes.c_int64(0)
         _check(lib().aed_dimension(self._h, ctypes.byref(d)))
         self.dim = d.value
+        self.vlen = 2 * self.dim if self.momentum else self.dim
+
+    def _host_vector(self, v):
+        """A host vector as the engine's layout: float64, interleaved (re, im) in a momentum sector."""
+        if self.momentum:
+            v = np.ascontiguousarray(v, dtype=np.complex128).view(np.float64)
+        else:
+            v = np.ascontiguousarray(v, dtype=np.float64)
+        if v.size != self.vlen:
+            raise AEDError(ERR_INVALID, f"vector of {v.size} values, the sector needs {self.vlen}")
+        return v
 
     def set_couplings(self, bonds, site_h=None, site_d=None):
         """Re-target this handle to a new bond list on the same sector."""
@@ -323,10 +388,28 @@ class Hamiltonian:
 
     @classmethod
     def from_parameters(cls, params, precision=FP64, device=0):
+        """The sector a parameter set names: its Sz_total, and its TOTAL_MOMENTUM when translation
+        symmetry is on (a set that loops over momenta needs TOTAL_MOMENTUM or TRANSLATION_SYMMETRY=false:
+        alps_b200.sparsediag runs the loops)."""
         m = model_from_parameters(params)
-        ham = cls(m["n_sites"], m["n_up"], m["bonds"], precision, device, m["site_h"], m["site_d"])
+        ks = lattice_momenta(params)
+        trans = None
+        if ks:
+            if len(ks) > 1:
+                raise AEDError(ERR_INVALID, "the parameters loop over momenta: give TOTAL_MOMENTUM (one sector per "
+                                            "handle; alps_b200.sparsediag loops over them) or TRANSLATION_SYMMETRY=false")
+            trans = lattice_translations(params, ks[0])
+        ham = cls(m["n_sites"], m["n_up"], m["bonds"], precision, device, m["site_h"], m["site_d"], translations=trans)
         ham.params = m
+        ham.total_momentum = ks[0] if ks else None
         return ham
+
+    def momentum_basis(self):
+        """(representative states, normalisations) of a momentum sector (aed_momentum_basis)."""
+        st = np.empty(self.dim, np.uint32)
+        nm = np.empty(self.dim)
+        _check(lib().aed_momentum_basis(self._h, st.ctypes.data_as(_U32P), _dp(nm), 0, self.dim))
+        return st, nm
 
     def close(self):
         if self._h:
@@ -419,7 +502,7 @@ class Hamiltonian:
               resume=False):
         """Lanczos eigenvalues (aed_solve).  resume=True continues the live FP64 recurrence (the last
         solve's, or one restored by lanczos_load) until nev values converge."""
-        st = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
+        st = None if start is None else self._host_vector(start)
         opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0, 1 if resume else 0)
         res = SolveResult()
         _check(lib().aed_solve(self._h, ctypes.byref(opts), ctypes.byref(res)))
@@ -432,7 +515,7 @@ class Hamiltonian:
     def eigenvectors(self, k=1, seed=0, start=None):
         """Ritz vectors of the k lowest eigenvalues of the last solve (aed_eigenvectors): the solve's
         seed / start must be given again.  Returns (vectors, evals, residuals)."""
-        st = None if start is None else np.ascontiguousarray(start, dtype=np.float64)
+        st = None if start is None else self._host_vector(start)
         opts = SolveOpts(k, 0, 0.0, 0.0, seed, _dp(st), 0, 0, 0)
         vecs = [self.new_vector() for _ in range(k)]
         arr = (_P * k)(*[v.ptr for v in vecs])

@@ -128,5 +128,13 @@ struct ParsedParams {
   std::vector<double> jz, jxy, kq, site_h, site_d;
 };
 int parse_parameters(const char* text, ParsedParams& out);
+// Momenta the sector loop visits (diag.h:93-114): TOTAL_MOMENTUM when given,
+// else every translation momentum when TRANSLATION_SYMMETRY (default true),
+// else none.  *n_dirs = periodic directions of the lattice.
+int lattice_momenta(const char* text, int* n_dirs, std::vector<std::vector<double>>& ks);
+// Translations of the lattice at momentum k: maps (n_trans x n_sites, site i
+// goes to maps[t * n_sites + i]) and phases exp(i k.R_t).
+int lattice_translations(const char* text, const double* k, int n_k, int* n_sites, std::vector<int>& maps,
+                         std::vector<double>& re, std::vector<double>& im);
 
 }  // namespace aed

@@ -1,6 +1,7 @@
 // api.cpp -- the C ABI of libaed.so (declared in include/aed.h).
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -141,8 +142,10 @@ void release(aed_handle* h) {
   handle_release_workspace(h);
   for (void* p : {(void*)h->d_thi, (void*)h->d_tlo, (void*)h->d_lolist, (void*)h->d_looff, (void*)h->d_tile_h,
                   (void*)h->d_tile_r, (void*)h->d_blk_h, (void*)h->d_tfirst, (void*)h->d_dg, (void*)h->d_ell,
-                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64})
+                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64,
+                  (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map})
     mem_dev_free(p, h->stream);
+  delete h->mp;
   mem_host_free(h->h_scal);
   if (h->stream) {
     cudaStreamSynchronize(h->stream);  // the frees are done: the memory is back in the pool
@@ -339,14 +342,51 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
 }  // namespace
 
 int handle_tune(aed_handle* h, bool f32, const void* x, void* y) {
+  if (h->mom) return AED_OK;  // one momentum kernel
   int& v = h->hv_var[f32 ? 1 : 0];
   return v < 0 ? pick_variant(h, f32, x, y, &v) : AED_OK;
 }
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+  if (h->mom)
+    return launch_mom_hv(*h->mp, h->dt, h->mom_tables(), (const double*)x, (double*)y, alpha_part, h->stream);
   const int rc = handle_tune(h, f32, x, y);
   if (rc) return rc;
   return launch_checked(h, f32, h->hv_var[f32 ? 1 : 0], x, y, alpha_part);
+}
+
+// Mean CUDA-event time of `reps` applies through handle_hv.
+int time_hv(aed_handle* h, const void* x, void* y, int reps, double* alpha_part, double* ms) {
+  int rc = AED_OK;
+  cudaEvent_t e0, e1;
+  AED_CUDA_TRY(cudaEventCreate(&e0));
+  AED_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEventRecord(e0, h->stream);
+  for (int r = 0; r < reps && !rc; ++r) rc = handle_hv(h, h->precision == AED_FP32, x, y, alpha_part);
+  cudaEventRecord(e1, h->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  *ms = (double)t / reps;
+  return AED_OK;
+}
+
+// Off-diagonal terms of the momentum apply: every bond whose spin-flip
+// element 0.5 Jxy - 0.25 K is nonzero, in bond order (the flip entry of the
+// spin-1/2 bond matrix, as in build_hv_params).
+void mom_flips(const Model& m, MomParams& mp) {
+  mp.n_flip = 0;
+  for (size_t b = 0; b < m.s1.size(); ++b) {
+    const double k = m.kq.empty() ? 0.0 : m.kq[b];
+    const double c = 0.5 * m.jxy[b] - 0.25 * k;
+    if (c == 0.0) continue;
+    mp.flip_mask[mp.n_flip] = (1u << (m.N - 1 - m.s1[b])) | (1u << (m.N - 1 - m.s2[b]));
+    mp.flip_c[mp.n_flip] = c;
+    ++mp.n_flip;
+  }
 }
 
 }  // namespace aed
@@ -475,7 +515,156 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     release(h);
     return rc ? rc : fail(AED_ERR_CUDA, std::string("diagonal table: ") + cudaGetErrorString(e2));
   }
+  h->dim = h->vlen = h->tab.D;
   *out = h;
+  return AED_OK;
+}
+
+int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out) {
+  if (!out || !model || !tr) return fail(AED_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AED_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(AED_ERR_INVALID, "device index out of range");
+  const int N = model->n_sites;
+  if (tr->n_trans < 1 || tr->n_trans > kMaxTrans) return fail(AED_ERR_INVALID, "n_trans must be in 1..62");
+  if (!tr->site_map || !tr->phase) return fail(AED_ERR_INVALID, "translations: NULL site_map or phase");
+  if (N < 1 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 1..32");
+  for (int t = 0; t < tr->n_trans; ++t) {
+    uint32_t seen = 0;
+    for (int i = 0; i < N; ++i) {
+      const int j = tr->site_map[(size_t)t * N + i];
+      if (j < 0 || j >= N || (seen >> j & 1u)) return fail(AED_ERR_INVALID, "translation is not a permutation of the sites");
+      if (t == 0 && j != i) return fail(AED_ERR_INVALID, "the first translation must be the identity");
+      seen |= 1u << j;
+    }
+  }
+  DeviceGuard g(device);
+  aed_handle* h = new aed_handle;
+  h->device = device;
+  h->precision = AED_FP64;
+  h->mom = true;
+  int rc = model_from_desc(model, h->model);
+  if (!rc) rc = build_tables(h->model.N, h->model.n_up, h->tab);
+  if (!rc) rc = build_hv_params(h->model, h->tab.Nlo, h->P);
+  if (rc) {
+    release(h);
+    return rc;
+  }
+  MomParams* mp = new MomParams();
+  h->mp = mp;
+  mp->N = N;
+  mp->n_trans = tr->n_trans;
+  mp->inv_sqrt_n = 1.0 / std::sqrt((double)N);
+  for (int t = 0; t < tr->n_trans; ++t) {
+    mp->phase_re[t] = tr->phase[2 * t];
+    mp->phase_im[t] = tr->phase[2 * t + 1];
+    for (int i = 0; i < N; ++i) mp->dst[t][i] = (uint8_t)(N - 1 - tr->site_map[(size_t)t * N + i]);
+  }
+  mom_flips(h->model, *mp);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    release(h);
+    return fail(AED_ERR_CUDA, "stream creation failed");
+  }
+  const size_t nlo = h->tab.tlo.size(), nhi = h->tab.thi.size();
+  void* hs = nullptr;
+  if ((rc = mem_dev_alloc_n(&h->d_thi, nhi)) || (rc = mem_dev_alloc_n(&h->d_tlo, nlo)) ||
+      (rc = mem_dev_alloc_n(&h->d_lolist, nlo)) || (rc = mem_dev_alloc_n(&h->d_looff, h->tab.looff.size())) ||
+      (rc = mem_dev_alloc_n(&h->d_scal, 8)) || (rc = mem_host_alloc(&hs, 8 * sizeof(double)))) {
+    release(h);
+    return rc;
+  }
+  h->h_scal = static_cast<double*>(hs);
+  cudaMemcpyAsync(h->d_thi, h->tab.thi.data(), nhi * 4, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_tlo, h->tab.tlo.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_lolist, h->tab.lolist.data(), nlo * 2, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(h->d_looff, h->tab.looff.data(), h->tab.looff.size() * 4, cudaMemcpyHostToDevice, h->stream);
+  const cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    release(h);
+    return fail(AED_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
+  }
+  DevTables& t = h->dt;
+  std::memset(&t, 0, sizeof t);
+  t.thi = h->d_thi;
+  t.tlo = h->d_tlo;
+  t.lolist = h->d_lolist;
+  t.looff = h->d_looff;
+  t.D = h->tab.D;
+  t.Nlo = h->tab.Nlo;
+  t.Nhi = h->tab.Nhi;
+  t.n_up = h->tab.n_up;
+  int64_t dim = 0;
+  if ((rc = mom_build(*mp, h->P, t, h->stream, &h->d_reps, &h->d_norm, &h->d_mdiag, &h->d_map, &dim))) {
+    release(h);
+    return rc;
+  }
+  h->dim = dim;
+  h->vlen = 2 * dim;
+  if ((rc = mem_dev_alloc_n(&h->d_partA, (size_t)mom_tiles(dim) + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_partB, (size_t)red_chunks(h->vlen) + 1))) {
+    release(h);
+    return rc;
+  }
+  *out = h;
+  return AED_OK;
+}
+
+int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count) {
+  if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
+  if (!h->mom) return fail(AED_ERR_INVALID, "aed_momentum_basis: not a momentum sector");
+  if (offset < 0 || count < 0 || offset + count > h->dim) return fail(AED_ERR_INVALID, "range outside the basis");
+  if (count == 0) return AED_OK;
+  DeviceGuard g(h->device);
+  if (states)
+    AED_CUDA_TRY(cudaMemcpyAsync(states, h->d_reps + offset, (size_t)count * 4, cudaMemcpyDeviceToHost, h->stream));
+  if (norms)
+    AED_CUDA_TRY(cudaMemcpyAsync(norms, h->d_norm + offset, (size_t)count * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
+int aed_lattice_momenta(const char* params, int32_t* n_momenta, int32_t* n_dirs, double* k, int32_t capacity) {
+  if (!params || !n_momenta || !n_dirs) return fail(AED_ERR_INVALID, "NULL argument");
+  std::vector<std::vector<double>> ks;
+  int nd = 0;
+  const int rc = lattice_momenta(params, &nd, ks);
+  if (rc) return rc;
+  *n_momenta = (int32_t)ks.size();
+  *n_dirs = nd;
+  if (k) {
+    if (capacity < (int32_t)ks.size()) return fail(AED_ERR_INVALID, "capacity too small");
+    for (size_t m = 0; m < ks.size(); ++m)
+      for (int d = 0; d < nd; ++d) k[m * nd + d] = ks[m][d];
+  }
+  return AED_OK;
+}
+
+int aed_lattice_translations(const char* params, const double* k, int32_t n_dirs, int32_t* n_trans, int32_t* n_sites,
+                             int32_t* site_map, double* phase, int32_t capacity) {
+  if (!params || !n_trans || !n_sites || (n_dirs > 0 && !k)) return fail(AED_ERR_INVALID, "NULL argument");
+  std::vector<int> maps;
+  std::vector<double> re, im;
+  int ns = 0;
+  const int rc = lattice_translations(params, k, n_dirs, &ns, maps, re, im);
+  if (rc) return rc;
+  *n_trans = (int32_t)re.size();
+  *n_sites = ns;
+  if (site_map || phase) {
+    if (capacity < (int32_t)re.size()) return fail(AED_ERR_INVALID, "capacity too small");
+    for (size_t t = 0; t < re.size(); ++t) {
+      if (phase) {
+        phase[2 * t] = re[t];
+        phase[2 * t + 1] = im[t];
+      }
+      if (site_map)
+        for (int i = 0; i < ns; ++i) site_map[t * ns + i] = maps[t * ns + i];
+    }
+  }
   return AED_OK;
 }
 
@@ -497,6 +686,12 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   h->last_beta.clear();
   h->rec_m = 0;
   h->rec_live = false;
+  if (h->mom) {  // same basis and translations: new flip list and diagonal
+    mom_flips(h->model, *h->mp);
+    if ((rc = launch_mom_diag(h->P, h->d_reps, h->dim, h->d_mdiag, h->stream))) return rc;
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return AED_OK;
+  }
   if ((rc = upload_lo_table(h))) return rc;
   rc = launch_diag_table(h->P, h->dt, h->d_dg, h->stream);
   if (rc) return rc;
@@ -524,15 +719,16 @@ int aed_empty_cache(int device) {
 
 int aed_dimension(const aed_handle* h, int64_t* dim) {
   if (!h || !dim) return fail(AED_ERR_INVALID, "NULL argument");
-  *dim = h->tab.D;
+  *dim = h->dim;
   return AED_OK;
 }
 
 int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t count) {
   if (!h || (!host_out && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
-  if (offset < 0 || count < 0 || offset + count > h->tab.D) return fail(AED_ERR_INVALID, "range outside the basis");
+  if (offset < 0 || count < 0 || offset + count > h->dim) return fail(AED_ERR_INVALID, "range outside the basis");
   if (count == 0) return AED_OK;
   DeviceGuard g(h->device);
+  if (h->mom) return aed_momentum_basis(h, host_out, nullptr, offset, count);
   uint32_t* d = nullptr;
   int rc = dev_alloc(&d, (size_t)count);
   if (rc) return rc;
@@ -548,6 +744,7 @@ int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t co
 
 int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t* host_idx) {
   if (!h || ((!host_states || !host_idx) && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
+  if (h->mom) return fail(AED_ERR_INVALID, "aed_index: not available for momentum sectors");
   if (count <= 0) return AED_OK;
   DeviceGuard g(h->device);
   uint32_t* ds = nullptr;
@@ -571,7 +768,7 @@ int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t
 int aed_vec_alloc(aed_handle* h, void** v) {
   if (!h || !v) return fail(AED_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
-  const size_t bytes = (size_t)h->tab.D * h->elem_size();
+  const size_t bytes = (size_t)h->vlen * h->elem_size();
   const cudaError_t e = cudaMalloc(v, bytes ? bytes : 8);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -596,7 +793,7 @@ int aed_vec_upload(aed_handle* h, void* v, const double* host) {
   if (rc) return rc;
   if (!host) return fail(AED_ERR_INVALID, "host is NULL");
   DeviceGuard g(h->device);
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   if (h->precision == AED_FP64) {
     AED_CUDA_TRY(cudaMemcpyAsync(v, host, D * 8, cudaMemcpyHostToDevice, h->stream));
   } else {
@@ -614,7 +811,7 @@ int aed_vec_download(aed_handle* h, const void* v, double* host) {
   if (rc) return rc;
   if (!host) return fail(AED_ERR_INVALID, "host is NULL");
   DeviceGuard g(h->device);
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   if (h->precision == AED_FP64) {
     AED_CUDA_TRY(cudaMemcpyAsync(host, v, D * 8, cudaMemcpyDeviceToHost, h->stream));
     AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -632,7 +829,7 @@ int aed_vec_copy(aed_handle* h, const void* x, void* y) {
   if (!rc) rc = check_vec(h, y, "y");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  AED_CUDA_TRY(cudaMemcpyAsync(y, x, h->tab.D * h->elem_size(), cudaMemcpyDeviceToDevice, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(y, x, h->vlen * h->elem_size(), cudaMemcpyDeviceToDevice, h->stream));
   return AED_OK;
 }
 
@@ -640,7 +837,7 @@ int aed_vec_clear(aed_handle* h, void* x) {
   int rc = check_vec(h, x, "x");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  AED_CUDA_TRY(cudaMemsetAsync(x, 0, h->tab.D * h->elem_size(), h->stream));
+  AED_CUDA_TRY(cudaMemsetAsync(x, 0, h->vlen * h->elem_size(), h->stream));
   return AED_OK;
 }
 
@@ -648,8 +845,8 @@ int aed_vec_fill_random(aed_handle* h, void* x, uint64_t seed) {
   int rc = check_vec(h, x, "x");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  if (h->precision == AED_FP64) return launch_fill_random((double*)x, h->tab.D, seed, h->stream);
-  return launch_fill_random((float*)x, h->tab.D, seed, h->stream);
+  if (h->precision == AED_FP64) return launch_fill_random((double*)x, h->vlen, seed, h->stream);
+  return launch_fill_random((float*)x, h->vlen, seed, h->stream);
 }
 
 int aed_mult(aed_handle* h, const void* x, void* y) {
@@ -664,10 +861,10 @@ int aed_mult(aed_handle* h, const void* x, void* y) {
 static int reduce_to_host(aed_handle* h, const void* x, const void* y, bool sq, bool take_sqrt, double* out) {
   int rc;
   if (h->precision == AED_FP64)
-    rc = launch_dot_partials((const double*)x, (const double*)y, h->tab.D, h->d_partB, sq, h->stream);
+    rc = launch_dot_partials((const double*)x, (const double*)y, h->vlen, h->d_partB, sq, h->stream);
   else
-    rc = launch_dot_partials((const float*)x, (const float*)y, h->tab.D, h->d_partB, sq, h->stream);
-  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(h->tab.D), h->d_scal, take_sqrt, h->stream);
+    rc = launch_dot_partials((const float*)x, (const float*)y, h->vlen, h->d_partB, sq, h->stream);
+  if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(h->vlen), h->d_scal, take_sqrt, h->stream);
   if (rc) return rc;
   AED_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->d_scal, 8, cudaMemcpyDeviceToHost, h->stream));
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -697,24 +894,24 @@ int aed_axpy(aed_handle* h, double a, const void* x, void* y) {
   if (!rc) rc = check_vec(h, y, "y");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  if (h->precision == AED_FP64) return launch_axpy(a, (const double*)x, (double*)y, h->tab.D, h->stream);
-  return launch_axpy(a, (const float*)x, (float*)y, h->tab.D, h->stream);
+  if (h->precision == AED_FP64) return launch_axpy(a, (const double*)x, (double*)y, h->vlen, h->stream);
+  return launch_axpy(a, (const float*)x, (float*)y, h->vlen, h->stream);
 }
 
 int aed_scal(aed_handle* h, double a, void* x) {
   int rc = check_vec(h, x, "x");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->tab.D, false, h->stream);
-  return launch_scal(a, (float*)x, h->tab.D, false, h->stream);
+  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->vlen, false, h->stream);
+  return launch_scal(a, (float*)x, h->vlen, false, h->stream);
 }
 
 int aed_div(aed_handle* h, double a, void* x) {
   int rc = check_vec(h, x, "x");
   if (rc) return rc;
   DeviceGuard g(h->device);
-  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->tab.D, true, h->stream);
-  return launch_scal(a, (float*)x, h->tab.D, true, h->stream);
+  if (h->precision == AED_FP64) return launch_scal(a, (double*)x, h->vlen, true, h->stream);
+  return launch_scal(a, (float*)x, h->vlen, true, h->stream);
 }
 
 int aed_lanczos_step(aed_handle* h, const void* v_prev, const void* v_cur, void* v_next, double beta_prev,
@@ -786,6 +983,10 @@ int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t 
   if (reps < 1 || !ms) return fail(AED_ERR_INVALID, "reps must be >= 1 and ms non-NULL");
   if (variant >= hv_num_variants()) return fail(AED_ERR_INVALID, "unknown variant");
   DeviceGuard g(h->device);
+  if (h->mom) {  // one kernel: aed_time_mult with the partials when asked
+    if (variant_used) *variant_used = -1;
+    return time_hv(h, x, y, reps, with_alpha ? h->d_partA : nullptr, ms);
+  }
   const bool f32 = h->precision == AED_FP32;
   int v = variant;
   if (v < 0) {
@@ -824,20 +1025,7 @@ int aed_time_mult(aed_handle* h, const void* x, void* y, int32_t reps, double* m
   if (rc) return rc;
   if (reps < 1 || !ms) return fail(AED_ERR_INVALID, "reps must be >= 1 and ms non-NULL");
   DeviceGuard g(h->device);
-  cudaEvent_t e0, e1;
-  AED_CUDA_TRY(cudaEventCreate(&e0));
-  AED_CUDA_TRY(cudaEventCreate(&e1));
-  cudaEventRecord(e0, h->stream);
-  for (int r = 0; r < reps && !rc; ++r) rc = handle_hv(h, h->precision == AED_FP32, x, y, nullptr);
-  cudaEventRecord(e1, h->stream);
-  cudaEventSynchronize(e1);
-  float t = 0.f;
-  cudaEventElapsedTime(&t, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (rc) return rc;
-  *ms = (double)t / reps;
-  return AED_OK;
+  return time_hv(h, x, y, reps, nullptr, ms);
 }
 
 int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap, double* evals, double* errors,

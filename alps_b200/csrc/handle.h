@@ -7,6 +7,7 @@
 
 #include "aed_internal.h"
 #include "kernels.cuh"
+#include "momentum.cuh"
 
 struct aed_handle {
   int device = 0;
@@ -35,6 +36,20 @@ struct aed_handle {
   double* h_scal = nullptr;   // 8 pinned host scalars
   int hv_var[2] = {-1, -1};  // apply variant per precision (FP64, FP32), -1 = not tuned yet
   size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }
+  // rows of H (D, or the representatives of a momentum sector) and the
+  // length of a vector in scalars (D, or 2 x rows: interleaved complex)
+  int64_t dim = 0;
+  int64_t vlen = 0;
+  // momentum sector (aed_create_momentum): the tables of momentum.cuh
+  bool mom = false;
+  aed::MomParams* mp = nullptr;  // host copy (large: kept off the handle's inline storage)
+  uint32_t* d_reps = nullptr;
+  double* d_norm = nullptr;
+  double* d_mdiag = nullptr;
+  uint32_t* d_map = nullptr;
+  aed::MomTables mom_tables() const { return {d_reps, d_norm, d_mdiag, d_map, dim}; }
+  // <x, y> partials of one apply (tiles of the real apply, or of the momentum apply)
+  int64_t alpha_tiles() const { return mom ? aed::mom_tiles(dim) : dt.n_tiles; }
   // solve workspaces, kept between solves (grown on demand, so that a solve
   // makes no allocation once the handle is warm): slot 0 = the three FP64
   // recurrence vectors, slot 1 = device alpha/beta pairs and Ritz coefficients

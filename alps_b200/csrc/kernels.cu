@@ -254,6 +254,8 @@ inline int check_launch(const char* what) {
 
 int64_t launch_count() { return g_launches.load(); }
 
+int check_launch_counted(const char* what) { return check_launch(what); }
+
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
                         bool accumulate, cudaStream_t st) {
   if (m < 1 || m > kMaxRitzTerms) return fail(AED_ERR_INVALID, "ritz_combine: bad number of terms");

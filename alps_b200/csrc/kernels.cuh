@@ -93,5 +93,8 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
                         bool accumulate, cudaStream_t st);
 
 int64_t launch_count();
+// After a launch in another translation unit: counts it and returns
+// AED_ERR_CUDA (with the launch error) if it failed.
+int check_launch_counted(const char* what);
 
 }  // namespace aed

@@ -90,8 +90,8 @@ double diag_of_state(const HvParams& P, uint32_t s) {
 // beta, normalise (lanczos.h:398-402).
 int lanczos_step_tail(aed_handle* h, bool f32, const void* vprev, const void* x, void* y, const double* beta_prev,
                       double* alpha, double* beta) {
-  const int64_t D = h->tab.D;
-  int rc = launch_finish_sum(h->d_partA, h->dt.n_tiles, alpha, false, h->stream);
+  const int64_t D = h->vlen;
+  int rc = launch_finish_sum(h->d_partA, h->alpha_tiles(), alpha, false, h->stream);
   if (rc) return rc;
   if (f32)
     rc = launch_lanczos_update(alpha, (const float*)x, (const float*)vprev, beta_prev, (float*)y, D, h->d_partB,
@@ -265,7 +265,7 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
 
 // The three rotating FP64 vectors of the recurrence in workspace slot 0.
 int recurrence_buffers(aed_handle* h, void* buf[3]) {
-  const size_t vb = ((size_t)h->tab.D * 8 + 255) & ~(size_t)255;
+  const size_t vb = ((size_t)h->vlen * 8 + 255) & ~(size_t)255;
   void* ws = nullptr;
   const int rc = handle_workspace(h, 0, 3 * vb, &ws);
   if (rc) return rc;
@@ -275,7 +275,7 @@ int recurrence_buffers(aed_handle* h, void* buf[3]) {
 
 // v_0 of a recurrence: copied from the device or the host, else seeded; normalised.
 int start_vector(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, double* v0) {
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   int rc;
   if (start_dev) {
     AED_CUDA_TRY(cudaMemcpyAsync(v0, start_dev, D * 8, cudaMemcpyDeviceToDevice, h->stream));
@@ -294,7 +294,7 @@ int start_vector(aed_handle* h, const double* start_host, const double* start_de
 int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, int nev,
                int max_iter, double rtol, double atol, bool energy_bound, double etol, int min_steps, bool profile,
                aed_solve_result* r, TmatInfo& T, bool resume = false) {
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   EventRing ring;
   int rc;
   const int m0 = resume ? h->rec_m : 0;
@@ -356,7 +356,7 @@ constexpr double kRefineEnergyTol = 1e-11;
 // FP32 phase with the Lanczos basis stored in HBM, then FP64 refinement.
 int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev, int max_iter, double rtol,
                 double atol, bool profile, aed_solve_result* r) {
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   // Lanczos basis store: chunks of kStoreChunk FP32 vectors, grown as the
   // recurrence advances and kept by the handle for later solves
   const size_t vbytes = (((size_t)D * 4 + 255) & ~(size_t)255);
@@ -451,12 +451,26 @@ int lanczos_step_kernels(aed_handle* h, bool f32, const void* v_prev, const void
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
   std::memset(r, 0, sizeof *r);
   const auto t0 = std::chrono::steady_clock::now();
-  const int64_t D = h->tab.D;
+  const int64_t D = h->dim;
   const int nev = o->nev;
   if (nev < 1 || nev > AED_MAX_NEV) return fail(AED_ERR_INVALID, "nev must be in 1..16");
   if (o->max_iter < 0) return fail(AED_ERR_INVALID, "max_iter must be >= 0");
   int rc = AED_OK;
   if (D == 0) {
+    r->converged = 1;
+  } else if (D == 1 && h->mom) {  // M(0,0) = Re (M e_0)_0: the diagonal terms and the flips back into the orbit
+    void* w = nullptr;
+    if ((rc = handle_workspace(h, 0, 64, &w))) return rc;
+    double* x = (double*)w;
+    double* y = x + 2;
+    const double one[2] = {1.0, 0.0};
+    double out[2] = {0.0, 0.0};
+    AED_CUDA_TRY(cudaMemcpyAsync(x, one, 16, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = handle_hv(h, false, x, y, nullptr))) return rc;
+    AED_CUDA_TRY(cudaMemcpyAsync(out, y, 16, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    r->n_evals = 1;
+    r->evals[0] = out[0];
     r->converged = 1;
   } else if (D == 1) {
     uint32_t s = 0;
@@ -493,7 +507,7 @@ namespace {
 
 // |v| on the host (deterministic reduction, FP64 vector).
 int host_norm(aed_handle* h, const double* v, double* out) {
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   int rc = launch_dot_partials(v, v, D, h->d_partB, true, h->stream);
   if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(D), h->d_scal + 6, true, h->stream);
   if (rc) return rc;
@@ -505,7 +519,7 @@ int host_norm(aed_handle* h, const double* v, double* out) {
 
 // FNV-1a of the model (sector and couplings): a saved recurrence only loads
 // into a handle of the same Hamiltonian.
-uint64_t model_hash(const Model& m) {
+uint64_t model_hash(const Model& m, const MomParams* mp) {
   uint64_t x = 1469598103934665603ull;
   auto mix = [&](const void* p, size_t n) {
     const unsigned char* b = (const unsigned char*)p;
@@ -522,6 +536,14 @@ uint64_t model_hash(const Model& m) {
   }
   for (double v : m.site_h) mix(&v, 8);
   for (double v : m.site_d) mix(&v, 8);
+  if (mp) {  // a momentum sector: its translations and phases
+    mix(&mp->n_trans, sizeof mp->n_trans);
+    for (int t = 0; t < mp->n_trans; ++t) {
+      mix(&mp->phase_re[t], 8);
+      mix(&mp->phase_im[t], 8);
+      mix(mp->dst[t], 32);
+    }
+  }
   return x;
 }
 
@@ -550,7 +572,7 @@ int eigenvectors(aed_handle* h, const aed_solve_opts* o, int k, void* const* vec
   if (m < 1) return fail(AED_ERR_INVALID, "eigenvectors: no solve to take eigenvectors from");
   for (int i = 0; i < k; ++i)
     if (!vecs[i]) return fail(AED_ERR_INVALID, "eigenvectors: NULL output vector");
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   const bool f32 = h->precision == AED_FP32;
   const std::vector<double>& al = h->last_alpha;
   const std::vector<double>& be = h->last_beta;
@@ -621,7 +643,7 @@ int eigenvectors(aed_handle* h, const aed_solve_opts* o, int k, void* const* vec
 
 int64_t lanczos_state_bytes(const aed_handle* h) {
   if (!h->rec_live) return 0;
-  return (int64_t)sizeof(StateHeader) + (int64_t)16 * h->rec_m + (int64_t)16 * h->tab.D;
+  return (int64_t)sizeof(StateHeader) + (int64_t)16 * h->rec_m + (int64_t)16 * h->vlen;
 }
 
 // Tmatrix::save + lanczos::save (src/ietl/tmatrix.h:66-77, lanczos.h:86-98):
@@ -631,14 +653,14 @@ int lanczos_save(aed_handle* h, void* buf, int64_t bytes) {
   if (!h->rec_live) return fail(AED_ERR_INVALID, "lanczos_save: no live Lanczos recurrence (solve first)");
   if (bytes < lanczos_state_bytes(h)) return fail(AED_ERR_INVALID, "lanczos_save: buffer too small");
   const int m = h->rec_m;
-  const int64_t D = h->tab.D;
+  const int64_t D = h->vlen;
   StateHeader hd{};
   std::memcpy(hd.magic, kStateMagic, 8);
   hd.D = D;
   hd.N = h->model.N;
   hd.n_up = h->model.n_up;
   hd.m = m;
-  hd.model = model_hash(h->model);
+  hd.model = model_hash(h->model, h->mp);
   char* p = (char*)buf;
   std::memcpy(p, &hd, sizeof hd);
   p += sizeof hd;
@@ -660,7 +682,7 @@ int lanczos_load(aed_handle* h, const void* buf, int64_t bytes) {
   StateHeader hd;
   std::memcpy(&hd, buf, sizeof hd);
   if (std::memcmp(hd.magic, kStateMagic, 8) != 0) return fail(AED_ERR_INVALID, "lanczos_load: not a saved recurrence");
-  if (hd.D != h->tab.D || hd.N != h->model.N || hd.n_up != h->model.n_up || hd.model != model_hash(h->model))
+  if (hd.D != h->vlen || hd.N != h->model.N || hd.n_up != h->model.n_up || hd.model != model_hash(h->model, h->mp))
     return fail(AED_ERR_INVALID, "lanczos_load: the state belongs to a different Hamiltonian");
   const int m = hd.m;
   const int64_t D = hd.D;

@@ -5,8 +5,10 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <map>
+#include <sstream>
 #include <stdexcept>
 
 #include "aed_internal.h"
@@ -515,7 +517,129 @@ bool lattice_spec(const std::string& name, LatticeSpec& L) {
   return true;
 }
 
+bool flag_true(const std::string& v) { return !(v == "false" || v == "0" || v == "False" || v == "FALSE"); }
+
+// Lattice of the parameters: its spec and extents (L, W with the lattice's
+// W default).
+struct Geometry {
+  LatticeSpec L;
+  int ext[2] = {1, 1};
+  int N = 0;
+};
+
+int read_geometry(const Params& p, Eval& ev, Geometry& g) {
+  auto it = p.kv.find("LATTICE");
+  const std::string latname = it == p.kv.end() ? "" : it->second;
+  if (!lattice_spec(latname, g.L)) return fail(AED_ERR_INVALID, "unsupported LATTICE \"" + latname + "\"");
+  g.ext[0] = (int)std::lround(ev.name("L"));
+  g.ext[1] = 1;
+  if (g.L.dim == 2) g.ext[1] = p.has("W") ? (int)std::lround(ev.name("W")) : (int)std::lround(ev.expr_str(g.L.ext_w_default));
+  if (g.ext[0] < 1 || g.ext[1] < 1) return fail(AED_ERR_INVALID, "lattice extents must be positive");
+  g.N = g.ext[0] * g.ext[1];
+  return AED_OK;
+}
+
 }  // namespace
+
+int lattice_momenta(const char* text, int* n_dirs, std::vector<std::vector<double>>& ks) {
+  Params p;
+  int rc = parse_kv(text, p);
+  if (rc) return rc;
+  Eval ev{p.kv, spin_defaults()};
+  ks.clear();
+  try {
+    Geometry g;
+    if ((rc = read_geometry(p, ev, g))) return rc;
+    std::vector<int> dirs;
+    for (int d = 0; d < g.L.dim; ++d)
+      if (g.L.periodic[d]) dirs.push_back(d);
+    *n_dirs = (int)dirs.size();
+    auto tm = p.kv.find("TOTAL_MOMENTUM");
+    if (tm != p.kv.end() && !tm->second.empty()) {
+      // read_vector_resize (vectorio.hpp:52-60): whitespace-separated components
+      std::istringstream in(tm->second);
+      std::vector<double> k;
+      std::string tok;
+      while (in >> tok) k.push_back(ev.expr_str(tok));
+      if (k.size() != dirs.size())
+        return fail(AED_ERR_INVALID, "TOTAL_MOMENTUM needs one component per periodic direction (hypercubic.h:428-430)");
+      ks.push_back(k);
+    } else if (flag_true(p.has("TRANSLATION_SYMMETRY") ? p.kv.at("TRANSLATION_SYMMETRY") : "true")) {
+      // translation_momenta (hypercubic.h:403-423): the first periodic direction slowest
+      for (int d : dirs) {
+        std::vector<std::vector<double>> nk;
+        if (ks.empty()) {
+          for (int j = 0; j < g.ext[d]; ++j) nk.push_back({2. * j * M_PI / g.ext[d]});
+        } else {
+          for (const auto& k : ks)
+            for (int j = 0; j < g.ext[d]; ++j) {
+              std::vector<double> kk = k;
+              kk.push_back(2. * j * M_PI / g.ext[d]);
+              nk.push_back(kk);
+            }
+        }
+        ks.swap(nk);
+      }
+    }
+  } catch (const std::exception& e) {
+    return fail(AED_ERR_INVALID, std::string("parameter error: ") + e.what());
+  }
+  return AED_OK;
+}
+
+int lattice_translations(const char* text, const double* k, int n_k, int* n_sites, std::vector<int>& maps,
+                         std::vector<double>& re, std::vector<double>& im) {
+  Params p;
+  int rc = parse_kv(text, p);
+  if (rc) return rc;
+  Eval ev{p.kv, spin_defaults()};
+  maps.clear();
+  re.clear();
+  im.clear();
+  try {
+    Geometry g;
+    if ((rc = read_geometry(p, ev, g))) return rc;
+    std::vector<int> dirs;
+    for (int d = 0; d < g.L.dim; ++d)
+      if (g.L.periodic[d]) dirs.push_back(d);
+    if (n_k != (int)dirs.size())
+      return fail(AED_ERR_INVALID, "one momentum component per periodic direction (hypercubic.h:428-430)");
+    *n_sites = g.N;
+    // hypercubic_lattice::translations (hypercubic.h:425-464): the first
+    // periodic direction fastest; translation t moves cell c to the cell at
+    // c + shift (one vertex per cell for these lattices)
+    std::vector<int> shift(dirs.size(), 0);
+    while (true) {
+      int off[2] = {0, 0};
+      double phase = 0.;
+      for (size_t i = 0; i < dirs.size(); ++i) {
+        off[dirs[i]] = shift[i];
+        phase += shift[i] * k[i];
+      }
+      const std::complex<double> ph = std::exp(std::complex<double>(0., phase));
+      re.push_back(ph.real());
+      im.push_back(ph.imag());
+      for (int c = 0; c < g.N; ++c) {
+        int cc[2] = {g.L.dim == 1 ? c : c / g.ext[1], g.L.dim == 1 ? 0 : c % g.ext[1]};
+        for (int d = 0; d < g.L.dim; ++d) cc[d] = (cc[d] + off[d]) % g.ext[d];
+        maps.push_back(g.L.dim == 1 ? cc[0] : cc[0] * g.ext[1] + cc[1]);
+      }
+      bool done = true;
+      for (size_t i = 0; i < shift.size(); ++i) {
+        if (++shift[i] >= g.ext[dirs[i]]) {
+          shift[i] = 0;
+        } else {
+          done = false;
+          break;
+        }
+      }
+      if (done) break;
+    }
+  } catch (const std::exception& e) {
+    return fail(AED_ERR_INVALID, std::string("parameter error: ") + e.what());
+  }
+  return AED_OK;
+}
 
 int parse_parameters(const char* text, ParsedParams& out) {
   Params p;
@@ -538,10 +662,6 @@ int parse_parameters(const char* text, ParsedParams& out) {
     const std::string cq = str("CONSERVED_QUANTUMNUMBERS", "");
     if (cq.find("Sz") == std::string::npos)
       return fail(AED_ERR_INVALID, "CONSERVED_QUANTUMNUMBERS must contain Sz (full Hilbert space not supported)");
-    const std::string ts = str("TRANSLATION_SYMMETRY", "true");
-    if (!(ts == "false" || ts == "0" || ts == "False" || ts == "FALSE"))
-      return fail(AED_ERR_INVALID,
-                  "TRANSLATION_SYMMETRY must be false: momentum sectors are not supported (factory.C:17-30)");
     if (!p.has("Sz_total"))
       return fail(AED_ERR_INVALID, "Sz_total must be given (one sector per handle; alps_b200.sparsediag loops over them)");
     const int Lx = (int)std::lround(ev.name("L"));

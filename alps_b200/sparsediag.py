@@ -8,7 +8,11 @@ given, every Sz_total from -N/2 to N/2 (step 1; diag.h:142-175 takes the range
 from the site bases) is a sector, each solved by SparseDiagMatrix::do_subspace
 (here `Hamiltonian.solve`, NUMBER_EIGENVALUES / MAX_ITERATIONS from the
 parameters); a fixed `Sz_total` gives one sector without quantum-number labels,
-as in the reference.  The ground-state energy and the gap are chosen as in
+as in the reference.  With translation symmetry (TRANSLATION_SYMMETRY, default
+true, on a lattice with periodic directions) each Sz sector splits into its
+momentum sectors, the momentum loop innermost, labelled TOTAL_MOMENTUM =
+write_vector(k) (diag.h:93-131); a given TOTAL_MOMENTUM fixes one momentum and
+adds no label.  The ground-state energy and the gap are chosen as in
 SparseDiagMatrix::write_xml_body (sparsediag.h:59-90), and `write_xml` writes
 the EIGENVALUES and AVERAGES elements of DiagTask::write_xml_body
 (src/alps/scheduler/diag.hpp:127-140) and sparsediag.h:80-88.  (The HDF5
@@ -22,7 +26,7 @@ from xml.sax.saxutils import escape
 
 import numpy as np
 
-from . import AEDError, FP64, Hamiltonian, model_from_parameters
+from . import AEDError, FP64, Hamiltonian, lattice_momenta, lattice_translations, model_from_parameters, momentum_label
 
 
 def half_integer_text(v: Fraction) -> str:
@@ -43,7 +47,8 @@ def _site_count(params: dict) -> int:
 
 def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
     """Eigenvalues of every sector: {"sectors": [{"quantumnumbers": [(name, value)], "energies": array,
-    "dimension": D, "iterations": m}], "ground_state_energy": E0, "energy_gap": gap}."""
+    "dimension": D, "iterations": m}], "ground_state_energy": E0, "energy_gap": gap}.  Momentum sectors
+    run in FP64 whatever `precision` says."""
     params = dict(params)
     qns = str(params.get("CONSERVED_QUANTUMNUMBERS", "")).replace(",", " ").split()
     sectors = []
@@ -52,18 +57,28 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
     else:
         n = _site_count(params)
         sz_values = [Fraction(k, 2) for k in range(-n, n + 1, 2)]
+    momenta = lattice_momenta(params)
+    label_k = bool(momenta) and not str(params.get("TOTAL_MOMENTUM", "")).strip()
     for sz in sz_values:
         p = params if sz is None else dict(params, Sz_total=float(sz))
-        ham = Hamiltonian.from_parameters(p, precision=precision, device=device)
-        try:
-            if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
-                continue
-            r = ham.solve(nev=max(1, ham.params["nev"]), max_iter=ham.params["max_iter"], seed=seed)
-            sectors.append({"quantumnumbers": [] if sz is None else [("Sz", half_integer_text(sz))],
-                            "energies": np.array(r["evals"]), "dimension": ham.dim,
-                            "iterations": r["iterations"], "converged": r["converged"]})
-        finally:
-            ham.close()
+        mp = model_from_parameters(p)
+        for k in momenta or [None]:
+            qn = [] if sz is None else [("Sz", half_integer_text(sz))]
+            if k is None:
+                ham = Hamiltonian.from_parameters(p, precision=precision, device=device)
+            else:
+                if label_k:
+                    qn.append(("TOTAL_MOMENTUM", momentum_label(k)))
+                ham = Hamiltonian(mp["n_sites"], mp["n_up"], mp["bonds"], FP64, device, mp["site_h"], mp["site_d"],
+                                  translations=lattice_translations(params, k))
+            try:
+                if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
+                    continue
+                r = ham.solve(nev=max(1, mp["nev"]), max_iter=mp["max_iter"], seed=seed)
+                sectors.append({"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
+                                "iterations": r["iterations"], "converged": r["converged"]})
+            finally:
+                ham.close()
     e0, gap = ground_state_and_gap([s["energies"] for s in sectors])
     return {"sectors": sectors, "ground_state_energy": e0, "energy_gap": gap}
 

@@ -80,7 +80,8 @@ typedef struct {
  * lattice, open square lattice, anisotropic square lattice, ladder, open
  * ladder} with L/W, couplings J, J0, J1, J', Jz, Jxy, Jz<n>, Jxy<n>, J<n>, K<n>,
  * h, D with the model library's defaults, CONSERVED_QUANTUMNUMBERS containing Sz, Sz_total,
- * NUMBER_EIGENVALUES, MAX_ITERATIONS, TRANSLATION_SYMMETRY=false.
+ * NUMBER_EIGENVALUES, MAX_ITERATIONS.  TRANSLATION_SYMMETRY and TOTAL_MOMENTUM
+ * select momentum sectors (aed_lattice_momenta); the bond list is the same.
  * Replaces the parameter path of SparseDiagFactory/DiagMatrix
  * (applications/diag/sparsediag/factory.C:17-30, applications/diag/diag.h:85-175,
  * src/alps/lattice/latticegraph.h:98-136, lib/xml/lattices.xml.in).
@@ -107,6 +108,43 @@ int aed_destroy(aed_handle* h);
  * `device`, all cached pinned host memory).  No reference counterpart: the
  * reference's matrices are freed with their task. */
 int aed_empty_cache(int device);
+
+/* ---- momentum sectors --------------------------------------------------- */
+/* Translations of a lattice at one momentum k: the identity first. */
+typedef struct {
+  int32_t n_trans;          /* number of translations (1..62)                          */
+  const int32_t* site_map;  /* n_trans x n_sites: translation t moves site i to         *
+                             * site_map[t * n_sites + i]                                 */
+  const double* phase;      /* n_trans x 2: exp(i k.R_t) as (re, im)                     */
+} aed_translations;
+
+/* A momentum sector of the Sz sector of `model`: rows are the representatives
+ * of the translation orbits with nonzero weight, vectors are complex, stored
+ * as interleaved (re, im) doubles (2 x aed_dimension doubles per vector; the
+ * aed_vec_* calls, aed_mult, aed_solve and aed_eigenvectors take them).  FP64.
+ * Replaces hamiltonian_matrix::build_basis with TOTAL_MOMENTUM set
+ * (src/alps/model/hamiltonian_matrix.hpp:402-417; bloch_basis_states::build,
+ * src/alps/model/blochbasisstates.h:92-271) and its matrix elements
+ * M(i,j) += val * phase * n_j / n_i (hamiltonian_matrix.hpp:307-345); the
+ * matrix stays implicit.  The sector's dimension may be 0. */
+int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out);
+/* Representatives (states as in aed_basis_copy) and normalisations of rows
+ * [offset, offset + count) of a momentum sector; either array may be NULL
+ * (bloch_basis_states' states and normalization(i)). */
+int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count);
+/* Momenta the sparsediag sector loop visits for a parameter file
+ * (DiagMatrix::dostep, applications/diag/diag.h:93-114): TOTAL_MOMENTUM when
+ * given, else every momentum of lattice.translation_momenta()
+ * (src/alps/lattice/hypercubic.h:403-423, the first periodic direction
+ * slowest) when TRANSLATION_SYMMETRY (default true), else none.  k: room for
+ * `capacity` momenta of n_dirs components, or NULL to query the counts. */
+int aed_lattice_momenta(const char* params, int32_t* n_momenta, int32_t* n_dirs, double* k, int32_t capacity);
+/* The lattice's translations at momentum k (hypercubic_lattice::translations,
+ * hypercubic.h:425-464: the first periodic direction fastest, phase
+ * exp(i sum_d shift_d k_d)).  site_map: room for capacity x n_sites entries,
+ * phase for capacity x 2; both NULL to query the counts. */
+int aed_lattice_translations(const char* params, const double* k, int32_t n_dirs, int32_t* n_trans,
+                             int32_t* n_sites, int32_t* site_map, double* phase, int32_t capacity);
 
 /* Replace the couplings of a handle (same N, n_up; any bond list), keeping its
  * basis tables, workspaces and apply tuning: the parameter sweeps sparsediag

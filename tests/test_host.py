@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import alps_b200 as ed
+from oracle import bloch
 import oracle
 from oracle import lattice
 
@@ -109,7 +110,6 @@ def test_parameter_file_syntax_and_defaults():
 
 
 @pytest.mark.parametrize("bad,msg", [
-    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n', "TRANSLATION"),
     ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nTRANSLATION_SYMMETRY=false\nCONSERVED_QUANTUMNUMBERS="Sz"\n',
      "Sz_total"),
     ('MODEL="boson Hubbard"\nLATTICE="chain lattice"\nL=8\n', "MODEL"),
@@ -188,3 +188,35 @@ def test_sparsediag_gap_rule_and_labels(tmp_path):
     assert ev.get("number") == "2" and ev.find("QUANTUMNUMBER").get("value") == "1/2"
     text = (ev.text or "") + "".join(c.tail or "" for c in ev)
     assert [float(v) for v in text.split()] == [-1.25, -0.75]
+
+
+MOMENTUM_CASES = [
+    ("chain lattice", {"L": 8}), ("nnn chain lattice", {"L": 7}), ("square lattice", {"L": 3, "W": 4}),
+    ("anisotropic square lattice", {"L": 4, "W": 2}), ("ladder", {"L": 5}), ("open chain lattice", {"L": 6}),
+    ("open ladder", {"L": 4}),
+]
+
+
+@pytest.mark.parametrize("lat,geo", MOMENTUM_CASES, ids=[c[0] for c in MOMENTUM_CASES])
+def test_lattice_momenta_and_translations_match_oracle(lat, geo):
+    """The engine's translation momenta and translations (site maps, phases) equal the oracle's restatement of
+    hypercubic_lattice (pinned by the example13-15 fixtures)."""
+    p = dict(geo, MODEL="spin", LATTICE=lat, CONSERVED_QUANTUMNUMBERS="Sz", Sz_total=0)
+    ks = ed.lattice_momenta(p)
+    ref = bloch.translation_momenta(lat, geo)
+    assert ks == ref
+    for k in ks:
+        got = ed.lattice_translations(p, k)
+        exp = bloch.translations(lat, geo, k)
+        assert [m for _, m in got] == [m for _, m in exp]
+        assert all(abs(a - b) <= 1e-15 for (a, _), (b, _) in zip(got, exp))
+    assert ed.lattice_momenta(dict(p, TRANSLATION_SYMMETRY="false")) == []
+    if ks:
+        one = ed.lattice_momenta(dict(p, TOTAL_MOMENTUM=ed.momentum_label(ks[-1])))
+        assert one == [ks[-1]]
+        assert ed.momentum_label(ks[-1]) == bloch.momentum_label(ks[-1])
+
+
+def test_total_momentum_needs_one_component_per_periodic_direction():
+    with pytest.raises(ed.AEDError, match="TOTAL_MOMENTUM"):
+        ed.lattice_momenta('MODEL="spin"\nLATTICE="square lattice"\nL=3\nTOTAL_MOMENTUM="0"\nSz_total=0\n')
