@@ -542,6 +542,33 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
       seen |= 1u << j;
     }
   }
+  {  // the Bloch basis needs H to commute with every translation (the reference
+     // offers no translations on inhomogeneous lattices, graph_helper.h:585-607)
+    Model m;
+    const int rc0 = model_from_desc(model, m);
+    if (rc0) return rc0;
+    std::map<std::pair<int, int>, std::tuple<double, double, double>> bond;
+    for (size_t b = 0; b < m.s1.size(); ++b) {
+      auto key = std::minmax(m.s1[b], m.s2[b]);
+      auto& v = bond[{key.first, key.second}];
+      std::get<0>(v) += m.jz[b];
+      std::get<1>(v) += m.jxy[b];
+      std::get<2>(v) += m.kq[b];
+    }
+    for (int t = 1; t < tr->n_trans; ++t) {
+      const int32_t* mp = tr->site_map + (size_t)t * N;
+      for (const auto& e : bond) {
+        auto key = std::minmax(mp[e.first.first], mp[e.first.second]);
+        auto it = bond.find({key.first, key.second});
+        if (it == bond.end() || it->second != e.second)
+          return fail(AED_ERR_INVALID, "the couplings are not invariant under the translations");
+      }
+      for (int i = 0; i < N; ++i)
+        if ((!m.site_h.empty() && m.site_h[mp[i]] != m.site_h[i]) ||
+            (!m.site_d.empty() && m.site_d[mp[i]] != m.site_d[i]))
+          return fail(AED_ERR_INVALID, "the site terms are not invariant under the translations");
+    }
+  }
   DeviceGuard g(device);
   aed_handle* h = new aed_handle;
   h->device = device;

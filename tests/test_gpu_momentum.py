@@ -153,3 +153,12 @@ def test_sparsediag_loops_over_momenta():
     assert labels == exp
     assert abs(res["ground_state_energy"] - ref["ground_state_energy"]) < 1e-10
     assert abs(res["energy_gap"] - ref["energy_gap"]) < 1e-9
+
+
+def test_momentum_rejects_couplings_that_break_translations():
+    lat, geo = "chain lattice", {"L": 8}
+    n, bonds = _bonds(lat, geo, {0: (1.0, 1.0)})
+    bonds[3] = (bonds[3][0], bonds[3][1], 1.5, 1.5, 0.0)
+    tr = ed.lattice_translations(_params(lat, geo), (0.0,))
+    with pytest.raises(ed.AEDError, match="invariant"):
+        ed.Hamiltonian(n, n // 2, bonds, translations=tr)
