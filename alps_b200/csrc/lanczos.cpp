@@ -19,6 +19,8 @@
 // r^2 / gap on each eigenvalue is below 1e-11 |lambda|.
 
 #include <algorithm>
+#include <future>
+#include <deque>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -105,6 +107,17 @@ int lanczos_step_tail(aed_handle* h, bool f32, const void* vprev, const void* x,
   return launch_lanczos_normalize(beta, (double*)y, D, h->stream);
 }
 
+// Steps the device runs ahead of the host's T-matrix analysis.  A step of a
+// large sector keeps the GPU busy longer than the analysis takes, so one step
+// ahead suffices; for small sectors (fewer than 2^24 vector scalars: the
+// momentum sectors, chains up to L = 26) three hide the analysis and the
+// launch latency.  The steps launched past the stop are discarded.  The
+// recurrence vectors rotate through lookahead + 2 slots, so that v_{m-1} and
+// v_m survive the extra steps (resume, checkpoint).
+constexpr int kMaxRing = 5;
+inline int lanczos_lookahead(const aed_handle* h) { return h->vlen >= ((int64_t)1 << 24) ? 1 : 3; }
+inline int ring_slots(const aed_handle* h) { return lanczos_lookahead(h) + 2; }
+
 // One Lanczos recurrence on device vectors of type T.  Vectors rotate through
 // `slot(j)`, the buffer that receives v_j.  Returns T-matrix and convergence.
 struct Recurrence {
@@ -112,6 +125,7 @@ struct Recurrence {
   bool f32;
   int64_t D;
   int max_iter;
+  int ahead;         // steps launched ahead of the host analysis
   double* d_ab;      // device alpha/beta pairs: d_ab[2j] = alpha_j, d_ab[2j+1] = beta_j
   double* h_ab;      // pinned host copy
   EventRing* ring;
@@ -213,8 +227,23 @@ struct StopRule {
 template <typename SlotFn>
 int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int* iters, int* failed,
                    TmatInfo& T) {
+  // T(m) is analysed for every m in turn, as the reference's iteration does
+  // (lanczos.h:366-372); with R.ahead > 1 the analyses of the next R.ahead
+  // sizes run on host threads side by side (each is independent of the
+  // others' outcome) and their verdicts are read in order.
+  const double thold = R.f32 ? kFp32MergeRel : 0.0;
+  // alpha / beta keep their storage while later steps append (capacity
+  // max_iter + 1); the maxima are taken over the first m pairs at submission
+  R.alpha.reserve((size_t)R.max_iter + 1);
+  R.beta.reserve((size_t)R.max_iter + 1);
+  const double* pa = R.alpha.data();
+  const double* pb = R.beta.data();
+  auto analysis = [pa, pb, thold](int m, double amax, double bmax) {
+    std::pair<int, TmatInfo> out;
+    out.first = tmatrix_analyze(m, pa, pb, amax, bmax, out.second, thold);
+    return out;
+  };
   int launched = 0;
-  int m = 1;
   *failed = 0;
   int rc = AED_OK;
   if (m0 == 0) {
@@ -226,11 +255,15 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
     launched = 1;
   } else {
     launched = m0;
-    m = m0;
   }
+  const int par = R.ahead;
+  std::deque<std::future<std::pair<int, TmatInfo>>> pending;  // analyses of T(check), T(check + 1), ...
+  int check = m0 == 0 ? 1 : m0;  // the T size whose verdict comes next
+  int submit = check;            // the next T size to analyse
+  int m = check;
   while (true) {
-    // keep the device one step ahead of the host analysis
-    while (launched < m + 1 && launched < R.max_iter) {
+    // keep the device R.ahead steps ahead of the verdicts
+    while (launched < check + R.ahead && launched < R.max_iter) {
       void* a = slot(launched - 1);
       void* b = slot(launched);
       void* c = slot(launched + 1);
@@ -239,23 +272,39 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
       if (rc) return rc;
       ++launched;
     }
-    if (m > m0) {
-      rc = R.wait_step(m - 1);
-      if (rc) return rc;
+    // analyses of the sizes whose recurrence coefficients are in
+    while (submit < check + par && submit <= R.max_iter && submit <= launched) {
+      if (submit > m0) {
+        rc = R.wait_step(submit - 1);
+        if (rc) return rc;
+      }
+      if (submit > 1) {
+        pending.push_back(std::async(par > 1 ? std::launch::async : std::launch::deferred, analysis, submit, R.amax,
+                                     R.bmax));
+      } else {
+        std::promise<std::pair<int, TmatInfo>> none;
+        none.set_value({AED_OK, TmatInfo()});
+        pending.push_back(none.get_future());
+      }
+      ++submit;
     }
+    m = check;
+    std::pair<int, TmatInfo> v = pending.front().get();
+    pending.pop_front();
+    if (v.first) return v.first;
     if (m > 1) {
-      rc = tmatrix_analyze(m, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, R.f32 ? kFp32MergeRel : 0.0);
-      if (rc) return rc;
+      T = std::move(v.second);
       if (stop.done(T, m)) break;
     }
     if (m >= R.max_iter) {
       *failed = 1;
       break;
     }
-    ++m;
+    ++check;
   }
+  for (auto& f : pending) f.wait();  // analyses of sizes past the stop: discarded
   if (m == 1) {
-    rc = tmatrix_analyze(1, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, R.f32 ? kFp32MergeRel : 0.0);
+    rc = tmatrix_analyze(1, R.alpha.data(), R.beta.data(), R.amax, R.bmax, T, thold);
     if (rc) return rc;
   }
   AED_CUDA_TRY(cudaStreamSynchronize(R.h->stream));
@@ -264,12 +313,13 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
 }
 
 // The three rotating FP64 vectors of the recurrence in workspace slot 0.
-int recurrence_buffers(aed_handle* h, void* buf[3]) {
+int recurrence_buffers(aed_handle* h, void* buf[kMaxRing]) {
   const size_t vb = ((size_t)h->vlen * 8 + 255) & ~(size_t)255;
+  const int nr = ring_slots(h);
   void* ws = nullptr;
-  const int rc = handle_workspace(h, 0, 3 * vb, &ws);
+  const int rc = handle_workspace(h, 0, (size_t)nr * vb, &ws);
   if (rc) return rc;
-  for (int q = 0; q < 3; ++q) buf[q] = (char*)ws + q * vb;
+  for (int q = 0; q < nr; ++q) buf[q] = (char*)ws + q * vb;
   return AED_OK;
 }
 
@@ -301,7 +351,7 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
   if (resume && (!h->rec_live || m0 < 1 || (int)h->last_alpha.size() != m0))
     return fail(AED_ERR_INVALID, "no live Lanczos recurrence to resume (solve or aed_lanczos_load first)");
   if (m0 >= max_iter) max_iter = m0 + 1;
-  void* buf[3];
+  void* buf[kMaxRing];
   void* ab = nullptr;  // device alpha/beta pairs
   double* hab = nullptr;
   if ((rc = recurrence_buffers(h, buf)) || (rc = handle_workspace(h, 1, (size_t)2 * (max_iter + 2) * 8, &ab)) ||
@@ -309,7 +359,8 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
     return rc;
   double* d_ab = (double*)ab;
   h->rec_live = false;  // from here on the slots change
-  Recurrence R{h, false, D, max_iter, d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
+  const int nr = ring_slots(h);
+  Recurrence R{h, false, D, max_iter, lanczos_lookahead(h), d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
   if (resume) {
     R.alpha = h->last_alpha;
     R.beta = h->last_beta;
@@ -327,7 +378,7 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
   }
   StopRule stop{nev, rtol, atol, energy_bound, etol, min_steps};
   int iters = 0, failed = 0;
-  rc = run_recurrence(R, stop, [&](int j) { return buf[j % 3]; }, m0, &iters, &failed, T);
+  rc = run_recurrence(R, stop, [&](int j) { return buf[j % nr]; }, m0, &iters, &failed, T);
   if (rc) return rc;
   const int n = std::min(nev, (int)T.evals.size());
   r->n_evals = n;
@@ -397,7 +448,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   }
   if ((rc = normalize(h, V0, D))) return rc;
   // phase 1: FP32 vectors, stop at FP32-level residual estimates
-  Recurrence R{h, true, D, cap - 1, d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
+  Recurrence R{h, true, D, cap - 1, lanczos_lookahead(h), d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
   const double tol32 = 2e-6;
   StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
@@ -668,11 +719,11 @@ int lanczos_save(aed_handle* h, void* buf, int64_t bytes) {
   p += (size_t)m * 8;
   std::memcpy(p, h->last_beta.data(), (size_t)m * 8);
   p += (size_t)m * 8;
-  void* slots[3];
+  void* slots[kMaxRing];
   int rc = recurrence_buffers(h, slots);
   if (rc) return rc;
-  AED_CUDA_TRY(cudaMemcpyAsync(p, slots[(m - 1) % 3], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
-  AED_CUDA_TRY(cudaMemcpyAsync(p + (size_t)D * 8, slots[m % 3], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(p, slots[(m - 1) % ring_slots(h)], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(p + (size_t)D * 8, slots[m % ring_slots(h)], (size_t)D * 8, cudaMemcpyDeviceToHost, h->stream));
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return AED_OK;
 }
@@ -693,11 +744,11 @@ int lanczos_load(aed_handle* h, const void* buf, int64_t bytes) {
   std::memcpy(al.data(), p, (size_t)m * 8);
   std::memcpy(be.data(), p + (size_t)m * 8, (size_t)m * 8);
   p += (size_t)16 * m;
-  void* slots[3];
+  void* slots[kMaxRing];
   int rc = recurrence_buffers(h, slots);
   if (rc) return rc;
-  AED_CUDA_TRY(cudaMemcpyAsync(slots[(m - 1) % 3], p, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
-  AED_CUDA_TRY(cudaMemcpyAsync(slots[m % 3], p + (size_t)D * 8, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(slots[(m - 1) % ring_slots(h)], p, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(slots[m % ring_slots(h)], p + (size_t)D * 8, (size_t)D * 8, cudaMemcpyHostToDevice, h->stream));
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->last_alpha = al;
   h->last_beta = be;

