@@ -128,6 +128,8 @@ struct ParsedParams {
   std::vector<double> jz, jxy, kq, site_h, site_d;
 };
 int parse_parameters(const char* text, ParsedParams& out);
+// Lattice dimension, extents and periodic flags of the parameters.
+int lattice_geometry(const char* text, int* dim, int ext[2], int periodic[2]);
 // Momenta the sector loop visits (diag.h:93-114): TOTAL_MOMENTUM when given,
 // else every translation momentum when TRANSLATION_SYMMETRY (default true),
 // else none.  *n_dirs = periodic directions of the lattice.

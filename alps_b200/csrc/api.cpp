@@ -695,6 +695,34 @@ int aed_lattice_translations(const char* params, const double* k, int32_t n_dirs
   return AED_OK;
 }
 
+int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
+                    const int32_t* site_j, double* out) {
+  if (!h || !psi || (n > 0 && (!site_i || !out || (kind != AED_OBS_SZ && !site_j))))
+    return fail(AED_ERR_INVALID, "NULL argument");
+  if (h->mom) return fail(AED_ERR_INVALID, "aed_expectation: Sz sectors only");
+  if (kind < AED_OBS_SZ || kind > AED_OBS_SPSM) return fail(AED_ERR_INVALID, "unknown observable kind");
+  const int N = h->model.N;
+  for (int p = 0; p < n; ++p)
+    if (site_i[p] < 0 || site_i[p] >= N || (kind != AED_OBS_SZ && (site_j[p] < 0 || site_j[p] >= N)))
+      return fail(AED_ERR_INVALID, "site index out of range");
+  if (n <= 0) return AED_OK;
+  DeviceGuard g(h->device);
+  return measure_pairs(h, psi, kind, n, site_i, site_j, out);
+}
+
+int aed_lattice_geometry(const char* params, int32_t* dim, int32_t* extent, int32_t* periodic) {
+  if (!params || !dim || !extent || !periodic) return fail(AED_ERR_INVALID, "NULL argument");
+  int d = 0, ext[2] = {1, 1}, per[2] = {0, 0};
+  const int rc = lattice_geometry(params, &d, ext, per);
+  if (rc) return rc;
+  *dim = d;
+  for (int i = 0; i < d; ++i) {
+    extent[i] = ext[i];
+    periodic[i] = per[i];
+  }
+  return AED_OK;
+}
+
 int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   if (!h || !model) return fail(AED_ERR_INVALID, "NULL argument");
   if (model->n_sites != h->model.N || model->n_up != h->model.n_up)

@@ -106,6 +106,15 @@ int mem_dev_alloc_n(T** p, size_t count) {
   return rc;
 }
 
+// Expectation values of site operators in one vector (measure.cu): kind
+// kMeasSz <Sz_i>, kMeasSzSz <Sz_i Sz_j>, kMeasSpSm <S+_i S-_j>, n pairs.
+constexpr int kMeasSz = AED_OBS_SZ, kMeasSzSz = AED_OBS_SZSZ, kMeasSpSm = AED_OBS_SPSM;
+constexpr int kMeasPairs = 32;  // pairs per pass over the vector
+struct MeasPairs {
+  uint32_t mi[kMeasPairs], mj[kMeasPairs];
+};
+int measure_pairs(aed_handle* h, const void* psi, int kind, int n, const int32_t* si, const int32_t* sj, double* out);
+
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
 // Choose the apply variant for this precision now (timed launches on x, y)
 // unless already chosen; handle_hv does this on its first call otherwise.

@@ -261,6 +261,11 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
   int check = m0 == 0 ? 1 : m0;  // the T size whose verdict comes next
   int submit = check;            // the next T size to analyse
   int m = check;
+  // beta_{j} = 0 exactly: the Krylov space is invariant, T(j + 1) holds exact
+  // eigenvalues and the next vector would be 0/0; the recurrence stops there
+  // (ietl divides by it regardless; an H with no off-diagonal coupling to the
+  // start vector's complement is the usual case)
+  int invariant_m = 0;
   while (true) {
     // keep the device R.ahead steps ahead of the verdicts
     while (launched < check + R.ahead && launched < R.max_iter) {
@@ -277,6 +282,7 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
       if (submit > m0) {
         rc = R.wait_step(submit - 1);
         if (rc) return rc;
+        if (!invariant_m && R.beta.back() == 0.0) invariant_m = submit;
       }
       if (submit > 1) {
         pending.push_back(std::async(par > 1 ? std::launch::async : std::launch::deferred, analysis, submit, R.amax,
@@ -296,6 +302,7 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
       T = std::move(v.second);
       if (stop.done(T, m)) break;
     }
+    if (m == invariant_m) break;  // exact: every value of T(m) is an eigenvalue
     if (m >= R.max_iter) {
       *failed = 1;
       break;

@@ -541,6 +541,25 @@ int read_geometry(const Params& p, Eval& ev, Geometry& g) {
 
 }  // namespace
 
+int lattice_geometry(const char* text, int* dim, int ext[2], int periodic[2]) {
+  Params p;
+  int rc = parse_kv(text, p);
+  if (rc) return rc;
+  Eval ev{p.kv, spin_defaults()};
+  try {
+    Geometry g;
+    if ((rc = read_geometry(p, ev, g))) return rc;
+    *dim = g.L.dim;
+    for (int d = 0; d < g.L.dim; ++d) {
+      ext[d] = g.ext[d];
+      periodic[d] = g.L.periodic[d] ? 1 : 0;
+    }
+  } catch (const std::exception& e) {
+    return fail(AED_ERR_INVALID, std::string("parameter error: ") + e.what());
+  }
+  return AED_OK;
+}
+
 int lattice_momenta(const char* text, int* n_dirs, std::vector<std::vector<double>>& ks) {
   Params p;
   int rc = parse_kv(text, p);

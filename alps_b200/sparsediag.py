@@ -27,6 +27,7 @@ from xml.sax.saxutils import escape
 import numpy as np
 
 from . import AEDError, FP64, Hamiltonian, lattice_momenta, lattice_translations, model_from_parameters, momentum_label
+from . import measure as _measure
 
 
 def half_integer_text(v: Fraction) -> str:
@@ -58,6 +59,11 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
         n = _site_count(params)
         sz_values = [Fraction(k, 2) for k in range(-n, n + 1, 2)]
     momenta = lattice_momenta(params)
+    req = _measure.requests(params)
+    measuring = any(req.values())
+    if measuring and momenta:
+        raise AEDError(-1, "measurements run in Sz sectors: set TRANSLATION_SYMMETRY=false")
+    geometry = _measure.Geometry(params) if measuring else None
     label_k = bool(momenta) and not str(params.get("TOTAL_MOMENTUM", "")).strip()
     for sz in sz_values:
         p = params if sz is None else dict(params, Sz_total=float(sz))
@@ -75,8 +81,15 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
                 if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
                     continue
                 r = ham.solve(nev=max(1, mp["nev"]), max_iter=mp["max_iter"], seed=seed)
-                sectors.append({"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
-                                "iterations": r["iterations"], "converged": r["converged"]})
+                sec = {"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
+                       "iterations": r["iterations"], "converged": r["converged"]}
+                if measuring and not ham.momentum and len(r["evals"]):
+                    # perform_measurements on every eigenvector (diag.h:191-314, sparsediag.h:151-159)
+                    vecs, _, _ = ham.eigenvectors(k=len(r["evals"]), seed=seed)
+                    sec["measurements"] = [_measure.measure(ham, v, params, geometry) for v in vecs]
+                    for v in vecs:
+                        v.free()
+                sectors.append(sec)
             finally:
                 ham.close()
     e0, gap = ground_state_and_gap([s["energies"] for s in sectors])

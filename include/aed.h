@@ -109,6 +109,23 @@ int aed_destroy(aed_handle* h);
  * reference's matrices are freed with their task. */
 int aed_empty_cache(int device);
 
+/* ---- measurements ------------------------------------------------------- */
+#define AED_OBS_SZ 0   /* <Sz_i>                       */
+#define AED_OBS_SZSZ 1 /* <Sz_i Sz_j>                  */
+#define AED_OBS_SPSM 2 /* <S+_i S-_j> (real vectors)   */
+/* Expectation values <psi| O |psi> of site operators in a device vector of
+ * the handle (not normalised by |psi|): out[p] for the site pair
+ * (site_i[p], site_j[p]) (site_j ignored for AED_OBS_SZ).  The quantities
+ * DiagMatrix::perform_measurements evaluates for MEASURE_AVERAGE, _LOCAL,
+ * _CORRELATIONS and _STRUCTURE_FACTOR (applications/diag/diag.h:191-314 via
+ * calculate(), :316-339), for the spin-1/2 operators Sz, Splus, Sminus.
+ * Sz sectors only (not momentum sectors). */
+int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
+                    const int32_t* site_j, double* out);
+/* Lattice of a parameter file: dimension, extents and periodic flags
+ * (boundary conditions) of each direction (lib/xml/lattices.xml.in). */
+int aed_lattice_geometry(const char* params, int32_t* dim, int32_t* extent, int32_t* periodic);
+
 /* ---- momentum sectors --------------------------------------------------- */
 /* Translations of a lattice at one momentum k: the identity first. */
 typedef struct {

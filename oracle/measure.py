@@ -1,0 +1,148 @@
+"""Oracle restatement of sparsediag's eigenvector measurements for spin-1/2 Sz sectors.
+
+TEST INFRASTRUCTURE ONLY: used by tests/ to check alps_b200.measure; the
+engine never imports this module.  Pure Python / numpy on explicit basis
+lists, for small sectors.
+
+Restates (paths relative to the ALPS source tree):
+  * MEASURE_* parameter parsing          src/alps/scheduler/measurement_operators.C:25-70
+  * perform_measurements: averages sum_i <op_i>/N, local <op_i>, correlations
+    at the first site pair of each distance class, structure factor
+    sum_ij Re(<a_i b_j> conj(e^{i k r_i}) e^{i k r_j}) / N
+                                         applications/diag/diag.h:191-314
+  * distance classes                     src/alps/lattice/hypercubic.h:325-349
+  * momenta (cell order, x > L/2 -> x - L)  hypercubic.h:371-387
+  * spin-1/2 site operators Sz = diag(-1/2, 1/2), S+ |down> = |up>, S- |up> = |down>
+                                         lib/xml/models.xml.in (spin site basis and operators)
+States are integers with site i at bit n-1-i, up = 1 (the basis order).
+"""
+
+from __future__ import annotations
+
+import math
+import re
+
+import numpy as np
+
+from .lattice import _LATTICES, _extents
+
+
+def requests(params: dict) -> dict:
+    out = {"average": {}, "local": {}, "correlations": {}, "structure_factor": {}}
+    for key, val in params.items():
+        m = re.match(r"^MEASURE_(AVERAGE|LOCAL|CORRELATIONS|STRUCTURE_FACTOR)\[(.*)\]$", str(key))
+        if not m:
+            continue
+        v = str(val).strip().strip('"')
+        if m.group(1) == "AVERAGE":
+            out["average"][m.group(2)] = v
+        elif m.group(1) == "LOCAL":
+            out["local"][m.group(2)] = v
+        else:
+            pair = tuple(v.split(":", 1)) if ":" in v else (v, v)
+            out["correlations" if m.group(1) == "CORRELATIONS" else "structure_factor"][m.group(2)] = pair
+    return out
+
+
+def _geometry(params):
+    _, ext_spec, bnd = _LATTICES[params["LATTICE"]]
+    ext = _extents(ext_spec, params)
+    n = int(np.prod(ext))
+    coords = []
+    for c in range(n):
+        cc = []
+        for d in range(len(ext) - 1, -1, -1):
+            cc.append(c % ext[d])
+            c //= ext[d]
+        coords.append(cc[::-1])
+    return ext, [b == "periodic" for b in bnd], coords
+
+
+def _distance(ext, per, x, y):
+    d = 0
+    for a, L in enumerate(ext):
+        if per[a]:
+            d = d * L + ((y[a] - x[a]) % L)
+        else:
+            d = L * (d * L + x[a]) + y[a]
+    return d
+
+
+def _num_distances(ext, per):
+    return int(np.prod([L if p else L * L for L, p in zip(ext, per)]))
+
+
+def _op_apply(op, site, n, s):
+    """op acting on site of state s: (coefficient, new state) or None."""
+    m = 1 << (n - 1 - site)
+    up = (s & m) != 0
+    if op == "Sz":
+        return (0.5 if up else -0.5), s
+    if op == "Splus":
+        return (1.0, s | m) if not up else None
+    if op == "Sminus":
+        return (1.0, s & ~m) if up else None
+    raise ValueError(op)
+
+
+def _expect(states, psi, n, ops):
+    """<psi| ops[0] ops[1] ... |psi> with ops = [(name, site)], the rightmost acting first."""
+    index = {int(s): k for k, s in enumerate(states)}
+    tot = 0.0
+    for k, s in enumerate(states):
+        s, c = int(s), 1.0
+        for name, site in reversed(ops):
+            r = _op_apply(name, site, n, s)
+            if r is None:
+                c = 0.0
+                break
+            c *= r[0]
+            s = r[1]
+        if c != 0.0 and s in index:
+            tot += c * psi[index[s]] * psi[k]
+    return tot
+
+
+def measure(states, psi, params) -> dict:
+    ext, per, coords = _geometry(params)
+    n_sites = len(coords)
+    req = requests(params)
+    out = {"average": {}, "local": {}, "correlations": {}, "structure_factor": {}}
+    for name, op in req["average"].items():
+        out["average"][name] = sum(_expect(states, psi, n_sites, [(op, i)]) for i in range(n_sites)) / n_sites
+    for name, op in req["local"].items():
+        out["local"][name] = [_expect(states, psi, n_sites, [(op, i)]) for i in range(n_sites)]
+    nd = _num_distances(ext, per)
+    for name, (a, b) in req["correlations"].items():
+        row, done = [0.0] * nd, [False] * nd
+        for i in range(n_sites):
+            for j in range(n_sites):
+                d = _distance(ext, per, coords[i], coords[j])
+                if not done[d]:
+                    row[d] = _expect(states, psi, n_sites, [(a, i), (b, j)])
+                    done[d] = True
+        out["correlations"][name] = row
+    for name, (a, b) in req["structure_factor"].items():
+        c = np.array([[_expect(states, psi, n_sites, [(a, i), (b, j)]) for j in range(n_sites)]
+                      for i in range(n_sites)])
+        ks = []
+        for cc in coords:
+            k = []
+            for a_, L in enumerate(ext):
+                x = cc[a_]
+                if x > L // 2:
+                    x -= L
+                k.append(2.0 * math.pi * x / L)
+            ks.append(k)
+        sk = []
+        for k in ks:
+            val = 0.0
+            for i in range(n_sites):
+                for j in range(n_sites):
+                    p1 = sum(k[d] * coords[i][d] for d in range(len(ext)))
+                    p2 = sum(k[d] * coords[j][d] for d in range(len(ext)))
+                    val += (c[i, j] * np.conj(complex(math.cos(p1), math.sin(p1))) *
+                            complex(math.cos(p2), math.sin(p2))).real / n_sites
+            sk.append(val)
+        out["structure_factor"][name] = sk
+    return out
