@@ -133,6 +133,7 @@ def lib():
                                                    ctypes.c_int, ctypes.POINTER(_P)]),
             "aed_momentum_basis": (ctypes.c_int, [_P, _U32P, _DP, _I64, _I64]),
             "aed_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
+            "aed_momentum_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
             "aed_lattice_geometry": (ctypes.c_int, [ctypes.c_char_p, _I32P, _I32P, _I32P]),
             "aed_lattice_momenta": (ctypes.c_int, [ctypes.c_char_p, _I32P, _I32P, _DP, _I32]),
             "aed_lattice_translations": (ctypes.c_int, [ctypes.c_char_p, _DP, _I32, _I32P, _I32P, _I32P, _DP, _I32]),

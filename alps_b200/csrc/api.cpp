@@ -695,11 +695,48 @@ int aed_lattice_translations(const char* params, const double* k, int32_t n_dirs
   return AED_OK;
 }
 
+int aed_momentum_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
+                             const int32_t* site_j, double* out) {
+  if (!h || !psi || !out || (n > 0 && (!site_i || (kind != AED_OBS_SZ && !site_j))))
+    return fail(AED_ERR_INVALID, "NULL argument");
+  if (!h->mom) return fail(AED_ERR_INVALID, "aed_momentum_expectation: not a momentum sector");
+  if (kind < AED_OBS_SZ || kind > AED_OBS_SPSM) return fail(AED_ERR_INVALID, "unknown observable kind");
+  const int N = h->model.N;
+  for (int p = 0; p < n; ++p)
+    if (site_i[p] < 0 || site_i[p] >= N || (kind != AED_OBS_SZ && (site_j[p] < 0 || site_j[p] >= N)))
+      return fail(AED_ERR_INVALID, "site index out of range");
+  *out = 0.0;
+  if (n <= 0 || h->dim == 0) return AED_OK;
+  DeviceGuard g(h->device);
+  const int grid = mom_expect_grid(h->dim);
+  void* w = nullptr;
+  int rc = handle_workspace(h, 1, (size_t)grid * 8, &w);
+  if (rc) return rc;
+  std::vector<double> hp((size_t)grid);
+  double total = 0.0;
+  for (int p0 = 0; p0 < n; p0 += kMomPairs) {
+    MomPairs pairs{};
+    pairs.n = std::min(kMomPairs, n - p0);
+    for (int p = 0; p < pairs.n; ++p) {
+      pairs.mi[p] = 1u << (N - 1 - site_i[p0 + p]);
+      pairs.mj[p] = kind == AED_OBS_SZ ? 0u : 1u << (N - 1 - site_j[p0 + p]);
+    }
+    if ((rc = mom_expectation(*h->mp, h->dt, h->mom_tables(), (const double*)psi, kind, pairs, (double*)w, grid,
+                              h->stream)))
+      return rc;
+    AED_CUDA_TRY(cudaMemcpyAsync(hp.data(), w, hp.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (double v : hp) total += v;
+  }
+  *out = total;
+  return AED_OK;
+}
+
 int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
                     const int32_t* site_j, double* out) {
   if (!h || !psi || (n > 0 && (!site_i || !out || (kind != AED_OBS_SZ && !site_j))))
     return fail(AED_ERR_INVALID, "NULL argument");
-  if (h->mom) return fail(AED_ERR_INVALID, "aed_expectation: Sz sectors only");
+  if (h->mom) return fail(AED_ERR_INVALID, "aed_expectation: Sz sectors only (aed_momentum_expectation)");
   if (kind < AED_OBS_SZ || kind > AED_OBS_SPSM) return fail(AED_ERR_INVALID, "unknown observable kind");
   const int N = h->model.N;
   for (int p = 0; p < n; ++p)

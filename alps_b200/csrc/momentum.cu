@@ -228,6 +228,56 @@ __global__ void __launch_bounds__(kMomThreads) mom_hv_kernel(const __grid_consta
   }
 }
 
+// One pass per call: each CTA sums its rows' terms into part[blockIdx.x].
+template <int KIND>
+__global__ void __launch_bounds__(kMomThreads) mom_expect_kernel(const __grid_constant__ MomParams mp,
+                                                                 const DevTables t, const MomTables m,
+                                                                 const double2* __restrict__ psi,
+                                                                 const __grid_constant__ MomPairs pairs,
+                                                                 double* __restrict__ part) {
+  __shared__ double pre[kMaxTrans], pim[kMaxTrans];
+  __shared__ double red[33];
+  for (int q = threadIdx.x; q < mp.n_trans; q += kMomThreads) {
+    pre[q] = mp.phase_re[q];
+    pim[q] = mp.phase_im[q];
+  }
+  __syncthreads();
+  const uint32_t lm = (1u << t.Nlo) - 1u;
+  const uint32_t jmask = (1u << kMomRepBits) - 1u;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kMomThreads + threadIdx.x; i < m.dim; i += (int64_t)gridDim.x * kMomThreads) {
+    const uint32_t r = m.reps[i];
+    const double2 pi = psi[i];
+    const double w = pi.x * pi.x + pi.y * pi.y;
+    double d = 0.0;    // diagonal part of the pair sum on r
+    double ore = 0.0;  // Re conj(psi_i) (off-diagonal part applied to psi)_i
+    for (int p = 0; p < pairs.n; ++p) {
+      const uint32_t mi = pairs.mi[p], mj = pairs.mj[p];
+      if (KIND == AED_OBS_SZ) {
+        d += (r & mi) ? 0.5 : -0.5;
+      } else if (KIND == AED_OBS_SZSZ) {
+        d += ((r & mi) ? 0.5 : -0.5) * ((r & mj) ? 0.5 : -0.5);
+      } else if (mi == mj) {
+        d += (r & mi) ? 1.0 : 0.0;
+      } else if (!(r & mi) && (r & mj)) {
+        const uint32_t s2 = r ^ mi ^ mj;
+        const uint32_t e = __ldg(m.map + __ldg(t.thi + (s2 >> t.Nlo)) + __ldg(t.tlo + (s2 & lm)));
+        if (e == kMomNone) continue;
+        const uint32_t j = e & jmask, tt = e >> kMomRepBits;
+        const double f = __ldg(m.norm + j) / m.norm[i];
+        const double cr = f * pre[tt], ci = f * pim[tt];
+        const double2 xj = psi[j];
+        // conj(psi_i) * (c * psi_j), real part
+        const double yr = cr * xj.x - ci * xj.y, yi = cr * xj.y + ci * xj.x;
+        ore += pi.x * yr + pi.y * yi;
+      }
+    }
+    acc += w * d + ore;
+  }
+  const double tot = block_sum_all<kMomThreads>(acc, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
 int grid_for(int64_t units) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -308,6 +358,20 @@ int launch_mom_diag(const HvParams& P, const uint32_t* reps, int64_t dim, double
   if (dim == 0) return AED_OK;
   mom_diag_kernel<<<grid_for((dim + kMomThreads - 1) / kMomThreads), kMomThreads, 0, st>>>(P, reps, dim, diag);
   return check_launch_counted("mom_diag_kernel");
+}
+
+int mom_expect_grid(int64_t dim) { return grid_for((dim + kMomThreads - 1) / kMomThreads); }
+
+int mom_expectation(const MomParams& mp, const DevTables& t, const MomTables& m, const double* psi, int kind,
+                    const MomPairs& pairs, double* part, int grid, cudaStream_t st) {
+  const double2* p2 = reinterpret_cast<const double2*>(psi);
+  if (kind == AED_OBS_SZ)
+    mom_expect_kernel<AED_OBS_SZ><<<grid, kMomThreads, 0, st>>>(mp, t, m, p2, pairs, part);
+  else if (kind == AED_OBS_SZSZ)
+    mom_expect_kernel<AED_OBS_SZSZ><<<grid, kMomThreads, 0, st>>>(mp, t, m, p2, pairs, part);
+  else
+    mom_expect_kernel<AED_OBS_SPSM><<<grid, kMomThreads, 0, st>>>(mp, t, m, p2, pairs, part);
+  return check_launch_counted("mom_expect_kernel");
 }
 
 int launch_mom_hv(const MomParams& mp, const DevTables& t, const MomTables& m, const double* x, double* y,

@@ -59,4 +59,19 @@ int launch_mom_hv(const MomParams& mp, const DevTables& t, const MomTables& m, c
                   double* alpha_part, cudaStream_t st);
 __host__ __device__ inline int64_t mom_tiles(int64_t dim) { return (dim + kMomTileRows - 1) / kMomTileRows; }
 
+// <psi| sum_p O(i_p, j_p) |psi> in a momentum sector for a list of site pairs
+// whose sum is translation invariant (a distance class): kind AED_OBS_SZ
+// (sum of Sz_i), AED_OBS_SZSZ, AED_OBS_SPSM (S+_i S-_j; i = j: the projector
+// on spin up).  Diagonal terms are read on the representative; S+_i S-_j maps
+// a representative with site j up and site i down to its image's orbit with
+// the same phase and normalisation factor as a Hamiltonian flip.
+constexpr int kMomPairs = 64;
+struct MomPairs {
+  int n;
+  uint32_t mi[kMomPairs], mj[kMomPairs];
+};
+int mom_expectation(const MomParams& mp, const DevTables& t, const MomTables& m, const double* psi, int kind,
+                    const MomPairs& pairs, double* part, int grid, cudaStream_t st);
+int mom_expect_grid(int64_t dim);
+
 }  // namespace aed

@@ -20,8 +20,14 @@ momenta (hypercubic.h:371-387: cell order, k_d = 2 pi x_d / L_d with
 x_d > L_d / 2 taken as x_d - L_d).  Operators: the spin-1/2 site operators
 Sz, Splus, Sminus.  The expectation values come from aed_expectation (one
 pass over the vector per 32 site pairs, on the GPU); this module only
-chooses the pairs and combines the numbers.  Sz sectors only: momentum
-sectors (Bloch bases) are not measured.
+chooses the pairs and combines the numbers.
+
+In a momentum sector (translation invariance) perform_measurements skips the
+local values, averages each correlation over all pairs of its distance class
+(divided by the class's multiplicity, diag.h:236-258), and sums the
+structure factor over all pairs; a class's pairs add up to a translation-
+invariant operator, whose Bloch-basis expectation aed_momentum_expectation
+returns, and e^{ik(r_j - r_i)} is the same for every pair of a class.
 """
 
 from __future__ import annotations
@@ -148,11 +154,76 @@ def _pair_values(ham, psi, a, b, si, sj):
     return np.zeros(si.size)  # the product changes Sz: zero in an Sz sector
 
 
+def momentum_sum(ham, psi, kind: int, si, sj=None) -> float:
+    """aed_momentum_expectation: <psi| sum_p O(si[p], sj[p]) |psi> in a momentum sector."""
+    si = np.ascontiguousarray(si, dtype=np.int32)
+    sj = np.ascontiguousarray(si if sj is None else sj, dtype=np.int32)
+    out = ctypes.c_double(0.0)
+    _check(lib().aed_momentum_expectation(ham._h, psi.ptr, kind, si.size, si.ctypes.data_as(_I32P),
+                                          sj.ctypes.data_as(_I32P), ctypes.byref(out)))
+    return out.value
+
+
+def _pair_sum(ham, psi, a, b, pairs) -> float:
+    """Momentum sector: <sum over pairs of a_i b_j> (the same site as the product a b of that site)."""
+    _check_op(a)
+    _check_op(b)
+    si = [p[0] for p in pairs]
+    sj = [p[1] for p in pairs]
+    if a == "Sz" and b == "Sz":
+        return momentum_sum(ham, psi, OBS_SZSZ, si, sj)
+    if (a, b) == ("Splus", "Sminus"):
+        return momentum_sum(ham, psi, OBS_SPSM, si, sj)
+    if (a, b) == ("Sminus", "Splus"):
+        diff = [(i, j) for i, j in pairs if i != j]
+        same = [i for i, j in pairs if i == j]
+        v = momentum_sum(ham, psi, OBS_SPSM, [j for i, j in diff], [i for i, j in diff]) if diff else 0.0
+        if same:  # S- S+ on one site: the projector on spin down, 1/2 - Sz
+            v += 0.5 * len(same) - momentum_sum(ham, psi, OBS_SZ, same)
+        return v
+    return 0.0
+
+
+def _measure_momentum(ham, psi, req, g) -> dict:
+    n = g.n
+    out = {"average": {}, "local": {}, "correlations": {}, "structure_factor": {}}
+    for name, op in req["average"].items():
+        _check_op(op)
+        out["average"][name] = momentum_sum(ham, psi, OBS_SZ, list(range(n))) / n if op == "Sz" else 0.0
+    classes = {}
+    for i in range(n):
+        for j in range(n):
+            classes.setdefault(g.distance(i, j), []).append((i, j))
+    nd = g.num_distances()
+    sums = {}
+    for name, (a, b) in list(req["correlations"].items()) + list(req["structure_factor"].items()):
+        if (a, b) not in sums:
+            sums[(a, b)] = {d: _pair_sum(ham, psi, a, b, ps) for d, ps in classes.items()}
+    for name, (a, b) in req["correlations"].items():
+        row = [0.0] * nd
+        for d, ps in classes.items():
+            row[d] = sums[(a, b)][d] / len(ps)
+        out["correlations"][name] = row
+    if req["structure_factor"]:
+        r = np.array(g.coords, dtype=float)
+        ks = g.momenta()
+        for name, (a, b) in req["structure_factor"].items():
+            sk = []
+            for k in ks:
+                val = 0.0
+                for d, ps in classes.items():
+                    i, j = ps[0]
+                    val += sums[(a, b)][d] * math.cos(float(np.dot(k, r[j] - r[i])))
+                sk.append(val / n)
+            out["structure_factor"][name] = sk
+    return out
+
+
 def measure(ham, psi, params, geometry: Geometry | None = None) -> dict:
-    """The MEASURE_* quantities of params in the (normalised) device vector psi of an Sz-sector handle."""
-    if getattr(ham, "momentum", False):
-        raise AEDError(ERR_INVALID, "measurements: Sz sectors only (TRANSLATION_SYMMETRY=false)")
+    """The MEASURE_* quantities of params in the (normalised) device vector psi of a handle."""
     req = requests(params)
+    if getattr(ham, "momentum", False):
+        return _measure_momentum(ham, psi, req, geometry or Geometry(params))
     g = geometry or Geometry(params)
     n = g.n
     out = {"average": {}, "local": {}, "correlations": {}, "structure_factor": {}}

@@ -61,8 +61,6 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
     momenta = lattice_momenta(params)
     req = _measure.requests(params)
     measuring = any(req.values())
-    if measuring and momenta:
-        raise AEDError(-1, "measurements run in Sz sectors: set TRANSLATION_SYMMETRY=false")
     geometry = _measure.Geometry(params) if measuring else None
     label_k = bool(momenta) and not str(params.get("TOTAL_MOMENTUM", "")).strip()
     for sz in sz_values:
@@ -83,7 +81,7 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
                 r = ham.solve(nev=max(1, mp["nev"]), max_iter=mp["max_iter"], seed=seed)
                 sec = {"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
                        "iterations": r["iterations"], "converged": r["converged"]}
-                if measuring and not ham.momentum and len(r["evals"]):
+                if measuring and len(r["evals"]):
                     # perform_measurements on every eigenvector (diag.h:191-314, sparsediag.h:151-159)
                     vecs, _, _ = ham.eigenvectors(k=len(r["evals"]), seed=seed)
                     sec["measurements"] = [_measure.measure(ham, v, params, geometry) for v in vecs]

@@ -122,6 +122,14 @@ int aed_empty_cache(int device);
  * Sz sectors only (not momentum sectors). */
 int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
                     const int32_t* site_j, double* out);
+/* Momentum sectors: <psi| sum_p O(site_i[p], site_j[p]) |psi> (the real part)
+ * for a list of pairs whose sum is translation invariant, such as all pairs
+ * of one distance class; *out gets the sum.  What perform_measurements
+ * accumulates over the pairs of a distance class in a translation-invariant
+ * sector (applications/diag/diag.h:236-258) before dividing by the class's
+ * multiplicity, and over all pairs for the structure factor (:262-307). */
+int aed_momentum_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
+                             const int32_t* site_j, double* out);
 /* Lattice of a parameter file: dimension, extents and periodic flags
  * (boundary conditions) of each direction (lib/xml/lattices.xml.in). */
 int aed_lattice_geometry(const char* params, int32_t* dim, int32_t* extent, int32_t* periodic);

@@ -83,8 +83,6 @@ def test_sparsediag_attaches_measurements():
     e0 = res["ground_state_energy"]
     d1 = m["correlations"]["Diagonal spin correlations"][1] + m["correlations"]["Offdiagonal spin correlations"][1]
     assert abs(d1 - e0 / 8) < 1e-9
-    with pytest.raises(ed.AEDError, match="TRANSLATION_SYMMETRY"):
-        sparsediag.run(dict(p, TRANSLATION_SYMMETRY="true"))
 
 
 def test_zero_coupling_stops_at_the_invariant_space():
@@ -99,3 +97,23 @@ def test_zero_coupling_stops_at_the_invariant_space():
     vecs, ev, res = ham.eigenvectors(k=1, seed=1)
     assert ev[0] == 0.0 and res[0] == 0.0
     ham.close()
+
+
+@pytest.mark.parametrize("lat,geo,couplings", [("nnn chain lattice", {"L": 10}, {"J": 1, "J1": 0.3}),
+                                               ("square lattice", {"L": 4, "W": 3}, {"J": 1})])
+def test_momentum_sector_measurements(lat, geo, couplings):
+    """With translation symmetry on, the sector holding the ground state reports the class-averaged
+    correlations, the average and the structure factors of the (non-degenerate) Sz=0 ground state,
+    computed by the oracle on the dense ground state (1e-8)."""
+    p = dict(geo, MODEL="spin", LATTICE=lat, CONSERVED_QUANTUMNUMBERS="Sz", Sz_total=0, NUMBER_EIGENVALUES=1,
+             **couplings, **{k: v for k, v in MEAS.items() if "LOCAL" not in k})
+    res = sparsediag.run(p)
+    best = min(res["sectors"], key=lambda s: s["energies"][0])
+    got = best["measurements"][0]
+    n, n_up, bonds = lattice.spin_model(dict(p, TRANSLATION_SYMMETRY="false"))
+    st, A = _dense(n, n_up, bonds, None)
+    w, Z = np.linalg.eigh(A)
+    assert abs(w[0] - best["energies"][0]) < 1e-9 and w[1] - w[0] > 1e-6
+    ref = omeasure.measure_translation_invariant(st, Z[:, 0], p)
+    assert got["local"] == {}
+    _close(got, ref, 1e-8)
