@@ -113,8 +113,39 @@ def ground_state_and_gap(energies):
     return (None if min_val == inf else min_val), (None if exc_val == inf else exc_val - min_val)
 
 
+def _num(v) -> str:
+    """A number as oxstream writes it (boost::lexical_cast<std::string>(double): 17 significant digits)."""
+    return "%.17g" % float(v)
+
+
+def _coord(c) -> str:
+    """alps::coordinate_to_string (src/alps/lattice/coordinate_traits.h:97-110), default precision."""
+    return "( " + ",".join("%g" % float(x) for x in c) + " )"
+
+
+def _labels(params):
+    """Site, distance and momentum labels of the lattice (graph_helper::site_labels,
+    hypercubic_lattice::distance_labels / momenta_labels, hypercubic.h:291-314)."""
+    g = _measure.Geometry(params)
+    sites = [_coord(c) for c in g.coords]
+    dist = [""] * g.num_distances()
+    for i in range(g.n):
+        for j in range(g.n):
+            d = g.distance(i, j)
+            if not dist[d]:
+                dist[d] = _coord(g.coords[i]) + " -- " + _coord(g.coords[j])
+    moms = [_coord(k) for k in g.momenta()]
+    return sites, dist, moms
+
+
 def write_xml(result: dict, path: str, params: dict | None = None) -> None:
-    """The spectrum in the reference's XML elements (diag.hpp:127-140, sparsediag.h:80-88)."""
+    """The spectrum and the eigenstate measurements in the reference's XML elements: AVERAGES with the
+    ground-state energy and gap (sparsediag.h:78-88), EIGENVALUES per sector, and EIGENSTATES per sector
+    with each eigenstate's measurements, "Energy" included (DiagTask::write_xml_body,
+    src/alps/scheduler/diag.hpp:127-160; EigenvectorMeasurements::write_xml_one_vector,
+    src/alps/scheduler/measurement_operators.h:209-266: averages, local values, correlations and
+    structure factors, each group in name order, indexed by site, distance and momentum labels)."""
+    params = params or {}
     lines = ["<?xml version=\"1.0\" encoding=\"UTF-8\"?>", "<SIMULATION>"]
     if params:
         lines.append("  <PARAMETERS>")
@@ -124,17 +155,44 @@ def write_xml(result: dict, path: str, params: dict | None = None) -> None:
     lines.append("  <AVERAGES>")
     if result["ground_state_energy"] is not None:
         lines.append("    <SCALAR_AVERAGE name=\"Ground State Energy\"><MEAN>"
-                     f"{result['ground_state_energy']!r}</MEAN></SCALAR_AVERAGE>")
+                     f"{_num(result['ground_state_energy'])}</MEAN></SCALAR_AVERAGE>")
     if result["energy_gap"] is not None:
-        lines.append(f"    <SCALAR_AVERAGE name=\"Energy Gap\"><MEAN>{result['energy_gap']!r}</MEAN></SCALAR_AVERAGE>")
+        lines.append(f"    <SCALAR_AVERAGE name=\"Energy Gap\"><MEAN>{_num(result['energy_gap'])}</MEAN></SCALAR_AVERAGE>")
     lines.append("  </AVERAGES>")
+
+    def qn_lines(s):
+        return [f"    <QUANTUMNUMBER name=\"{escape(name)}\" value=\"{escape(value)}\"/>"
+                for name, value in s["quantumnumbers"]]
+
     for s in result["sectors"]:
         ev = s["energies"]
         lines.append(f"  <EIGENVALUES number=\"{ev.size}\">")
-        for name, value in s["quantumnumbers"]:
-            lines.append(f"    <QUANTUMNUMBER name=\"{escape(name)}\" value=\"{escape(value)}\"/>")
-        lines += [f"{float(e)!r}" for e in ev]
+        lines += qn_lines(s)
+        lines += [_num(e) for e in ev]
         lines.append("  </EIGENVALUES>")
+    measuring = any(_measure.requests(params).values())
+    if measuring or str(params.get("MEASURE_ENERGY", "true")).lower() not in ("false", "0"):
+        labels = _labels(params) if measuring else None
+        for s in result["sectors"]:
+            ev = s["energies"]
+            lines.append(f"  <EIGENSTATES number=\"{ev.size}\">")
+            lines += qn_lines(s)
+            for j in range(ev.size):
+                lines.append(f"    <EIGENSTATE number=\"{j}\">")
+                m = s["measurements"][j] if "measurements" in s else {}
+                avg = dict(m.get("average", {}), Energy=float(ev[j]))
+                for name in sorted(avg):
+                    lines.append(f"      <SCALAR_AVERAGE name=\"{escape(name)}\"><MEAN>{_num(avg[name])}</MEAN>"
+                                 "</SCALAR_AVERAGE>")
+                for group, lab in (("local", 0), ("correlations", 1), ("structure_factor", 2)):
+                    for name in sorted(m.get(group, {})):
+                        lines.append(f"      <VECTOR_AVERAGE name=\"{escape(name)}\">")
+                        for idx, v in zip(labels[lab], m[group][name]):
+                            lines.append(f"        <SCALAR_AVERAGE indexvalue=\"{escape(idx)}\"><MEAN>{_num(v)}</MEAN>"
+                                         "</SCALAR_AVERAGE>")
+                        lines.append("      </VECTOR_AVERAGE>")
+                lines.append("    </EIGENSTATE>")
+            lines.append("  </EIGENSTATES>")
     lines.append("</SIMULATION>")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")

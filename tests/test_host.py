@@ -220,3 +220,36 @@ def test_lattice_momenta_and_translations_match_oracle(lat, geo):
 def test_total_momentum_needs_one_component_per_periodic_direction():
     with pytest.raises(ed.AEDError, match="TOTAL_MOMENTUM"):
         ed.lattice_momenta('MODEL="spin"\nLATTICE="square lattice"\nL=3\nTOTAL_MOMENTUM="0"\nSz_total=0\n')
+
+
+def test_sparsediag_xml_eigenstates_with_measurements(tmp_path):
+    """write_xml: EIGENVALUES and EIGENSTATES per sector, each eigenstate's SCALAR_AVERAGEs in name order
+    with Energy, VECTOR_AVERAGEs indexed by site / distance / momentum labels (DiagTask::write_xml_body,
+    write_xml_one_vector), numbers with 17 significant digits."""
+    import xml.etree.ElementTree as ET
+    from alps_b200 import sparsediag
+    p = {"MODEL": "spin", "LATTICE": "square lattice", "L": 2, "W": 3, "J": 1,
+         "MEASURE_AVERAGE[Magnetization]": "Sz", "MEASURE_LOCAL[Local magnetization]": "Sz",
+         "MEASURE_CORRELATIONS[Diagonal spin correlations]": "Sz",
+         "MEASURE_STRUCTURE_FACTOR[Structure Factor S]": "Sz"}
+    meas = {"average": {"Magnetization": 0.1}, "local": {"Local magnetization": list(np.arange(6) * 0.5)},
+            "correlations": {"Diagonal spin correlations": list(np.arange(6) * 0.25)},
+            "structure_factor": {"Structure Factor S": list(np.arange(6) * 1.0)}}
+    res = {"ground_state_energy": -1.0, "energy_gap": 0.5,
+           "sectors": [{"quantumnumbers": [("Sz", "0")], "energies": np.array([-1.0, 0.1]),
+                        "measurements": [meas, meas]}]}
+    out = tmp_path / "s.xml"
+    sparsediag.write_xml(res, str(out), p)
+    root = ET.parse(out).getroot()
+    st = root.findall("EIGENSTATES")
+    assert len(st) == 1 and st[0].get("number") == "2"
+    e1 = st[0].findall("EIGENSTATE")[1]
+    assert [a.get("name") for a in e1.findall("SCALAR_AVERAGE")] == ["Energy", "Magnetization"]
+    assert e1.findall("SCALAR_AVERAGE")[0].find("MEAN").text == "0.10000000000000001"
+    va = {v.get("name"): v for v in e1.findall("VECTOR_AVERAGE")}
+    assert [s.get("indexvalue") for s in va["Local magnetization"]] == \
+        ["( 0,0 )", "( 0,1 )", "( 0,2 )", "( 1,0 )", "( 1,1 )", "( 1,2 )"]
+    assert [s.get("indexvalue") for s in va["Diagonal spin correlations"]][:3] == \
+        ["( 0,0 ) -- ( 0,0 )", "( 0,0 ) -- ( 0,1 )", "( 0,0 ) -- ( 0,2 )"]
+    assert [s.get("indexvalue") for s in va["Structure Factor S"]][:4] == \
+        ["( 0,0 )", "( 0,2.0944 )", "( 0,-2.0944 )", "( 3.14159,0 )"]
