@@ -66,7 +66,7 @@ class ParamInfo(ctypes.Structure):
     _fields_ = [
         ("n_sites", ctypes.c_int32), ("n_up", ctypes.c_int32), ("n_bonds", ctypes.c_int32),
         ("number_eigenvalues", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
-        ("has_site_terms", ctypes.c_int32),
+        ("has_site_terms", ctypes.c_int32), ("two_s", ctypes.c_int32),
     ]
 
 
@@ -132,6 +132,9 @@ def lib():
             "aed_create_momentum": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.POINTER(Translations),
                                                    ctypes.c_int, ctypes.POINTER(_P)]),
             "aed_momentum_basis": (ctypes.c_int, [_P, _U32P, _DP, _I64, _I64]),
+            "aed_create_spin": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int32, ctypes.c_int,
+                                               ctypes.POINTER(_P)]),
+            "aed_spin_basis": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _I64, _I64]),
             "aed_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
             "aed_momentum_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
             "aed_lattice_geometry": (ctypes.c_int, [ctypes.c_char_p, _I32P, _I32P, _I32P]),
@@ -244,7 +247,7 @@ def parse_parameters(text: str):
                                       s2.ctypes.data_as(_I32P), _dp(jz), _dp(jxy), _dp(kq), _dp(sh), _dp(sd), nb, ns))
     bonds = [(int(s1[b]), int(s2[b]), float(jz[b]), float(jxy[b]), float(kq[b])) for b in range(nb)]
     return {"n_sites": ns, "n_up": info.n_up, "bonds": bonds, "nev": info.number_eigenvalues,
-            "max_iter": info.max_iterations,
+            "max_iter": info.max_iterations, "two_s": info.two_s,
             "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
 
 
@@ -332,7 +335,8 @@ class Hamiltonian:
     (phase, site map), the identity first, as lattice_translations returns) one momentum sector of it,
     whose vectors are complex."""
 
-    def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None, translations=None):
+    def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None, translations=None,
+                 two_s=1, generic=False):
         self.n_sites, self.n_up = int(n_sites), int(n_up)
         self.bonds = [tuple(b) for b in bonds]
         self.precision = precision
@@ -349,7 +353,15 @@ class Hamiltonian:
         h = _P()
         self._h = None
         self.momentum = translations is not None
-        if self.momentum:
+        self.two_s = int(two_s)
+        self.spin_s = self.two_s != 1 or generic  # the spin-S engine (aed_create_spin)
+        if self.spin_s:
+            if self.momentum:
+                raise AEDError(ERR_INVALID, "momentum sectors: local spin 1/2 only")
+            if precision != FP64:
+                raise AEDError(ERR_INVALID, "spin-S sectors are FP64")
+            _check(lib().aed_create_spin(ctypes.byref(desc), self.two_s, device, ctypes.byref(h)))
+        elif self.momentum:
             if precision != FP64:
                 raise AEDError(ERR_INVALID, "momentum sectors are FP64")
             self._tmap = np.ascontiguousarray([m for _, m in translations], dtype=np.int32).reshape(-1)
@@ -402,7 +414,8 @@ class Hamiltonian:
                 raise AEDError(ERR_INVALID, "the parameters loop over momenta: give TOTAL_MOMENTUM (one sector per "
                                             "handle; alps_b200.sparsediag loops over them) or TRANSLATION_SYMMETRY=false")
             trans = lattice_translations(params, ks[0])
-        ham = cls(m["n_sites"], m["n_up"], m["bonds"], precision, device, m["site_h"], m["site_d"], translations=trans)
+        ham = cls(m["n_sites"], m["n_up"], m["bonds"], precision, device, m["site_h"], m["site_d"], translations=trans,
+                  two_s=m["two_s"])
         ham.params = m
         ham.total_momentum = ks[0] if ks else None
         return ham
@@ -428,6 +441,10 @@ class Hamiltonian:
     # -- basis ---------------------------------------------------------------
     def basis(self, offset=0, count=None):
         count = self.dim - offset if count is None else count
+        if self.spin_s:  # packed digits, 64-bit (aed_spin_basis)
+            out = np.empty(count, np.uint64)
+            _check(lib().aed_spin_basis(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), offset, count))
+            return out
         out = np.empty(count, np.uint32)
         _check(lib().aed_basis_copy(self._h, out.ctypes.data_as(_U32P), offset, count))
         return out

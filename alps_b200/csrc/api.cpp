@@ -143,9 +143,12 @@ void release(aed_handle* h) {
   for (void* p : {(void*)h->d_thi, (void*)h->d_tlo, (void*)h->d_lolist, (void*)h->d_looff, (void*)h->d_tile_h,
                   (void*)h->d_tile_r, (void*)h->d_blk_h, (void*)h->d_tfirst, (void*)h->d_dg, (void*)h->d_ell,
                   (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64,
-                  (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map})
+                  (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map, (void*)h->d_sthi,
+                  (void*)h->d_stlo, (void*)h->d_slolist, (void*)h->d_slooff, (void*)h->d_sblk_hi,
+                  (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r})
     mem_dev_free(p, h->stream);
   delete h->mp;
+  delete h->sp;
   mem_host_free(h->h_scal);
   if (h->stream) {
     cudaStreamSynchronize(h->stream);  // the frees are done: the memory is back in the pool
@@ -342,12 +345,13 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
 }  // namespace
 
 int handle_tune(aed_handle* h, bool f32, const void* x, void* y) {
-  if (h->mom) return AED_OK;  // one momentum kernel
+  if (h->mom || h->gen) return AED_OK;  // one kernel
   int& v = h->hv_var[f32 ? 1 : 0];
   return v < 0 ? pick_variant(h, f32, x, y, &v) : AED_OK;
 }
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+  if (h->gen) return launch_spin_hv(*h->sp, h->sdev, (const double*)x, (double*)y, alpha_part, h->stream);
   if (h->mom)
     return launch_mom_hv(*h->mp, h->dt, h->mom_tables(), (const double*)x, (double*)y, alpha_part, h->stream);
   const int rc = handle_tune(h, f32, x, y);
@@ -616,7 +620,7 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
     return fail(AED_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
   }
   DevTables& t = h->dt;
-  std::memset(&t, 0, sizeof t);
+  t = DevTables{};
   t.thi = h->d_thi;
   t.tlo = h->d_tlo;
   t.lolist = h->d_lolist;
@@ -639,6 +643,133 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
   }
   *out = h;
   return AED_OK;
+}
+
+namespace {
+
+// Site terms and bonds of a spin-S handle's parameters.
+void spin_couplings(const Model& m, SpinParams& p) {
+  p.N = m.N;
+  p.n_bonds = (int)m.s1.size();
+  for (int i = 0; i < m.N; ++i) {
+    p.site_h[i] = m.site_h.empty() ? 0.0 : m.site_h[i];
+    p.site_d[i] = m.site_d.empty() ? 0.0 : m.site_d[i];
+  }
+  for (int b = 0; b < p.n_bonds; ++b) {
+    p.s1[b] = m.s1[b];
+    p.s2[b] = m.s2[b];
+    p.jz[b] = m.jz[b];
+    p.jxy[b] = m.jxy[b];
+    p.kq[b] = m.kq[b];
+  }
+}
+
+}  // namespace
+
+int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_handle** out) {
+  if (!out || !model) return fail(AED_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AED_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(AED_ERR_INVALID, "device index out of range");
+  if (two_s < 1 || two_s + 1 > kSpinMaxDim) return fail(AED_ERR_INVALID, "two_s must be in 1..4 (S = 1/2 .. 2)");
+  aed_model_desc md = *model;
+  md.n_up = 0;  // the digit sum is checked against the sector below
+  DeviceGuard g(device);
+  aed_handle* h = new aed_handle;
+  h->device = device;
+  h->precision = AED_FP64;
+  h->gen = true;
+  h->two_s = two_s;
+  int rc = model_from_desc(&md, h->model);
+  if (rc) {
+    release(h);
+    return rc;
+  }
+  h->model.n_up = model->n_up;
+  SpinTables tb;
+  if ((rc = build_spin_tables(h->model.N, two_s, model->n_up, tb))) {
+    release(h);
+    return rc;
+  }
+  h->sp = new SpinParams();
+  spin_couplings(h->model, *h->sp);
+  spin_transitions(two_s, *h->sp);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    release(h);
+    return fail(AED_ERR_CUDA, "stream creation failed");
+  }
+  struct Up {
+    uint32_t** d;
+    const std::vector<uint32_t>* v;
+  } ups[] = {{&h->d_sthi, &tb.thi},         {&h->d_stlo, &tb.tlo},         {&h->d_slolist, &tb.lolist},
+             {&h->d_slooff, &tb.looff},     {&h->d_sblk_hi, &tb.blk_hi},   {&h->d_sblk_off, &tb.blk_off},
+             {&h->d_stile_blk, &tb.tile_blk}, {&h->d_stile_r, &tb.tile_r}};
+  for (auto& u : ups) {
+    if ((rc = mem_dev_alloc_n(u.d, u.v->size() + 1))) {
+      release(h);
+      return rc;
+    }
+    if (!u.v->empty())
+      cudaMemcpyAsync(*u.d, u.v->data(), u.v->size() * 4, cudaMemcpyHostToDevice, h->stream);
+  }
+  const int64_t D = tb.D;
+  void* hs = nullptr;
+  if ((rc = mem_dev_alloc_n(&h->d_partA, tb.tile_blk.size() + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_partB, (size_t)red_chunks(D) + 1)) || (rc = mem_dev_alloc_n(&h->d_scal, 8)) ||
+      (rc = mem_host_alloc(&hs, 8 * sizeof(double)))) {
+    release(h);
+    return rc;
+  }
+  h->h_scal = static_cast<double*>(hs);
+  const cudaError_t e = cudaStreamSynchronize(h->stream);  // host tables go out of scope
+  if (e != cudaSuccess) {
+    release(h);
+    return fail(AED_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
+  }
+  SpinDev& t = h->sdev;
+  t.thi = h->d_sthi;
+  t.tlo = h->d_stlo;
+  t.lolist = h->d_slolist;
+  t.looff = h->d_slooff;
+  t.blk_hi = h->d_sblk_hi;
+  t.blk_off = h->d_sblk_off;
+  t.tile_blk = h->d_stile_blk;
+  t.tile_r = h->d_stile_r;
+  t.D = D;
+  t.n_blk = (int64_t)tb.blk_hi.size();
+  t.n_tiles = (int64_t)tb.tile_blk.size();
+  t.N = tb.N;
+  t.bits = tb.bits;
+  t.Nl = tb.Nl;
+  t.d = tb.d;
+  t.T = tb.T;
+  h->dim = h->vlen = D;
+  *out = h;
+  return AED_OK;
+}
+
+int aed_spin_basis(aed_handle* h, uint64_t* states, int64_t offset, int64_t count) {
+  if (!h || (!states && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
+  if (!h->gen) return fail(AED_ERR_INVALID, "aed_spin_basis: not a spin-S sector (aed_create_spin)");
+  if (offset < 0 || count < 0 || offset + count > h->dim) return fail(AED_ERR_INVALID, "range outside the basis");
+  if (count == 0) return AED_OK;
+  DeviceGuard g(h->device);
+  uint64_t* d = nullptr;
+  int rc = mem_dev_alloc_n(&d, (size_t)count);
+  if (rc) return rc;
+  rc = launch_spin_basis(h->sdev, d, offset, count, h->stream);
+  if (!rc) {
+    cudaMemcpyAsync(states, d, (size_t)count * 8, cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(AED_ERR_CUDA, std::string("basis copy: ") + cudaGetErrorString(e));
+  }
+  mem_dev_free(d, h->stream);
+  return rc;
 }
 
 int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count) {
@@ -737,6 +868,7 @@ int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, con
   if (!h || !psi || (n > 0 && (!site_i || !out || (kind != AED_OBS_SZ && !site_j))))
     return fail(AED_ERR_INVALID, "NULL argument");
   if (h->mom) return fail(AED_ERR_INVALID, "aed_expectation: Sz sectors only (aed_momentum_expectation)");
+  if (h->gen) return fail(AED_ERR_INVALID, "aed_expectation: spin-1/2 sectors only");
   if (kind < AED_OBS_SZ || kind > AED_OBS_SPSM) return fail(AED_ERR_INVALID, "unknown observable kind");
   const int N = h->model.N;
   for (int p = 0; p < n; ++p)
@@ -765,8 +897,11 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   if (model->n_sites != h->model.N || model->n_up != h->model.n_up)
     return fail(AED_ERR_INVALID, "aed_set_couplings: the sector (n_sites, n_up) must stay the same");
   Model m;
-  int rc = model_from_desc(model, m);
+  aed_model_desc md = *model;
+  if (h->gen) md.n_up = 0;  // a spin-S digit sum may exceed n_sites
+  int rc = model_from_desc(&md, m);
   if (rc) return rc;
+  m.n_up = model->n_up;
   HvParams P;
   if ((rc = build_hv_params(m, h->tab.Nlo, P))) return rc;
   DeviceGuard g(h->device);
@@ -778,6 +913,10 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   h->last_beta.clear();
   h->rec_m = 0;
   h->rec_live = false;
+  if (h->gen) {  // same sector: new site terms and bonds
+    spin_couplings(h->model, *h->sp);
+    return AED_OK;
+  }
   if (h->mom) {  // same basis and translations: new flip list and diagonal
     mom_flips(h->model, *h->mp);
     if ((rc = launch_mom_diag(h->P, h->d_reps, h->dim, h->d_mdiag, h->stream))) return rc;
@@ -821,6 +960,7 @@ int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t co
   if (count == 0) return AED_OK;
   DeviceGuard g(h->device);
   if (h->mom) return aed_momentum_basis(h, host_out, nullptr, offset, count);
+  if (h->gen) return fail(AED_ERR_INVALID, "aed_basis_copy: spin-S states are 64-bit (aed_spin_basis)");
   uint32_t* d = nullptr;
   int rc = dev_alloc(&d, (size_t)count);
   if (rc) return rc;
@@ -836,7 +976,7 @@ int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t co
 
 int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t* host_idx) {
   if (!h || ((!host_states || !host_idx) && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
-  if (h->mom) return fail(AED_ERR_INVALID, "aed_index: not available for momentum sectors");
+  if (h->mom || h->gen) return fail(AED_ERR_INVALID, "aed_index: spin-1/2 Sz sectors only");
   if (count <= 0) return AED_OK;
   DeviceGuard g(h->device);
   uint32_t* ds = nullptr;

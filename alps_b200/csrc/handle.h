@@ -8,6 +8,7 @@
 #include "aed_internal.h"
 #include "kernels.cuh"
 #include "momentum.cuh"
+#include "spin.cuh"
 
 struct aed_handle {
   int device = 0;
@@ -48,8 +49,15 @@ struct aed_handle {
   double* d_mdiag = nullptr;
   uint32_t* d_map = nullptr;
   aed::MomTables mom_tables() const { return {d_reps, d_norm, d_mdiag, d_map, dim}; }
-  // <x, y> partials of one apply (tiles of the real apply, or of the momentum apply)
-  int64_t alpha_tiles() const { return mom ? aed::mom_tiles(dim) : dt.n_tiles; }
+  // spin-S sector (aed_create_spin): tables of spin.cuh
+  bool gen = false;
+  aed::SpinParams* sp = nullptr;
+  aed::SpinDev sdev{};
+  int two_s = 1;
+  uint32_t *d_sthi = nullptr, *d_stlo = nullptr, *d_slolist = nullptr, *d_slooff = nullptr;
+  uint32_t *d_sblk_hi = nullptr, *d_sblk_off = nullptr, *d_stile_blk = nullptr, *d_stile_r = nullptr;
+  // <x, y> partials of one apply (tiles of the real apply, the momentum apply or the spin-S apply)
+  int64_t alpha_tiles() const { return mom ? aed::mom_tiles(dim) : gen ? sdev.n_tiles : dt.n_tiles; }
   // solve workspaces, kept between solves (grown on demand, so that a solve
   // makes no allocation once the handle is warm): slot 0 = the three FP64
   // recurrence vectors, slot 1 = device alpha/beta pairs and Ritz coefficients

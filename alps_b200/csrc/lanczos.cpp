@@ -516,14 +516,14 @@ int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
   int rc = AED_OK;
   if (D == 0) {
     r->converged = 1;
-  } else if (D == 1 && h->mom) {  // M(0,0) = Re (M e_0)_0: the diagonal terms and the flips back into the orbit
+  } else if (D == 1 && (h->mom || h->gen)) {  // M(0,0) = Re (M e_0)_0 (a momentum sector: flips back into the orbit)
     void* w = nullptr;
     if ((rc = handle_workspace(h, 0, 64, &w))) return rc;
     double* x = (double*)w;
     double* y = x + 2;
     const double one[2] = {1.0, 0.0};
     double out[2] = {0.0, 0.0};
-    AED_CUDA_TRY(cudaMemcpyAsync(x, one, 16, cudaMemcpyHostToDevice, h->stream));
+    AED_CUDA_TRY(cudaMemcpyAsync(x, one, h->mom ? 16 : 8, cudaMemcpyHostToDevice, h->stream));
     if ((rc = handle_hv(h, false, x, y, nullptr))) return rc;
     AED_CUDA_TRY(cudaMemcpyAsync(out, y, 16, cudaMemcpyDeviceToHost, h->stream));
     AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -577,7 +577,7 @@ int host_norm(aed_handle* h, const double* v, double* out) {
 
 // FNV-1a of the model (sector and couplings): a saved recurrence only loads
 // into a handle of the same Hamiltonian.
-uint64_t model_hash(const Model& m, const MomParams* mp) {
+uint64_t model_hash(const Model& m, const MomParams* mp, int two_s) {
   uint64_t x = 1469598103934665603ull;
   auto mix = [&](const void* p, size_t n) {
     const unsigned char* b = (const unsigned char*)p;
@@ -594,6 +594,7 @@ uint64_t model_hash(const Model& m, const MomParams* mp) {
   }
   for (double v : m.site_h) mix(&v, 8);
   for (double v : m.site_d) mix(&v, 8);
+  if (two_s != 1) mix(&two_s, sizeof two_s);
   if (mp) {  // a momentum sector: its translations and phases
     mix(&mp->n_trans, sizeof mp->n_trans);
     for (int t = 0; t < mp->n_trans; ++t) {
@@ -718,7 +719,7 @@ int lanczos_save(aed_handle* h, void* buf, int64_t bytes) {
   hd.N = h->model.N;
   hd.n_up = h->model.n_up;
   hd.m = m;
-  hd.model = model_hash(h->model, h->mp);
+  hd.model = model_hash(h->model, h->mp, h->two_s);
   char* p = (char*)buf;
   std::memcpy(p, &hd, sizeof hd);
   p += sizeof hd;
@@ -740,7 +741,7 @@ int lanczos_load(aed_handle* h, const void* buf, int64_t bytes) {
   StateHeader hd;
   std::memcpy(&hd, buf, sizeof hd);
   if (std::memcmp(hd.magic, kStateMagic, 8) != 0) return fail(AED_ERR_INVALID, "lanczos_load: not a saved recurrence");
-  if (hd.D != h->vlen || hd.N != h->model.N || hd.n_up != h->model.n_up || hd.model != model_hash(h->model, h->mp))
+  if (hd.D != h->vlen || hd.N != h->model.N || hd.n_up != h->model.n_up || hd.model != model_hash(h->model, h->mp, h->two_s))
     return fail(AED_ERR_INVALID, "lanczos_load: the state belongs to a different Hamiltonian");
   const int m = hd.m;
   const int64_t D = hd.D;

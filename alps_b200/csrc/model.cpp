@@ -674,7 +674,10 @@ int parse_parameters(const char* text, ParsedParams& out) {
     };
     const std::string model = str("MODEL", "");
     if (model != "spin") return fail(AED_ERR_INVALID, "MODEL must be \"spin\" (got \"" + model + "\")");
-    if (std::fabs(ev.name("local_S") - 0.5) > 1e-12) return fail(AED_ERR_INVALID, "only local_S=1/2 is supported");
+    const double spin = ev.name("local_S");
+    const int two_s = (int)std::lround(2.0 * spin);
+    if (std::fabs(2.0 * spin - two_s) > 1e-12 || two_s < 1 || two_s > 4)
+      return fail(AED_ERR_INVALID, "local_S must be one of 1/2, 1, 3/2, 2");
     const std::string latname = str("LATTICE", "");
     LatticeSpec L;
     if (!lattice_spec(latname, L)) return fail(AED_ERR_INVALID, "unsupported LATTICE \"" + latname + "\"");
@@ -689,10 +692,11 @@ int parse_parameters(const char* text, ParsedParams& out) {
     if (Lx < 1 || Wy < 1) return fail(AED_ERR_INVALID, "lattice extents must be positive");
     const int N = Lx * Wy;
     if (N < 2 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 2..32");
+    // the sector's digit sum Sz_total + N S (spin 1/2: the number of up spins)
     const double szt = ev.name("Sz_total");
-    const double nup_d = N / 2.0 + szt;
+    const double nup_d = N * two_s / 2.0 + szt;
     const int n_up = (int)std::lround(nup_d);
-    if (std::fabs(nup_d - n_up) > 1e-9 || n_up < 0 || n_up > N)
+    if (std::fabs(nup_d - n_up) > 1e-9 || n_up < 0 || n_up > N * two_s)
       return fail(AED_ERR_INVALID, "Sz_total incompatible with the number of sites");
     // edges: cell by cell (last coordinate fastest), unit-cell edge order,
     // open boundaries drop edges, self-loops are dropped (latticegraph.h:98-136)
@@ -757,6 +761,7 @@ int parse_parameters(const char* text, ParsedParams& out) {
     }
     out.info.n_sites = N;
     out.info.n_up = n_up;
+    out.info.two_s = two_s;
     out.info.n_bonds = (int)out.s1.size();
     out.info.number_eigenvalues = p.has("NUMBER_EIGENVALUES") ? (int)std::lround(ev.name("NUMBER_EIGENVALUES")) : 1;
     out.info.max_iterations = p.has("MAX_ITERATIONS") ? (int)std::lround(ev.name("MAX_ITERATIONS")) : 0;

@@ -1,0 +1,252 @@
+// spin.cu -- Sz sectors of spin-S models (S = 1/2, 1, 3/2, 2): the sector's
+// tables, the rank -> state copy and the apply y = H x.  Layout: spin.cuh.
+//
+// H = sum_i (-h_i Sz_i + D_i Sz_i^2) + sum_bonds (Jz Sz_i Sz_j + Jxy exchange_xy(i,j)
+//     + K biquadratic(i,j)), the spin HAMILTONIAN of lib/xml/models.xml.in:342-373
+// with the site operators of :24-36 (S+ |m> = sqrt(S(S+1) - m(m+1)) |m+1>) and
+// the bond operators of :290-300 (biquadratic = (exchange_xy + Sz Sz)^2).
+// Each row takes its site terms, then its bonds in order; a bond contributes
+// the transitions of its two digits (the diagonal one to M(i,i)).  Rows agree
+// with the reference's explicit matrix to rounding (the local elements come
+// from the operator algebra in another order than the reference's symbolic
+// evaluation); the spin-1/2 engine's bit-exact rows are the handles of
+// aed_create.
+//
+// Reference paths are relative to the ALPS source tree.
+
+#include <cmath>
+#include <vector>
+
+#include "handle.h"
+#include "reduce.cuh"
+#include "spin.cuh"
+
+namespace aed {
+
+int build_spin_tables(int N, int twoS, int T, SpinTables& t) {
+  t = SpinTables();
+  if (twoS < 1 || twoS + 1 > kSpinMaxDim) return fail(AED_ERR_INVALID, "local spin S must be in 1/2 .. 2");
+  const int d = twoS + 1;
+  int bits = 1;
+  while ((1 << bits) < d) ++bits;
+  if (N < 1 || N > kSpinMaxSites || N * bits > 48)
+    return fail(AED_ERR_INVALID, "spin sector: number of sites x bits per site must be at most 48");
+  t.N = N;
+  t.twoS = twoS;
+  t.d = d;
+  t.bits = bits;
+  t.Nl = N / 2;
+  t.Nh = N - t.Nl;
+  t.T = T;
+  const int maxlo = (d - 1) * t.Nl, maxhi = (d - 1) * t.Nh;
+  if (T < 0 || T > maxlo + maxhi) return fail(AED_ERR_INVALID, "Sz_total outside the range of the sites");
+  auto digits_ok_sum = [&](uint32_t code, int n, int* sum) {
+    int s = 0;
+    for (int i = 0; i < n; ++i) {
+      const int v = (int)((code >> (bits * i)) & ((1u << bits) - 1u));
+      if (v >= d) return false;
+      s += v;
+    }
+    *sum = s;
+    return true;
+  };
+  const uint32_t nlo = 1u << (bits * t.Nl), nhi = 1u << (bits * t.Nh);
+  std::vector<uint32_t> count(maxlo + 1, 0);
+  t.tlo.assign(nlo, kSpinNone);
+  std::vector<int> losum(nlo, -1);
+  for (uint32_t c = 0; c < nlo; ++c) {
+    int s;
+    if (digits_ok_sum(c, t.Nl, &s)) {
+      losum[c] = s;
+      t.tlo[c] = count[s]++;
+    }
+  }
+  t.looff.assign(maxlo + 2, 0);
+  for (int k = 0; k <= maxlo; ++k) t.looff[k + 1] = t.looff[k] + count[k];
+  t.lolist.assign(t.looff[maxlo + 1], 0);
+  {
+    std::vector<uint32_t> fill(t.looff.begin(), t.looff.end() - 1);
+    for (uint32_t c = 0; c < nlo; ++c)
+      if (losum[c] >= 0) t.lolist[fill[losum[c]]++] = c;
+  }
+  t.thi.assign(nhi, kSpinNone);
+  uint64_t run = 0;
+  for (uint32_t h = 0; h < nhi; ++h) {
+    int s;
+    if (!digits_ok_sum(h, t.Nh, &s)) continue;
+    const int k = T - s;
+    if (k < 0 || k > maxlo || count[k] == 0) continue;
+    t.thi[h] = (uint32_t)run;
+    t.blk_hi.push_back(h);
+    t.blk_off.push_back((uint32_t)run);
+    for (uint32_t r0 = 0; r0 < count[k]; r0 += kSpinTileRows) {
+      t.tile_blk.push_back((uint32_t)(t.blk_hi.size() - 1));
+      t.tile_r.push_back(r0);
+    }
+    run += count[k];
+    if (run >= 0xffffffffull) return fail(AED_ERR_INVALID, "spin sector larger than 2^32 states");
+  }
+  t.D = (int64_t)run;
+  return AED_OK;
+}
+
+void spin_transitions(int twoS, SpinParams& p) {
+  const int d = twoS + 1;
+  const double S = twoS / 2.0;
+  auto m = [&](int v) { return v - S; };
+  const int n2 = d * d;
+  // two-site matrices on (a, c) -> index a d + c: A = Sz Sz, B = exchange_xy, C = (A + B)^2
+  std::vector<double> A(n2 * n2, 0.0), B(n2 * n2, 0.0), X(n2 * n2, 0.0), C(n2 * n2, 0.0);
+  auto at = [&](std::vector<double>& M, int row, int col) -> double& { return M[(size_t)row * n2 + col]; };
+  for (int a = 0; a < d; ++a)
+    for (int c = 0; c < d; ++c) {
+      const int src = a * d + c;
+      at(A, src, src) = m(a) * m(c);
+      if (a + 1 < d && c - 1 >= 0)  // S+_i S-_j: <m+1|S+|m> <m-1|S-|m>
+        at(B, (a + 1) * d + (c - 1), src) += 0.5 * std::sqrt(S * (S + 1) - m(a) * (m(a) + 1)) *
+                                              std::sqrt(S * (S + 1) - m(c) * (m(c) - 1));
+      if (a - 1 >= 0 && c + 1 < d)  // S-_i S+_j
+        at(B, (a - 1) * d + (c + 1), src) += 0.5 * std::sqrt(S * (S + 1) - m(a) * (m(a) - 1)) *
+                                              std::sqrt(S * (S + 1) - m(c) * (m(c) + 1));
+    }
+  for (int k = 0; k < n2 * n2; ++k) X[k] = A[k] + B[k];
+  for (int r = 0; r < n2; ++r)
+    for (int c = 0; c < n2; ++c) {
+      double s = 0.0;
+      for (int q = 0; q < n2; ++q) s += X[(size_t)r * n2 + q] * X[(size_t)q * n2 + c];
+      C[(size_t)r * n2 + c] = s;
+    }
+  int n = 0;
+  for (int src = 0; src < n2; ++src) {
+    p.tstart[src] = n;
+    for (int dst = 0; dst < n2; ++dst) {  // targets in (a2, c2) order, as the reference loops js1, js2
+      const double a = at(A, dst, src), b = at(B, dst, src), c = at(C, dst, src);
+      if (a == 0.0 && b == 0.0 && c == 0.0) continue;
+      p.trans[n++] = {(uint8_t)(dst / d), (uint8_t)(dst % d), a, b, c};
+    }
+  }
+  p.tstart[n2] = n;
+}
+
+namespace {
+
+constexpr int kSpinThreads = 256;
+
+__device__ __forceinline__ int digit_of(uint64_t s, int site, int N, int bits) {
+  return (int)((s >> (bits * (N - 1 - site))) & ((1u << bits) - 1u));
+}
+
+__global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, int64_t offset, int64_t count) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= count) return;
+  const uint32_t idx = (uint32_t)(offset + n);
+  int64_t lo = 0, hi = t.n_blk - 1;
+  while (lo < hi) {  // the block holding row idx: the last with blk_off <= idx
+    const int64_t mid = lo + (hi - lo + 1) / 2;
+    if (t.blk_off[mid] <= idx)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const uint32_t h = t.blk_hi[lo];
+  int sum = 0;
+  for (int i = 0; i < t.N - t.Nl; ++i) sum += (int)((h >> (t.bits * i)) & ((1u << t.bits) - 1u));
+  const uint32_t r = idx - t.blk_off[lo];
+  out[n] = ((uint64_t)h << (t.bits * t.Nl)) | t.lolist[t.looff[t.T - sum] + r];
+}
+
+__global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_constant__ SpinParams p, const SpinDev t,
+                                                               const double* __restrict__ x, double* __restrict__ y,
+                                                               double* __restrict__ alpha_part) {
+  __shared__ SpinTrans tr[kSpinMaxTrans];
+  __shared__ int ts[kSpinMaxPairs + 1];
+  __shared__ int b1[kMaxBonds], b2[kMaxBonds];
+  __shared__ double bjz[kMaxBonds], bjxy[kMaxBonds], bk[kMaxBonds];
+  __shared__ double sh[kSpinMaxSites], sd[kSpinMaxSites];
+  __shared__ double red[33];
+  const int d = t.d, N = t.N, bits = t.bits;
+  for (int q = threadIdx.x; q <= d * d; q += kSpinThreads) ts[q] = p.tstart[q];
+  for (int q = threadIdx.x; q < p.tstart[d * d]; q += kSpinThreads) tr[q] = p.trans[q];
+  for (int q = threadIdx.x; q < p.n_bonds; q += kSpinThreads) {
+    b1[q] = p.s1[q];
+    b2[q] = p.s2[q];
+    bjz[q] = p.jz[q];
+    bjxy[q] = p.jxy[q];
+    bk[q] = p.kq[q];
+  }
+  for (int q = threadIdx.x; q < N; q += kSpinThreads) {
+    sh[q] = p.site_h[q];
+    sd[q] = p.site_d[q];
+  }
+  __syncthreads();
+  const double S = (d - 1) * 0.5;
+  const int shift = bits * t.Nl;
+  const uint64_t lm = (1ull << shift) - 1ull;
+  for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
+    const uint32_t b = t.tile_blk[it], r0 = t.tile_r[it];
+    const uint32_t h = t.blk_hi[b], base = t.blk_off[b];
+    int sum = 0;
+    for (int i = 0; i < N - t.Nl; ++i) sum += (int)((h >> (bits * i)) & ((1u << bits) - 1u));
+    const uint32_t lbase = t.looff[t.T - sum], rows = t.looff[t.T - sum + 1] - lbase;
+    const uint32_t r1 = rows < r0 + kSpinTileRows ? rows : r0 + kSpinTileRows;
+    double dot = 0.0;
+    for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
+      const uint64_t s = ((uint64_t)h << shift) | t.lolist[lbase + r];
+      const uint32_t row = base + r;
+      double dg = 0.0;
+      for (int i = 0; i < N; ++i) {  // site terms: -h Sz + D Sz^2
+        const double mi = digit_of(s, i, N, bits) - S;
+        dg += -sh[i] * mi + sd[i] * mi * mi;
+      }
+      double off = 0.0;
+      for (int q = 0; q < p.n_bonds; ++q) {
+        const int i = b1[q], j = b2[q];
+        const int a = digit_of(s, i, N, bits), c = digit_of(s, j, N, bits);
+        const int pr = a * d + c;
+        for (int e = ts[pr]; e < ts[pr + 1]; ++e) {
+          const SpinTrans& z = tr[e];
+          const double v = bjz[q] * z.A + bjxy[q] * z.B + bk[q] * z.C;
+          if (z.a2 == a && z.c2 == c) {
+            dg += v;
+          } else {
+            const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
+            const uint64_t s2 = s + (((uint64_t)z.a2) << wi) - (((uint64_t)a) << wi) + (((uint64_t)z.c2) << wj) -
+                                (((uint64_t)c) << wj);
+            const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
+            off = fma(v, __ldg(x + rk), off);
+          }
+        }
+      }
+      const double xi = x[row];
+      const double yi = fma(dg, xi, off);
+      y[row] = yi;
+      dot = fma(xi, yi, dot);
+    }
+    if (alpha_part) {
+      const double tot = block_sum_all<kSpinThreads>(dot, red);
+      if (threadIdx.x == 0) alpha_part[it] = tot;
+    }
+  }
+}
+
+}  // namespace
+
+int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st) {
+  if (count <= 0) return AED_OK;
+  spin_basis_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(t, out, offset, count);
+  return check_launch_counted("spin_basis_kernel");
+}
+
+int launch_spin_hv(const SpinParams& p, const SpinDev& t, const double* x, double* y, double* alpha_part,
+                   cudaStream_t st) {
+  if (t.n_tiles == 0) return AED_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t cap = (int64_t)sms * 8;
+  const int grid = (int)(t.n_tiles < cap ? t.n_tiles : cap);
+  spin_hv_kernel<<<grid, kSpinThreads, 0, st>>>(p, t, x, y, alpha_part);
+  return check_launch_counted("spin_hv_kernel");
+}
+
+}  // namespace aed

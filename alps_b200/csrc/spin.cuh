@@ -1,0 +1,75 @@
+// spin.cuh -- Sz sectors of spin-S models with S >= 1/2: tables and launch wrappers.
+//
+// Site i holds digit v_i = m_i + S in [0, 2S] (the index of its state in the
+// spin site basis, Sz ascending; lib/xml/models.xml.in:24-36), stored in
+// `bits` bits with site 0 most significant, so that integer order of the
+// packed states is the basis order of basis_states::build (odometer, last
+// site fastest; src/alps/model/basisstates.h:175-278).  The sector is the set
+// of states with digit sum T = Sz_total + N S.  Ranks use two tables: the
+// packed state splits into a hi part (the first Nh sites) and a lo part (the
+// last Nl); rank = thi[hi] + tlo[lo], tlo[lo] the rank of lo among lo codes
+// of the same digit sum, thi[hi] the number of sector states with a smaller
+// hi code.  The sector's states come in blocks of one hi code each.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace aed {
+
+constexpr int kSpinMaxSites = 32;
+constexpr int kSpinMaxDim = 5;                     // 2S + 1 <= 5 (S <= 2)
+constexpr int kSpinMaxPairs = kSpinMaxDim * kSpinMaxDim;
+constexpr int kSpinMaxTrans = kSpinMaxPairs * kSpinMaxDim;
+constexpr int kSpinTileRows = 1024;                // rows per <x, y> partial of the apply
+
+// Host tables of one sector.
+struct SpinTables {
+  int N = 0, twoS = 0, d = 0, bits = 0, Nh = 0, Nl = 0, T = 0;
+  int64_t D = 0;
+  std::vector<uint32_t> thi;      // 2^(bits Nh): states before hi code h (kSpinNone: not a digit string)
+  std::vector<uint32_t> tlo;      // 2^(bits Nl): rank of lo among lo codes of its digit sum
+  std::vector<uint32_t> lolist;   // valid lo codes grouped by digit sum, ascending
+  std::vector<uint32_t> looff;    // offsets into lolist per digit sum (max sum + 2 entries)
+  std::vector<uint32_t> blk_hi;   // hi code of every block (ascending = basis order)
+  std::vector<uint32_t> blk_off;  // first row of every block
+  std::vector<uint32_t> tile_blk, tile_r;  // work tiles: (block, first row within it)
+};
+constexpr uint32_t kSpinNone = 0xffffffffu;
+int build_spin_tables(int N, int twoS, int T, SpinTables& t);
+
+struct SpinDev {
+  const uint32_t *thi, *tlo, *lolist, *looff, *blk_hi, *blk_off, *tile_blk, *tile_r;
+  int64_t D, n_blk, n_tiles;
+  int N, bits, Nl, d, T;
+};
+
+// One transition of a bond's pair of digits (a, c) -> (a2, c2) with the
+// element Jz * A + Jxy * B + K * C (A: Sz Sz, B: exchange_xy, C: biquadratic).
+struct SpinTrans {
+  uint8_t a2, c2;
+  double A, B, C;
+};
+
+struct SpinParams {
+  int N, n_bonds;
+  double site_h[kSpinMaxSites], site_d[kSpinMaxSites];
+  int s1[kMaxBonds], s2[kMaxBonds];
+  double jz[kMaxBonds], jxy[kMaxBonds], kq[kMaxBonds];
+  int tstart[kSpinMaxPairs + 1];  // transitions of pair (a, c) = a d + c: [tstart[p], tstart[p+1])
+  SpinTrans trans[kSpinMaxTrans];
+};
+// The local operators of the spin model (models.xml.in:24-36, 282-300): the
+// transitions of Sz Sz, exchange_xy and biquadratic for spin S = twoS / 2.
+void spin_transitions(int twoS, SpinParams& p);
+
+int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st);
+int launch_spin_hv(const SpinParams& p, const SpinDev& t, const double* x, double* y, double* alpha_part,
+                   cudaStream_t st);
+__host__ __device__ inline int64_t spin_tiles_of(const SpinDev& t) { return t.n_tiles; }
+
+}  // namespace aed

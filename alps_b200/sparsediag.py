@@ -55,9 +55,11 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
     sectors = []
     if "Sz_total" in params or "Sz" not in qns:
         sz_values = [None]
-    else:
+    else:  # Sz_total from -N S to N S in steps of 1 (diag.h:142-175)
         n = _site_count(params)
-        sz_values = [Fraction(k, 2) for k in range(-n, n + 1, 2)]
+        two_s = model_from_parameters(dict(params, Sz_total=0 if n % 2 == 0 else 0.5))["two_s"] \
+            if "local_S" in params else 1
+        sz_values = [Fraction(k, 2) for k in range(-n * two_s, n * two_s + 1, 2)]
     momenta = lattice_momenta(params)
     req = _measure.requests(params)
     measuring = any(req.values())
@@ -73,6 +75,8 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
             else:
                 if label_k:
                     qn.append(("TOTAL_MOMENTUM", momentum_label(k)))
+                if mp["two_s"] != 1:
+                    raise AEDError(-1, "momentum sectors: local spin 1/2 only (set TRANSLATION_SYMMETRY=false)")
                 ham = Hamiltonian(mp["n_sites"], mp["n_up"], mp["bonds"], FP64, device, mp["site_h"], mp["site_d"],
                                   translations=lattice_translations(params, k))
             try:

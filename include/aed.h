@@ -71,6 +71,7 @@ typedef struct {
   int32_t number_eigenvalues; /* NUMBER_EIGENVALUES, default 1 (sparsediag.h:110)        */
   int32_t max_iterations;     /* MAX_ITERATIONS, 0 = default min(10 D, 1000) (sparsediag.h:109) */
   int32_t has_site_terms;     /* h or D present                                         */
+  int32_t two_s;              /* 2 local_S (1 .. 4); n_up is then the digit sum Sz_total + N S */
 } aed_param_info;
 
 /* Parse an ALPS parameter file ("KEY = value" lines, ';' or newline separated,
@@ -78,7 +79,8 @@ typedef struct {
  * order.  Supported: MODEL="spin", local_S=1/2, LATTICE in {chain lattice,
  * open chain lattice, nnn chain lattice, nnn open chain lattice, square
  * lattice, open square lattice, anisotropic square lattice, ladder, open
- * ladder} with L/W, couplings J, J0, J1, J', Jz, Jxy, Jz<n>, Jxy<n>, J<n>, K<n>,
+ * ladder} with L/W, local_S in {1/2, 1, 3/2, 2} (info->two_s; aed_create_spin
+ * for local_S > 1/2), couplings J, J0, J1, J', Jz, Jxy, Jz<n>, Jxy<n>, J<n>, K<n>,
  * h, D with the model library's defaults, CONSERVED_QUANTUMNUMBERS containing Sz, Sz_total,
  * NUMBER_EIGENVALUES, MAX_ITERATIONS.  TRANSLATION_SYMMETRY and TOTAL_MOMENTUM
  * select momentum sectors (aed_lattice_momenta); the bond list is the same.
@@ -133,6 +135,22 @@ int aed_momentum_expectation(aed_handle* h, const void* psi, int32_t kind, int32
 /* Lattice of a parameter file: dimension, extents and periodic flags
  * (boundary conditions) of each direction (lib/xml/lattices.xml.in). */
 int aed_lattice_geometry(const char* params, int32_t* dim, int32_t* extent, int32_t* periodic);
+
+/* ---- spin-S sectors ----------------------------------------------------- */
+/* An Sz sector of the spin model with local spin S = two_s / 2 (1/2 .. 2) on
+ * every site: site digits v = m + S in the basis order of basis_states::build
+ * (src/alps/model/basisstates.h:175-278, site 0 most significant, Sz
+ * ascending per site, lib/xml/models.xml.in:24-36); model->n_up is the
+ * digit sum Sz_total + N S (for S = 1/2 the number of up spins).  The
+ * Hamiltonian is the spin HAMILTONIAN of models.xml.in:342-373: site terms
+ * -h Sz + D Sz^2, bonds Jz Sz Sz + Jxy exchange_xy + K biquadratic (:290-300).
+ * FP64; vectors of aed_dimension doubles; aed_solve, aed_eigenvectors and the
+ * vector calls take them.  Replaces hamiltonian_matrix::build for local_S > 1/2
+ * (hamiltonian_matrix.hpp:402-450); the matrix stays implicit. */
+int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_handle** out);
+/* States of rows [offset, offset + count) of a spin-S sector, packed with
+ * ceil(log2(2S+1)) bits per site, site 0 most significant. */
+int aed_spin_basis(aed_handle* h, uint64_t* states, int64_t offset, int64_t count);
 
 /* ---- momentum sectors --------------------------------------------------- */
 /* Translations of a lattice at one momentum k: the identity first. */

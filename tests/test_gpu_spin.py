@@ -1,0 +1,93 @@
+"""Spin-S sectors (local_S = 1/2 .. 2) on the GPU against the oracle's Kronecker-product restatement."""
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as sla
+
+import alps_b200 as ed
+from alps_b200 import sparsediag
+from oracle import lattice
+from oracle import spin as ospin
+
+pytestmark = pytest.mark.gpu
+
+
+def _chain(L, jz=1.0, jxy=1.0, k=0.0):
+    return [(i, (i + 1) % L, jz, jxy, k) for i in range(L)]
+
+
+CASES = [(2, 8, "chain"), (2, 4, "square22"), (3, 6, "chain"), (4, 5, "chain"), (1, 10, "chain")]
+
+
+@pytest.mark.parametrize("two_s,n,kind", CASES, ids=[f"2S={c[0]}-{c[2]}{c[1]}" for c in CASES])
+def test_spin_s_basis_and_hv_match_oracle(two_s, n, kind):
+    """States in the reference's basis order, H x equal to the oracle's sparse H x (1e-12 of sum |H_ij x_j|),
+    random couplings with biquadratic terms, random fields and single-ion anisotropy."""
+    rng = np.random.default_rng(two_s * 100 + n)
+    if kind == "chain":
+        graph = [(i, (i + 1) % n) for i in range(n)]
+    else:
+        _, _, g = lattice.lattice_graph("square lattice", {"L": 2})
+        graph = [(s, t) for s, t, _ in g]
+    bonds = [(s, t, *rng.uniform(0.5, 1.5, 2), rng.uniform(-0.3, 0.3)) for s, t in graph]
+    h = rng.uniform(-0.3, 0.3, n)
+    dd = rng.uniform(-0.5, 0.5, n)
+    for T in sorted({n * two_s // 2, n * two_s // 2 - 1}):
+        ham = ed.Hamiltonian(n, T, bonds, site_h=h, site_d=dd, two_s=two_s, generic=True)
+        ref_states = ospin.packed_states(n, two_s, T)
+        assert ham.dim == len(ref_states)
+        assert np.array_equal(ham.basis(), ref_states)
+        H = ospin.hamiltonian(n, two_s, bonds, h, dd, digit_sum=T)
+        x = rng.normal(size=ham.dim)
+        y = ham.apply(x)
+        bound = 1e-12 * (abs(H) @ np.abs(x)) + 1e-14
+        assert np.all(np.abs(y - H @ x) <= bound)
+        r = ham.solve(nev=2, seed=3)
+        ev = np.linalg.eigvalsh(H.toarray()) if ham.dim < 3000 else sla.eigsh(H, k=4, which="SA")[0]
+        ev = np.sort(ev)
+        distinct = [ev[0]] + [v for v in ev[1:] if v - ev[0] > 1e-8][:1]
+        assert np.allclose(r["evals"][:len(distinct)], distinct[:len(r["evals"])], atol=1e-10)
+        ham.close()
+
+
+def test_spin_half_through_the_spin_s_engine_matches_the_bit_exact_engine():
+    rng = np.random.default_rng(4)
+    n = 12
+    bonds = [(i, (i + 1) % n, 1.0, 1.0, 0.0) for i in range(n)] + [(i, (i + 2) % n, 0.4, 0.4, 0.0) for i in range(n)]
+    h = rng.uniform(-0.2, 0.2, n)
+    a = ed.Hamiltonian(n, 6, bonds, site_h=h)
+    b = ed.Hamiltonian(n, 6, bonds, site_h=h, generic=True)
+    assert np.array_equal(a.basis().astype(np.uint64), b.basis())
+    x = rng.normal(size=a.dim)
+    assert np.allclose(a.apply(x), b.apply(x), rtol=1e-13, atol=1e-13)
+    assert np.allclose(a.solve(nev=2, seed=1)["evals"], b.solve(nev=2, seed=1)["evals"], atol=1e-11)
+    a.close()
+    b.close()
+
+
+def test_aklt_chain_closed_form():
+    """S=1 chain with J = 1, K = 1/3 (the AKLT point, periodic L = 10): ground-state energy -2L/3 exactly,
+    spin-1 dimer: S.S levels -2, -1, 1."""
+    L = 10
+    ham = ed.Hamiltonian(L, L, _chain(L, 1.0, 1.0, 1.0 / 3.0), two_s=2)
+    assert abs(ham.solve(nev=1, seed=2)["evals"][0] + 2 * L / 3) < 1e-10
+    ham.close()
+    levels = []
+    for T in (0, 1, 2):  # Sz_total = -2, -1, 0 of two spin-1 sites
+        d = ed.Hamiltonian(2, T, [(0, 1, 1.0, 1.0, 0.0)], two_s=2)
+        levels += list(d.solve(nev=3, seed=1)["evals"])
+        d.close()
+    assert np.allclose(sorted(set(np.round(levels, 12))), [-2.0, -1.0, 1.0])
+
+
+def test_sparsediag_spin_one_sector_loop():
+    """local_S = 1 in the parameters: sectors Sz_total = -L .. L, each against the oracle's spectrum."""
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": 6, "J": 1, "D": 0.3, "local_S": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz", "TRANSLATION_SYMMETRY": "false", "NUMBER_EIGENVALUES": 1}
+    res = sparsediag.run(p)
+    labels = [s["quantumnumbers"][0][1] for s in res["sectors"]]
+    assert labels == [str(k) for k in range(-6, 7)]
+    for s, T in zip(res["sectors"], range(0, 13)):
+        H = ospin.hamiltonian(6, 2, _chain(6), None, [0.3] * 6, digit_sum=T)
+        e0 = np.linalg.eigvalsh(H.toarray())[0]
+        assert abs(s["energies"][0] - e0) < 1e-10

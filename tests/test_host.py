@@ -114,7 +114,7 @@ def test_parameter_file_syntax_and_defaults():
      "Sz_total"),
     ('MODEL="boson Hubbard"\nLATTICE="chain lattice"\nL=8\n', "MODEL"),
     ('MODEL="spin"\nLATTICE="kagome lattice"\nL=8\n', "LATTICE"),
-    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nlocal_S=1\n', "local_S"),
+    ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nlocal_S=5/2\n', "local_S"),
     ('MODEL="spin"\nLATTICE="chain lattice"\nL=40\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n'
      'TRANSLATION_SYMMETRY=false\n', "sites"),
     ('MODEL="spin"\nLATTICE="chain lattice"\nL=8\nSz_total=0\nCONSERVED_QUANTUMNUMBERS="Sz"\n'
@@ -253,3 +253,13 @@ def test_sparsediag_xml_eigenstates_with_measurements(tmp_path):
         ["( 0,0 ) -- ( 0,0 )", "( 0,0 ) -- ( 0,1 )", "( 0,0 ) -- ( 0,2 )"]
     assert [s.get("indexvalue") for s in va["Structure Factor S"]][:4] == \
         ["( 0,0 )", "( 0,2.0944 )", "( 0,-2.0944 )", "( 3.14159,0 )"]
+
+
+def test_local_spin_parameters():
+    """local_S = 1: two_s = 2 and the sector's digit sum Sz_total + N S."""
+    m = ed.parse_parameters('MODEL="spin"\nLATTICE="chain lattice"\nL=6\nlocal_S=1\nJ=1\n'
+                            'CONSERVED_QUANTUMNUMBERS="Sz"\nSz_total=-2\nTRANSLATION_SYMMETRY=false\n')
+    assert m["two_s"] == 2 and m["n_up"] == 4
+    m = ed.parse_parameters('MODEL="spin"\nLATTICE="chain lattice"\nL=5\nlocal_S=3/2\nJ=1\n'
+                            'CONSERVED_QUANTUMNUMBERS="Sz"\nSz_total=1/2\nTRANSLATION_SYMMETRY=false\n')
+    assert m["two_s"] == 3 and m["n_up"] == 8
