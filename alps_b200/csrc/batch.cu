@@ -195,10 +195,14 @@ __global__ void b_advance(BatchArgs a) {
 }
 
 // End of a graph launch: T-matrix analysis of every stepping instance and the
-// phase rules.  One thread per instance.
+// phase rules.  Two threads per instance: the eigenvalue sweeps of T and of T
+// without its first row and column run side by side (tcore::analyze_t /
+// analyze_t2, the bulk of the work), then the first thread finishes.
 __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= *a.n_inst) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = g >> 1, lane = g & 1;
+  const unsigned pair = 3u << (threadIdx.x & 30);  // the two threads of this instance
+  if (s >= *a.n_inst) return;  // both threads of a pair leave together
   BInst& I = a.inst[s];
   if (I.phase != kPhLow && I.phase != kPhHigh) return;
   const int m = I.j;  // alpha_0 .. alpha_{j-1} are final
@@ -209,10 +213,17 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
   double* work = be + cap;      // 5 cap + 2
   double* z = work + 5 * cap + 2;  // cap
   double* inv = z + cap;         // 6 cap
+  if (lane == 0)
+    for (int q = 0; q < m; ++q) {
+      al[q] = I.ab[2 * q];
+      be[q] = I.ab[2 * q + 1];
+    }
+  __syncwarp(pair);
+  const int info = lane == 0 ? tcore::analyze_t(m, al, be, work) : tcore::analyze_t2(m, al, be, work);
+  const int info2 = __shfl_xor_sync(pair, info, 1);
+  if (lane != 0) return;
   double amax = I.ab[0], bmax = I.ab[1];
   for (int q = 0; q < m; ++q) {
-    al[q] = I.ab[2 * q];
-    be[q] = I.ab[2 * q + 1];
     amax = tcore::dmax(amax, al[q]);
     bmax = tcore::dmax(bmax, be[q]);
   }
@@ -220,9 +231,11 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
   double ev[AED_MAX_NEV + 1], er[AED_MAX_NEV + 1];
   int first[AED_MAX_NEV + 1], mults[AED_MAX_NEV + 1];
   tcore::TResult res;
+  res.count = 0;
   const int want = nev + 1;
-  const bool bad = tcore::analyze(m, al, be, amax, bmax, work, want, ev, er, mults, first, &res,
-                                  I.phase == kPhLow ? kFp32MergeRel : 0.0) != 0;
+  const bool bad = info != 0 || info2 != 0 ||
+                   tcore::analyze_walk(m, be, amax, bmax, work, want, ev, er, mults, first, &res,
+                                       I.phase == kPhLow ? kFp32MergeRel : 0.0) != 0;
   const int cnt = res.count;
   bool conv = !bad && cnt >= nev;
   if (I.phase == kPhLow) {
@@ -424,7 +437,7 @@ int batch_record_step(const BatchArgs& a, cudaStream_t st) {
 int batch_record_check(const BatchArgs& a, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
-  b_check<<<(ni + 31) / 32, 32, 0, st>>>(a);
+  b_check<<<(2 * ni + 31) / 32, 32, 0, st>>>(a);
   b_ritz<<<gchunk, kRedThreads, 0, st>>>(a);
   b_ritz_norm<<<ni, 256, 0, st>>>(a);
   b_ritz_scale<<<gchunk, kRedThreads, 0, st>>>(a);

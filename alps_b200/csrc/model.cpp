@@ -192,7 +192,13 @@ int build_tables(int N, int n_up, BasisTables& t) {
   t = BasisTables();
   t.N = N;
   t.n_up = n_up;
-  t.Nlo = (N + 1) / 2;
+  // lo part: half the sites, but at least 12 (two below N): hi blocks of a few
+  // hundred to a thousand rows, the lo-part flips read from shared memory.
+  // Small sectors with few rows per block paid a per-block overhead (program
+  // compile, staging, barriers) on few rows: 12 made the 512-chain batch
+  // 20-32 % faster than ceil(N/2) (11: 5-12 %, 13: FP64 only) and the
+  // single-instance apply of L = 18-22 up to 25 % faster.
+  t.Nlo = std::max((N + 1) / 2, std::min(12, N - 2));
   t.Nhi = N - t.Nlo;
   if (t.Nlo > 16) return fail(AED_ERR_INVALID, "N too large for 16-bit lo tables");
   const uint32_t nlo = 1u << t.Nlo, nhi = 1u << t.Nhi;

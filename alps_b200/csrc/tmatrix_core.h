@@ -127,22 +127,57 @@ struct TResult {
 // thold_rel * max|eigenvalue| (recurrences run with FP32 vectors, whose copies
 // of a converged eigenvalue differ by FP32 rounding, far above the FP64
 // threshold).  Returns 0 or the eigensolver's failure code.
+// analyze in three parts, so that two threads can run the two eigenvalue
+// sweeps side by side: analyze_t (eigenvalues and last eigenvector row of T),
+// analyze_t2 (eigenvalues of T without its first row and column), both into
+// disjoint parts of scratch, then analyze_walk.
+AED_HD inline int analyze_t(int n, const double* alpha, const double* beta, double* scratch) {
+  if (n < 1) return 0;
+  double* ev = scratch;    // n
+  double* e = ev + n;      // n + 1
+  double* zl = e + n + 1;  // n
+  for (int i = 0; i < n; ++i) ev[i] = alpha[i];
+  for (int i = 0; i <= n; ++i) e[i] = 0.0;
+  for (int i = 0; i + 1 < n; ++i) e[i] = beta[i];
+  return ql(n, ev, e, zl, nullptr);
+}
+
+AED_HD inline int analyze_t2(int n, const double* alpha, const double* beta, double* scratch) {
+  if (n < 2) return 0;
+  double* evg = scratch + 3 * n + 1;  // n
+  double* eg = evg + n;               // n + 1
+  for (int i = 1; i < n; ++i) evg[i - 1] = alpha[i];
+  for (int i = 0; i <= n; ++i) eg[i] = 0.0;
+  for (int i = 1; i + 1 < n; ++i) eg[i - 1] = beta[i];
+  return ql(n - 1, evg, eg, nullptr, nullptr);
+}
+
+AED_HD inline int analyze_walk(int n, const double* beta, double alpha_max, double beta_max, double* scratch,
+                               int cap, double* evals, double* errs, int* mults, int* first, TResult* res,
+                               double thold_rel = 0.0);
+
 AED_HD inline int analyze(int n, const double* alpha, const double* beta, double alpha_max, double beta_max,
                           double* scratch, int cap, double* evals, double* errs, int* mults, int* first,
                           TResult* res, double thold_rel = 0.0) {
   res->count = 0;
   res->thold = res->multol = 0.0;
   if (n < 1) return 0;
-  double* ev = scratch;             // n
-  double* e = ev + n;               // n + 1
-  double* zl = e + n + 1;           // n
-  double* evg = zl + n;             // n
-  double* eg = evg + n;             // n + 1
-  for (int i = 0; i < n; ++i) ev[i] = alpha[i];
-  for (int i = 0; i <= n; ++i) e[i] = 0.0;
-  for (int i = 0; i + 1 < n; ++i) e[i] = beta[i];
-  int info = ql(n, ev, e, zl, nullptr);
+  int info = analyze_t(n, alpha, beta, scratch);
   if (info) return info;
+  info = analyze_t2(n, alpha, beta, scratch);
+  if (info) return info;
+  return analyze_walk(n, beta, alpha_max, beta_max, scratch, cap, evals, errs, mults, first, res, thold_rel);
+}
+
+AED_HD inline int analyze_walk(int n, const double* beta, double alpha_max, double beta_max, double* scratch,
+                               int cap, double* evals, double* errs, int* mults, int* first, TResult* res,
+                               double thold_rel) {
+  res->count = 0;
+  res->thold = res->multol = 0.0;
+  if (n < 1) return 0;
+  double* ev = scratch;             // n
+  double* zl = ev + 2 * n + 1;      // n
+  double* evg = zl + n;             // n
   const double eps = DBL_EPSILON;
   const double error_tol = pow(eps, 2.0 / 3.0);  // tmatrix.h:32
   const double multol = dmax(alpha_max, beta_max) * 2 * eps * (10000 + n);
@@ -151,13 +186,6 @@ AED_HD inline int analyze(int n, const double* alpha, const double* beta, double
   res->thold = thold;
   res->multol = multol;
   const double bl = beta[n - 1];
-  if (n > 1) {
-    for (int i = 1; i < n; ++i) evg[i - 1] = alpha[i];
-    for (int i = 0; i <= n; ++i) eg[i] = 0.0;
-    for (int i = 1; i + 1 < n; ++i) eg[i - 1] = beta[i];
-    info = ql(n - 1, evg, eg, nullptr, nullptr);
-    if (info) return info;
-  }
   // walk the distinct values in ascending order; the ghost test of a simple
   // value only looks at reduced-T eigenvalues from the running index t2 on,
   // so the walk can stop once `cap` non-ghost values are out

@@ -308,7 +308,10 @@ def test_solve_fp64_matches_oracle(name, p, nev):
 
 
 def test_solve_matches_oracle_alpha_beta_start():
-    """Same start vector: the first alpha/beta agree with the oracle's recurrence to rounding."""
+    """Same start vector: the first alpha/beta agree with the oracle's recurrence to rounding.  The
+    partial sums of <x, y> and |w| are grouped differently from the oracle's sequential sums, so the two
+    recurrences part at the rounding level and the stop can come a few iterations apart (the bound:
+    a tenth of the count plus 3); the eigenvalues agree."""
     ham = ed.Hamiltonian.from_parameters(spin_params(LATTICE="chain lattice", L=16, J=1))
     M = _oracle_for(ham.params)
     r = ham.solve(nev=2, seed=123)
@@ -317,7 +320,8 @@ def test_solve_matches_oracle_alpha_beta_start():
     n = 10
     np.testing.assert_allclose(a[:n], o["alpha"][:n], rtol=1e-11)
     np.testing.assert_allclose(b[:n], o["beta"][:n], rtol=1e-10)
-    assert abs(r["iterations"] - o["iterations"]) <= 3
+    assert abs(r["iterations"] - o["iterations"]) <= 0.1 * o["iterations"] + 3
+    np.testing.assert_allclose(r["evals"][:2], o["evals"][:2], rtol=1e-12)
 
 
 def test_solve_deterministic():
