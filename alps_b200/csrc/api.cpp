@@ -546,32 +546,12 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
       seen |= 1u << j;
     }
   }
-  {  // the Bloch basis needs H to commute with every translation (the reference
-     // offers no translations on inhomogeneous lattices, graph_helper.h:585-607)
+  {
     Model m;
-    const int rc0 = model_from_desc(model, m);
+    int rc0 = model_from_desc(model, m);
     if (rc0) return rc0;
-    std::map<std::pair<int, int>, std::tuple<double, double, double>> bond;
-    for (size_t b = 0; b < m.s1.size(); ++b) {
-      auto key = std::minmax(m.s1[b], m.s2[b]);
-      auto& v = bond[{key.first, key.second}];
-      std::get<0>(v) += m.jz[b];
-      std::get<1>(v) += m.jxy[b];
-      std::get<2>(v) += m.kq[b];
-    }
-    for (int t = 1; t < tr->n_trans; ++t) {
-      const int32_t* mp = tr->site_map + (size_t)t * N;
-      for (const auto& e : bond) {
-        auto key = std::minmax(mp[e.first.first], mp[e.first.second]);
-        auto it = bond.find({key.first, key.second});
-        if (it == bond.end() || it->second != e.second)
-          return fail(AED_ERR_INVALID, "the couplings are not invariant under the translations");
-      }
-      for (int i = 0; i < N; ++i)
-        if ((!m.site_h.empty() && m.site_h[mp[i]] != m.site_h[i]) ||
-            (!m.site_d.empty() && m.site_d[mp[i]] != m.site_d[i]))
-          return fail(AED_ERR_INVALID, "the site terms are not invariant under the translations");
-    }
+    std::vector<int> maps(tr->site_map, tr->site_map + (size_t)tr->n_trans * N);
+    if ((rc0 = translation_invariant(m, tr->n_trans, maps.data()))) return rc0;
   }
   DeviceGuard g(device);
   aed_handle* h = new aed_handle;
@@ -646,6 +626,35 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
 }
 
 namespace {
+
+// The Bloch basis needs H to commute with every translation (the reference
+// offers no translations on inhomogeneous lattices, graph_helper.h:585-607).
+// maps: n_trans x N, site i -> maps[t * N + i].
+int translation_invariant(const Model& m, int n_trans, const int* maps) {
+  const int N = m.N;
+  std::map<std::pair<int, int>, std::tuple<double, double, double>> bond;
+  for (size_t b = 0; b < m.s1.size(); ++b) {
+    auto key = std::minmax(m.s1[b], m.s2[b]);
+    auto& v = bond[{key.first, key.second}];
+    std::get<0>(v) += m.jz[b];
+    std::get<1>(v) += m.jxy[b];
+    std::get<2>(v) += m.kq[b];
+  }
+  for (int t = 1; t < n_trans; ++t) {
+    const int* mp = maps + (size_t)t * N;
+    for (const auto& e : bond) {
+      auto key = std::minmax(mp[e.first.first], mp[e.first.second]);
+      auto it = bond.find({key.first, key.second});
+      if (it == bond.end() || it->second != e.second)
+        return fail(AED_ERR_INVALID, "the couplings are not invariant under the translations");
+    }
+    for (int i = 0; i < N; ++i)
+      if ((!m.site_h.empty() && m.site_h[mp[i]] != m.site_h[i]) ||
+          (!m.site_d.empty() && m.site_d[mp[i]] != m.site_d[i]))
+        return fail(AED_ERR_INVALID, "the site terms are not invariant under the translations");
+  }
+  return AED_OK;
+}
 
 // Site terms and bonds of a spin-S handle's parameters.
 void spin_couplings(const Model& m, SpinParams& p) {
@@ -903,7 +912,13 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   if (rc) return rc;
   m.n_up = model->n_up;
   HvParams P;
-  if ((rc = build_hv_params(m, h->tab.Nlo, P))) return rc;
+  if (!h->gen && (rc = build_hv_params(m, h->tab.Nlo, P))) return rc;
+  if (h->mom) {  // the new couplings must keep the translations a symmetry
+    std::vector<int> maps((size_t)h->mp->n_trans * m.N);
+    for (int t = 0; t < h->mp->n_trans; ++t)
+      for (int i = 0; i < m.N; ++i) maps[(size_t)t * m.N + i] = m.N - 1 - h->mp->dst[t][i];
+    if ((rc = translation_invariant(m, h->mp->n_trans, maps.data()))) return rc;
+  }
   DeviceGuard g(h->device);
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // no apply of the old couplings in flight
   h->model = m;
@@ -1215,7 +1230,7 @@ int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t 
   if (reps < 1 || !ms) return fail(AED_ERR_INVALID, "reps must be >= 1 and ms non-NULL");
   if (variant >= hv_num_variants()) return fail(AED_ERR_INVALID, "unknown variant");
   DeviceGuard g(h->device);
-  if (h->mom) {  // one kernel: aed_time_mult with the partials when asked
+  if (h->mom || h->gen) {  // one kernel: aed_time_mult with the partials when asked
     if (variant_used) *variant_used = -1;
     return time_hv(h, x, y, reps, with_alpha ? h->d_partA : nullptr, ms);
   }

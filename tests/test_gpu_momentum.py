@@ -162,3 +162,14 @@ def test_momentum_rejects_couplings_that_break_translations():
     tr = ed.lattice_translations(_params(lat, geo), (0.0,))
     with pytest.raises(ed.AEDError, match="invariant"):
         ed.Hamiltonian(n, n // 2, bonds, translations=tr)
+
+
+def test_momentum_set_couplings_keeps_translation_invariance():
+    lat, geo = "chain lattice", {"L": 8}
+    n, bonds = _bonds(lat, geo, {0: (1.0, 1.0)})
+    ham = ed.Hamiltonian(n, n // 2, bonds, translations=ed.lattice_translations(_params(lat, geo), (0.0,)))
+    bad = list(bonds)
+    bad[2] = (bad[2][0], bad[2][1], 2.0, 2.0, 0.0)
+    with pytest.raises(ed.AEDError, match="invariant"):
+        ham.set_couplings(bad)
+    ham.close()

@@ -91,3 +91,14 @@ def test_sparsediag_spin_one_sector_loop():
         H = ospin.hamiltonian(6, 2, _chain(6), None, [0.3] * 6, digit_sum=T)
         e0 = np.linalg.eigvalsh(H.toarray())[0]
         assert abs(s["energies"][0] - e0) < 1e-10
+
+
+def test_spin_s_set_couplings():
+    """New couplings on a spin-1 handle: the eigenvalues follow (oracle dense spectrum)."""
+    n = 8
+    ham = ed.Hamiltonian(n, n, _chain(n), two_s=2)
+    ham.set_couplings(_chain(n, 1.0, 0.5, 0.2))
+    H = ospin.hamiltonian(n, 2, _chain(n, 1.0, 0.5, 0.2), digit_sum=n)
+    e0 = np.linalg.eigvalsh(H.toarray())[0]
+    assert abs(ham.solve(nev=1, seed=1)["evals"][0] - e0) < 1e-10
+    ham.close()
