@@ -524,6 +524,10 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   return AED_OK;
 }
 
+namespace {
+int translation_invariant(const Model& m, int n_trans, const int* maps);
+}  // namespace
+
 int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out) {
   if (!out || !model || !tr) return fail(AED_ERR_INVALID, "NULL argument");
   *out = nullptr;
