@@ -662,19 +662,7 @@ int translation_invariant(const Model& m, int n_trans, const int* maps) {
 
 // Site terms and bonds of a spin-S handle's parameters.
 void spin_couplings(const Model& m, SpinParams& p) {
-  p.N = m.N;
-  p.n_bonds = (int)m.s1.size();
-  for (int i = 0; i < m.N; ++i) {
-    p.site_h[i] = m.site_h.empty() ? 0.0 : m.site_h[i];
-    p.site_d[i] = m.site_d.empty() ? 0.0 : m.site_d[i];
-  }
-  for (int b = 0; b < p.n_bonds; ++b) {
-    p.s1[b] = m.s1[b];
-    p.s2[b] = m.s2[b];
-    p.jz[b] = m.jz[b];
-    p.jxy[b] = m.jxy[b];
-    p.kq[b] = m.kq[b];
-  }
+  spin_set_couplings(m.s1, m.s2, m.jz, m.jxy, m.kq, m.site_h, m.site_d, m.N, p);
 }
 
 }  // namespace
@@ -709,8 +697,8 @@ int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_
     return rc;
   }
   h->sp = new SpinParams();
-  spin_couplings(h->model, *h->sp);
   spin_transitions(two_s, *h->sp);
+  spin_couplings(h->model, *h->sp);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     release(h);

@@ -90,7 +90,65 @@ int build_spin_tables(int N, int twoS, int T, SpinTables& t) {
   return AED_OK;
 }
 
+void spin_set_couplings(const std::vector<int>& s1, const std::vector<int>& s2, const std::vector<double>& jz,
+                        const std::vector<double>& jxy, const std::vector<double>& kq,
+                        const std::vector<double>& site_h, const std::vector<double>& site_d, int N, SpinParams& p) {
+  p.N = N;
+  p.n_bonds = (int)s1.size();
+  const int d = p.twoS + 1;
+  const double S = p.twoS / 2.0;
+  for (int i = 0; i < N; ++i) {
+    p.site_h[i] = site_h.empty() ? 0.0 : site_h[i];
+    p.site_d[i] = site_d.empty() ? 0.0 : site_d[i];
+    for (int v = 0; v < d; ++v) {
+      const double m = v - S;
+      p.sdiag[i][v] = -p.site_h[i] * m + p.site_d[i] * m * m;
+    }
+  }
+  p.n_cls = 0;
+  bool tab = true;
+  for (int b = 0; b < p.n_bonds; ++b) {
+    p.s1[b] = s1[b];
+    p.s2[b] = s2[b];
+    p.jz[b] = jz[b];
+    p.jxy[b] = jxy[b];
+    p.kq[b] = kq[b];
+    int c = 0;
+    while (c < p.n_cls && !(p.jz[p.cls[c]] == jz[b] && p.jxy[p.cls[c]] == jxy[b] && p.kq[p.cls[c]] == kq[b])) ++c;
+    if (c == p.n_cls) {  // a new class: cls[c] temporarily names its first bond
+      if (p.n_cls == kSpinMaxCls) {
+        tab = false;
+        break;
+      }
+      p.cls[p.n_cls++] = b;
+    }
+  }
+  if (!tab) {
+    for (int b = 0; b < p.n_bonds; ++b) {
+      p.s1[b] = s1[b];
+      p.s2[b] = s2[b];
+      p.jz[b] = jz[b];
+      p.jxy[b] = jxy[b];
+      p.kq[b] = kq[b];
+    }
+    p.n_cls = 0;
+    return;
+  }
+  const int ntr = p.tstart[d * d];
+  int first[kSpinMaxCls];
+  for (int c = 0; c < p.n_cls; ++c) first[c] = p.cls[c];
+  for (int c = 0; c < p.n_cls; ++c)
+    for (int e = 0; e < ntr; ++e)
+      p.cval[c][e] = p.jz[first[c]] * p.trans[e].A + p.jxy[first[c]] * p.trans[e].B + p.kq[first[c]] * p.trans[e].C;
+  for (int b = 0; b < p.n_bonds; ++b) {
+    int c = 0;
+    while (!(p.jz[first[c]] == jz[b] && p.jxy[first[c]] == jxy[b] && p.kq[first[c]] == kq[b])) ++c;
+    p.cls[b] = c;
+  }
+}
+
 void spin_transitions(int twoS, SpinParams& p) {
+  p.twoS = twoS;
   const int d = twoS + 1;
   const double S = twoS / 2.0;
   auto m = [&](int v) { return v - S; };
@@ -158,35 +216,48 @@ __global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, i
 __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_constant__ SpinParams p, const SpinDev t,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ alpha_part) {
-  __shared__ SpinTrans tr[kSpinMaxTrans];
+  __shared__ double cv[kSpinMaxCls * kSpinMaxTrans];  // tabulated elements, or A, B, C of each transition
+  __shared__ uint8_t ta[kSpinMaxTrans], tc[kSpinMaxTrans];
   __shared__ int ts[kSpinMaxPairs + 1];
-  __shared__ int b1[kMaxBonds], b2[kMaxBonds];
-  __shared__ double bjz[kMaxBonds], bjxy[kMaxBonds], bk[kMaxBonds];
-  __shared__ double sh[kSpinMaxSites], sd[kSpinMaxSites];
+  __shared__ int b1[kMaxBonds], b2[kMaxBonds], bc[kMaxBonds];
+  __shared__ double bj[3][kMaxBonds];
+  __shared__ double sdg[kSpinMaxSites * kSpinMaxDim];
   __shared__ double red[33];
   const int d = t.d, N = t.N, bits = t.bits;
+  const int ntr = p.tstart[d * d];
+  const bool tab = p.n_cls > 0;
   for (int q = threadIdx.x; q <= d * d; q += kSpinThreads) ts[q] = p.tstart[q];
-  for (int q = threadIdx.x; q < p.tstart[d * d]; q += kSpinThreads) tr[q] = p.trans[q];
+  for (int q = threadIdx.x; q < ntr; q += kSpinThreads) {
+    ta[q] = p.trans[q].a2;
+    tc[q] = p.trans[q].c2;
+  }
+  if (tab) {
+    for (int q = threadIdx.x; q < p.n_cls * ntr; q += kSpinThreads) cv[q] = p.cval[q / ntr][q % ntr];
+  } else {
+    for (int q = threadIdx.x; q < ntr; q += kSpinThreads) {
+      cv[3 * q] = p.trans[q].A;
+      cv[3 * q + 1] = p.trans[q].B;
+      cv[3 * q + 2] = p.trans[q].C;
+    }
+  }
   for (int q = threadIdx.x; q < p.n_bonds; q += kSpinThreads) {
     b1[q] = p.s1[q];
     b2[q] = p.s2[q];
-    bjz[q] = p.jz[q];
-    bjxy[q] = p.jxy[q];
-    bk[q] = p.kq[q];
+    bc[q] = tab ? p.cls[q] * ntr : 0;
+    bj[0][q] = p.jz[q];
+    bj[1][q] = p.jxy[q];
+    bj[2][q] = p.kq[q];
   }
-  for (int q = threadIdx.x; q < N; q += kSpinThreads) {
-    sh[q] = p.site_h[q];
-    sd[q] = p.site_d[q];
-  }
+  for (int q = threadIdx.x; q < N * d; q += kSpinThreads) sdg[q] = p.sdiag[q / d][q % d];
   __syncthreads();
-  const double S = (d - 1) * 0.5;
   const int shift = bits * t.Nl;
   const uint64_t lm = (1ull << shift) - 1ull;
+  const uint32_t dm = (1u << bits) - 1u;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
     const uint32_t b = t.tile_blk[it], r0 = t.tile_r[it];
     const uint32_t h = t.blk_hi[b], base = t.blk_off[b];
     int sum = 0;
-    for (int i = 0; i < N - t.Nl; ++i) sum += (int)((h >> (bits * i)) & ((1u << bits) - 1u));
+    for (int i = 0; i < N - t.Nl; ++i) sum += (int)((h >> (bits * i)) & dm);
     const uint32_t lbase = t.looff[t.T - sum], rows = t.looff[t.T - sum + 1] - lbase;
     const uint32_t r1 = rows < r0 + kSpinTileRows ? rows : r0 + kSpinTileRows;
     double dot = 0.0;
@@ -194,24 +265,22 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
       const uint64_t s = ((uint64_t)h << shift) | t.lolist[lbase + r];
       const uint32_t row = base + r;
       double dg = 0.0;
-      for (int i = 0; i < N; ++i) {  // site terms: -h Sz + D Sz^2
-        const double mi = digit_of(s, i, N, bits) - S;
-        dg += -sh[i] * mi + sd[i] * mi * mi;
-      }
+      for (int i = 0; i < N; ++i) dg += sdg[i * d + (int)((s >> (bits * (N - 1 - i))) & dm)];  // -h Sz + D Sz^2
       double off = 0.0;
       for (int q = 0; q < p.n_bonds; ++q) {
         const int i = b1[q], j = b2[q];
-        const int a = digit_of(s, i, N, bits), c = digit_of(s, j, N, bits);
+        const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
+        const int a = (int)((s >> wi) & dm), c = (int)((s >> wj) & dm);
         const int pr = a * d + c;
+        const int cb = bc[q];
         for (int e = ts[pr]; e < ts[pr + 1]; ++e) {
-          const SpinTrans& z = tr[e];
-          const double v = bjz[q] * z.A + bjxy[q] * z.B + bk[q] * z.C;
-          if (z.a2 == a && z.c2 == c) {
+          const double v = tab ? cv[cb + e] : bj[0][q] * cv[3 * e] + bj[1][q] * cv[3 * e + 1] + bj[2][q] * cv[3 * e + 2];
+          const int a2 = ta[e], c2 = tc[e];
+          if (a2 == a && c2 == c) {
             dg += v;
           } else {
-            const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
-            const uint64_t s2 = s + (((uint64_t)z.a2) << wi) - (((uint64_t)a) << wi) + (((uint64_t)z.c2) << wj) -
-                                (((uint64_t)c) << wj);
+            const uint64_t s2 = s + ((uint64_t)a2 << wi) - ((uint64_t)a << wi) + ((uint64_t)c2 << wj) -
+                                ((uint64_t)c << wj);
             const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
             off = fma(v, __ldg(x + rk), off);
           }

@@ -55,17 +55,31 @@ struct SpinTrans {
   double A, B, C;
 };
 
+constexpr int kSpinMaxCls = 8;  // coupling classes whose elements are tabulated
+
 struct SpinParams {
-  int N, n_bonds;
+  int N, n_bonds, twoS;
   double site_h[kSpinMaxSites], site_d[kSpinMaxSites];
   int s1[kMaxBonds], s2[kMaxBonds];
   double jz[kMaxBonds], jxy[kMaxBonds], kq[kMaxBonds];
   int tstart[kSpinMaxPairs + 1];  // transitions of pair (a, c) = a d + c: [tstart[p], tstart[p+1])
   SpinTrans trans[kSpinMaxTrans];
+  // bonds with the same (Jz, Jxy, K) share a class; with at most kSpinMaxCls
+  // classes the elements Jz A + Jxy B + K C are tabulated per class (n_cls = 0:
+  // formed per bond in the kernel)
+  int n_cls;
+  int cls[kMaxBonds];
+  double cval[kSpinMaxCls][kSpinMaxTrans];
+  double sdiag[kSpinMaxSites][kSpinMaxDim];  // -h m + D m^2 of every site and digit
 };
 // The local operators of the spin model (models.xml.in:24-36, 282-300): the
 // transitions of Sz Sz, exchange_xy and biquadratic for spin S = twoS / 2.
 void spin_transitions(int twoS, SpinParams& p);
+// Bonds, site terms, coupling classes and their tabulated elements (after
+// spin_transitions).
+void spin_set_couplings(const std::vector<int>& s1, const std::vector<int>& s2, const std::vector<double>& jz,
+                        const std::vector<double>& jxy, const std::vector<double>& kq,
+                        const std::vector<double>& site_h, const std::vector<double>& site_d, int N, SpinParams& p);
 
 int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st);
 int launch_spin_hv(const SpinParams& p, const SpinDev& t, const double* x, double* y, double* alpha_part,

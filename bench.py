@@ -568,6 +568,39 @@ def run_momentum(args):
     print(json.dumps(line))
 
 
+def run_spin(args):
+    """Spin-1 Heisenberg chain L=18, Sz=0 (6,536,382 states), FP64, lowest 2 eigenvalues, through the
+    spin-S engine (local_S = 1); apply roofline from the sampled mean of off-diagonal terms per row."""
+    import alps_b200 as ed
+
+    L = 18
+    bonds = [(i, (i + 1) % L, 1.0, 1.0, 0.0) for i in range(L)]
+    ham = ed.Hamiltonian(L, L, bonds, two_s=2)
+    x, y = ham.new_vector(), ham.new_vector()
+    ham.fill_random(x, 1)
+    ham.time_mult(x, y, 2)
+    ms = ham.time_mult(x, y, 10)
+    states = ham.basis(0, min(ham.dim, 200000))
+    digits = np.array([(states >> np.uint64(2 * (L - 1 - i))) & np.uint64(3) for i in range(L)]).astype(int)
+    a, c = digits, np.roll(digits, -1, axis=0)
+    nbar = float(np.mean(np.sum((a < 2) & (c > 0), axis=0) + np.sum((a > 0) & (c < 2), axis=0)))
+    b_row = 16 + nbar * 8  # x_i, y_i, and one gathered x_j per off-diagonal term
+    peak, peak_kind = read_peaks()
+    ach = ham.dim * b_row / (ms / 1e3) / 1e9
+    t0 = time.perf_counter()
+    r = ham.solve(nev=NEV, seed=1)
+    dt = time.perf_counter() - t0
+    line = {"metric": "spin-1 chain L=18 Sz=0 Lanczos solves/s (FP64, lowest 2)", "value": 1.0 / dt, "unit": "solves/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "spin-1 Heisenberg chain L=18 periodic, J=1, Sz_total=0, D=%d" % ham.dim},
+            "iterations": r["iterations"], "evals": r["evals"].tolist(),
+            "roofline": {"bound": "hbm", "kernel": "spin_hv_kernel", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_kind": peak_kind, "apply_ms": ms,
+                         "algorithmic_bytes_per_row": b_row, "offdiag_per_row_sampled": nbar}}
+    ham.close()
+    print(json.dumps(line))
+
+
 def run_batch(args):
     """Config 4: 512 J1-J2 chains through the batched engine, mixed and FP64, and through the
     single-instance FP64 drop-in one after the other."""
@@ -716,7 +749,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="l28", choices=["l28", "square", "batch", "serve", "momentum"])
+    ap.add_argument("--workload", default="l28", choices=["l28", "square", "batch", "serve", "momentum", "spin"])
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="serve: engine precision")
     ap.add_argument("--steps-per-launch", type=int, default=8)
@@ -727,6 +760,8 @@ def main():
         run_reference(args)
     elif args.workload == "momentum":
         run_momentum(args)
+    elif args.workload == "spin":
+        run_spin(args)
     elif args.workload == "square":
         run_square(args)
     elif args.workload == "batch":
