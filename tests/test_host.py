@@ -263,3 +263,24 @@ def test_local_spin_parameters():
     m = ed.parse_parameters('MODEL="spin"\nLATTICE="chain lattice"\nL=5\nlocal_S=3/2\nJ=1\n'
                             'CONSERVED_QUANTUMNUMBERS="Sz"\nSz_total=1/2\nTRANSLATION_SYMMETRY=false\n')
     assert m["two_s"] == 3 and m["n_up"] == 8
+
+
+@pytest.mark.parametrize("lat,geo", [("chain lattice", {"L": 6}), ("open chain lattice", {"L": 5}),
+                                     ("square lattice", {"L": 3, "W": 4}), ("ladder", {"L": 4}),
+                                     ("anisotropic square lattice", {"L": 2, "W": 3})])
+def test_measurement_geometry_matches_oracle(lat, geo):
+    """Distance classes, their count and the momenta of the measurement code (from the engine's lattice
+    geometry) equal the oracle's restatement of hypercubic_lattice."""
+    from alps_b200 import measure
+    from oracle import measure as om
+    p = dict(geo, LATTICE=lat)
+    g = measure.Geometry(p)
+    ext, per, coords = om._geometry(p)
+    assert g.coords == coords and g.num_distances() == om._num_distances(ext, per)
+    for i in range(g.n):
+        for j in range(g.n):
+            assert g.distance(i, j) == om._distance(ext, per, coords[i], coords[j])
+    ks = []
+    for cc in coords:
+        ks.append([2 * np.pi * ((x - L) if x > L // 2 else x) / L for x, L in zip(cc, ext)])
+    assert np.allclose(g.momenta(), ks)
