@@ -869,7 +869,6 @@ int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, con
   if (!h || !psi || (n > 0 && (!site_i || !out || (kind != AED_OBS_SZ && !site_j))))
     return fail(AED_ERR_INVALID, "NULL argument");
   if (h->mom) return fail(AED_ERR_INVALID, "aed_expectation: Sz sectors only (aed_momentum_expectation)");
-  if (h->gen) return fail(AED_ERR_INVALID, "aed_expectation: spin-1/2 sectors only");
   if (kind < AED_OBS_SZ || kind > AED_OBS_SPSM) return fail(AED_ERR_INVALID, "unknown observable kind");
   const int N = h->model.N;
   for (int p = 0; p < n; ++p)
@@ -877,6 +876,7 @@ int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, con
       return fail(AED_ERR_INVALID, "site index out of range");
   if (n <= 0) return AED_OK;
   DeviceGuard g(h->device);
+  if (h->gen) return spin_measure_pairs(h, static_cast<const double*>(psi), kind, n, site_i, site_j, out);
   return measure_pairs(h, psi, kind, n, site_i, site_j, out);
 }
 

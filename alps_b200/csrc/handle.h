@@ -122,6 +122,9 @@ struct MeasPairs {
   uint32_t mi[kMeasPairs], mj[kMeasPairs];
 };
 int measure_pairs(aed_handle* h, const void* psi, int kind, int n, const int32_t* si, const int32_t* sj, double* out);
+// The same for a spin-S sector (aed_create_spin; FP64 vectors): spin.cu.
+int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
+                       double* out);
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
 // Choose the apply variant for this precision now (timed launches on x, y)

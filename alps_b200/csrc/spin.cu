@@ -14,6 +14,7 @@
 //
 // Reference paths are relative to the ALPS source tree.
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -298,7 +299,130 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
   }
 }
 
+// Expectation values in one vector of the sector (the spin-S counterpart of
+// measure.cu's meas_kernel): per site pair p,
+//   kind SZ     sum_s psi_s^2 m_i(s)
+//   kind SZSZ   sum_s psi_s^2 m_i(s) m_j(s)
+//   kind SPSM   sum_s psi_{s'} psi_s <a+1|S+|a> <c-1|S-|c>, s' = s with digit a of
+//               site i raised and digit c of site j lowered (i = j: the diagonal
+//               S+ S- = S(S+1) - m^2 + m)
+// with S+- the site operators of models.xml.in:24-36.  Rows are walked by the
+// apply's work tiles; each CTA writes one partial sum per pair, which the host
+// adds in order.
+struct SpinMeasArgs {
+  int np;
+  int wi[kMeasPairs], wj[kMeasPairs];  // bit offsets of the digits of sites i and j
+  double m[kSpinMaxDim];               // Sz of each digit
+  double cp[kSpinMaxDim];              // <v+1|S+|v>
+  double cm[kSpinMaxDim];              // <v-1|S-|v>
+};
+
+constexpr int kSpinMeasThreads = 256;
+
+template <int KIND>
+__global__ void __launch_bounds__(kSpinMeasThreads, 1)
+    spin_meas_kernel(const SpinDev t, const double* __restrict__ psi, const __grid_constant__ SpinMeasArgs a,
+                     double* __restrict__ part) {
+  __shared__ double red[33];
+  double acc[kMeasPairs];
+#pragma unroll
+  for (int p = 0; p < kMeasPairs; ++p) acc[p] = 0.0;
+  const int N = t.N, bits = t.bits, d = t.d;
+  const int shift = bits * t.Nl;
+  const uint64_t lm = (1ull << shift) - 1ull;
+  const uint32_t dm = (1u << bits) - 1u;
+  for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
+    const uint32_t b = t.tile_blk[it], r0 = t.tile_r[it];
+    const uint32_t h = t.blk_hi[b], base = t.blk_off[b];
+    int sum = 0;
+    for (int i = 0; i < N - t.Nl; ++i) sum += (int)((h >> (bits * i)) & dm);
+    const uint32_t lbase = t.looff[t.T - sum], rows = t.looff[t.T - sum + 1] - lbase;
+    const uint32_t r1 = rows < r0 + kSpinTileRows ? rows : r0 + kSpinTileRows;
+    for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinMeasThreads) {
+      const uint64_t s = ((uint64_t)h << shift) | t.lolist[lbase + r];
+      const double v = psi[base + r];
+#pragma unroll
+      for (int p = 0; p < kMeasPairs; ++p) {
+        if (p >= a.np) continue;  // (no break: the accumulators stay in registers)
+        const int wi = a.wi[p];
+        const int da = (int)((s >> wi) & dm);
+        if (KIND == kMeasSz) {
+          acc[p] = fma(v * v, a.m[da], acc[p]);
+        } else if (KIND == kMeasSzSz) {
+          const int dc = (int)((s >> a.wj[p]) & dm);
+          acc[p] = fma(v * v, a.m[da] * a.m[dc], acc[p]);
+        } else {
+          const int wj = a.wj[p];
+          if (wi == wj) {
+            acc[p] = fma(v * v, a.cm[da] * a.cm[da], acc[p]);
+          } else {
+            const int dc = (int)((s >> wj) & dm);
+            if (da + 1 < d && dc > 0) {  // s' is a state of the same digit sum: its rank exists
+              const uint64_t s2 = s + (1ull << wi) - (1ull << wj);
+              const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
+              acc[p] = fma(__ldg(psi + rk) * v, a.cp[da] * a.cm[dc], acc[p]);
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < kMeasPairs; ++p) {
+    if (p >= a.np) continue;
+    const double tot = block_sum_all<kSpinMeasThreads>(acc[p], red);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * kMeasPairs + p] = tot;
+  }
+}
+
 }  // namespace
+
+int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
+                       double* out) {
+  const SpinDev& t = h->sdev;
+  if (t.n_tiles == 0) {
+    for (int p = 0; p < n; ++p) out[p] = 0.0;
+    return AED_OK;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<int64_t>(t.n_tiles, (int64_t)sms * 4);
+  void* w = nullptr;
+  int rc = handle_workspace(h, 1, (size_t)grid * kMeasPairs * 8, &w);
+  if (rc) return rc;
+  double* part = static_cast<double*>(w);
+  std::vector<double> hp((size_t)grid * kMeasPairs);
+  SpinMeasArgs a{};
+  const double S = t.d / 2.0 - 0.5;
+  for (int v = 0; v < t.d; ++v) {
+    const double m = v - S;
+    a.m[v] = m;
+    a.cp[v] = v + 1 < t.d ? std::sqrt(S * (S + 1) - m * (m + 1)) : 0.0;
+    a.cm[v] = v > 0 ? std::sqrt(S * (S + 1) - m * (m - 1)) : 0.0;
+  }
+  for (int p0 = 0; p0 < n; p0 += kMeasPairs) {
+    a.np = std::min(kMeasPairs, n - p0);
+    for (int p = 0; p < a.np; ++p) {
+      a.wi[p] = t.bits * (t.N - 1 - si[p0 + p]);
+      a.wj[p] = kind == kMeasSz ? 0 : t.bits * (t.N - 1 - sj[p0 + p]);
+    }
+    switch (kind) {
+      case kMeasSz: spin_meas_kernel<kMeasSz><<<grid, kSpinMeasThreads, 0, h->stream>>>(t, psi, a, part); break;
+      case kMeasSzSz: spin_meas_kernel<kMeasSzSz><<<grid, kSpinMeasThreads, 0, h->stream>>>(t, psi, a, part); break;
+      default: spin_meas_kernel<kMeasSpSm><<<grid, kSpinMeasThreads, 0, h->stream>>>(t, psi, a, part); break;
+    }
+    if ((rc = check_launch_counted("spin_meas_kernel"))) return rc;
+    AED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part, hp.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < a.np; ++p) {
+      double sum = 0.0;
+      for (int b = 0; b < grid; ++b) sum += hp[(size_t)b * kMeasPairs + p];
+      out[p0 + p] = sum;
+    }
+  }
+  return AED_OK;
+}
 
 int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st) {
   if (count <= 0) return AED_OK;

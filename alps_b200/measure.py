@@ -18,9 +18,10 @@ periodic direction (y - x) mod L, per open direction the pair itself), the
 same site giving <a_i b_i>; the structure factor runs over the lattice's
 momenta (hypercubic.h:371-387: cell order, k_d = 2 pi x_d / L_d with
 x_d > L_d / 2 taken as x_d - L_d).  Operators: the spin-1/2 site operators
-Sz, Splus, Sminus.  The expectation values come from aed_expectation (one
-pass over the vector per 32 site pairs, on the GPU); this module only
-chooses the pairs and combines the numbers.
+Sz, Splus, Sminus of the model's local spin (S = 1/2 .. 2, lib/xml/models.xml.in:24-36).
+The expectation values come from aed_expectation (one pass over the vector
+per 32 site pairs, on the GPU); this module only chooses the pairs and
+combines the numbers.
 
 In a momentum sector (translation invariance) perform_measurements skips the
 local values, averages each correlation over all pairs of its distance class
@@ -112,7 +113,7 @@ class Geometry:
 
 def _check_op(op):
     if op not in _SITE_OPS:
-        raise AEDError(ERR_INVALID, f"measurement operator {op!r}: only the spin-1/2 site operators "
+        raise AEDError(ERR_INVALID, f"measurement operator {op!r}: only the spin site operators "
                                     f"{', '.join(_SITE_OPS)} are supported")
 
 
@@ -144,12 +145,15 @@ def _pair_values(ham, psi, a, b, si, sj):
     if (a, b) == ("Splus", "Sminus"):
         return expectation(ham, psi, OBS_SPSM, si, sj)
     if (a, b) == ("Sminus", "Splus"):
-        # S-_i S+_j = S+_j S-_i for i != j; on one site S- S+ is the projector on spin down
+        # S-_i S+_j = S+_j S-_i for i != j; on one site S- S+ = S+ S- - 2 Sz
         v = expectation(ham, psi, OBS_SPSM, sj, si)
         same = si == sj
         if same.any():
-            norm2 = expectation(ham, psi, OBS_SZSZ, si[same], si[same]) * 4.0  # |psi|^2
-            v[same] = norm2 - v[same]
+            if getattr(ham, "two_s", 1) == 1:  # spin 1/2: S- S+ is the projector on spin down
+                norm2 = expectation(ham, psi, OBS_SZSZ, si[same], si[same]) * 4.0  # |psi|^2
+                v[same] = norm2 - v[same]
+            else:
+                v[same] = v[same] - 2.0 * expectation(ham, psi, OBS_SZ, si[same])
         return v
     return np.zeros(si.size)  # the product changes Sz: zero in an Sz sector
 

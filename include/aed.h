@@ -120,8 +120,10 @@ int aed_empty_cache(int device);
  * (site_i[p], site_j[p]) (site_j ignored for AED_OBS_SZ).  The quantities
  * DiagMatrix::perform_measurements evaluates for MEASURE_AVERAGE, _LOCAL,
  * _CORRELATIONS and _STRUCTURE_FACTOR (applications/diag/diag.h:191-314 via
- * calculate(), :316-339), for the spin-1/2 operators Sz, Splus, Sminus.
- * Sz sectors only (not momentum sectors). */
+ * calculate(), :316-339), for the spin operators Sz, Splus, Sminus of the
+ * handle's local spin (spin-1/2 handles of aed_create, spin-S handles of
+ * aed_create_spin; models.xml.in:24-36).  Sz sectors only (not momentum
+ * sectors). */
 int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
                     const int32_t* site_j, double* out);
 /* Momentum sectors: <psi| sum_p O(site_i[p], site_j[p]) |psi> (the real part)

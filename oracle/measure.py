@@ -1,4 +1,4 @@
-"""Oracle restatement of sparsediag's eigenvector measurements for spin-1/2 Sz sectors.
+"""Oracle restatement of sparsediag's eigenvector measurements for spin-S Sz sectors.
 
 TEST INFRASTRUCTURE ONLY: used by tests/ to check alps_b200.measure; the
 engine never imports this module.  Pure Python / numpy on explicit basis
@@ -12,9 +12,10 @@ Restates (paths relative to the ALPS source tree):
                                          applications/diag/diag.h:191-314
   * distance classes                     src/alps/lattice/hypercubic.h:325-349
   * momenta (cell order, x > L/2 -> x - L)  hypercubic.h:371-387
-  * spin-1/2 site operators Sz = diag(-1/2, 1/2), S+ |down> = |up>, S- |up> = |down>
-                                         lib/xml/models.xml.in (spin site basis and operators)
-States are integers with site i at bit n-1-i, up = 1 (the basis order).
+  * spin site operators: Sz |m> = m |m>, S+ |m> = sqrt(S(S+1) - m(m+1)) |m+1>,
+    S- |m> = sqrt(S(S+1) - m(m-1)) |m-1>  lib/xml/models.xml.in:24-36 (spin 1/2: S+ |down> = |up>)
+States are integers with site i at bit n-1-i, up = 1 (the basis order); for
+spin S the digit m + S of site i at bits (n-1-i) b .., b bits per site.
 """
 
 from __future__ import annotations
@@ -72,27 +73,32 @@ def _num_distances(ext, per):
     return int(np.prod([L if p else L * L for L, p in zip(ext, per)]))
 
 
-def _op_apply(op, site, n, s):
-    """op acting on site of state s: (coefficient, new state) or None."""
-    m = 1 << (n - 1 - site)
-    up = (s & m) != 0
+def _op_apply(op, site, n, s, two_s=1):
+    """op acting on site of state s: (coefficient, new state) or None.  Spin S = two_s / 2: the
+    site's digit v = m + S sits at bits (n-1-site) * b .. with b = bits per site (1 for spin 1/2,
+    where v is the up bit); S+ |m> = sqrt(S(S+1) - m(m+1)) |m+1>, S- |m> = sqrt(S(S+1) - m(m-1)) |m-1>."""
+    b = two_s.bit_length()  # enough bits for the digits 0 .. 2S
+    w = b * (n - 1 - site)
+    v = (s >> w) & ((1 << b) - 1)
+    S = two_s / 2.0
+    m = v - S
     if op == "Sz":
-        return (0.5 if up else -0.5), s
+        return m, s
     if op == "Splus":
-        return (1.0, s | m) if not up else None
+        return (math.sqrt(S * (S + 1) - m * (m + 1)), s + (1 << w)) if v < two_s else None
     if op == "Sminus":
-        return (1.0, s & ~m) if up else None
+        return (math.sqrt(S * (S + 1) - m * (m - 1)), s - (1 << w)) if v > 0 else None
     raise ValueError(op)
 
 
-def _expect(states, psi, n, ops):
+def _expect(states, psi, n, ops, two_s=1):
     """<psi| ops[0] ops[1] ... |psi> with ops = [(name, site)], the rightmost acting first."""
     index = {int(s): k for k, s in enumerate(states)}
     tot = 0.0
     for k, s in enumerate(states):
         s, c = int(s), 1.0
         for name, site in reversed(ops):
-            r = _op_apply(name, site, n, s)
+            r = _op_apply(name, site, n, s, two_s)
             if r is None:
                 c = 0.0
                 break
@@ -103,15 +109,21 @@ def _expect(states, psi, n, ops):
     return tot
 
 
-def measure(states, psi, params) -> dict:
+def measure(states, psi, params, two_s=1) -> dict:
+    """The MEASURE_* quantities in the vector psi over the basis `states` (spin S = two_s / 2: states
+    packed as aed_spin_basis lists them)."""
     ext, per, coords = _geometry(params)
     n_sites = len(coords)
     req = requests(params)
+
+    def ex(ops):
+        return _expect(states, psi, n_sites, ops, two_s)
+
     out = {"average": {}, "local": {}, "correlations": {}, "structure_factor": {}}
     for name, op in req["average"].items():
-        out["average"][name] = sum(_expect(states, psi, n_sites, [(op, i)]) for i in range(n_sites)) / n_sites
+        out["average"][name] = sum(ex([(op, i)]) for i in range(n_sites)) / n_sites
     for name, op in req["local"].items():
-        out["local"][name] = [_expect(states, psi, n_sites, [(op, i)]) for i in range(n_sites)]
+        out["local"][name] = [ex([(op, i)]) for i in range(n_sites)]
     nd = _num_distances(ext, per)
     for name, (a, b) in req["correlations"].items():
         row, done = [0.0] * nd, [False] * nd
@@ -119,11 +131,11 @@ def measure(states, psi, params) -> dict:
             for j in range(n_sites):
                 d = _distance(ext, per, coords[i], coords[j])
                 if not done[d]:
-                    row[d] = _expect(states, psi, n_sites, [(a, i), (b, j)])
+                    row[d] = ex([(a, i), (b, j)])
                     done[d] = True
         out["correlations"][name] = row
     for name, (a, b) in req["structure_factor"].items():
-        c = np.array([[_expect(states, psi, n_sites, [(a, i), (b, j)]) for j in range(n_sites)]
+        c = np.array([[ex([(a, i), (b, j)]) for j in range(n_sites)]
                       for i in range(n_sites)])
         ks = []
         for cc in coords:

@@ -90,3 +90,19 @@ def packed_states(n: int, two_s: int, digit_sum: int) -> np.ndarray:
     for i in range(n):
         out |= digits[:, i].astype(np.uint64) << np.uint64(bits * (n - 1 - i))
     return out
+
+
+def pair_expectation(n: int, two_s: int, digit_sum: int, psi, ops) -> float:
+    """<psi| ops[0] ops[1] ... |psi> in the sector of digit sum `digit_sum`, ops = [(name, site)] with
+    name in Sz, Splus, Sminus (Kronecker-product operators over the full space, restricted)."""
+    d = two_s + 1
+    sz, spl, smi = site_ops(two_s)
+    named = {"Sz": sz, "Splus": spl, "Sminus": smi}
+    O = sp.identity(d ** n, format="csr")
+    for name, site in ops:
+        O = O @ _embed(named[name], site, n, d)
+    keep, _ = sector(n, two_s, digit_sum)
+    psi = np.asarray(psi, dtype=float)
+    full = np.zeros(d ** n)
+    full[keep] = psi
+    return float(full @ (O @ full))

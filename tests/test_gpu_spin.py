@@ -102,3 +102,91 @@ def test_spin_s_set_couplings():
     e0 = np.linalg.eigvalsh(H.toarray())[0]
     assert abs(ham.solve(nev=1, seed=1)["evals"][0] - e0) < 1e-10
     ham.close()
+
+
+SPIN_MEAS = {
+    "MEASURE_AVERAGE[Magnetization]": "Sz",
+    "MEASURE_LOCAL[Local magnetization]": "Sz",
+    "MEASURE_CORRELATIONS[Diagonal spin correlations]": "Sz",
+    "MEASURE_CORRELATIONS[Offdiagonal spin correlations]": "Splus:Sminus",
+    "MEASURE_CORRELATIONS[Reverse offdiagonal]": "Sminus:Splus",
+    "MEASURE_STRUCTURE_FACTOR[Structure Factor S]": "Sz",
+    "MEASURE_STRUCTURE_FACTOR[Structure Factor mp]": "Sminus:Splus",
+}
+
+
+@pytest.mark.parametrize("two_s,n", [(2, 8), (3, 6), (4, 5)])
+def test_spin_s_expectation_matches_oracle(two_s, n):
+    """aed_expectation on a spin-S handle: <Sz_i>, <Sz_i Sz_j>, <S+_i S-_j> for every site pair of a random
+    vector equal the oracle's Kronecker-product operators (1e-12 relative)."""
+    from alps_b200 import measure
+    rng = np.random.default_rng(two_s * 7 + n)
+    T = n * two_s // 2 - 1
+    ham = ed.Hamiltonian(n, T, _chain(n), two_s=two_s)
+    psi = rng.normal(size=ham.dim)
+    v = ham.new_vector().upload(psi)
+    si = np.repeat(np.arange(n), n)
+    sj = np.tile(np.arange(n), n)
+    got_z = measure.expectation(ham, v, measure.OBS_SZ, np.arange(n))
+    got_zz = measure.expectation(ham, v, measure.OBS_SZSZ, si, sj)
+    got_pm = measure.expectation(ham, v, measure.OBS_SPSM, si, sj)
+    scale = float(psi @ psi) * (two_s / 2.0 + 1) ** 2
+    for i in range(n):
+        ref = ospin.pair_expectation(n, two_s, T, psi, [("Sz", i)])
+        assert abs(got_z[i] - ref) <= 1e-12 * scale
+    for p, (i, j) in enumerate(zip(si, sj)):
+        ref = ospin.pair_expectation(n, two_s, T, psi, [("Sz", i), ("Sz", j)])
+        assert abs(got_zz[p] - ref) <= 1e-12 * scale, (i, j)
+        ref = ospin.pair_expectation(n, two_s, T, psi, [("Splus", i), ("Sminus", j)])
+        assert abs(got_pm[p] - ref) <= 1e-12 * scale, (i, j)
+    v.free()
+    ham.close()
+
+
+@pytest.mark.parametrize("lat,geo,two_s", [("ladder", {"L": 4}, 2), ("chain lattice", {"L": 6}, 3),
+                                           ("open chain lattice", {"L": 5}, 4)])
+def test_spin_s_measurements_match_oracle(lat, geo, two_s):
+    """MEASURE_* quantities of the ground state of a spin-S sector (random couplings and fields: no
+    degeneracy) equal the oracle's on the dense eigenvector (1e-8: Ritz vectors to |H psi - E psi| ~ 1e-9)."""
+    from alps_b200 import measure
+    from oracle import measure as omeasure
+    rng = np.random.default_rng(two_s + 31)
+    n, _, graph = lattice.lattice_graph(lat, geo)
+    bonds = [(s, t, float(j), float(j), 0.0) for (s, t, _), j in zip(graph, rng.uniform(0.7, 1.3, len(graph)))]
+    h = rng.uniform(-0.2, 0.2, n)
+    params = dict(geo, LATTICE=lat, **SPIN_MEAS)
+    T = n * two_s // 2
+    ham = ed.Hamiltonian(n, T, bonds, site_h=h, two_s=two_s)
+    ham.solve(nev=1, seed=2)
+    vecs, ev, _ = ham.eigenvectors(k=1, seed=2)
+    H = ospin.hamiltonian(n, two_s, bonds, h, None, digit_sum=T).toarray()
+    w, Z = np.linalg.eigh(H)
+    assert abs(w[0] - ev[0]) < 1e-9 and w[1] - w[0] > 1e-6
+    got = measure.measure(ham, vecs[0], params)
+    ref = omeasure.measure(ham.basis(), Z[:, 0], params, two_s)
+    for key in ref:
+        for name in ref[key]:
+            a, b = np.asarray(got[key][name], float), np.asarray(ref[key][name], float)
+            assert a.shape == b.shape, (key, name)
+            assert np.allclose(a, b, atol=1e-8), (key, name, a, b)
+    vecs[0].free()
+    ham.close()
+
+
+def test_sparsediag_spin_one_measurements():
+    """local_S = 1 Heisenberg ring through sparsediag.run: zero magnetization at Sz_total = 0 and
+    <S_0 . S_1> = E0 / L (Sz Sz plus half of S+ S- and S- S+ at distance 1)."""
+    L = 6
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": L, "J": 1, "local_S": 1, "CONSERVED_QUANTUMNUMBERS": "Sz",
+         "Sz_total": 0, "NUMBER_EIGENVALUES": 1, "TRANSLATION_SYMMETRY": "false", **SPIN_MEAS}
+    res = sparsediag.run(p)
+    m = res["sectors"][0]["measurements"][0]
+    assert abs(m["average"]["Magnetization"]) < 1e-12
+    c = m["correlations"]
+    d1 = c["Diagonal spin correlations"][1] + 0.5 * (c["Offdiagonal spin correlations"][1] +
+                                                      c["Reverse offdiagonal"][1])
+    assert abs(d1 - res["ground_state_energy"] / L) < 1e-9
+    # on one site S.S = S(S+1) = 2: Sz^2 + (S+ S- + S- S+) / 2
+    d0 = c["Diagonal spin correlations"][0] + 0.5 * (c["Offdiagonal spin correlations"][0] +
+                                                      c["Reverse offdiagonal"][0])
+    assert abs(d0 - 2.0) < 1e-9

@@ -280,3 +280,21 @@ def _dense_real(n, n_up, bonds, st):
         e[j] = 1.0
         out[:, j] = M.mult(e)
     return out
+
+
+@pytest.mark.parametrize("two_s,n", [(1, 6), (2, 5), (3, 4), (4, 4)])
+def test_measure_oracle_spin_s_operators_match_kronecker_products(two_s, n):
+    """The oracle's digit-level site operators (measurements) equal the Kronecker-product operators of the
+    spin-S Hamiltonian oracle on a random vector: <Sz_i>, <Sz_i Sz_j>, <S+_i S-_j>, <S-_i S+_j>."""
+    from oracle import measure as omeasure
+    from oracle import spin as ospin
+    rng = np.random.default_rng(two_s * 10 + n)
+    T = n * two_s // 2
+    states = ospin.packed_states(n, two_s, T)
+    psi = rng.normal(size=len(states))
+    for ops in ([("Sz", 1)], [("Sz", 0), ("Sz", n - 1)], [("Sz", 2), ("Sz", 2)], [("Splus", 0), ("Sminus", 2)],
+                [("Sminus", 1), ("Splus", 3)], [("Splus", 1), ("Sminus", 1)], [("Sminus", 2), ("Splus", 2)],
+                [("Sz", 0), ("Splus", 1)]):
+        got = omeasure._expect(states, psi, n, ops, two_s)
+        ref = ospin.pair_expectation(n, two_s, T, psi, ops)
+        assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (ops, got, ref)
