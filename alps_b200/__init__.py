@@ -135,6 +135,9 @@ def lib():
             "aed_create_spin": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int32, ctypes.c_int,
                                                ctypes.POINTER(_P)]),
             "aed_spin_basis": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), _I64, _I64]),
+            "aed_create_spin_momentum": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int32,
+                                                        ctypes.POINTER(Translations), ctypes.c_int,
+                                                        ctypes.POINTER(_P)]),
             "aed_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
             "aed_momentum_expectation": (ctypes.c_int, [_P, _P, ctypes.c_int32, _I32, _I32P, _I32P, _DP]),
             "aed_lattice_geometry": (ctypes.c_int, [ctypes.c_char_p, _I32P, _I32P, _I32P]),
@@ -331,9 +334,9 @@ class DeviceVector:
 
 
 class Hamiltonian:
-    """One Sz sector of a spin-1/2 model on one GPU (an aed_handle); with `translations` (a list of
-    (phase, site map), the identity first, as lattice_translations returns) one momentum sector of it,
-    whose vectors are complex."""
+    """One Sz sector of a spin model on one GPU (an aed_handle; local spin two_s / 2, spin 1/2 on the
+    bit-exact engine unless `generic`); with `translations` (a list of (phase, site map), the identity
+    first, as lattice_translations returns) one momentum sector of it, whose vectors are complex."""
 
     def __init__(self, n_sites, n_up, bonds, precision=FP64, device=0, site_h=None, site_d=None, translations=None,
                  two_s=1, generic=False):
@@ -355,19 +358,21 @@ class Hamiltonian:
         self.momentum = translations is not None
         self.two_s = int(two_s)
         self.spin_s = self.two_s != 1 or generic  # the spin-S engine (aed_create_spin)
-        if self.spin_s:
-            if self.momentum:
-                raise AEDError(ERR_INVALID, "momentum sectors: local spin 1/2 only")
-            if precision != FP64:
-                raise AEDError(ERR_INVALID, "spin-S sectors are FP64")
-            _check(lib().aed_create_spin(ctypes.byref(desc), self.two_s, device, ctypes.byref(h)))
-        elif self.momentum:
+        if self.momentum:
             if precision != FP64:
                 raise AEDError(ERR_INVALID, "momentum sectors are FP64")
             self._tmap = np.ascontiguousarray([m for _, m in translations], dtype=np.int32).reshape(-1)
             self._tph = np.ascontiguousarray([[p.real, p.imag] for p, _ in translations], dtype=np.float64)
             tr = Translations(len(translations), self._tmap.ctypes.data_as(_I32P), _dp(self._tph))
-            _check(lib().aed_create_momentum(ctypes.byref(desc), ctypes.byref(tr), device, ctypes.byref(h)))
+            if self.spin_s:
+                _check(lib().aed_create_spin_momentum(ctypes.byref(desc), self.two_s, ctypes.byref(tr), device,
+                                                      ctypes.byref(h)))
+            else:
+                _check(lib().aed_create_momentum(ctypes.byref(desc), ctypes.byref(tr), device, ctypes.byref(h)))
+        elif self.spin_s:
+            if precision != FP64:
+                raise AEDError(ERR_INVALID, "spin-S sectors are FP64")
+            _check(lib().aed_create_spin(ctypes.byref(desc), self.two_s, device, ctypes.byref(h)))
         else:
             _check(lib().aed_create(ctypes.byref(desc), precision, device, ctypes.byref(h)))
         self._h = h
@@ -421,9 +426,14 @@ class Hamiltonian:
         return ham
 
     def momentum_basis(self):
-        """(representative states, normalisations) of a momentum sector (aed_momentum_basis)."""
-        st = np.empty(self.dim, np.uint32)
+        """(representative states, normalisations) of a momentum sector (aed_momentum_basis; a spin-S
+        sector's representatives are 64-bit packed digits, from aed_spin_basis)."""
         nm = np.empty(self.dim)
+        if self.spin_s:
+            st = self.basis()
+            _check(lib().aed_momentum_basis(self._h, None, _dp(nm), 0, self.dim))
+            return st, nm
+        st = np.empty(self.dim, np.uint32)
         _check(lib().aed_momentum_basis(self._h, st.ctypes.data_as(_U32P), _dp(nm), 0, self.dim))
         return st, nm
 

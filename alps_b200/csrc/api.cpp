@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 
@@ -145,7 +146,7 @@ void release(aed_handle* h) {
                   (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64,
                   (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map, (void*)h->d_sthi,
                   (void*)h->d_stlo, (void*)h->d_slolist, (void*)h->d_slooff, (void*)h->d_sblk_hi,
-                  (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r})
+                  (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r, (void*)h->d_sreps})
     mem_dev_free(p, h->stream);
   delete h->mp;
   delete h->sp;
@@ -351,6 +352,9 @@ int handle_tune(aed_handle* h, bool f32, const void* x, void* y) {
 }
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part) {
+  if (h->gen && h->mom)
+    return launch_spin_mom_hv(*h->sp, *h->mp, h->sdev, h->spin_mom_tables(), (const double*)x, (double*)y,
+                              alpha_part, h->stream);
   if (h->gen) return launch_spin_hv(*h->sp, h->sdev, (const double*)x, (double*)y, alpha_part, h->stream);
   if (h->mom)
     return launch_mom_hv(*h->mp, h->dt, h->mom_tables(), (const double*)x, (double*)y, alpha_part, h->stream);
@@ -528,16 +532,11 @@ namespace {
 int translation_invariant(const Model& m, int n_trans, const int* maps);
 }  // namespace
 
-int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out) {
-  if (!out || !model || !tr) return fail(AED_ERR_INVALID, "NULL argument");
-  *out = nullptr;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return fail(AED_ERR_CUDA, "no CUDA device available");
-  }
-  if (device < 0 || device >= ndev) return fail(AED_ERR_INVALID, "device index out of range");
-  const int N = model->n_sites;
+namespace {
+
+// Check the translations of a momentum sector (permutations of the N sites,
+// the identity first) and fill the phases and destinations of mp.
+int momentum_params(int N, const aed_translations* tr, MomParams& mp) {
   if (tr->n_trans < 1 || tr->n_trans > kMaxTrans) return fail(AED_ERR_INVALID, "n_trans must be in 1..62");
   if (!tr->site_map || !tr->phase) return fail(AED_ERR_INVALID, "translations: NULL site_map or phase");
   if (N < 1 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 1..32");
@@ -549,6 +548,34 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
       if (t == 0 && j != i) return fail(AED_ERR_INVALID, "the first translation must be the identity");
       seen |= 1u << j;
     }
+  }
+  mp.N = N;
+  mp.n_trans = tr->n_trans;
+  mp.inv_sqrt_n = 1.0 / std::sqrt((double)N);
+  for (int t = 0; t < tr->n_trans; ++t) {
+    mp.phase_re[t] = tr->phase[2 * t];
+    mp.phase_im[t] = tr->phase[2 * t + 1];
+    for (int i = 0; i < N; ++i) mp.dst[t][i] = (uint8_t)(N - 1 - tr->site_map[(size_t)t * N + i]);
+  }
+  return AED_OK;
+}
+
+}  // namespace
+
+int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out) {
+  if (!out || !model || !tr) return fail(AED_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AED_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(AED_ERR_INVALID, "device index out of range");
+  const int N = model->n_sites;
+  std::unique_ptr<MomParams> mpp(new MomParams());
+  {
+    const int rc0 = momentum_params(N, tr, *mpp);
+    if (rc0) return rc0;
   }
   {
     Model m;
@@ -569,16 +596,8 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
     release(h);
     return rc;
   }
-  MomParams* mp = new MomParams();
+  MomParams* mp = mpp.release();
   h->mp = mp;
-  mp->N = N;
-  mp->n_trans = tr->n_trans;
-  mp->inv_sqrt_n = 1.0 / std::sqrt((double)N);
-  for (int t = 0; t < tr->n_trans; ++t) {
-    mp->phase_re[t] = tr->phase[2 * t];
-    mp->phase_im[t] = tr->phase[2 * t + 1];
-    for (int i = 0; i < N; ++i) mp->dst[t][i] = (uint8_t)(N - 1 - tr->site_map[(size_t)t * N + i]);
-  }
   mom_flips(h->model, *mp);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
@@ -754,12 +773,56 @@ int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_
   return AED_OK;
 }
 
+int aed_create_spin_momentum(const aed_model_desc* model, int32_t two_s, const aed_translations* tr, int device,
+                             aed_handle** out) {
+  if (!out || !model || !tr) return fail(AED_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  std::unique_ptr<MomParams> mpp(new MomParams());
+  int rc = momentum_params(model->n_sites, tr, *mpp);
+  if (rc) return rc;
+  aed_handle* h = nullptr;
+  if ((rc = aed_create_spin(model, two_s, device, &h))) return rc;
+  {
+    std::vector<int> maps(tr->site_map, tr->site_map + (size_t)tr->n_trans * model->n_sites);
+    if ((rc = translation_invariant(h->model, tr->n_trans, maps.data()))) {
+      aed_destroy(h);
+      return rc;
+    }
+  }
+  DeviceGuard g(device);
+  h->mom = true;
+  h->mp = mpp.release();
+  // the Sz sector's partial-sum arrays give way to the momentum sector's
+  mem_dev_free(h->d_partA, h->stream);
+  mem_dev_free(h->d_partB, h->stream);
+  h->d_partA = h->d_partB = nullptr;
+  int64_t dim = 0;
+  if ((rc = spin_mom_build(*h->mp, h->sdev, h->stream, &h->d_sreps, &h->d_norm, &h->d_map, &dim))) {
+    release(h);
+    return rc;
+  }
+  h->dim = dim;
+  h->vlen = 2 * dim;
+  if ((rc = mem_dev_alloc_n(&h->d_partA, (size_t)mom_tiles(dim) + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_partB, (size_t)red_chunks(h->vlen) + 1))) {
+    release(h);
+    return rc;
+  }
+  *out = h;
+  return AED_OK;
+}
+
 int aed_spin_basis(aed_handle* h, uint64_t* states, int64_t offset, int64_t count) {
   if (!h || (!states && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
   if (!h->gen) return fail(AED_ERR_INVALID, "aed_spin_basis: not a spin-S sector (aed_create_spin)");
   if (offset < 0 || count < 0 || offset + count > h->dim) return fail(AED_ERR_INVALID, "range outside the basis");
   if (count == 0) return AED_OK;
   DeviceGuard g(h->device);
+  if (h->mom) {  // the representatives of a momentum sector
+    AED_CUDA_TRY(cudaMemcpyAsync(states, h->d_sreps + offset, (size_t)count * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return AED_OK;
+  }
   uint64_t* d = nullptr;
   int rc = mem_dev_alloc_n(&d, (size_t)count);
   if (rc) return rc;
@@ -776,6 +839,8 @@ int aed_spin_basis(aed_handle* h, uint64_t* states, int64_t offset, int64_t coun
 int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count) {
   if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
   if (!h->mom) return fail(AED_ERR_INVALID, "aed_momentum_basis: not a momentum sector");
+  if (h->gen && states)
+    return fail(AED_ERR_INVALID, "aed_momentum_basis: spin-S representatives are 64-bit (aed_spin_basis)");
   if (offset < 0 || count < 0 || offset + count > h->dim) return fail(AED_ERR_INVALID, "range outside the basis");
   if (count == 0) return AED_OK;
   DeviceGuard g(h->device);
@@ -840,6 +905,7 @@ int aed_momentum_expectation(aed_handle* h, const void* psi, int32_t kind, int32
   *out = 0.0;
   if (n <= 0 || h->dim == 0) return AED_OK;
   DeviceGuard g(h->device);
+  if (h->gen) return spin_mom_expectation(h, static_cast<const double*>(psi), kind, n, site_i, site_j, out);
   const int grid = mom_expect_grid(h->dim);
   void* w = nullptr;
   int rc = handle_workspace(h, 1, (size_t)grid * 8, &w);

@@ -49,6 +49,8 @@ struct aed_handle {
   double* d_mdiag = nullptr;
   uint32_t* d_map = nullptr;
   aed::MomTables mom_tables() const { return {d_reps, d_norm, d_mdiag, d_map, dim}; }
+  uint64_t* d_sreps = nullptr;  // representatives of a spin-S momentum sector (mom && gen)
+  aed::SpinMomTables spin_mom_tables() const { return {d_sreps, d_norm, d_map, dim}; }
   // spin-S sector (aed_create_spin): tables of spin.cuh
   bool gen = false;
   aed::SpinParams* sp = nullptr;
@@ -125,6 +127,9 @@ int measure_pairs(aed_handle* h, const void* psi, int kind, int n, const int32_t
 // The same for a spin-S sector (aed_create_spin; FP64 vectors): spin.cu.
 int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
                        double* out);
+// <psi| sum_p O(si[p], sj[p]) |psi> in a spin-S momentum sector (spin.cu).
+int spin_mom_expectation(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
+                         double* out);
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
 // Choose the apply variant for this precision now (timed launches on x, y)

@@ -5,6 +5,7 @@
 // Reference paths are relative to the ALPS source tree.
 
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "handle.h"
@@ -17,26 +18,57 @@ namespace {
 constexpr int kMomThreads = 256;
 constexpr int kMomChunk = kMomThreads * 8;  // states per chunk of the basis scan (8 per thread)
 
-__device__ __forceinline__ uint32_t translate(const MomParams& mp, uint32_t s, int t) {
-  uint32_t out = 0u;
-  const int N = mp.N;
-  for (int i = 0; i < N; ++i) out |= ((s >> (N - 1 - i)) & 1u) << mp.dst[t][i];
-  return out;
-}
+// States of the two kinds of site basis.  BitCodec: spin 1/2, one bit per
+// site (up = 1), ranks by the two tables of the Sz sector (kernels.cuh).
+// DigitCodec: spin S, the digit m + S of each site in `bits` bits, ranks by
+// the spin-S tables (spin.cuh).  Site i sits at position N-1-i in both, and a
+// translation moves it to position dst[t][i].
+struct BitCodec {
+  using Word = uint32_t;
+  DevTables t;
+  __device__ __forceinline__ Word translate(const MomParams& mp, Word s, int tr) const {
+    Word out = 0u;
+    const int N = mp.N;
+    for (int i = 0; i < N; ++i) out |= ((s >> (N - 1 - i)) & 1u) << mp.dst[tr][i];
+    return out;
+  }
+  __device__ __forceinline__ uint32_t rank(Word s) const {
+    return t.thi[s >> t.Nlo] + t.tlo[s & ((1u << t.Nlo) - 1u)];
+  }
+};
+
+struct DigitCodec {
+  using Word = uint64_t;
+  SpinDev t;
+  __device__ __forceinline__ Word translate(const MomParams& mp, Word s, int tr) const {
+    Word out = 0u;
+    const int N = t.N, b = t.bits;
+    const uint64_t dm = (1ull << b) - 1ull;
+    for (int i = 0; i < N; ++i) out |= ((s >> (b * (N - 1 - i))) & dm) << (b * mp.dst[tr][i]);
+    return out;
+  }
+  __device__ __forceinline__ uint32_t rank(Word s) const {
+    const int sh = t.bits * t.Nl;
+    return t.thi[(uint32_t)(s >> sh)] + t.tlo[(uint32_t)(s & ((1ull << sh) - 1ull))];
+  }
+};
 
 // The orbit of s: its smallest state, the first translation reaching it, and
 // the phase sum of the translations that fix s (identity included), in list
 // order as bloch_basis_states::build adds them (blochbasisstates.h:199-240).
+template <class W>
 struct Orbit {
-  uint32_t min;
+  W min;
   int tmin;
   double fre, fim;
 };
 
-__device__ __forceinline__ Orbit orbit_of(const MomParams& mp, uint32_t s) {
-  Orbit o{s, 0, 1.0, 0.0};
+template <class C>
+__device__ __forceinline__ Orbit<typename C::Word> orbit_of(const MomParams& mp, const C& c, typename C::Word s) {
+  using W = typename C::Word;
+  Orbit<W> o{s, 0, 1.0, 0.0};
   for (int t = 1; t < mp.n_trans; ++t) {
-    const uint32_t ts = translate(mp, s, t);
+    const W ts = c.translate(mp, s, t);
     if (ts < o.min) {
       o.min = ts;
       o.tmin = t;
@@ -50,10 +82,14 @@ __device__ __forceinline__ Orbit orbit_of(const MomParams& mp, uint32_t s) {
 }
 
 // sqrt|phase sum| of a representative (w of blochbasisstates.h:243)
-__device__ __forceinline__ double orbit_weight(const Orbit& o) { return sqrt(hypot(o.fre, o.fim)); }
+template <class W>
+__device__ __forceinline__ double orbit_weight(const Orbit<W>& o) {
+  return sqrt(hypot(o.fre, o.fim));
+}
 
-__device__ __forceinline__ bool kept_rep(const MomParams& mp, uint32_t s) {
-  const Orbit o = orbit_of(mp, s);
+template <class C>
+__device__ __forceinline__ bool kept_rep(const MomParams& mp, const C& c, typename C::Word s) {
+  const auto o = orbit_of(mp, c, s);
   return o.min == s && orbit_weight(o) >= 0.01;
 }
 
@@ -83,8 +119,9 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 }
 
 // Pass 1: flags of the kept representatives and their count per chunk.
-__global__ void __launch_bounds__(kMomThreads) mom_flag_kernel(const __grid_constant__ MomParams mp,
-                                                               const uint32_t* __restrict__ states, int64_t D,
+template <class C>
+__global__ void __launch_bounds__(kMomThreads) mom_flag_kernel(const __grid_constant__ MomParams mp, const C cd,
+                                                               const typename C::Word* __restrict__ states, int64_t D,
                                                                uint8_t* __restrict__ flag,
                                                                uint32_t* __restrict__ count) {
   __shared__ uint32_t sm[kMomThreads / 32];
@@ -95,7 +132,7 @@ __global__ void __launch_bounds__(kMomThreads) mom_flag_kernel(const __grid_cons
     for (int u = 0; u < 8; ++u) {
       const int64_t r = r0 + u;
       if (r < D) {
-        const bool k = kept_rep(mp, states[r]);
+        const bool k = kept_rep(mp, cd, states[r]);
         flag[r] = k ? 1 : 0;
         n += k ? 1u : 0u;
       }
@@ -117,13 +154,16 @@ __device__ __forceinline__ double diag_of(const HvParams& P, uint32_t s) {
 
 // Pass 2: representatives in order (chunk offsets from the host scan); the
 // map entry of every representative is its index, every other entry kMomNone.
+// diag (spin 1/2 only; may be null): the diagonal terms of each representative.
+template <class C>
 __global__ void __launch_bounds__(kMomThreads) mom_rep_kernel(const __grid_constant__ MomParams mp,
-                                                              const __grid_constant__ HvParams P,
-                                                              const uint32_t* __restrict__ states, int64_t D,
+                                                              const __grid_constant__ HvParams P, const C cd,
+                                                              const typename C::Word* __restrict__ states, int64_t D,
                                                               const uint8_t* __restrict__ flag,
                                                               const uint32_t* __restrict__ offset,
-                                                              uint32_t* __restrict__ reps, double* __restrict__ norm,
-                                                              double* __restrict__ diag, uint32_t* __restrict__ map) {
+                                                              typename C::Word* __restrict__ reps,
+                                                              double* __restrict__ norm, double* __restrict__ diag,
+                                                              uint32_t* __restrict__ map) {
   __shared__ uint32_t sm[kMomThreads / 32];
   const int64_t nch = (D + kMomChunk - 1) / kMomChunk;
   for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
@@ -136,10 +176,12 @@ __global__ void __launch_bounds__(kMomThreads) mom_rep_kernel(const __grid_const
       const int64_t r = r0 + u;
       if (r >= D) break;
       if (flag[r]) {
-        const uint32_t s = states[r];
+        const typename C::Word s = states[r];
         reps[idx] = s;
-        norm[idx] = orbit_weight(orbit_of(mp, s)) * mp.inv_sqrt_n;
-        diag[idx] = diag_of(P, s);
+        norm[idx] = orbit_weight(orbit_of(mp, cd, s)) * mp.inv_sqrt_n;
+        if constexpr (std::is_same<C, BitCodec>::value) {
+          if (diag) diag[idx] = diag_of(P, s);
+        }
         map[r] = idx;
         ++idx;
       } else {
@@ -153,16 +195,15 @@ __global__ void __launch_bounds__(kMomThreads) mom_rep_kernel(const __grid_const
 // representative of its orbit through the first translation reaching it
 // (blochbasisstates.h:221-230); reads only entries of orbit minima, which
 // this pass does not write.
-__global__ void __launch_bounds__(kMomThreads) mom_member_kernel(const __grid_constant__ MomParams mp,
-                                                                 const DevTables t,
-                                                                 const uint32_t* __restrict__ states, int64_t D,
-                                                                 uint32_t* __restrict__ map) {
-  const uint32_t lm = (1u << t.Nlo) - 1u;
+template <class C>
+__global__ void __launch_bounds__(kMomThreads) mom_member_kernel(const __grid_constant__ MomParams mp, const C cd,
+                                                                 const typename C::Word* __restrict__ states,
+                                                                 int64_t D, uint32_t* __restrict__ map) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < D; r += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t s = states[r];
-    const Orbit o = orbit_of(mp, s);
+    const typename C::Word s = states[r];
+    const auto o = orbit_of(mp, cd, s);
     if (o.min == s) continue;
-    const uint32_t e = map[t.thi[o.min >> t.Nlo] + t.tlo[o.min & lm]];
+    const uint32_t e = map[cd.rank(o.min)];
     map[r] = e == kMomNone ? kMomNone : ((uint32_t)o.tmin << kMomRepBits) | e;
   }
 }
@@ -286,18 +327,29 @@ int grid_for(int64_t units) {
   return (int)(units < 1 ? 1 : (units < cap ? units : cap));
 }
 
-}  // namespace
+// The sector's states in basis order (the two-table ranks' inverse).
+int fill_states(const BitCodec& c, uint32_t* states, int64_t D, cudaStream_t st) {
+  return launch_basis_copy(c.t, states, 0, D, st);
+}
+int fill_states(const DigitCodec& c, uint64_t* states, int64_t D, cudaStream_t st) {
+  return launch_spin_basis(c.t, states, 0, D, st);
+}
 
-int mom_build(const MomParams& mp, const HvParams& P, const DevTables& t, cudaStream_t st, uint32_t** reps,
-              double** norm, double** diag, uint32_t** map, int64_t* dim) {
+// The three passes over the D states of the Sz sector (flags and counts, host
+// scan of the counts, representatives, members).  diag == nullptr: no
+// diagonal array.
+template <class C>
+int mom_build_t(const MomParams& mp, const HvParams& P, const C& cd, int64_t D, cudaStream_t st,
+                typename C::Word** reps, double** norm, double** diag, uint32_t** map, int64_t* dim) {
+  using W = typename C::Word;
   *reps = nullptr;
-  *norm = *diag = nullptr;
+  *norm = nullptr;
+  if (diag) *diag = nullptr;
   *map = nullptr;
   *dim = 0;
-  const int64_t D = t.D;
   if (D == 0) return AED_OK;
   const int64_t nch = (D + kMomChunk - 1) / kMomChunk;
-  uint32_t* states = nullptr;
+  W* states = nullptr;
   uint8_t* flag = nullptr;
   uint32_t *count = nullptr, *offset = nullptr;
   int rc = AED_OK;
@@ -309,11 +361,11 @@ int mom_build(const MomParams& mp, const HvParams& P, const DevTables& t, cudaSt
   };
   if ((rc = mem_dev_alloc_n(&states, (size_t)D)) || (rc = mem_dev_alloc_n(&flag, (size_t)D)) ||
       (rc = mem_dev_alloc_n(&count, (size_t)nch)) || (rc = mem_dev_alloc_n(&offset, (size_t)nch)) ||
-      (rc = launch_basis_copy(t, states, 0, D, st))) {
+      (rc = fill_states(cd, states, D, st))) {
     cleanup();
     return rc;
   }
-  mom_flag_kernel<<<grid_for(nch), kMomThreads, 0, st>>>(mp, states, D, flag, count);
+  mom_flag_kernel<C><<<grid_for(nch), kMomThreads, 0, st>>>(mp, cd, states, D, flag, count);
   if ((rc = check_launch_counted("mom_flag_kernel"))) {
     cleanup();
     return rc;
@@ -335,14 +387,16 @@ int mom_build(const MomParams& mp, const HvParams& P, const DevTables& t, cudaSt
     return fail(AED_ERR_INVALID, "momentum sector larger than 2^26 representatives");
   }
   if ((rc = mem_dev_alloc_n(reps, (size_t)total)) || (rc = mem_dev_alloc_n(norm, (size_t)total)) ||
-      (rc = mem_dev_alloc_n(diag, (size_t)total)) || (rc = mem_dev_alloc_n(map, (size_t)D))) {
+      (diag && (rc = mem_dev_alloc_n(diag, (size_t)total))) || (rc = mem_dev_alloc_n(map, (size_t)D))) {
     cleanup();
     return rc;
   }
   cudaMemcpyAsync(offset, ho.data(), (size_t)nch * 4, cudaMemcpyHostToDevice, st);
-  mom_rep_kernel<<<grid_for(nch), kMomThreads, 0, st>>>(mp, P, states, D, flag, offset, *reps, *norm, *diag, *map);
+  mom_rep_kernel<C><<<grid_for(nch), kMomThreads, 0, st>>>(mp, P, cd, states, D, flag, offset, *reps, *norm,
+                                                          diag ? *diag : nullptr, *map);
   if (!(rc = check_launch_counted("mom_rep_kernel"))) {
-    mom_member_kernel<<<grid_for((D + kMomThreads - 1) / kMomThreads), kMomThreads, 0, st>>>(mp, t, states, D, *map);
+    mom_member_kernel<C><<<grid_for((D + kMomThreads - 1) / kMomThreads), kMomThreads, 0, st>>>(mp, cd, states, D,
+                                                                                                 *map);
     rc = check_launch_counted("mom_member_kernel");
   }
   if (!rc) {
@@ -352,6 +406,19 @@ int mom_build(const MomParams& mp, const HvParams& P, const DevTables& t, cudaSt
   cleanup();
   *dim = (int64_t)total;
   return rc;
+}
+
+}  // namespace
+
+int mom_build(const MomParams& mp, const HvParams& P, const DevTables& t, cudaStream_t st, uint32_t** reps,
+              double** norm, double** diag, uint32_t** map, int64_t* dim) {
+  return mom_build_t(mp, P, BitCodec{t}, t.D, st, reps, norm, diag, map, dim);
+}
+
+int spin_mom_build(const MomParams& mp, const SpinDev& t, cudaStream_t st, uint64_t** reps, double** norm,
+                   uint32_t** map, int64_t* dim) {
+  static const HvParams no_diag{};  // the spin-S apply forms its diagonal itself
+  return mom_build_t(mp, no_diag, DigitCodec{t}, t.D, st, reps, norm, (double**)nullptr, map, dim);
 }
 
 int launch_mom_diag(const HvParams& P, const uint32_t* reps, int64_t dim, double* diag, cudaStream_t st) {

@@ -21,6 +21,7 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "spin.cuh"
 
 namespace aed {
 
@@ -73,5 +74,21 @@ struct MomPairs {
 int mom_expectation(const MomParams& mp, const DevTables& t, const MomTables& m, const double* psi, int kind,
                     const MomPairs& pairs, double* part, int grid, cudaStream_t st);
 int mom_expect_grid(int64_t dim);
+
+// Momentum sectors of spin-S models (aed_create_spin_momentum): the same
+// Bloch basis over the spin-S sector's states (64-bit packed digits,
+// spin.cuh).  The apply forms each representative's diagonal itself, so
+// there is no diagonal array.
+struct SpinMomTables {
+  const uint64_t* reps;  // dim representative states, ascending
+  const double* norm;    // dim normalisations
+  const uint32_t* map;   // D entries: (t << kMomRepBits) | j, or kMomNone
+  int64_t dim;
+};
+int spin_mom_build(const MomParams& mp, const SpinDev& t, cudaStream_t st, uint64_t** reps, double** norm,
+                   uint32_t** map, int64_t* dim);
+// y = H x on interleaved complex vectors (spin.cu); alpha_part as launch_mom_hv.
+int launch_spin_mom_hv(const SpinParams& p, const MomParams& mp, const SpinDev& t, const SpinMomTables& m,
+                       const double* x, double* y, double* alpha_part, cudaStream_t st);
 
 }  // namespace aed

@@ -214,42 +214,82 @@ __global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, i
   out[n] = ((uint64_t)h << (t.bits * t.Nl)) | t.lolist[t.looff[t.T - sum] + r];
 }
 
+// The couplings of SpinParams staged in shared memory for the row walk.
+struct SpinShared {
+  double cv[kSpinMaxCls * kSpinMaxTrans];  // tabulated elements, or A, B, C of each transition
+  uint8_t ta[kSpinMaxTrans], tc[kSpinMaxTrans];
+  int ts[kSpinMaxPairs + 1];
+  int b1[kMaxBonds], b2[kMaxBonds], bc[kMaxBonds];
+  double bj[3][kMaxBonds];
+  double sdg[kSpinMaxSites * kSpinMaxDim];
+};
+
+// Fill sh (all threads of the CTA; the caller synchronises).
+__device__ __forceinline__ void stage_spin(const SpinParams& p, int d, int N, SpinShared& sh) {
+  const int ntr = p.tstart[d * d];
+  const bool tab = p.n_cls > 0;
+  for (int q = threadIdx.x; q <= d * d; q += blockDim.x) sh.ts[q] = p.tstart[q];
+  for (int q = threadIdx.x; q < ntr; q += blockDim.x) {
+    sh.ta[q] = p.trans[q].a2;
+    sh.tc[q] = p.trans[q].c2;
+  }
+  if (tab) {
+    for (int q = threadIdx.x; q < p.n_cls * ntr; q += blockDim.x) sh.cv[q] = p.cval[q / ntr][q % ntr];
+  } else {
+    for (int q = threadIdx.x; q < ntr; q += blockDim.x) {
+      sh.cv[3 * q] = p.trans[q].A;
+      sh.cv[3 * q + 1] = p.trans[q].B;
+      sh.cv[3 * q + 2] = p.trans[q].C;
+    }
+  }
+  for (int q = threadIdx.x; q < p.n_bonds; q += blockDim.x) {
+    sh.b1[q] = p.s1[q];
+    sh.b2[q] = p.s2[q];
+    sh.bc[q] = tab ? p.cls[q] * ntr : 0;
+    sh.bj[0][q] = p.jz[q];
+    sh.bj[1][q] = p.jxy[q];
+    sh.bj[2][q] = p.kq[q];
+  }
+  for (int q = threadIdx.x; q < N * d; q += blockDim.x) sh.sdg[q] = p.sdiag[q / d][q % d];
+}
+
+// One row of H on state s: returns its diagonal element (site terms, then the
+// diagonal transitions of the bonds in order) and calls off(v, s2) for every
+// off-diagonal transition to state s2, bonds in order.
+template <class Off>
+__device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bool tab, int N, int bits, int d,
+                                           uint64_t s, Off&& off) {
+  const uint32_t dm = (1u << bits) - 1u;
+  double dg = 0.0;
+  for (int i = 0; i < N; ++i) dg += sh.sdg[i * d + (int)((s >> (bits * (N - 1 - i))) & dm)];  // -h Sz + D Sz^2
+  for (int q = 0; q < n_bonds; ++q) {
+    const int i = sh.b1[q], j = sh.b2[q];
+    const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
+    const int a = (int)((s >> wi) & dm), c = (int)((s >> wj) & dm);
+    const int pr = a * d + c;
+    const int cb = sh.bc[q];
+    for (int e = sh.ts[pr]; e < sh.ts[pr + 1]; ++e) {
+      const double v = tab ? sh.cv[cb + e]
+                           : sh.bj[0][q] * sh.cv[3 * e] + sh.bj[1][q] * sh.cv[3 * e + 1] + sh.bj[2][q] * sh.cv[3 * e + 2];
+      const int a2 = sh.ta[e], c2 = sh.tc[e];
+      if (a2 == a && c2 == c) {
+        dg += v;
+      } else {
+        off(v, s + ((uint64_t)a2 << wi) - ((uint64_t)a << wi) + ((uint64_t)c2 << wj) - ((uint64_t)c << wj));
+      }
+    }
+  }
+  return dg;
+}
+
 __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_constant__ SpinParams p, const SpinDev t,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ alpha_part) {
-  __shared__ double cv[kSpinMaxCls * kSpinMaxTrans];  // tabulated elements, or A, B, C of each transition
-  __shared__ uint8_t ta[kSpinMaxTrans], tc[kSpinMaxTrans];
-  __shared__ int ts[kSpinMaxPairs + 1];
-  __shared__ int b1[kMaxBonds], b2[kMaxBonds], bc[kMaxBonds];
-  __shared__ double bj[3][kMaxBonds];
-  __shared__ double sdg[kSpinMaxSites * kSpinMaxDim];
+  __shared__ SpinShared sh;
   __shared__ double red[33];
   const int d = t.d, N = t.N, bits = t.bits;
-  const int ntr = p.tstart[d * d];
   const bool tab = p.n_cls > 0;
-  for (int q = threadIdx.x; q <= d * d; q += kSpinThreads) ts[q] = p.tstart[q];
-  for (int q = threadIdx.x; q < ntr; q += kSpinThreads) {
-    ta[q] = p.trans[q].a2;
-    tc[q] = p.trans[q].c2;
-  }
-  if (tab) {
-    for (int q = threadIdx.x; q < p.n_cls * ntr; q += kSpinThreads) cv[q] = p.cval[q / ntr][q % ntr];
-  } else {
-    for (int q = threadIdx.x; q < ntr; q += kSpinThreads) {
-      cv[3 * q] = p.trans[q].A;
-      cv[3 * q + 1] = p.trans[q].B;
-      cv[3 * q + 2] = p.trans[q].C;
-    }
-  }
-  for (int q = threadIdx.x; q < p.n_bonds; q += kSpinThreads) {
-    b1[q] = p.s1[q];
-    b2[q] = p.s2[q];
-    bc[q] = tab ? p.cls[q] * ntr : 0;
-    bj[0][q] = p.jz[q];
-    bj[1][q] = p.jxy[q];
-    bj[2][q] = p.kq[q];
-  }
-  for (int q = threadIdx.x; q < N * d; q += kSpinThreads) sdg[q] = p.sdiag[q / d][q % d];
+  stage_spin(p, d, N, sh);
   __syncthreads();
   const int shift = bits * t.Nl;
   const uint64_t lm = (1ull << shift) - 1ull;
@@ -265,28 +305,11 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
     for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
       const uint64_t s = ((uint64_t)h << shift) | t.lolist[lbase + r];
       const uint32_t row = base + r;
-      double dg = 0.0;
-      for (int i = 0; i < N; ++i) dg += sdg[i * d + (int)((s >> (bits * (N - 1 - i))) & dm)];  // -h Sz + D Sz^2
       double off = 0.0;
-      for (int q = 0; q < p.n_bonds; ++q) {
-        const int i = b1[q], j = b2[q];
-        const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
-        const int a = (int)((s >> wi) & dm), c = (int)((s >> wj) & dm);
-        const int pr = a * d + c;
-        const int cb = bc[q];
-        for (int e = ts[pr]; e < ts[pr + 1]; ++e) {
-          const double v = tab ? cv[cb + e] : bj[0][q] * cv[3 * e] + bj[1][q] * cv[3 * e + 1] + bj[2][q] * cv[3 * e + 2];
-          const int a2 = ta[e], c2 = tc[e];
-          if (a2 == a && c2 == c) {
-            dg += v;
-          } else {
-            const uint64_t s2 = s + ((uint64_t)a2 << wi) - ((uint64_t)a << wi) + ((uint64_t)c2 << wj) -
-                                ((uint64_t)c << wj);
-            const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
-            off = fma(v, __ldg(x + rk), off);
-          }
-        }
-      }
+      const double dg = spin_row(sh, p.n_bonds, tab, N, bits, d, s, [&](double v, uint64_t s2) {
+        const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
+        off = fma(v, __ldg(x + rk), off);
+      });
       const double xi = x[row];
       const double yi = fma(dg, xi, off);
       y[row] = yi;
@@ -295,6 +318,66 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
     if (alpha_part) {
       const double tot = block_sum_all<kSpinThreads>(dot, red);
       if (threadIdx.x == 0) alpha_part[it] = tot;
+    }
+  }
+}
+
+// y = H x on a momentum sector of a spin-S model, interleaved complex: row i
+// is representative r_i (ascending); its site terms and diagonal transitions
+// multiply x_i, and an off-diagonal transition to s' adds
+// v * phase_t * n_j / n_i * x_j with (j, t) the map entry of s'
+// (hamiltonian_matrix.hpp:307-345 with the Bloch basis of
+// blochbasisstates.h:92-271).  alpha_part: one partial of Re<x, y> per
+// kMomTileRows rows.
+__global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_constant__ SpinParams p,
+                                                                   const __grid_constant__ MomParams mp,
+                                                                   const SpinDev t, const SpinMomTables m,
+                                                                   const double2* __restrict__ x,
+                                                                   double2* __restrict__ y,
+                                                                   double* __restrict__ alpha_part) {
+  __shared__ SpinShared sh;
+  __shared__ double pre[kMaxTrans], pim[kMaxTrans];
+  __shared__ double red[33];
+  const int d = t.d, N = t.N, bits = t.bits;
+  const bool tab = p.n_cls > 0;
+  stage_spin(p, d, N, sh);
+  for (int q = threadIdx.x; q < mp.n_trans; q += kSpinThreads) {
+    pre[q] = mp.phase_re[q];
+    pim[q] = mp.phase_im[q];
+  }
+  __syncthreads();
+  const int shift = bits * t.Nl;
+  const uint64_t lm = (1ull << shift) - 1ull;
+  const uint32_t jmask = (1u << kMomRepBits) - 1u;
+  const int64_t ntile = mom_tiles(m.dim);
+  for (int64_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    double dot = 0.0;
+    for (int u = 0; u < kMomTileRows / kSpinThreads; ++u) {
+      const int64_t i = tile * kMomTileRows + u * kSpinThreads + threadIdx.x;
+      if (i >= m.dim) break;
+      const uint64_t r = m.reps[i];
+      const double ni = m.norm[i];
+      double are = 0.0, aim = 0.0;
+      const double dg = spin_row(sh, p.n_bonds, tab, N, bits, d, r, [&](double v, uint64_t s2) {
+        const uint32_t e =
+            __ldg(m.map + __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm)));
+        if (e == kMomNone) return;
+        const uint32_t j = e & jmask, tt = e >> kMomRepBits;
+        const double f = v * (__ldg(m.norm + j) / ni);
+        const double cr = f * pre[tt], ci = f * pim[tt];
+        const double2 xj = x[j];
+        are = fma(cr, xj.x, fma(-ci, xj.y, are));
+        aim = fma(cr, xj.y, fma(ci, xj.x, aim));
+      });
+      const double2 xi = x[i];
+      are = fma(dg, xi.x, are);
+      aim = fma(dg, xi.y, aim);
+      y[i] = make_double2(are, aim);
+      dot = fma(xi.x, are, fma(xi.y, aim, dot));
+    }
+    if (alpha_part) {
+      const double tot = block_sum_all<kSpinThreads>(dot, red);
+      if (threadIdx.x == 0) alpha_part[tile] = tot;
     }
   }
 }
@@ -375,6 +458,90 @@ __global__ void __launch_bounds__(kSpinMeasThreads, 1)
   }
 }
 
+// <psi| sum_p O(i_p, j_p) |psi> in a spin-S momentum sector for site pairs
+// whose sum is translation invariant (mom_expect_kernel's rule with digits):
+// diagonal parts on the representative, S+_i S-_j through the map with the
+// phase and n_j / n_i of a Hamiltonian transition.
+struct SpinMomPairs {
+  int n;
+  int wi[kMomPairs], wj[kMomPairs];  // bit offsets of the digits of sites i and j
+  double m[kSpinMaxDim], cp[kSpinMaxDim], cm[kSpinMaxDim];
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(kSpinThreads) spin_mom_expect_kernel(const __grid_constant__ MomParams mp,
+                                                                       const SpinDev t, const SpinMomTables m,
+                                                                       const double2* __restrict__ psi,
+                                                                       const __grid_constant__ SpinMomPairs a,
+                                                                       double* __restrict__ part) {
+  __shared__ double pre[kMaxTrans], pim[kMaxTrans];
+  __shared__ double red[33];
+  for (int q = threadIdx.x; q < mp.n_trans; q += kSpinThreads) {
+    pre[q] = mp.phase_re[q];
+    pim[q] = mp.phase_im[q];
+  }
+  __syncthreads();
+  const int shift = t.bits * t.Nl, d = t.d;
+  const uint64_t lm = (1ull << shift) - 1ull;
+  const uint32_t dm = (1u << t.bits) - 1u;
+  const uint32_t jmask = (1u << kMomRepBits) - 1u;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kSpinThreads + threadIdx.x; i < m.dim;
+       i += (int64_t)gridDim.x * kSpinThreads) {
+    const uint64_t r = m.reps[i];
+    const double2 pi = psi[i];
+    const double w = pi.x * pi.x + pi.y * pi.y;
+    double dsum = 0.0;  // diagonal part of the pair sum on r
+    double ore = 0.0;   // Re conj(psi_i) (off-diagonal part applied to psi)_i
+    for (int p = 0; p < a.n; ++p) {
+      const int wi = a.wi[p];
+      const int da = (int)((r >> wi) & dm);
+      if (KIND == kMeasSz) {
+        dsum += a.m[da];
+      } else if (KIND == kMeasSzSz) {
+        dsum += a.m[da] * a.m[(int)((r >> a.wj[p]) & dm)];
+      } else if (wi == a.wj[p]) {
+        dsum += a.cm[da] * a.cm[da];
+      } else {
+        const int wj = a.wj[p];
+        const int dc = (int)((r >> wj) & dm);
+        if (da + 1 >= d || dc == 0) continue;
+        const uint64_t s2 = r + (1ull << wi) - (1ull << wj);
+        const uint32_t e =
+            __ldg(m.map + __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm)));
+        if (e == kMomNone) continue;
+        const uint32_t j = e & jmask, tt = e >> kMomRepBits;
+        const double f = a.cp[da] * a.cm[dc] * (__ldg(m.norm + j) / m.norm[i]);
+        const double cr = f * pre[tt], ci = f * pim[tt];
+        const double2 xj = psi[j];
+        const double yr = cr * xj.x - ci * xj.y, yi = cr * xj.y + ci * xj.x;
+        ore += pi.x * yr + pi.y * yi;
+      }
+    }
+    acc += w * dsum + ore;
+  }
+  const double tot = block_sum_all<kSpinThreads>(acc, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+// Sz, <v+1|S+|v> and <v-1|S-|v> of every digit v of spin S = (d - 1) / 2.
+void spin_factors(int d, double* m, double* cp, double* cm) {
+  const double S = d / 2.0 - 0.5;
+  for (int v = 0; v < d; ++v) {
+    const double mv = v - S;
+    m[v] = mv;
+    cp[v] = v + 1 < d ? std::sqrt(S * (S + 1) - mv * (mv + 1)) : 0.0;
+    cm[v] = v > 0 ? std::sqrt(S * (S + 1) - mv * (mv - 1)) : 0.0;
+  }
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 }  // namespace
 
 int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
@@ -394,13 +561,7 @@ int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const 
   double* part = static_cast<double*>(w);
   std::vector<double> hp((size_t)grid * kMeasPairs);
   SpinMeasArgs a{};
-  const double S = t.d / 2.0 - 0.5;
-  for (int v = 0; v < t.d; ++v) {
-    const double m = v - S;
-    a.m[v] = m;
-    a.cp[v] = v + 1 < t.d ? std::sqrt(S * (S + 1) - m * (m + 1)) : 0.0;
-    a.cm[v] = v > 0 ? std::sqrt(S * (S + 1) - m * (m - 1)) : 0.0;
-  }
+  spin_factors(t.d, a.m, a.cp, a.cm);
   for (int p0 = 0; p0 < n; p0 += kMeasPairs) {
     a.np = std::min(kMeasPairs, n - p0);
     for (int p = 0; p < a.np; ++p) {
@@ -422,6 +583,57 @@ int spin_measure_pairs(aed_handle* h, const double* psi, int kind, int n, const 
     }
   }
   return AED_OK;
+}
+
+int spin_mom_expectation(aed_handle* h, const double* psi, int kind, int n, const int32_t* si, const int32_t* sj,
+                         double* out) {
+  *out = 0.0;
+  if (n <= 0 || h->dim == 0) return AED_OK;
+  const SpinDev& t = h->sdev;
+  const SpinMomTables m = h->spin_mom_tables();
+  const int grid = mom_expect_grid(h->dim);
+  void* w = nullptr;
+  int rc = handle_workspace(h, 1, (size_t)grid * 8, &w);
+  if (rc) return rc;
+  double* part = static_cast<double*>(w);
+  std::vector<double> hp((size_t)grid);
+  SpinMomPairs a{};
+  spin_factors(t.d, a.m, a.cp, a.cm);
+  const double2* p2 = reinterpret_cast<const double2*>(psi);
+  double total = 0.0;
+  for (int p0 = 0; p0 < n; p0 += kMomPairs) {
+    a.n = std::min(kMomPairs, n - p0);
+    for (int p = 0; p < a.n; ++p) {
+      a.wi[p] = t.bits * (t.N - 1 - si[p0 + p]);
+      a.wj[p] = kind == kMeasSz ? 0 : t.bits * (t.N - 1 - sj[p0 + p]);
+    }
+    switch (kind) {
+      case kMeasSz:
+        spin_mom_expect_kernel<kMeasSz><<<grid, kSpinThreads, 0, h->stream>>>(*h->mp, t, m, p2, a, part);
+        break;
+      case kMeasSzSz:
+        spin_mom_expect_kernel<kMeasSzSz><<<grid, kSpinThreads, 0, h->stream>>>(*h->mp, t, m, p2, a, part);
+        break;
+      default:
+        spin_mom_expect_kernel<kMeasSpSm><<<grid, kSpinThreads, 0, h->stream>>>(*h->mp, t, m, p2, a, part);
+        break;
+    }
+    if ((rc = check_launch_counted("spin_mom_expect_kernel"))) return rc;
+    AED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part, hp.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (double v : hp) total += v;
+  }
+  *out = total;
+  return AED_OK;
+}
+
+int launch_spin_mom_hv(const SpinParams& p, const MomParams& mp, const SpinDev& t, const SpinMomTables& m,
+                       const double* x, double* y, double* alpha_part, cudaStream_t st) {
+  if (m.dim == 0) return AED_OK;
+  const int64_t tiles = mom_tiles(m.dim), cap = (int64_t)sm_count() * 8;
+  spin_mom_hv_kernel<<<(int)(tiles < cap ? tiles : cap), kSpinThreads, 0, st>>>(
+      p, mp, t, m, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), alpha_part);
+  return check_launch_counted("spin_mom_hv_kernel");
 }
 
 int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st) {

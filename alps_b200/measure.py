@@ -182,8 +182,11 @@ def _pair_sum(ham, psi, a, b, pairs) -> float:
         diff = [(i, j) for i, j in pairs if i != j]
         same = [i for i, j in pairs if i == j]
         v = momentum_sum(ham, psi, OBS_SPSM, [j for i, j in diff], [i for i, j in diff]) if diff else 0.0
-        if same:  # S- S+ on one site: the projector on spin down, 1/2 - Sz
-            v += 0.5 * len(same) - momentum_sum(ham, psi, OBS_SZ, same)
+        if same:
+            if getattr(ham, "two_s", 1) == 1:  # S- S+ on one site: the projector on spin down, 1/2 - Sz
+                v += 0.5 * len(same) - momentum_sum(ham, psi, OBS_SZ, same)
+            else:  # S- S+ = S+ S- - 2 Sz on one site
+                v += momentum_sum(ham, psi, OBS_SPSM, same, same) - 2.0 * momentum_sum(ham, psi, OBS_SZ, same)
         return v
     return 0.0
 

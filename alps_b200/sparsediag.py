@@ -3,8 +3,8 @@
 Reference paths are relative to the ALPS source tree.
 
 `run(params)` follows DiagMatrix::dostep (applications/diag/diag.h:85-137) for
-the Sz-conserved spin-1/2 models the engine handles: when `Sz_total` is not
-given, every Sz_total from -N/2 to N/2 (step 1; diag.h:142-175 takes the range
+the Sz-conserved spin models the engine handles (local_S = 1/2 .. 2): when
+`Sz_total` is not given, every Sz_total from -N S to N S (step 1; diag.h:142-175 takes the range
 from the site bases) is a sector, each solved by SparseDiagMatrix::do_subspace
 (here `Hamiltonian.solve`, NUMBER_EIGENVALUES / MAX_ITERATIONS from the
 parameters); a fixed `Sz_total` gives one sector without quantum-number labels,
@@ -75,10 +75,8 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
             else:
                 if label_k:
                     qn.append(("TOTAL_MOMENTUM", momentum_label(k)))
-                if mp["two_s"] != 1:
-                    raise AEDError(-1, "momentum sectors: local spin 1/2 only (set TRANSLATION_SYMMETRY=false)")
                 ham = Hamiltonian(mp["n_sites"], mp["n_up"], mp["bonds"], FP64, device, mp["site_h"], mp["site_d"],
-                                  translations=lattice_translations(params, k))
+                                  translations=lattice_translations(params, k), two_s=mp["two_s"])
             try:
                 if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
                     continue

@@ -122,8 +122,8 @@ int aed_empty_cache(int device);
  * _CORRELATIONS and _STRUCTURE_FACTOR (applications/diag/diag.h:191-314 via
  * calculate(), :316-339), for the spin operators Sz, Splus, Sminus of the
  * handle's local spin (spin-1/2 handles of aed_create, spin-S handles of
- * aed_create_spin; models.xml.in:24-36).  Sz sectors only (not momentum
- * sectors). */
+ * aed_create_spin; models.xml.in:24-36).  Sz sectors only (momentum
+ * sectors: aed_momentum_expectation). */
 int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
                     const int32_t* site_j, double* out);
 /* Momentum sectors: <psi| sum_p O(site_i[p], site_j[p]) |psi> (the real part)
@@ -177,6 +177,15 @@ int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr,
  * [offset, offset + count) of a momentum sector; either array may be NULL
  * (bloch_basis_states' states and normalization(i)). */
 int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count);
+/* A momentum sector of a spin-S Sz sector (local spin S = two_s / 2, the
+ * states and Hamiltonian of aed_create_spin): the Bloch basis and matrix
+ * elements of aed_create_momentum over the spin-S states (DiagMatrix with
+ * TRANSLATION_SYMMETRY for local_S > 1/2).  aed_spin_basis lists its
+ * representatives (64-bit packed digits), aed_momentum_basis their
+ * normalisations (states NULL); vectors, solves and aed_momentum_expectation
+ * as for aed_create_momentum. */
+int aed_create_spin_momentum(const aed_model_desc* model, int32_t two_s, const aed_translations* tr, int device,
+                             aed_handle** out);
 /* Momenta the sparsediag sector loop visits for a parameter file
  * (DiagMatrix::dostep, applications/diag/diag.h:93-114): TOTAL_MOMENTUM when
  * given, else every momentum of lattice.translation_momenta()

@@ -1,4 +1,4 @@
-"""Oracle restatement of ALPS momentum (Bloch) sectors for spin-1/2 models.
+"""Oracle restatement of ALPS momentum (Bloch) sectors for spin models.
 
 TEST INFRASTRUCTURE ONLY: used by tests/ to check the engine's momentum
 sectors; the engine has its own implementation (alps_b200/csrc/momentum.cu,
@@ -22,7 +22,9 @@ Restates (paths relative to the ALPS source tree):
   * the TOTAL_MOMENTUM label: write_vector with 20 significant digits
                                        src/alps/utility/vectorio.hpp:170-180
 States are integers with site i at bit n-1-i and spin up = 1, so that integer
-order is the reference's basis order (site 0 most significant, index 0 = down).
+order is the reference's basis order (site 0 most significant, index 0 = down);
+spin-S states pack the digit m + S of every site in `bits` bits the same way
+(bloch_basis_of, translate_digits, hamiltonian_from_sector).
 Pinned by tests/golden/bloch_example13/14/15.json (the reference's
 test/model/example13-15.output).
 """
@@ -125,21 +127,36 @@ def translate(state: int, mp, n: int) -> int:
     return out
 
 
+def translate_digits(state: int, mp, n: int, bits: int) -> int:
+    """A translation of a spin-S state packed with `bits` bits per site (site 0 most significant)."""
+    out = 0
+    mask = (1 << bits) - 1
+    for i in range(n):
+        out |= ((state >> (bits * (n - 1 - i))) & mask) << (bits * (n - 1 - mp[i]))
+    return out
+
+
 def bloch_basis(n: int, n_up, trans):
     """bloch_basis_states::build for spin-1/2 sites (n_up = None: no Sz constraint).
 
     Returns dict(reps=[state], norm=[float], rep_of={state: (representative index, phase)})."""
+    states = (s for s in range(1 << n) if n_up is None or bin(s).count("1") == n_up)
+    return bloch_basis_of(states, n, trans, lambda s, mp: translate(s, mp, n))
+
+
+def bloch_basis_of(states, n: int, trans, translate_fn):
+    """bloch_basis_states::build over `states` in basis order (any site basis whose states translate
+    with translate_fn(state, site map))."""
     l = math.sqrt(float(n))
     reps, norm = [], []
     rep_of = {}
-    for s in range(1 << n):
-        if n_up is not None and bin(s).count("1") != n_up:
-            continue
+    for s in states:
+        s = int(s)
         rep_number = None
         ph = 1.0 + 0.0j
         phase_sum = 1.0 + 0.0j
         for phase, mp in trans[1:]:
-            t = translate(s, mp, n)
+            t = translate_fn(s, mp)
             if t > s:
                 continue
             if t == s:
@@ -200,4 +217,23 @@ def hamiltonian(n: int, bonds, basis, site_h=None, site_d=None) -> np.ndarray:
             for new_state, val in (terms[::-1] if a else terms):
                 if val != 0.0:
                     add(i, new_state, val)
+    return M
+
+
+def hamiltonian_from_sector(H, states, basis) -> np.ndarray:
+    """Dense complex M of the Bloch basis from the sector's real matrix H over `states` (basis order):
+    M(i, j) += <s|H|r_i> * phase * n_j / n_i for every state s with H[s, r_i] != 0 that maps to
+    representative j (hamiltonian_matrix.hpp:307-345; any site basis)."""
+    reps, norm, rep_of = basis["reps"], basis["norm"], basis["rep_of"]
+    index = {int(s): k for k, s in enumerate(states)}
+    Hc = H.tocsc()
+    M = np.zeros((len(reps), len(reps)), dtype=complex)
+    for i, r in enumerate(reps):
+        col = index[int(r)]
+        for k in range(Hc.indptr[col], Hc.indptr[col + 1]):
+            hit = rep_of.get(int(states[Hc.indices[k]]))
+            if hit is None:
+                continue
+            j, phase = hit
+            M[i, j] += Hc.data[k] * (phase * norm[j] / norm[i])
     return M

@@ -160,14 +160,14 @@ def measure(states, psi, params, two_s=1) -> dict:
     return out
 
 
-def measure_translation_invariant(states, psi, params) -> dict:
+def measure_translation_invariant(states, psi, params, two_s=1) -> dict:
     """perform_measurements with translation invariance (diag.h:213, 236-258): no local values, each
     correlation the mean over all site pairs of its distance class; averages and structure factors as
     in measure()."""
     ext, per, coords = _geometry(params)
     n_sites = len(coords)
     out = measure(states, psi, {k: v for k, v in params.items() if not str(k).startswith("MEASURE_CORRELATIONS")
-                                and not str(k).startswith("MEASURE_LOCAL")})
+                                and not str(k).startswith("MEASURE_LOCAL")}, two_s)
     req = requests(params)
     nd = _num_distances(ext, per)
     for name, (a, b) in req["correlations"].items():
@@ -175,7 +175,7 @@ def measure_translation_invariant(states, psi, params) -> dict:
         for i in range(n_sites):
             for j in range(n_sites):
                 d = _distance(ext, per, coords[i], coords[j])
-                tot[d] += _expect(states, psi, n_sites, [(a, i), (b, j)])
+                tot[d] += _expect(states, psi, n_sites, [(a, i), (b, j)], two_s)
                 cnt[d] += 1
         out["correlations"][name] = [t / c if c else 0.0 for t, c in zip(tot, cnt)]
     return out

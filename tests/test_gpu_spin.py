@@ -190,3 +190,90 @@ def test_sparsediag_spin_one_measurements():
     d0 = c["Diagonal spin correlations"][0] + 0.5 * (c["Offdiagonal spin correlations"][0] +
                                                       c["Reverse offdiagonal"][0])
     assert abs(d0 - 2.0) < 1e-9
+
+
+SPIN_MOM_CASES = [(2, "chain lattice", {"L": 6}), (3, "chain lattice", {"L": 5}), (4, "chain lattice", {"L": 4}),
+                  (2, "square lattice", {"L": 2, "W": 3})]
+
+
+@pytest.mark.parametrize("two_s,lat,geo", SPIN_MOM_CASES, ids=[f"2S={c[0]}-{c[1]}" for c in SPIN_MOM_CASES])
+def test_spin_s_momentum_sectors_match_oracle(two_s, lat, geo):
+    """Spin-S momentum sectors (aed_create_spin_momentum): representatives equal the oracle's Bloch basis
+    over packed digits, normalisations to 1e-14, H x equal to the oracle's complex matrix (built from the
+    sector's Kronecker-product H) to 1e-12 of sum |M_ij x_j|, the lowest eigenvalues to 1e-10, and the
+    dimensions over all momenta add up to the Sz sector's."""
+    from oracle import bloch
+    rng = np.random.default_rng(two_s * 13 + len(geo))
+    n, _, graph = lattice.lattice_graph(lat, geo)
+    bonds = [(s, t, 1.0, 0.9, 0.15) for s, t, _ in graph]
+    h, dd = [0.1] * n, [0.25] * n
+    bits = two_s.bit_length()
+    p = dict(geo, MODEL="spin", LATTICE=lat, CONSERVED_QUANTUMNUMBERS="Sz")
+    for T in (n * two_s // 2, n * two_s // 2 - 1):
+        H = ospin.hamiltonian(n, two_s, bonds, h, dd, digit_sum=T)
+        states = ospin.packed_states(n, two_s, T)
+        total = 0
+        for k in ed.lattice_momenta(p):
+            tr = ed.lattice_translations(p, k)
+            b = bloch.bloch_basis_of(states, n, tr, lambda s, mp: bloch.translate_digits(s, mp, n, bits))
+            ham = ed.Hamiltonian(n, T, bonds, site_h=h, site_d=dd, translations=tr, two_s=two_s)
+            try:
+                assert ham.dim == len(b["reps"]), k
+                total += ham.dim
+                if ham.dim == 0:
+                    continue
+                st, nm = ham.momentum_basis()
+                assert np.array_equal(st, np.array(b["reps"], np.uint64)), k
+                assert np.allclose(nm, b["norm"], rtol=1e-14, atol=0), k
+                M = bloch.hamiltonian_from_sector(H, states, b)
+                x = rng.normal(size=ham.dim) + 1j * rng.normal(size=ham.dim)
+                y = ham.apply(x)
+                bound = 1e-12 * (np.abs(M) @ np.abs(x)) + 1e-14
+                assert np.all(np.abs(y - M @ x) <= bound), k
+                ev = np.sort(np.linalg.eigvals(M).real)
+                r = ham.solve(nev=1, seed=3)
+                assert r["converged"] and abs(r["evals"][0] - ev[0]) < 1e-10, k
+            finally:
+                ham.close()
+        assert total == len(states)
+
+
+def test_sparsediag_spin_one_momentum_loop():
+    """local_S = 1 with the reference's default TRANSLATION_SYMMETRY: every (Sz, TOTAL_MOMENTUM) sector, whose
+    lowest values over all momenta equal each Sz sector's ground state without translation symmetry."""
+    L = 6
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": L, "J": 1, "D": 0.2, "local_S": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz", "NUMBER_EIGENVALUES": 1}
+    res = sparsediag.run(p)
+    plain = sparsediag.run(dict(p, TRANSLATION_SYMMETRY="false"))
+    names = {tuple(q[0] for q in s["quantumnumbers"]) for s in res["sectors"]}
+    assert names == {("Sz", "TOTAL_MOMENTUM")}
+    for s0 in plain["sectors"]:
+        sz = s0["quantumnumbers"][0][1]
+        lows = [s["energies"][0] for s in res["sectors"] if s["quantumnumbers"][0][1] == sz]
+        assert abs(min(lows) - s0["energies"][0]) < 1e-10, sz
+    assert abs(res["ground_state_energy"] - plain["ground_state_energy"]) < 1e-10
+
+
+def test_spin_s_momentum_sector_measurements():
+    """Spin-1 ring with translation symmetry: the sector of the (non-degenerate) Sz=0 ground state reports
+    the class-averaged correlations, the average and the structure factors the oracle computes on the dense
+    ground state (1e-8)."""
+    from oracle import measure as omeasure
+    L = 6
+    meas = {k: v for k, v in SPIN_MEAS.items() if "LOCAL" not in k}
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": L, "J": 1, "D": 0.2, "local_S": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0, "NUMBER_EIGENVALUES": 1, **meas}
+    res = sparsediag.run(p)
+    best = min(res["sectors"], key=lambda s: s["energies"][0])
+    got = best["measurements"][0]
+    H = ospin.hamiltonian(L, 2, _chain(L), None, [0.2] * L, digit_sum=L)
+    w, Z = np.linalg.eigh(H.toarray())
+    assert abs(w[0] - best["energies"][0]) < 1e-9 and w[1] - w[0] > 1e-6
+    ref = omeasure.measure_translation_invariant(ospin.packed_states(L, 2, L), Z[:, 0], p, 2)
+    assert got["local"] == {}
+    for key in ref:
+        for name in ref[key]:
+            a, b = np.asarray(got[key][name], float), np.asarray(ref[key][name], float)
+            assert a.shape == b.shape, (key, name)
+            assert np.allclose(a, b, atol=1e-8), (key, name, a, b)

@@ -298,3 +298,43 @@ def test_measure_oracle_spin_s_operators_match_kronecker_products(two_s, n):
         got = omeasure._expect(states, psi, n, ops, two_s)
         ref = ospin.pair_expectation(n, two_s, T, psi, ops)
         assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (ops, got, ref)
+
+
+def test_bloch_matrix_from_the_sector_matrix_equals_the_spin_half_restatement():
+    """hamiltonian_from_sector (any site basis) on the spin-1/2 sector matrix gives the spin-1/2 Bloch
+    matrix of bloch.hamiltonian at every momentum of an 8-site ring with nnn bonds and a field."""
+    from oracle import spin as ospin
+    n, n_up = 8, 4
+    bonds = [(i, (i + 1) % n, 1.0, 0.8, 0.0) for i in range(n)] + [(i, (i + 2) % n, 0.3, 0.3, 0.0) for i in range(n)]
+    h = [0.15] * n
+    H = ospin.hamiltonian(n, 1, bonds, h, None, digit_sum=n_up)
+    states = ospin.packed_states(n, 1, n_up)
+    for k in bloch.translation_momenta("chain lattice", {"L": n}):
+        tr = bloch.translations("chain lattice", {"L": n}, k)
+        basis = bloch.bloch_basis(n, n_up, tr)
+        M1 = bloch.hamiltonian(n, bonds, basis, site_h=h)
+        M2 = bloch.hamiltonian_from_sector(H, states, basis)
+        assert np.allclose(M1, M2, atol=1e-13)
+
+
+@pytest.mark.parametrize("two_s,L", [(2, 6), (3, 4), (4, 4)])
+def test_spin_s_momentum_sectors_partition_the_sz_spectrum(two_s, L):
+    """Spin-S Bloch sectors (bloch_basis_of over packed digits): dimensions add up to the Sz sector's,
+    and the union of the momentum spectra is its spectrum (ring with exchange, biquadratic, field and
+    single-ion terms)."""
+    from oracle import spin as ospin
+    bits = two_s.bit_length()
+    bonds = [(i, (i + 1) % L, 1.0, 0.9, 0.2) for i in range(L)]
+    T = L * two_s // 2
+    H = ospin.hamiltonian(L, two_s, bonds, [0.1] * L, [0.3] * L, digit_sum=T)
+    states = ospin.packed_states(L, two_s, T)
+    evs, dims = [], 0
+    for k in bloch.translation_momenta("chain lattice", {"L": L}):
+        tr = bloch.translations("chain lattice", {"L": L}, k)
+        basis = bloch.bloch_basis_of(states, L, tr, lambda s, mp: bloch.translate_digits(s, mp, L, bits))
+        dims += len(basis["reps"])
+        if basis["reps"]:
+            M = bloch.hamiltonian_from_sector(H, states, basis)
+            evs += list(np.linalg.eigvals(M).real)
+    assert dims == len(states)
+    assert np.allclose(np.sort(evs), np.linalg.eigvalsh(H.toarray()), atol=1e-10)
