@@ -191,10 +191,6 @@ namespace {
 
 constexpr int kSpinThreads = 256;
 
-__device__ __forceinline__ int digit_of(uint64_t s, int site, int N, int bits) {
-  return (int)((s >> (bits * (N - 1 - site))) & ((1u << bits) - 1u));
-}
-
 __global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, int64_t offset, int64_t count) {
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= count) return;
@@ -214,25 +210,31 @@ __global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, i
   out[n] = ((uint64_t)h << (t.bits * t.Nl)) | t.lolist[t.looff[t.T - sum] + r];
 }
 
-// The couplings of SpinParams staged in shared memory for the row walk.
+// The couplings of SpinParams staged in shared memory for the row walk.  A
+// state is a hi word (the first Nh = N - Nl sites) and a lo word (the last Nl
+// sites), each with `bits` bits per site; bw1 / bw2 are the shifts of a bond's
+// two digits within their words and bk its kind: 0 both sites in lo, 1 both
+// in hi, 2 site i in hi and j in lo, 3 site i in lo and j in hi.
 struct SpinShared {
   double cv[kSpinMaxCls * kSpinMaxTrans];  // tabulated elements, or A, B, C of each transition
-  uint8_t ta[kSpinMaxTrans], tc[kSpinMaxTrans];
+  short2 dl[kSpinMaxTrans];                // digit changes (a2 - a, c2 - c) of each transition
   int ts[kSpinMaxPairs + 1];
-  int b1[kMaxBonds], b2[kMaxBonds], bc[kMaxBonds];
+  int bw1[kMaxBonds], bw2[kMaxBonds], bk[kMaxBonds], bc[kMaxBonds];
   double bj[3][kMaxBonds];
   double sdg[kSpinMaxSites * kSpinMaxDim];
 };
 
-// Fill sh (all threads of the CTA; the caller synchronises).
-__device__ __forceinline__ void stage_spin(const SpinParams& p, int d, int N, SpinShared& sh) {
+// Fill sh (all threads of the CTA); returns whether this thread staged a
+// nonzero site term (the caller reduces it with __syncthreads_or, which is
+// also the barrier after the staging).
+__device__ __forceinline__ int stage_spin(const SpinParams& p, const SpinDev& t, SpinShared& sh) {
+  const int d = t.d, N = t.N, bits = t.bits, Nl = t.Nl, Nh = N - Nl;
   const int ntr = p.tstart[d * d];
   const bool tab = p.n_cls > 0;
   for (int q = threadIdx.x; q <= d * d; q += blockDim.x) sh.ts[q] = p.tstart[q];
-  for (int q = threadIdx.x; q < ntr; q += blockDim.x) {
-    sh.ta[q] = p.trans[q].a2;
-    sh.tc[q] = p.trans[q].c2;
-  }
+  for (int pr = threadIdx.x; pr < d * d; pr += blockDim.x)
+    for (int e = p.tstart[pr]; e < p.tstart[pr + 1]; ++e)
+      sh.dl[e] = make_short2((short)(p.trans[e].a2 - pr / d), (short)(p.trans[e].c2 - pr % d));
   if (tab) {
     for (int q = threadIdx.x; q < p.n_cls * ntr; q += blockDim.x) sh.cv[q] = p.cval[q / ntr][q % ntr];
   } else {
@@ -243,40 +245,68 @@ __device__ __forceinline__ void stage_spin(const SpinParams& p, int d, int N, Sp
     }
   }
   for (int q = threadIdx.x; q < p.n_bonds; q += blockDim.x) {
-    sh.b1[q] = p.s1[q];
-    sh.b2[q] = p.s2[q];
+    const int i = p.s1[q], j = p.s2[q];
+    const bool li = i >= Nh, lj = j >= Nh;
+    sh.bw1[q] = li ? bits * (N - 1 - i) : bits * (Nh - 1 - i);
+    sh.bw2[q] = lj ? bits * (N - 1 - j) : bits * (Nh - 1 - j);
+    sh.bk[q] = (li && lj) ? 0 : (!li && !lj) ? 1 : !li ? 2 : 3;
     sh.bc[q] = tab ? p.cls[q] * ntr : 0;
     sh.bj[0][q] = p.jz[q];
     sh.bj[1][q] = p.jxy[q];
     sh.bj[2][q] = p.kq[q];
   }
-  for (int q = threadIdx.x; q < N * d; q += blockDim.x) sh.sdg[q] = p.sdiag[q / d][q % d];
+  int nz = 0;
+  for (int q = threadIdx.x; q < N * d; q += blockDim.x) {
+    sh.sdg[q] = p.sdiag[q / d][q % d];
+    nz |= sh.sdg[q] != 0.0;
+  }
+  return nz;
 }
 
-// One row of H on state s: returns its diagonal element (site terms, then the
-// diagonal transitions of the bonds in order) and calls off(v, s2) for every
-// off-diagonal transition to state s2, bonds in order.
+// One row of H: state (h, lo), its block's first row `base` and its rank r
+// within the block (row = base + r).  Returns the diagonal element (site
+// terms in site order unless all are zero, then the diagonal transitions of
+// the bonds in order) and calls off(v, rank) for every off-diagonal
+// transition, bonds in order.  A bond inside lo keeps the hi word (rank =
+// base + tlo[lo']), a bond inside hi keeps lo (rank = thi[h'] + r); only
+// bonds across the split rank through both tables.
 template <class Off>
-__device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bool tab, int N, int bits, int d,
-                                           uint64_t s, Off&& off) {
+__device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bool tab, bool has_site,
+                                           const SpinDev& t, uint32_t h, uint32_t lo, uint32_t base, uint32_t r,
+                                           Off&& off) {
+  const int d = t.d, N = t.N, bits = t.bits, Nh = N - t.Nl;
   const uint32_t dm = (1u << bits) - 1u;
   double dg = 0.0;
-  for (int i = 0; i < N; ++i) dg += sh.sdg[i * d + (int)((s >> (bits * (N - 1 - i))) & dm)];  // -h Sz + D Sz^2
+  if (has_site) {  // -h Sz + D Sz^2
+    for (int i = 0; i < Nh; ++i) dg += sh.sdg[i * d + (int)((h >> (bits * (Nh - 1 - i))) & dm)];
+    for (int i = Nh; i < N; ++i) dg += sh.sdg[i * d + (int)((lo >> (bits * (N - 1 - i))) & dm)];
+  }
   for (int q = 0; q < n_bonds; ++q) {
-    const int i = sh.b1[q], j = sh.b2[q];
-    const int wi = bits * (N - 1 - i), wj = bits * (N - 1 - j);
-    const int a = (int)((s >> wi) & dm), c = (int)((s >> wj) & dm);
+    const int k = sh.bk[q], wi = sh.bw1[q], wj = sh.bw2[q];
+    const uint32_t wa = (k == 0 || k == 3) ? lo : h;  // the word holding site i
+    const uint32_t wc = (k == 0 || k == 2) ? lo : h;  // the word holding site j
+    const int a = (int)((wa >> wi) & dm), c = (int)((wc >> wj) & dm);
     const int pr = a * d + c;
     const int cb = sh.bc[q];
     for (int e = sh.ts[pr]; e < sh.ts[pr + 1]; ++e) {
       const double v = tab ? sh.cv[cb + e]
                            : sh.bj[0][q] * sh.cv[3 * e] + sh.bj[1][q] * sh.cv[3 * e + 1] + sh.bj[2][q] * sh.cv[3 * e + 2];
-      const int a2 = sh.ta[e], c2 = sh.tc[e];
-      if (a2 == a && c2 == c) {
+      const short2 dl = sh.dl[e];
+      if (dl.x == 0 && dl.y == 0) {
         dg += v;
-      } else {
-        off(v, s + ((uint64_t)a2 << wi) - ((uint64_t)a << wi) + ((uint64_t)c2 << wj) - ((uint64_t)c << wj));
+        continue;
       }
+      const uint32_t di = (uint32_t)((int)dl.x * (1 << wi)), dj = (uint32_t)((int)dl.y * (1 << wj));
+      uint32_t rk;
+      if (k == 0)
+        rk = base + __ldg(t.tlo + (lo + di + dj));
+      else if (k == 1)
+        rk = __ldg(t.thi + (h + di + dj)) + r;
+      else if (k == 2)
+        rk = __ldg(t.thi + (h + di)) + __ldg(t.tlo + (lo + dj));
+      else
+        rk = __ldg(t.thi + (h + dj)) + __ldg(t.tlo + (lo + di));
+      off(v, rk);
     }
   }
   return dg;
@@ -287,12 +317,9 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
                                                                double* __restrict__ alpha_part) {
   __shared__ SpinShared sh;
   __shared__ double red[33];
-  const int d = t.d, N = t.N, bits = t.bits;
+  const int N = t.N, bits = t.bits;
   const bool tab = p.n_cls > 0;
-  stage_spin(p, d, N, sh);
-  __syncthreads();
-  const int shift = bits * t.Nl;
-  const uint64_t lm = (1ull << shift) - 1ull;
+  const bool has_site = __syncthreads_or(stage_spin(p, t, sh)) != 0;
   const uint32_t dm = (1u << bits) - 1u;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
     const uint32_t b = t.tile_blk[it], r0 = t.tile_r[it];
@@ -303,13 +330,11 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
     const uint32_t r1 = rows < r0 + kSpinTileRows ? rows : r0 + kSpinTileRows;
     double dot = 0.0;
     for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
-      const uint64_t s = ((uint64_t)h << shift) | t.lolist[lbase + r];
+      const uint32_t lo = t.lolist[lbase + r];
       const uint32_t row = base + r;
       double off = 0.0;
-      const double dg = spin_row(sh, p.n_bonds, tab, N, bits, d, s, [&](double v, uint64_t s2) {
-        const uint32_t rk = __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm));
-        off = fma(v, __ldg(x + rk), off);
-      });
+      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, h, lo, base, r,
+                                 [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
       const double xi = x[row];
       const double yi = fma(dg, xi, off);
       y[row] = yi;
@@ -338,15 +363,14 @@ __global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_
   __shared__ SpinShared sh;
   __shared__ double pre[kMaxTrans], pim[kMaxTrans];
   __shared__ double red[33];
-  const int d = t.d, N = t.N, bits = t.bits;
   const bool tab = p.n_cls > 0;
-  stage_spin(p, d, N, sh);
+  const int nz = stage_spin(p, t, sh);
   for (int q = threadIdx.x; q < mp.n_trans; q += kSpinThreads) {
     pre[q] = mp.phase_re[q];
     pim[q] = mp.phase_im[q];
   }
-  __syncthreads();
-  const int shift = bits * t.Nl;
+  const bool has_site = __syncthreads_or(nz) != 0;
+  const int shift = t.bits * t.Nl;
   const uint64_t lm = (1ull << shift) - 1ull;
   const uint32_t jmask = (1u << kMomRepBits) - 1u;
   const int64_t ntile = mom_tiles(m.dim);
@@ -356,11 +380,12 @@ __global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_
       const int64_t i = tile * kMomTileRows + u * kSpinThreads + threadIdx.x;
       if (i >= m.dim) break;
       const uint64_t r = m.reps[i];
+      const uint32_t rh = (uint32_t)(r >> shift), rl = (uint32_t)(r & lm);
       const double ni = m.norm[i];
       double are = 0.0, aim = 0.0;
-      const double dg = spin_row(sh, p.n_bonds, tab, N, bits, d, r, [&](double v, uint64_t s2) {
-        const uint32_t e =
-            __ldg(m.map + __ldg(t.thi + (uint32_t)(s2 >> shift)) + __ldg(t.tlo + (uint32_t)(s2 & lm)));
+      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, rh, rl, __ldg(t.thi + rh), __ldg(t.tlo + rl),
+                                 [&](double v, uint32_t rk) {
+        const uint32_t e = __ldg(m.map + rk);
         if (e == kMomNone) return;
         const uint32_t j = e & jmask, tt = e >> kMomRepBits;
         const double f = v * (__ldg(m.norm + j) / ni);

@@ -2,7 +2,7 @@
 
     python -m alps_b200.profile_spin --reps 3
 
-Workload: spin-1 Heisenberg chain L=18, Sz=0 (6,536,382 states), FP64.
+Workload: spin-1 Heisenberg chain L=18, Sz=0 (44,152,809 states), FP64.
 Prints the mean CUDA-event time per apply.
 """
 

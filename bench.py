@@ -569,7 +569,7 @@ def run_momentum(args):
 
 
 def run_spin(args):
-    """Spin-1 Heisenberg chain L=18, Sz=0 (6,536,382 states), FP64, lowest 2 eigenvalues, through the
+    """Spin-1 Heisenberg chain L=18, Sz=0 (44,152,809 states), FP64, lowest 2 eigenvalues, through the
     spin-S engine (local_S = 1); apply roofline from the sampled mean of off-diagonal terms per row."""
     import alps_b200 as ed
 
