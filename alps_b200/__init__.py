@@ -146,6 +146,7 @@ def lib():
             "aed_set_couplings": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc)]),
             "aed_dimension": (ctypes.c_int, [_P, _I64P]),
             "aed_basis_copy": (ctypes.c_int, [_P, _U32P, _I64, _I64]),
+            "aed_basis_state": (ctypes.c_int, [_P, _I64, ctypes.POINTER(ctypes.c_uint64)]),
             "aed_index": (ctypes.c_int, [_P, _U32P, _I64, _I64P]),
             "aed_vec_alloc": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
             "aed_vec_free": (ctypes.c_int, [_P, _P]),
@@ -458,6 +459,12 @@ class Hamiltonian:
         out = np.empty(count, np.uint32)
         _check(lib().aed_basis_copy(self._h, out.ctypes.data_as(_U32P), offset, count))
         return out
+
+    def state(self, idx: int) -> int:
+        """The state of row idx (aed_basis_state): bit string, representative or packed digits."""
+        out = ctypes.c_uint64(0)
+        _check(lib().aed_basis_state(self._h, int(idx), ctypes.byref(out)))
+        return out.value
 
     def index(self, states):
         st = np.ascontiguousarray(states, dtype=np.uint32)

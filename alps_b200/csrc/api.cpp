@@ -1047,6 +1047,16 @@ int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t co
   return rc;
 }
 
+int aed_basis_state(aed_handle* h, int64_t idx, uint64_t* state) {
+  if (!h || !state) return fail(AED_ERR_INVALID, "NULL argument");
+  if (idx < 0 || idx >= h->dim) return fail(AED_ERR_INVALID, "index outside the basis");
+  if (h->gen) return aed_spin_basis(h, state, idx, 1);
+  uint32_t s = 0;
+  const int rc = aed_basis_copy(h, &s, idx, 1);
+  if (!rc) *state = s;
+  return rc;
+}
+
 int aed_index(aed_handle* h, const uint32_t* host_states, int64_t count, int64_t* host_idx) {
   if (!h || ((!host_states || !host_idx) && count > 0)) return fail(AED_ERR_INVALID, "NULL argument");
   if (h->mom || h->gen) return fail(AED_ERR_INVALID, "aed_index: spin-1/2 Sz sectors only");

@@ -216,6 +216,11 @@ const char* aed_last_error(void);
 /* Basis states [offset, offset+count) as bit strings (site s <-> bit N-1-s,
  * up = 1), in the reference's order (basisstates.h:175-278).  host_out is host memory. */
 int aed_basis_copy(aed_handle* h, uint32_t* host_out, int64_t offset, int64_t count);
+/* The state of row idx, widened to 64 bits, for any kind of handle: the bit
+ * string of a spin-1/2 Sz sector, the representative of a momentum sector, the
+ * packed digits of a spin-S sector (element idx of basis_states, a
+ * std::vector of states, src/alps/model/basisstates.h:44-46). */
+int aed_basis_state(aed_handle* h, int64_t idx, uint64_t* state);
 
 /* Ranks of `count` host bit strings through the device tables: the row index
  * of each state, or D when the state is outside the sector

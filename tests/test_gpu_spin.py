@@ -277,3 +277,21 @@ def test_spin_s_momentum_sector_measurements():
             a, b = np.asarray(got[key][name], float), np.asarray(ref[key][name], float)
             assert a.shape == b.shape, (key, name)
             assert np.allclose(a, b, atol=1e-8), (key, name, a, b)
+
+
+def test_basis_state_of_every_kind_of_handle():
+    """aed_basis_state: row idx of a spin-1/2 Sz sector, a spin-1/2 momentum sector, a spin-S Sz sector and a
+    spin-S momentum sector equals the handle's basis listing at that row; out-of-range rows are refused."""
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": 6, "CONSERVED_QUANTUMNUMBERS": "Sz"}
+    k = ed.lattice_momenta(p)[1]
+    tr = ed.lattice_translations(p, k)
+    bonds = _chain(6)
+    hams = [ed.Hamiltonian(6, 3, bonds), ed.Hamiltonian(6, 3, bonds, translations=tr),
+            ed.Hamiltonian(6, 6, bonds, two_s=2), ed.Hamiltonian(6, 6, bonds, translations=tr, two_s=2)]
+    for ham in hams:
+        listing = ham.momentum_basis()[0] if ham.momentum else ham.basis()
+        for idx in (0, ham.dim // 2, ham.dim - 1):
+            assert ham.state(idx) == int(listing[idx])
+        with pytest.raises(ed.AEDError):
+            ham.state(ham.dim)
+        ham.close()
