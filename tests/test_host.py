@@ -284,3 +284,26 @@ def test_measurement_geometry_matches_oracle(lat, geo):
     for cc in coords:
         ks.append([2 * np.pi * ((x - L) if x > L // 2 else x) / L for x, L in zip(cc, ext)])
     assert np.allclose(g.momenta(), ks)
+
+
+def test_spin_momentum_constructor_checks_translations_before_the_device():
+    """aed_create_spin_momentum refuses translations that are not permutations of the sites, or that do not
+    start with the identity, before it looks for a device; spin-S momentum handles are FP64 only."""
+    n = 4
+    s1 = np.arange(n, dtype=np.int32)
+    s2 = ((np.arange(n) + 1) % n).astype(np.int32)
+    j = np.ones(n)
+    desc = ed.ModelDesc(n, n, n, s1.ctypes.data_as(ed._I32P), s2.ctypes.data_as(ed._I32P), ed._dp(j), ed._dp(j),
+                        None, None, None)
+    ph = np.array([1.0, 0.0, 1.0, 0.0])
+    h = ed._P()
+    for maps, msg in (([0, 1, 2, 3, 1, 1, 2, 3], "permutation"), ([1, 2, 3, 0, 0, 1, 2, 3], "identity")):
+        mp = np.array(maps, dtype=np.int32)
+        tr = ed.Translations(2, mp.ctypes.data_as(ed._I32P), ed._dp(ph))
+        rc = ed.lib().aed_create_spin_momentum(ctypes.byref(desc), 2, ctypes.byref(tr), 0, ctypes.byref(h))
+        assert rc == ed.ERR_INVALID
+        assert msg in ed.lib().aed_last_error().decode()
+    tr = [(1.0 + 0j, [0, 1, 2, 3]), (1.0 + 0j, [1, 2, 3, 0])]
+    with pytest.raises(ed.AEDError, match="FP64"):
+        ed.Hamiltonian(n, n, [(i, (i + 1) % n, 1.0, 1.0) for i in range(n)], precision=ed.FP32, translations=tr,
+                       two_s=2)
