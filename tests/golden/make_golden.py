@@ -9,6 +9,7 @@ Reads (paths relative to the ALPS source tree) and writes JSON beside this scrip
   test/model/example12.output   -> basis_example12.json  (2x2 square, Sz_total = 0)
   test/model/example3.output    -> spin_terms_example3.json (HSpinSite, HSpinBond)
   test/model/example4.output    -> spin_half_example4.json  (two-site HSpinHalf)
+                                   spin_one_example4.json   (two-site HSpinOne, local_S = 1)
   test/lattice/example5.output  -> lattice_example5.json (anisotropic square 10x4 sites)
   test/lattice/example6.output  -> lattice_example6.json (anisotropic square 10x4 bonds)
   test/model/example13.output   -> bloch_example13.json (4-site chain, Bloch bases at k = 2 pi m / 4)
@@ -137,6 +138,10 @@ def main(alps):
     out["spin_half_example4.json"] = {
         "source": "test/model/example4.output",
         "HSpinHalf": _nested(_block(t, "HSpinHalf")),
+    }
+    out["spin_one_example4.json"] = {
+        "source": "test/model/example4.output",
+        "HSpinOne": _nested(_block(t, "HSpinOne")),
     }
     t = open(os.path.join(alps, "test/lattice/example5.output")).read()
     sites = []

@@ -2,6 +2,7 @@
 
 import json
 import os
+import re
 
 import numpy as np
 import pytest
@@ -77,9 +78,11 @@ def test_lattice_example6_bonds():
 
 
 def _eval_matrix_expr(expr, vals):
+    """A matrix element of the reference's symbolic output at the given couplings (numbers, + - * /, parens)."""
     e = expr.replace(" ", "")
     for k, v in vals.items():
-        e = e.replace(k, f"({v!r})")
+        e = e.replace(k, f"({float(v)!r})")
+    assert re.fullmatch(r"[0-9eE.+\-*/()]*", e), expr
     return eval(e) if e else 0.0
 
 
@@ -338,3 +341,38 @@ def test_spin_s_momentum_sectors_partition_the_sz_spectrum(two_s, L):
             evs += list(np.linalg.eigvals(M).real)
     assert dims == len(states)
     assert np.allclose(np.sort(evs), np.linalg.eigvalsh(H.toarray()), atol=1e-10)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_spin_s_oracle_at_spin_half_matches_example3_example4(seed):
+    """The spin-S oracle's operator algebra (S+-, exchange_xy, biquadratic = (exchange_xy + Sz Sz)^2, site terms
+    -h Sz + D Sz^2) at S = 1/2 reproduces the reference's HSpinBond (example3) and HSpinHalf (example4) at
+    random couplings: rows/columns in the two-site product order (0,0), (0,1), (1,0), (1,1)."""
+    from oracle import spin as ospin
+    rng = np.random.default_rng(seed)
+    jz, jxy, k, h, d = rng.uniform(-2, 2, 5)
+    vals = {"Jz0": jz, "Jxy0": jxy, "K0": k, "h0": h, "D0": d, "Gamma0": 0.0}
+    g4 = np.array(_nested_eval(gold("spin_half_example4.json")["HSpinHalf"], vals), dtype=float)
+    H = ospin.hamiltonian(2, 1, [(0, 1, jz, jxy, k)], [h, h], [d, d]).toarray()
+    np.testing.assert_allclose(H, g4, rtol=0, atol=1e-13)
+    g3 = np.array(_nested_eval(gold("spin_terms_example3.json")["HSpinBond"], vals), dtype=float)
+    B = ospin.hamiltonian(2, 1, [(0, 1, jz, jxy, k)]).toarray()
+    for is1 in range(2):
+        for is2 in range(2):
+            for js1 in range(2):
+                for js2 in range(2):
+                    assert abs(B[(is1 << 1) | is2, (js1 << 1) | js2] - g3[is1][is2][js1][js2]) < 1e-13
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_spin_s_oracle_at_spin_one_matches_example4(seed):
+    """The spin-S oracle at S = 1 (two sites, one bond with Jz, Jxy and biquadratic K, site terms h and D)
+    equals the reference's HSpinOne (example4, local_S = 1) at random couplings; Gamma = 0 (the engine
+    rejects it), so every remaining coefficient is printed exactly (0, 1, 2)."""
+    from oracle import spin as ospin
+    rng = np.random.default_rng(10 + seed)
+    jz, jxy, k, h, d = rng.uniform(-2, 2, 5)
+    vals = {"Jz0": jz, "Jxy0": jxy, "K0": k, "h0": h, "D0": d, "Gamma0": 0.0}
+    g = np.array(_nested_eval(gold("spin_one_example4.json")["HSpinOne"], vals), dtype=float)
+    H = ospin.hamiltonian(2, 2, [(0, 1, jz, jxy, k)], [h, h], [d, d]).toarray()
+    np.testing.assert_allclose(H, g, rtol=0, atol=1e-12)
