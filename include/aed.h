@@ -131,7 +131,9 @@ int aed_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, con
  * of one distance class; *out gets the sum.  What perform_measurements
  * accumulates over the pairs of a distance class in a translation-invariant
  * sector (applications/diag/diag.h:236-258) before dividing by the class's
- * multiplicity, and over all pairs for the structure factor (:262-307). */
+ * multiplicity, and over all pairs for the structure factor (:262-307).
+ * Spin-1/2 and spin-S momentum sectors (aed_create_momentum,
+ * aed_create_spin_momentum). */
 int aed_momentum_expectation(aed_handle* h, const void* psi, int32_t kind, int32_t n, const int32_t* site_i,
                              const int32_t* site_j, double* out);
 /* Lattice of a parameter file: dimension, extents and periodic flags
@@ -175,7 +177,8 @@ typedef struct {
 int aed_create_momentum(const aed_model_desc* model, const aed_translations* tr, int device, aed_handle** out);
 /* Representatives (states as in aed_basis_copy) and normalisations of rows
  * [offset, offset + count) of a momentum sector; either array may be NULL
- * (bloch_basis_states' states and normalization(i)). */
+ * (bloch_basis_states' states and normalization(i)).  A spin-S sector's
+ * representatives are 64-bit: states must be NULL (aed_spin_basis lists them). */
 int aed_momentum_basis(aed_handle* h, uint32_t* states, double* norms, int64_t offset, int64_t count);
 /* A momentum sector of a spin-S Sz sector (local spin S = two_s / 2, the
  * states and Hamiltonian of aed_create_spin): the Bloch basis and matrix
