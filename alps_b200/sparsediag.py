@@ -21,6 +21,7 @@ archive, diag.hpp:112-124, needs h5py, which this image lacks.)
 
 from __future__ import annotations
 
+import re
 from fractions import Fraction
 from xml.sax.saxutils import escape
 
@@ -36,14 +37,124 @@ def half_integer_text(v: Fraction) -> str:
     return str(twice // 2) if twice % 2 == 0 else f"{twice}/2"
 
 
-def _site_count(params: dict) -> int:
-    """Number of sites of the lattice (the parser needs a compatible Sz_total)."""
+_VALUE_CHARS = set("#'()*+-./^_")
+
+
+def parameter_list(text: str) -> list:
+    """The tasks of an ALPS parameter file (alps::ParameterList::parse, src/alps/parameter/parameterlist.C:16-40
+    with the grammars of parameterlist_p.h:35-47, parameters_p.h:19-26 and parameter_p.h:22-41): `key=value`
+    assignments separated by ';', ',' or line ends set global values; a `{ ... }` block is one task, the
+    globals at that point plus its own assignments (an empty block: the globals alone); `#clear` drops the
+    globals, `#stop` ends the list; blanks and // and /* */ comments are skipped.  Keys start with a letter
+    and continue with letters, digits, _ ' # or a [...] suffix; values are "..." or '...' or a run of
+    letters, digits and # ' ( ) * + - . / ^ _.  Returns one dict of string values per task."""
+    s = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    s = re.sub(r"//[^\n]*", "", s)
+    n, i = len(s), 0
+    glob, tasks = {}, []
+
+    def err(msg):
+        line = s.count("\n", 0, i) + 1
+        raise AEDError(-1, f"parameter list, line {line}: {msg}")
+
+    def skip(eol):
+        nonlocal i
+        while i < n and (s[i] in " \t\r" or (eol and s[i] == "\n")):
+            i += 1
+
+    def assignment(target):
+        nonlocal i
+        j = i
+        if not s[i].isalpha():
+            err(f"a parameter name expected at {s[i:i + 20]!r}")
+        i += 1
+        while i < n and (s[i].isalnum() or s[i] in "_'#" or s[i] == "["):
+            if s[i] == "[":
+                k = s.find("]", i)
+                if k < 0:
+                    err("unterminated [ in a parameter name")
+                i = k
+            i += 1
+        key = s[j:i]
+        skip(False)
+        if i >= n or s[i] != "=":
+            err(f"'=' expected after {key}")
+        i += 1
+        skip(False)
+        if i < n and s[i] in "\"'":
+            k = s.find(s[i], i + 1)
+            if k < 0:
+                err(f"unterminated string for {key}")
+            val, i = s[i + 1:k], k + 1
+        else:
+            j = i
+            while i < n and (s[i].isalnum() or s[i] in _VALUE_CHARS or s.startswith("${", i)):
+                if s.startswith("${", i):
+                    k = s.find("}", i)
+                    if k < 0:
+                        err("unterminated ${")
+                    i = k
+                i += 1
+            val = s[j:i]
+        target[key] = val
+        skip(False)
+        if i < n and s[i] in ";,":
+            i += 1
+
+    while True:
+        skip(True)
+        if i >= n:
+            break
+        if s.startswith("#stop", i):
+            break
+        if s.startswith("#clear", i):
+            glob.clear()
+            i += len("#clear")
+            skip(False)
+            if i < n and s[i] == ";":
+                i += 1
+            continue
+        if s[i] == "{":
+            i += 1
+            local = dict(glob)
+            while True:
+                skip(True)
+                if i >= n:
+                    err("unterminated {")
+                if s[i] == "}":
+                    i += 1
+                    break
+                assignment(local)
+            tasks.append(local)
+            continue
+        assignment(glob)
+    return tasks
+
+
+def run_list(text: str, precision=FP64, device=0, seed=0) -> list:
+    """run() for every task of a parameter file (parameter_list): [(task parameters, result)]."""
+    return [(p, run(p, precision=precision, device=device, seed=seed)) for p in parameter_list(text)]
+
+
+def _site_info(params: dict):
+    """(number of sites, 2 S) of the model (the parser needs a compatible Sz_total: 0 or 1/2)."""
     for trial in (0, 0.5):
         try:
-            return model_from_parameters(dict(params, Sz_total=trial))["n_sites"]
+            m = model_from_parameters(dict(params, Sz_total=trial))
+            return m["n_sites"], m["two_s"]
         except AEDError:
             continue
     raise AEDError(-1, "cannot read the lattice from the parameters")
+
+
+def sz_sectors(params: dict) -> list:
+    """The Sz_total values of the sector loop: [None] (one unlabelled sector) when Sz_total is given or Sz is
+    not conserved, else -N S .. N S in steps of 1 (diag.h:142-175)."""
+    qns = str(params.get("CONSERVED_QUANTUMNUMBERS", "")).replace(",", " ").split()
+    if "Sz_total" in params or "Sz" not in qns:
+        return [None]
+    n, two_s = _site_info(params)
+    return [Fraction(k, 2) for k in range(-n * two_s, n * two_s + 1, 2)]
 
 
 def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
@@ -51,15 +162,8 @@ def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
     "dimension": D, "iterations": m}], "ground_state_energy": E0, "energy_gap": gap}.  Momentum sectors
     run in FP64 whatever `precision` says."""
     params = dict(params)
-    qns = str(params.get("CONSERVED_QUANTUMNUMBERS", "")).replace(",", " ").split()
     sectors = []
-    if "Sz_total" in params or "Sz" not in qns:
-        sz_values = [None]
-    else:  # Sz_total from -N S to N S in steps of 1 (diag.h:142-175)
-        n = _site_count(params)
-        two_s = model_from_parameters(dict(params, Sz_total=0 if n % 2 == 0 else 0.5))["two_s"] \
-            if "local_S" in params else 1
-        sz_values = [Fraction(k, 2) for k in range(-n * two_s, n * two_s + 1, 2)]
+    sz_values = sz_sectors(params)
     momenta = lattice_momenta(params)
     req = _measure.requests(params)
     measuring = any(req.values())

@@ -307,3 +307,38 @@ def test_spin_momentum_constructor_checks_translations_before_the_device():
     with pytest.raises(ed.AEDError, match="FP64"):
         ed.Hamiltonian(n, n, [(i, (i + 1) % n, 1.0, 1.0) for i in range(n)], precision=ed.FP32, translations=tr,
                        two_s=2)
+
+
+def test_parameter_list_tasks():
+    """ALPS parameter files: globals, one task per { } block with the globals at that point, separators ; , and
+    line ends, quoted values, bracketed and primed keys, comments, #clear and #stop."""
+    from alps_b200 import sparsediag
+    txt = ('MODEL="spin";\nLATTICE="chain lattice";  // nearest neighbours\nCONSERVED_QUANTUMNUMBERS="Sz";\n'
+           'local_S=1;\nJ=1;\nSz_total=0\n{L=4}\n{L=6}\nSz_total=1\n'
+           "{ L=4, J'=0.5; MEASURE_AVERAGE[Magnetization]=Sz }\n/* { L=99 } */\n{}\n#clear\n{ L = 3 }\n#stop\n{ L=100 }\n")
+    tasks = sparsediag.parameter_list(txt)
+    assert [t.get("L") for t in tasks] == ["4", "6", "4", None, "3"]
+    assert [t.get("Sz_total") for t in tasks] == ["0", "0", "1", "1", None]
+    assert tasks[2]["J'"] == "0.5" and tasks[2]["MEASURE_AVERAGE[Magnetization]"] == "Sz"
+    assert tasks[0]["LATTICE"] == "chain lattice" and tasks[4] == {"L": "3"}
+    m = ed.model_from_parameters(tasks[1])
+    assert (m["n_sites"], m["two_s"], m["n_up"]) == (6, 2, 6)
+    m = ed.model_from_parameters(tasks[2])
+    assert (m["n_sites"], m["two_s"], m["n_up"]) == (4, 2, 5)
+    with pytest.raises(ed.AEDError, match="line 2"):
+        sparsediag.parameter_list("L=4\n{ J=1 ")
+    with pytest.raises(ed.AEDError, match="'='"):
+        sparsediag.parameter_list("L 4")
+
+
+@pytest.mark.parametrize("local_s,L,expect", [("1/2", 5, [f"{k}/2" for k in range(-5, 6, 2)]),
+                                              ("1", 5, [str(k) for k in range(-5, 6)]),
+                                              ("3/2", 3, [f"{k}/2" for k in range(-9, 10, 2)]),
+                                              ("2", 2, [str(k) for k in range(-4, 5)])])
+def test_sz_sector_loop_covers_minus_ns_to_ns(local_s, L, expect):
+    """Without Sz_total the loop runs Sz_total = -N S .. N S in steps of 1, odd chains of integer spin included."""
+    from alps_b200 import sparsediag
+    p = {"MODEL": "spin", "LATTICE": "chain lattice", "L": L, "local_S": local_s, "J": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz"}
+    assert [sparsediag.half_integer_text(v) for v in sparsediag.sz_sectors(p)] == expect
+    assert sparsediag.sz_sectors(dict(p, Sz_total=0)) == [None]
