@@ -295,3 +295,19 @@ def test_basis_state_of_every_kind_of_handle():
         with pytest.raises(ed.AEDError):
             ham.state(ham.dim)
         ham.close()
+
+
+def test_parameter_file_with_odd_spin_one_chain():
+    """A parameter file of two spin-1 chain tasks (L = 5 and 4, every Sz sector) through sparsediag.run_list: the
+    odd chain loops over Sz_total = -5 .. 5, and every sector's lowest value equals the oracle's dense spectrum."""
+    txt = ('MODEL="spin"; LATTICE="chain lattice"; CONSERVED_QUANTUMNUMBERS="Sz"; local_S=1; J=1;\n'
+           'TRANSLATION_SYMMETRY=false; NUMBER_EIGENVALUES=1\n{ L=5 }\n{ L=4; D=0.3 }\n')
+    out = sparsediag.run_list(txt)
+    assert [p["L"] for p, _ in out] == ["5", "4"]
+    for (p, res), dd in zip(out, (0.0, 0.3)):
+        L = int(p["L"])
+        labels = [s["quantumnumbers"][0][1] for s in res["sectors"]]
+        assert labels == [str(k) for k in range(-L, L + 1)]
+        for s, T in zip(res["sectors"], range(0, 2 * L + 1)):
+            H = ospin.hamiltonian(L, 2, _chain(L), None, [dd] * L, digit_sum=T)
+            assert abs(s["energies"][0] - np.linalg.eigvalsh(H.toarray())[0]) < 1e-10
