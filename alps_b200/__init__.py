@@ -125,6 +125,9 @@ def lib():
             "aed_last_error": (ctypes.c_char_p, []),
             "aed_parse_parameters": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ParamInfo), _I32P, _I32P, _DP,
                                                     _DP, _DP, _DP, _DP, _I32, _I32]),
+            "aed_parse_graph_parameters": (ctypes.c_int, [ctypes.c_char_p, _I32, _I32P, _I32, _I32P, _I32P, _I32P,
+                                                          ctypes.POINTER(ParamInfo), _I32P, _I32P, _DP, _DP, _DP,
+                                                          _DP, _DP, _I32, _I32]),
             "aed_create": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(_P)]),
             "aed_destroy": (ctypes.c_int, [_P]),
@@ -255,6 +258,80 @@ def parse_parameters(text: str):
             "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
 
 
+def read_graph(path: str, name: str):
+    """<GRAPH name="..."> of a lattice library file (read_graph_xml, src/alps/lattice/graph.h:121-222):
+    (number of vertices, vertex types, edges [(source, target, type)] in file order), vertices numbered from
+    0; None when the file holds no graph of that name.  A VERTEX without id takes the next number of its
+    own counter, types default to 0, and an edge to a vertex beyond the list adds it."""
+    import xml.etree.ElementTree as ET
+    root = ET.parse(path).getroot()
+    for g in ([root] if root.tag == "GRAPH" else root.iter("GRAPH")):
+        if g.get("name") != name:
+            continue
+        fixed = bool(g.get("vertices"))
+        vtype = [0] * (int(g.get("vertices")) if fixed else 0)
+        counter, edges = 0, []
+        for el in g:
+            if el.tag == "VERTEX":
+                if el.get("id"):
+                    vid = int(el.get("id")) - 1
+                else:
+                    vid, counter = counter, counter + 1
+                if vid >= len(vtype):
+                    if fixed:
+                        raise AEDError(ERR_INVALID, f"graph {name!r}: too many vertices in <GRAPH>")
+                    vtype += [0] * (vid + 1 - len(vtype))
+                vtype[vid] = int(el.get("type") or 0)
+            elif el.tag == "EDGE":
+                edges.append((int(el.get("source")) - 1, int(el.get("target")) - 1, int(el.get("type") or 0)))
+            else:
+                raise AEDError(ERR_INVALID, f"graph {name!r}: illegal element <{el.tag}> in <GRAPH>")
+        n = max([len(vtype)] + [max(a, b) + 1 for a, b, _ in edges])
+        return n, vtype + [0] * (n - len(vtype)), edges
+    return None
+
+
+def graph_of(params):
+    """The <GRAPH> a parameter dict names (graph_helper::make_graph, src/alps/lattice/graph_helper.h:653-684):
+    GRAPH, or a LATTICE that LATTICE_LIBRARY holds as a <GRAPH>; None for the built-in lattices."""
+    if not isinstance(params, dict):
+        return None
+    has_g, has_l = "GRAPH" in params, "LATTICE" in params
+    if has_g and has_l:
+        raise AEDError(ERR_INVALID, "both GRAPH and LATTICE were specified")
+    name = str(params.get("GRAPH", params.get("LATTICE", ""))).strip().strip('"')
+    lib_path = str(params.get("LATTICE_LIBRARY", "")).strip().strip('"')
+    g = read_graph(lib_path, name) if lib_path and os.path.isfile(lib_path) else None
+    if g is None and has_g:
+        raise AEDError(ERR_INVALID, f"GRAPH {name!r} not found (LATTICE_LIBRARY must name the file holding it)")
+    return g
+
+
+def parse_graph_parameters(text: str, graph):
+    """parse_parameters for a graph (n, vertex types, edges) instead of a built-in lattice
+    (aed_parse_graph_parameters)."""
+    n, vtype, edges = graph
+    vt = np.ascontiguousarray(vtype, dtype=np.int32)
+    es = np.ascontiguousarray([e[0] for e in edges] or [0], dtype=np.int32)
+    et = np.ascontiguousarray([e[1] for e in edges] or [0], dtype=np.int32)
+    ey = np.ascontiguousarray([e[2] for e in edges] or [0], dtype=np.int32)
+    ne = len(edges)
+    info = ParamInfo()
+    args = (text.encode(), n, vt.ctypes.data_as(_I32P), ne, es.ctypes.data_as(_I32P), et.ctypes.data_as(_I32P),
+            ey.ctypes.data_as(_I32P), ctypes.byref(info))
+    _check(lib().aed_parse_graph_parameters(*args, None, None, None, None, None, None, None, 0, 0))
+    nb, ns = info.n_bonds, info.n_sites
+    s1, s2 = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+    jz, jxy, kq = np.zeros(max(nb, 1)), np.zeros(max(nb, 1)), np.zeros(max(nb, 1))
+    sh, sd = np.zeros(ns), np.zeros(ns)
+    _check(lib().aed_parse_graph_parameters(*args, s1.ctypes.data_as(_I32P), s2.ctypes.data_as(_I32P), _dp(jz),
+                                            _dp(jxy), _dp(kq), _dp(sh), _dp(sd), nb, ns))
+    bonds = [(int(s1[b]), int(s2[b]), float(jz[b]), float(jxy[b]), float(kq[b])) for b in range(nb)]
+    return {"n_sites": ns, "n_up": info.n_up, "bonds": bonds, "nev": info.number_eigenvalues,
+            "max_iter": info.max_iterations, "two_s": info.two_s,
+            "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
+
+
 def _params_text(params) -> str:
     if isinstance(params, dict):
         lines = []
@@ -268,13 +345,20 @@ def _params_text(params) -> str:
 
 
 def model_from_parameters(params) -> dict:
-    """dict or text of ALPS parameters -> parse_parameters() result."""
+    """dict or text of ALPS parameters -> parse_parameters() result (a dict naming a <GRAPH>: its bonds)."""
+    g = graph_of(params)
+    if g is not None:
+        return parse_graph_parameters(_params_text(params), g)
     return parse_parameters(_params_text(params))
 
 
 def lattice_momenta(params) -> list:
     """Momenta of the sparsediag sector loop (aed_lattice_momenta): TOTAL_MOMENTUM when given, else every
-    translation momentum when TRANSLATION_SYMMETRY (default true), else []."""
+    translation momentum when TRANSLATION_SYMMETRY (default true), else [].  A <GRAPH> has no translations."""
+    if graph_of(params) is not None:
+        if str(params.get("TOTAL_MOMENTUM", "")).strip():
+            raise AEDError(ERR_INVALID, "TOTAL_MOMENTUM on a GRAPH: a graph has no translations")
+        return []
     txt = _params_text(params).encode()
     n, nd = ctypes.c_int32(0), ctypes.c_int32(0)
     _check(lib().aed_lattice_momenta(txt, ctypes.byref(n), ctypes.byref(nd), None, 0))

@@ -127,7 +127,15 @@ struct ParsedParams {
   std::vector<int> s1, s2;
   std::vector<double> jz, jxy, kq, site_h, site_d;
 };
-int parse_parameters(const char* text, ParsedParams& out);
+// A graph of a lattice library (<GRAPH>, src/alps/lattice/graph.h:121-222):
+// n vertices with their types, edges (source, target, type) in file order,
+// vertices numbered from 0.
+struct GraphSpec {
+  int n = 0;
+  std::vector<int> vtype, src, tgt, etype;
+};
+// graph == nullptr: the lattice the parameters name.
+int parse_parameters(const char* text, ParsedParams& out, const GraphSpec* graph = nullptr);
 // Lattice dimension, extents and periodic flags of the parameters.
 int lattice_geometry(const char* text, int* dim, int ext[2], int periodic[2]);
 // Momenta the sector loop visits (diag.h:93-114): TOTAL_MOMENTUM when given,

@@ -405,12 +405,11 @@ extern "C" {
 
 const char* aed_last_error(void) { return last_error_cstr(); }
 
-int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy,
-                         double* kq, double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity) {
-  if (!info) return fail(AED_ERR_INVALID, "info is NULL");
-  ParsedParams pp;
-  const int rc = parse_parameters(text, pp);
-  if (rc) return rc;
+namespace {
+
+// Copy a parse result to the caller's arrays (any of them may be NULL).
+int copy_parsed(const ParsedParams& pp, aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy,
+                double* kq, double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity) {
   *info = pp.info;
   const int nb = pp.info.n_bonds;
   if (s1 || s2 || jz || jxy || kq) {
@@ -431,6 +430,42 @@ int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* s1, in
     }
   }
   return AED_OK;
+}
+
+}  // namespace
+
+int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy,
+                         double* kq, double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity) {
+  if (!info) return fail(AED_ERR_INVALID, "info is NULL");
+  if (!text) return fail(AED_ERR_INVALID, "text is NULL");
+  ParsedParams pp;
+  const int rc = parse_parameters(text, pp);
+  if (rc) return rc;
+  return copy_parsed(pp, info, s1, s2, jz, jxy, kq, site_h, site_d, bond_capacity, site_capacity);
+}
+
+int aed_parse_graph_parameters(const char* text, int32_t n_vertices, const int32_t* vertex_type, int32_t n_edges,
+                               const int32_t* edge_source, const int32_t* edge_target, const int32_t* edge_type,
+                               aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy, double* kq,
+                               double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity) {
+  if (!info || !text) return fail(AED_ERR_INVALID, "NULL argument");
+  if (n_vertices < 0 || n_edges < 0 || (n_edges > 0 && (!edge_source || !edge_target)))
+    return fail(AED_ERR_INVALID, "graph: bad vertex or edge arrays");
+  if (n_edges > kMaxBonds) return fail(AED_ERR_INVALID, "too many bonds");
+  GraphSpec g;
+  g.n = n_vertices;
+  g.vtype.assign(n_vertices, 0);
+  if (vertex_type)
+    for (int i = 0; i < n_vertices; ++i) g.vtype[i] = vertex_type[i];
+  for (int e = 0; e < n_edges; ++e) {
+    g.src.push_back(edge_source[e]);
+    g.tgt.push_back(edge_target[e]);
+    g.etype.push_back(edge_type ? edge_type[e] : 0);
+  }
+  ParsedParams pp;
+  const int rc = parse_parameters(text, pp, &g);
+  if (rc) return rc;
+  return copy_parsed(pp, info, s1, s2, jz, jxy, kq, site_h, site_d, bond_capacity, site_capacity);
 }
 
 int aed_create(const aed_model_desc* model, int precision, int device, aed_handle** out) {

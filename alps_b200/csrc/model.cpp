@@ -666,7 +666,7 @@ int lattice_translations(const char* text, const double* k, int n_k, int* n_site
   return AED_OK;
 }
 
-int parse_parameters(const char* text, ParsedParams& out) {
+int parse_parameters(const char* text, ParsedParams& out, const GraphSpec* graph) {
   Params p;
   int rc = parse_kv(text, p);
   if (rc) return rc;
@@ -686,54 +686,85 @@ int parse_parameters(const char* text, ParsedParams& out) {
       return fail(AED_ERR_INVALID, "local_S must be one of 1/2, 1, 3/2, 2");
     const std::string latname = str("LATTICE", "");
     LatticeSpec L;
-    if (!lattice_spec(latname, L)) return fail(AED_ERR_INVALID, "unsupported LATTICE \"" + latname + "\"");
+    if (!graph && !lattice_spec(latname, L))
+      return fail(AED_ERR_INVALID, "unsupported LATTICE \"" + latname + "\"");
     const std::string cq = str("CONSERVED_QUANTUMNUMBERS", "");
     if (cq.find("Sz") == std::string::npos)
       return fail(AED_ERR_INVALID, "CONSERVED_QUANTUMNUMBERS must contain Sz (full Hilbert space not supported)");
     if (!p.has("Sz_total"))
       return fail(AED_ERR_INVALID, "Sz_total must be given (one sector per handle; alps_b200.sparsediag loops over them)");
-    const int Lx = (int)std::lround(ev.name("L"));
-    int Wy = 1;
-    if (L.dim == 2) Wy = p.has("W") ? (int)std::lround(ev.name("W")) : (int)std::lround(ev.expr_str(L.ext_w_default));
-    if (Lx < 1 || Wy < 1) return fail(AED_ERR_INVALID, "lattice extents must be positive");
-    const int N = Lx * Wy;
-    if (N < 2 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 2..32");
+    // the graph: edges (source, target, type) in graph order and the type of every vertex
+    std::vector<int> esrc, etgt, etyp, vtyp;
+    int N = 0;
+    if (graph) {
+      N = graph->n;
+      if (N < 2 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 2..32");
+      if ((int)graph->vtype.size() != N) return fail(AED_ERR_INVALID, "one type per vertex expected");
+      vtyp = graph->vtype;
+      for (size_t e = 0; e < graph->src.size(); ++e) {
+        const int si = graph->src[e], ti = graph->tgt[e];
+        if (si < 0 || si >= N || ti < 0 || ti >= N) return fail(AED_ERR_INVALID, "edge vertex out of range");
+        if (si == ti) return fail(AED_ERR_INVALID, "an edge joins a vertex to itself");
+        if (graph->etype[e] < 0) return fail(AED_ERR_INVALID, "negative edge type");
+        esrc.push_back(si);
+        etgt.push_back(ti);
+        etyp.push_back(graph->etype[e]);
+      }
+      for (int t : vtyp)
+        if (t < 0) return fail(AED_ERR_INVALID, "negative vertex type");
+    } else {
+      const int Lx = (int)std::lround(ev.name("L"));
+      int Wy = 1;
+      if (L.dim == 2) Wy = p.has("W") ? (int)std::lround(ev.name("W")) : (int)std::lround(ev.expr_str(L.ext_w_default));
+      if (Lx < 1 || Wy < 1) return fail(AED_ERR_INVALID, "lattice extents must be positive");
+      N = Lx * Wy;
+      if (N < 2 || N > 32) return fail(AED_ERR_INVALID, "number of sites must be in 2..32");
+      // edges: cell by cell (last coordinate fastest), unit-cell edge order,
+      // open boundaries drop edges, self-loops are dropped (latticegraph.h:98-136)
+      const int ext[2] = {Lx, Wy};
+      for (int c = 0; c < N; ++c) {
+        int cc[2];
+        if (L.dim == 1) {
+          cc[0] = c;
+          cc[1] = 0;
+        } else {
+          cc[0] = c / Wy;
+          cc[1] = c % Wy;
+        }
+        for (int e = 0; e < L.n_edges; ++e) {
+          int src[2], tgt[2];
+          bool ok = true;
+          for (int d = 0; d < L.dim; ++d) {
+            src[d] = cc[d] + L.off_src[e][d];
+            tgt[d] = cc[d] + L.off_tgt[e][d];
+            for (int* v : {&src[d], &tgt[d]}) {
+              if (*v < 0 || *v >= ext[d]) {
+                if (!L.periodic[d]) ok = false;
+                *v = ((*v % ext[d]) + ext[d]) % ext[d];
+              }
+            }
+          }
+          if (!ok) continue;
+          const int si = L.dim == 1 ? src[0] : src[0] * Wy + src[1];
+          const int ti = L.dim == 1 ? tgt[0] : tgt[0] * Wy + tgt[1];
+          if (si == ti) continue;
+          esrc.push_back(si);
+          etgt.push_back(ti);
+          etyp.push_back(L.etype[e]);
+        }
+      }
+      vtyp.assign(N, 0);  // the supported lattices have one site type
+    }
     // the sector's digit sum Sz_total + N S (spin 1/2: the number of up spins)
     const double szt = ev.name("Sz_total");
     const double nup_d = N * two_s / 2.0 + szt;
     const int n_up = (int)std::lround(nup_d);
     if (std::fabs(nup_d - n_up) > 1e-9 || n_up < 0 || n_up > N * two_s)
       return fail(AED_ERR_INVALID, "Sz_total incompatible with the number of sites");
-    // edges: cell by cell (last coordinate fastest), unit-cell edge order,
-    // open boundaries drop edges, self-loops are dropped (latticegraph.h:98-136)
-    const int ext[2] = {Lx, Wy};
-    for (int c = 0; c < N; ++c) {
-      int cc[2];
-      if (L.dim == 1) {
-        cc[0] = c;
-        cc[1] = 0;
-      } else {
-        cc[0] = c / Wy;
-        cc[1] = c % Wy;
-      }
-      for (int e = 0; e < L.n_edges; ++e) {
-        int src[2], tgt[2];
-        bool ok = true;
-        for (int d = 0; d < L.dim; ++d) {
-          src[d] = cc[d] + L.off_src[e][d];
-          tgt[d] = cc[d] + L.off_tgt[e][d];
-          for (int* v : {&src[d], &tgt[d]}) {
-            if (*v < 0 || *v >= ext[d]) {
-              if (!L.periodic[d]) ok = false;
-              *v = ((*v % ext[d]) + ext[d]) % ext[d];
-            }
-          }
-        }
-        if (!ok) continue;
-        const int si = L.dim == 1 ? src[0] : src[0] * Wy + src[1];
-        const int ti = L.dim == 1 ? tgt[0] : tgt[0] * Wy + tgt[1];
-        if (si == ti) continue;
-        const std::string t = std::to_string(L.etype[e]);
+    {
+      for (size_t e = 0; e < esrc.size(); ++e) {
+        const int si = esrc[e], ti = etgt[e];
+        const std::string t = std::to_string(etyp[e]);
         // Jz# / Jxy# / K#: HAMILTONIAN parameters first, then BONDTERM default J#
         auto coupling = [&](const std::string& base) {
           const std::string n = base + t;
@@ -755,14 +786,23 @@ int parse_parameters(const char* text, ParsedParams& out) {
         out.kq.push_back(kq);
       }
     }
-    // site terms (site type 0): h0 = h, D0 = D, Gamma0 = Gamma
-    const double h0 = p.has("h0") ? ev.name("h0") : ev.name("h");
-    const double d0 = p.has("D0") ? ev.name("D0") : ev.name("D");
-    const double g0 = p.has("Gamma0") ? ev.name("Gamma0") : ev.name("Gamma");
-    if (g0 != 0.0) return fail(AED_ERR_INVALID, "Gamma (transverse field) breaks Sz conservation");
-    if (h0 != 0.0 || d0 != 0.0) {
-      out.site_h.assign(N, h0);
-      out.site_d.assign(N, d0);
+    // site terms of vertex type t: h# = h, D# = D, Gamma# = Gamma (SITETERM
+    // defaults, models.xml.in:360-365)
+    std::vector<double> sh(N), sd(N);
+    bool any_site = false;
+    for (int i = 0; i < N; ++i) {
+      const std::string t = std::to_string(vtyp[i]);
+      const double h = p.has("h" + t) ? ev.name("h" + t) : ev.name("h");
+      const double d = p.has("D" + t) ? ev.name("D" + t) : ev.name("D");
+      const double g = p.has("Gamma" + t) ? ev.name("Gamma" + t) : ev.name("Gamma");
+      if (g != 0.0) return fail(AED_ERR_INVALID, "Gamma (transverse field) breaks Sz conservation");
+      sh[i] = h;
+      sd[i] = d;
+      any_site = any_site || h != 0.0 || d != 0.0;
+    }
+    if (any_site) {
+      out.site_h = sh;
+      out.site_d = sd;
       out.info.has_site_terms = 1;
     }
     out.info.n_sites = N;

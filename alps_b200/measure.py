@@ -39,7 +39,7 @@ import re
 
 import numpy as np
 
-from . import AEDError, ERR_INVALID, _check, _dp, _I32P, _params_text, lib
+from . import AEDError, ERR_INVALID, _check, _dp, _I32P, _params_text, graph_of, lib
 
 OBS_SZ, OBS_SZSZ, OBS_SPSM = 0, 1, 2
 _SITE_OPS = ("Sz", "Splus", "Sminus")
@@ -67,6 +67,8 @@ class Geometry:
     """Sites, coordinates, distance classes and momenta of the lattice of a parameter set."""
 
     def __init__(self, params):
+        if graph_of(params) is not None:
+            raise AEDError(ERR_INVALID, "measurements need a lattice's coordinates and distances: not on a GRAPH")
         dim, ext, per = ctypes.c_int32(0), (ctypes.c_int32 * 2)(), (ctypes.c_int32 * 2)()
         _check(lib().aed_lattice_geometry(_params_text(params).encode(), ctypes.byref(dim), ext, per))
         self.dim = dim.value

@@ -92,6 +92,18 @@ typedef struct {
 int aed_parse_parameters(const char* text, aed_param_info* info, int32_t* bond_s1, int32_t* bond_s2,
                          double* bond_jz, double* bond_jxy, double* bond_k, double* site_h,
                          double* site_d, int32_t bond_capacity, int32_t site_capacity);
+/* The same for a graph of a lattice library (<GRAPH>: VERTEX id / type, EDGE
+ * source / target / type; read_graph_xml, src/alps/lattice/graph.h:121-222,
+ * chosen by LATTICE or GRAPH, graph_helper.h:653-684): the parameter text
+ * gives the model and sector (its LATTICE is not read); n_vertices vertices
+ * numbered from 0 with their types (NULL: all 0), n_edges edges in file order
+ * with their types (NULL: all 0).  Bond b = edge b, with the couplings of its
+ * edge type (Jz#, Jxy#, J#, K#); the site terms of a vertex are those of its
+ * type (h#, D#, defaults h, D; models.xml.in:360-371). */
+int aed_parse_graph_parameters(const char* text, int32_t n_vertices, const int32_t* vertex_type, int32_t n_edges,
+                               const int32_t* edge_source, const int32_t* edge_target, const int32_t* edge_type,
+                               aed_param_info* info, int32_t* s1, int32_t* s2, double* jz, double* jxy, double* kq,
+                               double* site_h, double* site_d, int32_t bond_capacity, int32_t site_capacity);
 
 /* ---- handles -------------------------------------------------------------- */
 typedef struct aed_handle aed_handle;

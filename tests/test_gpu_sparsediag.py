@@ -56,3 +56,30 @@ def test_fixed_sector_and_half_integer_labels():
     assert len(res["sectors"]) == 1 and res["sectors"][0]["quantumnumbers"] == []
     odd = sparsediag.run(dict(PARAMS, LATTICE="chain lattice", L=5, NUMBER_EIGENVALUES=1))
     assert [s["quantumnumbers"][0][1] for s in odd["sectors"]] == ["-5/2", "-3/2", "-1/2", "1/2", "3/2", "5/2"]
+
+
+def test_sparsediag_on_a_graph_of_a_lattice_library(tmp_path):
+    """A <GRAPH> of a lattice library (10 vertices of two types, edges of three types in file order): every Sz
+    sector's ground state equals the oracle's dense spectrum of the same bonds and site terms (1e-10)."""
+    n = 10
+    edges = [(i, (i + 1) % n, 0) for i in range(n)] + [(i, (i + 3) % n, 1) for i in range(0, n, 2)] + \
+        [(0, 5, 2), (2, 7, 2)]
+    vt = [i % 2 for i in range(n)]
+    xml = ['<LATTICES>', f'<GRAPH name="test graph" vertices="{n}">']
+    xml += [f'  <VERTEX id="{i + 1}" type="{t}"/>' for i, t in enumerate(vt)]
+    xml += [f'  <EDGE type="{t}" source="{s + 1}" target="{d + 1}"/>' for s, d, t in edges]
+    xml += ['</GRAPH>', '</LATTICES>']
+    f = tmp_path / "g.xml"
+    f.write_text("\n".join(xml))
+    J = {0: (1.0, 0.9), 1: (0.4, 0.4), 2: (0.7, 1.1)}
+    h = {0: 0.05, 1: -0.1}
+    p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "test graph", "Jz0": J[0][0], "Jxy0": J[0][1],
+         "J1": J[1][0], "Jz2": J[2][0], "Jxy2": J[2][1], "h0": h[0], "h1": h[1], "CONSERVED_QUANTUMNUMBERS": "Sz",
+         "NUMBER_EIGENVALUES": 1}
+    res = sparsediag.run(p)
+    bonds = [(s, d, J[t][0], J[t][1], 0.0) for s, d, t in edges]
+    site_h = [h[t] for t in vt]
+    assert [s["quantumnumbers"][0][1] for s in res["sectors"]] == [str(k) for k in range(-5, 6)]
+    for s, n_up in zip(res["sectors"], range(0, n + 1)):
+        w = np.linalg.eigvalsh(oracle.Matrix(n, n_up, bonds, site_h=site_h).dense())
+        assert abs(s["energies"][0] - w[0]) < 1e-10, n_up

@@ -342,3 +342,59 @@ def test_sz_sector_loop_covers_minus_ns_to_ns(local_s, L, expect):
          "CONSERVED_QUANTUMNUMBERS": "Sz"}
     assert [sparsediag.half_integer_text(v) for v in sparsediag.sz_sectors(p)] == expect
     assert sparsediag.sz_sectors(dict(p, Sz_total=0)) == [None]
+
+
+GRAPH_XML = """<LATTICES>
+<GRAPH name="two dimers" vertices="4">
+  <VERTEX id="1" type="0"/>
+  <VERTEX id="2" type="0"/>
+  <VERTEX id="3" type="1"/>
+  <VERTEX id="4" type="1"/>
+  <EDGE type="0" source="1" target="2"/>
+  <EDGE type="0" source="3" target="4"/>
+  <EDGE type="1" source="1" target="3"/>
+  <EDGE type="1" source="2" target="4"/>
+</GRAPH>
+<GRAPH name="grown">
+  <VERTEX type="2"/>
+  <VERTEX/>
+  <EDGE source="1" target="2"/>
+  <EDGE source="2" target="5" type="3"/>
+</GRAPH>
+</LATTICES>
+"""
+
+
+def test_graph_of_a_lattice_library(tmp_path):
+    """<GRAPH> lattices: vertices and edges as read_graph_xml reads them, bonds in file order with the couplings
+    of their edge type, site terms of their vertex type, no translations; GRAPH and LATTICE are exclusive."""
+    f = tmp_path / "graphs.xml"
+    f.write_text(GRAPH_XML)
+    assert ed.read_graph(str(f), "grown") == (5, [2, 0, 0, 0, 0], [(0, 1, 0), (1, 4, 3)])
+    assert ed.read_graph(str(f), "none") is None
+    p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "two dimers", "J0": 1, "J1": 0.25, "Jz1": 0.5,
+         "h1": 0.3, "D": 0.1, "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
+    m = ed.model_from_parameters(p)
+    assert (m["n_sites"], m["n_up"], m["two_s"]) == (4, 2, 1)
+    assert m["bonds"] == [(0, 1, 1.0, 1.0, 0.0), (2, 3, 1.0, 1.0, 0.0), (0, 2, 0.5, 0.25, 0.0), (1, 3, 0.5, 0.25, 0.0)]
+    assert list(m["site_h"]) == [0.0, 0.0, 0.3, 0.3] and list(m["site_d"]) == [0.1] * 4
+    g = dict(p, GRAPH="two dimers")
+    del g["LATTICE"]
+    assert ed.model_from_parameters(g)["bonds"] == m["bonds"]
+    assert ed.lattice_momenta(p) == []
+    from alps_b200 import measure, sparsediag
+    assert [sparsediag.half_integer_text(v) for v in sparsediag.sz_sectors({k: v for k, v in p.items()
+                                                                           if k != "Sz_total"})] == ["-2", "-1", "0",
+                                                                                                    "1", "2"]
+    with pytest.raises(ed.AEDError, match="both GRAPH and LATTICE"):
+        ed.model_from_parameters(dict(p, GRAPH="two dimers"))
+    with pytest.raises(ed.AEDError, match="not found"):
+        ed.model_from_parameters({k: v for k, v in g.items() if k != "LATTICE_LIBRARY"})
+    with pytest.raises(ed.AEDError, match="GRAPH"):
+        measure.Geometry(p)
+    with pytest.raises(ed.AEDError, match="translations"):
+        ed.lattice_momenta(dict(p, TOTAL_MOMENTUM="0"))
+    # a lattice library without that graph: the built-in lattices by name
+    q = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "chain lattice", "L": 4, "J": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
+    assert ed.model_from_parameters(q)["n_sites"] == 4
