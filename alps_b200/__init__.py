@@ -258,11 +258,22 @@ def parse_parameters(text: str):
             "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
 
 
+class Graph(tuple):
+    """(n, vertex types, edges [(source, target, type)]) with the vertices' coordinates (empty lists where
+    the file gives none) as .coords."""
+
+    def __new__(cls, n, vtype, edges, coords):
+        g = super().__new__(cls, (n, vtype, edges))
+        g.coords = coords
+        return g
+
+
 def read_graph(path: str, name: str):
     """<GRAPH name="..."> of a lattice library file (read_graph_xml, src/alps/lattice/graph.h:121-222):
-    (number of vertices, vertex types, edges [(source, target, type)] in file order), vertices numbered from
-    0; None when the file holds no graph of that name.  A VERTEX without id takes the next number of its
-    own counter, types default to 0, and an edge to a vertex beyond the list adds it."""
+    a Graph (number of vertices, vertex types, edges [(source, target, type)] in file order; vertex
+    COORDINATEs as .coords), vertices numbered from 0; None when the file holds no graph of that name.  A
+    VERTEX without id takes the next number of its own counter, types default to 0, and an edge to a vertex
+    beyond the list adds it."""
     import xml.etree.ElementTree as ET
     root = ET.parse(path).getroot()
     for g in ([root] if root.tag == "GRAPH" else root.iter("GRAPH")):
@@ -270,7 +281,7 @@ def read_graph(path: str, name: str):
             continue
         fixed = bool(g.get("vertices"))
         vtype = [0] * (int(g.get("vertices")) if fixed else 0)
-        counter, edges = 0, []
+        counter, edges, coords = 0, [], {}
         for el in g:
             if el.tag == "VERTEX":
                 if el.get("id"):
@@ -282,12 +293,15 @@ def read_graph(path: str, name: str):
                         raise AEDError(ERR_INVALID, f"graph {name!r}: too many vertices in <GRAPH>")
                     vtype += [0] * (vid + 1 - len(vtype))
                 vtype[vid] = int(el.get("type") or 0)
+                c = el.find("COORDINATE")
+                if c is not None and (c.text or "").strip():
+                    coords[vid] = [float(v) for v in c.text.replace(",", " ").split()]
             elif el.tag == "EDGE":
                 edges.append((int(el.get("source")) - 1, int(el.get("target")) - 1, int(el.get("type") or 0)))
             else:
                 raise AEDError(ERR_INVALID, f"graph {name!r}: illegal element <{el.tag}> in <GRAPH>")
         n = max([len(vtype)] + [max(a, b) + 1 for a, b, _ in edges])
-        return n, vtype + [0] * (n - len(vtype)), edges
+        return Graph(n, vtype + [0] * (n - len(vtype)), edges, [coords.get(i, []) for i in range(n)])
     return None
 
 

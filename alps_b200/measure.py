@@ -64,11 +64,16 @@ def requests(params: dict) -> dict:
 
 
 class Geometry:
-    """Sites, coordinates, distance classes and momenta of the lattice of a parameter set."""
+    """Sites, coordinates, distance classes and momenta of the lattice of a parameter set (a GRAPH: its
+    vertices, their coordinates, one distance class per ordered pair, no momenta)."""
 
     def __init__(self, params):
-        if graph_of(params) is not None:
-            raise AEDError(ERR_INVALID, "measurements need a lattice's coordinates and distances: not on a GRAPH")
+        g = graph_of(params)
+        self.graph = g is not None
+        if self.graph:  # no lattice: every ordered site pair is its own distance class (graph_helper.h:516-582)
+            self.n, self.dim, self.ext, self.periodic = g[0], 0, [], []
+            self.coords = g.coords
+            return
         dim, ext, per = ctypes.c_int32(0), (ctypes.c_int32 * 2)(), (ctypes.c_int32 * 2)()
         _check(lib().aed_lattice_geometry(_params_text(params).encode(), ctypes.byref(dim), ext, per))
         self.dim = dim.value
@@ -84,12 +89,16 @@ class Geometry:
             self.coords.append(cc)
 
     def num_distances(self) -> int:
+        if self.graph:
+            return self.n * self.n
         d = 1
         for L, p in zip(self.ext, self.periodic):
             d *= L if p else L * L
         return d
 
     def distance(self, i: int, j: int) -> int:
+        if self.graph:
+            return i * self.n + j
         x, y = self.coords[i], self.coords[j]
         d = 0
         for a in range(self.dim):
@@ -101,6 +110,8 @@ class Geometry:
         return d
 
     def momenta(self):
+        if self.graph:
+            raise AEDError(ERR_INVALID, "structure factors need the momenta of a lattice: not on a GRAPH")
         out = []
         for cc in self.coords:
             k = []

@@ -238,9 +238,9 @@ def _labels(params):
     for i in range(g.n):
         for j in range(g.n):
             d = g.distance(i, j)
-            if not dist[d]:
-                dist[d] = _coord(g.coords[i]) + " -- " + _coord(g.coords[j])
-    moms = [_coord(k) for k in g.momenta()]
+            if not dist[d]:  # a graph: the vertex numbers (graph_helper::distance_labels, graph_helper.h:535-553)
+                dist[d] = f"{i} -- {j}" if g.graph else _coord(g.coords[i]) + " -- " + _coord(g.coords[j])
+    moms = [] if g.graph else [_coord(k) for k in g.momenta()]
     return sites, dist, moms
 
 

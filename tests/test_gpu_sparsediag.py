@@ -83,3 +83,36 @@ def test_sparsediag_on_a_graph_of_a_lattice_library(tmp_path):
     for s, n_up in zip(res["sectors"], range(0, n + 1)):
         w = np.linalg.eigvalsh(oracle.Matrix(n, n_up, bonds, site_h=site_h).dense())
         assert abs(s["energies"][0] - w[0]) < 1e-10, n_up
+
+
+def test_measurements_on_a_graph(tmp_path):
+    """MEASURE_AVERAGE / _LOCAL / _CORRELATIONS on a <GRAPH> (one distance class per ordered vertex pair) equal the
+    oracle's operator expectations in the dense ground state (1e-8)."""
+    from oracle import measure as omeasure
+    n = 8
+    edges = [(i, (i + 1) % n) for i in range(n)] + [(0, 4), (1, 6)]
+    vt = [i % 3 for i in range(n)]
+    hs = {0: 0.07, 1: -0.05, 2: 0.11}
+    xml = ['<LATTICES>', f'<GRAPH name="ring+" vertices="{n}">']
+    xml += [f'  <VERTEX id="{i + 1}" type="{t}"/>' for i, t in enumerate(vt)]
+    xml += [f'  <EDGE source="{s + 1}" target="{d + 1}"/>' for s, d in edges]
+    xml += ['</GRAPH>', '</LATTICES>']
+    f = tmp_path / "g.xml"
+    f.write_text("\n".join(xml))
+    meas = {"MEASURE_AVERAGE[M]": "Sz", "MEASURE_LOCAL[Local]": "Sz", "MEASURE_CORRELATIONS[ZZ]": "Sz",
+            "MEASURE_CORRELATIONS[PM]": "Splus:Sminus", "MEASURE_CORRELATIONS[MP]": "Sminus:Splus"}
+    p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "ring+", "J": 1, "h0": hs[0], "h1": hs[1],
+         "h2": hs[2], "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 1, "NUMBER_EIGENVALUES": 1, **meas}
+    res = sparsediag.run(p)
+    got = res["sectors"][0]["measurements"][0]
+    bonds = [(s, d, 1.0, 1.0, 0.0) for s, d in edges]
+    M = oracle.Matrix(n, 5, bonds, site_h=[hs[t] for t in vt])
+    w, Z = np.linalg.eigh(M.dense())
+    assert abs(w[0] - res["sectors"][0]["energies"][0]) < 1e-9 and w[1] - w[0] > 1e-6
+    st, psi = M.states(), Z[:, 0]
+    ex = lambda ops: omeasure._expect(st, psi, n, ops)
+    assert abs(got["average"]["M"] - sum(ex([("Sz", i)]) for i in range(n)) / n) < 1e-8
+    np.testing.assert_allclose(got["local"]["Local"], [ex([("Sz", i)]) for i in range(n)], atol=1e-8)
+    for name, (a, b) in (("ZZ", ("Sz", "Sz")), ("PM", ("Splus", "Sminus")), ("MP", ("Sminus", "Splus"))):
+        ref = [ex([(a, i), (b, j)]) for i in range(n) for j in range(n)]
+        np.testing.assert_allclose(got["correlations"][name], ref, atol=1e-8)

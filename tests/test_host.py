@@ -390,11 +390,32 @@ def test_graph_of_a_lattice_library(tmp_path):
         ed.model_from_parameters(dict(p, GRAPH="two dimers"))
     with pytest.raises(ed.AEDError, match="not found"):
         ed.model_from_parameters({k: v for k, v in g.items() if k != "LATTICE_LIBRARY"})
-    with pytest.raises(ed.AEDError, match="GRAPH"):
-        measure.Geometry(p)
+    assert measure.Geometry(p).graph
     with pytest.raises(ed.AEDError, match="translations"):
         ed.lattice_momenta(dict(p, TOTAL_MOMENTUM="0"))
     # a lattice library without that graph: the built-in lattices by name
     q = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "chain lattice", "L": 4, "J": 1,
          "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
     assert ed.model_from_parameters(q)["n_sites"] == 4
+
+
+def test_graph_geometry_and_labels(tmp_path):
+    """Measurement geometry of a <GRAPH>: one distance class per ordered vertex pair (i N + j, labelled "i -- j"),
+    site labels from the vertices' COORDINATEs ("(  )" without), no momenta (structure factors refused)."""
+    from alps_b200 import measure, sparsediag
+    f = tmp_path / "g.xml"
+    f.write_text('<LATTICES><GRAPH name="tri" vertices="3">'
+                 '<VERTEX id="1"><COORDINATE>0 0</COORDINATE></VERTEX><VERTEX id="2"><COORDINATE>1 0</COORDINATE>'
+                 '</VERTEX><VERTEX id="3"/>'
+                 '<EDGE source="1" target="2"/><EDGE source="2" target="3"/><EDGE source="3" target="1"/>'
+                 '</GRAPH></LATTICES>')
+    p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "tri", "J": 1, "CONSERVED_QUANTUMNUMBERS": "Sz",
+         "MEASURE_CORRELATIONS[C]": "Sz"}
+    g = measure.Geometry(p)
+    assert g.graph and g.n == 3 and g.num_distances() == 9
+    assert [g.distance(i, j) for i in range(3) for j in range(3)] == list(range(9))
+    sites, dist, moms = sparsediag._labels(p)
+    assert sites == ["( 0,0 )", "( 1,0 )", "(  )"]
+    assert dist[:4] == ["0 -- 0", "0 -- 1", "0 -- 2", "1 -- 0"] and moms == []
+    with pytest.raises(ed.AEDError, match="momenta"):
+        g.momenta()
