@@ -10,6 +10,7 @@ Reads (paths relative to the ALPS source tree) and writes JSON beside this scrip
   test/model/example3.output    -> spin_terms_example3.json (HSpinSite, HSpinBond)
   test/model/example4.output    -> spin_half_example4.json  (two-site HSpinHalf)
                                    spin_one_example4.json   (two-site HSpinOne, local_S = 1)
+  test/lattice/label.output     -> labels_square4.json (4x4 square: site, bond, momentum, distance labels)
   test/lattice/example5.output  -> lattice_example5.json (anisotropic square 10x4 sites)
   test/lattice/example6.output  -> lattice_example6.json (anisotropic square 10x4 bonds)
   test/model/example13.output   -> bloch_example13.json (4-site chain, Bloch bases at k = 2 pi m / 4)
@@ -142,6 +143,19 @@ def main(alps):
     out["spin_one_example4.json"] = {
         "source": "test/model/example4.output",
         "HSpinOne": _nested(_block(t, "HSpinOne")),
+    }
+    t = open(os.path.join(alps, "test/lattice/label.output")).read()
+    sec, lab = None, {}
+    for line in t.splitlines():
+        if line.endswith("labels:"):
+            sec = line[:-len(" labels:")].lower()
+            lab[sec] = []
+        elif sec and line.strip():
+            lab[sec].append(line.strip())
+    out["labels_square4.json"] = {
+        "source": "test/lattice/label.output",
+        "params": {"LATTICE": "square lattice", "L": 4},
+        "sites": lab["site"], "bonds": lab["bond"], "momenta": lab["momenta"], "distances": lab["distance"],
     }
     t = open(os.path.join(alps, "test/lattice/example5.output")).read()
     sites = []

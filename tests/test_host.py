@@ -419,3 +419,19 @@ def test_graph_geometry_and_labels(tmp_path):
     assert dist[:4] == ["0 -- 0", "0 -- 1", "0 -- 2", "1 -- 0"] and moms == []
     with pytest.raises(ed.AEDError, match="momenta"):
         g.momenta()
+
+
+def test_xml_labels_match_the_reference_label_output():
+    """Site, bond, momentum and distance labels of the 4x4 square lattice (the index values of the XML
+    eigenstate measurements) equal the reference's test/lattice/label.output; the bond labels follow the
+    engine's bond list, so they also pin its bond order."""
+    from alps_b200 import sparsediag
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "labels_square4.json")))
+    p = {"MODEL": "spin", "LATTICE": "square lattice", "L": 4, "J": 1, "CONSERVED_QUANTUMNUMBERS": "Sz",
+         "Sz_total": 0}
+    sites, dist, moms = sparsediag._labels(p)
+    assert sites == g["sites"]
+    assert moms == g["momenta"]
+    assert dist == g["distances"]
+    bonds = ed.model_from_parameters(p)["bonds"]
+    assert [f"{sites[a]} -- {sites[b]}" for a, b, *_ in bonds] == g["bonds"]
