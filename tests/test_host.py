@@ -435,3 +435,30 @@ def test_xml_labels_match_the_reference_label_output():
     assert dist == g["distances"]
     bonds = ed.model_from_parameters(p)["bonds"]
     assert [f"{sites[a]} -- {sites[b]}" for a, b, *_ in bonds] == g["bonds"]
+
+
+def test_graph_parameters_refuse_bad_graphs():
+    """aed_parse_graph_parameters: an edge joining a vertex to itself, an edge vertex out of range, a negative
+    type, too many edges or sites are refused with a message."""
+    text = 'MODEL="spin"\nJ=1\nCONSERVED_QUANTUMNUMBERS="Sz"\nSz_total=0\n'.encode()
+
+    def parse(n, edges, vtype=None):
+        info = ed.ParamInfo()
+        src = np.array([e[0] for e in edges] or [0], np.int32)
+        tgt = np.array([e[1] for e in edges] or [0], np.int32)
+        typ = np.array([e[2] for e in edges] or [0], np.int32)
+        vt = None if vtype is None else np.array(vtype, np.int32).ctypes.data_as(ed._I32P)
+        rc = ed.lib().aed_parse_graph_parameters(text, n, vt, len(edges), src.ctypes.data_as(ed._I32P),
+                                                 tgt.ctypes.data_as(ed._I32P), typ.ctypes.data_as(ed._I32P),
+                                                 ctypes.byref(info), None, None, None, None, None, None, None, 0, 0)
+        return rc, ed.lib().aed_last_error().decode(), info
+
+    rc, _, info = parse(4, [(0, 1, 0), (1, 2, 0), (2, 3, 1)])
+    assert rc == 0 and (info.n_sites, info.n_bonds, info.n_up) == (4, 3, 2)
+    for n, edges, vtype, msg in ((4, [(1, 1, 0)], None, "itself"), (4, [(0, 4, 0)], None, "out of range"),
+                                 (4, [(0, 1, -1)], None, "negative edge type"),
+                                 (4, [(0, 1, 0)], [0, -2, 0, 0], "negative vertex type"),
+                                 (40, [(0, 1, 0)], None, "number of sites"),
+                                 (4, [(0, 1, 0)] * 129, None, "too many bonds")):
+        rc, err, _ = parse(n, edges, vtype)
+        assert rc == ed.ERR_INVALID and msg in err, (msg, err)
