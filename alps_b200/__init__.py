@@ -315,7 +315,14 @@ def graph_of(params):
         raise AEDError(ERR_INVALID, "both GRAPH and LATTICE were specified")
     name = str(params.get("GRAPH", params.get("LATTICE", ""))).strip().strip('"')
     lib_path = str(params.get("LATTICE_LIBRARY", "")).strip().strip('"')
-    g = read_graph(lib_path, name) if lib_path and os.path.isfile(lib_path) else None
+    g = None
+    if lib_path and os.path.isfile(lib_path):
+        import xml.etree.ElementTree as ET
+        try:
+            g = read_graph(lib_path, name)
+        except ET.ParseError as e:
+            if has_g:
+                raise AEDError(ERR_INVALID, f"LATTICE_LIBRARY {lib_path!r}: {e}") from None
     if g is None and has_g:
         raise AEDError(ERR_INVALID, f"GRAPH {name!r} not found (LATTICE_LIBRARY must name the file holding it)")
     return g

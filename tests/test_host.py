@@ -462,3 +462,13 @@ def test_graph_parameters_refuse_bad_graphs():
                                  (4, [(0, 1, 0)] * 129, None, "too many bonds")):
         rc, err, _ = parse(n, edges, vtype)
         assert rc == ed.ERR_INVALID and msg in err, (msg, err)
+
+
+def test_unreadable_lattice_library_falls_back_to_built_in_lattices(tmp_path):
+    f = tmp_path / "broken.xml"
+    f.write_text("<LATTICES><GRAPH name='x'>")
+    p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "chain lattice", "L": 4, "J": 1,
+         "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
+    assert ed.model_from_parameters(p)["n_sites"] == 4
+    with pytest.raises(ed.AEDError, match="LATTICE_LIBRARY"):
+        ed.model_from_parameters({k: v for k, v in dict(p, GRAPH="x").items() if k != "LATTICE"})
