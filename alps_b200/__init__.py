@@ -237,25 +237,28 @@ def launch_count() -> int:
     return c.value
 
 
-def parse_parameters(text: str):
-    """ALPS parameter text -> dict(n_sites, n_up, bonds=[(s1, s2, Jz, Jxy, K)], nev, max_iter, site_h, site_d)."""
+def _parsed_model(call):
+    """Run a parse entry point twice (counts, then arrays) and return its model dict; call(info, arrays...)
+    takes the ParamInfo and the seven output arrays with their capacities."""
     info = ParamInfo()
-    _check(lib().aed_parse_parameters(text.encode(), ctypes.byref(info), None, None, None, None, None, None, None,
-                                      0, 0))
+    _check(call(ctypes.byref(info), None, None, None, None, None, None, None, 0, 0))
     nb, ns = info.n_bonds, info.n_sites
-    s1 = np.zeros(max(nb, 1), np.int32)
-    s2 = np.zeros(max(nb, 1), np.int32)
-    jz = np.zeros(max(nb, 1))
-    jxy = np.zeros(max(nb, 1))
-    kq = np.zeros(max(nb, 1))
-    sh = np.zeros(ns)
-    sd = np.zeros(ns)
-    _check(lib().aed_parse_parameters(text.encode(), ctypes.byref(info), s1.ctypes.data_as(_I32P),
-                                      s2.ctypes.data_as(_I32P), _dp(jz), _dp(jxy), _dp(kq), _dp(sh), _dp(sd), nb, ns))
+    s1, s2 = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+    jz, jxy, kq = np.zeros(max(nb, 1)), np.zeros(max(nb, 1)), np.zeros(max(nb, 1))
+    sh, sd = np.zeros(ns), np.zeros(ns)
+    _check(call(ctypes.byref(info), s1.ctypes.data_as(_I32P), s2.ctypes.data_as(_I32P), _dp(jz), _dp(jxy), _dp(kq),
+                _dp(sh), _dp(sd), nb, ns))
     bonds = [(int(s1[b]), int(s2[b]), float(jz[b]), float(jxy[b]), float(kq[b])) for b in range(nb)]
     return {"n_sites": ns, "n_up": info.n_up, "bonds": bonds, "nev": info.number_eigenvalues,
             "max_iter": info.max_iterations, "two_s": info.two_s,
             "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
+
+
+def parse_parameters(text: str):
+    """ALPS parameter text -> dict(n_sites, n_up, bonds=[(s1, s2, Jz, Jxy, K)], nev, max_iter, two_s, site_h,
+    site_d)."""
+    t = text.encode()
+    return _parsed_model(lambda *a: lib().aed_parse_parameters(t, *a))
 
 
 class Graph(tuple):
@@ -336,21 +339,10 @@ def parse_graph_parameters(text: str, graph):
     es = np.ascontiguousarray([e[0] for e in edges] or [0], dtype=np.int32)
     et = np.ascontiguousarray([e[1] for e in edges] or [0], dtype=np.int32)
     ey = np.ascontiguousarray([e[2] for e in edges] or [0], dtype=np.int32)
-    ne = len(edges)
-    info = ParamInfo()
-    args = (text.encode(), n, vt.ctypes.data_as(_I32P), ne, es.ctypes.data_as(_I32P), et.ctypes.data_as(_I32P),
-            ey.ctypes.data_as(_I32P), ctypes.byref(info))
-    _check(lib().aed_parse_graph_parameters(*args, None, None, None, None, None, None, None, 0, 0))
-    nb, ns = info.n_bonds, info.n_sites
-    s1, s2 = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
-    jz, jxy, kq = np.zeros(max(nb, 1)), np.zeros(max(nb, 1)), np.zeros(max(nb, 1))
-    sh, sd = np.zeros(ns), np.zeros(ns)
-    _check(lib().aed_parse_graph_parameters(*args, s1.ctypes.data_as(_I32P), s2.ctypes.data_as(_I32P), _dp(jz),
-                                            _dp(jxy), _dp(kq), _dp(sh), _dp(sd), nb, ns))
-    bonds = [(int(s1[b]), int(s2[b]), float(jz[b]), float(jxy[b]), float(kq[b])) for b in range(nb)]
-    return {"n_sites": ns, "n_up": info.n_up, "bonds": bonds, "nev": info.number_eigenvalues,
-            "max_iter": info.max_iterations, "two_s": info.two_s,
-            "site_h": sh if info.has_site_terms else None, "site_d": sd if info.has_site_terms else None}
+    t = text.encode()
+    return _parsed_model(lambda *a: lib().aed_parse_graph_parameters(
+        t, n, vt.ctypes.data_as(_I32P), len(edges), es.ctypes.data_as(_I32P), et.ctypes.data_as(_I32P),
+        ey.ctypes.data_as(_I32P), *a))
 
 
 def _params_text(params) -> str:
