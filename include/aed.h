@@ -430,7 +430,10 @@ int aed_launch_count(int64_t* count);
  * inside libaed.so that every GPU loading the library keeps until the process
  * exits, so n is limited to 268,435,456 elements (larger n: AED_ERR_INVALID,
  * nothing launched).  The first call on a device looks up that array's device
- * address; make that first call before any stream capture.  Every call
+ * address; make that first call before any stream capture.  That address is
+ * kept for the life of the process: after a cudaDeviceReset of that device
+ * (which unloads the library's module there) it is stale, so do not call
+ * aed_dot_noalloc on a device that was reset.  Every call
  * overwrites the partials it then reads, so nothing needs clearing, but all
  * calls share the one array: calls that overlap on the GPU (different
  * streams, different host threads) race and can return wrong sums; order

@@ -86,6 +86,10 @@ def lib():
         L.orc_sample_times.argtypes = [ctypes.c_int, _c_u32_p, ctypes.c_int64, ctypes.c_int, _c_int_p, _c_int_p,
                                        _c_dbl_p, _c_dbl_p, ctypes.c_int64, ctypes.c_int64, _c_dbl_p, _c_dbl_p,
                                        _c_dbl_p]
+        L.orc_rows_mult.restype = None
+        L.orc_rows_mult.argtypes = [ctypes.c_int, _c_u32_p, ctypes.c_int64, _c_dbl_p, _c_dbl_p, ctypes.c_int,
+                                    _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, ctypes.c_int64,
+                                    ctypes.c_int64, _c_dbl_p, _c_dbl_p]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_num_threads.argtypes = []
         _lib = L
@@ -327,6 +331,30 @@ def sample_times(N, states, bonds, r0, r1):
                            _p(jz, _c_dbl_p), _p(jxy, _c_dbl_p), r0, r1, ctypes.byref(tb), ctypes.byref(tp),
                            ctypes.byref(tv))
     return tb.value, tp.value, tv.value
+
+
+def rows_mult(N, states, bonds, x, r0, r1, site_h=None, site_d=None):
+    """Rows [r0, r1) of the explicit matrix (reference element order) times x, for sectors too large
+    to build whole; ``states`` is the full sector (``basis_fast``), ``x`` the full vector.  Returns
+    (y, sum_j |M_ij x_j|) over the window."""
+    states = np.ascontiguousarray(states, dtype=np.uint32)
+    D = states.size
+    r1 = min(r1, D)
+    s1 = np.array([b[0] for b in bonds], dtype=np.int32)
+    s2 = np.array([b[1] for b in bonds], dtype=np.int32)
+    jz = np.array([b[2] for b in bonds], dtype=np.float64)
+    jxy = np.array([b[3] for b in bonds], dtype=np.float64)
+    kq = np.array([b[4] if len(b) > 4 else 0.0 for b in bonds], dtype=np.float64)
+    sh = None if site_h is None else np.ascontiguousarray(site_h, dtype=np.float64)
+    sd = None if site_d is None else np.ascontiguousarray(site_d, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    assert x.size == D
+    y = np.empty(r1 - r0)
+    ya = np.empty(r1 - r0)
+    lib().orc_rows_mult(N, _p(states, _c_u32_p), D, _p(sh, _c_dbl_p), _p(sd, _c_dbl_p), len(bonds),
+                        _p(s1, _c_int_p), _p(s2, _c_int_p), _p(jz, _c_dbl_p), _p(jxy, _c_dbl_p),
+                        _p(kq, _c_dbl_p), _p(x, _c_dbl_p), r0, r1, _p(y, _c_dbl_p), _p(ya, _c_dbl_p))
+    return y, ya
 
 
 def num_threads() -> int:

@@ -752,6 +752,65 @@ void orc_sample_times(int N, const uint32_t* states, int64_t D, int nb, const in
   *t_vec = std::chrono::duration<double>(t4 - t3).count();
 }
 
+// Rows [r0, r1) of the explicit matrix of a sector whose full state list is
+// `states`, built row by row in the reference's element order, then
+// y[i - r0] = prod(M, x)_i.  Per element M(i,j) the additions come in the order
+// of build_matrix (initialized_matrix's +1 -1, the site terms by site, the
+// bonds by bond and (js1, js2)), so the rows equal build_matrix's bit for bit;
+// this serves sectors too large for the whole matrix (10^8 states): x is the
+// full vector, only the window's rows are formed.  yabs (optional) receives
+// sum_j |M_ij x_j| per row (the scale of a row's rounding error).  OpenMP
+// over rows.
+void orc_rows_mult(int N, const uint32_t* states, int64_t D, const double* site_h, const double* site_d, int nb,
+                   const int* s1, const int* s2, const double* jz, const double* jxy, const double* kq,
+                   const double* x, int64_t r0, int64_t r1, double* y, double* yabs) {
+  if (r1 > D) r1 = D;
+  std::vector<BondTensor> bt(nb);
+  for (int b = 0; b < nb; ++b) bt[b] = spin_bond(jz[b], jxy[b], kq ? kq[b] : 0.0);
+#pragma omp parallel
+  {
+    std::vector<Entry> row;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t i = r0; i < r1; ++i) {
+      row.clear();
+      row_add(row, i, 1.0);
+      row_add(row, i, -1.0);
+      const uint32_t state = states[i];
+      if (site_h || site_d) {
+        for (int s = 0; s < N; ++s) {
+          const double h = site_h ? site_h[s] : 0.0;
+          const double dd = site_d ? site_d[s] : 0.0;
+          const double mat[2] = {0.25 * dd + 0.5 * h, 0.25 * dd - 0.5 * h};
+          const double v = mat[(state >> (N - 1 - s)) & 1];
+          if (v != 0.0) row_add(row, i, v);
+        }
+      }
+      for (int b = 0; b < nb; ++b) {
+        const int b1 = N - 1 - s1[b], b2 = N - 1 - s2[b];
+        const int is1 = (state >> b1) & 1, is2 = (state >> b2) & 1;
+        for (int js1 = 0; js1 < 2; ++js1)
+          for (int js2 = 0; js2 < 2; ++js2) {
+            const double v = bt[b].m[is1][is2][js1][js2];
+            if (v == 0.0) continue;
+            uint32_t ns = state;
+            ns = (ns & ~(1u << b1)) | ((uint32_t)js1 << b1);
+            ns = (ns & ~(1u << b2)) | ((uint32_t)js2 << b2);
+            const int64_t j = lb_index(states, D, ns);
+            if (j < D) row_add(row, j, v);
+          }
+      }
+      std::sort(row.begin(), row.end(), [](const Entry& a, const Entry& b) { return a.j < b.j; });
+      double t = 0.0, ta = 0.0;
+      for (auto& e : row) {
+        t += e.v * x[e.j];
+        ta += std::fabs(e.v * x[e.j]);
+      }
+      y[i - r0] = t;
+      if (yabs) yabs[i - r0] = ta;
+    }
+  }
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -212,6 +212,27 @@ def test_csr_is_symmetric_and_matches_matfree():
     assert np.array_equal(y1, y2)
 
 
+@pytest.mark.parametrize("seed", [0, 1])
+def test_row_windows_equal_the_whole_explicit_matrix(seed):
+    """oracle.rows_mult (the windows the full-size GPU parity tests sample) builds the same rows as the
+    whole explicit matrix, bit for bit, with site terms, biquadratic couplings and duplicate bonds."""
+    n, _, raw = lattice.lattice_graph("square lattice", {"L": 4, "W": 4})
+    rng = np.random.default_rng(seed)
+    bonds = [(s, t, float(j), float(j) * 0.7, 0.1 * seed) for (s, t, _), j in zip(raw, rng.uniform(0.5, 1.5, len(raw)))]
+    bonds.append(bonds[3])
+    sh, sd = rng.normal(size=n), rng.normal(size=n)
+    m = oracle.Matrix(n, 8, bonds, site_h=sh, site_d=sd)
+    x = rng.normal(size=m.D)
+    y = m.mult(x)
+    states = oracle.basis_fast(n, 8)
+    rp, col, val = m.csr()
+    absrow = np.add.reduceat(np.abs(val) * np.abs(x[col]), rp[:-1])
+    for r0, r1 in [(0, 1), (0, 700), (5000, 9000), (m.D - 333, m.D)]:
+        yw, ya = oracle.rows_mult(n, states, bonds, x, r0, r1, site_h=sh, site_d=sd)
+        assert np.array_equal(yw, y[r0:r1])
+        np.testing.assert_allclose(ya, absrow[r0:r1], rtol=1e-14)
+
+
 # ---------------------------------------------------------------- momentum sectors
 def _bloch_cases():
     out = []
