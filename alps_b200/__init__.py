@@ -26,6 +26,8 @@ LIB_PATH = os.path.join(_HERE, "libaed.so")
 FP64 = 0
 FP32 = 1
 MAX_NEV = 16
+# aed_solve_result.refined_by: how a mixed solve's FP32 values were refined
+REFINED_BY = {0: "none", 1: "rayleigh_ritz", 2: "lanczos"}
 MAX_BONDS = 128
 
 OK = 0
@@ -83,7 +85,7 @@ class SolveResult(ctypes.Structure):
         ("n_evals", ctypes.c_int32), ("iterations", ctypes.c_int32), ("iterations_low", ctypes.c_int32),
         ("converged", ctypes.c_int32), ("evals", ctypes.c_double * MAX_NEV),
         ("errors", ctypes.c_double * MAX_NEV), ("evals_low", ctypes.c_double * MAX_NEV),
-        ("seconds", ctypes.c_double), ("apply_ms", ctypes.c_double),
+        ("seconds", ctypes.c_double), ("apply_ms", ctypes.c_double), ("refined_by", ctypes.c_int32),
     ]
 
 
@@ -644,7 +646,7 @@ class Hamiltonian:
         return {"evals": np.array(res.evals[:n]), "errors": np.array(res.errors[:n]),
                 "iterations": res.iterations, "iterations_low": res.iterations_low,
                 "evals_low": np.array(res.evals_low[:n]), "converged": bool(res.converged),
-                "seconds": res.seconds, "apply_ms": res.apply_ms}
+                "seconds": res.seconds, "apply_ms": res.apply_ms, "refined_by": REFINED_BY[res.refined_by]}
 
     def eigenvectors(self, k=1, seed=0, start=None):
         """Ritz vectors of the k lowest eigenvalues of the last solve (aed_eigenvectors): the solve's

@@ -25,9 +25,10 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
              "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["kernels.cu", "noalloc.cu", "batch.cu", "momentum.cu", "measure.cu", "spin.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu", "batch.cu", "momentum.cu", "measure.cu", "spin.cu", "refine.cu"]
 CPP_SOURCES = ["model.cpp", "tmatrix.cpp", "api.cpp", "lanczos.cpp", "server.cpp"]
-HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "apply_blocks.cuh", "tmatrix_core.h",
+HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "apply_blocks.cuh", "apply_stream.cuh",
+           "tmatrix_core.h",
            "batch.cuh", "momentum.cuh", "spin.cuh"]
 
 

@@ -143,7 +143,7 @@ void release(aed_handle* h) {
   handle_release_workspace(h);
   for (void* p : {(void*)h->d_thi, (void*)h->d_tlo, (void*)h->d_lolist, (void*)h->d_looff, (void*)h->d_tile_h,
                   (void*)h->d_tile_r, (void*)h->d_blk_h, (void*)h->d_tfirst, (void*)h->d_dg, (void*)h->d_ell,
-                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_start64,
+                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_flag, (void*)h->d_start64,
                   (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map, (void*)h->d_sthi,
                   (void*)h->d_stlo, (void*)h->d_slolist, (void*)h->d_slooff, (void*)h->d_sblk_hi,
                   (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r, (void*)h->d_sreps})
@@ -243,7 +243,8 @@ void handle_release_workspace(aed_handle* h) {
   for (void* p : h->store_chunks) mem_dev_free(p, h->stream);
   h->store_chunks.clear();
   h->store_chunk_bytes = 0;
-  for (int k = 0; k < 2; ++k) {
+  h->last_rr = false;
+  for (int k = 0; k < aed_handle::kWorkspaces; ++k) {
     mem_dev_free(h->ws[k], h->stream);
     h->ws[k] = nullptr;
     h->ws_bytes[k] = 0;
@@ -363,6 +364,16 @@ int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_par
   return launch_checked(h, f32, h->hv_var[f32 ? 1 : 0], x, y, alpha_part);
 }
 
+int handle_check_flag(aed_handle* h) {
+  if (!h->d_flag) return AED_OK;
+  uint32_t* hf = reinterpret_cast<uint32_t*>(h->h_scal + 5);
+  AED_CUDA_TRY(cudaMemcpyAsync(hf, h->d_flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (*hf == 0u) return AED_OK;
+  AED_CUDA_TRY(cudaMemsetAsync(h->d_flag, 0, sizeof(uint32_t), h->stream));
+  return fail(AED_ERR_TIMEOUT, "a bounded device wait of the apply gave up; its result is not valid");
+}
+
 // Mean CUDA-event time of `reps` applies through handle_hv.
 int time_hv(aed_handle* h, const void* x, void* y, int reps, double* alpha_part, double* ms) {
   int rc = AED_OK;
@@ -377,7 +388,7 @@ int time_hv(aed_handle* h, const void* x, void* y, int reps, double* alpha_part,
   cudaEventElapsedTime(&t, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (rc) return rc;
+  if (rc || (rc = handle_check_flag(h))) return rc;
   *ms = (double)t / reps;
   return AED_OK;
 }
@@ -505,7 +516,8 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   if ((rc = mem_dev_alloc_n(&h->d_thi, nhi)) || (rc = mem_dev_alloc_n(&h->d_tlo, nlo)) ||
       (rc = mem_dev_alloc_n(&h->d_lolist, nlo)) || (rc = mem_dev_alloc_n(&h->d_looff, h->tab.looff.size())) ||
       (rc = mem_dev_alloc_n(&h->d_tile_h, th.size())) || (rc = mem_dev_alloc_n(&h->d_tile_r, tr.size())) ||
-      (rc = mem_dev_alloc_n(&h->d_scal, 8)) || (rc = mem_dev_alloc_n(&h->d_blk_h, blk.size() + 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_scal, 8)) || (rc = mem_dev_alloc_n(&h->d_flag, 1)) ||
+      (rc = mem_dev_alloc_n(&h->d_blk_h, blk.size() + 1)) ||
       (rc = mem_dev_alloc_n(&h->d_tfirst, tf.size() + 1)) || (rc = mem_dev_alloc_n(&h->d_xtab, xt.size() + 1)) ||
       (rc = mem_dev_alloc_n(&h->d_dg, (size_t)h->tab.D)) || (rc = mem_dev_alloc_n(&h->d_partA, th.size() + 1)) ||
       (rc = mem_dev_alloc_n(&h->d_partB, (size_t)red_chunks(h->tab.D) + 1)) ||
@@ -525,6 +537,7 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   if (!blk.empty()) cudaMemcpyAsync(h->d_blk_h, blk.data(), blk.size() * 4, cudaMemcpyHostToDevice, h->stream);
   if (!tf.empty()) cudaMemcpyAsync(h->d_tfirst, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice, h->stream);
   if (!xt.empty()) cudaMemcpyAsync(h->d_xtab, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, h->stream);
+  cudaMemsetAsync(h->d_flag, 0, sizeof(uint32_t), h->stream);
   const cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     release(h);
@@ -548,6 +561,7 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
   t.Nhi = h->tab.Nhi;
   t.n_up = h->tab.n_up;
   t.dg = h->d_dg;
+  t.flag = h->d_flag;
   if ((rc = upload_lo_table(h))) {
     release(h);
     return rc;
@@ -1287,14 +1301,16 @@ int aed_lanczos_step(aed_handle* h, const void* v_prev, const void* v_cur, void*
 int aed_solve(aed_handle* h, const aed_solve_opts* opts, aed_solve_result* res) {
   if (!h || !opts || !res) return fail(AED_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
-  return solve(h, opts, res);
+  const int rc = solve(h, opts, res);
+  return rc ? rc : handle_check_flag(h);
 }
 
 int aed_eigenvectors(aed_handle* h, const aed_solve_opts* opts, int32_t k, void* const* vecs, double* evals,
                      double* residuals) {
   if (!h) return fail(AED_ERR_INVALID, "handle is NULL");
   DeviceGuard g(h->device);
-  return eigenvectors(h, opts, k, vecs, evals, residuals);
+  const int rc = eigenvectors(h, opts, k, vecs, evals, residuals);
+  return rc ? rc : handle_check_flag(h);
 }
 
 int aed_lanczos_state_bytes(aed_handle* h, int64_t* bytes) {
@@ -1357,7 +1373,7 @@ int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t 
   cudaEventElapsedTime(&t, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (rc) return rc;
+  if (rc || (rc = handle_check_flag(h))) return rc;
   *ms = (double)t / reps;
   if (variant_used) *variant_used = v;
   return AED_OK;

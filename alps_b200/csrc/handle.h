@@ -34,6 +34,7 @@ struct aed_handle {
   double* d_partA = nullptr;  // per-tile partial sums (n_tiles)
   double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
   double* d_scal = nullptr;   // 8 device scalars
+  uint32_t* d_flag = nullptr;  // raised by a kernel whose bounded wait gave up
   double* h_scal = nullptr;   // 8 pinned host scalars
   int hv_var[2] = {-1, -1};  // apply variant per precision (FP64, FP32), -1 = not tuned yet
   size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }
@@ -62,9 +63,12 @@ struct aed_handle {
   int64_t alpha_tiles() const { return mom ? aed::mom_tiles(dim) : gen ? sdev.n_tiles : dt.n_tiles; }
   // solve workspaces, kept between solves (grown on demand, so that a solve
   // makes no allocation once the handle is warm): slot 0 = the three FP64
-  // recurrence vectors, slot 1 = device alpha/beta pairs and Ritz coefficients
-  void* ws[2] = {nullptr, nullptr};
-  size_t ws_bytes[2] = {0, 0};
+  // recurrence vectors, slot 1 = device alpha/beta pairs and Ritz coefficients,
+  // slot 2 = the Ritz vectors, their images and the partial sums of the mixed
+  // path's Rayleigh-Ritz refinement
+  static constexpr int kWorkspaces = 3;
+  void* ws[kWorkspaces] = {nullptr, nullptr, nullptr};
+  size_t ws_bytes[kWorkspaces] = {0, 0, 0};
   std::vector<void*> store_chunks;  // FP32 Lanczos basis of the mixed path, kStoreChunk vectors each
   size_t store_chunk_bytes = 0;
   double* h_ab = nullptr;  // pinned alpha/beta staging
@@ -76,6 +80,11 @@ struct aed_handle {
   int rec_m = 0;
   bool rec_live = false;
   bool last_mixed = false;      // the last solve was the mixed path
+  // a mixed solve refined by Rayleigh-Ritz: eigenvector i is
+  // sum_j rr_coef[i * rr_m + j] v_j over the FP32 Lanczos basis kept in store_chunks
+  bool last_rr = false;
+  int rr_m = 0;
+  std::vector<double> rr_coef, rr_evals;
   double* d_start64 = nullptr;  // mixed path: start vector of its FP64 phase (D doubles)
 };
 
@@ -132,6 +141,9 @@ int spin_mom_expectation(aed_handle* h, const double* psi, int kind, int n, cons
                          double* out);
 
 int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_part);
+// AED_ERR_TIMEOUT (and the flag cleared) when a kernel of the handle gave up a
+// bounded wait since the last check; waits for the handle's stream.
+int handle_check_flag(aed_handle* h);
 // Choose the apply variant for this precision now (timed launches on x, y)
 // unless already chosen; handle_hv does this on its first call otherwise.
 int handle_tune(aed_handle* h, bool f32, const void* x, void* y);

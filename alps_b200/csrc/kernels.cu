@@ -16,6 +16,7 @@
 
 #include "apply.cuh"
 #include "apply_blocks.cuh"
+#include "apply_stream.cuh"
 #include "kernels.cuh"
 #include "reduce.cuh"
 
@@ -56,6 +57,9 @@ __global__ void __launch_bounds__(kHvThreads, MINB) hvb_kernel(const __grid_cons
   for (int64_t ub = blockIdx.x; ub < nb; ub += gridDim.x)
     bapply::apply_bundle<T, Acc, R, B>(c, t, ub, x, y, alpha_part, sm, xs, rc);
 }
+
+// y = H x with the flips' x segments staged by bulk copies (apply_stream.cuh).
+using sapply::hvs_kernel;
 
 // Diagonal M(i,i) of every row, accumulated in the reference's term order
 // (site terms, then bonds; hamiltonian_matrix.hpp:387-397 starting from the
@@ -267,13 +271,14 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
 // Tile apply (apply.cuh): R rows per thread, MINB CTAs per SM.  Bundle apply
 // (apply_blocks.cuh): B hi blocks per CTA with x in shared memory.
 struct HvVariant {
-  int B, R, minb;  // B = 0: tile apply
+  int B, R, minb;  // B = 0: tile apply; B = -1: stream apply (R = rows per thread, minb = own-x buffers)
   const char* name;
 };
 constexpr HvVariant kVariants[] = {
     {0, 4, 6, "r4b6"},      {0, 4, 5, "r4b5"},      {0, 4, 4, "r4b4"},      {0, 2, 8, "r2b8"},
     {0, 2, 6, "r2b6"},      {0, 8, 3, "r8b3"},      {1, 4, 3, "blk1r4b3"},  {2, 2, 4, "blk2r2b4"},
     {2, 4, 2, "blk2r4b2"},  {2, 2, 3, "blk2r2b3"},  {1, 4, 4, "blk1r4b4"},  {1, 2, 4, "blk1r2b4"},
+    {-1, 14, 2, "str14o2"}, {-1, 14, 1, "str14o1"}, {-1, 26, 2, "str26o2"}, {-1, 26, 1, "str26o1"},
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -332,11 +337,72 @@ int launch_bundle(const HvParams& P, const DevTables& t, const T* x, T* y, doubl
   return check_launch("hvb_kernel");
 }
 
+// Stream apply: one CTA per SM with OB own-x buffers and as many ring stages
+// as the shared memory holds (at most sapply::kMaxStages).  Not applicable to
+// sectors whose blocks need more than U rows per thread, to lo parts under
+// 8 bits (the crossing-table rows must be 16-byte multiples), or to vectors
+// that are not 16-byte aligned (bulk copies).
+struct StreamGrid {
+  int maxrows = -1;
+  int grid = 0;
+  sapply::StreamCfg cfg{};
+  size_t dyn = 0;
+};
+
+template <typename T, typename Acc, int U>
+int launch_stream(int OB, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
+                  cudaStream_t st, StreamGrid* cache) {
+  if (!t.blk_h || !t.flag || t.maxrows <= 0 || t.Nlo < 8 || t.Nlo > 16) return kVariantNotApplicable;
+  if ((t.maxrows + kHvThreads - 1) / kHvThreads > U) return kVariantNotApplicable;
+  if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(t.xtab)) & 15u)
+    return kVariantNotApplicable;
+  auto kern = hvs_kernel<T, Acc, U>;
+  if (cache->maxrows != t.maxrows) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+      const cudaError_t e = cudaGetLastError();
+      return fail(AED_ERR_CUDA, std::string("hvs_kernel attributes: ") + cudaGetErrorString(e));
+    }
+    sapply::StreamCfg cfg{};
+    cfg.own_bytes = (uint32_t)bapply::bundle_align16((size_t)t.maxrows * sizeof(T) + 32);
+    cfg.xoff = cfg.own_bytes;
+    cfg.stage_bytes = cfg.xoff + (uint32_t)bapply::bundle_align16((size_t)t.maxrows * 2 + 32);
+    const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024;
+    const int64_t S = (avail - (int64_t)OB * cfg.own_bytes) / (int64_t)cfg.stage_bytes;
+    if (S < 2) return kVariantNotApplicable;
+    cfg.S = (int)(S < sapply::kMaxStages ? S : sapply::kMaxStages);
+    cfg.OB = OB;
+    const size_t dyn = (size_t)OB * cfg.own_bytes + (size_t)cfg.S * cfg.stage_bytes;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
+      const cudaError_t e = cudaGetLastError();
+      return fail(AED_ERR_CUDA, std::string("hvs_kernel shared memory: ") + cudaGetErrorString(e));
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sapply::kThreads, dyn);
+    if (per_sm < 1) return kVariantNotApplicable;
+    cache->cfg = cfg;
+    cache->dyn = dyn;
+    cache->grid = num_sms();
+    cache->maxrows = t.maxrows;
+  }
+  sapply::StreamCfg cfg = cache->cfg;
+  cfg.flag = t.flag;
+  int64_t grid = cache->grid;
+  if (grid > t.n_blk) grid = t.n_blk;
+  if (grid < 1) return AED_OK;
+  kern<<<(unsigned)grid, sapply::kThreads, cache->dyn, st>>>(P, t, x, y, alpha_part, cfg);
+  return check_launch("hvs_kernel");
+}
+
 template <typename T, typename Acc>
 int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
                 cudaStream_t st) {
   static int grids[kNumVariants] = {};
   static BundleGrid bgrid[kNumVariants];
+  static StreamGrid sgrid[kNumVariants];
   if (t.n_tiles == 0) return AED_OK;
   switch (v) {
     case 0: return launch_one<T, Acc, 4, 6>(P, t, x, y, alpha_part, st, &grids[0]);
@@ -351,6 +417,10 @@ int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, 
     case 9: return launch_bundle<T, Acc, 2, 2, 3>(P, t, x, y, alpha_part, st, &bgrid[9]);
     case 10: return launch_bundle<T, Acc, 4, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[10]);
     case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[11]);
+    case 12: return launch_stream<T, Acc, 14>(2, P, t, x, y, alpha_part, st, &sgrid[12]);
+    case 13: return launch_stream<T, Acc, 14>(1, P, t, x, y, alpha_part, st, &sgrid[13]);
+    case 14: return launch_stream<T, Acc, 26>(2, P, t, x, y, alpha_part, st, &sgrid[14]);
+    case 15: return launch_stream<T, Acc, 26>(1, P, t, x, y, alpha_part, st, &sgrid[15]);
     default: return fail(AED_ERR_INVALID, "unknown apply variant");
   }
 }

@@ -30,6 +30,8 @@ struct DevTables {
   const uint32_t* tfirst = nullptr;  // 2^Nhi: index of the first tile of each hi block
   int64_t n_blk = 0;
   int maxrows = 0;  // rows of the largest hi block
+  // raised by a kernel whose bounded wait gave up (read and cleared by the host)
+  uint32_t* flag = nullptr;
 };
 
 constexpr int kHvThreads = 256;
@@ -91,6 +93,25 @@ int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t s
 constexpr int kMaxRitzTerms = 4096;
 int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, double* out, int64_t n,
                         bool accumulate, cudaStream_t st);
+
+// ---- Rayleigh-Ritz refinement of the mixed path (refine.cu) ----
+constexpr int kMaxRR = 6;     // Ritz vectors in one refinement
+constexpr int kMaxComb = 16;  // stored vectors per ritz_combine_multi call (a store chunk)
+struct VecSet {
+  double* p[kMaxRR];
+};
+struct ResidCoef {
+  double cw[kMaxRR][kMaxRR], cx[kMaxRR][kMaxRR];
+};
+// out.p[k][i] (+)= sum_j coef[k * m + j] V[j * ld + i], k < K, m <= kMaxComb.
+int launch_ritz_combine_multi(const float* V, int64_t ld, int m, const double* coef, int K, const VecSet& out,
+                              int64_t n, bool accumulate, cudaStream_t st);
+// out = [<X_a, X_b> for a <= b (row-major upper triangle), <X_a, Y_b> for all a, b];
+// part: (K(K+1)/2 + K^2) * red_chunks(n) doubles of scratch.
+int launch_gram(const VecSet& X, const VecSet& Y, int K, int64_t n, double* part, double* out, cudaStream_t st);
+// out[r] = |sum_k cw[r][k] Y_k + cx[r][k] X_k|^2 for r < R; part: R * red_chunks(n) doubles.
+int launch_resid(const VecSet& X, const VecSet& Y, const ResidCoef& rc, int K, int R, int64_t n, double* part,
+                 double* out, cudaStream_t st);
 
 int64_t launch_count();
 // After a launch in another translation unit: counts it and returns

@@ -411,9 +411,215 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
 // energy agreement the mixed path promises.
 constexpr double kRefineEnergyTol = 1e-11;
 
+// Rayleigh-Ritz acceptance: every reported value's error bound below
+// kRRTol * |theta|, 10x inside the 1e-9 relative agreement.
+constexpr double kRRTol = 1e-10;
+
+// Eigen-decomposition of a symmetric n x n matrix a (row-major, destroyed) by
+// cyclic Jacobi rotations (Jacobi 1846; the threshold-free cyclic form of
+// Rutishauser, Handbook for Automatic Computation II, 1971): w ascending,
+// column k of v (v[i * n + k]) its eigenvector.  n <= kMaxRR.
+void jacobi_eigen(int n, double* a, double* w, double* v) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) v[i * n + j] = i == j ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int i = 0; i < n; ++i) {
+      diag += a[i * n + i] * a[i * n + i];
+      for (int j = i + 1; j < n; ++j) off += a[i * n + j] * a[i * n + j];
+    }
+    if (off <= 1e-34 * diag || off == 0.0) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[p * n + q];
+        if (apq == 0.0) continue;
+        // rotation angle that zeroes a_pq: tan(phi) = t, the smaller root of t^2 + 2 theta t - 1 = 0
+        const double theta = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = a[k * n + p], akq = a[k * n + q];
+          a[k * n + p] = c * akp - s * akq;
+          a[k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = a[p * n + k], aqk = a[q * n + k];
+          a[p * n + k] = c * apk - s * aqk;
+          a[q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = v[k * n + p], vkq = v[k * n + q];
+          v[k * n + p] = c * vkp - s * vkq;
+          v[k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return a[x * n + x] < a[y * n + y]; });
+  std::vector<double> vs((size_t)n * n);
+  for (int k = 0; k < n; ++k) {
+    w[k] = a[ord[k] * n + ord[k]];
+    for (int i = 0; i < n; ++i) vs[i * n + k] = v[i * n + ord[k]];
+  }
+  std::copy(vs.begin(), vs.end(), v);
+}
+
+// The mixed path's FP64 Rayleigh-Ritz refinement.  The K Ritz vectors of
+// T(m1) that span the nev lowest clusters (tcore::ritz_span: ghost copies and
+// pairs closer than FP32 resolves included) are formed in FP64 from the
+// stored FP32 basis, H is applied to each in FP64, and the projected pencil
+// (Psi^T H Psi, Psi^T Psi) is solved on the host: directions whose Gram
+// eigenvalue is below 1e-10 of the largest (ghost copies of one vector) are
+// dropped, the rest orthonormalised.  The K' Ritz pairs (theta_i, Psi c_i)
+// get their FP64 residuals r_i = |H Psi c_i - theta_i Psi c_i|, and the
+// block residual bound (Kato-Temple for a Ritz subspace)
+//   0 <= theta_i - lambda_i <= sum_r r_r^2 / (lambda_next - theta_{K'-1})
+// holds whenever lambda_next, the lowest eigenvalue outside the subspace, is
+// above theta_{K'-1}; lambda_next is bounded below by the FP32 phase's next
+// distinct value minus its error estimate (and its FP32 resolution).  The
+// values are accepted when the bound is below kRRTol |theta_i| for every
+// reported value; otherwise *accepted stays false and the caller refines by
+// FP64 Lanczos.
+template <typename SlotFn>
+int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<double>& Z, int nev, SlotFn slot,
+                  int64_t ldv, double* coef_dev, aed_solve_result* r, bool* accepted) {
+  *accepted = false;
+  const int64_t D = h->vlen;
+  const int c = std::min(nev, (int)T1.evals.size());
+  if (c < 1 || (int)T1.evals.size() <= c) return AED_OK;  // no value above the clusters to bound the gap
+  const int K = tcore::ritz_span((int)T1.evals.size(), nev, T1.first.data(), T1.mults.data(), m1);
+  if (K < 1 || K > kMaxRR) return AED_OK;
+  // coefficients chunk by chunk of the store: [K x cnt] blocks at K * j0
+  std::vector<double> cf((size_t)K * m1);
+  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
+    const int cnt = std::min(kStoreChunk, m1 - j0);
+    for (int k = 0; k < K; ++k)
+      for (int j = 0; j < cnt; ++j) cf[(size_t)K * j0 + (size_t)k * cnt + j] = Z[(size_t)k * m1 + j0 + j];
+  }
+  const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
+  const int64_t nch = red_chunks(D);
+  const int np = K * (K + 1) / 2 + K * K;
+  const size_t part_bytes = (((size_t)np * nch * 8) + 255) & ~(size_t)255;
+  void* ws = nullptr;
+  int rc = handle_workspace(h, 2, 2 * (size_t)K * vb + part_bytes + 64 * 8, &ws);
+  if (rc) return rc;
+  VecSet psi{}, img{};
+  for (int k = 0; k < K; ++k) {
+    psi.p[k] = (double*)((char*)ws + (size_t)k * vb);
+    img.p[k] = (double*)((char*)ws + (size_t)(K + k) * vb);
+  }
+  double* part = (double*)((char*)ws + 2 * (size_t)K * vb);
+  double* outd = (double*)((char*)part + part_bytes);
+  double* hout = nullptr;
+  if ((rc = handle_pinned(h, 128, &hout))) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(coef_dev, cf.data(), cf.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
+    const int cnt = std::min(kStoreChunk, m1 - j0);
+    if ((rc = launch_ritz_combine_multi((const float*)slot(j0), ldv, cnt, coef_dev + (size_t)K * j0, K, psi, D,
+                                        j0 > 0, h->stream)))
+      return rc;
+  }
+  for (int k = 0; k < K; ++k)
+    if ((rc = handle_hv(h, false, psi.p[k], img.p[k], nullptr))) return rc;
+  if ((rc = launch_gram(psi, img, K, D, part, outd, h->stream))) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(hout, outd, (size_t)np * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // the host copy of cf is read by the copy above too
+  double G[kMaxRR * kMaxRR], A[kMaxRR * kMaxRR];
+  int p = 0;
+  for (int a = 0; a < K; ++a)
+    for (int b = a; b < K; ++b, ++p) G[a * K + b] = G[b * K + a] = hout[p];
+  for (int a = 0; a < K; ++a)
+    for (int b = 0; b < K; ++b, ++p) A[a * K + b] = hout[p];
+  for (int a = 0; a < K; ++a)
+    for (int b = a + 1; b < K; ++b) A[a * K + b] = A[b * K + a] = 0.5 * (A[a * K + b] + A[b * K + a]);
+  // orthonormal basis of span(Psi): B = Q_kept diag(g)^{-1/2}
+  double g[kMaxRR], Q[kMaxRR * kMaxRR], Gc[kMaxRR * kMaxRR];
+  std::copy(G, G + K * K, Gc);
+  jacobi_eigen(K, Gc, g, Q);
+  const double gmax = g[K - 1];
+  if (!(gmax > 0)) return AED_OK;
+  double B[kMaxRR * kMaxRR];
+  int Kp = 0;
+  for (int k = K - 1; k >= 0; --k) {
+    if (!(g[k] > 1e-10 * gmax)) continue;
+    const double s = 1.0 / std::sqrt(g[k]);
+    for (int i = 0; i < K; ++i) B[i * K + Kp] = Q[i * K + k] * s;
+    ++Kp;
+  }
+  // C = B^T A B (Kp x Kp)
+  double AB[kMaxRR * kMaxRR], C[kMaxRR * kMaxRR], th[kMaxRR], Y[kMaxRR * kMaxRR];
+  for (int i = 0; i < K; ++i)
+    for (int j = 0; j < Kp; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < K; ++k) s += A[i * K + k] * B[k * K + j];
+      AB[i * K + j] = s;
+    }
+  for (int i = 0; i < Kp; ++i)
+    for (int j = 0; j < Kp; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < K; ++k) s += B[k * K + i] * AB[k * K + j];
+      C[i * Kp + j] = s;
+    }
+  for (int i = 0; i < Kp; ++i)
+    for (int j = i + 1; j < Kp; ++j) C[i * Kp + j] = C[j * Kp + i] = 0.5 * (C[i * Kp + j] + C[j * Kp + i]);
+  jacobi_eigen(Kp, C, th, Y);
+  // coefficients over Psi of the Ritz pairs: c_r = B y_r
+  double cr[kMaxRR][kMaxRR];
+  ResidCoef rcoef{};
+  for (int q = 0; q < Kp; ++q)
+    for (int k = 0; k < K; ++k) {
+      double s = 0.0;
+      for (int j = 0; j < Kp; ++j) s += B[k * K + j] * Y[j * Kp + q];
+      cr[q][k] = s;
+      rcoef.cw[q][k] = s;
+      rcoef.cx[q][k] = -th[q] * s;
+    }
+  if ((rc = launch_resid(psi, img, rcoef, K, Kp, D, part, outd, h->stream))) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(hout, outd, (size_t)Kp * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  double r2 = 0.0;
+  for (int q = 0; q < Kp; ++q) r2 += hout[q];
+  // lowest eigenvalue outside the subspace, from below: the FP32 phase's next
+  // distinct value less its error estimate and its FP32 resolution
+  const double next = T1.evals[c];
+  const double next_lo = next - std::max(T1.errs[c], kFp32MergeRel * std::fabs(next)) -
+                         kFp32MergeRel * std::max(std::fabs(T1.evals.front()), std::fabs(T1.evals.back()));
+  const double gap = next_lo - th[Kp - 1];
+  if (!(gap > 0)) return AED_OK;
+  const double bound = r2 / gap;
+  // distinct values: merged below the FP64 T-matrix threshold eps^(2/3) max|lambda| (tmatrix.h:148-150)
+  const double scale = std::max(std::fabs(T1.evals.front()), std::fabs(T1.evals.back()));
+  const double thold = std::pow(2.220446049250313e-16, 2.0 / 3.0) * scale;
+  std::vector<int> pick;
+  for (int q = 0; q < Kp && (int)pick.size() < nev; ++q)
+    if (pick.empty() || th[q] - th[pick.back()] > thold) pick.push_back(q);
+  if ((int)pick.size() < c) return AED_OK;  // fewer distinct values than the FP32 phase resolved
+  for (int q : pick)
+    if (!(bound <= kRRTol * std::max(std::fabs(th[q]), 1e-300))) return AED_OK;
+  // accepted: the values and, for aed_eigenvectors, their coefficients over the stored basis
+  const int n = (int)pick.size();
+  r->n_evals = n;
+  h->rr_m = m1;
+  h->rr_coef.assign((size_t)n * m1, 0.0);
+  h->rr_evals.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    r->evals[i] = th[pick[i]];
+    h->rr_evals[i] = th[pick[i]];
+    r->errors[i] = bound;
+    for (int k = 0; k < K; ++k)
+      for (int j = 0; j < m1; ++j) h->rr_coef[(size_t)i * m1 + j] += cr[pick[i]][k] * Z[(size_t)k * m1 + j];
+  }
+  r->iterations = K;
+  r->converged = 1;
+  r->refined_by = AED_REFINE_RAYLEIGH_RITZ;
+  *accepted = true;
+  return AED_OK;
+}
+
 // FP32 phase with the Lanczos basis stored in HBM, then FP64 refinement.
 int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev, int max_iter, double rtol,
-                double atol, bool profile, aed_solve_result* r) {
+                double atol, bool profile, bool rayleigh_ritz_first, aed_solve_result* r) {
   const int64_t D = h->vlen;
   // Lanczos basis store: chunks of kStoreChunk FP32 vectors, grown as the
   // recurrence advances and kept by the handle for later solves
@@ -426,7 +632,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   double* hab = nullptr;
   int rc;
   const size_t ab_bytes = (((size_t)2 * (cap + 2) * 8 + 255) & ~(size_t)255);
-  if ((rc = handle_workspace(h, 1, ab_bytes + (size_t)kStoreChunk * 8, &small)) ||
+  if ((rc = handle_workspace(h, 1, ab_bytes + (size_t)kMaxRR * (cap + kStoreChunk) * 8, &small)) ||
       (rc = handle_pinned(h, (size_t)2 * (cap + 2), &hab)) || (rc = ring.init()))
     return rc;
   // the FP64 phase's start stays with the handle (eigenvector replay)
@@ -468,12 +674,30 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   for (int i = 0; i < n1; ++i) r->evals_low[i] = T1.evals[i];
   r->iterations_low = m1;
   const double apply32_ms = profile ? R.apply_ms() : 0.0;
-  // Ritz start: the eigenvectors of T(m1) up to the end of the nev-th
-  // distinct cluster with seeded weights (tcore::ritz_span / ritz_weight),
-  // accumulated in FP64 chunk by chunk from the stored basis
+  // eigenvectors of T(m1): the Rayleigh-Ritz refinement's Ritz vectors, or
+  // the FP64 Lanczos refinement's start
   std::vector<double> ev(R.alpha.begin(), R.alpha.begin() + m1), e(m1 + 1, 0.0), Z((size_t)m1 * m1);
   for (int i = 0; i + 1 < m1; ++i) e[i] = R.beta[i];
   if (tridiag_eigen(m1, ev.data(), e.data(), nullptr, Z.data())) return fail(AED_ERR_TRIDIAG, "tridiagonal eigensolver failed");
+  h->last_rr = false;
+  if (rayleigh_ritz_first) {
+    bool accepted = false;
+    if ((rc = rayleigh_ritz(h, T1, m1, Z, nev, slot, ldv, coef, r, &accepted))) return rc;
+    if (oom) return AED_ERR_NOMEM;
+    if (accepted) {
+      h->last_mixed = true;
+      h->last_rr = true;
+      h->rec_live = false;  // no FP64 recurrence to save or resume
+      h->last_alpha.assign(R.alpha.begin(), R.alpha.begin() + m1);
+      h->last_beta.assign(R.beta.begin(), R.beta.begin() + m1);
+      if (profile) r->apply_ms = apply32_ms;
+      return AED_OK;
+    }
+  }
+  // Ritz start of the FP64 Lanczos refinement: the eigenvectors of T(m1) up
+  // to the end of the nev-th distinct cluster with seeded weights
+  // (tcore::ritz_span / ritz_weight), accumulated in FP64 chunk by chunk from
+  // the stored basis
   const int K = tcore::ritz_span((int)T1.evals.size(), nev, T1.first.data(), T1.mults.data(), m1);
   std::vector<double> c(m1, 0.0);
   for (int k = 0; k < K; ++k) {
@@ -546,12 +770,16 @@ int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
     const double eps = 2.220446049250313e-16;
     const double rtol = o->rtol > 0 ? o->rtol : 100 * eps;
     const double atol = o->atol > 0 ? o->atol : 100 * eps;
+    if (o->refine < -1 || o->refine > 1) return fail(AED_ERR_INVALID, "refine must be -1, 0 or 1");
     if (o->resume) {  // continue the live FP64 recurrence (any handle precision)
       TmatInfo T;
+      h->last_rr = false;
       rc = solve_fp64(h, nullptr, nullptr, 0, nev, max_iter, rtol, atol, false, 0.0, 0, o->profile != 0, r, T, true);
     } else if (h->precision == AED_FP32 && o->refine != -1) {
-      rc = solve_mixed(h, o->start, o->seed, nev, max_iter, rtol, atol, o->profile != 0, r);
+      rc = solve_mixed(h, o->start, o->seed, nev, max_iter, rtol, atol, o->profile != 0, o->refine == 0, r);
+      if (!rc && r->refined_by == AED_REFINE_NONE) r->refined_by = AED_REFINE_LANCZOS;
     } else {
+      h->last_rr = false;
       TmatInfo T;
       rc = solve_fp64(h, o->start, nullptr, o->seed, nev, max_iter, rtol, atol, false, 0.0, 0, o->profile != 0, r, T);
       h->last_mixed = false;
@@ -617,6 +845,69 @@ constexpr char kStateMagic[8] = {'A', 'E', 'D', 'L', 'N', 'C', 'Z', '1'};
 
 }  // namespace
 
+// Ritz vectors of a mixed solve refined by Rayleigh-Ritz: psi_i =
+// sum_j rr_coef[i][j] v_j over the FP32 Lanczos basis the handle kept,
+// accumulated in FP64 (ritz_combine_multi, kMaxRR vectors per pass),
+// normalised; residual |H psi_i - theta_i psi_i| with the FP64 apply.
+int rr_eigenvectors(aed_handle* h, int k, void* const* vecs, double* evals, double* resid) {
+  const int n = (int)h->rr_evals.size(), m1 = h->rr_m;
+  if (k > n) return fail(AED_ERR_INVALID, "eigenvectors: k exceeds the distinct eigenvalues found");
+  for (int i = 0; i < k; ++i)
+    if (!vecs[i]) return fail(AED_ERR_INVALID, "eigenvectors: NULL output vector");
+  const int64_t D = h->vlen;
+  const size_t cb = h->store_chunk_bytes;
+  if (cb == 0 || (int)h->store_chunks.size() * kStoreChunk < m1)
+    return fail(AED_ERR_INVALID, "eigenvectors: the mixed solve's Lanczos basis is gone");
+  const int64_t ldv = (int64_t)(cb / kStoreChunk / 4);
+  const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
+  DevMem rb, cd;
+  int rc;
+  if ((rc = rb.alloc((size_t)(k + 1) * vb)) || (rc = cd.alloc((size_t)kMaxRR * m1 * 8))) return rc;
+  std::vector<double*> acc(k);
+  for (int i = 0; i < k; ++i) acc[i] = (double*)((char*)rb.p + (size_t)i * vb);
+  double* w = (double*)((char*)rb.p + (size_t)k * vb);
+  for (int i0 = 0; i0 < k; i0 += kMaxRR) {
+    const int K = std::min(kMaxRR, k - i0);
+    std::vector<double> cf((size_t)K * m1);
+    for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
+      const int cnt = std::min(kStoreChunk, m1 - j0);
+      for (int q = 0; q < K; ++q)
+        for (int j = 0; j < cnt; ++j) cf[(size_t)K * j0 + (size_t)q * cnt + j] = h->rr_coef[(size_t)(i0 + q) * m1 + j0 + j];
+    }
+    AED_CUDA_TRY(cudaMemcpyAsync(cd.p, cf.data(), cf.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    VecSet out{};
+    for (int q = 0; q < K; ++q) out.p[q] = acc[i0 + q];
+    for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
+      const int cnt = std::min(kStoreChunk, m1 - j0);
+      const float* V = (const float*)h->store_chunks[j0 / kStoreChunk];
+      if ((rc = launch_ritz_combine_multi(V, ldv, cnt, (const double*)cd.p + (size_t)K * j0, K, out, D, j0 > 0,
+                                          h->stream)))
+        return rc;
+    }
+    AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // cf and the coefficient buffer are reused
+  }
+  const bool f32 = h->precision == AED_FP32;
+  for (int i = 0; i < k; ++i) {
+    double nrm = 0.0;
+    if ((rc = host_norm(h, acc[i], &nrm))) return rc;
+    if (!(nrm > 0.0)) return fail(AED_ERR_INVALID, "eigenvectors: zero Ritz vector");
+    if ((rc = launch_scal<double>(nrm, acc[i], D, true, h->stream))) return rc;
+    if ((rc = handle_hv(h, false, acc[i], w, nullptr))) return rc;
+    if ((rc = launch_axpy<double>(-h->rr_evals[i], acc[i], w, D, h->stream))) return rc;
+    double rn = 0.0;
+    if ((rc = host_norm(h, w, &rn))) return rc;
+    if (resid) resid[i] = rn;
+    if (evals) evals[i] = h->rr_evals[i];
+    if (f32)
+      rc = launch_round_to_f32(acc[i], (float*)vecs[i], D, h->stream);
+    else
+      rc = launch_copy<double>(acc[i], (double*)vecs[i], D, h->stream);
+    if (rc) return rc;
+  }
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return AED_OK;
+}
+
 // lanczos::eigenvectors (src/ietl/lanczos.h:134-336): the Lanczos vectors are
 // not stored, so the recurrence of the last solve is run again from its start
 // (the seeded or given vector of `o`; for a mixed solve the kept start of its
@@ -627,6 +918,7 @@ constexpr char kStateMagic[8] = {'A', 'E', 'D', 'L', 'N', 'C', 'Z', '1'};
 // |H psi_i - lambda_i psi_i| (lanczos.h:284-295).
 int eigenvectors(aed_handle* h, const aed_solve_opts* o, int k, void* const* vecs, double* evals, double* resid) {
   if (!o || !vecs || k < 1) return fail(AED_ERR_INVALID, "eigenvectors: NULL argument or k < 1");
+  if (h->last_rr) return rr_eigenvectors(h, k, vecs, evals, resid);
   const int m = (int)h->last_alpha.size();
   if (m < 1) return fail(AED_ERR_INVALID, "eigenvectors: no solve to take eigenvectors from");
   for (int i = 0; i < k; ++i)

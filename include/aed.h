@@ -279,7 +279,10 @@ typedef struct {
   double rtol, atol;    /* lanczos_iteration_nlowest tolerances, 0 = 100 eps (iteration.h:110-113) */
   uint64_t seed;        /* start-vector seed                                           */
   const double* start;  /* optional HOST start vector (D doubles), else seeded          */
-  int32_t refine;       /* AED_FP32 handles: 0 = mixed FP32 + FP64 refinement (default),
+  int32_t refine;       /* AED_FP32 handles: 0 = mixed: FP32 Lanczos, then FP64
+                           Rayleigh-Ritz over its Ritz vectors, FP64 Lanczos from them
+                           when the Rayleigh-Ritz error bound is not met (default);
+                           1 = mixed with the FP64 Lanczos refinement only;
                            -1 = plain FP64 Lanczos on the same handle                  */
   int32_t profile;      /* 1: time every apply with CUDA events (res->apply_ms)         */
   int32_t resume;       /* 1: continue the handle's live FP64 recurrence (the last solve's
@@ -291,15 +294,23 @@ typedef struct {
 #define AED_MAX_NEV 16
 typedef struct {
   int32_t n_evals;              /* min(nev, #distinct non-ghost values) (sparsediag.h:115-118) */
-  int32_t iterations;           /* T-matrix size at convergence (FP64 phase for FP32 handles)   */
+  int32_t iterations;           /* T-matrix size at convergence (FP64 phase for FP32 handles;
+                                   the number of FP64 applies when refined_by is
+                                   AED_REFINE_RAYLEIGH_RITZ)                                     */
   int32_t iterations_low;       /* FP32 phase iterations (0 for FP64 handles)                    */
   int32_t converged;            /* 1 when all nev errors met the tolerance                       */
   double evals[AED_MAX_NEV];    /* lowest distinct eigenvalues, ascending                        */
-  double errors[AED_MAX_NEV];   /* |beta_m z_{m,i}| error estimates (tmatrix.h:159-183)          */
+  double errors[AED_MAX_NEV];   /* |beta_m z_{m,i}| error estimates (tmatrix.h:159-183); for
+                                   AED_REFINE_RAYLEIGH_RITZ the bound on lambda_i's error     */
   double evals_low[AED_MAX_NEV];/* FP32-phase eigenvalues before refinement (FP32 handles)       */
   double seconds;               /* wall time of the solve                                        */
   double apply_ms;              /* mean device time of one H*x inside the solve                  */
+  int32_t refined_by;           /* FP32 handles: how the FP32 values were refined (AED_REFINE_*) */
 } aed_solve_result;
+
+#define AED_REFINE_NONE 0           /* an FP64 solve                                         */
+#define AED_REFINE_RAYLEIGH_RITZ 1  /* FP64 Rayleigh-Ritz over the FP32 Ritz vectors          */
+#define AED_REFINE_LANCZOS 2        /* FP64 Lanczos from the FP32 Ritz vectors                */
 
 /* Lanczos eigenvalues: SparseDiagMatrix::do_subspace's Lanczos part
  * (applications/diag/sparsediag/sparsediag.h:104-118) with ietl::lanczos

@@ -383,6 +383,26 @@ def test_mixed_precision_within_1e9_of_fp64(name, p, nev):
     assert r32["iterations_low"] > 0
 
 
+@pytest.mark.parametrize("name,p,nev", MIXED_CASES, ids=[c[0] for c in MIXED_CASES])
+def test_mixed_refinements_agree(name, p, nev):
+    """Both FP64 refinements of the FP32 phase -- Rayleigh-Ritz over its Ritz vectors (the default)
+    and FP64 Lanczos from their combination (refine=1) -- land within 1e-9 of the FP64 solve, and the
+    Rayleigh-Ritz error bound it reports holds against the FP64 values."""
+    p = spin_params(**p)
+    r64 = ed.Hamiltonian.from_parameters(p).solve(nev=nev, seed=2)
+    h32 = ed.Hamiltonian.from_parameters(p, precision=ed.FP32)
+    rr = h32.solve(nev=nev, seed=2)
+    lz = h32.solve(nev=nev, seed=2, refine=1)
+    assert rr["refined_by"] == "rayleigh_ritz", rr
+    assert lz["refined_by"] == "lanczos"
+    for r in (rr, lz):
+        assert r["converged"] and len(r["evals"]) == len(r64["evals"])
+        assert np.all(np.abs(r["evals"] - r64["evals"]) <= 1e-9 * np.abs(r64["evals"]))
+    # the Rayleigh-Ritz values lie above the true ones by at most the bound (plus FP64 rounding)
+    d = rr["evals"] - r64["evals"]
+    assert np.all(d >= -1e-12 * np.abs(r64["evals"])) and np.all(d <= rr["errors"] + 1e-12 * np.abs(r64["evals"]))
+
+
 @pytest.mark.parametrize("L,seed", [(22, 2), (24, 2), (24, 5)])
 def test_mixed_precision_near_degenerate_pair(L, seed):
     """J1-J2 chain near the Majumdar-Ghosh point (J2 = 0.49972474): the two lowest states are
