@@ -312,7 +312,11 @@ def read_graph(path: str, name: str):
 
 def graph_of(params):
     """The <GRAPH> a parameter dict names (graph_helper::make_graph, src/alps/lattice/graph_helper.h:653-684):
-    GRAPH, or a LATTICE that LATTICE_LIBRARY holds as a <GRAPH>; None for the built-in lattices."""
+    GRAPH, or a LATTICE that LATTICE_LIBRARY holds as a <GRAPH>; None for the built-in lattices (no
+    LATTICE_LIBRARY: the reference's own lattices.xml, which the engine restates).  As LatticeLibrary
+    (src/alps/lattice/latticelibrary.C:25-74) a LATTICE_LIBRARY that is missing or not well-formed is an
+    error, and so is a name the library does not hold; a <LATTICEGRAPH> of a library is not read by this
+    engine and is refused rather than replaced by a built-in lattice of the same name."""
     if not isinstance(params, dict):
         return None
     has_g, has_l = "GRAPH" in params, "LATTICE" in params
@@ -320,17 +324,25 @@ def graph_of(params):
         raise AEDError(ERR_INVALID, "both GRAPH and LATTICE were specified")
     name = str(params.get("GRAPH", params.get("LATTICE", ""))).strip().strip('"')
     lib_path = str(params.get("LATTICE_LIBRARY", "")).strip().strip('"')
-    g = None
-    if lib_path and os.path.isfile(lib_path):
-        import xml.etree.ElementTree as ET
-        try:
-            g = read_graph(lib_path, name)
-        except ET.ParseError as e:
-            if has_g:
-                raise AEDError(ERR_INVALID, f"LATTICE_LIBRARY {lib_path!r}: {e}") from None
-    if g is None and has_g:
-        raise AEDError(ERR_INVALID, f"GRAPH {name!r} not found (LATTICE_LIBRARY must name the file holding it)")
-    return g
+    if not lib_path:
+        if has_g:
+            raise AEDError(ERR_INVALID, f"GRAPH {name!r} not found (LATTICE_LIBRARY must name the file holding it)")
+        return None
+    if not os.path.isfile(lib_path):
+        raise AEDError(ERR_INVALID, f"Could not find lattice library file {lib_path!r} (LATTICE_LIBRARY)")
+    import xml.etree.ElementTree as ET
+    try:
+        g = read_graph(lib_path, name)
+        if g is not None:
+            return g
+        root = ET.parse(lib_path).getroot()
+    except ET.ParseError as e:
+        raise AEDError(ERR_INVALID, f"LATTICE_LIBRARY {lib_path!r}: {e}") from None
+    if any(el.get("name") == name for el in root.iter("LATTICEGRAPH")):
+        raise AEDError(ERR_INVALID, f"lattice {name!r} of LATTICE_LIBRARY {lib_path!r} is a <LATTICEGRAPH>: only "
+                                    "<GRAPH> elements of a lattice library are supported")
+    raise AEDError(ERR_INVALID, f"{'GRAPH' if has_g else 'LATTICE'} {name!r} not found in LATTICE_LIBRARY "
+                                f"{lib_path!r}")
 
 
 def parse_graph_parameters(text: str, graph):

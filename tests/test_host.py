@@ -393,9 +393,13 @@ def test_graph_of_a_lattice_library(tmp_path):
     assert measure.Geometry(p).graph
     with pytest.raises(ed.AEDError, match="translations"):
         ed.lattice_momenta(dict(p, TOTAL_MOMENTUM="0"))
-    # a lattice library without that graph: the built-in lattices by name
+    # a lattice library without that lattice: an error, as LatticeLibrary has it; without a library the
+    # built-in lattices
     q = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "chain lattice", "L": 4, "J": 1,
          "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
+    with pytest.raises(ed.AEDError, match="not found in LATTICE_LIBRARY"):
+        ed.model_from_parameters(q)
+    del q["LATTICE_LIBRARY"]
     assert ed.model_from_parameters(q)["n_sites"] == 4
 
 
@@ -464,11 +468,21 @@ def test_graph_parameters_refuse_bad_graphs():
         assert rc == ed.ERR_INVALID and msg in err, (msg, err)
 
 
-def test_unreadable_lattice_library_falls_back_to_built_in_lattices(tmp_path):
+def test_lattice_library_errors_as_the_reference(tmp_path):
+    """A LATTICE_LIBRARY that is missing or not well-formed is an error (latticelibrary.C:25-39), whether
+    GRAPH or LATTICE names the lattice; a library <LATTICEGRAPH> is refused, not replaced by the built-in
+    lattice of the same name."""
     f = tmp_path / "broken.xml"
     f.write_text("<LATTICES><GRAPH name='x'>")
     p = {"MODEL": "spin", "LATTICE_LIBRARY": str(f), "LATTICE": "chain lattice", "L": 4, "J": 1,
          "CONSERVED_QUANTUMNUMBERS": "Sz", "Sz_total": 0}
-    assert ed.model_from_parameters(p)["n_sites"] == 4
+    with pytest.raises(ed.AEDError, match="LATTICE_LIBRARY"):
+        ed.model_from_parameters(p)
     with pytest.raises(ed.AEDError, match="LATTICE_LIBRARY"):
         ed.model_from_parameters({k: v for k, v in dict(p, GRAPH="x").items() if k != "LATTICE"})
+    with pytest.raises(ed.AEDError, match="Could not find lattice library file"):
+        ed.model_from_parameters(dict(p, LATTICE_LIBRARY=str(tmp_path / "missing.xml")))
+    g = tmp_path / "latticegraphs.xml"
+    g.write_text("<LATTICES><LATTICEGRAPH name='chain lattice'><FINITELATTICE/></LATTICEGRAPH></LATTICES>")
+    with pytest.raises(ed.AEDError, match="LATTICEGRAPH"):
+        ed.model_from_parameters(dict(p, LATTICE_LIBRARY=str(g)))
