@@ -741,6 +741,55 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def apply_case_bonds(name):
+    """Workloads of `--workload apply`: l24 / l26 / l28 (J1-J2 chain, J2 = 0.25), sq6x5 (6x5 square lattice,
+    per-bond J ~ U[0.8, 1.2] seed 3005)."""
+    if name in ("l24", "l26", "l28"):
+        L = int(name[1:])
+        return L, L // 2, chain_bonds(L, 0.25)
+    if name == "sq6x5":
+        return 30, 15, square_bonds(6, 5, 3005)
+    raise SystemExit(f"unknown apply case {name!r}")
+
+
+def run_apply(args):
+    """A few applies y = H x of one workload, timed with CUDA events (the commands the ncu summaries under
+    profiles/ use; plain text, not a bench line).  --case spin1_l18: spin-1 Heisenberg chain L=18, Sz=0;
+    --case mom_l28: J1-J2 chain L=28 (J2 = 0.25), Sz=0, momentum index --k."""
+    import alps_b200 as ed
+    if args.case == "spin1_l18":
+        L = 18
+        ham = ed.Hamiltonian(L, L, [(i, (i + 1) % L, 1.0, 1.0, 0.0) for i in range(L)], two_s=2)
+    elif args.case == "mom_l28":
+        params = {"MODEL": "spin", "LATTICE": "nnn chain lattice", "L": 28}
+        k = ed.lattice_momenta(params)[args.k]
+        ham = ed.Hamiltonian(28, 14, chain_bonds(28, 0.25), translations=ed.lattice_translations(params, k))
+    else:
+        N, n_up, bonds = apply_case_bonds(args.case)
+        ham = ed.Hamiltonian(N, n_up, bonds, precision=ed.FP64 if args.apply_precision == "fp64" else ed.FP32)
+    x, y = ham.new_vector(), ham.new_vector()
+    ham.fill_random(x, 1)
+    if args.case in ("spin1_l18", "mom_l28"):
+        ham.time_mult(x, y, 1)
+        print(f"{args.case} rows={ham.dim} apply_ms={ham.time_mult(x, y, args.reps):.4f}")
+        return
+    names = ed.apply_variants()
+    if args.sweep:
+        for v, name in enumerate(names):
+            try:
+                m0, _ = ham.time_apply(x, y, args.reps, v, False)
+                m1, _ = ham.time_apply(x, y, args.reps, v, True)
+                print(f"{args.case} {args.apply_precision} variant {v} ({name}): apply_ms={m0:.4f} "
+                      f"with_alpha_ms={m1:.4f}")
+            except ed.AEDError as e:
+                print(f"{args.case} {args.apply_precision} variant {v} ({name}): {e}")
+        return
+    ham.time_apply(x, y, 1, args.variant, args.alpha)
+    ms, v = ham.time_apply(x, y, args.reps, args.variant, args.alpha)
+    print(f"{args.case} {args.apply_precision} D={ham.dim} variant={v} ({names[v]}) alpha={int(args.alpha)} "
+          f"apply_ms={ms:.4f}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -749,14 +798,24 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="l28", choices=["l28", "square", "batch", "serve", "momentum", "spin"])
+    ap.add_argument("--workload", default="l28",
+                    choices=["l28", "square", "batch", "serve", "momentum", "spin", "apply"])
+    ap.add_argument("--case", default="l28", help="apply: l24, l26, l28, sq6x5, spin1_l18, mom_l28")
+    ap.add_argument("--apply-precision", default="fp64", choices=["fp64", "fp32"], help="apply: vector precision")
+    ap.add_argument("--variant", type=int, default=-1, help="apply: variant index (-1: autotuned)")
+    ap.add_argument("--reps", type=int, default=3, help="apply: timed applies")
+    ap.add_argument("--sweep", action="store_true", help="apply: time every variant with and without partials")
+    ap.add_argument("--alpha", action="store_true", help="apply: with the Lanczos step's <x,y> partials")
+    ap.add_argument("--k", type=int, default=0, help="apply mom_l28: momentum index")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="serve: engine precision")
     ap.add_argument("--steps-per-launch", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "apply":
+        run_apply(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "momentum":
         run_momentum(args)
