@@ -390,6 +390,12 @@ def run_ours(args):
         cpu = cpu_sample(float(j2s[W]), int(round(np.mean(iters))))
         cpu_all = cpu_matfree_sample(float(j2s[W]), int(round(np.mean(iters))))
     ham.close()
+    # the other configurations, on one GPU only (their own sections, not part of `value`)
+    others = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        others = {"cfg1_chain16": chain16_result(ed), "cfg3_square6x5": square_result(ed),
+                  "cfg4_batch512": batch_result(ed, args.steps_per_launch, with_cpu=not args.no_cpu)}
+        print(f"[bench] configs: {json.dumps(others)[:2000]}", file=sys.stderr)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -401,7 +407,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (each vector 321 MB); no flush"},
             "iterations": iters, "evals": evals, "wall_s": wall,
             "roofline": roof, "cpu_baseline": cpu, "cpu_baseline_all_cores": cpu_all, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(), "mixed": mixed,
+            "clocks": clocks.summary(), "mixed": mixed, "configs": others,
         }
         print(json.dumps(line))
     if pg is not None:
@@ -479,37 +485,75 @@ def cpu_solve_estimate(N, bonds, nev, iterations, rows=200_000):
     return (tb + iterations * (tp + tv)) * D / r, f"sample {r} rows"
 
 
-def run_square(args):
-    """Config 3: 6x5 square lattice, per-bond J ~ U[0.8,1.2] (seed 3005): mixed vs plain FP64."""
-    import alps_b200 as ed
-
+def square_result(ed, solves=1):
+    """Config 3: 6x5 square lattice, per-bond J ~ U[0.8,1.2] (seed 3005), lowest eigenvalue: FP64 and mixed
+    solves (the apply variant tuned and the FP32 store grown by an untimed solve first), with the applies'
+    achieved bandwidth by algorithmic bytes."""
     bonds = square_bonds(6, 5, 3005)
     out = {}
     for name, prec in (("fp64", ed.FP64), ("mixed", ed.FP32)):
         ham = ed.Hamiltonian(30, 15, bonds, precision=prec)
-        x, y = ham.new_vector(), ham.new_vector()  # untimed: the apply variant is tuned once per process
-        ham.fill_random(x, 1)
-        ham.time_apply(x, y, 1)
-        x.free()
-        y.free()
-        t0 = time.perf_counter()
-        r = ham.solve(nev=1, seed=1, profile=True)
-        out[name] = {"seconds": time.perf_counter() - t0, "evals": r["evals"].tolist(), "iterations": r["iterations"],
-                     "iterations_low": r["iterations_low"], "apply_ms": r["apply_ms"]}
+        ham.solve(nev=1, seed=1)
+        ts, rs = [], []
+        for _ in range(solves):
+            t0 = time.perf_counter()
+            rs.append(ham.solve(nev=1, seed=1, profile=True))
+            ts.append(time.perf_counter() - t0)
+        r = rs[-1]
+        out[name] = {"seconds": float(np.mean(ts)), "evals": r["evals"].tolist(), "iterations": r["iterations"],
+                     "iterations_low": r["iterations_low"], "apply_ms": r["apply_ms"],
+                     "refined_by": r.get("refined_by")}
         ham.close()
     D = 155117520
     nbar = 60 * 2 * comb(28, 14) / D
-    rel = abs(out["mixed"]["evals"][0] - out["fp64"]["evals"][0]) / abs(out["fp64"]["evals"][0])
     peak, _ = read_peaks()
     g64 = D * ((1 + nbar) * 8 + 8) / (out["fp64"]["apply_ms"] / 1e3) / 1e9
     g32 = D * ((1 + nbar) * 4 + 4) / (out["mixed"]["apply_ms"] / 1e3) / 1e9
-    line = {"metric": "6x5 square lattice ground state: solves/s, mixed vs FP64", "value": 1.0 / out["mixed"]["seconds"],
-            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "square lattice 6x5 periodic, Sz=0, D=155117520, J_b~U[0.8,1.2] seed 3005, k=1"},
-            "fp64": out["fp64"], "mixed": out["mixed"], "speedup_mixed_vs_fp64": out["fp64"]["seconds"] / out["mixed"]["seconds"],
+    rel = abs(out["mixed"]["evals"][0] - out["fp64"]["evals"][0]) / abs(out["fp64"]["evals"][0])
+    return {"workload": "square lattice 6x5 periodic, Sz=0, D=155117520, J_b~U[0.8,1.2] seed 3005, k=1",
+            "fp64": out["fp64"], "mixed": out["mixed"],
+            "fp64_solves_per_s": 1.0 / out["fp64"]["seconds"], "mixed_solves_per_s": 1.0 / out["mixed"]["seconds"],
+            "speedup_mixed_vs_fp64": out["fp64"]["seconds"] / out["mixed"]["seconds"],
             "rel_energy_err_mixed_vs_fp64": rel,
-            "hv_gbs": {"fp64": g64, "fp32": g32, "peak": peak, "frac_fp32": g32 / peak, "frac_fp64": g64 / peak}}
+            "hv_gbs": {"fp64": g64, "fp32": g32, "peak": peak, "frac_fp64": g64 / peak, "frac_fp32": g32 / peak,
+                       "bytes_per_row_fp64": (1 + nbar) * 8 + 8, "bytes_per_row_fp32": (1 + nbar) * 4 + 4}}
+
+
+def run_square(args):
+    """Config 3 alone: one JSON line."""
+    import alps_b200 as ed
+
+    sq = square_result(ed, solves=max(1, args.steps))
+    line = {"metric": "6x5 square lattice ground state: solves/s, mixed vs FP64", "value": sq["mixed_solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": sq["workload"]}}
+    line.update({k: v for k, v in sq.items() if k != "workload"})
     print(json.dumps(line))
+
+
+def chain16_result(ed, reps=20):
+    """Config 1: Heisenberg chain L=16 periodic, J=1, Sz=0 (D=12,870), lowest 4 eigenvalues, FP64: complete
+    solves on the GPU (after one untimed solve) and the oracle's complete solve of the reference algorithm
+    (explicit matrix in hamiltonian_matrix's element order, ietl Lanczos) on one host core."""
+    import oracle
+
+    bonds = [(i, (i + 1) % 16, 1.0, 1.0, 0.0) for i in range(16)]
+    ham = ed.Hamiltonian(16, 8, bonds)
+    ham.solve(nev=4, seed=1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r = ham.solve(nev=4, seed=1)
+    gpu_s = (time.perf_counter() - t0) / reps
+    ham.close()
+    t0 = time.perf_counter()
+    M = oracle.Matrix(16, 8, bonds)
+    o = M.lanczos(nev=4, seed=1)
+    cpu_s = time.perf_counter() - t0
+    return {"workload": "Heisenberg chain L=16 periodic, J=1, Sz=0, D=12870, lowest 4 eigenvalues, FP64",
+            "gpu_solves_per_s": 1.0 / gpu_s, "gpu_iterations": r["iterations"], "evals": r["evals"].tolist(),
+            "cpu_reference_port_solves_per_s": 1.0 / cpu_s, "cpu_iterations": o["iterations"],
+            "cpu_cores": 1, "max_rel_diff_vs_cpu": float(np.max(np.abs(r["evals"] - o["evals"]) / np.abs(o["evals"]))),
+            "speedup_gpu_vs_cpu": cpu_s / gpu_s}
 
 
 def run_momentum(args):
@@ -601,15 +645,13 @@ def run_spin(args):
     print(json.dumps(line))
 
 
-def run_batch(args):
+def batch_result(ed, steps_per_launch=8, with_cpu=True):
     """Config 4: 512 J1-J2 chains through the batched engine, mixed and FP64, and through the
     single-instance FP64 drop-in one after the other."""
-    import alps_b200 as ed
-
     reqs = batch_requests()
     res = {}
     for name, prec in (("mixed", ed.FP32), ("fp64", ed.FP64)):
-        srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1)  # pool mapped up front
+        srv = ed.Server(precision=prec, max_slots=512, steps=steps_per_launch, reserve=-1)  # pool mapped up front
         w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs[:8]]  # warm-up
         srv.run(w)
         t0 = time.perf_counter()
@@ -637,32 +679,40 @@ def run_batch(args):
         h.close()
     rel = compare_energies(res["mixed"]["evals"], single)
     rel64 = compare_energies(res["fp64"]["evals"], single)
-    line = {"metric": "batched Lanczos solves/s (512 J1-J2 chains, L 12..22), mixed vs plain FP64",
-            "value": res["mixed"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
-            "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "512 J1-J2 chains, L~U{12..22} even, J2~U[0,1] seed 5124, Sz=0, k=2",
-                       "steps_per_graph": args.steps_per_launch},
-            "mixed_batched": {k: v for k, v in res["mixed"].items() if k != "evals"},
-            "fp64_batched": {k: v for k, v in res["fp64"].items() if k != "evals"},
-            "fp64_single_instance": {"seconds": t_single, "solves_per_s": len(reqs) / t_single},
-            "speedup_mixed_batched_vs_fp64_single": res["mixed"]["solves_per_s"] / (len(reqs) / t_single),
-            "speedup_mixed_batched_vs_fp64_batched": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
-            "rel_energy_err_mixed_vs_fp64_single": rel, "rel_energy_err_fp64_batched_vs_single": rel64}
-    if not args.no_cpu:
-        classes = {}
+    out = {"workload": "512 J1-J2 chains, L~U{12..22} even, J2~U[0,1] seed 5124, Sz=0, k=2",
+           "steps_per_graph": steps_per_launch,
+           "mixed_batched": {k: v for k, v in res["mixed"].items() if k != "evals"},
+           "fp64_batched": {k: v for k, v in res["fp64"].items() if k != "evals"},
+           "fp64_single_instance": {"seconds": t_single, "solves_per_s": len(reqs) / t_single},
+           "speedup_mixed_batched_vs_fp64_single": res["mixed"]["solves_per_s"] / (len(reqs) / t_single),
+           "speedup_mixed_batched_vs_fp64_batched": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
+           "rel_energy_err_mixed_vs_fp64_single": rel, "rel_energy_err_fp64_batched_vs_single": rel64}
+    if with_cpu:
+        classes, counts = {}, {}
         for n, b, nev, sd in reqs:
             classes.setdefault(n, (b, nev))
-        tot, notes = 0.0, {}
-        counts = {}
-        for n, b, nev, sd in reqs:
             counts[n] = counts.get(n, 0) + 1
+        tot, notes = 0.0, {}
         for n, (b, nev) in sorted(classes.items()):
             t, how = cpu_solve_estimate(n, b, nev, 120)
             tot += t * counts[n]
             notes[n] = f"{t:.3g} s ({how})"
-        line["cpu_baseline"] = {"value": len(reqs) / tot, "unit": "solves/s", "cores": 1, "kind": "port",
-                                "sample": "one instance per chain length, explicit-matrix Lanczos on one core "
-                                          "(row sample x 120 iterations above 60000 states): " + json.dumps(notes)}
+        out["cpu_baseline"] = {"value": len(reqs) / tot, "unit": "solves/s", "cores": 1, "kind": "port",
+                               "sample": "one instance per chain length, explicit-matrix Lanczos on one core "
+                                         "(row sample x 120 iterations above 60000 states): " + json.dumps(notes)}
+    return out
+
+
+def run_batch(args):
+    """Config 4 alone: one JSON line."""
+    import alps_b200 as ed
+
+    b = batch_result(ed, args.steps_per_launch, with_cpu=not args.no_cpu)
+    line = {"metric": "batched Lanczos solves/s (512 J1-J2 chains, L 12..22), mixed vs plain FP64",
+            "value": b["mixed_batched"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": b["workload"], "steps_per_graph": b["steps_per_graph"]}}
+    line.update({k: v for k, v in b.items() if k not in ("workload", "steps_per_graph")})
     print(json.dumps(line))
 
 
@@ -711,7 +761,37 @@ def run_serve(args):
     print(json.dumps(line))
 
 
+def reference_complete_solves():
+    """Complete solves of the reference algorithm's restatement (explicit matrix in hamiltonian_matrix's
+    element order, ietl Lanczos and T-matrix rules) on one host core, the reference path being single-threaded:
+    config 1 (Heisenberg chain L=16, lowest 4) and one chain of each config-4 length up to L=20 (the first
+    of the seed-5124 requests with that length, lowest 2)."""
+    import oracle
+
+    out = {}
+    cases = [("cfg1_chain16_k4", 16, [(i, (i + 1) % 16, 1.0, 1.0, 0.0) for i in range(16)], 4)]
+    seen = set()
+    for n, b, nev, _ in batch_requests():
+        if n <= 20 and n not in seen:
+            seen.add(n)
+            cases.append((f"cfg4_chain{n}_k{nev}", n, b, nev))
+    for name, n, b, nev in sorted(cases, key=lambda c: c[1]):
+        t0 = time.perf_counter()
+        M = oracle.Matrix(n, n // 2, b)
+        o = M.lanczos(nev=nev, seed=1)
+        dt = time.perf_counter() - t0
+        out[name] = {"dimension": int(M.D), "seconds": dt, "solves_per_s": 1.0 / dt, "iterations": o["iterations"],
+                     "evals": o["evals"].tolist()}
+    return out
+
+
 def run_reference(args):
+    """The reference's algorithm on the host cores (the oracle port: the reference itself needs Boost and
+    LAPACK, absent here) for the default workload.  A complete L=28 solve of the reference algorithm does not
+    fit the run (its explicit matrix alone is ~75 GB of map nodes), so each step is a bounded sample: the
+    explicit-matrix build, the row sums and the make_step vector passes over a block of rows with all host
+    threads, scaled by D / rows to the sector and by the iteration count of the FP64 solve to one solve.
+    Complete solves of configs 1 and 4 ride along in their own section."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -721,23 +801,37 @@ def run_reference(args):
     K, W = args.steps, args.warmup
     j2s = j2_stream(W + K)
     threads = oracle.num_threads()
-    vals = []
-    sample = None
+    N, n_up = L28, L28 // 2
+    states = oracle.basis_fast(N, n_up)
+    D = states.size
+    rows = min(D // 4, 120_000 * threads)
+    r0 = D // 3
+    vals, walls, parts = [], [], None
     for k, j2 in enumerate(j2s):
-        s = cpu_sample(float(j2), FP64_ITERATIONS_FALLBACK, threads_note="1 thread (the reference path is "
-                       "single-threaded; no OpenMP on it)", rows=200_000)
+        t0 = time.perf_counter()
+        tb, tp, tv = oracle.sample_times_mt(N, states, chain_bonds(L28, float(j2)), r0, r0 + rows)
+        wall = time.perf_counter() - t0
+        scale = D / rows
+        solve_s = tb * scale + FP64_ITERATIONS_FALLBACK * (tp + tv) * scale
         if k >= W:
-            vals.append(s["value"])
-            sample = s
+            vals.append(1.0 / solve_s)
+            walls.append(wall)
+            parts = (tb, tp, tv)
     v = float(np.mean(vals))
+    sample = (f"rows [{r0}, {r0 + rows}) of the L=28 sector ({rows / D:.2%}) per step on {threads} threads: "
+              f"explicit-matrix row build ({parts[0]:.2f} s), row sums ({parts[1] * 1e3:.1f} ms), make_step vector "
+              f"passes ({parts[2] * 1e3:.1f} ms), scaled by D/rows = {D / rows:.1f} and build once + "
+              f"{FP64_ITERATIONS_FALLBACK} iterations (the mean FP64 iteration count of these inputs)")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "impl": "reference",
+            "ms_per_step": float(np.mean(walls)) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": "J1-J2 chain L=28 periodic, Sz=0, D=40116600, J1=1, J2~U[0,0.5] seed 2802, "
                                    "lowest 2 eigenvalues, FP64 Lanczos (ietl rule 100 eps)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample["sample"],
-                             "host_threads_available": threads},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "value_from": "extrapolated: a step is a bounded row sample (ms_per_step is its wall time); value is "
+                          "that sample scaled to one complete solve",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "complete_solves": reference_complete_solves()}
     print(json.dumps(line))
 
 
@@ -798,6 +892,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the config-1/3/4 sections of the default line")
     ap.add_argument("--workload", default="l28",
                     choices=["l28", "square", "batch", "serve", "momentum", "spin", "apply"])
     ap.add_argument("--case", default="l28", help="apply: l24, l26, l28, sq6x5, spin1_l18, mom_l28")

@@ -90,6 +90,8 @@ def lib():
         L.orc_rows_mult.argtypes = [ctypes.c_int, _c_u32_p, ctypes.c_int64, _c_dbl_p, _c_dbl_p, ctypes.c_int,
                                     _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, ctypes.c_int64,
                                     ctypes.c_int64, _c_dbl_p, _c_dbl_p]
+        L.orc_sample_times_mt.restype = None
+        L.orc_sample_times_mt.argtypes = L.orc_sample_times.argtypes
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_num_threads.argtypes = []
         _lib = L
@@ -330,6 +332,21 @@ def sample_times(N, states, bonds, r0, r1):
     lib().orc_sample_times(N, _p(states, _c_u32_p), states.size, len(bonds), _p(s1, _c_int_p), _p(s2, _c_int_p),
                            _p(jz, _c_dbl_p), _p(jxy, _c_dbl_p), r0, r1, ctypes.byref(tb), ctypes.byref(tp),
                            ctypes.byref(tv))
+    return tb.value, tp.value, tv.value
+
+
+def sample_times_mt(N, states, bonds, r0, r1):
+    """sample_times with all host threads (contiguous row blocks per thread): wall seconds of the
+    matrix build, the row sums and the vector passes over rows [r0, r1)."""
+    states = np.ascontiguousarray(states, dtype=np.uint32)
+    s1 = np.array([b[0] for b in bonds], dtype=np.int32)
+    s2 = np.array([b[1] for b in bonds], dtype=np.int32)
+    jz = np.array([b[2] for b in bonds], dtype=np.float64)
+    jxy = np.array([b[3] for b in bonds], dtype=np.float64)
+    tb, tp, tv = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+    lib().orc_sample_times_mt(N, _p(states, _c_u32_p), states.size, len(bonds), _p(s1, _c_int_p), _p(s2, _c_int_p),
+                              _p(jz, _c_dbl_p), _p(jxy, _c_dbl_p), r0, r1, ctypes.byref(tb), ctypes.byref(tp),
+                              ctypes.byref(tv))
     return tb.value, tp.value, tv.value
 
 

@@ -811,6 +811,99 @@ void orc_rows_mult(int N, const uint32_t* states, int64_t D, const double* site_
   }
 }
 
+// orc_sample_times with all host threads: the rows [r0, r1) are dealt to the
+// OpenMP threads in contiguous blocks; each thread builds its block's rows of
+// the explicit matrix (reference element order, lower_bound lookups), then
+// forms its rows of y = prod(M, x), then the make_step vector passes over as
+// many elements.  Wall times of the three phases (each ends at a barrier).
+void orc_sample_times_mt(int N, const uint32_t* states, int64_t D, int nb, const int* s1, const int* s2,
+                         const double* jz, const double* jxy, int64_t r0, int64_t r1, double* t_build,
+                         double* t_prod, double* t_vec) {
+  using clk = std::chrono::steady_clock;
+  if (r1 > D) r1 = D;
+  const int64_t R = r1 - r0;
+  std::vector<BondTensor> bt(nb);
+  for (int b = 0; b < nb; ++b) bt[b] = spin_bond(jz[b], jxy[b], 0.0);
+  std::vector<double> x(D), y(R);
+  for (int64_t i = 0; i < D; ++i) x[i] = start_value(1, (uint64_t)i);
+  double tb = 0, tp = 0, tv = 0, dot_total = 0.0;
+#pragma omp parallel
+  {
+    int nt = 1, id = 0;
+#ifdef _OPENMP
+    nt = omp_get_num_threads();
+    id = omp_get_thread_num();
+#endif
+    const int64_t a = r0 + R * id / nt, b = r0 + R * (id + 1) / nt;
+    std::vector<int64_t> rp(b - a + 1, 0);
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    std::vector<Entry> row;
+#pragma omp barrier
+    clk::time_point t0 = clk::now();
+    for (int64_t i = a; i < b; ++i) {
+      row.clear();
+      row_add(row, i, 1.0);
+      row_add(row, i, -1.0);
+      const uint32_t state = states[i];
+      for (int q = 0; q < nb; ++q) {
+        const int b1 = N - 1 - s1[q], b2 = N - 1 - s2[q];
+        const int is1 = (state >> b1) & 1, is2 = (state >> b2) & 1;
+        for (int js1 = 0; js1 < 2; ++js1)
+          for (int js2 = 0; js2 < 2; ++js2) {
+            const double v = bt[q].m[is1][is2][js1][js2];
+            if (v == 0.0) continue;
+            uint32_t ns = state;
+            ns = (ns & ~(1u << b1)) | ((uint32_t)js1 << b1);
+            ns = (ns & ~(1u << b2)) | ((uint32_t)js2 << b2);
+            const int64_t j = lb_index(states, D, ns);
+            if (j < D) row_add(row, j, v);
+          }
+      }
+      std::sort(row.begin(), row.end(), [](const Entry& e1, const Entry& e2) { return e1.j < e2.j; });
+      for (auto& e : row) {
+        col.push_back((int32_t)e.j);
+        val.push_back(e.v);
+      }
+      rp[i - a + 1] = (int64_t)col.size();
+    }
+#pragma omp barrier
+    clk::time_point t1 = clk::now();
+    for (int64_t i = a; i < b; ++i) {
+      double t = 0.0;
+      for (int64_t p = rp[i - a]; p < rp[i - a + 1]; ++p) t += val[p] * x[col[p]];
+      y[i - r0] = t;
+    }
+#pragma omp barrier
+    clk::time_point t2 = clk::now();
+    // make_step's vector passes over this thread's elements (dot, two axpy, norm, divide)
+    double dd = 0.0;
+    for (int64_t i = a; i < b; ++i) dd += x[i] * y[i - r0];
+#pragma omp atomic
+    dot_total += dd;
+#pragma omp barrier
+    const double al = dot_total;
+    double nn = 0.0;
+    for (int64_t i = a; i < b; ++i) {
+      y[i - r0] -= al * x[i];
+      y[i - r0] -= 0.3 * x[i];
+      nn += y[i - r0] * y[i - r0];
+    }
+    for (int64_t i = a; i < b; ++i) y[i - r0] /= (nn + 1.0);
+#pragma omp barrier
+    clk::time_point t3 = clk::now();
+#pragma omp single
+    {
+      tb = std::chrono::duration<double>(t1 - t0).count();
+      tp = std::chrono::duration<double>(t2 - t1).count();
+      tv = std::chrono::duration<double>(t3 - t2).count();
+    }
+  }
+  *t_build = tb;
+  *t_prod = tp;
+  *t_vec = tv;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
