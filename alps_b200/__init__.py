@@ -77,6 +77,7 @@ class SolveOpts(ctypes.Structure):
         ("nev", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("rtol", ctypes.c_double),
         ("atol", ctypes.c_double), ("seed", ctypes.c_uint64), ("start", ctypes.POINTER(ctypes.c_double)),
         ("refine", ctypes.c_int32), ("profile", ctypes.c_int32), ("resume", ctypes.c_int32),
+        ("reorth", ctypes.c_int32),
     ]
 
 
@@ -178,6 +179,8 @@ def lib():
             "aed_apply_variant_count": (_I32, []),
             "aed_apply_variant_name": (ctypes.c_char_p, [_I32]),
             "aed_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+            "aed_lanczos_vector": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+            "aed_last_tmatrix_fp32": (ctypes.c_int, [_P, _DP, _DP, _I32, _I32P]),
             "aed_launch_count": (ctypes.c_int, [_I64P]),
             "aed_dot_noalloc": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
             "aed_tmatrix": (ctypes.c_int, [_I32, _DP, _DP, _I32, _DP, _DP, _I32P, _I32P]),
@@ -647,11 +650,13 @@ class Hamiltonian:
 
     # -- solves ---------------------------------------------------------------------
     def solve(self, nev=1, max_iter=0, seed=0, start=None, rtol=0.0, atol=0.0, refine=0, profile=False,
-              resume=False):
+              resume=False, reorth=False):
         """Lanczos eigenvalues (aed_solve).  resume=True continues the live FP64 recurrence (the last
-        solve's, or one restored by lanczos_load) until nev values converge."""
+        solve's, or one restored by lanczos_load) until nev values converge.  reorth=True (FP32 handles)
+        reorthogonalises every FP32 Lanczos vector against the stored basis."""
         st = None if start is None else self._host_vector(start)
-        opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0, 1 if resume else 0)
+        opts = SolveOpts(nev, max_iter, rtol, atol, seed, _dp(st), refine, 1 if profile else 0, 1 if resume else 0,
+                         1 if reorth else 0)
         res = SolveResult()
         _check(lib().aed_solve(self._h, ctypes.byref(opts), ctypes.byref(res)))
         n = res.n_evals
@@ -692,12 +697,23 @@ class Hamiltonian:
         _check(lib().aed_get_stream(self._h, ctypes.byref(p)))
         return p.value or 0
 
-    def last_tmatrix(self):
+    def lanczos_vector(self, j):
+        """v_j of the FP32 Lanczos basis the last mixed solve stored (aed_lanczos_vector), as float64."""
+        v = self.new_vector()
+        _check(lib().aed_lanczos_vector(self._h, j, v.ptr))
+        out = v.download()
+        v.free()
+        return out
+
+    def last_tmatrix(self, fp32_phase=False):
+        """alpha, beta of the last solve's FP64 recurrence (aed_last_tmatrix), or with fp32_phase=True of the
+        last mixed solve's FP32 phase (aed_last_tmatrix_fp32)."""
+        f = lib().aed_last_tmatrix_fp32 if fp32_phase else lib().aed_last_tmatrix
         n = ctypes.c_int32(0)
-        _check(lib().aed_last_tmatrix(self._h, None, None, 0, ctypes.byref(n)))
+        _check(f(self._h, None, None, 0, ctypes.byref(n)))
         a = np.zeros(max(n.value, 1))
         b = np.zeros(max(n.value, 1))
-        _check(lib().aed_last_tmatrix(self._h, _dp(a), _dp(b), n.value, ctypes.byref(n)))
+        _check(f(self._h, _dp(a), _dp(b), n.value, ctypes.byref(n)))
         return a[: n.value], b[: n.value]
 
 

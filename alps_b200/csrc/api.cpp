@@ -243,6 +243,7 @@ void handle_release_workspace(aed_handle* h) {
   for (void* p : h->store_chunks) mem_dev_free(p, h->stream);
   h->store_chunks.clear();
   h->store_chunk_bytes = 0;
+  h->store_m = 0;
   h->last_rr = false;
   for (int k = 0; k < aed_handle::kWorkspaces; ++k) {
     mem_dev_free(h->ws[k], h->stream);
@@ -1341,6 +1342,16 @@ int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, in
   return AED_OK;
 }
 
+int aed_last_tmatrix_fp32(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n) {
+  if (!h || !n) return fail(AED_ERR_INVALID, "NULL argument");
+  *n = (int32_t)h->low_alpha.size();
+  for (int32_t i = 0; i < *n && i < cap; ++i) {
+    if (alpha) alpha[i] = h->low_alpha[i];
+    if (beta) beta[i] = h->low_beta[i];
+  }
+  return AED_OK;
+}
+
 int aed_time_apply(aed_handle* h, const void* x, void* y, int32_t reps, int32_t variant, int32_t with_alpha,
                    double* ms, int32_t* variant_used) {
   int rc = check_vec(h, x, "x");
@@ -1414,6 +1425,19 @@ int aed_tmatrix(int32_t n, const double* alpha, const double* beta, int32_t cap,
     if (mults) mults[i] = t.mults[i];
   }
   *count = c;
+  return AED_OK;
+}
+
+int aed_lanczos_vector(aed_handle* h, int32_t j, void* out) {
+  if (!h || !out) return fail(AED_ERR_INVALID, "NULL argument");
+  if (h->precision != AED_FP32 || j < 0 || j >= h->store_m || h->store_chunk_bytes == 0 ||
+      (size_t)(j / kStoreChunk) >= h->store_chunks.size())
+    return fail(AED_ERR_INVALID, "lanczos_vector: no such vector of a mixed solve's FP32 phase");
+  DeviceGuard g(h->device);
+  const size_t vbytes = h->store_chunk_bytes / kStoreChunk;
+  const char* src = (const char*)h->store_chunks[j / kStoreChunk] + (size_t)(j % kStoreChunk) * vbytes;
+  AED_CUDA_TRY(cudaMemcpyAsync(out, src, (size_t)h->vlen * 4, cudaMemcpyDeviceToDevice, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return AED_OK;
 }
 

@@ -71,6 +71,8 @@ struct aed_handle {
   size_t ws_bytes[kWorkspaces] = {0, 0, 0};
   std::vector<void*> store_chunks;  // FP32 Lanczos basis of the mixed path, kStoreChunk vectors each
   size_t store_chunk_bytes = 0;
+  int store_m = 0;  // vectors of the last mixed solve's FP32 phase in the store (v_0 .. v_{m-1})
+  std::vector<double> low_alpha, low_beta;  // that FP32 phase's recurrence
   double* h_ab = nullptr;  // pinned alpha/beta staging
   size_t h_ab_n = 0;
   // last solve: the alpha/beta recurrence of its FP64 phase.  v_{m-1} and v_m

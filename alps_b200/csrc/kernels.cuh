@@ -113,6 +113,15 @@ int launch_gram(const VecSet& X, const VecSet& Y, int K, int64_t n, double* part
 int launch_resid(const VecSet& X, const VecSet& Y, const ResidCoef& rc, int K, int R, int64_t n, double* part,
                  double* out, cudaStream_t st);
 
+// Full reorthogonalisation of the mixed path (refine.cu): chunk partials of
+// <V_k, w> for the m <= kMaxComb vectors of one store chunk into
+// part[(k0 + k) * red_chunks(n) + c]; the sums of np such rows; w -= t with
+// one rounding to FP32.
+int launch_block_dot(const float* V, int64_t ld, int m, const float* w, int64_t n, double* part, int k0,
+                     cudaStream_t st);
+int launch_finish_many(const double* part, int64_t nch, int np, double* out, cudaStream_t st);
+int launch_sub_round(const double* t, float* w, int64_t n, cudaStream_t st);
+
 int64_t launch_count();
 // After a launch in another translation unit: counts it and returns
 // AED_ERR_CUDA (with the launch error) if it failed.

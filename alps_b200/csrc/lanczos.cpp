@@ -22,6 +22,7 @@
 #include <future>
 #include <deque>
 #include <chrono>
+#include <functional>
 #include <cmath>
 #include <cstring>
 
@@ -118,6 +119,40 @@ constexpr int kMaxRing = 5;
 inline int lanczos_lookahead(const aed_handle* h) { return h->vlen >= ((int64_t)1 << 24) ? 1 : 3; }
 inline int ring_slots(const aed_handle* h) { return lanczos_lookahead(h) + 2; }
 
+// Full reorthogonalisation of an FP32 recurrence whose vectors v_0 .. v_j are
+// kept in the FP32 store (chunks of kStoreChunk vectors, stride ldv): after
+// the update, w -= V (V^T w) twice (classical Gram-Schmidt with one repeat,
+// Daniel, Gragg, Kaufman & Stewart, Math. Comp. 30 (1976) 772-795), the dots
+// and the combination accumulated in FP64, w rounded to FP32 once per pass;
+// the T-matrix keeps the recurrence's alpha and beta.  All on the device.
+struct Reorth {
+  bool on = false;
+  std::function<void*(int)> vec;  // v_j in the store
+  int64_t ldv = 0;
+  double* part = nullptr;  // (cap) x red_chunks(D) chunk partials
+  double* coef = nullptr;  // cap coefficients
+  double* tmp = nullptr;   // D doubles: V c
+  int cap = 0;
+};
+
+int reorthogonalise(aed_handle* h, const Reorth& ro, int j, float* w) {
+  const int64_t D = h->vlen, nch = red_chunks(D);
+  const int m = j + 1;  // against v_0 .. v_j
+  if (m > ro.cap) return fail(AED_ERR_INVALID, "reorthogonalisation: more vectors than the store holds");
+  int rc = AED_OK;
+  for (int pass = 0; pass < 2 && !rc; ++pass) {
+    for (int k0 = 0; k0 < m && !rc; k0 += kStoreChunk)
+      rc = launch_block_dot((const float*)ro.vec(k0), ro.ldv, std::min(kStoreChunk, m - k0), w, D, ro.part, k0,
+                            h->stream);
+    if (!rc) rc = launch_finish_many(ro.part, nch, m, ro.coef, h->stream);
+    for (int k0 = 0; k0 < m && !rc; k0 += kStoreChunk)
+      rc = launch_ritz_combine((const float*)ro.vec(k0), ro.ldv, std::min(kStoreChunk, m - k0), ro.coef + k0, ro.tmp,
+                               D, k0 > 0, h->stream);
+    if (!rc) rc = launch_sub_round(ro.tmp, w, D, h->stream);
+  }
+  return rc;
+}
+
 // One Lanczos recurrence on device vectors of type T.  Vectors rotate through
 // `slot(j)`, the buffer that receives v_j.  Returns T-matrix and convergence.
 struct Recurrence {
@@ -133,6 +168,7 @@ struct Recurrence {
   double amax = 0, bmax = 0;
   bool profile = false;
   std::vector<cudaEvent_t> tev;  // (start, stop) per apply when profiling
+  const Reorth* reorth = nullptr;  // FP32 recurrences over the store: full reorthogonalisation
 
   ~Recurrence() {
     for (auto e : tev) cudaEventDestroy(e);
@@ -167,7 +203,20 @@ struct Recurrence {
     if (rc) return rc;
     if (profile) AED_CUDA_TRY(cudaEventRecord(e1, h->stream));
     const double* bprev = j > 0 ? d_ab + 2 * (j - 1) + 1 : nullptr;
-    rc = lanczos_step_tail(h, f32, vprev, x, y, bprev, d_ab + 2 * j, d_ab + 2 * j + 1);
+    if (reorth && reorth->on && f32) {
+      // update, then w -= V V^T w, then beta = |w| and the normalisation (lanczos.h:398-402)
+      double* alpha = d_ab + 2 * j;
+      double* beta = d_ab + 2 * j + 1;
+      rc = launch_finish_sum(h->d_partA, h->alpha_tiles(), alpha, false, h->stream);
+      if (!rc) rc = launch_lanczos_update(alpha, (const float*)x, (const float*)vprev, bprev, (float*)y, D,
+                                          h->d_partB, h->stream);
+      if (!rc) rc = reorthogonalise(h, *reorth, j, (float*)y);
+      if (!rc) rc = launch_dot_partials((const float*)y, (const float*)y, D, h->d_partB, true, h->stream);
+      if (!rc) rc = launch_finish_sum(h->d_partB, red_chunks(D), beta, true, h->stream);
+      if (!rc) rc = launch_lanczos_normalize(beta, (float*)y, D, h->stream);
+    } else {
+      rc = lanczos_step_tail(h, f32, vprev, x, y, bprev, d_ab + 2 * j, d_ab + 2 * j + 1);
+    }
     if (rc) return rc;
     AED_CUDA_TRY(cudaMemcpyAsync(h_ab + 2 * j, d_ab + 2 * j, 16, cudaMemcpyDeviceToHost, h->stream));
     AED_CUDA_TRY(cudaEventRecord(ring->ev[j % EventRing::kN], h->stream));
@@ -619,7 +668,7 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
 
 // FP32 phase with the Lanczos basis stored in HBM, then FP64 refinement.
 int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev, int max_iter, double rtol,
-                double atol, bool profile, bool rayleigh_ritz_first, aed_solve_result* r) {
+                double atol, bool profile, bool rayleigh_ritz_first, bool reorth, aed_solve_result* r) {
   const int64_t D = h->vlen;
   // Lanczos basis store: chunks of kStoreChunk FP32 vectors, grown as the
   // recurrence advances and kept by the handle for later solves
@@ -662,6 +711,21 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   if ((rc = normalize(h, V0, D))) return rc;
   // phase 1: FP32 vectors, stop at FP32-level residual estimates
   Recurrence R{h, true, D, cap - 1, lanczos_lookahead(h), d_ab, hab, &ring, {}, {}, 0, 0, profile, {}};
+  Reorth ro;
+  if (reorth) {
+    const size_t part_bytes = (((size_t)cap * red_chunks(D) * 8) + 255) & ~(size_t)255;
+    const size_t coef_bytes = (((size_t)cap * 8) + 255) & ~(size_t)255;
+    void* w = nullptr;
+    if ((rc = handle_workspace(h, 2, part_bytes + coef_bytes + (size_t)D * 8, &w))) return rc;
+    ro.on = true;
+    ro.vec = slot;
+    ro.ldv = ldv;
+    ro.part = (double*)w;
+    ro.coef = (double*)((char*)w + part_bytes);
+    ro.tmp = (double*)((char*)w + part_bytes + coef_bytes);
+    ro.cap = cap;
+    R.reorth = &ro;
+  }
   const double tol32 = 2e-6;
   StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
@@ -670,6 +734,9 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   if (oom) return AED_ERR_NOMEM;
   if (rc) return rc;
   const int m1 = it1;
+  h->store_m = m1 + 1;  // v_0 .. v_m1 of this FP32 phase stay in the store
+  h->low_alpha.assign(R.alpha.begin(), R.alpha.begin() + m1);
+  h->low_beta.assign(R.beta.begin(), R.beta.begin() + m1);
   const int n1 = std::min(nev, (int)T1.evals.size());
   for (int i = 0; i < n1; ++i) r->evals_low[i] = T1.evals[i];
   r->iterations_low = m1;
@@ -771,12 +838,15 @@ int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r) {
     const double rtol = o->rtol > 0 ? o->rtol : 100 * eps;
     const double atol = o->atol > 0 ? o->atol : 100 * eps;
     if (o->refine < -1 || o->refine > 1) return fail(AED_ERR_INVALID, "refine must be -1, 0 or 1");
+    if (o->reorth && (h->precision != AED_FP32 || o->refine == -1 || o->resume))
+      return fail(AED_ERR_INVALID, "reorth needs the mixed path of an AED_FP32 handle (its Lanczos basis is stored)");
     if (o->resume) {  // continue the live FP64 recurrence (any handle precision)
       TmatInfo T;
       h->last_rr = false;
       rc = solve_fp64(h, nullptr, nullptr, 0, nev, max_iter, rtol, atol, false, 0.0, 0, o->profile != 0, r, T, true);
     } else if (h->precision == AED_FP32 && o->refine != -1) {
-      rc = solve_mixed(h, o->start, o->seed, nev, max_iter, rtol, atol, o->profile != 0, o->refine == 0, r);
+      rc = solve_mixed(h, o->start, o->seed, nev, max_iter, rtol, atol, o->profile != 0, o->refine == 0,
+                       o->reorth != 0, r);
       if (!rc && r->refined_by == AED_REFINE_NONE) r->refined_by = AED_REFINE_LANCZOS;
     } else {
       h->last_rr = false;

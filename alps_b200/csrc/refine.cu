@@ -129,6 +129,42 @@ __global__ void __launch_bounds__(kRedThreads) resid_partials_kernel(VecSet X, V
   }
 }
 
+// Chunk partials of <V_k, w> for the m <= kMaxComb stored FP32 vectors of one
+// store chunk (stride ld) and an FP32 vector w: part[(k0 + k) * pstride + c],
+// FP64 sums in chunk c's thread order and block tree.
+__global__ void __launch_bounds__(kRedThreads) block_dot_partials_kernel(const float* __restrict__ V, int64_t ld,
+                                                                        int m, const float* __restrict__ w,
+                                                                        int64_t n, double* __restrict__ part,
+                                                                        int k0, int64_t pstride) {
+  __shared__ double sm[33];
+  const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e0 = c * kRedChunk, e1 = e0 + kRedChunk < n ? e0 + kRedChunk : n;
+    double acc[kMaxComb];
+#pragma unroll
+    for (int k = 0; k < kMaxComb; ++k) acc[k] = 0.0;
+    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+      const double wv = (double)__ldg(w + i);
+#pragma unroll
+      for (int k = 0; k < kMaxComb; ++k)
+        if (k < m) acc[k] = fma((double)__ldg(V + (int64_t)k * ld + i), wv, acc[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxComb; ++k) {
+      if (k < m) {
+        const double tot = block_sum_all<kRedThreads>(acc[k], sm);
+        if (threadIdx.x == 0) part[(int64_t)(k0 + k) * pstride + c] = tot;
+      }
+    }
+  }
+}
+
+// w = (float)((double)w - t)
+__global__ void sub_round_kernel(const double* __restrict__ t, float* __restrict__ w, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = __double2float_rn((double)w[i] - t[i]);
+}
+
 // out[p] = sum of part[p * nch .. p * nch + nch) for p < np (one CTA each, finish_sum's order).
 __global__ void __launch_bounds__(kFinishThreads) finish_many_kernel(const double* __restrict__ part, int64_t nch,
                                                                      double* __restrict__ out) {
@@ -195,6 +231,29 @@ int launch_resid(const VecSet& X, const VecSet& Y, const ResidCoef& rcoef, int K
   if (rc) return rc;
   finish_many_kernel<<<R, kFinishThreads, 0, st>>>(part, nch, out);
   return check_launch_counted("finish_many_kernel");
+}
+
+int launch_block_dot(const float* V, int64_t ld, int m, const float* w, int64_t n, double* part, int k0,
+                     cudaStream_t st) {
+  if (m < 1 || m > kMaxComb) return fail(AED_ERR_INVALID, "block_dot: bad sizes");
+  const int64_t nch = red_chunks(n);
+  block_dot_partials_kernel<<<grid_for(nch), kRedThreads, 0, st>>>(V, ld, m, w, n, part, k0, nch);
+  return check_launch_counted("block_dot_partials_kernel");
+}
+
+int launch_finish_many(const double* part, int64_t nch, int np, double* out, cudaStream_t st) {
+  if (np < 1) return AED_OK;
+  finish_many_kernel<<<np, kFinishThreads, 0, st>>>(part, nch, out);
+  return check_launch_counted("finish_many_kernel");
+}
+
+int launch_sub_round(const double* t, float* w, int64_t n, cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (n + 255) / 256, cap = (int64_t)sms * 8;
+  sub_round_kernel<<<(int)(want < 1 ? 1 : (want < cap ? want : cap)), 256, 0, st>>>(t, w, n);
+  return check_launch_counted("sub_round_kernel");
 }
 
 }  // namespace aed

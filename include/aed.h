@@ -289,6 +289,10 @@ typedef struct {
                            or one aed_lanczos_load restored) until the stop rule holds
                            for nev values: ietl's more_eigenvalues (lanczos.h:77-78);
                            start / seed / refine are then ignored                      */
+  int32_t reorth;       /* 1: full reorthogonalisation of the mixed path's FP32 Lanczos
+                           vectors against the stored basis (classical Gram-Schmidt,
+                           twice, FP64 sums) each step; AED_FP32 handles, refine 0 or 1.
+                           An engine option: ietl's lanczos has no reorthogonalisation */
 } aed_solve_opts;
 
 #define AED_MAX_NEV 16
@@ -341,9 +345,13 @@ int aed_lanczos_state_bytes(aed_handle* h, int64_t* bytes);
 int aed_lanczos_save(aed_handle* h, void* buf, int64_t bytes);
 int aed_lanczos_load(aed_handle* h, const void* buf, int64_t bytes);
 
-/* Copy the alpha/beta recurrence of the last aed_solve (FP64 phase) to host;
+/* Copy the alpha/beta recurrence of the last aed_solve (FP64 phase; a mixed
+ * solve refined by Rayleigh-Ritz has none and gives its FP32 phase) to host;
  * *n receives its length (at most cap entries are written). */
 int aed_last_tmatrix(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n);
+/* The same for the FP32 phase of the last mixed solve of an AED_FP32 handle.
+ * Engine addition, no reference counterpart. */
+int aed_last_tmatrix_fp32(aed_handle* h, double* alpha, double* beta, int32_t cap, int32_t* n);
 
 /* Tmatrix::compute(true) on a host recurrence (src/ietl/tmatrix.h:121-228):
  * distinct non-ghost eigenvalues of T (alpha[0..n), beta[0..n-1) off-diagonal,
@@ -416,6 +424,12 @@ int aed_server_step(aed_server* s, int32_t* n_pending);
 int aed_server_poll(aed_server* s, int64_t ticket, aed_solve_result* out);
 int aed_server_cancel(aed_server* s, int64_t ticket);
 int aed_server_get_stats(aed_server* s, aed_server_stats* out);
+
+/* Copy v_j (D floats, device memory) of the FP32 Lanczos basis that the last
+ * mixed solve of an AED_FP32 handle stored, j < iterations_low + 1: for
+ * checking the basis (orthogonality, with and without opts.reorth).  Engine
+ * addition, no reference counterpart (ietl keeps no basis). */
+int aed_lanczos_vector(aed_handle* h, int32_t j, void* out);
 
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own
  * work or record timing events on it.  Engine addition, no reference counterpart. */

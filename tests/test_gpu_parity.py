@@ -403,6 +403,40 @@ def test_mixed_refinements_agree(name, p, nev):
     assert np.all(d >= -1e-12 * np.abs(r64["evals"])) and np.all(d <= rr["errors"] + 1e-12 * np.abs(r64["evals"]))
 
 
+def _basis_and_copies(ham, r):
+    """The stored FP32 Lanczos basis V (m x D) of the last mixed solve, max |V V^T - I|, and how many
+    eigenvalues of its T-matrix lie within 1e-5 relative of the lowest (1 + the ghost copies)."""
+    m = r["iterations_low"] + 1
+    V = np.array([ham.lanczos_vector(j) for j in range(m)])
+    orth = float(np.max(np.abs(V @ V.T - np.eye(m))))
+    a, b = ham.last_tmatrix(fp32_phase=True)
+    T = np.diag(a) + np.diag(b[:-1], 1) + np.diag(b[:-1], -1)
+    w = np.linalg.eigvalsh(T)
+    return orth, int(np.sum(np.abs(w - w[0]) <= 1e-5 * abs(w[0])))
+
+
+def test_full_reorthogonalisation_of_the_fp32_basis():
+    """Option reorth (FP32 handles): every FP32 Lanczos vector is reorthogonalised against the stored basis.
+    The basis stays orthonormal to FP32 rounding (|V V^T - I| <= 1e-5) where plain Lanczos loses it, the
+    T-matrix holds one copy of the ground state (plain Lanczos run as long makes ghost copies), and the
+    eigenvalues still agree with the FP64 solve to 1e-9."""
+    p = spin_params(LATTICE="square lattice", L=4, J=1)
+    r64 = ed.Hamiltonian.from_parameters(p).solve(nev=6, seed=3)
+    h32 = ed.Hamiltonian.from_parameters(p, precision=ed.FP32)
+    plain = h32.solve(nev=6, seed=3)
+    orth0, copies0 = _basis_and_copies(h32, plain)
+    ro = h32.solve(nev=6, seed=3, reorth=True)
+    orth1, copies1 = _basis_and_copies(h32, ro)
+    assert orth1 <= 1e-5, orth1
+    assert copies1 == 1, copies1
+    assert orth0 > 10 * orth1 and copies0 >= copies1, (orth0, copies0)
+    for r in (plain, ro):
+        assert r["converged"] and len(r["evals"]) == len(r64["evals"])
+        assert np.all(np.abs(r["evals"] - r64["evals"]) <= 1e-9 * np.abs(r64["evals"]))
+    with pytest.raises(ed.AEDError):
+        ed.Hamiltonian.from_parameters(p).solve(nev=1, reorth=True)  # FP64 handles store no basis
+
+
 @pytest.mark.parametrize("L,seed", [(22, 2), (24, 2), (24, 5)])
 def test_mixed_precision_near_degenerate_pair(L, seed):
     """J1-J2 chain near the Majumdar-Ghosh point (J2 = 0.49972474): the two lowest states are
