@@ -143,7 +143,8 @@ void release(aed_handle* h) {
   handle_release_workspace(h);
   for (void* p : {(void*)h->d_thi, (void*)h->d_tlo, (void*)h->d_lolist, (void*)h->d_looff, (void*)h->d_tile_h,
                   (void*)h->d_tile_r, (void*)h->d_blk_h, (void*)h->d_tfirst, (void*)h->d_dg, (void*)h->d_ell,
-                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_flag, (void*)h->d_start64,
+                  (void*)h->d_xtab, (void*)h->d_partA, (void*)h->d_partB, (void*)h->d_scal, (void*)h->d_flag, (void*)h->d_dgf,
+                  (void*)h->d_start64,
                   (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map, (void*)h->d_sthi,
                   (void*)h->d_stlo, (void*)h->d_slolist, (void*)h->d_slooff, (void*)h->d_sblk_hi,
                   (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r, (void*)h->d_sreps})
@@ -568,6 +569,11 @@ int aed_create(const aed_model_desc* model, int precision, int device, aed_handl
     return rc;
   }
   rc = launch_diag_table(h->P, t, h->d_dg, h->stream);
+  if (!rc && precision == AED_FP32) {  // the FP32 applies read the diagonal rounded to FP32
+    rc = mem_dev_alloc_n(&h->d_dgf, (size_t)h->tab.D);
+    if (!rc) rc = launch_round_to_f32(h->d_dg, h->d_dgf, h->tab.D, h->stream);
+    t.dgf = h->d_dgf;
+  }
   const cudaError_t e2 = rc ? cudaSuccess : cudaStreamSynchronize(h->stream);
   if (rc || e2 != cudaSuccess) {
     release(h);
@@ -1048,6 +1054,7 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   }
   if ((rc = upload_lo_table(h))) return rc;
   rc = launch_diag_table(h->P, h->dt, h->d_dg, h->stream);
+  if (!rc && h->d_dgf) rc = launch_round_to_f32(h->d_dg, h->d_dgf, h->tab.D, h->stream);
   if (rc) return rc;
   AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return AED_OK;

@@ -224,6 +224,14 @@ struct ApplyCtx {
   uint32_t lm;
 };
 
+// M(i,i) for an FP32 row: the FP32 copy of the diagonal when the handle keeps
+// one (single-instance FP32 handles: half the bytes of the FP64 table; the
+// FP32 phase tolerates the rounding, its FP64 refinement uses dg), else dg.
+// Every FP32 variant reads it the same way, so their rows stay identical.
+__device__ __forceinline__ double diag_fp32(const DevTables& t, uint32_t i) {
+  return t.dgf ? (double)__ldg(t.dgf + i) : __ldg(t.dg + i);
+}
+
 // Shared memory of one CTA running tiles.
 struct ApplySmem {
   SPair low[kMaxBonds];
@@ -450,7 +458,7 @@ __device__ __forceinline__ void apply_tile(const ApplyCtx& c, const DevTables& t
       for (int u = 0; u < R; ++u)
         if ((uint32_t)u < nrow) {
           const uint32_t i = base + rt + u * kHvThreads;
-          acc[u].add(__ldg(t.dg + i), __ldg(x + i));
+          acc[u].add(diag_fp32(t, i), __ldg(x + i));
         }
       run_hihi<T, Acc, R>(sm.prog, 0, nlow, nrow, rt, x, acc);
       run_cross<T, Acc, R>(sm.prog, nlow, nops, t.xtab + lbase + rt, 1u << c.Nlo, nrow, x, acc);

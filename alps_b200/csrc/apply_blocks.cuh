@@ -261,7 +261,7 @@ __device__ __forceinline__ void bundle_pass(const ApplyCtx& c, const DevTables& 
         const uint32_t r = rt + u * kHvThreads;
 #pragma unroll
         for (int j = 0; j < B; ++j)
-          if (j < nv) acc[j][u].add(__ldg(t.dg + q.bj[j] + r), q.xs[(size_t)j * q.maxrows + r]);
+          if (j < nv) acc[j][u].add(apply::diag_fp32(t, q.bj[j] + r), q.xs[(size_t)j * q.maxrows + r]);
       }
     }
 #pragma unroll

@@ -498,7 +498,7 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
 #pragma unroll
       for (int j = 0; j < U; ++j) {
         const uint32_t r = tid + j * kHvThreads;
-        if (r < nk) acc[j].add(__ldg(t.dg + base + r), ox[r]);
+        if (r < nk) acc[j].add(apply::diag_fp32(t, base + r), ox[r]);
       }
       if (!consume_ops<T, Acc, U>(pg, 0, pg.nops, q, nlo, cfg, sm, ring, acc)) return;
       for (int e = 0; e < t.ell_w; e += 2) {

@@ -35,6 +35,7 @@ struct aed_handle {
   double* d_partB = nullptr;  // per-chunk partial sums (red_chunks(D))
   double* d_scal = nullptr;   // 8 device scalars
   uint32_t* d_flag = nullptr;  // raised by a kernel whose bounded wait gave up
+  float* d_dgf = nullptr;      // FP32 handles: the diagonal rounded to FP32
   double* h_scal = nullptr;   // 8 pinned host scalars
   int hv_var[2] = {-1, -1};  // apply variant per precision (FP64, FP32), -1 = not tuned yet
   size_t elem_size() const { return precision == AED_FP32 ? 4 : 8; }

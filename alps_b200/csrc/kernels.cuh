@@ -32,6 +32,9 @@ struct DevTables {
   int maxrows = 0;  // rows of the largest hi block
   // raised by a kernel whose bounded wait gave up (read and cleared by the host)
   uint32_t* flag = nullptr;
+  // FP32 handles: M(i,i) rounded to FP32 (D floats), read by the FP32 applies
+  // in place of dg (half its bytes; the FP64 applies keep dg)
+  const float* dgf = nullptr;
 };
 
 constexpr int kHvThreads = 256;
