@@ -361,9 +361,13 @@ int handle_hv(aed_handle* h, bool f32, const void* x, void* y, double* alpha_par
   if (h->gen) return launch_spin_hv(*h->sp, h->sdev, (const double*)x, (double*)y, alpha_part, h->stream);
   if (h->mom)
     return launch_mom_hv(*h->mp, h->dt, h->mom_tables(), (const double*)x, (double*)y, alpha_part, h->stream);
-  const int rc = handle_tune(h, f32, x, y);
+  int rc = handle_tune(h, f32, x, y);
   if (rc) return rc;
-  return launch_checked(h, f32, h->hv_var[f32 ? 1 : 0], x, y, alpha_part);
+  rc = launch_variant(h, f32, h->hv_var[f32 ? 1 : 0], x, y, alpha_part);
+  // the tuned variant may not take these vectors (bulk copies need 16-byte
+  // aligned x and y): the tile apply takes any, with the same rows and partials
+  if (rc == kVariantNotApplicable) rc = launch_checked(h, f32, 0, x, y, alpha_part);
+  return rc;
 }
 
 int handle_check_flag(aed_handle* h) {
