@@ -721,7 +721,8 @@ def run_serve(args):
     scheduled arrival to the harvest of the result."""
     import alps_b200 as ed
 
-    reqs = serve_requests(args.requests)
+    # the seed-2000 stream; --rate rescales its arrival times (the same requests at another offered rate)
+    reqs = [(arr * 200.0 / args.rate,) + tuple(r) for arr, *r in serve_requests(args.requests)]
     prec = ed.FP32 if args.precision == "mixed" else ed.FP64
     srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1)  # pool mapped up front
     w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for _, n, b, nev, sd in reqs[:16]]
@@ -749,15 +750,16 @@ def run_serve(args):
     st = srv.stats()
     srv.close()
     lat = np.array(lat)
-    line = {"metric": "served Lanczos: solves/s and latency (Poisson 200 req/s)", "value": len(reqs) / wall,
+    line = {"metric": f"served Lanczos: solves/s and latency (Poisson {args.rate:g} req/s)", "value": len(reqs) / wall,
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64" if prec == ed.FP32 else "f64",
             "data": "synthetic",
-            "config": {"workload": f"{len(reqs)} requests, Poisson 200/s seed 2000, chain L 14..26 or ladder 2x7..2x12, "
+            "config": {"workload": f"{len(reqs)} requests, Poisson {args.rate:g}/s seed 2000, chain L 14..26 or "
+                                   "ladder 2x7..2x12, "
                                    "J_leg,J_rung~U[0.5,1.5], k~U{1..4}", "precision": args.precision,
                        "steps_per_graph": args.steps_per_launch},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "mean": float(lat.mean()), "max": float(lat.max())},
-            "offered_rate": 200.0, "graph_launches": st["graph_launches"], "wall_s": wall}
+            "offered_rate": args.rate, "graph_launches": st["graph_launches"], "wall_s": wall}
     print(json.dumps(line))
 
 
@@ -903,6 +905,7 @@ def main():
     ap.add_argument("--alpha", action="store_true", help="apply: with the Lanczos step's <x,y> partials")
     ap.add_argument("--k", type=int, default=0, help="apply mom_l28: momentum index")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: offered rate, requests/s (the stream's is 200)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="serve: engine precision")
     ap.add_argument("--steps-per-launch", type=int, default=8)
     args = ap.parse_args()
