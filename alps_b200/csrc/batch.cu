@@ -43,19 +43,15 @@ __device__ __forceinline__ float* low_vec(const BInst& I, int j) {
 __device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v64[j % 3]; }
 
 // The apply of every stepping instance over its (instance, bundle) items: the
-// bundle apply (apply_blocks.cuh, one hi block at a time) with the
-// instance's tables; the staged pairs and the shared-memory layout change
-// with the instance.  One kernel per phase and block size, so that each has
-// the registers of its own path: FP32 vectors with small hi blocks
-// (maxrows <= kSmallBlock: one block at a time, 1 row per thread, 6 CTAs per
-// SM -- 1.45x the solves/s of 2 rows per thread on the 512-chain batch of
-// L = 12..22) or larger ones (both blocks of an item at once, 2 rows per
-// thread, 4 CTAs per SM, as the single-instance blk2r2b4), and FP64 vectors (b_hv64:
-// 4 rows per thread, 3 CTAs per SM).
-constexpr int kSmallBlock = 512;
-
-template <int R, int MINB, int B, bool kSmall>
-__global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a) {
+// bundle apply (apply_blocks.cuh) with the instance's tables; the staged
+// pairs and the shared-memory layout change with the instance.  FP32 vectors:
+// one kernel per sector-size bucket (the rows of the largest hi block,
+// maxrows in (mr_lo, mr_hi]), each a template instance picked for its bucket
+// by the autotuner (batch_tune_bucket): R rows per thread, MINB CTAs per SM,
+// B = 1 (the item's hi blocks one at a time) or kBatchBundle (both at once).
+// FP64 vectors (b_hv64): 4 rows per thread, 3 CTAs per SM.
+template <int R, int MINB, int B>
+__global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a, int mr_lo, int mr_hi) {
   static_assert(B == 1 || B == kBatchBundle, "an item is one bundle or its blocks one by one");
   extern __shared__ __align__(16) unsigned char b_dyn[];
   __shared__ bapply::BundleSmem<B> sm;
@@ -65,7 +61,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a) {
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     const BItem w = a.tiles[it];
     const BInst& I = a.inst[w.inst];
-    if (I.phase != kPhLow || !stepping(I) || (I.t.maxrows <= kSmallBlock) != kSmall)
+    if (I.phase != kPhLow || !stepping(I) || I.t.maxrows <= mr_lo || I.t.maxrows > mr_hi)
       continue;  // same for every thread of the CTA
     const int j = I.j;
     if (w.inst != cur) {
@@ -369,9 +365,19 @@ int sms() {
   return g_sms;
 }
 
-int g_hv32s = 0, g_hv32s_smem = -1, g_hv32l = 0, g_hv32l_smem = -1, g_hv64 = 0, g_hv64_smem = -1;
-#define B_HV32_SMALL b_hv32<1, 6, 1, true>
-#define B_HV32_LARGE b_hv32<2, 4, kBatchBundle, false>
+// The FP32 apply candidates of the autotuner.  Every candidate adds each
+// row's terms in the same order (apply_blocks.cuh), so the choice changes the
+// speed, not the results.
+struct Cand32 {
+  void (*kern)(BatchArgs, int, int);
+  const char* name;
+};
+const Cand32 kCand32[kBatchCand32] = {
+    {b_hv32<1, 6, 1>, "r1b6"},          {b_hv32<2, 4, kBatchBundle>, "blk2r2b4"}, {b_hv32<2, 4, 1>, "r2b4"},
+    {b_hv32<1, 4, kBatchBundle>, "blk2r1b4"}, {b_hv32<4, 3, 1>, "r4b3"},
+};
+int g_c32[kBatchCand32] = {}, g_c32_smem[kBatchCand32] = {-1, -1, -1, -1, -1};
+int g_hv64 = 0, g_hv64_smem = -1;
 
 // Grid of an apply kernel for `smem` bytes of dynamic shared memory (cached per size).
 template <typename K>
@@ -404,27 +410,77 @@ size_t batch_hv_smem_limit() {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncAttributes f32s{}, f32l{}, f64{};
-  cudaFuncGetAttributes(&f32s, B_HV32_SMALL);
-  cudaFuncGetAttributes(&f32l, B_HV32_LARGE);
+  cudaFuncAttributes f64{};
   cudaFuncGetAttributes(&f64, b_hv64);
-  size_t st = f32s.sharedSizeBytes > f64.sharedSizeBytes ? f32s.sharedSizeBytes : f64.sharedSizeBytes;
-  if (f32l.sharedSizeBytes > st) st = f32l.sharedSizeBytes;
+  size_t st = f64.sharedSizeBytes;
+  for (const Cand32& c : kCand32) {
+    cudaFuncAttributes f{};
+    cudaFuncGetAttributes(&f, c.kern);
+    if (f.sharedSizeBytes > st) st = f.sharedSizeBytes;
+  }
   return optin > (int)st ? (size_t)optin - st : 0;
 }
 
 int batch_prepare(const BatchArgs& a) {
-  hv_grid(B_HV32_SMALL, a.hv_smem, &g_hv32s, &g_hv32s_smem);
-  hv_grid(B_HV32_LARGE, a.hv_smem, &g_hv32l, &g_hv32l_smem);
+  for (int c = 0; c < kBatchCand32; ++c) hv_grid(kCand32[c].kern, a.hv_smem, &g_c32[c], &g_c32_smem[c]);
   hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem);
   return check("batched apply attributes");
 }
 
-int batch_record_step(const BatchArgs& a, cudaStream_t st) {
+int batch_bucket_of(int maxrows) {
+  int b = 0;
+  while (b + 1 < kBatchBuckets && maxrows > kBatchBucketHi[b]) ++b;
+  return b;
+}
+
+const char* batch_cand32_name(int c) { return (c >= 0 && c < kBatchCand32) ? kCand32[c].name : "?"; }
+
+int batch_launch_hv32(const BatchArgs& a, int cand, int bucket, cudaStream_t st) {
+  if (cand < 0 || cand >= kBatchCand32 || bucket < 0 || bucket >= kBatchBuckets)
+    return fail(AED_ERR_INVALID, "batched apply: bad candidate or bucket");
+  const int lo = bucket == 0 ? -1 : kBatchBucketHi[bucket - 1];
+  const int hi = bucket + 1 == kBatchBuckets ? 0x7fffffff : kBatchBucketHi[bucket];
+  kCand32[cand].kern<<<hv_grid(kCand32[cand].kern, a.hv_smem, &g_c32[cand], &g_c32_smem[cand]), kHvThreads,
+                       a.hv_smem, st>>>(a, lo, hi);
+  return check("batched FP32 apply");
+}
+
+// Time every FP32 candidate on the resident work of `bucket` (one warm-up and
+// three timed launches each; the applies only rewrite y = H x of the current
+// step, which the next step computes again) and return the fastest.
+int batch_tune_bucket(const BatchArgs& a, int bucket, cudaStream_t st, int* best, float* best_ms) {
+  cudaEvent_t e0, e1;
+  AED_CUDA_TRY(cudaEventCreate(&e0));
+  AED_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = AED_OK;
+  *best = -1;
+  *best_ms = 0.f;
+  for (int c = 0; c < kBatchCand32 && !rc; ++c) {
+    rc = batch_launch_hv32(a, c, bucket, st);
+    if (!rc) AED_CUDA_TRY(cudaEventRecord(e0, st));
+    for (int r = 0; r < 3 && !rc; ++r) rc = batch_launch_hv32(a, c, bucket, st);
+    if (rc) break;
+    AED_CUDA_TRY(cudaEventRecord(e1, st));
+    AED_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (*best < 0 || ms < *best_ms) {
+      *best = c;
+      *best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+int batch_record_step(const BatchArgs& a, const int* choice32, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
-  B_HV32_SMALL<<<hv_grid(B_HV32_SMALL, a.hv_smem, &g_hv32s, &g_hv32s_smem), kHvThreads, a.hv_smem, st>>>(a);
-  B_HV32_LARGE<<<hv_grid(B_HV32_LARGE, a.hv_smem, &g_hv32l, &g_hv32l_smem), kHvThreads, a.hv_smem, st>>>(a);
+  for (int b = 0; b < kBatchBuckets; ++b) {
+    const int rc = batch_launch_hv32(a, choice32[b], b, st);
+    if (rc) return rc;
+  }
   b_hv64<<<hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem), kHvThreads, a.hv_smem, st>>>(a);
   b_alpha<<<ni, 256, 0, st>>>(a);
   b_update<<<gchunk, kRedThreads, 0, st>>>(a);

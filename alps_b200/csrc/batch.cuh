@@ -94,7 +94,19 @@ size_t batch_hv_smem_bytes(int maxrows, const HvParams& P);
 size_t batch_hv_smem_limit();
 // Set the apply kernels' shared-memory limits for a.hv_smem; call before capturing.
 int batch_prepare(const BatchArgs& a);
-int batch_record_step(const BatchArgs& a, cudaStream_t st);
+// The FP32 apply is tuned per sector-size bucket: bucket b holds the sectors
+// whose largest hi block has maxrows in (kBatchBucketHi[b-1], kBatchBucketHi[b]]
+// (the last bucket: everything above).  kBatchCand32 kernel candidates;
+// choice32[b] is bucket b's.  Untuned: kBatchDefault32[b].
+constexpr int kBatchBuckets = 4;
+constexpr int kBatchBucketHi[kBatchBuckets] = {300, 1000, 4000, 0x7fffffff};
+constexpr int kBatchCand32 = 5;
+constexpr int kBatchDefault32[kBatchBuckets] = {0, 1, 1, 1};
+int batch_bucket_of(int maxrows);
+const char* batch_cand32_name(int c);
+int batch_launch_hv32(const BatchArgs& a, int cand, int bucket, cudaStream_t st);
+int batch_tune_bucket(const BatchArgs& a, int bucket, cudaStream_t st, int* best, float* best_ms);
+int batch_record_step(const BatchArgs& a, const int* choice32, cudaStream_t st);
 int batch_record_check(const BatchArgs& a, cudaStream_t st);
 int batch_max_inst_grid();
 

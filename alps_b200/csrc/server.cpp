@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <map>
 #include <memory>
@@ -93,6 +95,10 @@ struct aed_server {
   bool graph_stale = true;
   int hv_smem = 0;  // dynamic shared memory of the apply in the graph
   int64_t launches = 0;
+  // the FP32 apply kernel of each sector-size bucket (batch.cuh), tuned on
+  // the first resident work of the bucket unless AED_BATCH_VARIANT forces one
+  int choice32[aed::kBatchBuckets] = {};
+  bool tuned32[aed::kBatchBuckets] = {};
 };
 
 namespace aed {
@@ -374,6 +380,33 @@ int rebuild_items(aed_server* s) {
   return AED_OK;
 }
 
+// Autotuner of the batched apply: every bucket that has instances in the
+// FP32 phase and no choice yet gets the fastest candidate on that work
+// (batch_tune_bucket; the choice is kept for the server's life); the graph is
+// captured again with it.
+int tune_buckets(aed_server* s) {
+  bool want[kBatchBuckets] = {};
+  for (const Slot& sl : s->slots)
+    if (sl.used && sl.inst.phase == kPhLow) want[batch_bucket_of(sl.inst.t.maxrows)] = true;
+  BatchArgs a{s->d_inst, s->d_counts, s->d_tiles, s->d_counts + 1, s->d_chunks, s->d_counts + 2, s->max_slots,
+              s->hv_smem};
+  for (int b = 0; b < kBatchBuckets; ++b) {
+    if (!want[b] || s->tuned32[b]) continue;
+    int rc = batch_prepare(a);
+    int best = -1;
+    float ms = 0.f;
+    if (!rc) rc = batch_tune_bucket(a, b, s->stream, &best, &ms);
+    if (rc) return rc;
+    s->choice32[b] = best;
+    s->tuned32[b] = true;
+    s->graph_stale = true;
+    if (std::getenv("AED_VERBOSE"))
+      std::fprintf(stderr, "[aed] batched FP32 apply, bucket %d: %s (%.3f ms for 3 launches)\n", b,
+                   batch_cand32_name(best), ms);
+  }
+  return AED_OK;
+}
+
 int capture_graph(aed_server* s) {
   if (s->graph) {
     cudaGraphExecDestroy(s->graph);
@@ -386,7 +419,7 @@ int capture_graph(aed_server* s) {
   if (rp) return rp;
   AED_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int rc = AED_OK;
-  for (int k = 0; k < s->S && !rc; ++k) rc = batch_record_step(a, s->stream);
+  for (int k = 0; k < s->S && !rc; ++k) rc = batch_record_step(a, s->choice32, s->stream);
   if (!rc) rc = batch_record_check(a, s->stream);
   const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
   if (rc) {
@@ -461,6 +494,15 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
     } else {
       cudaGetLastError();
     }
+  }
+  for (int b = 0; b < kBatchBuckets; ++b) s->choice32[b] = kBatchDefault32[b];
+  if (const char* env = std::getenv("AED_BATCH_VARIANT")) {  // one candidate for every bucket, no tuning
+    const int v = std::atoi(env);
+    if (v >= 0 && v < kBatchCand32)
+      for (int b = 0; b < kBatchBuckets; ++b) {
+        s->choice32[b] = v;
+        s->tuned32[b] = true;
+      }
   }
   s->slots.resize(s->max_slots);
   s->h_inst.resize(s->max_slots);
@@ -589,6 +631,7 @@ int aed_server_step(aed_server* s, int32_t* n_pending) {
     s->dirty = true;
   }
   if (s->dirty && (rc = rebuild_items(s))) return rc;
+  if ((rc = tune_buckets(s))) return rc;
   if (s->graph_stale && (rc = capture_graph(s))) return rc;
   int resident = 0;
   for (auto& sl : s->slots) resident += sl.used ? 1 : 0;

@@ -92,6 +92,27 @@ def test_batch_matches_oracle(prec, tol):
     srv.close()
 
 
+def test_batched_apply_candidates_give_the_same_results(monkeypatch):
+    """The autotuner of the batched engine picks one of several FP32 apply kernels per sector-size bucket
+    (rows per thread, CTAs per SM, hi blocks per pass); each adds every row's terms in the same order, so
+    forcing any one of them (AED_BATCH_VARIANT) gives the same eigenvalues bit for bit, and the tuned
+    server gives them too."""
+    reqs = mixed_requests(31, 10)
+    got = []
+    for cand in [None, 0, 1, 2, 3, 4]:
+        if cand is None:
+            monkeypatch.delenv("AED_BATCH_VARIANT", raising=False)
+        else:
+            monkeypatch.setenv("AED_BATCH_VARIANT", str(cand))
+        srv = ed.Server(precision=ed.FP32, max_slots=32, steps=4)
+        ts = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+        res = srv.run(ts)
+        got.append([res[t]["evals"].tolist() for t in ts])
+        srv.close()
+    for g in got[1:]:
+        assert g == got[0]
+
+
 @pytest.mark.parametrize("prec", [ed.FP32, ed.FP64])
 def test_result_is_the_same_alone_and_in_the_mix(prec):
     probe = (16, j1j2(16, 0.37), 2, 77)
