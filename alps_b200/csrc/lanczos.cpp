@@ -461,8 +461,14 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
 constexpr double kRefineEnergyTol = 1e-11;
 
 // Rayleigh-Ritz acceptance: every reported value's error bound below
-// kRRTol * |theta|, 10x inside the 1e-9 relative agreement.
-constexpr double kRRTol = 1e-10;
+// kRRTol * |theta|, 4x inside the 1e-9 relative agreement (the bound is
+// rigorous: the FP64 values lie within it).
+constexpr double kRRTol = 2.5e-10;
+
+// FP32 phase stop: Ritz residual estimates below kTol32 |lambda|.  The FP64
+// Rayleigh-Ritz error bound goes with the square of the residuals, so this
+// tolerance sets how often the refinement needs no FP64 Lanczos steps.
+constexpr double kTol32 = 1e-6;
 
 // Eigen-decomposition of a symmetric n x n matrix a (row-major, destroyed) by
 // cyclic Jacobi rotations (Jacobi 1846; the threshold-free cyclic form of
@@ -726,8 +732,7 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
     ro.cap = cap;
     R.reorth = &ro;
   }
-  const double tol32 = 2e-6;
-  StopRule stop1{nev, tol32, tol32 * 1e-3, false, 0.0, 2};
+  StopRule stop1{nev, kTol32, kTol32 * 1e-3, false, 0.0, 2};
   TmatInfo T1;
   int it1 = 0, failed1 = 0;
   rc = run_recurrence(R, stop1, slot, 0, &it1, &failed1, T1);
