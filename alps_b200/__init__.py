@@ -94,14 +94,14 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("max_slots", ctypes.c_int32), ("steps_per_launch", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("hbm_fraction", ctypes.c_double), ("hbm_budget_bytes", ctypes.c_int64),
-        ("reserve_bytes", ctypes.c_int64),
+        ("reserve_bytes", ctypes.c_int64), ("max_lanes", ctypes.c_int32), ("lane_min_dim", ctypes.c_int64),
     ]
 
 
 class ServerStats(ctypes.Structure):
     _fields_ = [
         ("resident", ctypes.c_int32), ("queued", ctypes.c_int32), ("bytes_used", ctypes.c_int64),
-        ("bytes_budget", ctypes.c_int64), ("graph_launches", ctypes.c_int64),
+        ("bytes_budget", ctypes.c_int64), ("graph_launches", ctypes.c_int64), ("lanes", ctypes.c_int32),
     ]
 
 
@@ -730,9 +730,11 @@ class Server:
     graph launch; new requests join at the next step."""
 
     def __init__(self, precision=FP32, device=0, max_slots=512, steps=8, hbm_fraction=0.0, hbm_budget=0,
-                 reserve=0):
-        """reserve: bytes of device memory to map into the server's pool up front (-1: the whole budget)."""
-        o = ServerOpts(device, max_slots, steps, precision, hbm_fraction, hbm_budget, reserve)
+                 reserve=0, max_lanes=0, lane_min_dim=0):
+        """reserve: bytes of device memory to map into the server's pool up front (-1: the whole budget).
+        Requests of dimension >= lane_min_dim (0: 2^21; -1: none) run as single-instance solves beside the
+        batch, max_lanes (0: 2) at once."""
+        o = ServerOpts(device, max_slots, steps, precision, hbm_fraction, hbm_budget, reserve, max_lanes, lane_min_dim)
         h = _P()
         self._h = None
         _check(lib().aed_server_create(ctypes.byref(o), ctypes.byref(h)))
@@ -786,7 +788,7 @@ class Server:
         st = ServerStats()
         _check(lib().aed_server_get_stats(self._h, ctypes.byref(st)))
         return {"resident": st.resident, "queued": st.queued, "bytes_used": st.bytes_used,
-                "bytes_budget": st.bytes_budget, "graph_launches": st.graph_launches}
+                "bytes_budget": st.bytes_budget, "graph_launches": st.graph_launches, "lanes": st.lanes}
 
     def run(self, tickets, max_steps=100000):
         """Step until every ticket finished; returns {ticket: result}."""

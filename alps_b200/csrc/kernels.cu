@@ -12,6 +12,8 @@
 
 #include <atomic>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "apply.cuh"
@@ -228,17 +230,16 @@ __global__ void __launch_bounds__(256) ritz_combine_kernel(const float* __restri
   }
 }
 
-int g_num_sms = 0;
 std::atomic<int64_t> g_launches{0};
 
 int num_sms() {
-  if (!g_num_sms) {
-    int dev = 0;
+  static const int n = [] {  // thread-safe one-time initialisation
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
+  return n;
 }
 
 inline int elem_grid(int64_t n) {
@@ -282,58 +283,83 @@ constexpr HvVariant kVariants[] = {
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
-template <typename T, typename Acc, int R, int B>
-int launch_one(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st,
-               int* grid_cache) {
-  if (*grid_cache <= 0) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<T, Acc, R, B>, kHvThreads, 0);
-    *grid_cache = num_sms() * (per_sm < 1 ? 1 : per_sm);
+// Launch shapes are computed once per kernel (and per shared-memory size or
+// sector shape) and kept in maps guarded by g_grid_mu: handles on several host
+// threads launch the same kernels.  The dynamic shared-memory limit of a
+// kernel is raised once, to the most the device allows, so that a launch on
+// one thread never sees another thread's smaller limit.
+std::mutex g_grid_mu;
+
+template <typename K>
+int raise_smem_limit(K kern, size_t* static_bytes) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    return fail(AED_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(e));
   }
-  int grid = *grid_cache;
+  const int most = optin - (int)fa.sharedSizeBytes;
+  if (most > 0 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most) != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    return fail(AED_ERR_CUDA, std::string("kernel shared memory limit: ") + cudaGetErrorString(e));
+  }
+  *static_bytes = fa.sharedSizeBytes;
+  return most > 0 ? AED_OK : kVariantNotApplicable;
+}
+
+template <typename T, typename Acc, int R, int B>
+int launch_one(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st) {
+  static int grid_all = 0;
+  int grid;
+  {
+    std::lock_guard<std::mutex> lk(g_grid_mu);
+    if (grid_all <= 0) {
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hv_kernel<T, Acc, R, B>, kHvThreads, 0);
+      grid_all = num_sms() * (per_sm < 1 ? 1 : per_sm);
+    }
+    grid = grid_all;
+  }
   if (grid > t.n_tiles) grid = (int)t.n_tiles;
   hv_kernel<T, Acc, R, B><<<grid, kHvThreads, 0, st>>>(P, t, x, y, alpha_part);
   return check_launch("hv_kernel");
 }
 
-// Occupancy of a bundle kernel for `dyn` bytes of dynamic shared memory,
-// cached per kernel and size (sectors of one process share a few sizes).
-struct BundleGrid {
-  size_t dyn = 0;
-  int grid = 0;
-};
-
+// Bundle apply: grid from the occupancy at this sector's dynamic shared
+// memory (sectors of one process share a few sizes).
 template <typename T, typename Acc, int R, int B, int MINB>
-int launch_bundle(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st,
-                  BundleGrid* cache) {
+int launch_bundle(const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part, cudaStream_t st) {
   if (!t.blk_h || t.maxrows <= 0) return kVariantNotApplicable;
   const size_t dyn = bapply::bundle_smem_bytes<T>(B, t.maxrows, P.n_pairs, P.n_lolo);
   auto kern = hvb_kernel<T, Acc, R, B, MINB>;
-  if (cache->dyn != dyn || cache->grid <= 0) {
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
-      const cudaError_t e = cudaGetLastError();
-      return fail(AED_ERR_CUDA, std::string("hvb_kernel attributes: ") + cudaGetErrorString(e));
+  static int limit_rc = -1;
+  static size_t static_bytes = 0;
+  static std::map<size_t, int> grids;  // dyn -> grid (0: does not fit)
+  int grid = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_grid_mu);
+    if (limit_rc < 0) limit_rc = raise_smem_limit(kern, &static_bytes);
+    if (limit_rc == AED_ERR_CUDA) return limit_rc;
+    auto it = grids.find(dyn);
+    if (it == grids.end()) {
+      int per_sm = 0;
+      int dev = 0, optin = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      if (limit_rc == AED_OK && static_bytes + dyn <= (size_t)optin)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHvThreads, dyn);
+      it = grids.emplace(dyn, per_sm < 1 ? 0 : num_sms() * per_sm).first;
     }
-    if (fa.sharedSizeBytes + dyn > (size_t)optin) return kVariantNotApplicable;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
-      const cudaError_t e = cudaGetLastError();
-      return fail(AED_ERR_CUDA, std::string("hvb_kernel shared memory: ") + cudaGetErrorString(e));
-    }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHvThreads, dyn);
-    if (per_sm < 1) return kVariantNotApplicable;
-    cache->dyn = dyn;
-    cache->grid = num_sms() * per_sm;
+    grid = it->second;
   }
-  int64_t grid = cache->grid;
+  if (grid <= 0) return kVariantNotApplicable;
+  int64_t g = grid;
   const int64_t nb = t.n_blk / B;
-  if (grid > nb) grid = nb;
-  if (grid < 1) return AED_OK;
-  kern<<<(unsigned)grid, kHvThreads, dyn, st>>>(P, t, x, y, alpha_part);
+  if (g > nb) g = nb;
+  if (g < 1) return AED_OK;
+  kern<<<(unsigned)g, kHvThreads, dyn, st>>>(P, t, x, y, alpha_part);
   return check_launch("hvb_kernel");
 }
 
@@ -342,85 +368,83 @@ int launch_bundle(const HvParams& P, const DevTables& t, const T* x, T* y, doubl
 // sectors whose blocks need more than U rows per thread, to lo parts under
 // 8 bits (the crossing-table rows must be 16-byte multiples), or to vectors
 // that are not 16-byte aligned (bulk copies).
-struct StreamGrid {
-  int maxrows = -1;
-  int grid = 0;
+struct StreamShape {
   sapply::StreamCfg cfg{};
   size_t dyn = 0;
+  bool fits = false;
 };
 
 template <typename T, typename Acc, int U>
 int launch_stream(int OB, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
-                  cudaStream_t st, StreamGrid* cache) {
+                  cudaStream_t st) {
   if (!t.blk_h || !t.flag || t.maxrows <= 0 || t.Nlo < 8 || t.Nlo > 16) return kVariantNotApplicable;
   if ((t.maxrows + kHvThreads - 1) / kHvThreads > U) return kVariantNotApplicable;
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(t.xtab)) & 15u)
     return kVariantNotApplicable;
   auto kern = hvs_kernel<T, Acc, U>;
-  if (cache->maxrows != t.maxrows) {
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
-      const cudaError_t e = cudaGetLastError();
-      return fail(AED_ERR_CUDA, std::string("hvs_kernel attributes: ") + cudaGetErrorString(e));
+  static int limit_rc = -1;
+  static size_t static_bytes = 0;
+  static std::map<std::pair<int, int>, StreamShape> shapes;  // (maxrows, OB) -> shape
+  StreamShape sh;
+  {
+    std::lock_guard<std::mutex> lk(g_grid_mu);
+    if (limit_rc < 0) limit_rc = raise_smem_limit(kern, &static_bytes);
+    if (limit_rc == AED_ERR_CUDA) return limit_rc;
+    const auto key = std::make_pair(t.maxrows, OB);
+    auto it = shapes.find(key);
+    if (it == shapes.end()) {
+      StreamShape n;
+      int dev = 0, optin = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      n.cfg.own_bytes = (uint32_t)bapply::bundle_align16((size_t)t.maxrows * sizeof(T) + 32);
+      n.cfg.xoff = n.cfg.own_bytes;
+      n.cfg.stage_bytes = n.cfg.xoff + (uint32_t)bapply::bundle_align16((size_t)t.maxrows * 2 + 32);
+      const int64_t avail = (int64_t)optin - (int64_t)static_bytes - 1024;
+      const int64_t S = (avail - (int64_t)OB * n.cfg.own_bytes) / (int64_t)n.cfg.stage_bytes;
+      if (limit_rc == AED_OK && S >= 2) {
+        n.cfg.S = (int)(S < sapply::kMaxStages ? S : sapply::kMaxStages);
+        n.cfg.OB = OB;
+        n.dyn = (size_t)OB * n.cfg.own_bytes + (size_t)n.cfg.S * n.cfg.stage_bytes;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sapply::kThreads, n.dyn);
+        n.fits = per_sm >= 1;
+      }
+      it = shapes.emplace(key, n).first;
     }
-    sapply::StreamCfg cfg{};
-    cfg.own_bytes = (uint32_t)bapply::bundle_align16((size_t)t.maxrows * sizeof(T) + 32);
-    cfg.xoff = cfg.own_bytes;
-    cfg.stage_bytes = cfg.xoff + (uint32_t)bapply::bundle_align16((size_t)t.maxrows * 2 + 32);
-    const int64_t avail = (int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024;
-    const int64_t S = (avail - (int64_t)OB * cfg.own_bytes) / (int64_t)cfg.stage_bytes;
-    if (S < 2) return kVariantNotApplicable;
-    cfg.S = (int)(S < sapply::kMaxStages ? S : sapply::kMaxStages);
-    cfg.OB = OB;
-    const size_t dyn = (size_t)OB * cfg.own_bytes + (size_t)cfg.S * cfg.stage_bytes;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess) {
-      const cudaError_t e = cudaGetLastError();
-      return fail(AED_ERR_CUDA, std::string("hvs_kernel shared memory: ") + cudaGetErrorString(e));
-    }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sapply::kThreads, dyn);
-    if (per_sm < 1) return kVariantNotApplicable;
-    cache->cfg = cfg;
-    cache->dyn = dyn;
-    cache->grid = num_sms();
-    cache->maxrows = t.maxrows;
+    sh = it->second;
   }
-  sapply::StreamCfg cfg = cache->cfg;
+  if (!sh.fits) return kVariantNotApplicable;
+  sapply::StreamCfg cfg = sh.cfg;
   cfg.flag = t.flag;
-  int64_t grid = cache->grid;
+  int64_t grid = num_sms();
   if (grid > t.n_blk) grid = t.n_blk;
   if (grid < 1) return AED_OK;
-  kern<<<(unsigned)grid, sapply::kThreads, cache->dyn, st>>>(P, t, x, y, alpha_part, cfg);
+  kern<<<(unsigned)grid, sapply::kThreads, sh.dyn, st>>>(P, t, x, y, alpha_part, cfg);
   return check_launch("hvs_kernel");
 }
 
 template <typename T, typename Acc>
 int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
                 cudaStream_t st) {
-  static int grids[kNumVariants] = {};
-  static BundleGrid bgrid[kNumVariants];
-  static StreamGrid sgrid[kNumVariants];
   if (t.n_tiles == 0) return AED_OK;
   switch (v) {
-    case 0: return launch_one<T, Acc, 4, 6>(P, t, x, y, alpha_part, st, &grids[0]);
-    case 1: return launch_one<T, Acc, 4, 5>(P, t, x, y, alpha_part, st, &grids[1]);
-    case 2: return launch_one<T, Acc, 4, 4>(P, t, x, y, alpha_part, st, &grids[2]);
-    case 3: return launch_one<T, Acc, 2, 8>(P, t, x, y, alpha_part, st, &grids[3]);
-    case 4: return launch_one<T, Acc, 2, 6>(P, t, x, y, alpha_part, st, &grids[4]);
-    case 5: return launch_one<T, Acc, 8, 3>(P, t, x, y, alpha_part, st, &grids[5]);
-    case 6: return launch_bundle<T, Acc, 4, 1, 3>(P, t, x, y, alpha_part, st, &bgrid[6]);
-    case 7: return launch_bundle<T, Acc, 2, 2, 4>(P, t, x, y, alpha_part, st, &bgrid[7]);
-    case 8: return launch_bundle<T, Acc, 4, 2, 2>(P, t, x, y, alpha_part, st, &bgrid[8]);
-    case 9: return launch_bundle<T, Acc, 2, 2, 3>(P, t, x, y, alpha_part, st, &bgrid[9]);
-    case 10: return launch_bundle<T, Acc, 4, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[10]);
-    case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st, &bgrid[11]);
-    case 12: return launch_stream<T, Acc, 14>(2, P, t, x, y, alpha_part, st, &sgrid[12]);
-    case 13: return launch_stream<T, Acc, 14>(1, P, t, x, y, alpha_part, st, &sgrid[13]);
-    case 14: return launch_stream<T, Acc, 26>(2, P, t, x, y, alpha_part, st, &sgrid[14]);
-    case 15: return launch_stream<T, Acc, 26>(1, P, t, x, y, alpha_part, st, &sgrid[15]);
+    case 0: return launch_one<T, Acc, 4, 6>(P, t, x, y, alpha_part, st);
+    case 1: return launch_one<T, Acc, 4, 5>(P, t, x, y, alpha_part, st);
+    case 2: return launch_one<T, Acc, 4, 4>(P, t, x, y, alpha_part, st);
+    case 3: return launch_one<T, Acc, 2, 8>(P, t, x, y, alpha_part, st);
+    case 4: return launch_one<T, Acc, 2, 6>(P, t, x, y, alpha_part, st);
+    case 5: return launch_one<T, Acc, 8, 3>(P, t, x, y, alpha_part, st);
+    case 6: return launch_bundle<T, Acc, 4, 1, 3>(P, t, x, y, alpha_part, st);
+    case 7: return launch_bundle<T, Acc, 2, 2, 4>(P, t, x, y, alpha_part, st);
+    case 8: return launch_bundle<T, Acc, 4, 2, 2>(P, t, x, y, alpha_part, st);
+    case 9: return launch_bundle<T, Acc, 2, 2, 3>(P, t, x, y, alpha_part, st);
+    case 10: return launch_bundle<T, Acc, 4, 1, 4>(P, t, x, y, alpha_part, st);
+    case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st);
+    case 12: return launch_stream<T, Acc, 14>(2, P, t, x, y, alpha_part, st);
+    case 13: return launch_stream<T, Acc, 14>(1, P, t, x, y, alpha_part, st);
+    case 14: return launch_stream<T, Acc, 26>(2, P, t, x, y, alpha_part, st);
+    case 15: return launch_stream<T, Acc, 26>(1, P, t, x, y, alpha_part, st);
     default: return fail(AED_ERR_INVALID, "unknown apply variant");
   }
 }

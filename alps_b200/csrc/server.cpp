@@ -13,6 +13,7 @@
 // stream and returned with cudaFreeAsync.
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "batch.cuh"
@@ -46,6 +48,7 @@ struct Sector {
 
 struct Request {
   int64_t ticket = 0;
+  int64_t dim = 0;  // sector dimension
   Model model;
   aed_solve_opts opts{};
   clk::time_point t_submit;
@@ -63,6 +66,15 @@ struct Slot {
   std::vector<void*> allocs;  // freed at retirement
   size_t bytes = 0;
   BInst inst{};
+};
+
+// A request solved on its own handle (single-instance engine: the tuned apply
+// variants, the Rayleigh-Ritz refinement) by a host thread, beside the batch.
+struct Lane {
+  std::shared_ptr<Request> req;
+  std::thread th;
+  std::atomic<bool> done{false};
+  size_t bytes = 0;
 };
 
 }  // namespace
@@ -99,6 +111,10 @@ struct aed_server {
   // the first resident work of the bucket unless AED_BATCH_VARIANT forces one
   int choice32[aed::kBatchBuckets] = {};
   bool tuned32[aed::kBatchBuckets] = {};
+  // single-instance lanes for the large sectors
+  int max_lanes = 2;
+  int64_t lane_min_dim = (int64_t)1 << 21;
+  std::vector<std::unique_ptr<aed::Lane>> lanes;
 };
 
 namespace aed {
@@ -407,6 +423,57 @@ int tune_buckets(aed_server* s) {
   return AED_OK;
 }
 
+// Device bytes of a single-instance solve of dimension D with FP32 store
+// capacity n_store: the handle's per-row tables and vectors (diagonal in FP64
+// and FP32, five recurrence vectors, the refinement's start and Rayleigh-Ritz
+// vectors) and the FP32 basis.
+size_t lane_bytes(const aed_server* s, int64_t D, int n_store) {
+  const size_t per_row = 8 + 4 + 5 * 8 + 8 + 2 * kMaxRR * 8 + (s->precision == AED_FP32 ? 4 * (size_t)n_store : 0);
+  return (size_t)D * per_row + ((size_t)64 << 20);
+}
+
+void lane_main(aed_server* s, Lane* L) {
+  cudaSetDevice(s->device);
+  Request& r = *L->req;
+  const Model& m = r.model;
+  std::vector<int32_t> s1(m.s1.begin(), m.s1.end()), s2(m.s2.begin(), m.s2.end());
+  const aed_model_desc md{m.N,          m.n_up,      (int32_t)s1.size(),
+                          s1.data(),    s2.data(),   m.jz.data(),
+                          m.jxy.data(), m.kq.data(), m.site_h.empty() ? nullptr : m.site_h.data(),
+                          m.site_d.empty() ? nullptr : m.site_d.data()};
+  aed_handle* h = nullptr;
+  aed_solve_result res{};
+  int rc = aed_create(&md, s->precision, s->device, &h);
+  if (!rc) {
+    aed_solve_opts o = r.opts;
+    rc = aed_solve(h, &o, &res);
+  }
+  if (h) aed_destroy(h);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!r.cancelled) {
+      r.res = res;
+      r.res.seconds = std::chrono::duration<double>(clk::now() - r.t_submit).count();
+      r.status = rc ? rc : AED_OK;
+    }
+    s->used -= std::min(s->used, L->bytes);
+  }
+  L->done = true;
+}
+
+// Join the lanes whose solve has finished (they set `done` after their last
+// use of the server's lock).
+void reap_lanes(aed_server* s) {
+  for (size_t i = 0; i < s->lanes.size();) {
+    if (s->lanes[i]->done) {
+      s->lanes[i]->th.join();
+      s->lanes.erase(s->lanes.begin() + (long)i);
+    } else {
+      ++i;
+    }
+  }
+}
+
 int capture_graph(aed_server* s) {
   if (s->graph) {
     cudaGraphExecDestroy(s->graph);
@@ -495,6 +562,9 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
       cudaGetLastError();
     }
   }
+  if (o->max_lanes > 0) s->max_lanes = o->max_lanes;
+  if (o->lane_min_dim > 0) s->lane_min_dim = o->lane_min_dim;
+  if (o->lane_min_dim < 0) s->max_lanes = 0;
   for (int b = 0; b < kBatchBuckets; ++b) s->choice32[b] = kBatchDefault32[b];
   if (const char* env = std::getenv("AED_BATCH_VARIANT")) {  // one candidate for every bucket, no tuning
     const int v = std::atoi(env);
@@ -531,6 +601,8 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
 int aed_server_destroy(aed_server* s) {
   if (!s) return AED_OK;
   DeviceGuard g(s->device);
+  for (auto& L : s->lanes) L->th.join();  // a lane's solve cannot be interrupted: wait for it
+  s->lanes.clear();
   cudaStreamSynchronize(s->stream);
   for (int k = 0; k < (int)s->slots.size(); ++k)
     if (s->slots[k].used) release_slot(s, k);
@@ -565,6 +637,7 @@ int aed_server_submit(aed_server* s, const aed_model_desc* model, const aed_solv
   if (t.D < 2) return fail(AED_ERR_INVALID, "the server solves sectors of dimension >= 2 (use aed_solve)");
   r->opts = *opts;
   r->opts.start = nullptr;  // the server draws its own start vectors
+  r->dim = t.D;
   const int cap = cap_of(*r, t.D);
   const int n_store = s->precision == AED_FP32 ? std::min(kServerStore, cap + 1) : 0;
   r->footprint = request_bytes(s, r->model.N, t.D, opts->nev, cap, n_store);
@@ -595,7 +668,7 @@ int aed_server_cancel(aed_server* s, int64_t ticket) {
 int aed_server_step(aed_server* s, int32_t* n_pending) {
   if (!s) return fail(AED_ERR_INVALID, "NULL argument");
   DeviceGuard g(s->device);
-  std::lock_guard<std::mutex> lk(s->mu);
+  std::unique_lock<std::mutex> lk(s->mu);
   int rc;
   // drop cancelled requests that are still resident
   for (int k = 0; k < (int)s->slots.size(); ++k)
@@ -603,11 +676,42 @@ int aed_server_step(aed_server* s, int32_t* n_pending) {
       release_slot(s, k);
       s->dirty = true;
     }
-  // admit in arrival order while the budget and the slots allow
-  while (!s->queue.empty()) {
-    auto r = s->queue.front();
+  reap_lanes(s);
+  const bool use_lanes = s->max_lanes > 0 && s->lane_min_dim > 0;
+  // large sectors: single-instance lanes, in arrival order while lanes and budget allow
+  if (use_lanes) {
+    for (auto it = s->queue.begin(); it != s->queue.end() && (int)s->lanes.size() < s->max_lanes;) {
+      auto r = *it;
+      if (r->cancelled) {
+        it = s->queue.erase(it);
+        continue;
+      }
+      if (r->dim < s->lane_min_dim) {
+        ++it;
+        continue;
+      }
+      const size_t need = lane_bytes(s, r->dim, std::min(kServerStore, cap_of(*r, r->dim) + 1));
+      if (s->used + need > s->budget) break;
+      std::unique_ptr<Lane> L(new Lane);
+      L->req = r;
+      L->bytes = need;
+      s->used += need;
+      Lane* lp = L.get();
+      L->th = std::thread(lane_main, s, lp);
+      s->lanes.push_back(std::move(L));
+      it = s->queue.erase(it);
+    }
+  }
+  // the rest: admitted to the batch in arrival order while the budget and the
+  // slots allow (large requests waiting for a lane are passed over)
+  for (auto qit = s->queue.begin(); qit != s->queue.end();) {
+    auto r = *qit;
     if (r->cancelled) {
-      s->queue.pop_front();
+      qit = s->queue.erase(qit);
+      continue;
+    }
+    if (use_lanes && r->dim >= s->lane_min_dim) {
+      ++qit;
       continue;
     }
     const auto key = std::make_pair(r->model.N, r->model.n_up);
@@ -620,7 +724,7 @@ int aed_server_step(aed_server* s, int32_t* n_pending) {
         break;
       }
     if (k < 0) break;
-    s->queue.pop_front();
+    qit = s->queue.erase(qit);
     rc = admit(s, k, r);
     if (rc) {
       r->status = rc;
@@ -652,7 +756,12 @@ int aed_server_step(aed_server* s, int32_t* n_pending) {
       }
     }
   }
-  if (n_pending) *n_pending = resident + (int32_t)s->queue.size();
+  if (resident == 0 && !s->lanes.empty()) {  // only lanes at work: do not spin the caller
+    lk.unlock();
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
+    lk.lock();
+  }
+  if (n_pending) *n_pending = resident + (int32_t)s->queue.size() + (int32_t)s->lanes.size();
   return AED_OK;
 }
 
@@ -678,6 +787,7 @@ int aed_server_get_stats(aed_server* s, aed_server_stats* out) {
   out->bytes_used = (int64_t)s->used;
   out->bytes_budget = (int64_t)s->budget;
   out->graph_launches = s->launches;
+  out->lanes = (int32_t)s->lanes.size();
   return AED_OK;
 }
 

@@ -402,12 +402,18 @@ typedef struct {
   int64_t reserve_bytes;     /* device memory mapped into the server's pool at creation
                                 (-1: the whole budget; 0: none), so that requests do not
                                 pay for mapping fresh memory on first use               */
+  int32_t max_lanes;         /* requests of dimension >= lane_min_dim run as single-instance
+                                solves (their own handle, stream and host thread, the
+                                fastest apply variants) beside the batch, at most this
+                                many at once (default 2)                                  */
+  int64_t lane_min_dim;      /* 0: default 2^21; -1: no lanes (every request batched)    */
 } aed_server_opts;
 
 typedef struct {
   int32_t resident, queued;
   int64_t bytes_used, bytes_budget;
   int64_t graph_launches;
+  int32_t lanes;             /* single-instance solves running                           */
 } aed_server_stats;
 
 int aed_server_create(const aed_server_opts* opts, aed_server** out);

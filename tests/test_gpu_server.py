@@ -1,6 +1,8 @@
 """The batched / served engine (aed_server_*): parity with single solves, batch
 independence, admission by HBM footprint, continuous batching (needs a B200)."""
 
+from math import comb
+
 import numpy as np
 import pytest
 
@@ -111,6 +113,42 @@ def test_batched_apply_candidates_give_the_same_results(monkeypatch):
         srv.close()
     for g in got[1:]:
         assert g == got[0]
+
+
+@pytest.mark.parametrize("prec,tol", [(ed.FP32, 1e-9), (ed.FP64, 1e-11)])
+def test_large_requests_run_in_single_instance_lanes(prec, tol):
+    """Requests at or above lane_min_dim run as single-instance solves on their own handle, beside the
+    batch: the mix finishes, lanes were in use, every result agrees with the single-instance solve of the
+    same request (to the tolerance of the batched test), and a lane result is the same alone and in the mix."""
+    reqs = mixed_requests(777, 14)
+    srv = ed.Server(precision=prec, max_slots=32, steps=4, max_lanes=2, lane_min_dim=10000)
+    ts = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+    seen_lanes = 0
+    out = {}
+    for _ in range(100000):
+        if len(out) == len(ts):
+            break
+        srv.step()
+        seen_lanes = max(seen_lanes, srv.stats()["lanes"])
+        for t in ts:
+            if t not in out:
+                r = srv.poll(t)
+                if r is not None:
+                    out[t] = r
+    assert len(out) == len(ts) and seen_lanes >= 1
+    for t, (n, b, nev, sd) in zip(ts, reqs):
+        ref = reference(n, b, nev)
+        assert out[t]["converged"] and len(out[t]["evals"]) == len(ref)
+        assert np.all(np.abs(out[t]["evals"] - ref) <= tol * np.abs(ref)), (n, out[t]["evals"], ref)
+    big = [(t, q) for t, q in zip(ts, reqs) if comb(q[0], q[0] // 2) >= 10000]
+    assert big
+    t0, (n, b, nev, sd) = big[0]
+    alone = ed.Server(precision=prec, max_slots=4, steps=4, max_lanes=1, lane_min_dim=10000)
+    ta = alone.submit(n, n // 2, b, nev=nev, seed=sd)
+    ra = alone.run([ta])[ta]
+    alone.close()
+    assert np.array_equal(ra["evals"], out[t0]["evals"])
+    srv.close()
 
 
 @pytest.mark.parametrize("prec", [ed.FP32, ed.FP64])
