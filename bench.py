@@ -724,7 +724,8 @@ def run_serve(args):
     # the seed-2000 stream; --rate rescales its arrival times (the same requests at another offered rate)
     reqs = [(arr * 200.0 / args.rate,) + tuple(r) for arr, *r in serve_requests(args.requests)]
     prec = ed.FP32 if args.precision == "mixed" else ed.FP64
-    srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1)  # pool mapped up front
+    srv = ed.Server(precision=prec, max_slots=512, steps=args.steps_per_launch, reserve=-1,  # pool mapped up front
+                    max_lanes=args.lanes, lane_min_dim=args.lane_min_dim if args.lanes > 0 else -1)
     w = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for _, n, b, nev, sd in reqs[:16]]
     srv.run(w)
     pending = {}
@@ -756,7 +757,8 @@ def run_serve(args):
             "config": {"workload": f"{len(reqs)} requests, Poisson {args.rate:g}/s seed 2000, chain L 14..26 or "
                                    "ladder 2x7..2x12, "
                                    "J_leg,J_rung~U[0.5,1.5], k~U{1..4}", "precision": args.precision,
-                       "steps_per_graph": args.steps_per_launch},
+                       "steps_per_graph": args.steps_per_launch,
+                       "lanes": {"max": args.lanes, "min_dim": args.lane_min_dim if args.lanes > 0 else None}},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "mean": float(lat.mean()), "max": float(lat.max())},
             "offered_rate": args.rate, "graph_launches": st["graph_launches"], "wall_s": wall}
@@ -906,6 +908,8 @@ def main():
     ap.add_argument("--k", type=int, default=0, help="apply mom_l28: momentum index")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered rate, requests/s (the stream's is 200)")
+    ap.add_argument("--lanes", type=int, default=2, help="serve: single-instance lanes for large requests (0: none)")
+    ap.add_argument("--lane-min-dim", type=int, default=1 << 21, help="serve: smallest dimension sent to a lane")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="serve: engine precision")
     ap.add_argument("--steps-per-launch", type=int, default=8)
     args = ap.parse_args()
