@@ -78,6 +78,8 @@ struct AccExact64 {  // FP64 vectors, the reference's rounding
 struct AccWide32 {  // FP32 vectors, FP64 accumulator
   double a = 0.0;
   __device__ __forceinline__ void add(double c, float xv) { a = fma(c, (double)xv, a); }
+  // an FP32 value already widened (exactly) to FP64: the same arithmetic
+  __device__ __forceinline__ void add(double c, double xv) { a = fma(c, xv, a); }
   __device__ __forceinline__ float value() const { return (float)a; }
 };
 
@@ -93,6 +95,7 @@ struct AccTwoSum32 {  // FP32 vectors, TwoSum + exact product error in FP32
     s = t;
     e = __fadd_rn(e, __fadd_rn(se, __fmaf_rn(cl, xv, pe)));
   }
+  __device__ __forceinline__ void add(double c, double xv) { add(c, (float)xv); }  // xv holds an FP32 value
   __device__ __forceinline__ float value() const { return __fadd_rn(s, e); }
 };
 

@@ -80,6 +80,8 @@ struct StreamCfg {
   int S;                 // ring stages
   int OB;                // own-x buffers (1 or 2)
   uint32_t own_bytes;    // bytes per own-x buffer (16-byte multiple)
+  uint32_t ownd_off;     // FP32 rows widened once: the block's own x in FP64 at this offset
+  uint32_t ring_off;     // offset of the ring
   uint32_t xoff;         // offset of the crossing-table rows in a stage
   uint32_t stage_bytes;  // bytes per stage (16-byte multiple)
   uint32_t* flag;        // raised on a wait timeout
@@ -163,6 +165,7 @@ struct StreamSmem {
   uint64_t own_full[2], own_empty[2];
   uint64_t prog_full[2], prog_empty[2];
   uint64_t red_full[2], red_empty[2];  // the per-tile reduction across the consumer warps
+  uint64_t cvt_done, ownd_free;        // the widened own x: written by all warps / free again
   int abort;
 };
 
@@ -431,10 +434,14 @@ __device__ __forceinline__ bool consume_ops(const Prog& pg, int o0, int o1, uint
   return true;
 }
 
-template <typename T, typename Acc, int U>
+// kOwnD (FP32 rows): the block's own x is widened to FP64 once into a shared
+// buffer, so that the diagonal, the lo-part flips and the <x, y> partials
+// read it without a conversion each (the FP32 -> FP64 conversions run on a
+// quarter-rate pipe); the FP32 own buffer is released right after.
+template <typename T, typename Acc, int U, bool kOwnD>
 __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T* __restrict__ y,
                                         double* __restrict__ alpha_part, const StreamCfg& cfg, StreamSmem& sm,
-                                        const unsigned char* own, const unsigned char* ring) {
+                                        const unsigned char* own, const unsigned char* ring, double* ownd) {
   constexpr bool kOrdered = sizeof(T) == 8;
   const uint32_t tid = threadIdx.x;
   const int lane = (int)(tid & 31u), warp = (int)(tid >> 5);
@@ -495,10 +502,30 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
       if (!consume_ops<T, Acc, U>(pg, pg.nlow, pg.nops, q, nlo, cfg, sm, ring, acc)) return;
     } else {
       if (!wait_phase(&sm.own_full[os], (b / (uint32_t)cfg.OB) & 1u, &sm.abort, cfg.flag)) return;
+      if (kOwnD) {
+        // the widened buffer is free once every warp finished the previous block
+        if (b > 0 && !wait_phase(&sm.ownd_free, (b - 1u) & 1u, &sm.abort, cfg.flag)) return;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+          const uint32_t r = tid + j * kHvThreads;
+          if (r < nk) ownd[r] = (double)ox[r];
+        }
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&sm.own_empty[os]);  // the FP32 copy is no longer read
+          mbar_arrive(&sm.cvt_done);
+        }
+        if (!wait_phase(&sm.cvt_done, b & 1u, &sm.abort, cfg.flag)) return;
+      }
 #pragma unroll
       for (int j = 0; j < U; ++j) {
         const uint32_t r = tid + j * kHvThreads;
-        if (r < nk) acc[j].add(apply::diag_fp32(t, base + r), ox[r]);
+        if (r < nk) {
+          if (kOwnD)
+            acc[j].add(apply::diag_fp32(t, base + r), ownd[r]);
+          else
+            acc[j].add(apply::diag_fp32(t, base + r), ox[r]);
+        }
       }
       if (!consume_ops<T, Acc, U>(pg, 0, pg.nops, q, nlo, cfg, sm, ring, acc)) return;
       for (int e = 0; e < t.ell_w; e += 2) {
@@ -517,7 +544,12 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
         for (int v = 0; v < 2; ++v)
 #pragma unroll
           for (int j = 0; j < U; ++j)
-            if (ent[v][j] != kEllPad) acc[j].add(sm.lolo_c[ent[v][j] >> 16], ox[ent[v][j] & 0xffffu]);
+            if (ent[v][j] != kEllPad) {
+              if (kOwnD)
+                acc[j].add(sm.lolo_c[ent[v][j] >> 16], ownd[ent[v][j] & 0xffffu]);
+              else
+                acc[j].add(sm.lolo_c[ent[v][j] >> 16], ox[ent[v][j] & 0xffffu]);
+            }
       }
     }
     // the rows, then the <x, y> partials per 2048-row tile (tree of block_sum_all)
@@ -539,7 +571,7 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
             const int j = tq * kJ + jj;
             if (j < U) {
               const uint32_t r = tid + j * kHvThreads;
-              if (r < nk) dot = fma((double)ox[r], (double)yv[j], dot);
+              if (r < nk) dot = fma(kOwnD ? ownd[r] : (double)ox[r], (double)yv[j], dot);
             }
           }
           for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
@@ -566,7 +598,10 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
     }
     __syncwarp();
     if (lane == 0) {
-      mbar_arrive(&sm.own_empty[os]);
+      if (kOwnD)
+        mbar_arrive(&sm.ownd_free);
+      else
+        mbar_arrive(&sm.own_empty[os]);
       mbar_arrive(&sm.prog_empty[pb]);
     }
     ++b;
@@ -574,10 +609,11 @@ __device__ __forceinline__ void consume(const ApplyCtx& c, const DevTables& t, T
 }
 
 // y = H x, one CTA per SM: warps 0-7 consume, warp 8 produces.
-template <typename T, typename Acc, int U>
+template <typename T, typename Acc, int U, bool kOwnD>
 __global__ void __launch_bounds__(kThreads, 1) hvs_kernel(const __grid_constant__ HvParams P, const DevTables t,
                                                          const T* __restrict__ x, T* __restrict__ y,
                                                          double* __restrict__ alpha_part, const StreamCfg cfg) {
+  static_assert(!kOwnD || sizeof(T) == 4, "the widened own x is for FP32 rows");
   extern __shared__ __align__(128) unsigned char hvs_dyn[];
   __shared__ StreamSmem sm;
   for (int q = threadIdx.x; q < P.n_pairs; q += kThreads) {
@@ -599,17 +635,20 @@ __global__ void __launch_bounds__(kThreads, 1) hvs_kernel(const __grid_constant_
       mbar_init(&sm.red_full[s], kConsumerWarps);
       mbar_init(&sm.red_empty[s], 1);
     }
+    mbar_init(&sm.cvt_done, kConsumerWarps);
+    mbar_init(&sm.ownd_free, kConsumerWarps);
     sm.abort = 0;
     mbar_fence_init();
   }
   __syncthreads();
   const ApplyCtx c = apply::ctx_of(P);
   unsigned char* own = hvs_dyn;
-  unsigned char* ring = hvs_dyn + (size_t)cfg.OB * cfg.own_bytes;
+  unsigned char* ring = hvs_dyn + cfg.ring_off;
+  double* ownd = reinterpret_cast<double*>(hvs_dyn + cfg.ownd_off);
   if (threadIdx.x >= kHvThreads)
     produce<T>(c, t, x, cfg, sm, own, ring);
   else
-    consume<T, Acc, U>(c, t, y, alpha_part, cfg, sm, own, ring);
+    consume<T, Acc, U, kOwnD>(c, t, y, alpha_part, cfg, sm, own, ring, ownd);
 }
 
 }  // namespace sapply

@@ -280,6 +280,7 @@ constexpr HvVariant kVariants[] = {
     {0, 2, 6, "r2b6"},      {0, 8, 3, "r8b3"},      {1, 4, 3, "blk1r4b3"},  {2, 2, 4, "blk2r2b4"},
     {2, 4, 2, "blk2r4b2"},  {2, 2, 3, "blk2r2b3"},  {1, 4, 4, "blk1r4b4"},  {1, 2, 4, "blk1r2b4"},
     {-1, 14, 2, "str14o2"}, {-1, 14, 1, "str14o1"}, {-1, 26, 2, "str26o2"}, {-1, 26, 1, "str26o1"},
+    {-1, 14, 1, "str14w"},  {-1, 26, 1, "str26w"},  // FP32: own x widened once
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -374,14 +375,17 @@ struct StreamShape {
   bool fits = false;
 };
 
-template <typename T, typename Acc, int U>
+template <typename T, typename Acc, int U, bool kOwnD>
 int launch_stream(int OB, const HvParams& P, const DevTables& t, const T* x, T* y, double* alpha_part,
                   cudaStream_t st) {
+  if constexpr (kOwnD && sizeof(T) != 4) {
+    return kVariantNotApplicable;  // FP64 rows read their own x as it is
+  } else {
   if (!t.blk_h || !t.flag || t.maxrows <= 0 || t.Nlo < 8 || t.Nlo > 16) return kVariantNotApplicable;
   if ((t.maxrows + kHvThreads - 1) / kHvThreads > U) return kVariantNotApplicable;
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(t.xtab)) & 15u)
     return kVariantNotApplicable;
-  auto kern = hvs_kernel<T, Acc, U>;
+  auto kern = hvs_kernel<T, Acc, U, kOwnD>;
   static int limit_rc = -1;
   static size_t static_bytes = 0;
   static std::map<std::pair<int, int>, StreamShape> shapes;  // (maxrows, OB) -> shape
@@ -400,12 +404,15 @@ int launch_stream(int OB, const HvParams& P, const DevTables& t, const T* x, T* 
       n.cfg.own_bytes = (uint32_t)bapply::bundle_align16((size_t)t.maxrows * sizeof(T) + 32);
       n.cfg.xoff = n.cfg.own_bytes;
       n.cfg.stage_bytes = n.cfg.xoff + (uint32_t)bapply::bundle_align16((size_t)t.maxrows * 2 + 32);
+      const uint32_t ownd_bytes = kOwnD ? (uint32_t)bapply::bundle_align16((size_t)t.maxrows * 8 + 32) : 0u;
+      n.cfg.ownd_off = (uint32_t)OB * n.cfg.own_bytes;
+      n.cfg.ring_off = n.cfg.ownd_off + ownd_bytes;
       const int64_t avail = (int64_t)optin - (int64_t)static_bytes - 1024;
-      const int64_t S = (avail - (int64_t)OB * n.cfg.own_bytes) / (int64_t)n.cfg.stage_bytes;
+      const int64_t S = (avail - (int64_t)n.cfg.ring_off) / (int64_t)n.cfg.stage_bytes;
       if (limit_rc == AED_OK && S >= 2) {
         n.cfg.S = (int)(S < sapply::kMaxStages ? S : sapply::kMaxStages);
         n.cfg.OB = OB;
-        n.dyn = (size_t)OB * n.cfg.own_bytes + (size_t)n.cfg.S * n.cfg.stage_bytes;
+        n.dyn = (size_t)n.cfg.ring_off + (size_t)n.cfg.S * n.cfg.stage_bytes;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sapply::kThreads, n.dyn);
         n.fits = per_sm >= 1;
@@ -422,6 +429,7 @@ int launch_stream(int OB, const HvParams& P, const DevTables& t, const T* x, T* 
   if (grid < 1) return AED_OK;
   kern<<<(unsigned)grid, sapply::kThreads, sh.dyn, st>>>(P, t, x, y, alpha_part, cfg);
   return check_launch("hvs_kernel");
+  }
 }
 
 template <typename T, typename Acc>
@@ -441,10 +449,12 @@ int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, 
     case 9: return launch_bundle<T, Acc, 2, 2, 3>(P, t, x, y, alpha_part, st);
     case 10: return launch_bundle<T, Acc, 4, 1, 4>(P, t, x, y, alpha_part, st);
     case 11: return launch_bundle<T, Acc, 2, 1, 4>(P, t, x, y, alpha_part, st);
-    case 12: return launch_stream<T, Acc, 14>(2, P, t, x, y, alpha_part, st);
-    case 13: return launch_stream<T, Acc, 14>(1, P, t, x, y, alpha_part, st);
-    case 14: return launch_stream<T, Acc, 26>(2, P, t, x, y, alpha_part, st);
-    case 15: return launch_stream<T, Acc, 26>(1, P, t, x, y, alpha_part, st);
+    case 12: return launch_stream<T, Acc, 14, false>(2, P, t, x, y, alpha_part, st);
+    case 13: return launch_stream<T, Acc, 14, false>(1, P, t, x, y, alpha_part, st);
+    case 14: return launch_stream<T, Acc, 26, false>(2, P, t, x, y, alpha_part, st);
+    case 15: return launch_stream<T, Acc, 26, false>(1, P, t, x, y, alpha_part, st);
+    case 16: return launch_stream<T, Acc, 14, true>(1, P, t, x, y, alpha_part, st);
+    case 17: return launch_stream<T, Acc, 26, true>(1, P, t, x, y, alpha_part, st);
     default: return fail(AED_ERR_INVALID, "unknown apply variant");
   }
 }
