@@ -393,14 +393,29 @@ def test_mixed_refinements_agree(name, p, nev):
     h32 = ed.Hamiltonian.from_parameters(p, precision=ed.FP32)
     rr = h32.solve(nev=nev, seed=2)
     lz = h32.solve(nev=nev, seed=2, refine=1)
-    assert rr["refined_by"] == "rayleigh_ritz", rr
+    # the default takes Rayleigh-Ritz when its bound holds and FP64 Lanczos otherwise
+    assert rr["refined_by"] in ("rayleigh_ritz", "lanczos"), rr
     assert lz["refined_by"] == "lanczos"
     for r in (rr, lz):
         assert r["converged"] and len(r["evals"]) == len(r64["evals"])
         assert np.all(np.abs(r["evals"] - r64["evals"]) <= 1e-9 * np.abs(r64["evals"]))
-    # the Rayleigh-Ritz values lie above the true ones by at most the bound (plus FP64 rounding)
-    d = rr["evals"] - r64["evals"]
-    assert np.all(d >= -1e-12 * np.abs(r64["evals"])) and np.all(d <= rr["errors"] + 1e-12 * np.abs(r64["evals"]))
+    if rr["refined_by"] == "rayleigh_ritz":
+        # the Rayleigh-Ritz values lie above the true ones by at most the bound (plus FP64 rounding)
+        d = rr["evals"] - r64["evals"]
+        assert np.all(d >= -1e-12 * np.abs(r64["evals"]))
+        assert np.all(d <= rr["errors"] + 1e-12 * np.abs(r64["evals"]))
+
+
+@pytest.mark.parametrize("L,j2", [(20, 0.2), (22, 0.3)])
+def test_rayleigh_ritz_refinement_taken_on_a_gapped_ground_state(L, j2):
+    """A J1-J2 chain's ground state (a clear gap to the next level): the FP32 phase's Ritz vector refined
+    by Rayleigh-Ritz alone (K FP64 applies, no FP64 Lanczos steps), within 1e-9 of the FP64 solve."""
+    p = spin_params(LATTICE="nnn chain lattice", L=L, J=1, J1=j2)
+    r64 = ed.Hamiltonian.from_parameters(p).solve(nev=1, seed=4)
+    r32 = ed.Hamiltonian.from_parameters(p, precision=ed.FP32).solve(nev=1, seed=4)
+    assert r32["refined_by"] == "rayleigh_ritz", r32
+    assert r32["iterations"] <= 6  # the FP64 applies of the refinement
+    assert abs(r32["evals"][0] - r64["evals"][0]) <= 1e-9 * abs(r64["evals"][0])
 
 
 def _basis_and_copies(ham, r):
