@@ -19,12 +19,16 @@
 // r^2 / gap on each eigenvalue is below 1e-11 |lambda|.
 
 #include <algorithm>
-#include <future>
-#include <deque>
 #include <chrono>
-#include <functional>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <future>
+#include <mutex>
+#include <thread>
+#include <vector>
 
 #include "handle.h"
 #include "tmatrix_core.h"
@@ -64,8 +68,65 @@ struct HostPinned {
   }
 };
 
+// Host threads for the T-matrix analyses of the recurrences (shared by all
+// handles and server lanes of the process; started on first use).  A small
+// sector's step takes the GPU microseconds while the analysis of T(m) takes
+// O(m^2) host time, so the analyses of several sizes run side by side.
+class AnalysisPool {
+ public:
+  static AnalysisPool& get() {
+    static AnalysisPool pool;
+    return pool;
+  }
+  int threads() const { return (int)th_.size(); }
+  template <typename F>
+  auto submit(F f) -> std::future<decltype(f())> {
+    auto task = std::make_shared<std::packaged_task<decltype(f())()>>(std::move(f));
+    auto fut = task->get_future();
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      q_.emplace_back([task] { (*task)(); });
+    }
+    cv_.notify_one();
+    return fut;
+  }
+
+ private:
+  AnalysisPool() {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int n = (int)std::max(2u, std::min(hc ? hc : 2u, 16u));
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { work(); });
+  }
+  ~AnalysisPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void work() {
+    while (true) {
+      std::function<void()> job;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return stop_ || !q_.empty(); });
+        if (q_.empty()) return;
+        job = std::move(q_.front());
+        q_.pop_front();
+      }
+      job();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> q_;
+  std::vector<std::thread> th_;
+  bool stop_ = false;
+};
+
 struct EventRing {
-  static constexpr int kN = 4;
+  static constexpr int kN = 16;  // > the largest lookahead + 1
   cudaEvent_t ev[kN] = {};
   ~EventRing() {
     for (auto& e : ev)
@@ -110,13 +171,19 @@ int lanczos_step_tail(aed_handle* h, bool f32, const void* vprev, const void* x,
 
 // Steps the device runs ahead of the host's T-matrix analysis.  A step of a
 // large sector keeps the GPU busy longer than the analysis takes, so one step
-// ahead suffices; for small sectors (fewer than 2^24 vector scalars: the
+// ahead suffices; for mid-size sectors (fewer than 2^24 vector scalars: the
 // momentum sectors, chains up to L = 26) three hide the analysis and the
-// launch latency.  The steps launched past the stop are discarded.  The
-// recurrence vectors rotate through lookahead + 2 slots, so that v_{m-1} and
-// v_m survive the extra steps (resume, checkpoint).
-constexpr int kMaxRing = 5;
-inline int lanczos_lookahead(const aed_handle* h) { return h->vlen >= ((int64_t)1 << 24) ? 1 : 3; }
+// launch latency; below 2^20 scalars a step takes the GPU a few microseconds
+// and the O(m^2) analyses set the pace, so ten run side by side.  The steps
+// launched past the stop are discarded.  The recurrence vectors rotate
+// through lookahead + 2 slots, so that v_{m-1} and v_m survive the extra
+// steps (resume, checkpoint).
+constexpr int kMaxRing = 12;
+inline int lanczos_lookahead(const aed_handle* h) {
+  if (h->vlen >= ((int64_t)1 << 24)) return 1;
+  if (h->vlen >= ((int64_t)1 << 20)) return 3;
+  return std::min(10, AnalysisPool::get().threads());
+}
 inline int ring_slots(const aed_handle* h) { return lanczos_lookahead(h) + 2; }
 
 // Full reorthogonalisation of an FP32 recurrence whose vectors v_0 .. v_j are
@@ -307,6 +374,14 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
   }
   const int par = R.ahead;
   std::deque<std::future<std::pair<int, TmatInfo>>> pending;  // analyses of T(check), T(check + 1), ...
+  // the pool's tasks read alpha / beta: every return waits for them first
+  struct Drain {
+    std::deque<std::future<std::pair<int, TmatInfo>>>& d;
+    ~Drain() {
+      for (auto& f : d)
+        if (f.valid()) f.wait();
+    }
+  } drain{pending};
   int check = m0 == 0 ? 1 : m0;  // the T size whose verdict comes next
   int submit = check;            // the next T size to analyse
   int m = check;
@@ -334,8 +409,13 @@ int run_recurrence(Recurrence& R, const StopRule& stop, SlotFn slot, int m0, int
         if (!invariant_m && R.beta.back() == 0.0) invariant_m = submit;
       }
       if (submit > 1) {
-        pending.push_back(std::async(par > 1 ? std::launch::async : std::launch::deferred, analysis, submit, R.amax,
-                                     R.bmax));
+        if (par > 1) {
+          const double am = R.amax, bm = R.bmax;
+          const int ms = submit;
+          pending.push_back(AnalysisPool::get().submit([analysis, ms, am, bm] { return analysis(ms, am, bm); }));
+        } else {
+          pending.push_back(std::async(std::launch::deferred, analysis, submit, R.amax, R.bmax));
+        }
       } else {
         std::promise<std::pair<int, TmatInfo>> none;
         none.set_value({AED_OK, TmatInfo()});
