@@ -721,7 +721,8 @@ def _result_dict(res):
     n = res.n_evals
     return {"evals": np.array(res.evals[:n]), "errors": np.array(res.errors[:n]), "iterations": res.iterations,
             "iterations_low": res.iterations_low, "evals_low": np.array(res.evals_low[:n]),
-            "converged": bool(res.converged), "seconds": res.seconds}
+            "converged": bool(res.converged), "seconds": res.seconds,
+            "refined_by": REFINED_BY.get(res.refined_by, str(res.refined_by))}
 
 
 class Server:

@@ -314,6 +314,7 @@ int pick_variant(aed_handle* h, bool f32, const void* x, void* y, int* out) {
   int rc = AED_OK;
   // as solves run them: with the per-tile <x,y> partials; best of three
   for (int v = 0; v < hv_num_variants() && !rc; ++v) {
+    if (!hv_variant_tuned(v)) continue;
     rc = launch_variant(h, f32, v, x, y, h->d_partA);  // warm-up
     if (rc == kVariantNotApplicable) {  // does not fit this sector
       rc = AED_OK;

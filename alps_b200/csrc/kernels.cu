@@ -460,6 +460,10 @@ int launch_hv_t(int v, const HvParams& P, const DevTables& t, const T* x, T* y, 
 }
 
 int hv_num_variants() { return kNumVariants; }
+// The stream applies trail the bundle applies on every sector measured (1.9 to
+// 2.3 times slower: one CTA per SM leaves too few warps to issue), so the
+// autotuner does not time them; AED_HV_VARIANT still selects them.
+bool hv_variant_tuned(int v) { return v >= 0 && v < kNumVariants && kVariants[v].B >= 0; }
 const char* hv_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
 
 int launch_hv_f64(int variant, const HvParams& P, const DevTables& t, const double* x, double* y,

@@ -52,6 +52,8 @@ int launch_hv_f32(int variant, const HvParams& P, const DevTables& t, const floa
 constexpr int kVariantNotApplicable = 2;
 int hv_num_variants();
 const char* hv_variant_name(int v);
+// Whether the autotuner times variant v (the stream applies are left out).
+bool hv_variant_tuned(int v);
 
 // per-row diagonal table (once per handle)
 int launch_diag_table(const HvParams& P, const DevTables& t, double* dg, cudaStream_t st);

@@ -510,6 +510,8 @@ void finish_request(aed_server* s, int k) {
   r.res.iterations = I.iters;
   r.res.iterations_low = s->precision == AED_FP32 ? I.m_low : 0;
   r.res.converged = I.converged;
+  // the batched mixed path refines with FP64 Lanczos steps
+  r.res.refined_by = s->precision == AED_FP32 ? AED_REFINE_LANCZOS : AED_REFINE_NONE;
   for (int i = 0; i < I.n_evals && i < AED_MAX_NEV; ++i) {
     r.res.evals[i] = I.evals[i];
     r.res.errors[i] = I.errs[i];

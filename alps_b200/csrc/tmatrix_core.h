@@ -54,6 +54,24 @@ AED_HD inline int ql(int n, double* d, double* e, double* zl, double* zf) {
       bool split = false;
       for (int i = m - 1; i >= l; --i) {
         const double f = s * e[i], b = c * e[i];
+#ifdef __CUDA_ARCH__
+        // one reciprocal square root instead of a square root and two
+        // divisions, whose long dependent chains set the pace of the batched
+        // check (a GPU thread per matrix); rsqrt is within 1 ulp, so the
+        // rotation stays orthogonal to a few ulps and QL backward stable
+        const double h2 = f * f + g * g;
+        if (h2 == 0.0) {
+          e[i + 1] = 0.0;
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          split = true;
+          break;
+        }
+        const double ri = rsqrt(h2);
+        e[i + 1] = h2 * ri;
+        s = f * ri;
+        c = g * ri;
+#else
         const double r = sqrt(f * f + g * g);
         e[i + 1] = r;
         if (r == 0.0) {
@@ -64,6 +82,7 @@ AED_HD inline int ql(int n, double* d, double* e, double* zl, double* zf) {
         }
         s = f / r;
         c = g / r;
+#endif
         const double gg = d[i + 1] - p;
         const double t = (d[i] - gg) * s + 2.0 * c * b;
         p = s * t;

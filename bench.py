@@ -730,13 +730,16 @@ def run_serve(args):
     srv.run(w)
     pending = {}
     lat = []
+    large = []  # whether each finished request was one for a single-instance lane
+    work = {p: {"iterations_low": 0, "iterations": 0, "refined_by": {}} for p in ("lanes", "batch")}
+    min_dim = args.lane_min_dim if args.lanes > 0 else None
     i = 0
     t0 = time.perf_counter()
     while i < len(reqs) or pending:
         now = time.perf_counter() - t0
         while i < len(reqs) and reqs[i][0] <= now:
             arr, n, b, nev, sd = reqs[i]
-            pending[srv.submit(n, n // 2, b, nev=nev, seed=sd)] = arr
+            pending[srv.submit(n, n // 2, b, nev=nev, seed=sd)] = (arr, comb(n, n // 2))
             i += 1
         if pending:
             srv.step()
@@ -744,13 +747,26 @@ def run_serve(args):
             for t in list(pending):
                 r = srv.poll(t)
                 if r is not None:
-                    lat.append(done_t - pending.pop(t))
+                    arr, dim = pending.pop(t)
+                    lat.append(done_t - arr)
+                    big = min_dim is not None and dim >= min_dim
+                    large.append(big)
+                    w = work["lanes" if big else "batch"]
+                    w["iterations_low"] += r["iterations_low"]
+                    w["iterations"] += r["iterations"]
+                    w["refined_by"][r["refined_by"]] = w["refined_by"].get(r["refined_by"], 0) + 1
         elif i < len(reqs):
             time.sleep(max(0.0, min(0.002, reqs[i][0] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
     lat = np.array(lat)
+    large = np.array(large, dtype=bool)
+
+    def pct(a):
+        return {"n": int(a.size), "p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99))} if a.size \
+            else {"n": 0}
+
     line = {"metric": f"served Lanczos: solves/s and latency (Poisson {args.rate:g} req/s)", "value": len(reqs) / wall,
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64" if prec == ed.FP32 else "f64",
             "data": "synthetic",
@@ -761,6 +777,8 @@ def run_serve(args):
                        "lanes": {"max": args.lanes, "min_dim": args.lane_min_dim if args.lanes > 0 else None}},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "mean": float(lat.mean()), "max": float(lat.max())},
+            "latency_s_by_path": {"lanes": pct(lat[large]), "batch": pct(lat[~large])},
+            "work_by_path": work,
             "offered_rate": args.rate, "graph_launches": st["graph_launches"], "wall_s": wall}
     print(json.dumps(line))
 
