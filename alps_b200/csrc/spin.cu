@@ -332,30 +332,9 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
     for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
       const uint32_t lo = t.lolist[lbase + r];
       const uint32_t row = base + r;
-      // off-diagonal terms four at a time: the x loads of four targets are in
-      // flight together, and the terms are added in the walk's order (the
-      // pending ones shift through p0..p3, oldest in p3)
       double off = 0.0;
-      double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
-      uint32_t k0 = 0, k1 = 0, k2 = 0, k3 = 0;
-      int np = 0;
-      auto flush = [&]() {
-        const double x3 = np > 3 ? __ldg(x + k3) : 0.0, x2 = np > 2 ? __ldg(x + k2) : 0.0;
-        const double x1 = np > 1 ? __ldg(x + k1) : 0.0, x0 = np > 0 ? __ldg(x + k0) : 0.0;
-        if (np > 3) off = fma(v3, x3, off);
-        if (np > 2) off = fma(v2, x2, off);
-        if (np > 1) off = fma(v1, x1, off);
-        if (np > 0) off = fma(v0, x0, off);
-        np = 0;
-      };
-      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, h, lo, base, r, [&](double v, uint32_t rk) {
-        v3 = v2; k3 = k2;
-        v2 = v1; k2 = k1;
-        v1 = v0; k1 = k0;
-        v0 = v; k0 = rk;
-        if (++np == 4) flush();
-      });
-      flush();
+      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, h, lo, base, r,
+                                 [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
       const double xi = x[row];
       const double yi = fma(dg, xi, off);
       y[row] = yi;
