@@ -246,46 +246,18 @@ __global__ void __launch_bounds__(kMomThreads) mom_hv_kernel(const __grid_consta
       const double2 xi = x[i];
       const double d = m.diag[i];
       double are = d * xi.x, aim = d * xi.y;
-      // kF flips at a time: each level of the dependent chain (ranks of the
-      // flipped states, their map entries, then n_j and x_j) is issued for
-      // all kF flips before the next, and the terms are added in flip order
-      // afterwards, so the sums are the ones of a flip-by-flip walk
-      constexpr int kF = 4;
-      for (int q0 = 0; q0 < nf; q0 += kF) {
-        bool live[kF];
-        uint32_t rk[kF];
-#pragma unroll
-        for (int v = 0; v < kF; ++v) {
-          const int q = q0 + v;
-          const uint32_t fmq = q < nf ? fm[q] : 0u;
-          const uint32_t b = r & fmq;
-          live[v] = q < nf && b != 0u && b != fmq;  // antiparallel spins: a flip
-          const uint32_t s2 = r ^ fmq;
-          rk[v] = live[v] ? __ldg(t.thi + (s2 >> t.Nlo)) + __ldg(t.tlo + (s2 & lm)) : 0u;
-        }
-        uint32_t e[kF];
-#pragma unroll
-        for (int v = 0; v < kF; ++v) {
-          e[v] = live[v] ? __ldg(m.map + rk[v]) : kMomNone;
-          live[v] = live[v] && e[v] != kMomNone;
-        }
-        double nj[kF];
-        double2 xj[kF];
-#pragma unroll
-        for (int v = 0; v < kF; ++v) {
-          const uint32_t j = e[v] & jmask;
-          nj[v] = live[v] ? __ldg(m.norm + j) : 0.0;
-          xj[v] = live[v] ? x[j] : make_double2(0.0, 0.0);
-        }
-#pragma unroll
-        for (int v = 0; v < kF; ++v) {
-          if (!live[v]) continue;
-          const uint32_t tt = e[v] >> kMomRepBits;
-          const double f = fc[q0 + v] * (nj[v] / ni);
-          const double cr = f * pre[tt], ci = f * pim[tt];
-          are = fma(cr, xj[v].x, fma(-ci, xj[v].y, are));
-          aim = fma(cr, xj[v].y, fma(ci, xj[v].x, aim));
-        }
+      for (int q = 0; q < nf; ++q) {
+        const uint32_t b = r & fm[q];
+        if (b == 0u || b == fm[q]) continue;  // parallel spins: no flip
+        const uint32_t s2 = r ^ fm[q];
+        const uint32_t e = __ldg(m.map + __ldg(t.thi + (s2 >> t.Nlo)) + __ldg(t.tlo + (s2 & lm)));
+        if (e == kMomNone) continue;
+        const uint32_t j = e & jmask, tt = e >> kMomRepBits;
+        const double f = fc[q] * (__ldg(m.norm + j) / ni);
+        const double cr = f * pre[tt], ci = f * pim[tt];
+        const double2 xj = x[j];
+        are = fma(cr, xj.x, fma(-ci, xj.y, are));
+        aim = fma(cr, xj.y, fma(ci, xj.x, aim));
       }
       y[i] = make_double2(are, aim);
       dot = fma(xi.x, are, fma(xi.y, aim, dot));
