@@ -100,7 +100,7 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
                         bool accumulate, cudaStream_t st);
 
 // ---- Rayleigh-Ritz refinement of the mixed path (refine.cu) ----
-constexpr int kMaxRR = 6;     // Ritz vectors in one refinement
+constexpr int kMaxRR = 8;     // Ritz vectors in one refinement
 constexpr int kMaxComb = 16;  // stored vectors per ritz_combine_multi call (a store chunk)
 struct VecSet {
   double* p[kMaxRR];

@@ -22,6 +22,8 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -624,7 +626,11 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   const int c = std::min(nev, (int)T1.evals.size());
   if (c < 1 || (int)T1.evals.size() <= c) return AED_OK;  // no value above the clusters to bound the gap
   const int K = tcore::ritz_span((int)T1.evals.size(), nev, T1.first.data(), T1.mults.data(), m1);
-  if (K < 1 || K > kMaxRR) return AED_OK;
+  const bool verbose = std::getenv("AED_VERBOSE") != nullptr;
+  if (K < 1 || K > kMaxRR) {
+    if (verbose) std::fprintf(stderr, "[aed] rayleigh-ritz: %d Ritz vectors span the clusters (at most %d)\n", K, kMaxRR);
+    return AED_OK;
+  }
   // coefficients chunk by chunk of the store: [K x cnt] blocks at K * j0
   std::vector<double> cf((size_t)K * m1);
   for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
@@ -637,7 +643,10 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   const int np = K * (K + 1) / 2 + K * K;
   const size_t part_bytes = (((size_t)np * nch * 8) + 255) & ~(size_t)255;
   void* ws = nullptr;
-  int rc = handle_workspace(h, 2, 2 * (size_t)K * vb + part_bytes + 64 * 8, &ws);
+  // the finished sums: np Gram entries, then (reused) the residuals
+  constexpr int kMaxSums = kMaxRR * (kMaxRR + 1) / 2 + kMaxRR * kMaxRR;
+  static_assert(kMaxSums >= kMaxRR, "residual sums fit the Gram buffer");
+  int rc = handle_workspace(h, 2, 2 * (size_t)K * vb + part_bytes + (size_t)kMaxSums * 8, &ws);
   if (rc) return rc;
   VecSet psi{}, img{};
   for (int k = 0; k < K; ++k) {
@@ -647,7 +656,7 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   double* part = (double*)((char*)ws + 2 * (size_t)K * vb);
   double* outd = (double*)((char*)part + part_bytes);
   double* hout = nullptr;
-  if ((rc = handle_pinned(h, 128, &hout))) return rc;
+  if ((rc = handle_pinned(h, kMaxSums, &hout))) return rc;
   AED_CUDA_TRY(cudaMemcpyAsync(coef_dev, cf.data(), cf.size() * 8, cudaMemcpyHostToDevice, h->stream));
   for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
     const int cnt = std::min(kStoreChunk, m1 - j0);
@@ -699,36 +708,73 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   for (int i = 0; i < Kp; ++i)
     for (int j = i + 1; j < Kp; ++j) C[i * Kp + j] = C[j * Kp + i] = 0.5 * (C[i * Kp + j] + C[j * Kp + i]);
   jacobi_eigen(Kp, C, th, Y);
-  // coefficients over Psi of the Ritz pairs: c_r = B y_r
+  // coefficients over Psi of the Ritz pairs: c_r = B y_r; each value is then
+  // taken as the Rayleigh quotient c^T A c / c^T G c of its own vector, which
+  // rounding in an ill-conditioned B cannot move (a ghost copy of a
+  // converged vector leaves a nearly dependent pair in Psi)
   double cr[kMaxRR][kMaxRR];
-  ResidCoef rcoef{};
-  for (int q = 0; q < Kp; ++q)
+  std::vector<std::pair<double, int>> byval;
+  for (int q = 0; q < Kp; ++q) {
     for (int k = 0; k < K; ++k) {
       double s = 0.0;
       for (int j = 0; j < Kp; ++j) s += B[k * K + j] * Y[j * Kp + q];
       cr[q][k] = s;
-      rcoef.cw[q][k] = s;
-      rcoef.cx[q][k] = -th[q] * s;
     }
-  if ((rc = launch_resid(psi, img, rcoef, K, Kp, D, part, outd, h->stream))) return rc;
-  AED_CUDA_TRY(cudaMemcpyAsync(hout, outd, (size_t)Kp * 8, cudaMemcpyDeviceToHost, h->stream));
-  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  double r2 = 0.0;
-  for (int q = 0; q < Kp; ++q) r2 += hout[q];
-  // lowest eigenvalue outside the subspace, from below: the FP32 phase's next
-  // distinct value less its error estimate and its FP32 resolution
+    double num = 0.0, den = 0.0;
+    for (int a = 0; a < K; ++a)
+      for (int b = 0; b < K; ++b) {
+        num += cr[q][a] * A[a * K + b] * cr[q][b];
+        den += cr[q][a] * G[a * K + b] * cr[q][b];
+      }
+    th[q] = den > 0 ? num / den : th[q];
+    byval.push_back({th[q], q});
+  }
+  std::sort(byval.begin(), byval.end());
+  // lowest eigenvalue outside the Ritz pairs that are bounded, from below: the
+  // FP32 phase's next distinct value less its error estimate and its FP32
+  // resolution.  Only the pairs below it are bounded (block Kato-Temple over
+  // their span: 0 <= sum (theta_i - lambda_i) <= sum |r_i|^2 / (lambda_next -
+  // theta_max)); a pair above it (the difference of a vector and its ghost
+  // copy, mostly FP32 noise) is left out
   const double next = T1.evals[c];
   const double next_lo = next - std::max(T1.errs[c], kFp32MergeRel * std::fabs(next)) -
                          kFp32MergeRel * std::max(std::fabs(T1.evals.front()), std::fabs(T1.evals.back()));
-  const double gap = next_lo - th[Kp - 1];
+  int nb = 0;
+  while (nb < Kp && byval[nb].first < next_lo) ++nb;
+  if (nb < 1) return AED_OK;
+  ResidCoef rcoef{};
+  for (int i = 0; i < nb; ++i) {
+    const int q = byval[i].second;
+    for (int k = 0; k < K; ++k) {
+      rcoef.cw[i][k] = cr[q][k];
+      rcoef.cx[i][k] = -th[q] * cr[q][k];
+    }
+  }
+  if ((rc = launch_resid(psi, img, rcoef, K, nb, D, part, outd, h->stream))) return rc;
+  AED_CUDA_TRY(cudaMemcpyAsync(hout, outd, (size_t)nb * 8, cudaMemcpyDeviceToHost, h->stream));
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  double r2 = 0.0, rn2 = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    const int q = byval[i].second;
+    double den = 0.0;  // |Psi c_q|^2
+    for (int a = 0; a < K; ++a)
+      for (int b = 0; b < K; ++b) den += cr[q][a] * G[a * K + b] * cr[q][b];
+    r2 += hout[i];
+    rn2 += den > 0 ? hout[i] / den : hout[i];
+  }
+  const double gap = next_lo - byval[nb - 1].first;
+  const double bound = rn2 / gap;
+  if (verbose)
+    std::fprintf(stderr,
+                 "[aed] rayleigh-ritz: K=%d kept=%d bounded=%d m=%d sum r^2=%.3e gap=%.3e bound=%.3e (accept <= %.3e)\n",
+                 K, Kp, nb, m1, r2, gap, bound, kRRTol * std::fabs(byval[0].first));
   if (!(gap > 0)) return AED_OK;
-  const double bound = r2 / gap;
   // distinct values: merged below the FP64 T-matrix threshold eps^(2/3) max|lambda| (tmatrix.h:148-150)
   const double scale = std::max(std::fabs(T1.evals.front()), std::fabs(T1.evals.back()));
   const double thold = std::pow(2.220446049250313e-16, 2.0 / 3.0) * scale;
   std::vector<int> pick;
-  for (int q = 0; q < Kp && (int)pick.size() < nev; ++q)
-    if (pick.empty() || th[q] - th[pick.back()] > thold) pick.push_back(q);
+  for (int i = 0; i < nb && (int)pick.size() < nev; ++i)
+    if (pick.empty() || th[byval[i].second] - th[pick.back()] > thold) pick.push_back(byval[i].second);
   if ((int)pick.size() < c) return AED_OK;  // fewer distinct values than the FP32 phase resolved
   for (int q : pick)
     if (!(bound <= kRRTol * std::max(std::fabs(th[q]), 1e-300))) return AED_OK;

@@ -192,7 +192,7 @@ int launch_ritz_combine_multi(const float* V, int64_t ld, int m, const double* c
   switch (K) {
 #define AED_CASE(k) \
   case k: ritz_combine_multi_kernel<k><<<grid, kCombThreads, 0, st>>>(V, ld, m, coef, out, n, accumulate); break;
-    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6)
+    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6) AED_CASE(7) AED_CASE(8)
 #undef AED_CASE
     default: return fail(AED_ERR_INVALID, "ritz_combine_multi: K");
   }
@@ -204,7 +204,7 @@ int launch_gram(const VecSet& X, const VecSet& Y, int K, int64_t n, double* part
   const int grid = grid_for(nch);
   switch (K) {
 #define AED_CASE(k) case k: gram_partials_kernel<k><<<grid, kRedThreads, 0, st>>>(X, Y, n, part, nch); break;
-    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6)
+    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6) AED_CASE(7) AED_CASE(8)
 #undef AED_CASE
     default: return fail(AED_ERR_INVALID, "gram: K");
   }
@@ -223,7 +223,7 @@ int launch_resid(const VecSet& X, const VecSet& Y, const ResidCoef& rcoef, int K
   switch (K) {
 #define AED_CASE(k) \
   case k: resid_partials_kernel<k><<<grid, kRedThreads, 0, st>>>(X, Y, rcoef, R, n, part, nch); break;
-    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6)
+    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6) AED_CASE(7) AED_CASE(8)
 #undef AED_CASE
     default: return fail(AED_ERR_INVALID, "resid: K");
   }

@@ -56,6 +56,7 @@ struct Request {
   aed_solve_result res{};
   size_t footprint = 0;
   bool cancelled = false;
+  std::string error;  // message of a failed request (the solving thread's aed_last_error)
 };
 
 struct Slot {
@@ -448,6 +449,7 @@ void lane_main(aed_server* s, Lane* L) {
     aed_solve_opts o = r.opts;
     rc = aed_solve(h, &o, &res);
   }
+  const std::string err = rc ? std::string(aed_last_error()) : std::string();
   if (h) aed_destroy(h);
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -455,6 +457,7 @@ void lane_main(aed_server* s, Lane* L) {
       r.res = res;
       r.res.seconds = std::chrono::duration<double>(clk::now() - r.t_submit).count();
       r.status = rc ? rc : AED_OK;
+      r.error = err;
     }
     s->used -= std::min(s->used, L->bytes);
   }
@@ -730,6 +733,7 @@ int aed_server_step(aed_server* s, int32_t* n_pending) {
     rc = admit(s, k, r);
     if (rc) {
       r->status = rc;
+      r->error = aed_last_error();
       release_slot(s, k);
       continue;
     }
@@ -775,8 +779,9 @@ int aed_server_poll(aed_server* s, int64_t ticket, aed_solve_result* out) {
   const int st = it->second->status;
   if (st == AED_PENDING) return AED_PENDING;
   *out = it->second->res;
+  const std::string err = it->second->error;
   s->requests.erase(it);
-  if (st != AED_OK) return fail(st, "request failed or was cancelled");
+  if (st != AED_OK) return fail(st, err.empty() ? std::string("request failed or was cancelled") : "request failed: " + err);
   return AED_OK;
 }
 

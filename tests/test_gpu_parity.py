@@ -418,6 +418,24 @@ def test_rayleigh_ritz_refinement_taken_on_a_gapped_ground_state(L, j2):
     assert abs(r32["evals"][0] - r64["evals"][0]) <= 1e-9 * abs(r64["evals"][0])
 
 
+@pytest.mark.parametrize("nev", [3, 4])
+def test_rayleigh_ritz_with_ghost_copies_in_the_clusters(nev):
+    """Heisenberg chain L=22 (uniform J): the FP32 phase runs long enough for a ghost copy of the ground
+    state, so the Ritz vectors of the nev lowest clusters (K > nev) hold a nearly dependent pair.  The
+    Rayleigh-Ritz step still bounds the nev lowest pairs (the pair made of the copy's FP32 noise lies
+    above the gap and is left out), and every value agrees with the FP64 solve within its reported
+    bound and 1e-9."""
+    b = [(i, (i + 1) % 22, 1.0, 1.0, 0.0) for i in range(22)]
+    r64 = ed.Hamiltonian(22, 11, b).solve(nev=nev, seed=2)
+    r32 = ed.Hamiltonian(22, 11, b, precision=ed.FP32).solve(nev=nev, seed=2)
+    assert r32["refined_by"] == "rayleigh_ritz", r32
+    assert r32["iterations"] > nev  # K Ritz vectors: the clusters held a ghost copy
+    assert len(r32["evals"]) == nev == len(r64["evals"])
+    for e32, e64, err in zip(r32["evals"], r64["evals"], r32["errors"]):
+        assert abs(e32 - e64) <= 1e-9 * abs(e64)
+        assert e32 - e64 <= err + 1e-12 * abs(e64)  # the bound holds (values from above)
+
+
 def _basis_and_copies(ham, r):
     """The stored FP32 Lanczos basis V (m x D) of the last mixed solve, max |V V^T - I|, and how many
     eigenvalues of its T-matrix lie within 1e-5 relative of the lowest (1 + the ghost copies)."""
