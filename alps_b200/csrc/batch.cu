@@ -16,6 +16,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cfloat>
+
 #include "apply.cuh"
 #include "apply_blocks.cuh"
 #include "batch.cuh"
@@ -190,15 +192,160 @@ __global__ void b_advance(BatchArgs a) {
   if (stepping(I)) I.j += 1;
 }
 
+// ---- lowest part of a T-matrix spectrum, one warp per T ----------------------
+// The check needs the lowest few distinct non-ghost eigenvalues of T(m)
+// (Tmatrix::compute's walk, tmatrix.h:121-228, stops after `want` of them),
+// the matching low eigenvalues of T without its first row and column (the
+// ghost test), the largest eigenvalue of T (the merge threshold) and, for
+// each reported simple value, the last component of its eigenvector (the
+// error estimate).  A QL sweep over the whole spectrum costs O(m^2) serial
+// plane rotations on one thread (9.6 ms for the longest T of a served batch);
+// here 32 lanes bracket one eigenvalue at a time by Sturm counts at 32
+// points (multisection, 33x narrower per round), O(m) per count, and the
+// eigenvector components come from inverse iteration, one lane each.
+
+// Number of eigenvalues below x of the symmetric tridiagonal matrix with
+// diagonal a[0..n) and off-diagonal b[0..n-1): sign changes of the leading
+// principal minors det(T_k - x) (Sturm), by the three-term recurrence kept
+// in range by power-of-two rescaling.  A zero minor counts as a change (the
+// pivot taken as a tiny negative, as dstebz does).
+__device__ __forceinline__ int sturm_count(const double* __restrict__ a, const double* __restrict__ b, int n,
+                                           double x) {
+  constexpr double kBig = 0x1p400, kSmall = 0x1p-400, kTiny = 0x1p-800;
+  double p0 = 1.0, p1 = a[0] - x;
+  if (p1 == 0.0) p1 = -kTiny;
+  int cnt = p1 < 0.0 ? 1 : 0;
+  for (int k = 1; k < n; ++k) {
+    const double bb = b[k - 1];
+    double p2 = fma(a[k] - x, p1, -(bb * bb) * p0);
+    if (p2 == 0.0) p2 = p1 > 0.0 ? -kTiny : kTiny;
+    cnt += (p2 < 0.0) != (p1 < 0.0) ? 1 : 0;
+    const double ap = fabs(p2);
+    if (ap > kBig) {
+      p2 *= kSmall;
+      p1 *= kSmall;
+    } else if (ap < kSmall && fabs(p1) < kSmall) {
+      p2 *= kBig;
+      p1 *= kBig;
+    }
+    p0 = p1;
+    p1 = p2;
+  }
+  return cnt;
+}
+
+// The k-th smallest eigenvalue (0-based) of (a, b, n) by multisection of
+// [lo, hi] (count(lo) <= k < count(hi)); all 32 lanes take part and get it.
+// At most 40 rounds (each narrows the bracket 33x; it stops once the bracket
+// is within 2 eps of its ends or stops moving).
+__device__ double warp_eigenvalue(const double* __restrict__ a, const double* __restrict__ b, int n, int k,
+                                  double lo, double hi) {
+  const int lane = threadIdx.x & 31;
+  for (int it = 0; it < 40; ++it) {
+    const double w = hi - lo;
+    if (!(w > 2.0 * DBL_EPSILON * tcore::dmax(fabs(lo), fabs(hi)))) break;
+    const double x = fma(w, (double)(lane + 1) * (1.0 / 33.0), lo);
+    const unsigned above = __ballot_sync(0xffffffffu, sturm_count(a, b, n, x) > k);
+    const int j = above ? __ffs(above) - 1 : 32;  // first point with more than k eigenvalues below
+    const double xh = __shfl_sync(0xffffffffu, x, j < 32 ? j : 31);
+    const double xl = __shfl_sync(0xffffffffu, x, j > 0 ? j - 1 : 0);
+    const double nlo = j > 0 ? xl : lo, nhi = j < 32 ? xh : hi;
+    if (nlo == lo && nhi == hi) break;
+    lo = nlo;
+    hi = nhi;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Gershgorin interval of (a, b, n), widened by a few ulps of its scale.
+__device__ void gershgorin(const double* __restrict__ a, const double* __restrict__ b, int n, double* lo,
+                           double* hi) {
+  double l = a[0], h = a[0];
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < n ? fabs(b[i]) : 0.0);
+    l = fmin(l, a[i] - r);
+    h = fmax(h, a[i] + r);
+  }
+  const double pad = 8.0 * DBL_EPSILON * tcore::dmax(fabs(l), fabs(h)) + DBL_MIN;
+  *lo = l - pad;
+  *hi = h + pad;
+}
+
+// Eigenvalues k0 .. kn-1 of (a, b, n), ascending, into out (lane 0 writes;
+// out[0..k0) hold the lower ones already); each bracket starts just below
+// the previous value.
+__device__ void warp_lowest(const double* __restrict__ a, const double* __restrict__ b, int n, int k0, int kn,
+                            double glo, double ghi, double* out) {
+  const double margin = 8.0 * DBL_EPSILON * tcore::dmax(fabs(glo), fabs(ghi));
+  double lo = k0 > 0 ? __shfl_sync(0xffffffffu, out[k0 - 1], 0) - margin : glo;
+  for (int k = k0; k < kn; ++k) {
+    const double e = warp_eigenvalue(a, b, n, k, lo, ghi);
+    if ((threadIdx.x & 31) == 0) out[k] = e;
+    lo = e - margin;
+  }
+}
+
+// One value of the walk: its first index in the sorted spectrum, its
+// multiplicity and the index whose eigenvector's last component gives its
+// error (-1: a multiple value, error 0).
+struct WalkItem {
+  double value;
+  int first, mult, zidx;
+};
+
+// tcore::analyze_walk over the prefixes ev[0..nt) of T's sorted spectrum and
+// evg[0..ng) of the reduced T's, top = T's largest eigenvalue.  Returns the
+// number of values written to items (at most cap), or -1 when the walk needs
+// an eigenvalue past a prefix.
+__device__ int walk_prefix(int n, double alpha_max, double beta_max, const double* ev, int nt, double top,
+                           const double* evg, int ng, int cap, double thold_rel, WalkItem* items, double* thold_out,
+                           double* multol_out) {
+  const double eps = DBL_EPSILON;
+  const double error_tol = pow(eps, 2.0 / 3.0);
+  const double multol = tcore::dmax(alpha_max, beta_max) * 2 * eps * (10000 + n);
+  double thold = tcore::dmax(error_tol * tcore::dmax(ev[0], top), 5 * multol);
+  if (thold_rel > 0.0) thold = tcore::dmax(thold, thold_rel * tcore::dmax(fabs(ev[0]), fabs(top)));
+  *thold_out = thold;
+  *multol_out = multol;
+  int t2 = 0, out = 0, i0 = 0;
+  while (i0 < n && out < cap) {
+    if (i0 >= nt) return -1;
+    const double temp = ev[i0];
+    int i1 = i0 + 1;
+    while (i1 < n) {
+      if (i1 >= nt) return -1;
+      if ((ev[i1] - temp) > thold) break;
+      ++i1;
+    }
+    int mult = i1 - i0;
+    if (mult == 1) {
+      for (int j = t2; j < n - 2; ++j, ++t2) {
+        if (j >= ng) return -1;
+        if ((evg[j] - temp) >= multol) break;
+        if (fabs(temp - evg[j]) < multol) {
+          mult = 0;
+          ++t2;
+          break;
+        }
+      }
+    }
+    if (mult != 0) items[out++] = {temp, i0, mult, mult == 1 ? i1 - 1 : -1};
+    i0 = i1;
+  }
+  return out;
+}
+
 // End of a graph launch: T-matrix analysis of every stepping instance and the
-// phase rules.  Two threads per instance: the eigenvalue sweeps of T and of T
-// without its first row and column run side by side (tcore::analyze_t /
-// analyze_t2, the bulk of the work), then the first thread finishes.
+// phase rules, one warp per instance.  The lowest want + 4 eigenvalues of T
+// and want + 5 of the reduced T, and T's largest, by warp multisection; the
+// walk over them on lane 0; the error estimates' eigenvector components by
+// inverse iteration, eight lanes at a time.  A walk that needs more of the
+// spectrum (many ghost copies) falls back to the QL sweeps of tmatrix_core.h
+// (lanes 0 and 1: T and the reduced T side by side).
 __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = g >> 1, lane = g & 1;
-  const unsigned pair = 3u << (threadIdx.x & 30);  // the two threads of this instance
-  if (s >= *a.n_inst) return;  // both threads of a pair leave together
+  const int s = blockIdx.x;
+  const int lane = threadIdx.x & 31;
+  if (s >= *a.n_inst) return;  // the whole warp leaves together
   BInst& I = a.inst[s];
   if (I.phase != kPhLow && I.phase != kPhHigh) return;
   const int m = I.j;  // alpha_0 .. alpha_{j-1} are final
@@ -206,32 +353,91 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
   const int cap = I.cap;
   double* al = I.scratch;
   double* be = al + cap;
-  double* work = be + cap;      // 5 cap + 2
+  double* work = be + cap;         // 5 cap + 2: sorted spectrum of T (prefix and top), reduced T's
   double* z = work + 5 * cap + 2;  // cap
-  double* inv = z + cap;         // 6 cap
-  if (lane == 0)
-    for (int q = 0; q < m; ++q) {
-      al[q] = I.ab[2 * q];
-      be[q] = I.ab[2 * q + 1];
-    }
-  __syncwarp(pair);
-  const int info = lane == 0 ? tcore::analyze_t(m, al, be, work) : tcore::analyze_t2(m, al, be, work);
-  const int info2 = __shfl_xor_sync(pair, info, 1);
-  if (lane != 0) return;
+  double* inv = z + cap;           // 6 cap
+  double* zz = I.scratch + 16 * cap;  // kCheckLanes x 7 cap: the lanes' inverse iterations
+  for (int q = lane; q < m; q += 32) {
+    al[q] = I.ab[2 * q];
+    be[q] = I.ab[2 * q + 1];
+  }
+  __syncwarp();
   double amax = I.ab[0], bmax = I.ab[1];
   for (int q = 0; q < m; ++q) {
     amax = tcore::dmax(amax, al[q]);
     bmax = tcore::dmax(bmax, be[q]);
   }
   const int nev = I.nev;
+  const int want = nev + 1;
+  const double thold_rel = I.phase == kPhLow ? kFp32MergeRel : 0.0;
+  double* evt = work;              // T's sorted spectrum (prefix), its largest at work[m - 1]
+  double* evg = work + 3 * cap + 1;  // the reduced T's (prefix)
+  double glo, ghi, glo2, ghi2;
+  gershgorin(al, be, m, &glo, &ghi);
+  gershgorin(al + 1, be + 1, m - 1, &glo2, &ghi2);
+  const double top = warp_eigenvalue(al, be, m, m - 1, glo, ghi);
+  __shared__ WalkItem items[AED_MAX_NEV + 1];
+  __shared__ double zlast[kCheckLanes];
+  __shared__ int n_items;
+  __shared__ double walk_thold, walk_multol;
+  // prefixes of want + 4 and want + 5 values, grown (up to three times) while
+  // the walk needs more; the largest of T stays apart at work[m - 1]
+  int nt = m < want + 4 ? m : want + 4, ng = m - 1 < want + 5 ? m - 1 : want + 5, pt = 0, pg = 0;
+  for (int round = 0; round < 4; ++round) {
+    warp_lowest(al, be, m, pt, nt, glo, ghi, evt);
+    warp_lowest(al + 1, be + 1, m - 1, pg, ng, glo2, ghi2, evg);
+    __syncwarp();
+    if (lane == 0)
+      n_items = walk_prefix(m, amax, bmax, evt, nt, top, evg, ng, want, thold_rel, items, &walk_thold, &walk_multol);
+    __syncwarp();
+    if (n_items >= 0) break;
+    pt = nt;
+    pg = ng;
+    nt = 2 * nt + 4 < m ? 2 * nt + 4 : m;
+    ng = 2 * ng + 4 < m - 1 ? 2 * ng + 4 : m - 1;
+  }
+  if (lane == 0) evt[m - 1] = top;
+  __syncwarp();
   double ev[AED_MAX_NEV + 1], er[AED_MAX_NEV + 1];
   int first[AED_MAX_NEV + 1], mults[AED_MAX_NEV + 1];
   tcore::TResult res;
   res.count = 0;
-  const int want = nev + 1;
-  const bool bad = info != 0 || info2 != 0 ||
-                   tcore::analyze_walk(m, be, amax, bmax, work, want, ev, er, mults, first, &res,
-                                       I.phase == kPhLow ? kFp32MergeRel : 0.0) != 0;
+  bool bad = false;
+  if (n_items >= 0) {
+    // error estimates |beta_m z_{m,i}| of the simple values, eight lanes at a time
+    const double bl = be[m - 1];
+    for (int r0 = 0; r0 < n_items; r0 += kCheckLanes) {
+      const int r = r0 + lane;
+      if (lane < kCheckLanes && r < n_items && items[r].zidx >= 0) {
+        double* zr = zz + (size_t)lane * 7 * cap;
+        tcore::inverse_iteration(m, al, be, evt[items[r].zidx], zr, zr + cap);
+        zlast[lane] = zr[m - 1];
+      }
+      __syncwarp();
+      if (lane == 0)
+        for (int q = r0; q < n_items && q < r0 + kCheckLanes; ++q)
+          er[q] = items[q].zidx >= 0 ? fabs(bl * zlast[q - r0]) : 0.0;
+      __syncwarp();
+    }
+    if (lane != 0) return;
+    for (int q = 0; q < n_items; ++q) {
+      ev[q] = items[q].value;
+      mults[q] = items[q].mult;
+      first[q] = items[q].first;
+    }
+    res.count = n_items;
+    res.thold = walk_thold;
+    res.multol = walk_multol;
+  } else {
+    // fallback: the full QL sweeps (T on lane 0, the reduced T on lane 1)
+    int info = 0;
+    if (lane == 0) info = tcore::analyze_t(m, al, be, work);
+    if (lane == 1) info = tcore::analyze_t2(m, al, be, work);
+    const int info2 = __shfl_sync(0xffffffffu, info, 1);
+    if (lane != 0) return;
+    bad = info != 0 || info2 != 0 ||
+          tcore::analyze_walk(m, be, amax, bmax, work, want, ev, er, mults, first, &res, thold_rel) != 0;
+  }
   const int cnt = res.count;
   bool conv = !bad && cnt >= nev;
   if (I.phase == kPhLow) {
@@ -253,6 +459,14 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
     }
     if (K == 0) I.coef[0] = 1.0;
     for (int i = 0; i < n1; ++i) I.evals_low[i] = ev[i];
+    // lower bound on the eigenvalue above the nev lowest: the next distinct
+    // value less its error estimate and the FP32 resolution (work[0..m): the
+    // sorted eigenvalues of T)
+    I.next_lo = -1e300;
+    if (!bad && cnt > nev) {
+      const double scale = tcore::dmax(fabs(work[0]), fabs(work[m - 1]));
+      I.next_lo = ev[nev] - tcore::dmax(er[nev], kFp32MergeRel * fabs(ev[nev])) - kFp32MergeRel * scale;
+    }
     I.m_low = m;
     I.phase = kPhRitz;
   } else {
@@ -265,6 +479,17 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
       const double gap = ev[i + 1] - ev[i];
       if (!(gap > 0.0) || !(er[i] * er[i] / gap <= I.etol * fabs(ev[i]))) energy = false;
     }
+    // block Kato-Temple against the FP32 phase's bound on the next eigenvalue
+    bool block = conv && I.etol > 0.0 && I.next_lo > -1e299;
+    if (block) {
+      double r2 = 0.0;
+      for (int i = 0; i < nev; ++i) r2 += er[i] * er[i];
+      const double gap = I.next_lo - ev[nev - 1];
+      block = gap > 0.0;
+      for (int i = 0; block && i < nev; ++i)
+        if (!(r2 / gap <= kBatchBlockTol * fabs(ev[i]))) block = false;
+    }
+    energy = energy || block;
     const bool full = !stepping(I);
     if (!(ietl || energy || full || bad)) return;
     const int n = cnt < nev ? cnt : nev;
@@ -493,7 +718,7 @@ int batch_record_step(const BatchArgs& a, const int* choice32, cudaStream_t st) 
 int batch_record_check(const BatchArgs& a, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
-  b_check<<<(2 * ni + 31) / 32, 32, 0, st>>>(a);
+  b_check<<<ni, 32, 0, st>>>(a);
   b_ritz<<<gchunk, kRedThreads, 0, st>>>(a);
   b_ritz_norm<<<ni, 256, 0, st>>>(a);
   b_ritz_scale<<<gchunk, kRedThreads, 0, st>>>(a);

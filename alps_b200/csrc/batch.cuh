@@ -43,6 +43,7 @@ struct BInst {
   int64_t ldv;        // stride of stored FP32 vectors (elements)
   double tol32;       // FP32 phase: residual estimate <= tol32 * |lambda|
   double etol;        // FP64 phase: r^2 / gap <= etol * |lambda| (0: ietl rule only)
+  double next_lo;     // mixed: the FP32 phase's lower bound on the eigenvalue above the nev lowest (-1e300: none)
   double rtol, atol;  // ietl rule
   uint64_t seed;      // the request's seed (start vector, Ritz weights)
   float* chunk[kBatchMaxChunks];
@@ -50,7 +51,7 @@ struct BInst {
   double* partA;      // n_tiles
   double* partB;      // n_chunks
   double* ab;         // 2 * cap: alpha_j, beta_j of the current phase
-  double* scratch;    // 12 * cap doubles for the T-matrix analysis
+  double* scratch;    // kCheckScratch * cap doubles for the T-matrix analysis
   double* coef;       // cap: Ritz coefficients
   // dynamic
   int32_t phase;
@@ -64,6 +65,17 @@ struct BInst {
   double errs[AED_MAX_NEV];
   double evals_low[AED_MAX_NEV];
 };
+
+// Mixed FP64 phase, block Kato-Temple stop: sum_i r_i^2 / (next_lo - theta_max)
+// <= kBatchBlockTol |theta_i| over the nev lowest Ritz pairs of the FP64 T,
+// next_lo from the FP32 phase (the single-instance Rayleigh-Ritz acceptance).
+constexpr double kBatchBlockTol = 2.5e-10;
+
+// Per-instance T-matrix scratch of the check, in doubles per step of capacity:
+// alpha, beta, the spectra and one inverse iteration (16), and kCheckLanes
+// lanes' inverse iterations (7 each).
+constexpr int kCheckLanes = 8;
+constexpr int kCheckScratch = 16 + 7 * kCheckLanes;
 
 struct BItem {
   int32_t inst;

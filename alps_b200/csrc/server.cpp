@@ -142,7 +142,7 @@ size_t request_bytes(const aed_server* s, int N, int64_t D, int nev, int cap, in
   b += 3 * (((size_t)D * 8 + 255) & ~(size_t)255);  // FP64 vectors
   if (s->precision == AED_FP32) b += ldv * (size_t)((n_store + kStoreChunkB - 1) / kStoreChunkB) * kStoreChunkB;
   b += (size_t)sector_tiles_est(D) * 8 + (size_t)red_chunks(D) * 8;  // partials
-  b += (size_t)cap * 8 * (2 + 16 + 1);                               // alpha/beta, scratch, coefficients
+  b += (size_t)cap * 8 * (2 + kCheckScratch + 1);                               // alpha/beta, scratch, coefficients
   b += sizeof(HvParams) + 4096;
   b += (size_t)40 * ((size_t)1 << ((N + 1) / 2)) * 4;  // lo-neighbour table (width <= 40)
   (void)nev;
@@ -259,7 +259,7 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
     if ((rc = take((void**)&I.v64[q], (size_t)D * 8))) return rc;
   if ((rc = take((void**)&I.partA, (size_t)sec->n_tiles * 8 + 8)) ||
       (rc = take((void**)&I.partB, (size_t)red_chunks(D) * 8 + 8)) || (rc = take((void**)&I.ab, (size_t)cap * 16)) ||
-      (rc = take((void**)&I.scratch, (size_t)cap * 16 * 8 + 64)) || (rc = take((void**)&I.coef, (size_t)cap * 8)))
+      (rc = take((void**)&I.scratch, (size_t)cap * kCheckScratch * 8 + 64)) || (rc = take((void**)&I.coef, (size_t)cap * 8)))
     return rc;
   const size_t vb = ((size_t)D * 4 + 255) & ~(size_t)255;
   I.ldv = (int64_t)(vb / 4);
@@ -311,6 +311,7 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
   I.atol = r->opts.atol > 0 ? r->opts.atol : 100 * eps;
   I.tol32 = 2e-6;
   I.etol = s->precision == AED_FP32 ? 1e-11 : 0.0;
+  I.next_lo = -1e300;
   I.j = 0;
   // start vector, normalised (lanczos.h:381-383)
   double* nrm = I.scratch;
