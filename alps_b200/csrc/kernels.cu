@@ -198,6 +198,48 @@ __global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const doubl
   }
 }
 
+// The update with alpha's finishing sum folded in: every CTA sums the
+// apply's tile partials itself (the order of finish_sum, so the same alpha to
+// the bit) and CTA 0 stores it.  For sectors with few tiles, where this saves
+// a launch per step.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) lanczos_update_fin_kernel(
+    const double* __restrict__ alpha_part, int64_t n_apart, double* __restrict__ alpha_out, const T* __restrict__ x,
+    const T* __restrict__ vprev, const double* __restrict__ beta_prev, T* __restrict__ y, int64_t n,
+    double* __restrict__ partB) {
+  __shared__ double sm[33];
+  const double alpha = finish_sum_in_cta<kRedThreads>(alpha_part, n_apart, sm);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *alpha_out = alpha;
+  const double b = vprev ? *beta_prev : 0.0;
+  const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
+    double acc = 0.0;
+    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+      double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
+      if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
+      const T wt = (T)w;
+      y[i] = wt;
+      acc = fma((double)wt, (double)wt, acc);
+    }
+    const double tot = block_sum_all<kRedThreads>(acc, sm);
+    if (threadIdx.x == 0) partB[c] = tot;
+  }
+}
+
+// The normalisation with beta's finishing sum folded in (as above).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) lanczos_normalize_fin_kernel(const double* __restrict__ beta_part,
+                                                                           int64_t n_bpart,
+                                                                           double* __restrict__ beta_out,
+                                                                           T* __restrict__ y, int64_t n) {
+  __shared__ double sm[33];
+  const double beta = sqrt(finish_sum_in_cta<kRedThreads>(beta_part, n_bpart, sm));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *beta_out = beta;
+  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
+    y[i] = (T)__ddiv_rn((double)y[i], beta);
+}
+
 // make_step tail (lanczos.h:402): w /= b
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const double* __restrict__ beta_p,
@@ -553,6 +595,23 @@ int launch_lanczos_update(const double* alpha, const T* x, const T* vprev, const
 }
 
 template <typename T>
+int launch_lanczos_update_fin(const double* alpha_part, int64_t n_apart, double* alpha, const T* x, const T* vprev,
+                              const double* beta_prev, T* y, int64_t n, double* partB, cudaStream_t st) {
+  const int64_t nch = red_chunks(n);
+  const int grid = (int)(nch < (int64_t)num_sms() * 8 ? nch : (int64_t)num_sms() * 8);
+  lanczos_update_fin_kernel<T><<<grid < 1 ? 1 : grid, kRedThreads, 0, st>>>(alpha_part, n_apart, alpha, x, vprev,
+                                                                           beta_prev, y, n, partB);
+  return check_launch("lanczos_update_fin_kernel");
+}
+
+template <typename T>
+int launch_lanczos_normalize_fin(const double* beta_part, int64_t n_bpart, double* beta, T* y, int64_t n,
+                                 cudaStream_t st) {
+  lanczos_normalize_fin_kernel<T><<<elem_grid(n), kRedThreads, 0, st>>>(beta_part, n_bpart, beta, y, n);
+  return check_launch("lanczos_normalize_fin_kernel");
+}
+
+template <typename T>
 int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t st) {
   lanczos_normalize_kernel<T><<<elem_grid(n), kRedThreads, 0, st>>>(beta, y, n);
   return check_launch("lanczos_normalize_kernel");
@@ -566,7 +625,10 @@ int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t s
   template int launch_dot_partials<T>(const T*, const T*, int64_t, double*, bool, cudaStream_t);             \
   template int launch_lanczos_update<T>(const double*, const T*, const T*, const double*, T*, int64_t,      \
                                         double*, cudaStream_t);                                              \
-  template int launch_lanczos_normalize<T>(const double*, T*, int64_t, cudaStream_t);
+  template int launch_lanczos_normalize<T>(const double*, T*, int64_t, cudaStream_t);                          \
+  template int launch_lanczos_update_fin<T>(const double*, int64_t, double*, const T*, const T*, const double*, T*, \
+                                            int64_t, double*, cudaStream_t);                                      \
+  template int launch_lanczos_normalize_fin<T>(const double*, int64_t, double*, T*, int64_t, cudaStream_t);
 AED_INST(double)
 AED_INST(float)
 #undef AED_INST

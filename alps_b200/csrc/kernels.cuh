@@ -92,6 +92,17 @@ int launch_lanczos_update(const double* alpha, const T* x, const T* vprev, const
                           int64_t n, double* partB, cudaStream_t st);
 template <typename T>
 int launch_lanczos_normalize(const double* beta, T* y, int64_t n, cudaStream_t st);
+// The same two kernels with the finishing sums of alpha (the apply's tile
+// partials) and beta (the update's chunk partials) done inside every CTA, in
+// finish_sum's order: the same alpha and beta to the bit and two launches
+// fewer per step; for short partial lists (kFoldFinishMax).
+constexpr int64_t kFoldFinishMax = 2048;
+template <typename T>
+int launch_lanczos_update_fin(const double* alpha_part, int64_t n_apart, double* alpha, const T* x, const T* vprev,
+                              const double* beta_prev, T* y, int64_t n, double* partB, cudaStream_t st);
+template <typename T>
+int launch_lanczos_normalize_fin(const double* beta_part, int64_t n_bpart, double* beta, T* y, int64_t n,
+                                 cudaStream_t st);
 
 // out[i] = sum_j coef[j] * V[j*ld + i] (FP32 Lanczos store -> FP64 vector),
 // coef in device memory (m <= kMaxRitzTerms).

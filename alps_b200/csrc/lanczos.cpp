@@ -157,6 +157,27 @@ double diag_of_state(const HvParams& P, uint32_t s) {
 int lanczos_step_tail(aed_handle* h, bool f32, const void* vprev, const void* x, void* y, const double* beta_prev,
                       double* alpha, double* beta) {
   const int64_t D = h->vlen;
+  const int64_t na = h->alpha_tiles(), nb = red_chunks(D);
+  // AED_FOLD_FINISH=0 keeps the separate finishing kernels (a test compares
+  // the two paths bit for bit)
+  static const bool fold = [] {
+    const char* e = std::getenv("AED_FOLD_FINISH");
+    return !(e && e[0] == '0');
+  }();
+  if (fold && na <= kFoldFinishMax && nb <= kFoldFinishMax) {
+    // short partial lists: the finishing sums inside the update and the
+    // normalisation (same alpha and beta to the bit, two launches fewer)
+    int rc;
+    if (f32)
+      rc = launch_lanczos_update_fin(h->d_partA, na, alpha, (const float*)x, (const float*)vprev, beta_prev,
+                                     (float*)y, D, h->d_partB, h->stream);
+    else
+      rc = launch_lanczos_update_fin(h->d_partA, na, alpha, (const double*)x, (const double*)vprev, beta_prev,
+                                     (double*)y, D, h->d_partB, h->stream);
+    if (rc) return rc;
+    if (f32) return launch_lanczos_normalize_fin(h->d_partB, nb, beta, (float*)y, D, h->stream);
+    return launch_lanczos_normalize_fin(h->d_partB, nb, beta, (double*)y, D, h->stream);
+  }
   int rc = launch_finish_sum(h->d_partA, h->alpha_tiles(), alpha, false, h->stream);
   if (rc) return rc;
   if (f32)

@@ -66,4 +66,35 @@ __device__ __forceinline__ void finish_sum(const double* __restrict__ part, int6
   if (threadIdx.x == 0) *out = take_sqrt ? sqrt(tot) : tot;
 }
 
+// The total finish_sum forms, computed by any CTA of NT threads (NT a
+// multiple of 32 dividing kFinishThreads) and returned to every thread: real
+// warp r plays the kFinishThreads / NT virtual warps r, r + NT/32, ...; each
+// virtual thread sums its strided share and each virtual warp its shuffle
+// tree exactly as in finish_sum, so the result is bit-identical.  For short
+// partial lists, where every CTA of a kernel can afford to read them all.
+template <int NT>
+__device__ __forceinline__ double finish_sum_in_cta(const double* __restrict__ part, int64_t n, double* sm) {
+  static_assert(NT % 32 == 0 && kFinishThreads % NT == 0, "block size");
+  constexpr int kVirt = kFinishThreads / NT;  // virtual warps per real warp
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int q = 0; q < kVirt; ++q) {
+    const int vw = w + q * (NT / 32);  // virtual warp
+    const int vt = vw * 32 + l;        // virtual thread of finish_sum
+    double v = 0.0;
+    for (int64_t i = vt; i < n; i += kFinishThreads) v += part[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (l == 0) sm[vw] = v;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double r = sm[l];  // kFinishThreads / 32 = 32 virtual warp sums
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    if (l == 0) sm[32] = r;
+  }
+  __syncthreads();
+  const double r = sm[32];
+  __syncthreads();
+  return r;
+}
+
 }  // namespace aed
