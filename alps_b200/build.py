@@ -27,7 +27,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-para
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "batch.cu", "momentum.cu", "measure.cu", "spin.cu", "refine.cu"]
 CPP_SOURCES = ["model.cpp", "tmatrix.cpp", "api.cpp", "lanczos.cpp", "server.cpp"]
-HEADERS = ["aed_internal.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "apply_blocks.cuh", "apply_stream.cuh",
+HEADERS = ["aed_internal.h", "rr_core.h", "kernels.cuh", "handle.h", "reduce.cuh", "apply.cuh", "apply_blocks.cuh", "apply_stream.cuh",
            "tmatrix_core.h",
            "batch.cuh", "momentum.cuh", "spin.cuh"]
 

@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "handle.h"
+#include "rr_core.h"
 #include "tmatrix_core.h"
 
 namespace aed {
@@ -564,64 +565,15 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
 constexpr double kRefineEnergyTol = 1e-11;
 
 // Rayleigh-Ritz acceptance: every reported value's error bound below
-// kRRTol * |theta|, 4x inside the 1e-9 relative agreement (the bound is
+// kRRTol * |theta|, 2x inside the 1e-9 relative agreement (the bound is
 // rigorous: the FP64 values lie within it).
-constexpr double kRRTol = 2.5e-10;
+constexpr double kRRTol = 5e-10;
 
 // FP32 phase stop: Ritz residual estimates below kTol32 |lambda|.  The FP64
 // Rayleigh-Ritz error bound goes with the square of the residuals, so this
 // tolerance sets how often the refinement needs no FP64 Lanczos steps.
 constexpr double kTol32 = 1e-6;
 
-// Eigen-decomposition of a symmetric n x n matrix a (row-major, destroyed) by
-// cyclic Jacobi rotations (Jacobi 1846; the threshold-free cyclic form of
-// Rutishauser, Handbook for Automatic Computation II, 1971): w ascending,
-// column k of v (v[i * n + k]) its eigenvector.  n <= kMaxRR.
-void jacobi_eigen(int n, double* a, double* w, double* v) {
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) v[i * n + j] = i == j ? 1.0 : 0.0;
-  for (int sweep = 0; sweep < 64; ++sweep) {
-    double off = 0.0, diag = 0.0;
-    for (int i = 0; i < n; ++i) {
-      diag += a[i * n + i] * a[i * n + i];
-      for (int j = i + 1; j < n; ++j) off += a[i * n + j] * a[i * n + j];
-    }
-    if (off <= 1e-34 * diag || off == 0.0) break;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = a[p * n + q];
-        if (apq == 0.0) continue;
-        // rotation angle that zeroes a_pq: tan(phi) = t, the smaller root of t^2 + 2 theta t - 1 = 0
-        const double theta = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < n; ++k) {  // columns p, q
-          const double akp = a[k * n + p], akq = a[k * n + q];
-          a[k * n + p] = c * akp - s * akq;
-          a[k * n + q] = s * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {  // rows p, q
-          const double apk = a[p * n + k], aqk = a[q * n + k];
-          a[p * n + k] = c * apk - s * aqk;
-          a[q * n + k] = s * apk + c * aqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double vkp = v[k * n + p], vkq = v[k * n + q];
-          v[k * n + p] = c * vkp - s * vkq;
-          v[k * n + q] = s * vkp + c * vkq;
-        }
-      }
-  }
-  std::vector<int> ord(n);
-  for (int i = 0; i < n; ++i) ord[i] = i;
-  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return a[x * n + x] < a[y * n + y]; });
-  std::vector<double> vs((size_t)n * n);
-  for (int k = 0; k < n; ++k) {
-    w[k] = a[ord[k] * n + ord[k]];
-    for (int i = 0; i < n; ++i) vs[i * n + k] = v[i * n + ord[k]];
-  }
-  std::copy(vs.begin(), vs.end(), v);
-}
 
 // The mixed path's FP64 Rayleigh-Ritz refinement.  The K Ritz vectors of
 // T(m1) that span the nev lowest clusters (tcore::ritz_span: ghost copies and
@@ -646,7 +598,7 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   const int64_t D = h->vlen;
   const int c = std::min(nev, (int)T1.evals.size());
   if (c < 1 || (int)T1.evals.size() <= c) return AED_OK;  // no value above the clusters to bound the gap
-  const int K = tcore::ritz_span((int)T1.evals.size(), nev, T1.first.data(), T1.mults.data(), m1);
+  const int K = tcore::ritz_span((int)T1.evals.size(), c, T1.first.data(), T1.mults.data(), m1);
   const bool verbose = std::getenv("AED_VERBOSE") != nullptr;
   if (K < 1 || K > kMaxRR) {
     if (verbose) std::fprintf(stderr, "[aed] rayleigh-ritz: %d Ritz vectors span the clusters (at most %d)\n", K, kMaxRR);
@@ -696,61 +648,15 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
     for (int b = a; b < K; ++b, ++p) G[a * K + b] = G[b * K + a] = hout[p];
   for (int a = 0; a < K; ++a)
     for (int b = 0; b < K; ++b, ++p) A[a * K + b] = hout[p];
+  // Ritz pairs of the pencil, values as Rayleigh quotients (rr_core.h)
+  double th[kMaxRR], cr[kMaxRR][kMaxRR];
+  int ord[kMaxRR];
+  const int Kp = rrcore::ritz_pairs(K, G, A, th, cr, ord);
+  if (Kp < 1) return AED_OK;
   for (int a = 0; a < K; ++a)
     for (int b = a + 1; b < K; ++b) A[a * K + b] = A[b * K + a] = 0.5 * (A[a * K + b] + A[b * K + a]);
-  // orthonormal basis of span(Psi): B = Q_kept diag(g)^{-1/2}
-  double g[kMaxRR], Q[kMaxRR * kMaxRR], Gc[kMaxRR * kMaxRR];
-  std::copy(G, G + K * K, Gc);
-  jacobi_eigen(K, Gc, g, Q);
-  const double gmax = g[K - 1];
-  if (!(gmax > 0)) return AED_OK;
-  double B[kMaxRR * kMaxRR];
-  int Kp = 0;
-  for (int k = K - 1; k >= 0; --k) {
-    if (!(g[k] > 1e-10 * gmax)) continue;
-    const double s = 1.0 / std::sqrt(g[k]);
-    for (int i = 0; i < K; ++i) B[i * K + Kp] = Q[i * K + k] * s;
-    ++Kp;
-  }
-  // C = B^T A B (Kp x Kp)
-  double AB[kMaxRR * kMaxRR], C[kMaxRR * kMaxRR], th[kMaxRR], Y[kMaxRR * kMaxRR];
-  for (int i = 0; i < K; ++i)
-    for (int j = 0; j < Kp; ++j) {
-      double s = 0.0;
-      for (int k = 0; k < K; ++k) s += A[i * K + k] * B[k * K + j];
-      AB[i * K + j] = s;
-    }
-  for (int i = 0; i < Kp; ++i)
-    for (int j = 0; j < Kp; ++j) {
-      double s = 0.0;
-      for (int k = 0; k < K; ++k) s += B[k * K + i] * AB[k * K + j];
-      C[i * Kp + j] = s;
-    }
-  for (int i = 0; i < Kp; ++i)
-    for (int j = i + 1; j < Kp; ++j) C[i * Kp + j] = C[j * Kp + i] = 0.5 * (C[i * Kp + j] + C[j * Kp + i]);
-  jacobi_eigen(Kp, C, th, Y);
-  // coefficients over Psi of the Ritz pairs: c_r = B y_r; each value is then
-  // taken as the Rayleigh quotient c^T A c / c^T G c of its own vector, which
-  // rounding in an ill-conditioned B cannot move (a ghost copy of a
-  // converged vector leaves a nearly dependent pair in Psi)
-  double cr[kMaxRR][kMaxRR];
   std::vector<std::pair<double, int>> byval;
-  for (int q = 0; q < Kp; ++q) {
-    for (int k = 0; k < K; ++k) {
-      double s = 0.0;
-      for (int j = 0; j < Kp; ++j) s += B[k * K + j] * Y[j * Kp + q];
-      cr[q][k] = s;
-    }
-    double num = 0.0, den = 0.0;
-    for (int a = 0; a < K; ++a)
-      for (int b = 0; b < K; ++b) {
-        num += cr[q][a] * A[a * K + b] * cr[q][b];
-        den += cr[q][a] * G[a * K + b] * cr[q][b];
-      }
-    th[q] = den > 0 ? num / den : th[q];
-    byval.push_back({th[q], q});
-  }
-  std::sort(byval.begin(), byval.end());
+  for (int i = 0; i < Kp; ++i) byval.push_back({th[ord[i]], ord[i]});
   // lowest eigenvalue outside the Ritz pairs that are bounded, from below: the
   // FP32 phase's next distinct value less its error estimate and its FP32
   // resolution.  Only the pairs below it are bounded (block Kato-Temple over
