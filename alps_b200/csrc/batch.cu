@@ -22,6 +22,7 @@
 #include "apply_blocks.cuh"
 #include "batch.cuh"
 #include "reduce.cuh"
+#include "rr_core.h"
 #include "tmatrix_core.h"
 
 namespace aed {
@@ -452,10 +453,15 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
     const int n1 = cnt < nev ? cnt : nev;
     for (int q = 0; q < m; ++q) I.coef[q] = 0.0;
     const int K = bad ? 0 : tcore::ritz_span(cnt, nev, first, mults, m);
+    // the Rayleigh-Ritz step needs a value above the clusters (the gap) and
+    // room for its K vectors
+    const bool rr = !bad && K > 0 && K <= I.rr_kmax && cnt > nev;
     for (int k = 0; k < K; ++k) {
       tcore::inverse_iteration(m, al, be, work[k], z, inv);
       const double w = tcore::ritz_weight(I.seed, k);
       for (int q = 0; q < m; ++q) I.coef[q] += w * z[q];
+      if (rr)
+        for (int q = 0; q < m; ++q) I.rr_coef[(size_t)k * cap + q] = z[q];
     }
     if (K == 0) I.coef[0] = 1.0;
     for (int i = 0; i < n1; ++i) I.evals_low[i] = ev[i];
@@ -468,7 +474,11 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
       I.next_lo = ev[nev] - tcore::dmax(er[nev], kFp32MergeRel * fabs(ev[nev])) - kFp32MergeRel * scale;
     }
     I.m_low = m;
-    I.phase = kPhRitz;
+    I.rr_k = rr ? K : 0;
+    I.rr_need = cnt < nev ? cnt : nev;
+    I.rr_scale = tcore::dmax(fabs(work[0]), fabs(work[m - 1]));
+    I.rr_done = 0;
+    I.phase = rr && I.next_lo > -1e299 ? kPhRR : kPhRitz;
   } else {
     if (m < nev + 2) conv = false;
     bool ietl = conv;
@@ -502,6 +512,298 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
     I.converged = (ietl || energy) ? 1 : 0;
     I.phase = kPhDone;
   }
+}
+
+// ---- Rayleigh-Ritz hand-over of the mixed path (phase kPhRR) -----------------
+// The single-instance refinement of lanczos.cpp (rayleigh_ritz) for every
+// request whose FP32 phase ended at this graph launch: the K Ritz vectors of
+// T that span its nev lowest clusters are formed in FP64 from the stored
+// basis, H is applied to each (the FP64 bundle apply), the Gram matrices
+// Psi^T Psi and Psi^T H Psi are summed per chunk and finished per request,
+// one thread per request solves the K x K pencil (rr_core.h), the residuals
+// of the pairs below the FP32 phase's gap bound are summed, and the block
+// Kato-Temple bound sum |r|^2 / (next_lo - theta_max) decides: at most
+// kBatchBlockTol |theta| for every reported value and the result is taken
+// (K FP64 applies instead of 16-24 FP64 Lanczos steps); otherwise the request
+// goes on to the FP64 Lanczos refinement (phase kPhRitz, below).  Every sum
+// has a fixed order, so a request's result does not depend on the batch.
+
+__device__ __forceinline__ double* rr_psi(const BInst& I, int k) { return I.rr_v + (size_t)k * I.D; }
+__device__ __forceinline__ double* rr_img(const BInst& I, int k) { return I.rr_v + (size_t)(I.rr_kmax + k) * I.D; }
+
+// Psi_k = sum_j coef_k[j] v_j over the stored FP32 basis (FP64, ascending j).
+__global__ void __launch_bounds__(kRedThreads) b_rr_combine(BatchArgs a) {
+  __shared__ double cs[kStoreChunkB * kMaxRR];
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRR) continue;
+    const int K = I.rr_k, m = I.m_low;
+    const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+    for (int64_t i0 = e0; i0 < e1; i0 += kRedThreads) {
+      const int64_t i = i0 + threadIdx.x;
+      double acc[kMaxRR];
+#pragma unroll
+      for (int k = 0; k < kMaxRR; ++k) acc[k] = 0.0;
+      for (int j0 = 0; j0 < m; j0 += kStoreChunkB) {
+        const int cnt = m - j0 < kStoreChunkB ? m - j0 : kStoreChunkB;
+        __syncthreads();
+        for (int q = threadIdx.x; q < cnt * K; q += kRedThreads)
+          cs[q] = I.rr_coef[(size_t)(q % K) * I.cap + j0 + q / K];  // cs[jj * K + k]
+        __syncthreads();
+        if (i < e1)
+          for (int jj = 0; jj < cnt; ++jj) {
+            const double v = (double)low_vec(I, j0 + jj)[i];
+#pragma unroll
+            for (int k = 0; k < kMaxRR; ++k)
+              if (k < K) acc[k] = fma(cs[jj * K + k], v, acc[k]);
+          }
+      }
+      if (i < e1)
+        for (int k = 0; k < K; ++k) rr_psi(I, k)[i] = acc[k];
+    }
+  }
+}
+
+// H Psi_k for k < K over the request's (bundle) items: the FP64 bundle apply.
+__global__ void __launch_bounds__(kHvThreads, 3) b_rr_apply(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char b_dyn[];
+  __shared__ bapply::BundleSmem<1> sm;
+  const int n = *a.n_tiles;
+  int cur = -1, rc = 0;
+  double* xs = nullptr;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.tiles[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRR) continue;
+    if (w.inst != cur) {
+      __syncthreads();
+      xs = bapply::carve<double, 1>(*I.P, I.t, b_dyn, sm);
+      bapply::stage_pairs<1>(*I.P, sm);
+      cur = w.inst;
+    }
+    const ApplyCtx c = apply::ctx_of(*I.P);
+    for (int k = 0; k < I.rr_k; ++k)
+      for (int q = 0; q < kBatchBundle; ++q)
+        bapply::apply_bundle<double, AccExact64, 4, 1>(c, I.t, (int64_t)w.idx * kBatchBundle + q, rr_psi(I, k),
+                                                       rr_img(I, k), nullptr, sm, xs, rc);
+  }
+}
+
+// Chunk partials of the Gram matrices: G(a, b), a <= b, then A(a, b) =
+// <Psi_a, H Psi_b>, at part[p * n_chunks + chunk].
+template <int K>
+__device__ __forceinline__ void rr_gram_chunk(const BInst& I, int64_t c, double* red) {
+  constexpr int NP = K * (K + 1) / 2 + K * K;
+  const int64_t e0 = c * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+  double acc[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) acc[p] = 0.0;
+  for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+    double x[K], y[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      x[k] = rr_psi(I, k)[i];
+      y[k] = rr_img(I, k)[i];
+    }
+    int p = 0;
+#pragma unroll
+    for (int u = 0; u < K; ++u)
+#pragma unroll
+      for (int v = u; v < K; ++v) {
+        acc[p] = fma(x[u], x[v], acc[p]);
+        ++p;
+      }
+#pragma unroll
+    for (int u = 0; u < K; ++u)
+#pragma unroll
+      for (int v = 0; v < K; ++v) {
+        acc[p] = fma(x[u], y[v], acc[p]);
+        ++p;
+      }
+  }
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const double tot = block_sum_all<kRedThreads>(acc[p], red);
+    if (threadIdx.x == 0) I.rr_part[(size_t)p * I.n_chunks + c] = tot;
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) b_rr_gram(BatchArgs a) {
+  __shared__ double red[33];
+  const int n = *a.n_chunks;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRR) continue;
+    switch (I.rr_k) {
+      case 1: rr_gram_chunk<1>(I, w.idx, red); break;
+      case 2: rr_gram_chunk<2>(I, w.idx, red); break;
+      case 3: rr_gram_chunk<3>(I, w.idx, red); break;
+      case 4: rr_gram_chunk<4>(I, w.idx, red); break;
+      case 5: rr_gram_chunk<5>(I, w.idx, red); break;
+      case 6: rr_gram_chunk<6>(I, w.idx, red); break;
+      case 7: rr_gram_chunk<7>(I, w.idx, red); break;
+      case 8: rr_gram_chunk<8>(I, w.idx, red); break;
+      default: break;
+    }
+  }
+}
+
+// rr_small[p] = the request's sum of partial p over its chunks (finish_sum's
+// order), for p < np (np: the Gram entries, or the bounded pairs' residuals).
+__global__ void __launch_bounds__(256) b_rr_finish(BatchArgs a, int residuals) {
+  __shared__ double red[33];
+  if ((int)blockIdx.x >= *a.n_inst) return;
+  const BInst& I = a.inst[blockIdx.x];
+  if (I.phase != kPhRR) return;
+  const int K = I.rr_k;
+  const int np = residuals ? I.rr_nb : K * (K + 1) / 2 + K * K;
+  for (int p = 0; p < np; ++p) {
+    const double tot = finish_sum_in_cta<256>(I.rr_part + (size_t)p * I.n_chunks, I.n_chunks, red);
+    if (threadIdx.x == 0) I.rr_small[p] = tot;
+  }
+}
+
+// One thread per request: the Ritz pairs of the pencil, the pairs below the
+// gap bound and their residual coefficients.
+__global__ void b_rr_solve(BatchArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *a.n_inst) return;
+  BInst& I = a.inst[s];
+  if (I.phase != kPhRR) return;
+  const int K = I.rr_k;
+  double G[kMaxRR * kMaxRR], A[kMaxRR * kMaxRR];
+  const double* sum = I.rr_small;
+  int p = 0;
+  for (int u = 0; u < K; ++u)
+    for (int v = u; v < K; ++v, ++p) G[u * K + v] = G[v * K + u] = sum[p];
+  for (int u = 0; u < K; ++u)
+    for (int v = 0; v < K; ++v, ++p) A[u * K + v] = sum[p];
+  double th[kMaxRR], cr[kMaxRR][kMaxRR];
+  int ord[kMaxRR];
+  const int Kp = rrcore::ritz_pairs(K, G, A, th, cr, ord);
+  int nb = 0;
+  while (nb < Kp && th[ord[nb]] < I.next_lo) ++nb;
+  if (nb < 1) {
+    I.phase = kPhRitz;
+    return;
+  }
+  double* sm = I.rr_small;
+  for (int i = 0; i < nb; ++i) {
+    const int q = ord[i];
+    sm[100 + i] = th[q];
+    for (int k = 0; k < kMaxRR; ++k) {
+      sm[116 + i * kMaxRR + k] = k < K ? cr[q][k] : 0.0;
+      sm[180 + i * kMaxRR + k] = k < K ? -th[q] * cr[q][k] : 0.0;
+    }
+    sm[244 + i] = rrcore::form(K, G, cr[q], cr[q]);
+  }
+  I.rr_nb = nb;
+}
+
+// Chunk partials of |sum_k cw[r][k] H Psi_k + cx[r][k] Psi_k|^2 for r < nb.
+template <int K>
+__device__ __forceinline__ void rr_resid_chunk(const BInst& I, int64_t c, double* red, const double* cw,
+                                               const double* cx) {
+  const int nb = I.rr_nb;
+  const int64_t e0 = c * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
+  double acc[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) acc[r] = 0.0;
+  for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+    double x[K], y[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      x[k] = rr_psi(I, k)[i];
+      y[k] = rr_img(I, k)[i];
+    }
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      if (r < nb) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) t = fma(cw[r * kMaxRR + k], y[k], fma(cx[r * kMaxRR + k], x[k], t));
+        acc[r] = fma(t, t, acc[r]);
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    if (r < nb) {
+      const double tot = block_sum_all<kRedThreads>(acc[r], red);
+      if (threadIdx.x == 0) I.rr_part[(size_t)r * I.n_chunks + c] = tot;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) b_rr_resid(BatchArgs a) {
+  __shared__ double red[33];
+  __shared__ double cw[kMaxRR * kMaxRR], cx[kMaxRR * kMaxRR];
+  const int n = *a.n_chunks;
+  int cur = -1;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const BItem w = a.chunks[it];
+    const BInst& I = a.inst[w.inst];
+    if (I.phase != kPhRR) continue;
+    if (w.inst != cur) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < kMaxRR * kMaxRR; q += kRedThreads) {
+        cw[q] = I.rr_small[116 + q];
+        cx[q] = I.rr_small[180 + q];
+      }
+      __syncthreads();
+      cur = w.inst;
+    }
+    switch (I.rr_k) {
+      case 1: rr_resid_chunk<1>(I, w.idx, red, cw, cx); break;
+      case 2: rr_resid_chunk<2>(I, w.idx, red, cw, cx); break;
+      case 3: rr_resid_chunk<3>(I, w.idx, red, cw, cx); break;
+      case 4: rr_resid_chunk<4>(I, w.idx, red, cw, cx); break;
+      case 5: rr_resid_chunk<5>(I, w.idx, red, cw, cx); break;
+      case 6: rr_resid_chunk<6>(I, w.idx, red, cw, cx); break;
+      case 7: rr_resid_chunk<7>(I, w.idx, red, cw, cx); break;
+      case 8: rr_resid_chunk<8>(I, w.idx, red, cw, cx); break;
+      default: break;
+    }
+  }
+}
+
+// One thread per request: the block Kato-Temple bound and the verdict.
+__global__ void b_rr_accept(BatchArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= *a.n_inst) return;
+  BInst& I = a.inst[s];
+  if (I.phase != kPhRR) return;
+  const double* sm = I.rr_small;
+  const int nb = I.rr_nb;
+  double rn2 = 0.0;
+  for (int i = 0; i < nb; ++i) rn2 += sm[244 + i] > 0.0 ? sm[i] / sm[244 + i] : sm[i];
+  const double gap = I.next_lo - sm[100 + nb - 1];
+  const double bound = rn2 / gap;
+  // distinct values: merged below the FP64 T-matrix threshold eps^(2/3) max|lambda| (tmatrix.h:148-150)
+  const double thold = pow(DBL_EPSILON, 2.0 / 3.0) * I.rr_scale;
+  double vals[AED_MAX_NEV];
+  int n = 0;
+  for (int i = 0; i < nb && n < I.nev; ++i)
+    if (n == 0 || sm[100 + i] - vals[n - 1] > thold) vals[n++] = sm[100 + i];
+  bool ok = gap > 0.0 && n >= I.rr_need;
+  for (int i = 0; ok && i < n; ++i)
+    if (!(bound <= kBatchBlockTol * fabs(vals[i]))) ok = false;
+  if (!ok) {
+    I.phase = kPhRitz;  // on to the FP64 Lanczos refinement
+    return;
+  }
+  for (int i = 0; i < n; ++i) {
+    I.evals[i] = vals[i];
+    I.errs[i] = bound;
+  }
+  I.n_evals = n;
+  I.iters = I.rr_k;  // the FP64 applies of the refinement
+  I.converged = 1;
+  I.rr_done = 1;
+  I.phase = kPhDone;
 }
 
 // FP64 start of the refinement: v = sum_q coef[q] v_q (stored FP32 basis),
@@ -603,6 +905,7 @@ const Cand32 kCand32[kBatchCand32] = {
 };
 int g_c32[kBatchCand32] = {}, g_c32_smem[kBatchCand32] = {-1, -1, -1, -1, -1};
 int g_hv64 = 0, g_hv64_smem = -1;
+int g_rr = 0, g_rr_smem = -1;
 
 // Grid of an apply kernel for `smem` bytes of dynamic shared memory (cached per size).
 template <typename K>
@@ -649,6 +952,7 @@ size_t batch_hv_smem_limit() {
 int batch_prepare(const BatchArgs& a) {
   for (int c = 0; c < kBatchCand32; ++c) hv_grid(kCand32[c].kern, a.hv_smem, &g_c32[c], &g_c32_smem[c]);
   hv_grid(b_hv64, a.hv_smem, &g_hv64, &g_hv64_smem);
+  hv_grid(b_rr_apply, a.hv_smem, &g_rr, &g_rr_smem);
   return check("batched apply attributes");
 }
 
@@ -719,6 +1023,14 @@ int batch_record_check(const BatchArgs& a, cudaStream_t st) {
   const int ni = a.max_inst;
   const int gchunk = sms() * 8;
   b_check<<<ni, 32, 0, st>>>(a);
+  b_rr_combine<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_rr_apply<<<hv_grid(b_rr_apply, a.hv_smem, &g_rr, &g_rr_smem), kHvThreads, a.hv_smem, st>>>(a);
+  b_rr_gram<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_rr_finish<<<ni, 256, 0, st>>>(a, 0);
+  b_rr_solve<<<(ni + 127) / 128, 128, 0, st>>>(a);
+  b_rr_resid<<<gchunk, kRedThreads, 0, st>>>(a);
+  b_rr_finish<<<ni, 256, 0, st>>>(a, 1);
+  b_rr_accept<<<(ni + 127) / 128, 128, 0, st>>>(a);
   b_ritz<<<gchunk, kRedThreads, 0, st>>>(a);
   b_ritz_norm<<<ni, 256, 0, st>>>(a);
   b_ritz_scale<<<gchunk, kRedThreads, 0, st>>>(a);

@@ -28,7 +28,15 @@ enum : int32_t {
   kPhRitz = 2,   // FP32 phase done: Ritz vectors being assembled into the FP64 start
   kPhHigh = 3,   // FP64 Lanczos recurrence (refinement, or the whole solve in FP64 mode)
   kPhDone = 4,   // results ready
+  kPhRR = 5,     // FP32 phase done: the Rayleigh-Ritz step on its Ritz vectors, in FP64
 };
+
+// Rayleigh-Ritz hand-over of the batched mixed path: chunk sums of the Gram
+// matrices (K (K + 1) / 2 + K^2 for K <= kMaxRR) and the per-request small
+// arrays: sums [0, 100), values [100, 108), value order [108, 116), residual
+// coefficients cw [116, 180) and cx [180, 244), squared norms [244, 252).
+constexpr int kRRSums = kMaxRR * (kMaxRR + 1) / 2 + kMaxRR * kMaxRR;
+constexpr int kRRSmall = 256;
 
 struct BInst {
   // set at admission
@@ -61,6 +69,17 @@ struct BInst {
   int32_t iters;      // FP64 phase T size at the end
   int32_t converged;
   double ritz_norm;
+  // Rayleigh-Ritz hand-over (mixed servers; rr_kmax = 0: none)
+  int32_t rr_kmax;    // Ritz vectors budgeted at admission
+  int32_t rr_k;       // Ritz vectors of this hand-over
+  int32_t rr_nb;      // Ritz pairs below the gap bound
+  int32_t rr_need;    // distinct values it must resolve
+  int32_t rr_done;    // 1: the result is the Rayleigh-Ritz step's
+  double rr_scale;    // largest |eigenvalue| of the FP32 phase's T (merge threshold)
+  double* rr_v;       // 2 rr_kmax D doubles: Psi_k at k D, H Psi_k at (rr_kmax + k) D
+  double* rr_coef;    // rr_kmax cap: coefficients of the Ritz vectors over the stored basis
+  double* rr_part;    // kRRSums n_chunks chunk partials
+  double* rr_small;   // kRRSmall doubles
   double evals[AED_MAX_NEV];
   double errs[AED_MAX_NEV];
   double evals_low[AED_MAX_NEV];
@@ -69,7 +88,7 @@ struct BInst {
 // Mixed FP64 phase, block Kato-Temple stop: sum_i r_i^2 / (next_lo - theta_max)
 // <= kBatchBlockTol |theta_i| over the nev lowest Ritz pairs of the FP64 T,
 // next_lo from the FP32 phase (the single-instance Rayleigh-Ritz acceptance).
-constexpr double kBatchBlockTol = 2.5e-10;
+constexpr double kBatchBlockTol = 5e-10;
 
 // Per-instance T-matrix scratch of the check, in doubles per step of capacity:
 // alpha, beta, the spectra and one inverse iteration (16), and kCheckLanes

@@ -135,6 +135,11 @@ int dmalloc(aed_server* s, void** p, size_t bytes) {
   return AED_OK;
 }
 
+// Ritz vectors a request's Rayleigh-Ritz hand-over may use (the clusters of
+// its nev lowest values with a few ghost copies); more falls back to the
+// FP64 Lanczos refinement.
+int rr_kmax_of(int nev) { return std::min(kMaxRR, nev + 3); }
+
 // Bytes a request holds while resident (the admission footprint).
 size_t request_bytes(const aed_server* s, int N, int64_t D, int nev, int cap, int n_store) {
   const size_t ldv = ((size_t)D * 4 + 255) & ~(size_t)255;
@@ -145,7 +150,11 @@ size_t request_bytes(const aed_server* s, int N, int64_t D, int nev, int cap, in
   b += (size_t)cap * 8 * (2 + kCheckScratch + 1);                               // alpha/beta, scratch, coefficients
   b += sizeof(HvParams) + 4096;
   b += (size_t)40 * ((size_t)1 << ((N + 1) / 2)) * 4;  // lo-neighbour table (width <= 40)
-  (void)nev;
+  if (s->precision == AED_FP32) {  // the Rayleigh-Ritz hand-over: K vectors and their images, sums
+    const size_t k = (size_t)rr_kmax_of(nev);
+    b += 2 * k * (((size_t)D * 8 + 255) & ~(size_t)255) + k * (size_t)cap * 8 +
+         (size_t)kRRSums * (size_t)red_chunks(D) * 8 + (size_t)kRRSmall * 8;
+  }
   return b;
 }
 
@@ -261,6 +270,20 @@ int admit(aed_server* s, int k, const std::shared_ptr<Request>& r) {
       (rc = take((void**)&I.partB, (size_t)red_chunks(D) * 8 + 8)) || (rc = take((void**)&I.ab, (size_t)cap * 16)) ||
       (rc = take((void**)&I.scratch, (size_t)cap * kCheckScratch * 8 + 64)) || (rc = take((void**)&I.coef, (size_t)cap * 8)))
     return rc;
+  I.rr_kmax = 0;
+  I.rr_k = 0;
+  I.rr_done = 0;
+  if (s->precision == AED_FP32) {
+    const int k = rr_kmax_of(r->opts.nev);
+    const size_t vd = ((size_t)D * 8 + 255) & ~(size_t)255;
+    void* pv = nullptr;
+    if ((rc = take(&pv, 2 * (size_t)k * vd)) || (rc = take((void**)&I.rr_coef, (size_t)k * cap * 8)) ||
+        (rc = take((void**)&I.rr_part, (size_t)kRRSums * (size_t)red_chunks(D) * 8 + 8)) ||
+        (rc = take((void**)&I.rr_small, (size_t)kRRSmall * 8)))
+      return rc;
+    I.rr_v = (double*)pv;
+    I.rr_kmax = k;
+  }
   const size_t vb = ((size_t)D * 4 + 255) & ~(size_t)255;
   I.ldv = (int64_t)(vb / 4);
   for (int c = 0; c * kStoreChunkB < n_store; ++c)
@@ -514,8 +537,10 @@ void finish_request(aed_server* s, int k) {
   r.res.iterations = I.iters;
   r.res.iterations_low = s->precision == AED_FP32 ? I.m_low : 0;
   r.res.converged = I.converged;
-  // the batched mixed path refines with FP64 Lanczos steps
-  r.res.refined_by = s->precision == AED_FP32 ? AED_REFINE_LANCZOS : AED_REFINE_NONE;
+  // the batched mixed path refines by the Rayleigh-Ritz step or FP64 Lanczos steps
+  r.res.refined_by = s->precision != AED_FP32 ? AED_REFINE_NONE
+                     : I.rr_done           ? AED_REFINE_RAYLEIGH_RITZ
+                                           : AED_REFINE_LANCZOS;
   for (int i = 0; i < I.n_evals && i < AED_MAX_NEV; ++i) {
     r.res.evals[i] = I.evals[i];
     r.res.errors[i] = I.errs[i];
