@@ -94,6 +94,29 @@ def test_batch_matches_oracle(prec, tol):
     srv.close()
 
 
+def test_batched_rayleigh_ritz_hand_over_bounds_hold():
+    """Mixed batch: requests whose FP32 phase ends go through the batched Rayleigh-Ritz step first.  Most
+    take its result (refined_by 'rayleigh_ritz', K FP64 applies); every value lies above the oracle's by at
+    most its reported bound (the block Kato-Temple bound of the step) and within 1e-9; the others took the
+    FP64 Lanczos refinement."""
+    reqs = mixed_requests(99, 16)
+    srv = ed.Server(precision=ed.FP32, max_slots=32, steps=8)
+    tickets = [srv.submit(n, n // 2, b, nev=nev, seed=sd) for n, b, nev, sd in reqs]
+    res = srv.run(tickets)
+    kinds = [res[t]["refined_by"] for t in tickets]
+    assert kinds.count("rayleigh_ritz") >= len(tickets) // 2, kinds
+    assert set(kinds) <= {"rayleigh_ritz", "lanczos"}
+    for t, (n, b, nev, sd) in zip(tickets, reqs):
+        r = res[t]
+        o = oracle.Matrix(n, n // 2, [tuple(x) + (0.0,) for x in b]).lanczos(nev=nev, seed=sd)
+        assert len(r["evals"]) == len(o["evals"])
+        assert np.all(np.abs(r["evals"] - o["evals"]) <= 1e-9 * np.abs(o["evals"]))
+        if r["refined_by"] == "rayleigh_ritz":
+            assert r["iterations"] <= 8  # the FP64 applies of the step
+            assert np.all(r["evals"] - o["evals"] <= r["errors"] + 1e-12 * np.abs(o["evals"]))
+    srv.close()
+
+
 def test_batched_apply_candidates_give_the_same_results(monkeypatch):
     """The autotuner of the batched engine picks one of several FP32 apply kernels per sector-size bucket
     (rows per thread, CTAs per SM, hi blocks per pass); each adds every row's terms in the same order, so
