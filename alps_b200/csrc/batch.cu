@@ -201,9 +201,10 @@ __global__ void b_advance(BatchArgs a) {
 // each reported simple value, the last component of its eigenvector (the
 // error estimate).  A QL sweep over the whole spectrum costs O(m^2) serial
 // plane rotations on one thread (9.6 ms for the longest T of a served batch);
-// here 32 lanes bracket one eigenvalue at a time by Sturm counts at 32
-// points (multisection, 33x narrower per round), O(m) per count, and the
-// eigenvector components come from inverse iteration, one lane each.
+// here each lane bisects one of the low eigenvalues by Sturm counts, O(m)
+// per count, the largest is bracketed by all 32 lanes at once (multisection,
+// 33x narrower per round), and the eigenvector components come from inverse
+// iteration, one lane each.
 
 // Number of eigenvalues below x of the symmetric tridiagonal matrix with
 // diagonal a[0..n) and off-diagonal b[0..n-1): sign changes of the leading
@@ -272,17 +273,33 @@ __device__ void gershgorin(const double* __restrict__ a, const double* __restric
   *hi = h + pad;
 }
 
-// Eigenvalues k0 .. kn-1 of (a, b, n), ascending, into out (lane 0 writes;
-// out[0..k0) hold the lower ones already); each bracket starts just below
-// the previous value.
+// Eigenvalues k0 .. kn-1 of (a, b, n), ascending, into out: lane i bisects
+// eigenvalue k0 + 32 g + i of group g on its own (count(x) > k: the upper
+// half), so a group of 32 values costs the rounds of one (about 55 Sturm
+// counts at full precision; at most 80).  Ghost-rich FP32 T-matrices need
+// tens of values before the walk has nev + 1 distinct ones.
 __device__ void warp_lowest(const double* __restrict__ a, const double* __restrict__ b, int n, int k0, int kn,
                             double glo, double ghi, double* out) {
-  const double margin = 8.0 * DBL_EPSILON * tcore::dmax(fabs(glo), fabs(ghi));
-  double lo = k0 > 0 ? __shfl_sync(0xffffffffu, out[k0 - 1], 0) - margin : glo;
-  for (int k = k0; k < kn; ++k) {
-    const double e = warp_eigenvalue(a, b, n, k, lo, ghi);
-    if ((threadIdx.x & 31) == 0) out[k] = e;
-    lo = e - margin;
+  const int lane = threadIdx.x & 31;
+  for (int g0 = k0; g0 < kn; g0 += 32) {
+    const int k = g0 + lane;
+    bool done = k >= kn;
+    double lo = glo, hi = ghi;
+    for (int it = 0; it < 80; ++it) {
+      if (__all_sync(0xffffffffu, done)) break;
+      if (!done) {
+        const double w = hi - lo;
+        const double x = lo + 0.5 * w;
+        if (!(w > 2.0 * DBL_EPSILON * tcore::dmax(fabs(lo), fabs(hi))) || x == lo || x == hi) {
+          done = true;
+        } else if (sturm_count(a, b, n, x) > k) {
+          hi = x;
+        } else {
+          lo = x;
+        }
+      }
+    }
+    if (k < kn) out[k] = 0.5 * (lo + hi);
   }
 }
 
@@ -338,7 +355,7 @@ __device__ int walk_prefix(int n, double alpha_max, double beta_max, const doubl
 
 // End of a graph launch: T-matrix analysis of every stepping instance and the
 // phase rules, one warp per instance.  The lowest want + 4 eigenvalues of T
-// and want + 5 of the reduced T, and T's largest, by warp multisection; the
+// and want + 5 of the reduced T (a lane per value) and T's largest; the
 // walk over them on lane 0; the error estimates' eigenvector components by
 // inverse iteration, eight lanes at a time.  A walk that needs more of the
 // spectrum (many ghost copies) falls back to the QL sweeps of tmatrix_core.h
