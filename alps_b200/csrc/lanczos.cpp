@@ -339,6 +339,11 @@ int normalize(aed_handle* h, T* v, int64_t D) {
   return rc;
 }
 
+// Rayleigh-Ritz acceptance: every reported value's error bound below
+// kRRTol * |theta|, 2x inside the 1e-9 relative agreement (the bound is
+// rigorous: the FP64 values lie within it).
+constexpr double kRRTol = 5e-10;
+
 // Stopping rule of one recurrence.
 struct StopRule {
   int nev;
@@ -346,9 +351,21 @@ struct StopRule {
   bool energy_bound;    // mixed refinement: err_i^2 / gap_i <= etol |lambda_i|
   double etol;
   int min_steps;
+  // mixed refinement, block Kato-Temple stop: sum_i err_i^2 / (next_lo -
+  // lambda_{nev-1}) <= block_tol |lambda_i|, next_lo a lower bound on the
+  // eigenvalue above the nev lowest from the FP32 phase (block_tol 0: off)
+  double next_lo = -1e300, block_tol = 0.0;
   bool done(const TmatInfo& t, int m) const {
     if (m < min_steps) return false;
     if (nlowest_converged(t, nev, rtol, atol)) return true;
+    if (block_tol > 0.0 && (int)t.evals.size() >= nev && next_lo > t.evals[nev - 1]) {
+      double r2 = 0.0;
+      for (int i = 0; i < nev; ++i) r2 += t.errs[i] * t.errs[i];
+      bool ok = true;
+      for (int i = 0; ok && i < nev; ++i)
+        ok = r2 / (next_lo - t.evals[nev - 1]) <= block_tol * std::fabs(t.evals[i]);
+      if (ok) return true;
+    }
     if (!energy_bound || (int)t.evals.size() < nev + 1) return false;
     for (int i = 0; i < nev; ++i) {
       const double gap = t.evals[i + 1] - t.evals[i];
@@ -503,7 +520,7 @@ int start_vector(aed_handle* h, const double* start_host, const double* start_de
 // (lanczos.h:77-78) after a load (lanczos.h:86-98).
 int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev, uint64_t seed, int nev,
                int max_iter, double rtol, double atol, bool energy_bound, double etol, int min_steps, bool profile,
-               aed_solve_result* r, TmatInfo& T, bool resume = false) {
+               aed_solve_result* r, TmatInfo& T, bool resume = false, double next_lo = -1e300) {
   const int64_t D = h->vlen;
   EventRing ring;
   int rc;
@@ -537,6 +554,10 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
     return rc;
   }
   StopRule stop{nev, rtol, atol, energy_bound, etol, min_steps};
+  if (energy_bound && next_lo > -1e299) {
+    stop.next_lo = next_lo;
+    stop.block_tol = kRRTol;
+  }
   int iters = 0, failed = 0;
   rc = run_recurrence(R, stop, [&](int j) { return buf[j % nr]; }, m0, &iters, &failed, T);
   if (rc) return rc;
@@ -564,10 +585,6 @@ int solve_fp64(aed_handle* h, const double* start_host, const double* start_dev,
 // energy agreement the mixed path promises.
 constexpr double kRefineEnergyTol = 1e-11;
 
-// Rayleigh-Ritz acceptance: every reported value's error bound below
-// kRRTol * |theta|, 2x inside the 1e-9 relative agreement (the bound is
-// rigorous: the FP64 values lie within it).
-constexpr double kRRTol = 5e-10;
 
 // FP32 phase stop: Ritz residual estimates below kTol32 |lambda|.  The FP64
 // Rayleigh-Ritz error bound goes with the square of the residuals, so this
@@ -839,7 +856,19 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   // phase 2: FP64 refinement from the Ritz combination
   TmatInfo T2;
   const int max2 = std::max(max_iter, nev + 4);
-  rc = solve_fp64(h, nullptr, start64, seed, nev, max2, rtol, atol, true, kRefineEnergyTol, nev + 2, false, r, T2);
+  // the FP32 phase's lower bound on the eigenvalue above the nev lowest (as
+  // in rayleigh_ritz) for the block Kato-Temple stop of the refinement
+  double next_lo = -1e300;
+  {
+    const int c = std::min(nev, (int)T1.evals.size());
+    if (c >= 1 && (int)T1.evals.size() > c) {
+      const double nx = T1.evals[c];
+      next_lo = nx - std::max(T1.errs[c], kFp32MergeRel * std::fabs(nx)) -
+                kFp32MergeRel * std::max(std::fabs(T1.evals.front()), std::fabs(T1.evals.back()));
+    }
+  }
+  rc = solve_fp64(h, nullptr, start64, seed, nev, max2, rtol, atol, true, kRefineEnergyTol, nev + 2, false, r, T2,
+                  false, next_lo);
   h->last_mixed = true;
   // apply_ms of a mixed solve: the FP32 applies (the bulk of the work)
   if (profile) r->apply_ms = apply32_ms;
