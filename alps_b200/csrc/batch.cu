@@ -206,36 +206,6 @@ __global__ void b_advance(BatchArgs a) {
 // 33x narrower per round), and the eigenvector components come from inverse
 // iteration, one lane each.
 
-// Number of eigenvalues below x of the symmetric tridiagonal matrix with
-// diagonal a[0..n) and off-diagonal b[0..n-1): sign changes of the leading
-// principal minors det(T_k - x) (Sturm), by the three-term recurrence kept
-// in range by power-of-two rescaling.  A zero minor counts as a change (the
-// pivot taken as a tiny negative, as dstebz does).
-__device__ __forceinline__ int sturm_count(const double* __restrict__ a, const double* __restrict__ b, int n,
-                                           double x) {
-  constexpr double kBig = 0x1p400, kSmall = 0x1p-400, kTiny = 0x1p-800;
-  double p0 = 1.0, p1 = a[0] - x;
-  if (p1 == 0.0) p1 = -kTiny;
-  int cnt = p1 < 0.0 ? 1 : 0;
-  for (int k = 1; k < n; ++k) {
-    const double bb = b[k - 1];
-    double p2 = fma(a[k] - x, p1, -(bb * bb) * p0);
-    if (p2 == 0.0) p2 = p1 > 0.0 ? -kTiny : kTiny;
-    cnt += (p2 < 0.0) != (p1 < 0.0) ? 1 : 0;
-    const double ap = fabs(p2);
-    if (ap > kBig) {
-      p2 *= kSmall;
-      p1 *= kSmall;
-    } else if (ap < kSmall && fabs(p1) < kSmall) {
-      p2 *= kBig;
-      p1 *= kBig;
-    }
-    p0 = p1;
-    p1 = p2;
-  }
-  return cnt;
-}
-
 // The k-th smallest eigenvalue (0-based) of (a, b, n) by multisection of
 // [lo, hi] (count(lo) <= k < count(hi)); all 32 lanes take part and get it.
 // At most 40 rounds (each narrows the bracket 33x; it stops once the bracket
@@ -247,7 +217,7 @@ __device__ double warp_eigenvalue(const double* __restrict__ a, const double* __
     const double w = hi - lo;
     if (!(w > 2.0 * DBL_EPSILON * tcore::dmax(fabs(lo), fabs(hi)))) break;
     const double x = fma(w, (double)(lane + 1) * (1.0 / 33.0), lo);
-    const unsigned above = __ballot_sync(0xffffffffu, sturm_count(a, b, n, x) > k);
+    const unsigned above = __ballot_sync(0xffffffffu, tcore::sturm_count(a, b, n, x) > k);
     const int j = above ? __ffs(above) - 1 : 32;  // first point with more than k eigenvalues below
     const double xh = __shfl_sync(0xffffffffu, x, j < 32 ? j : 31);
     const double xl = __shfl_sync(0xffffffffu, x, j > 0 ? j - 1 : 0);
@@ -257,20 +227,6 @@ __device__ double warp_eigenvalue(const double* __restrict__ a, const double* __
     hi = nhi;
   }
   return 0.5 * (lo + hi);
-}
-
-// Gershgorin interval of (a, b, n), widened by a few ulps of its scale.
-__device__ void gershgorin(const double* __restrict__ a, const double* __restrict__ b, int n, double* lo,
-                           double* hi) {
-  double l = a[0], h = a[0];
-  for (int i = 0; i < n; ++i) {
-    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < n ? fabs(b[i]) : 0.0);
-    l = fmin(l, a[i] - r);
-    h = fmax(h, a[i] + r);
-  }
-  const double pad = 8.0 * DBL_EPSILON * tcore::dmax(fabs(l), fabs(h)) + DBL_MIN;
-  *lo = l - pad;
-  *hi = h + pad;
 }
 
 // Eigenvalues k0 .. kn-1 of (a, b, n), ascending, into out: lane i bisects
@@ -292,7 +248,7 @@ __device__ void warp_lowest(const double* __restrict__ a, const double* __restri
         const double x = lo + 0.5 * w;
         if (!(w > 2.0 * DBL_EPSILON * tcore::dmax(fabs(lo), fabs(hi))) || x == lo || x == hi) {
           done = true;
-        } else if (sturm_count(a, b, n, x) > k) {
+        } else if (tcore::sturm_count(a, b, n, x) > k) {
           hi = x;
         } else {
           lo = x;
@@ -301,56 +257,6 @@ __device__ void warp_lowest(const double* __restrict__ a, const double* __restri
     }
     if (k < kn) out[k] = 0.5 * (lo + hi);
   }
-}
-
-// One value of the walk: its first index in the sorted spectrum, its
-// multiplicity and the index whose eigenvector's last component gives its
-// error (-1: a multiple value, error 0).
-struct WalkItem {
-  double value;
-  int first, mult, zidx;
-};
-
-// tcore::analyze_walk over the prefixes ev[0..nt) of T's sorted spectrum and
-// evg[0..ng) of the reduced T's, top = T's largest eigenvalue.  Returns the
-// number of values written to items (at most cap), or -1 when the walk needs
-// an eigenvalue past a prefix.
-__device__ int walk_prefix(int n, double alpha_max, double beta_max, const double* ev, int nt, double top,
-                           const double* evg, int ng, int cap, double thold_rel, WalkItem* items, double* thold_out,
-                           double* multol_out) {
-  const double eps = DBL_EPSILON;
-  const double error_tol = pow(eps, 2.0 / 3.0);
-  const double multol = tcore::dmax(alpha_max, beta_max) * 2 * eps * (10000 + n);
-  double thold = tcore::dmax(error_tol * tcore::dmax(ev[0], top), 5 * multol);
-  if (thold_rel > 0.0) thold = tcore::dmax(thold, thold_rel * tcore::dmax(fabs(ev[0]), fabs(top)));
-  *thold_out = thold;
-  *multol_out = multol;
-  int t2 = 0, out = 0, i0 = 0;
-  while (i0 < n && out < cap) {
-    if (i0 >= nt) return -1;
-    const double temp = ev[i0];
-    int i1 = i0 + 1;
-    while (i1 < n) {
-      if (i1 >= nt) return -1;
-      if ((ev[i1] - temp) > thold) break;
-      ++i1;
-    }
-    int mult = i1 - i0;
-    if (mult == 1) {
-      for (int j = t2; j < n - 2; ++j, ++t2) {
-        if (j >= ng) return -1;
-        if ((evg[j] - temp) >= multol) break;
-        if (fabs(temp - evg[j]) < multol) {
-          mult = 0;
-          ++t2;
-          break;
-        }
-      }
-    }
-    if (mult != 0) items[out++] = {temp, i0, mult, mult == 1 ? i1 - 1 : -1};
-    i0 = i1;
-  }
-  return out;
 }
 
 // End of a graph launch: T-matrix analysis of every stepping instance and the
@@ -391,10 +297,10 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
   double* evt = work;              // T's sorted spectrum (prefix), its largest at work[m - 1]
   double* evg = work + 3 * cap + 1;  // the reduced T's (prefix)
   double glo, ghi, glo2, ghi2;
-  gershgorin(al, be, m, &glo, &ghi);
-  gershgorin(al + 1, be + 1, m - 1, &glo2, &ghi2);
+  tcore::gershgorin(al, be, m, &glo, &ghi);
+  tcore::gershgorin(al + 1, be + 1, m - 1, &glo2, &ghi2);
   const double top = warp_eigenvalue(al, be, m, m - 1, glo, ghi);
-  __shared__ WalkItem items[AED_MAX_NEV + 1];
+  __shared__ tcore::WalkItem items[AED_MAX_NEV + 1];
   __shared__ double zlast[kCheckLanes];
   __shared__ int n_items;
   __shared__ double walk_thold, walk_multol;
@@ -406,7 +312,7 @@ __global__ void __launch_bounds__(32) b_check(BatchArgs a) {
     warp_lowest(al + 1, be + 1, m - 1, pg, ng, glo2, ghi2, evg);
     __syncwarp();
     if (lane == 0)
-      n_items = walk_prefix(m, amax, bmax, evt, nt, top, evg, ng, want, thold_rel, items, &walk_thold, &walk_multol);
+      n_items = tcore::walk_prefix(m, amax, bmax, evt, nt, top, evg, ng, want, thold_rel, items, &walk_thold, &walk_multol);
     __syncwarp();
     if (n_items >= 0) break;
     pt = nt;

@@ -337,5 +337,114 @@ AED_HD inline void inverse_iteration(int n, const double* alpha, const double* b
   }
 }
 
+// Number of eigenvalues below x of the symmetric tridiagonal matrix with
+// diagonal a[0..n) and off-diagonal b[0..n-1): sign changes of the leading
+// principal minors det(T_k - x) (Sturm), by the three-term recurrence kept
+// in range by power-of-two rescaling.  A zero minor counts as a change (the
+// pivot taken as a tiny negative, as dstebz does).
+AED_HD inline int sturm_count(const double* __restrict__ a, const double* __restrict__ b, int n,
+                                           double x) {
+  constexpr double kBig = 0x1p400, kSmall = 0x1p-400, kTiny = 0x1p-800;
+  double p0 = 1.0, p1 = a[0] - x;
+  if (p1 == 0.0) p1 = -kTiny;
+  int cnt = p1 < 0.0 ? 1 : 0;
+  for (int k = 1; k < n; ++k) {
+    const double bb = b[k - 1];
+    double p2 = fma(a[k] - x, p1, -(bb * bb) * p0);
+    if (p2 == 0.0) p2 = p1 > 0.0 ? -kTiny : kTiny;
+    cnt += (p2 < 0.0) != (p1 < 0.0) ? 1 : 0;
+    const double ap = fabs(p2);
+    if (ap > kBig) {
+      p2 *= kSmall;
+      p1 *= kSmall;
+    } else if (ap < kSmall && fabs(p1) < kSmall) {
+      p2 *= kBig;
+      p1 *= kBig;
+    }
+    p0 = p1;
+    p1 = p2;
+  }
+  return cnt;
+}
+
+// Gershgorin interval of (a, b, n), widened by a few ulps of its scale.
+AED_HD inline void gershgorin(const double* __restrict__ a, const double* __restrict__ b, int n, double* lo,
+                           double* hi) {
+  double l = a[0], h = a[0];
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < n ? fabs(b[i]) : 0.0);
+    l = fmin(l, a[i] - r);
+    h = fmax(h, a[i] + r);
+  }
+  const double pad = 8.0 * DBL_EPSILON * dmax(fabs(l), fabs(h)) + DBL_MIN;
+  *lo = l - pad;
+  *hi = h + pad;
+}
+
+// The k-th smallest eigenvalue (0-based) of (a, b, n) by bisection of
+// [lo, hi] (count(lo) <= k < count(hi)): the rule of the batched check's
+// lanes (one value per lane), for a host to reproduce.
+AED_HD inline double bisect_eigenvalue(const double* a, const double* b, int n, int k, double lo, double hi) {
+  for (int it = 0; it < 80; ++it) {
+    const double w = hi - lo, x = lo + 0.5 * w;
+    if (!(w > 2.0 * DBL_EPSILON * dmax(fabs(lo), fabs(hi))) || x == lo || x == hi) break;
+    if (sturm_count(a, b, n, x) > k)
+      hi = x;
+    else
+      lo = x;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// One value of the walk: its first index in the sorted spectrum, its
+// multiplicity and the index whose eigenvector's last component gives its
+// error (-1: a multiple value, error 0).
+struct WalkItem {
+  double value;
+  int first, mult, zidx;
+};
+
+// tcore::analyze_walk over the prefixes ev[0..nt) of T's sorted spectrum and
+// evg[0..ng) of the reduced T's, top = T's largest eigenvalue.  Returns the
+// number of values written to items (at most cap), or -1 when the walk needs
+// an eigenvalue past a prefix.
+AED_HD inline int walk_prefix(int n, double alpha_max, double beta_max, const double* ev, int nt, double top,
+                           const double* evg, int ng, int cap, double thold_rel, WalkItem* items, double* thold_out,
+                           double* multol_out) {
+  const double eps = DBL_EPSILON;
+  const double error_tol = pow(eps, 2.0 / 3.0);
+  const double multol = dmax(alpha_max, beta_max) * 2 * eps * (10000 + n);
+  double thold = dmax(error_tol * dmax(ev[0], top), 5 * multol);
+  if (thold_rel > 0.0) thold = dmax(thold, thold_rel * dmax(fabs(ev[0]), fabs(top)));
+  *thold_out = thold;
+  *multol_out = multol;
+  int t2 = 0, out = 0, i0 = 0;
+  while (i0 < n && out < cap) {
+    if (i0 >= nt) return -1;
+    const double temp = ev[i0];
+    int i1 = i0 + 1;
+    while (i1 < n) {
+      if (i1 >= nt) return -1;
+      if ((ev[i1] - temp) > thold) break;
+      ++i1;
+    }
+    int mult = i1 - i0;
+    if (mult == 1) {
+      for (int j = t2; j < n - 2; ++j, ++t2) {
+        if (j >= ng) return -1;
+        if ((evg[j] - temp) >= multol) break;
+        if (fabs(temp - evg[j]) < multol) {
+          mult = 0;
+          ++t2;
+          break;
+        }
+      }
+    }
+    if (mult != 0) items[out++] = {temp, i0, mult, mult == 1 ? i1 - 1 : -1};
+    i0 = i1;
+  }
+  return out;
+}
+
 }  // namespace tcore
 }  // namespace aed
