@@ -157,45 +157,59 @@ def sz_sectors(params: dict) -> list:
     return [Fraction(k, 2) for k in range(-n * two_s, n * two_s + 1, 2)]
 
 
-def run(params: dict, precision=FP64, device=0, seed=0) -> dict:
+def run(params: dict, precision=FP64, device=0, seed=0, workers=1) -> dict:
     """Eigenvalues of every sector: {"sectors": [{"quantumnumbers": [(name, value)], "energies": array,
     "dimension": D, "iterations": m}], "ground_state_energy": E0, "energy_gap": gap}.  Momentum sectors
-    run in FP64 whatever `precision` says."""
+    run in FP64 whatever `precision` says.  workers > 1 solves that many sectors at once (each on its own
+    handle and stream, host threads; the sectors are independent, so the results and their order are those
+    of the one-by-one loop)."""
     params = dict(params)
-    sectors = []
-    sz_values = sz_sectors(params)
     momenta = lattice_momenta(params)
     req = _measure.requests(params)
     measuring = any(req.values())
     geometry = _measure.Geometry(params) if measuring else None
     label_k = bool(momenta) and not str(params.get("TOTAL_MOMENTUM", "")).strip()
-    for sz in sz_values:
+    jobs = []
+    for sz in sz_sectors(params):
         p = params if sz is None else dict(params, Sz_total=float(sz))
         mp = model_from_parameters(p)
         for k in momenta or [None]:
-            qn = [] if sz is None else [("Sz", half_integer_text(sz))]
-            if k is None:
-                ham = Hamiltonian.from_parameters(p, precision=precision, device=device)
-            else:
-                if label_k:
-                    qn.append(("TOTAL_MOMENTUM", momentum_label(k)))
-                ham = Hamiltonian(mp["n_sites"], mp["n_up"], mp["bonds"], FP64, device, mp["site_h"], mp["site_d"],
-                                  translations=lattice_translations(params, k), two_s=mp["two_s"])
-            try:
-                if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
-                    continue
-                r = ham.solve(nev=max(1, mp["nev"]), max_iter=mp["max_iter"], seed=seed)
-                sec = {"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
-                       "iterations": r["iterations"], "converged": r["converged"]}
-                if measuring and len(r["evals"]):
-                    # perform_measurements on every eigenvector (diag.h:191-314, sparsediag.h:151-159)
-                    vecs, _, _ = ham.eigenvectors(k=len(r["evals"]), seed=seed)
-                    sec["measurements"] = [_measure.measure(ham, v, params, geometry) for v in vecs]
-                    for v in vecs:
-                        v.free()
-                sectors.append(sec)
-            finally:
-                ham.close()
+            jobs.append((sz, p, mp, k))
+
+    def solve_sector(job):
+        sz, p, mp, k = job
+        qn = [] if sz is None else [("Sz", half_integer_text(sz))]
+        if k is None:
+            ham = Hamiltonian.from_parameters(p, precision=precision, device=device)
+        else:
+            if label_k:
+                qn.append(("TOTAL_MOMENTUM", momentum_label(k)))
+            ham = Hamiltonian(mp["n_sites"], mp["n_up"], mp["bonds"], FP64, device, mp["site_h"], mp["site_d"],
+                              translations=lattice_translations(params, k), two_s=mp["two_s"])
+        try:
+            if ham.dim == 0:  # empty sector: skipped, as dostep does (diag.h:114)
+                return None
+            r = ham.solve(nev=max(1, mp["nev"]), max_iter=mp["max_iter"], seed=seed)
+            sec = {"quantumnumbers": qn, "energies": np.array(r["evals"]), "dimension": ham.dim,
+                   "iterations": r["iterations"], "converged": r["converged"]}
+            if measuring and len(r["evals"]):
+                # perform_measurements on every eigenvector (diag.h:191-314, sparsediag.h:151-159)
+                vecs, _, _ = ham.eigenvectors(k=len(r["evals"]), seed=seed)
+                sec["measurements"] = [_measure.measure(ham, v, params, geometry) for v in vecs]
+                for v in vecs:
+                    v.free()
+            return sec
+        finally:
+            ham.close()
+
+    if workers > 1 and len(jobs) > 1:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=workers) as pool:
+            done = list(pool.map(solve_sector, jobs))
+    else:
+        done = [solve_sector(j) for j in jobs]
+    sectors = [sec for sec in done if sec is not None]
     e0, gap = ground_state_and_gap([s["energies"] for s in sectors])
     return {"sectors": sectors, "ground_state_energy": e0, "energy_gap": gap}
 

@@ -155,6 +155,24 @@ def test_sparsediag_loops_over_momenta():
     assert abs(res["energy_gap"] - ref["energy_gap"]) < 1e-9
 
 
+def test_sparsediag_sectors_at_once_give_the_same_results():
+    """sparsediag.run(workers=4) solves four sectors at a time on their own handles: every sector's
+    energies, dimension and iteration count, and their order, equal the one-by-one loop's (momentum
+    sectors of a chain, and the plain Sz loop of a ladder)."""
+    for p in ({"MODEL": "spin", "LATTICE": "chain lattice", "L": 12, "CONSERVED_QUANTUMNUMBERS": "Sz",
+               "NUMBER_EIGENVALUES": 2},
+              {"MODEL": "spin", "LATTICE": "ladder", "L": 6, "J0": 1.0, "J1": 0.7, "CONSERVED_QUANTUMNUMBERS": "Sz",
+               "NUMBER_EIGENVALUES": 2, "TRANSLATION_SYMMETRY": "false"}):
+        one = sparsediag.run(p)
+        many = sparsediag.run(p, workers=4)
+        assert len(one["sectors"]) == len(many["sectors"]) > 4
+        for a, b in zip(one["sectors"], many["sectors"]):
+            assert a["quantumnumbers"] == b["quantumnumbers"]
+            assert a["dimension"] == b["dimension"] and a["iterations"] == b["iterations"]
+            assert np.array_equal(a["energies"], b["energies"])
+        assert one["ground_state_energy"] == many["ground_state_energy"]
+
+
 def test_momentum_rejects_couplings_that_break_translations():
     lat, geo = "chain lattice", {"L": 8}
     n, bonds = _bonds(lat, geo, {0: (1.0, 1.0)})
