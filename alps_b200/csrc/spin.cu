@@ -135,12 +135,33 @@ void spin_set_couplings(const std::vector<int>& s1, const std::vector<int>& s2, 
     p.n_cls = 0;
     return;
   }
-  const int ntr = p.tstart[d * d];
   int first[kSpinMaxCls];
   for (int c = 0; c < p.n_cls; ++c) first[c] = p.cls[c];
+  p.pmo = 0;
   for (int c = 0; c < p.n_cls; ++c)
-    for (int e = 0; e < ntr; ++e)
-      p.cval[c][e] = p.jz[first[c]] * p.trans[e].A + p.jxy[first[c]] * p.trans[e].B + p.kq[first[c]] * p.trans[e].C;
+    for (int pr = 0; pr < d * d; ++pr) {
+      const int a = pr / d, cc = pr % d;
+      int n = 0;
+      p.pdg[c][pr] = 0.0;
+      p.pk[c][pr] = 0;
+      for (int s = 0; s < kSpinMaxOff; ++s) p.pov[c][pr][s] = 0.0;
+      for (int e = p.tstart[pr]; e < p.tstart[pr + 1]; ++e) {
+        const double v = p.jz[first[c]] * p.trans[e].A + p.jxy[first[c]] * p.trans[e].B + p.kq[first[c]] * p.trans[e].C;
+        const int k = p.trans[e].a2 - a;
+        if (k == 0 && p.trans[e].c2 == cc) {
+          p.pdg[c][pr] = v;
+        } else if (v != 0.0) {
+          if (k == 0 || p.trans[e].c2 - cc != -k || n == kSpinMaxOff) {  // not of the form (a + k, c - k)
+            p.n_cls = 0;
+            return;
+          }
+          p.pov[c][pr][n] = v;
+          p.pk[c][pr] |= (uint32_t)(k & 255) << (8 * n);
+          ++n;
+        }
+      }
+      p.pmo = std::max(p.pmo, n);
+    }
   for (int b = 0; b < p.n_bonds; ++b) {
     int c = 0;
     while (!(p.jz[first[c]] == jz[b] && p.jxy[first[c]] == jxy[b] && p.kq[first[c]] == kq[b])) ++c;
@@ -210,19 +231,49 @@ __global__ void spin_basis_kernel(const SpinDev t, uint64_t* __restrict__ out, i
   out[n] = ((uint64_t)h << (t.bits * t.Nl)) | t.lolist[t.looff[t.T - sum] + r];
 }
 
-// The couplings of SpinParams staged in shared memory for the row walk.  A
+// The couplings of SpinParams staged in shared memory for the row walk, when
+// more than kSpinMaxCls coupling classes leave the elements untabulated.  A
 // state is a hi word (the first Nh = N - Nl sites) and a lo word (the last Nl
 // sites), each with `bits` bits per site; bw1 / bw2 are the shifts of a bond's
 // two digits within their words and bk its kind: 0 both sites in lo, 1 both
 // in hi, 2 site i in hi and j in lo, 3 site i in lo and j in hi.
 struct SpinShared {
-  double cv[kSpinMaxCls * kSpinMaxTrans];  // tabulated elements, or A, B, C of each transition
-  short2 dl[kSpinMaxTrans];                // digit changes (a2 - a, c2 - c) of each transition
+  double cv[3 * kSpinMaxTrans];  // A, B, C of each transition
+  short2 dl[kSpinMaxTrans];      // digit changes (a2 - a, c2 - c) of each transition
   int ts[kSpinMaxPairs + 1];
-  int bw1[kMaxBonds], bw2[kMaxBonds], bk[kMaxBonds], bc[kMaxBonds];
+  int bw1[kMaxBonds], bw2[kMaxBonds], bk[kMaxBonds];
   double bj[3][kMaxBonds];
   double sdg[kSpinMaxSites * kSpinMaxDim];
 };
+
+// The tabulated form (every bond in one of at most kSpinMaxCls coupling
+// classes; D = 2S + 1 digits, MO >= SpinParams::pmo off-diagonal slots):
+// per class and digit pair the diagonal element, the nonzero off-diagonal
+// ones and their k; per bond one record
+//   x  class x D^2 (its pair tables),
+//   y  wi | wj << 8 | (site i in hi) << 16 | (site j in hi) << 17,
+//   z  bh, w  bl: the change of the hi and of the lo word per unit of k.
+// A transition (a, c) -> (a + k, c - k) moves hi to hi + k bh and lo to
+// lo + k bl; a word it leaves alone keeps its part of the rank (the block's
+// first row for hi, the rank r within the block for lo), so a bond inside one
+// word looks up one table and only a bond across the split looks up both.
+template <int D, int MO>
+struct SpinTabShared {
+  double dg[kSpinMaxCls * D * D];
+  double ov[kSpinMaxCls * D * D * MO];
+  uint32_t pk[kSpinMaxCls * D * D];
+  int4 bond[kMaxBonds];
+  double sdg[kSpinMaxSites * D];
+};
+
+__device__ __forceinline__ int stage_site_terms(const SpinParams& p, int N, int d, double* sdg) {
+  int nz = 0;
+  for (int q = threadIdx.x; q < N * d; q += blockDim.x) {
+    sdg[q] = p.sdiag[q / d][q % d];
+    nz |= sdg[q] != 0.0;
+  }
+  return nz;
+}
 
 // Fill sh (all threads of the CTA); returns whether this thread staged a
 // nonzero site term (the caller reduces it with __syncthreads_or, which is
@@ -230,19 +281,14 @@ struct SpinShared {
 __device__ __forceinline__ int stage_spin(const SpinParams& p, const SpinDev& t, SpinShared& sh) {
   const int d = t.d, N = t.N, bits = t.bits, Nl = t.Nl, Nh = N - Nl;
   const int ntr = p.tstart[d * d];
-  const bool tab = p.n_cls > 0;
   for (int q = threadIdx.x; q <= d * d; q += blockDim.x) sh.ts[q] = p.tstart[q];
   for (int pr = threadIdx.x; pr < d * d; pr += blockDim.x)
     for (int e = p.tstart[pr]; e < p.tstart[pr + 1]; ++e)
       sh.dl[e] = make_short2((short)(p.trans[e].a2 - pr / d), (short)(p.trans[e].c2 - pr % d));
-  if (tab) {
-    for (int q = threadIdx.x; q < p.n_cls * ntr; q += blockDim.x) sh.cv[q] = p.cval[q / ntr][q % ntr];
-  } else {
-    for (int q = threadIdx.x; q < ntr; q += blockDim.x) {
-      sh.cv[3 * q] = p.trans[q].A;
-      sh.cv[3 * q + 1] = p.trans[q].B;
-      sh.cv[3 * q + 2] = p.trans[q].C;
-    }
+  for (int q = threadIdx.x; q < ntr; q += blockDim.x) {
+    sh.cv[3 * q] = p.trans[q].A;
+    sh.cv[3 * q + 1] = p.trans[q].B;
+    sh.cv[3 * q + 2] = p.trans[q].C;
   }
   for (int q = threadIdx.x; q < p.n_bonds; q += blockDim.x) {
     const int i = p.s1[q], j = p.s2[q];
@@ -250,17 +296,46 @@ __device__ __forceinline__ int stage_spin(const SpinParams& p, const SpinDev& t,
     sh.bw1[q] = li ? bits * (N - 1 - i) : bits * (Nh - 1 - i);
     sh.bw2[q] = lj ? bits * (N - 1 - j) : bits * (Nh - 1 - j);
     sh.bk[q] = (li && lj) ? 0 : (!li && !lj) ? 1 : !li ? 2 : 3;
-    sh.bc[q] = tab ? p.cls[q] * ntr : 0;
     sh.bj[0][q] = p.jz[q];
     sh.bj[1][q] = p.jxy[q];
     sh.bj[2][q] = p.kq[q];
   }
-  int nz = 0;
-  for (int q = threadIdx.x; q < N * d; q += blockDim.x) {
-    sh.sdg[q] = p.sdiag[q / d][q % d];
-    nz |= sh.sdg[q] != 0.0;
+  return stage_site_terms(p, N, d, sh.sdg);
+}
+
+template <int D, int MO>
+__device__ __forceinline__ int stage_spin(const SpinParams& p, const SpinDev& t, SpinTabShared<D, MO>& sh) {
+  constexpr int P = D * D;
+  const int N = t.N, bits = t.bits, Nh = N - t.Nl;
+  for (int q = threadIdx.x; q < p.n_cls * P; q += blockDim.x) {
+    const int c = q / P, pr = q % P;
+    sh.dg[q] = p.pdg[c][pr];
+    sh.pk[q] = p.pk[c][pr];
+#pragma unroll
+    for (int s = 0; s < MO; ++s) sh.ov[q * MO + s] = s < kSpinMaxOff ? p.pov[c][pr][s] : 0.0;
   }
-  return nz;
+  for (int q = threadIdx.x; q < p.n_bonds; q += blockDim.x) {
+    const int i = p.s1[q], j = p.s2[q];
+    const bool li = i >= Nh, lj = j >= Nh;
+    const int wi = li ? bits * (N - 1 - i) : bits * (Nh - 1 - i);
+    const int wj = lj ? bits * (N - 1 - j) : bits * (Nh - 1 - j);
+    int bh, bl;
+    if (li && lj) {
+      bh = 0;
+      bl = (1 << wi) - (1 << wj);
+    } else if (!li && !lj) {
+      bh = (1 << wi) - (1 << wj);
+      bl = 0;
+    } else if (!li) {
+      bh = 1 << wi;
+      bl = -(1 << wj);
+    } else {
+      bh = -(1 << wj);
+      bl = 1 << wi;
+    }
+    sh.bond[q] = make_int4(p.cls[q] * P, wi | (wj << 8) | ((int)!li << 16) | ((int)!lj << 17), bh, bl);
+  }
+  return stage_site_terms(p, N, D, sh.sdg);
 }
 
 // One row of H: state (h, lo), its block's first row `base` and its rank r
@@ -271,9 +346,8 @@ __device__ __forceinline__ int stage_spin(const SpinParams& p, const SpinDev& t,
 // base + tlo[lo']), a bond inside hi keeps lo (rank = thi[h'] + r); only
 // bonds across the split rank through both tables.
 template <class Off>
-__device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bool tab, bool has_site,
-                                           const SpinDev& t, uint32_t h, uint32_t lo, uint32_t base, uint32_t r,
-                                           Off&& off) {
+__device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bool has_site, const SpinDev& t,
+                                           uint32_t h, uint32_t lo, uint32_t base, uint32_t r, Off&& off) {
   const int d = t.d, N = t.N, bits = t.bits, Nh = N - t.Nl;
   const uint32_t dm = (1u << bits) - 1u;
   double dg = 0.0;
@@ -287,10 +361,8 @@ __device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bo
     const uint32_t wc = (k == 0 || k == 2) ? lo : h;  // the word holding site j
     const int a = (int)((wa >> wi) & dm), c = (int)((wc >> wj) & dm);
     const int pr = a * d + c;
-    const int cb = sh.bc[q];
     for (int e = sh.ts[pr]; e < sh.ts[pr + 1]; ++e) {
-      const double v = tab ? sh.cv[cb + e]
-                           : sh.bj[0][q] * sh.cv[3 * e] + sh.bj[1][q] * sh.cv[3 * e + 1] + sh.bj[2][q] * sh.cv[3 * e + 2];
+      const double v = sh.bj[0][q] * sh.cv[3 * e] + sh.bj[1][q] * sh.cv[3 * e + 1] + sh.bj[2][q] * sh.cv[3 * e + 2];
       const short2 dl = sh.dl[e];
       if (dl.x == 0 && dl.y == 0) {
         dg += v;
@@ -312,13 +384,47 @@ __device__ __forceinline__ double spin_row(const SpinShared& sh, int n_bonds, bo
   return dg;
 }
 
+// The same row from the tabulated form: the same diagonal sum and the same
+// off-diagonal calls in the same order, less the zero elements.
+template <int D, int MO, class Off>
+__device__ __forceinline__ double spin_row(const SpinTabShared<D, MO>& sh, int n_bonds, bool has_site,
+                                           const SpinDev& t, uint32_t h, uint32_t lo, uint32_t base, uint32_t r,
+                                           Off&& off) {
+  constexpr int BITS = D <= 2 ? 1 : D <= 4 ? 2 : 3;
+  constexpr uint32_t dm = (1u << BITS) - 1u;
+  const int N = t.N, Nh = N - t.Nl;
+  double dg = 0.0;
+  if (has_site) {
+    for (int i = 0; i < Nh; ++i) dg += sh.sdg[i * D + (int)((h >> (BITS * (Nh - 1 - i))) & dm)];
+    for (int i = Nh; i < N; ++i) dg += sh.sdg[i * D + (int)((lo >> (BITS * (N - 1 - i))) & dm)];
+  }
+  for (int q = 0; q < n_bonds; ++q) {
+    const int4 b = sh.bond[q];
+    const uint32_t wa = (b.y & 0x10000) ? h : lo, wc = (b.y & 0x20000) ? h : lo;
+    const int a = (int)((wa >> (b.y & 255)) & dm), c = (int)((wc >> ((b.y >> 8) & 255)) & dm);
+    const int pr = b.x + a * D + c;
+    dg += sh.dg[pr];
+    const uint32_t kp = sh.pk[pr];
+#pragma unroll
+    for (int s = 0; s < MO; ++s) {
+      const int k = (int)(int8_t)(uint8_t)(kp >> (8 * s));
+      if (k != 0) {
+        const uint32_t th = b.z ? __ldg(t.thi + (h + (uint32_t)(k * b.z))) : base;
+        const uint32_t tl = b.w ? __ldg(t.tlo + (lo + (uint32_t)(k * b.w))) : r;
+        off(sh.ov[pr * MO + s], th + tl);
+      }
+    }
+  }
+  return dg;
+}
+
+template <class Sh>
 __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_constant__ SpinParams p, const SpinDev t,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ alpha_part) {
-  __shared__ SpinShared sh;
+  __shared__ Sh sh;
   __shared__ double red[33];
   const int N = t.N, bits = t.bits;
-  const bool tab = p.n_cls > 0;
   const bool has_site = __syncthreads_or(stage_spin(p, t, sh)) != 0;
   const uint32_t dm = (1u << bits) - 1u;
   for (int64_t it = blockIdx.x; it < t.n_tiles; it += gridDim.x) {
@@ -333,7 +439,7 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
       const uint32_t lo = t.lolist[lbase + r];
       const uint32_t row = base + r;
       double off = 0.0;
-      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, h, lo, base, r,
+      const double dg = spin_row(sh, p.n_bonds, has_site, t, h, lo, base, r,
                                  [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
       const double xi = x[row];
       const double yi = fma(dg, xi, off);
@@ -354,16 +460,16 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
 // (hamiltonian_matrix.hpp:307-345 with the Bloch basis of
 // blochbasisstates.h:92-271).  alpha_part: one partial of Re<x, y> per
 // kMomTileRows rows.
+template <class Sh>
 __global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_constant__ SpinParams p,
                                                                    const __grid_constant__ MomParams mp,
                                                                    const SpinDev t, const SpinMomTables m,
                                                                    const double2* __restrict__ x,
                                                                    double2* __restrict__ y,
                                                                    double* __restrict__ alpha_part) {
-  __shared__ SpinShared sh;
+  __shared__ Sh sh;
   __shared__ double pre[kMaxTrans], pim[kMaxTrans];
   __shared__ double red[33];
-  const bool tab = p.n_cls > 0;
   const int nz = stage_spin(p, t, sh);
   for (int q = threadIdx.x; q < mp.n_trans; q += kSpinThreads) {
     pre[q] = mp.phase_re[q];
@@ -383,7 +489,7 @@ __global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_
       const uint32_t rh = (uint32_t)(r >> shift), rl = (uint32_t)(r & lm);
       const double ni = m.norm[i];
       double are = 0.0, aim = 0.0;
-      const double dg = spin_row(sh, p.n_bonds, tab, has_site, t, rh, rl, __ldg(t.thi + rh), __ldg(t.tlo + rl),
+      const double dg = spin_row(sh, p.n_bonds, has_site, t, rh, rl, __ldg(t.thi + rh), __ldg(t.tlo + rl),
                                  [&](double v, uint32_t rk) {
         const uint32_t e = __ldg(m.map + rk);
         if (e == kMomNone) return;
@@ -652,12 +758,39 @@ int spin_mom_expectation(aed_handle* h, const double* psi, int kind, int n, cons
   return AED_OK;
 }
 
+template <class T>
+struct Form {
+  using type = T;
+};
+
+// Calls f(Form<shared layout>) with the layout of the apply for p: the
+// tabulated form with D = d digits and enough off-diagonal slots, or the
+// per-bond form when the couplings have more than kSpinMaxCls classes.
+template <class F>
+void with_spin_form(const SpinParams& p, const SpinDev& t, F&& f) {
+  if (p.n_cls == 0) return f(Form<SpinShared>{});
+  switch (t.d) {
+    case 2:
+      return f(Form<SpinTabShared<2, 1>>{});
+    case 3:
+      return f(Form<SpinTabShared<3, 2>>{});
+    case 4:
+      return p.pmo <= 2 ? f(Form<SpinTabShared<4, 2>>{}) : f(Form<SpinTabShared<4, 3>>{});
+    default:
+      return p.pmo <= 2 ? f(Form<SpinTabShared<5, 2>>{}) : f(Form<SpinTabShared<5, 4>>{});
+  }
+}
+
 int launch_spin_mom_hv(const SpinParams& p, const MomParams& mp, const SpinDev& t, const SpinMomTables& m,
                        const double* x, double* y, double* alpha_part, cudaStream_t st) {
   if (m.dim == 0) return AED_OK;
   const int64_t tiles = mom_tiles(m.dim), cap = (int64_t)sm_count() * 8;
-  spin_mom_hv_kernel<<<(int)(tiles < cap ? tiles : cap), kSpinThreads, 0, st>>>(
-      p, mp, t, m, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), alpha_part);
+  const int grid = (int)(tiles < cap ? tiles : cap);
+  const double2* xc = reinterpret_cast<const double2*>(x);
+  double2* yc = reinterpret_cast<double2*>(y);
+  with_spin_form(p, t, [&](auto form) {
+    spin_mom_hv_kernel<typename decltype(form)::type><<<grid, kSpinThreads, 0, st>>>(p, mp, t, m, xc, yc, alpha_part);
+  });
   return check_launch_counted("spin_mom_hv_kernel");
 }
 
@@ -675,7 +808,9 @@ int launch_spin_hv(const SpinParams& p, const SpinDev& t, const double* x, doubl
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t cap = (int64_t)sms * 8;
   const int grid = (int)(t.n_tiles < cap ? t.n_tiles : cap);
-  spin_hv_kernel<<<grid, kSpinThreads, 0, st>>>(p, t, x, y, alpha_part);
+  with_spin_form(p, t, [&](auto form) {
+    spin_hv_kernel<typename decltype(form)::type><<<grid, kSpinThreads, 0, st>>>(p, t, x, y, alpha_part);
+  });
   return check_launch_counted("spin_hv_kernel");
 }
 

@@ -56,6 +56,7 @@ struct SpinTrans {
 };
 
 constexpr int kSpinMaxCls = 8;  // coupling classes whose elements are tabulated
+constexpr int kSpinMaxOff = kSpinMaxDim - 1;  // off-diagonal transitions of one digit pair (they keep a + c)
 
 struct SpinParams {
   int N, n_bonds, twoS;
@@ -65,11 +66,18 @@ struct SpinParams {
   int tstart[kSpinMaxPairs + 1];  // transitions of pair (a, c) = a d + c: [tstart[p], tstart[p+1])
   SpinTrans trans[kSpinMaxTrans];
   // bonds with the same (Jz, Jxy, K) share a class; with at most kSpinMaxCls
-  // classes the elements Jz A + Jxy B + K C are tabulated per class (n_cls = 0:
-  // formed per bond in the kernel)
+  // classes the elements Jz A + Jxy B + K C are tabulated per class and digit
+  // pair (a, c) = a d + c (n_cls = 0: formed per bond in the kernel): pdg the
+  // diagonal element, pov the off-diagonal elements that are nonzero (zero
+  // elements are skipped, hamiltonian_matrix.hpp:316) in target order (a2, c2),
+  // each with k = a2 - a = c - c2 in one signed byte of pk (byte s for pov[s],
+  // 0 past the last); pmo the most off-diagonal elements of any class and pair
   int n_cls;
   int cls[kMaxBonds];
-  double cval[kSpinMaxCls][kSpinMaxTrans];
+  int pmo;
+  double pdg[kSpinMaxCls][kSpinMaxPairs];
+  double pov[kSpinMaxCls][kSpinMaxPairs][kSpinMaxOff];
+  uint32_t pk[kSpinMaxCls][kSpinMaxPairs];
   double sdiag[kSpinMaxSites][kSpinMaxDim];  // -h m + D m^2 of every site and digit
 };
 // The local operators of the spin model (models.xml.in:24-36, 282-300): the
