@@ -147,7 +147,8 @@ void release(aed_handle* h) {
                   (void*)h->d_start64,
                   (void*)h->d_reps, (void*)h->d_norm, (void*)h->d_mdiag, (void*)h->d_map, (void*)h->d_sthi,
                   (void*)h->d_stlo, (void*)h->d_slolist, (void*)h->d_slooff, (void*)h->d_sblk_hi,
-                  (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r, (void*)h->d_sreps})
+                  (void*)h->d_sblk_off, (void*)h->d_stile_blk, (void*)h->d_stile_r, (void*)h->d_sreps,
+                  (void*)h->d_slol})
     mem_dev_free(p, h->stream);
   delete h->mp;
   delete h->sp;
@@ -746,6 +747,28 @@ void spin_couplings(const Model& m, SpinParams& p) {
   spin_set_couplings(m.s1, m.s2, m.jz, m.jxy, m.kq, m.site_h, m.site_d, m.N, p);
 }
 
+// The lo table of a spin-S Sz-sector handle for its current couplings (none
+// for a momentum sector, whose apply walks representatives, or a form
+// without one); filled on the handle's stream and waited for.
+int spin_lo_table(aed_handle* h) {
+  SpinDev& t = h->sdev;
+  size_t bytes = h->mom ? 0 : spin_lo_table_bytes(*h->sp, t);
+  if (bytes > (size_t(1) << 30)) bytes = 0;  // a bond list this long walks the lo words instead
+  t.lol = nullptr;
+  if (bytes == 0) return AED_OK;
+  if (bytes > h->slol_bytes) {
+    mem_dev_free(h->d_slol, h->stream);
+    h->d_slol = nullptr;
+    h->slol_bytes = 0;
+    if (int rc = mem_dev_alloc_n(&h->d_slol, bytes / sizeof(uint2))) return rc;
+    h->slol_bytes = bytes;
+  }
+  if (int rc = launch_spin_lo_table(*h->sp, t, h->d_slol, h->stream)) return rc;
+  AED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  t.lol = h->d_slol;
+  return AED_OK;
+}
+
 }  // namespace
 
 int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_handle** out) {
@@ -830,7 +853,12 @@ int aed_create_spin(const aed_model_desc* model, int32_t two_s, int device, aed_
   t.Nl = tb.Nl;
   t.d = tb.d;
   t.T = tb.T;
+  t.n_lo = (int64_t)tb.lolist.size();
   h->dim = h->vlen = D;
+  if ((rc = spin_lo_table(h))) {
+    release(h);
+    return rc;
+  }
   *out = h;
   return AED_OK;
 }
@@ -854,6 +882,10 @@ int aed_create_spin_momentum(const aed_model_desc* model, int32_t two_s, const a
   DeviceGuard g(device);
   h->mom = true;
   h->mp = mpp.release();
+  h->sdev.lol = nullptr;  // the momentum apply walks representatives, not tiles
+  mem_dev_free(h->d_slol, h->stream);
+  h->d_slol = nullptr;
+  h->slol_bytes = 0;
   // the Sz sector's partial-sum arrays give way to the momentum sector's
   mem_dev_free(h->d_partA, h->stream);
   mem_dev_free(h->d_partB, h->stream);
@@ -1050,7 +1082,7 @@ int aed_set_couplings(aed_handle* h, const aed_model_desc* model) {
   h->rec_live = false;
   if (h->gen) {  // same sector: new site terms and bonds
     spin_couplings(h->model, *h->sp);
-    return AED_OK;
+    return spin_lo_table(h);
   }
   if (h->mom) {  // same basis and translations: new flip list and diagonal
     mom_flips(h->model, *h->mp);

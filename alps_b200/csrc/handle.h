@@ -60,6 +60,8 @@ struct aed_handle {
   int two_s = 1;
   uint32_t *d_sthi = nullptr, *d_stlo = nullptr, *d_slolist = nullptr, *d_slooff = nullptr;
   uint32_t *d_sblk_hi = nullptr, *d_sblk_off = nullptr, *d_stile_blk = nullptr, *d_stile_r = nullptr;
+  uint2* d_slol = nullptr;  // the lo table of the tabulated Sz-sector apply (sdev.lol), slol_bytes allocated
+  size_t slol_bytes = 0;
   // <x, y> partials of one apply (tiles of the real apply, the momentum apply or the spin-S apply)
   int64_t alpha_tiles() const { return mom ? aed::mom_tiles(dim) : gen ? sdev.n_tiles : dt.n_tiles; }
   // solve workspaces, kept between solves (grown on demand, so that a solve

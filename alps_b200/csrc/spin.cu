@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "handle.h"
@@ -266,6 +267,28 @@ struct SpinTabShared {
   double sdg[kSpinMaxSites * D];
 };
 
+// In the Sz-sector apply all rows of a work tile share their hi word, so a
+// bond with both sites in hi has the same digits, elements and target hi
+// words in every row: the CTA forms them once per tile.  tb = thi of the
+// target hi word (the target row is tb + r), kSpinNone for an empty slot.
+template <int MO>
+struct SpinTileHi {
+  double dg[kMaxBonds];
+  double v[kMaxBonds][MO];
+  uint32_t tb[kMaxBonds][MO];
+};
+template <class Sh>
+struct TileHiOf {
+  using type = char;
+};
+template <int D, int MO>
+struct TileHiOf<SpinTabShared<D, MO>> {
+  using type = SpinTileHi<MO>;
+};
+
+// Bond record flags: bit 0 site i in hi, bit 1 site j in hi.
+__device__ __forceinline__ int bond_side(const int4& b) { return (b.y >> 16) & 3; }
+
 __device__ __forceinline__ int stage_site_terms(const SpinParams& p, int N, int d, double* sdg) {
   int nz = 0;
   for (int q = threadIdx.x; q < N * d; q += blockDim.x) {
@@ -418,11 +441,123 @@ __device__ __forceinline__ double spin_row(const SpinTabShared<D, MO>& sh, int n
   return dg;
 }
 
+// The hi-hi bonds' shared entries of the tile whose hi word is h (all threads
+// of the CTA; barriers before, against the readers of the last tile, and after).
+template <int D, int MO>
+__device__ __forceinline__ void tile_hi_entries(const SpinTabShared<D, MO>& sh, SpinTileHi<MO>& hh, int n_bonds,
+                                                const SpinDev& t, uint32_t h) {
+  constexpr int BITS = D <= 2 ? 1 : D <= 4 ? 2 : 3;
+  constexpr uint32_t dm = (1u << BITS) - 1u;
+  __syncthreads();
+  for (int q = threadIdx.x; q < n_bonds; q += blockDim.x) {
+    const int4 b = sh.bond[q];
+    if (bond_side(b) != 3) continue;
+    const int a = (int)((h >> (b.y & 255)) & dm), c = (int)((h >> ((b.y >> 8) & 255)) & dm);
+    const int pr = b.x + a * D + c;
+    hh.dg[q] = sh.dg[pr];
+    const uint32_t kp = sh.pk[pr];
+#pragma unroll
+    for (int s = 0; s < MO; ++s) {
+      const int k = (int)(int8_t)(uint8_t)(kp >> (8 * s));
+      hh.v[q][s] = sh.ov[pr * MO + s];
+      hh.tb[q][s] = k != 0 ? __ldg(t.thi + (h + (uint32_t)(k * b.z))) : kSpinNone;
+    }
+  }
+  __syncthreads();
+}
+
+// The tabulated row of the Sz-sector apply: hi-hi bonds from the tile's
+// entries, lo-lo bonds from the lo table (u = the row's lo code's index in
+// lolist), bonds across the split as spin_row.  The same diagonal sum and the
+// same off-diagonal calls in the same order as spin_row.
+template <int D, int MO, class Off>
+__device__ __forceinline__ double spin_row_tile(const SpinTabShared<D, MO>& sh, const SpinTileHi<MO>& hh, int n_bonds,
+                                                bool has_site, const SpinDev& t, uint32_t h, uint32_t lo,
+                                                uint32_t base, uint32_t r, uint32_t u, Off&& off) {
+  constexpr int BITS = D <= 2 ? 1 : D <= 4 ? 2 : 3;
+  constexpr uint32_t dm = (1u << BITS) - 1u;
+  const int N = t.N, Nh = N - t.Nl;
+  const bool lot = MO <= 2 && t.lol != nullptr;
+  double dg = 0.0;
+  if (has_site) {
+    for (int i = 0; i < Nh; ++i) dg += sh.sdg[i * D + (int)((h >> (BITS * (Nh - 1 - i))) & dm)];
+    for (int i = Nh; i < N; ++i) dg += sh.sdg[i * D + (int)((lo >> (BITS * (N - 1 - i))) & dm)];
+  }
+  const uint2* lol = t.lol + u;
+  for (int q = 0; q < n_bonds; ++q) {
+    const int4 b = sh.bond[q];
+    const int side = bond_side(b);
+    if (side == 3) {
+      dg += hh.dg[q];
+#pragma unroll
+      for (int s = 0; s < MO; ++s) {
+        const uint32_t tb = hh.tb[q][s];
+        if (tb != kSpinNone) off(hh.v[q][s], tb + r);
+      }
+      continue;
+    }
+    if (side == 0 && lot) {
+      const uint2 e = __ldg(lol);
+      lol += t.n_lo;
+      const int pr = b.x + (int)(e.x >> 26);
+      dg += sh.dg[pr];
+      const uint32_t r0 = e.x & kSpinLoNone;
+      if (r0 != kSpinLoNone) off(sh.ov[pr * MO], base + r0);
+      if (MO > 1 && e.y != kSpinLoNone) off(sh.ov[pr * MO + (MO > 1 ? 1 : 0)], base + e.y);
+      continue;
+    }
+    const uint32_t wa = (b.y & 0x10000) ? h : lo, wc = (b.y & 0x20000) ? h : lo;
+    const int a = (int)((wa >> (b.y & 255)) & dm), c = (int)((wc >> ((b.y >> 8) & 255)) & dm);
+    const int pr = b.x + a * D + c;
+    dg += sh.dg[pr];
+    const uint32_t kp = sh.pk[pr];
+#pragma unroll
+    for (int s = 0; s < MO; ++s) {
+      const int k = (int)(int8_t)(uint8_t)(kp >> (8 * s));
+      if (k != 0) {
+        const uint32_t th = b.z ? __ldg(t.thi + (h + (uint32_t)(k * b.z))) : base;
+        const uint32_t tl = b.w ? __ldg(t.tlo + (lo + (uint32_t)(k * b.w))) : r;
+        off(sh.ov[pr * MO + s], th + tl);
+      }
+    }
+  }
+  return dg;
+}
+
+// The lo table (SpinDev::lol): one thread per (lo-lo bond j, lo code u).
+template <int D, int MO>
+__global__ void spin_lo_table_kernel(const __grid_constant__ SpinParams p, const SpinDev t, uint2* __restrict__ out) {
+  constexpr int BITS = D <= 2 ? 1 : D <= 4 ? 2 : 3;
+  constexpr uint32_t dm = (1u << BITS) - 1u;
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= t.n_lo * t.n_ll) return;
+  const int j = (int)(n / t.n_lo);
+  const int64_t u = n - (int64_t)j * t.n_lo;
+  const int N = t.N, Nh = N - t.Nl;
+  int q = 0;
+  for (int c = -1; q < p.n_bonds; ++q)
+    if (p.s1[q] >= Nh && p.s2[q] >= Nh && ++c == j) break;
+  const int wi = BITS * (N - 1 - p.s1[q]), wj = BITS * (N - 1 - p.s2[q]);
+  const uint32_t lo = t.lolist[u];
+  const int pr = (int)((lo >> wi) & dm) * D + (int)((lo >> wj) & dm);
+  const uint32_t kp = p.pk[p.cls[q]][pr];
+  const int bl = (1 << wi) - (1 << wj);
+  uint32_t rk[2] = {kSpinLoNone, kSpinLoNone};
+#pragma unroll
+  for (int s = 0; s < MO && s < 2; ++s) {
+    const int k = (int)(int8_t)(uint8_t)(kp >> (8 * s));
+    if (k != 0) rk[s] = t.tlo[lo + (uint32_t)(k * bl)];
+  }
+  out[n] = make_uint2(rk[0] | ((uint32_t)pr << 26), rk[1]);
+}
+
 template <class Sh>
 __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_constant__ SpinParams p, const SpinDev t,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ alpha_part) {
+  constexpr bool kTab = !std::is_same<Sh, SpinShared>::value;
   __shared__ Sh sh;
+  __shared__ typename TileHiOf<Sh>::type hh;
   __shared__ double red[33];
   const int N = t.N, bits = t.bits;
   const bool has_site = __syncthreads_or(stage_spin(p, t, sh)) != 0;
@@ -435,16 +570,30 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
     const uint32_t lbase = t.looff[t.T - sum], rows = t.looff[t.T - sum + 1] - lbase;
     const uint32_t r1 = rows < r0 + kSpinTileRows ? rows : r0 + kSpinTileRows;
     double dot = 0.0;
-    for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
-      const uint32_t lo = t.lolist[lbase + r];
-      const uint32_t row = base + r;
-      double off = 0.0;
-      const double dg = spin_row(sh, p.n_bonds, has_site, t, h, lo, base, r,
-                                 [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
-      const double xi = x[row];
-      const double yi = fma(dg, xi, off);
-      y[row] = yi;
-      dot = fma(xi, yi, dot);
+    if constexpr (kTab) {
+      tile_hi_entries(sh, hh, p.n_bonds, t, h);
+      for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
+        const uint32_t lo = t.lolist[lbase + r];
+        double off = 0.0;
+        const double dg = spin_row_tile(sh, hh, p.n_bonds, has_site, t, h, lo, base, r, lbase + r,
+                                        [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
+        const double xi = x[base + r];
+        const double yi = fma(dg, xi, off);
+        y[base + r] = yi;
+        dot = fma(xi, yi, dot);
+      }
+    } else {
+      for (uint32_t r = r0 + threadIdx.x; r < r1; r += kSpinThreads) {
+        const uint32_t lo = t.lolist[lbase + r];
+        const uint32_t row = base + r;
+        double off = 0.0;
+        const double dg = spin_row(sh, p.n_bonds, has_site, t, h, lo, base, r,
+                                   [&](double v, uint32_t rk) { off = fma(v, __ldg(x + rk), off); });
+        const double xi = x[row];
+        const double yi = fma(dg, xi, off);
+        y[row] = yi;
+        dot = fma(xi, yi, dot);
+      }
     }
     if (alpha_part) {
       const double tot = block_sum_all<kSpinThreads>(dot, red);
@@ -792,6 +941,36 @@ int launch_spin_mom_hv(const SpinParams& p, const MomParams& mp, const SpinDev& 
     spin_mom_hv_kernel<typename decltype(form)::type><<<grid, kSpinThreads, 0, st>>>(p, mp, t, m, xc, yc, alpha_part);
   });
   return check_launch_counted("spin_mom_hv_kernel");
+}
+
+size_t spin_lo_table_bytes(const SpinParams& p, SpinDev& t) {
+  const int Nh = t.N - t.Nl;
+  t.n_ll = 0;
+  for (int q = 0; q < p.n_bonds; ++q) t.n_ll += p.s1[q] >= Nh && p.s2[q] >= Nh;
+  // the forms with at most two off-diagonal slots (tile row walk, MO <= 2)
+  const bool two = p.n_cls > 0 && (t.d <= 3 || p.pmo <= 2);
+  return two && t.n_ll > 0 && t.n_lo > 0 ? (size_t)t.n_lo * t.n_ll * sizeof(uint2) : 0;
+}
+
+int launch_spin_lo_table(const SpinParams& p, const SpinDev& t, uint2* dst, cudaStream_t st) {
+  const int64_t n = t.n_lo * t.n_ll;
+  if (n == 0) return AED_OK;
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  switch (t.d) {
+    case 2:
+      spin_lo_table_kernel<2, 1><<<grid, 256, 0, st>>>(p, t, dst);
+      break;
+    case 3:
+      spin_lo_table_kernel<3, 2><<<grid, 256, 0, st>>>(p, t, dst);
+      break;
+    case 4:
+      spin_lo_table_kernel<4, 2><<<grid, 256, 0, st>>>(p, t, dst);
+      break;
+    default:
+      spin_lo_table_kernel<5, 2><<<grid, 256, 0, st>>>(p, t, dst);
+      break;
+  }
+  return check_launch_counted("spin_lo_table_kernel");
 }
 
 int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st) {

@@ -46,7 +46,16 @@ struct SpinDev {
   const uint32_t *thi, *tlo, *lolist, *looff, *blk_hi, *blk_off, *tile_blk, *tile_r;
   int64_t D, n_blk, n_tiles;
   int N, bits, Nl, d, T;
+  // the lo table of the tabulated form (nullptr: none): per bond with both
+  // sites in lo (the j-th such bond, in bond order) and per lo code u (its
+  // index in lolist), entry [j n_lo + u] = (r0 | pr << 26, r1): the digit
+  // pair pr = a d + c and the ranks within the block (tlo of the target lo
+  // code) of the pair's off-diagonal slots 0 and 1, kSpinLoNone where empty
+  const uint2* lol;
+  int64_t n_lo;
+  int n_ll;
 };
+constexpr uint32_t kSpinLoNone = (1u << 26) - 1u;
 
 // One transition of a bond's pair of digits (a, c) -> (a2, c2) with the
 // element Jz * A + Jxy * B + K * C (A: Sz Sz, B: exchange_xy, C: biquadratic).
@@ -92,6 +101,10 @@ void spin_set_couplings(const std::vector<int>& s1, const std::vector<int>& s2, 
 int launch_spin_basis(const SpinDev& t, uint64_t* out, int64_t offset, int64_t count, cudaStream_t st);
 int launch_spin_hv(const SpinParams& p, const SpinDev& t, const double* x, double* y, double* alpha_part,
                    cudaStream_t st);
+// Bytes of the lo table for p and t (0: the apply's form uses none), and its
+// fill (the table at dst, t.n_lo set); t.n_ll is set by the first call.
+size_t spin_lo_table_bytes(const SpinParams& p, SpinDev& t);
+int launch_spin_lo_table(const SpinParams& p, const SpinDev& t, uint2* dst, cudaStream_t st);
 __host__ __device__ inline int64_t spin_tiles_of(const SpinDev& t) { return t.n_tiles; }
 
 }  // namespace aed

@@ -104,6 +104,30 @@ def test_spin_s_set_couplings():
     ham.close()
 
 
+def test_spin_s_set_couplings_through_every_apply_form():
+    """One spin-3/2 handle (8 sites: bonds inside the lo word, inside the hi word and across) through
+    new couplings that change the apply's form: Heisenberg (two off-diagonal slots, lo table), with a
+    biquadratic term (three slots, no lo table), one class per bond (16 classes, more than 8: per-bond
+    form), and Heisenberg again with next-nearest bonds (a longer lo table); H x equals the oracle's
+    each time (1e-12 of sum |H_ij x_j|)."""
+    n, two_s, T = 8, 3, 12
+    rng = np.random.default_rng(31)
+    nnn = [(i, (i + 2) % n, 0.4, 0.3, 0.0) for i in range(n)]
+    forms = [_chain(n, 1.0, 0.8), _chain(n, 1.0, 1.0, 0.25),
+             [(s, t, *rng.uniform(0.5, 1.5, 2), rng.uniform(-0.3, 0.3)) for s, t, *_ in _chain(n) + nnn],
+             _chain(n) + nnn]
+    ham = ed.Hamiltonian(n, T, forms[0], two_s=two_s)
+    try:
+        for bonds in forms:
+            ham.set_couplings(bonds)
+            H = ospin.hamiltonian(n, two_s, bonds, digit_sum=T)
+            x = rng.normal(size=ham.dim)
+            y = ham.apply(x)
+            assert np.all(np.abs(y - H @ x) <= 1e-12 * (abs(H) @ np.abs(x)) + 1e-14)
+    finally:
+        ham.close()
+
+
 SPIN_MEAS = {
     "MEASURE_AVERAGE[Magnetization]": "Sz",
     "MEASURE_LOCAL[Local magnetization]": "Sz",
