@@ -609,8 +609,11 @@ __global__ void __launch_bounds__(kSpinThreads) spin_hv_kernel(const __grid_cons
 // (hamiltonian_matrix.hpp:307-345 with the Bloch basis of
 // blochbasisstates.h:92-271).  alpha_part: one partial of Re<x, y> per
 // kMomTileRows rows.
+// Five CTAs per SM (48 registers, no spill in the tabulated forms): the walk is
+// bound by its dependent loads, and a fifth CTA hides more of them than the
+// registers it takes away (0.366 against 0.452 ms on the spin-1 chain L=18).
 template <class Sh>
-__global__ void __launch_bounds__(kSpinThreads) spin_mom_hv_kernel(const __grid_constant__ SpinParams p,
+__global__ void __launch_bounds__(kSpinThreads, 5) spin_mom_hv_kernel(const __grid_constant__ SpinParams p,
                                                                    const __grid_constant__ MomParams mp,
                                                                    const SpinDev t, const SpinMomTables m,
                                                                    const double2* __restrict__ x,
