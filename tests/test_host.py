@@ -486,3 +486,14 @@ def test_lattice_library_errors_as_the_reference(tmp_path):
     g.write_text("<LATTICES><LATTICEGRAPH name='chain lattice'><FINITELATTICE/></LATTICEGRAPH></LATTICES>")
     with pytest.raises(ed.AEDError, match="LATTICEGRAPH"):
         ed.model_from_parameters(dict(p, LATTICE_LIBRARY=str(g)))
+
+
+def test_bench_seeded_start_equals_the_engines_start_vector():
+    """bench.py's end-to-end leg builds the seed-1 start vector on the host: it equals the oracle's
+    restatement of the engine's fill_random (pinned to the GPU's bit for bit by the parity tests), across
+    the chunk boundary of its generator."""
+    import bench
+
+    n = (1 << 22) + 1000
+    assert np.array_equal(bench.seeded_start(1, n), oracle.start_vector(1, n))
+    assert np.array_equal(bench.seeded_start(7, 5000), oracle.start_vector(7, 5000))
