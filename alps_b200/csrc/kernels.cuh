@@ -112,16 +112,19 @@ int launch_ritz_combine(const float* V, int64_t ld, int m, const double* coef, d
 
 // ---- Rayleigh-Ritz refinement of the mixed path (refine.cu) ----
 constexpr int kMaxRR = 8;     // Ritz vectors in one refinement
-constexpr int kMaxComb = 16;  // stored vectors per ritz_combine_multi call (a store chunk)
+constexpr int kMaxComb = 16;  // vectors of one chunk of the FP32 basis store
 struct VecSet {
   double* p[kMaxRR];
 };
 struct ResidCoef {
   double cw[kMaxRR][kMaxRR], cx[kMaxRR][kMaxRR];
 };
-// out.p[k][i] (+)= sum_j coef[k * m + j] V[j * ld + i], k < K, m <= kMaxComb.
-int launch_ritz_combine_multi(const float* V, int64_t ld, int m, const double* coef, int K, const VecSet& out,
-                              int64_t n, bool accumulate, cudaStream_t st);
+// The FP32 basis store: chunk c holds v_{kMaxComb c} .. v_{kMaxComb c + kMaxComb - 1}, ld apart.
+// out.p[k][i] = sum_{j < m} coef[k * m + j] v_j[i] for k < K: one pass over the m stored vectors
+// (kCombChunks chunks per launch, the K sums held in registers throughout), FP64 sums in ascending j.
+constexpr int kCombChunks = 32;
+int launch_ritz_combine_chunks(const float* const* chunks, int64_t ld, int m, const double* coef, int K,
+                               const VecSet& out, int64_t n, cudaStream_t st);
 // out = [<X_a, X_b> for a <= b (row-major upper triangle), <X_a, Y_b> for all a, b];
 // part: (K(K+1)/2 + K^2) * red_chunks(n) doubles of scratch.
 int launch_gram(const VecSet& X, const VecSet& Y, int K, int64_t n, double* part, double* out, cudaStream_t st);

@@ -621,13 +621,11 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
     if (verbose) std::fprintf(stderr, "[aed] rayleigh-ritz: %d Ritz vectors span the clusters (at most %d)\n", K, kMaxRR);
     return AED_OK;
   }
-  // coefficients chunk by chunk of the store: [K x cnt] blocks at K * j0
-  std::vector<double> cf((size_t)K * m1);
-  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
-    const int cnt = std::min(kStoreChunk, m1 - j0);
-    for (int k = 0; k < K; ++k)
-      for (int j = 0; j < cnt; ++j) cf[(size_t)K * j0 + (size_t)k * cnt + j] = Z[(size_t)k * m1 + j0 + j];
-  }
+  // coefficients [k * m1 + j] (Z's layout) and the store's chunks
+  static_assert(kStoreChunk == kMaxComb, "the combine walks the store chunk by chunk");
+  std::vector<double> cf(Z.begin(), Z.begin() + (size_t)K * m1);
+  std::vector<const float*> chunks;
+  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) chunks.push_back((const float*)slot(j0));
   const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
   const int64_t nch = red_chunks(D);
   const int np = K * (K + 1) / 2 + K * K;
@@ -648,12 +646,7 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   double* hout = nullptr;
   if ((rc = handle_pinned(h, kMaxSums, &hout))) return rc;
   AED_CUDA_TRY(cudaMemcpyAsync(coef_dev, cf.data(), cf.size() * 8, cudaMemcpyHostToDevice, h->stream));
-  for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
-    const int cnt = std::min(kStoreChunk, m1 - j0);
-    if ((rc = launch_ritz_combine_multi((const float*)slot(j0), ldv, cnt, coef_dev + (size_t)K * j0, K, psi, D,
-                                        j0 > 0, h->stream)))
-      return rc;
-  }
+  if ((rc = launch_ritz_combine_chunks(chunks.data(), ldv, m1, coef_dev, K, psi, D, h->stream))) return rc;
   for (int k = 0; k < K; ++k)
     if ((rc = handle_hv(h, false, psi.p[k], img.p[k], nullptr))) return rc;
   if ((rc = launch_gram(psi, img, K, D, part, outd, h->stream))) return rc;
@@ -1004,7 +997,7 @@ constexpr char kStateMagic[8] = {'A', 'E', 'D', 'L', 'N', 'C', 'Z', '1'};
 
 // Ritz vectors of a mixed solve refined by Rayleigh-Ritz: psi_i =
 // sum_j rr_coef[i][j] v_j over the FP32 Lanczos basis the handle kept,
-// accumulated in FP64 (ritz_combine_multi, kMaxRR vectors per pass),
+// accumulated in FP64 (ritz_combine_chunks, kMaxRR vectors per pass),
 // normalised; residual |H psi_i - theta_i psi_i| with the FP64 apply.
 int rr_eigenvectors(aed_handle* h, int k, void* const* vecs, double* evals, double* resid) {
   const int n = (int)h->rr_evals.size(), m1 = h->rr_m;
@@ -1025,22 +1018,14 @@ int rr_eigenvectors(aed_handle* h, int k, void* const* vecs, double* evals, doub
   double* w = (double*)((char*)rb.p + (size_t)k * vb);
   for (int i0 = 0; i0 < k; i0 += kMaxRR) {
     const int K = std::min(kMaxRR, k - i0);
-    std::vector<double> cf((size_t)K * m1);
-    for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
-      const int cnt = std::min(kStoreChunk, m1 - j0);
-      for (int q = 0; q < K; ++q)
-        for (int j = 0; j < cnt; ++j) cf[(size_t)K * j0 + (size_t)q * cnt + j] = h->rr_coef[(size_t)(i0 + q) * m1 + j0 + j];
-    }
+    std::vector<double> cf(h->rr_coef.begin() + (size_t)i0 * m1, h->rr_coef.begin() + (size_t)(i0 + K) * m1);
     AED_CUDA_TRY(cudaMemcpyAsync(cd.p, cf.data(), cf.size() * 8, cudaMemcpyHostToDevice, h->stream));
     VecSet out{};
     for (int q = 0; q < K; ++q) out.p[q] = acc[i0 + q];
-    for (int j0 = 0; j0 < m1; j0 += kStoreChunk) {
-      const int cnt = std::min(kStoreChunk, m1 - j0);
-      const float* V = (const float*)h->store_chunks[j0 / kStoreChunk];
-      if ((rc = launch_ritz_combine_multi(V, ldv, cnt, (const double*)cd.p + (size_t)K * j0, K, out, D, j0 > 0,
-                                          h->stream)))
-        return rc;
-    }
+    std::vector<const float*> chunks;
+    for (int j0 = 0; j0 < m1; j0 += kStoreChunk) chunks.push_back((const float*)h->store_chunks[j0 / kStoreChunk]);
+    if ((rc = launch_ritz_combine_chunks(chunks.data(), ldv, m1, (const double*)cd.p, K, out, D, h->stream)))
+      return rc;
     AED_CUDA_TRY(cudaStreamSynchronize(h->stream));  // cf and the coefficient buffer are reused
   }
   const bool f32 = h->precision == AED_FP32;

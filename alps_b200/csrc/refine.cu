@@ -22,24 +22,43 @@ namespace {
 
 constexpr int kCombThreads = 256;
 
-// out_k[i] = (accumulate ? out_k[i] : 0) + sum_j coef[k * m + j] * V[j * ld + i]
-// for k < K: one pass over the m stored vectors, FP64 sums in ascending j.
+struct ChunkSet {
+  const float* p[kCombChunks];
+};
+
+// out_k[i] = (accumulate ? out_k[i] : 0) + sum_{j < mg} coef[k * m + j0 + j] v_j[i] for k < K, v_j the
+// stored vector j of this launch's chunks: FP64 sums in ascending j, the coefficients of the launch in
+// shared memory, a chunk's kMaxComb loads issued before their sums.
 template <int K>
-__global__ void __launch_bounds__(kCombThreads) ritz_combine_multi_kernel(const float* __restrict__ V, int64_t ld,
-                                                                         int m, const double* __restrict__ coef,
-                                                                         VecSet out, int64_t n, bool accumulate) {
-  __shared__ double cs[K * kMaxComb];
-  for (int q = threadIdx.x; q < K * m; q += kCombThreads) cs[q] = coef[q];
+__global__ void __launch_bounds__(kCombThreads) ritz_combine_chunks_kernel(const __grid_constant__ ChunkSet V,
+                                                                          int64_t ld, int mg, int m, int j0,
+                                                                          const double* __restrict__ coef,
+                                                                          VecSet out, int64_t n, bool accumulate) {
+  extern __shared__ double cs[];  // [K][mg]
+  for (int q = threadIdx.x; q < K * mg; q += kCombThreads) cs[q] = coef[(int64_t)(q / mg) * m + j0 + q % mg];
   __syncthreads();
   const int64_t stride = (int64_t)gridDim.x * kCombThreads;
   for (int64_t i = (int64_t)blockIdx.x * kCombThreads + threadIdx.x; i < n; i += stride) {
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = accumulate ? out.p[k][i] : 0.0;
-    for (int j = 0; j < m; ++j) {
-      const double v = (double)__ldg(V + (int64_t)j * ld + i);
+    for (int j = 0; j < mg; j += kMaxComb) {
+      const float* base = V.p[j / kMaxComb] + i;
+      if (j + kMaxComb <= mg) {
+        float v[kMaxComb];
 #pragma unroll
-      for (int k = 0; k < K; ++k) acc[k] = fma(cs[k * m + j], v, acc[k]);
+        for (int u = 0; u < kMaxComb; ++u) v[u] = __ldg(base + (int64_t)u * ld);
+#pragma unroll
+        for (int u = 0; u < kMaxComb; ++u)
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = fma(cs[k * mg + j + u], (double)v[u], acc[k]);
+      } else {
+        for (int u = 0; u < mg - j; ++u) {
+          const double v = (double)__ldg(base + (int64_t)u * ld);
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = fma(cs[k * mg + j + u], v, acc[k]);
+        }
+      }
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) out.p[k][i] = acc[k];
@@ -181,22 +200,32 @@ int grid_for(int64_t nch) {
 
 }  // namespace
 
-int launch_ritz_combine_multi(const float* V, int64_t ld, int m, const double* coef, int K, const VecSet& out,
-                              int64_t n, bool accumulate, cudaStream_t st) {
-  if (m < 1 || m > kMaxComb || K < 1 || K > kMaxRR) return fail(AED_ERR_INVALID, "ritz_combine_multi: bad sizes");
+int launch_ritz_combine_chunks(const float* const* chunks, int64_t ld, int m, const double* coef, int K,
+                               const VecSet& out, int64_t n, cudaStream_t st) {
+  if (m < 1 || K < 1 || K > kMaxRR) return fail(AED_ERR_INVALID, "ritz_combine_chunks: bad sizes");
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t want = (n + kCombThreads - 1) / kCombThreads, cap = (int64_t)sms * 8;
   const int grid = (int)(want < 1 ? 1 : (want < cap ? want : cap));
-  switch (K) {
-#define AED_CASE(k) \
-  case k: ritz_combine_multi_kernel<k><<<grid, kCombThreads, 0, st>>>(V, ld, m, coef, out, n, accumulate); break;
-    AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6) AED_CASE(7) AED_CASE(8)
+  constexpr int kGroup = kCombChunks * kMaxComb;  // vectors per launch
+  for (int j0 = 0; j0 < m; j0 += kGroup) {
+    const int mg = m - j0 < kGroup ? m - j0 : kGroup;
+    ChunkSet cs{};
+    for (int c = 0; c < (mg + kMaxComb - 1) / kMaxComb; ++c) cs.p[c] = chunks[j0 / kMaxComb + c];
+    const size_t smem = (size_t)K * mg * sizeof(double);  // at most 32 KB
+    switch (K) {
+#define AED_CASE(k)                                                                                   \
+  case k:                                                                                             \
+    ritz_combine_chunks_kernel<k><<<grid, kCombThreads, smem, st>>>(cs, ld, mg, m, j0, coef, out, n, j0 > 0); \
+    break;
+      AED_CASE(1) AED_CASE(2) AED_CASE(3) AED_CASE(4) AED_CASE(5) AED_CASE(6) AED_CASE(7) AED_CASE(8)
 #undef AED_CASE
-    default: return fail(AED_ERR_INVALID, "ritz_combine_multi: K");
+      default: return fail(AED_ERR_INVALID, "ritz_combine_chunks: K");
+    }
+    if (int rc = check_launch_counted("ritz_combine_chunks_kernel")) return rc;
   }
-  return check_launch_counted("ritz_combine_multi_kernel");
+  return AED_OK;
 }
 
 int launch_gram(const VecSet& X, const VecSet& Y, int K, int64_t n, double* part, double* out, cudaStream_t st) {
