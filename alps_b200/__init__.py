@@ -135,6 +135,7 @@ def lib():
                                           ctypes.POINTER(_P)]),
             "aed_destroy": (ctypes.c_int, [_P]),
             "aed_empty_cache": (ctypes.c_int, [ctypes.c_int]),
+            "aed_reserve_basis": (ctypes.c_int, [_P, _I32]),
             "aed_create_momentum": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.POINTER(Translations),
                                                    ctypes.c_int, ctypes.POINTER(_P)]),
             "aed_momentum_basis": (ctypes.c_int, [_P, _U32P, _DP, _I64, _I64]),
@@ -642,6 +643,11 @@ class Hamiltonian:
         _check(lib().aed_time_apply(self._h, x.ptr, y.ptr, reps, variant, 1 if with_alpha else 0, ctypes.byref(ms),
                                     ctypes.byref(v)))
         return ms.value, v.value
+
+    def reserve_basis(self, vectors):
+        """Allocate the FP32 Lanczos basis store of a mixed-precision handle for `vectors` vectors now
+        (aed_reserve_basis), so that no later solve grows it."""
+        _check(lib().aed_reserve_basis(self._h, int(vectors)))
 
     def time_mult(self, x, y, reps=10):
         ms = ctypes.c_double(0)

@@ -1106,6 +1106,18 @@ int aed_destroy(aed_handle* h) {
   return AED_OK;
 }
 
+int aed_reserve_basis(aed_handle* h, int32_t vectors) {
+  if (!h) return fail(AED_ERR_INVALID, "NULL handle");
+  if (h->precision != AED_FP32 || h->mom || h->gen)
+    return fail(AED_ERR_INVALID, "aed_reserve_basis: only mixed-precision spin-1/2 Sz-sector handles keep a basis");
+  if (vectors < 0 || vectors > kMaxRitzTerms) return fail(AED_ERR_INVALID, "aed_reserve_basis: vectors out of range");
+  DeviceGuard g(h->device);
+  const size_t cb = store_chunk_bytes_of(h->vlen);
+  for (int c = 0; c * kStoreChunk < vectors; ++c)
+    if (!handle_store_chunk(h, c, cb)) return AED_ERR_NOMEM;
+  return AED_OK;
+}
+
 int aed_empty_cache(int device) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {

@@ -157,6 +157,9 @@ int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out);
 int handle_pinned(aed_handle* h, size_t n, double** out);
 void handle_release_workspace(aed_handle* h);
 constexpr int kStoreChunk = 16;
+// Bytes of one chunk of the FP32 basis store for vectors of D floats, each
+// vector 256-byte aligned within the chunk.
+inline size_t store_chunk_bytes_of(int64_t D) { return (((size_t)D * 4 + 255) & ~(size_t)255) * kStoreChunk; }
 // Pointer to chunk `c` of the FP32 basis store (allocated on first use), or nullptr.
 void* handle_store_chunk(aed_handle* h, int c, size_t chunk_bytes);
 int solve(aed_handle* h, const aed_solve_opts* o, aed_solve_result* r);

@@ -171,6 +171,66 @@ __global__ void __launch_bounds__(kFinishThreads) finish_sum_kernel(const double
   finish_sum(part, n, out, take_sqrt);
 }
 
+// This thread's elements e0 + threadIdx.x + u kRedThreads of the chunk [e0, e1) of the update
+// w = (y - a x) - b v_prev (stored into y), and the sum of their w^2 in element order.  FP32 vectors
+// in a full chunk issue all their loads before the arithmetic (4-byte loads leave too few bytes in
+// flight otherwise); the arithmetic and the order of the sum are the same, so are the bits.
+template <typename T>
+__device__ __forceinline__ double update_chunk(double alpha, double b, const T* __restrict__ x,
+                                               const T* __restrict__ vprev, T* __restrict__ y, int64_t e0,
+                                               int64_t e1) {
+  double acc = 0.0;
+  if constexpr (sizeof(T) == 4) {
+    constexpr int U = (int)(kRedChunk / kRedThreads);
+    if (e1 - e0 == kRedChunk) {
+      const int64_t i0 = e0 + threadIdx.x;
+      T yv[U], xv[U], pv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        yv[u] = y[i0 + u * kRedThreads];
+        xv[u] = x[i0 + u * kRedThreads];
+        pv[u] = vprev ? vprev[i0 + u * kRedThreads] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        double w = __dsub_rn((double)yv[u], __dmul_rn(alpha, (double)xv[u]));
+        if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)pv[u]));
+        const T wt = (T)w;
+        y[i0 + u * kRedThreads] = wt;
+        acc = fma((double)wt, (double)wt, acc);
+      }
+      return acc;
+    }
+  }
+  for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
+    double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
+    if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
+    const T wt = (T)w;
+    y[i] = wt;
+    acc = fma((double)wt, (double)wt, acc);
+  }
+  return acc;
+}
+
+// y /= beta over the grid-stride elements of this thread; FP32 vectors load four elements before
+// dividing (elementwise: the order does not matter).
+template <typename T>
+__device__ __forceinline__ void normalize_elems(double beta, T* __restrict__ y, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * kRedThreads;
+  int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x;
+  if constexpr (sizeof(T) == 4) {
+    constexpr int U = 4;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+      T v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = y[i + u * stride];
+#pragma unroll
+      for (int u = 0; u < U; ++u) y[i + u * stride] = (T)__ddiv_rn((double)v[u], beta);
+    }
+  }
+  for (; i < n; i += stride) y[i] = (T)__ddiv_rn((double)y[i], beta);
+}
+
 // make_step middle part (lanczos.h:398-401): w -= a v; w -= b v_prev; chunk partials of |w|^2
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const double* __restrict__ alpha_p,
@@ -185,14 +245,7 @@ __global__ void __launch_bounds__(kRedThreads) lanczos_update_kernel(const doubl
   const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
   for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
     const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
-    double acc = 0.0;
-    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
-      double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
-      if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
-      const T wt = (T)w;
-      y[i] = wt;
-      acc = fma((double)wt, (double)wt, acc);
-    }
+    const double acc = update_chunk(alpha, b, x, vprev, y, e0, e1);
     const double tot = block_sum_all<kRedThreads>(acc, sm);
     if (threadIdx.x == 0) partB[c] = tot;
   }
@@ -214,14 +267,7 @@ __global__ void __launch_bounds__(kRedThreads) lanczos_update_fin_kernel(
   const int64_t nch = (n + kRedChunk - 1) / kRedChunk;
   for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
     const int64_t e0 = c * kRedChunk, e1 = min(n, e0 + kRedChunk);
-    double acc = 0.0;
-    for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
-      double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
-      if (vprev) w = __dsub_rn(w, __dmul_rn(b, (double)vprev[i]));
-      const T wt = (T)w;
-      y[i] = wt;
-      acc = fma((double)wt, (double)wt, acc);
-    }
+    const double acc = update_chunk(alpha, b, x, vprev, y, e0, e1);
     const double tot = block_sum_all<kRedThreads>(acc, sm);
     if (threadIdx.x == 0) partB[c] = tot;
   }
@@ -236,8 +282,7 @@ __global__ void __launch_bounds__(kRedThreads) lanczos_normalize_fin_kernel(cons
   __shared__ double sm[33];
   const double beta = sqrt(finish_sum_in_cta<kRedThreads>(beta_part, n_bpart, sm));
   if (blockIdx.x == 0 && threadIdx.x == 0) *beta_out = beta;
-  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
-    y[i] = (T)__ddiv_rn((double)y[i], beta);
+  normalize_elems(beta, y, n);
 }
 
 // make_step tail (lanczos.h:402): w /= b
@@ -245,8 +290,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) lanczos_normalize_kernel(const double* __restrict__ beta_p,
                                                                        T* __restrict__ y, int64_t n) {
   const double beta = *beta_p;
-  for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRedThreads)
-    y[i] = (T)__ddiv_rn((double)y[i], beta);
+  normalize_elems(beta, y, n);
 }
 
 // Ritz vector from the stored FP32 Lanczos basis, accumulated in FP64.

@@ -741,9 +741,9 @@ int solve_mixed(aed_handle* h, const double* start_host, uint64_t seed, int nev,
   const int64_t D = h->vlen;
   // Lanczos basis store: chunks of kStoreChunk FP32 vectors, grown as the
   // recurrence advances and kept by the handle for later solves
-  const size_t vbytes = (((size_t)D * 4 + 255) & ~(size_t)255);
+  const size_t chunk_bytes = store_chunk_bytes_of(D);
+  const size_t vbytes = chunk_bytes / kStoreChunk;
   const int64_t ldv = (int64_t)(vbytes / 4);  // stride of the stored vectors (256-byte aligned)
-  const size_t chunk_bytes = vbytes * kStoreChunk;
   const int cap = std::min(max_iter + 1, kMaxRitzTerms);
   EventRing ring;
   void* small = nullptr;  // alpha/beta pairs | Ritz coefficients (workspace slot 1, reused by the FP64 phase after)

@@ -378,7 +378,10 @@ def run_ours(args):
     mixed = None
     if not args.no_mixed:
         h32 = ed.Hamiltonian(N, n_up, chain_bonds(L28, j2s[0]), precision=ed.FP32, device=local)
-        h32.solve(nev=NEV, seed=1)  # grows the FP32 basis store once
+        # warm-up: the FP32 basis store sized once for 256 vectors (40 GB; the FP32 phases here take 88-214
+        # steps), as a long-running caller keeps it, so that no timed solve waits on a device allocation
+        h32.reserve_basis(256)
+        h32.solve(nev=NEV, seed=1)
         barrier(pg)
         s32 = torch.cuda.ExternalStream(h32.stream())
         m0 = torch.cuda.Event(enable_timing=True)

@@ -122,6 +122,12 @@ int aed_destroy(aed_handle* h);
  * `device`, all cached pinned host memory).  No reference counterpart: the
  * reference's matrices are freed with their task. */
 int aed_empty_cache(int device);
+/* Allocate now the FP32 Lanczos basis store of a mixed-precision (AED_FP32)
+ * spin-1/2 Sz-sector handle for `vectors` vectors; the store otherwise grows
+ * chunk by chunk inside the solves that need it, and is kept until
+ * aed_destroy.  A long-running caller sizes it once so that no solve pays for
+ * a device allocation.  No reference counterpart: the reference keeps no basis. */
+int aed_reserve_basis(aed_handle* h, int32_t vectors);
 
 /* ---- measurements ------------------------------------------------------- */
 #define AED_OBS_SZ 0   /* <Sz_i>                       */

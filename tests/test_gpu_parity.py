@@ -436,6 +436,28 @@ def test_rayleigh_ritz_with_ghost_copies_in_the_clusters(nev):
         assert e32 - e64 <= err + 1e-12 * abs(e64)  # the bound holds (values from above)
 
 
+def test_reserved_basis_store_gives_the_same_solve():
+    """aed_reserve_basis sizes the FP32 basis store ahead (here for more vectors than the solve takes,
+    and for fewer): the mixed solve's values, errors and iteration counts equal those of a handle whose
+    store grew inside the solve, bit for bit; the FP64 handle, which keeps no basis, refuses."""
+    b = [(i, (i + 1) % 20, 1.0, 1.0, 0.0) for i in range(20)] + [(i, (i + 2) % 20, 0.3, 0.3, 0.0) for i in range(20)]
+    grown = ed.Hamiltonian(20, 10, b, precision=ed.FP32)
+    r0 = grown.solve(nev=2, seed=5)
+    for n in (300, 20):
+        h = ed.Hamiltonian(20, 10, b, precision=ed.FP32)
+        h.reserve_basis(n)
+        r = h.solve(nev=2, seed=5)
+        for k in ("evals", "errors"):
+            assert np.array_equal(r[k], r0[k]), (n, k)
+        assert (r["iterations"], r["iterations_low"]) == (r0["iterations"], r0["iterations_low"])
+        h.close()
+    grown.close()
+    h64 = ed.Hamiltonian(20, 10, b)
+    with pytest.raises(ed.AEDError, match="basis"):
+        h64.reserve_basis(16)
+    h64.close()
+
+
 def _basis_and_copies(ham, r):
     """The stored FP32 Lanczos basis V (m x D) of the last mixed solve, max |V V^T - I|, and how many
     eigenvalues of its T-matrix lie within 1e-5 relative of the lowest (1 + the ghost copies)."""
