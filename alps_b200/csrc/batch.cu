@@ -120,10 +120,35 @@ __global__ void __launch_bounds__(256) b_alpha(BatchArgs a) {
   if (threadIdx.x == 0) I.ab[2 * I.j] = tot;
 }
 
+// This thread's elements e0 + threadIdx.x + u kRedThreads of the chunk [e0, e1): w = (y - alpha x) -
+// b v_prev into y, and the sum of w^2 in element order.  FP32 in a full chunk: all loads issued before
+// the arithmetic (the same operations in the same order, so the same bits).
 template <typename T>
 __device__ __forceinline__ double update_chunk(const T* x, const T* vp, T* y, int64_t e0, int64_t e1, double alpha,
                                                double b) {
   double acc = 0.0;
+  if constexpr (sizeof(T) == 4) {
+    constexpr int U = (int)(kRedChunk / kRedThreads);
+    if (e1 - e0 == kRedChunk) {
+      const int64_t i0 = e0 + threadIdx.x;
+      T yv[U], xv[U], pv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        yv[u] = y[i0 + u * kRedThreads];
+        xv[u] = x[i0 + u * kRedThreads];
+        pv[u] = vp ? vp[i0 + u * kRedThreads] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        double w = __dsub_rn((double)yv[u], __dmul_rn(alpha, (double)xv[u]));
+        if (vp) w = __dsub_rn(w, __dmul_rn(b, (double)pv[u]));
+        const T wt = (T)w;
+        y[i0 + u * kRedThreads] = wt;
+        acc = fma((double)wt, (double)wt, acc);
+      }
+      return acc;
+    }
+  }
   for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) {
     double w = __dsub_rn((double)y[i], __dmul_rn(alpha, (double)x[i]));
     if (vp) w = __dsub_rn(w, __dmul_rn(b, (double)vp[i]));
@@ -178,7 +203,16 @@ __global__ void __launch_bounds__(kRedThreads) b_norm(BatchArgs a) {
     const int64_t e0 = (int64_t)w.idx * kRedChunk, e1 = e0 + kRedChunk < I.D ? e0 + kRedChunk : I.D;
     if (I.phase == kPhLow) {
       float* y = low_vec(I, j + 1);
-      for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) y[i] = (float)__ddiv_rn((double)y[i], beta);
+      constexpr int U = (int)(kRedChunk / kRedThreads);
+      if (e1 - e0 == kRedChunk) {  // a full chunk: every load before the divisions
+        float v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = y[e0 + threadIdx.x + u * kRedThreads];
+#pragma unroll
+        for (int u = 0; u < U; ++u) y[e0 + threadIdx.x + u * kRedThreads] = (float)__ddiv_rn((double)v[u], beta);
+      } else {
+        for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) y[i] = (float)__ddiv_rn((double)y[i], beta);
+      }
     } else {
       double* y = high_vec(I, j + 1);
       for (int64_t i = e0 + threadIdx.x; i < e1; i += kRedThreads) y[i] = __ddiv_rn(y[i], beta);
