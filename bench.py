@@ -911,11 +911,18 @@ def apply_case_bonds(name):
 def run_apply(args):
     """A few applies y = H x of one workload, timed with CUDA events (the commands the ncu summaries under
     profiles/ use; plain text, not a bench line).  --case spin1_l18: spin-1 Heisenberg chain L=18, Sz=0;
-    --case mom_l28: J1-J2 chain L=28 (J2 = 0.25), Sz=0, momentum index --k."""
+    --case mom_l28: J1-J2 chain L=28 (J2 = 0.25), Sz=0, momentum index --k; --case spin1mom_l18: the
+    spin-1 chain's Sz=0 momentum sector of index --k."""
     import alps_b200 as ed
     if args.case == "spin1_l18":
         L = 18
         ham = ed.Hamiltonian(L, L, [(i, (i + 1) % L, 1.0, 1.0, 0.0) for i in range(L)], two_s=2)
+    elif args.case == "spin1mom_l18":
+        L = 18
+        params = {"MODEL": "spin", "LATTICE": "chain lattice", "L": L}
+        k = ed.lattice_momenta(params)[args.k]
+        ham = ed.Hamiltonian(L, L, [(i, (i + 1) % L, 1.0, 1.0, 0.0) for i in range(L)], two_s=2,
+                             translations=ed.lattice_translations(params, k))
     elif args.case == "mom_l28":
         params = {"MODEL": "spin", "LATTICE": "nnn chain lattice", "L": 28}
         k = ed.lattice_momenta(params)[args.k]
@@ -925,7 +932,7 @@ def run_apply(args):
         ham = ed.Hamiltonian(N, n_up, bonds, precision=ed.FP64 if args.apply_precision == "fp64" else ed.FP32)
     x, y = ham.new_vector(), ham.new_vector()
     ham.fill_random(x, 1)
-    if args.case in ("spin1_l18", "mom_l28"):
+    if args.case in ("spin1_l18", "mom_l28", "spin1mom_l18"):
         ham.time_mult(x, y, 1)
         print(f"{args.case} rows={ham.dim} apply_ms={ham.time_mult(x, y, args.reps):.4f}")
         return
@@ -957,13 +964,13 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the config-1/3/4 sections of the default line")
     ap.add_argument("--workload", default="l28",
                     choices=["l28", "square", "batch", "serve", "momentum", "spin", "apply"])
-    ap.add_argument("--case", default="l28", help="apply: l24, l26, l28, sq6x5, spin1_l18, mom_l28")
+    ap.add_argument("--case", default="l28", help="apply: l24, l26, l28, sq6x5, spin1_l18, mom_l28, spin1mom_l18")
     ap.add_argument("--apply-precision", default="fp64", choices=["fp64", "fp32"], help="apply: vector precision")
     ap.add_argument("--variant", type=int, default=-1, help="apply: variant index (-1: autotuned)")
     ap.add_argument("--reps", type=int, default=3, help="apply: timed applies")
     ap.add_argument("--sweep", action="store_true", help="apply: time every variant with and without partials")
     ap.add_argument("--alpha", action="store_true", help="apply: with the Lanczos step's <x,y> partials")
-    ap.add_argument("--k", type=int, default=0, help="apply mom_l28: momentum index")
+    ap.add_argument("--k", type=int, default=0, help="apply mom_l28 / spin1mom_l18: momentum index")
     ap.add_argument("--sector-workers", type=int, default=4, help="momentum: sectors solved at once")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests (20000 = full stream)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered rate, requests/s (the stream's is 200)")
