@@ -128,6 +128,24 @@ def test_spin_s_set_couplings_through_every_apply_form():
         ham.close()
 
 
+@pytest.mark.parametrize("two_s,n", [(4, 7), (3, 8)], ids=["2S=4-chain7", "2S=3-chain8"])
+def test_spin_s_lo_table_with_site_terms(two_s, n):
+    """Spin 2 and spin 3/2 with nearest and next-nearest Heisenberg bonds (two coupling classes, no
+    biquadratic term: two off-diagonal slots, so the apply reads the lo table), fields and single-ion
+    anisotropy on every site: H x equals the oracle's (1e-12 of sum |H_ij x_j|) in two Sz sectors."""
+    rng = np.random.default_rng(two_s * 31 + n)
+    bonds = _chain(n, 1.0, 0.9) + [(i, (i + 2) % n, 0.35, 0.3, 0.0) for i in range(n)]
+    h = rng.uniform(-0.3, 0.3, n)
+    dd = rng.uniform(-0.5, 0.5, n)
+    for T in (n * two_s // 2, n * two_s // 2 - 1):
+        ham = ed.Hamiltonian(n, T, bonds, site_h=h, site_d=dd, two_s=two_s)
+        H = ospin.hamiltonian(n, two_s, bonds, h, dd, digit_sum=T)
+        x = rng.normal(size=ham.dim)
+        y = ham.apply(x)
+        assert np.all(np.abs(y - H @ x) <= 1e-12 * (abs(H) @ np.abs(x)) + 1e-14)
+        ham.close()
+
+
 SPIN_MEAS = {
     "MEASURE_AVERAGE[Magnetization]": "Sz",
     "MEASURE_LOCAL[Local magnetization]": "Sz",
