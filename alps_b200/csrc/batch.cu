@@ -54,14 +54,14 @@ __device__ __forceinline__ double* high_vec(const BInst& I, int j) { return I.v6
 // B = 1 (the item's hi blocks one at a time) or kBatchBundle (both at once).
 // FP64 vectors (b_hv64): 4 rows per thread, 3 CTAs per SM.
 template <int R, int MINB, int B>
-__global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a, int mr_lo, int mr_hi) {
+__global__ void __launch_bounds__(kHvThreads, MINB) b_hv32(BatchArgs a, int bucket, int mr_lo, int mr_hi) {
   static_assert(B == 1 || B == kBatchBundle, "an item is one bundle or its blocks one by one");
   extern __shared__ __align__(16) unsigned char b_dyn[];
   __shared__ bapply::BundleSmem<B> sm;
-  const int n = *a.n_tiles;
+  const int i0 = a.tile_start[bucket], i1 = a.tile_start[bucket + 1];  // this bucket's items
   int cur = -1, rc = 0;
   float* xs = nullptr;
-  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+  for (int it = i0 + (int)blockIdx.x; it < i1; it += gridDim.x) {
     const BItem w = a.tiles[it];
     const BInst& I = a.inst[w.inst];
     if (I.phase != kPhLow || !stepping(I) || I.t.maxrows <= mr_lo || I.t.maxrows > mr_hi)
@@ -853,7 +853,7 @@ int sms() {
 // row's terms in the same order (apply_blocks.cuh), so the choice changes the
 // speed, not the results.
 struct Cand32 {
-  void (*kern)(BatchArgs, int, int);
+  void (*kern)(BatchArgs, int, int, int);
   const char* name;
 };
 const Cand32 kCand32[kBatchCand32] = {
@@ -927,7 +927,7 @@ int batch_launch_hv32(const BatchArgs& a, int cand, int bucket, cudaStream_t st)
   const int lo = bucket == 0 ? -1 : kBatchBucketHi[bucket - 1];
   const int hi = bucket + 1 == kBatchBuckets ? 0x7fffffff : kBatchBucketHi[bucket];
   kCand32[cand].kern<<<hv_grid(kCand32[cand].kern, a.hv_smem, &g_c32[cand], &g_c32_smem[cand]), kHvThreads,
-                       a.hv_smem, st>>>(a, lo, hi);
+                       a.hv_smem, st>>>(a, bucket, lo, hi);
   return check("batched FP32 apply");
 }
 

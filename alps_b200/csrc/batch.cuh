@@ -113,6 +113,9 @@ struct BatchArgs {
   int32_t* n_chunks;
   int max_inst;
   int hv_smem;         // dynamic shared memory of the apply (batch_hv_smem_bytes, max over residents)
+  // tiles are ordered by FP32 size bucket: bucket b's items are [tile_start[b], tile_start[b + 1])
+  // (kBatchBuckets + 1 offsets, device), so each bucket's apply walks only its own items
+  int32_t* tile_start;
 };
 
 // Hi blocks per work item of the batched apply (entries ub * kBatchBundle ..

@@ -81,6 +81,11 @@ struct Lane {
 }  // namespace
 }  // namespace aed
 
+// The server's device counters: n_inst, n_tiles, n_chunks, one unused, then the
+// start of every FP32 size bucket's apply items and the end of the last.
+constexpr int kBucketStarts = 4;
+constexpr int kCounts = kBucketStarts + aed::kBatchBuckets + 1;
+
 struct aed_server {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -97,7 +102,7 @@ struct aed_server {
   std::map<std::pair<int, int>, aed::Sector> sectors;
   // device tables of the engine
   aed::BInst* d_inst = nullptr;
-  int32_t* d_counts = nullptr;  // n_inst, n_tiles, n_chunks
+  int32_t* d_counts = nullptr;  // n_inst, n_tiles, n_chunks, (unused), the buckets' tile starts (kCounts)
   aed::BItem* d_tiles = nullptr;
   aed::BItem* d_chunks = nullptr;
   size_t cap_tiles = 0, cap_chunks = 0;
@@ -379,17 +384,24 @@ void release_slot(aed_server* s, int k) {
 }
 
 int rebuild_items(aed_server* s) {
-  std::vector<BItem> tiles, chunks;
+  std::vector<BItem> tiles, chunks, by_bucket[kBatchBuckets];
   int n_inst = 0;
   for (int k = 0; k < (int)s->slots.size(); ++k) {
     if (!s->slots[k].used) continue;
     n_inst = k + 1;
     const BInst& I = s->slots[k].inst;
     const std::vector<uint32_t>& blk = s->sectors.at(s->slots[k].sector).blk;
+    std::vector<BItem>& mine = by_bucket[batch_bucket_of(I.t.maxrows)];
     for (size_t ub = 0; ub * kBatchBundle < blk.size(); ++ub)  // bundles holding at least one block
-      if (blk[ub * kBatchBundle] != kNoBlockEntry) tiles.push_back({k, (int32_t)ub});
+      if (blk[ub * kBatchBundle] != kNoBlockEntry) mine.push_back({k, (int32_t)ub});
     for (int64_t c = 0; c < I.n_chunks; ++c) chunks.push_back({k, (int32_t)c});
   }
+  // the apply items bucket by bucket (an instance's items stay together), with each bucket's start
+  for (int b = 0; b < kBatchBuckets; ++b) {
+    s->h_counts[kBucketStarts + b] = (int32_t)tiles.size();
+    tiles.insert(tiles.end(), by_bucket[b].begin(), by_bucket[b].end());
+  }
+  s->h_counts[kBucketStarts + kBatchBuckets] = (int32_t)tiles.size();
   if (tiles.size() > s->cap_tiles || chunks.size() > s->cap_chunks) {
     AED_CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (s->d_tiles) cudaFree(s->d_tiles);
@@ -414,7 +426,7 @@ int rebuild_items(aed_server* s) {
   s->h_counts[0] = n_inst;
   s->h_counts[1] = (int32_t)tiles.size();
   s->h_counts[2] = (int32_t)chunks.size();
-  AED_CUDA_TRY(cudaMemcpyAsync(s->d_counts, s->h_counts, 3 * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+  AED_CUDA_TRY(cudaMemcpyAsync(s->d_counts, s->h_counts, kCounts * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
   // tiles/chunks are host temporaries: finish the copies before they go
   AED_CUDA_TRY(cudaStreamSynchronize(s->stream));
   s->dirty = false;
@@ -430,7 +442,7 @@ int tune_buckets(aed_server* s) {
   for (const Slot& sl : s->slots)
     if (sl.used && sl.inst.phase == kPhLow) want[batch_bucket_of(sl.inst.t.maxrows)] = true;
   BatchArgs a{s->d_inst, s->d_counts, s->d_tiles, s->d_counts + 1, s->d_chunks, s->d_counts + 2, s->max_slots,
-              s->hv_smem};
+              s->hv_smem, s->d_counts + kBucketStarts};
   for (int b = 0; b < kBatchBuckets; ++b) {
     if (!want[b] || s->tuned32[b]) continue;
     int rc = batch_prepare(a);
@@ -507,7 +519,7 @@ int capture_graph(aed_server* s) {
     s->graph = nullptr;
   }
   BatchArgs a{s->d_inst, s->d_counts, s->d_tiles, s->d_counts + 1, s->d_chunks, s->d_counts + 2, s->max_slots,
-              s->hv_smem};
+              s->hv_smem, s->d_counts + kBucketStarts};
   cudaGraph_t g = nullptr;
   const int rp = batch_prepare(a);
   if (rp) return rp;
@@ -609,13 +621,13 @@ int aed_server_create(const aed_server_opts* o, aed_server** out) {
   s->h_inst.resize(s->max_slots);
   for (auto& b : s->h_inst) b = BInst{};
   if (cudaMalloc(&s->d_inst, sizeof(BInst) * s->max_slots) != cudaSuccess ||
-      cudaMalloc(&s->d_counts, 4 * sizeof(int32_t)) != cudaSuccess ||
-      cudaMallocHost(&s->h_counts, 4 * sizeof(int32_t)) != cudaSuccess) {
+      cudaMalloc(&s->d_counts, kCounts * sizeof(int32_t)) != cudaSuccess ||
+      cudaMallocHost(&s->h_counts, kCounts * sizeof(int32_t)) != cudaSuccess) {
     cudaGetLastError();
     return fail(AED_ERR_NOMEM, "server tables");
   }
   AED_CUDA_TRY(cudaMemset(s->d_inst, 0, sizeof(BInst) * s->max_slots));
-  AED_CUDA_TRY(cudaMemset(s->d_counts, 0, 4 * sizeof(int32_t)));
+  AED_CUDA_TRY(cudaMemset(s->d_counts, 0, kCounts * sizeof(int32_t)));
   s->cap_tiles = s->cap_chunks = 1 << 14;
   if (cudaMalloc(&s->d_tiles, s->cap_tiles * sizeof(BItem)) != cudaSuccess ||
       cudaMalloc(&s->d_chunks, s->cap_chunks * sizeof(BItem)) != cudaSuccess) {
