@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "apply.cuh"
 #include "apply_blocks.cuh"
@@ -212,8 +213,11 @@ __device__ __forceinline__ double update_chunk(double alpha, double b, const T* 
   return acc;
 }
 
-// y /= beta over the grid-stride elements of this thread; FP32 vectors load four elements before
-// dividing (elementwise: the order does not matter).
+// y /= beta over the grid-stride elements of this thread; each element is
+// divided on its own, so the grouping below does not change the bits.  FP32:
+// four elements loaded before dividing (float4 vectors measured slower);
+// FP64: 16-byte double2 vectors, two in flight, when y is 16-byte aligned,
+// then the tail element by element.
 template <typename T>
 __device__ __forceinline__ void normalize_elems(double beta, T* __restrict__ y, int64_t n) {
   const int64_t stride = (int64_t)gridDim.x * kRedThreads;
@@ -227,6 +231,26 @@ __device__ __forceinline__ void normalize_elems(double beta, T* __restrict__ y, 
 #pragma unroll
       for (int u = 0; u < U; ++u) y[i + u * stride] = (T)__ddiv_rn((double)v[u], beta);
     }
+  } else if ((reinterpret_cast<uintptr_t>(y) & 15u) == 0) {
+    const int64_t nv = n / 2, t0 = i;
+    double2* yv = reinterpret_cast<double2*>(y);
+    int64_t k = t0;
+    for (; k + stride < nv; k += 2 * stride) {
+      double2 a = yv[k], b = yv[k + stride];
+      a.x = __ddiv_rn(a.x, beta);
+      a.y = __ddiv_rn(a.y, beta);
+      b.x = __ddiv_rn(b.x, beta);
+      b.y = __ddiv_rn(b.y, beta);
+      yv[k] = a;
+      yv[k + stride] = b;
+    }
+    for (; k < nv; k += stride) {
+      double2 a = yv[k];
+      a.x = __ddiv_rn(a.x, beta);
+      a.y = __ddiv_rn(a.y, beta);
+      yv[k] = a;
+    }
+    i = nv * 2 + t0;
   }
   for (; i < n; i += stride) y[i] = (T)__ddiv_rn((double)y[i], beta);
 }
