@@ -1115,7 +1115,9 @@ int aed_reserve_basis(aed_handle* h, int32_t vectors) {
   const size_t cb = store_chunk_bytes_of(h->vlen);
   for (int c = 0; c * kStoreChunk < vectors; ++c)
     if (!handle_store_chunk(h, c, cb)) return AED_ERR_NOMEM;
-  return AED_OK;
+  // and the Rayleigh-Ritz step's workspace for the most Ritz vectors it takes
+  void* ws = nullptr;
+  return vectors > 0 ? handle_workspace(h, 2, rr_workspace_bytes(h->vlen, kMaxRR), &ws) : AED_OK;
 }
 
 int aed_empty_cache(int device) {

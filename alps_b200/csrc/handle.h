@@ -154,6 +154,9 @@ int handle_check_flag(aed_handle* h);
 int handle_tune(aed_handle* h, bool f32, const void* x, void* y);
 // Workspace of at least `bytes` device bytes / `n` pinned doubles, reused across solves.
 int handle_workspace(aed_handle* h, int slot, size_t bytes, void** out);
+// Workspace slot 2 of the mixed path's Rayleigh-Ritz step with K Ritz vectors
+// of D scalars: the K vectors, their images, the Gram partials and sums.
+size_t rr_workspace_bytes(int64_t D, int K);
 int handle_pinned(aed_handle* h, size_t n, double** out);
 void handle_release_workspace(aed_handle* h);
 constexpr int kStoreChunk = 16;

@@ -37,6 +37,15 @@
 #include "tmatrix_core.h"
 
 namespace aed {
+
+size_t rr_workspace_bytes(int64_t D, int K) {
+  const size_t vb = ((size_t)D * 8 + 255) & ~(size_t)255;
+  const int np = K * (K + 1) / 2 + K * K;
+  const size_t part_bytes = (((size_t)np * red_chunks(D) * 8) + 255) & ~(size_t)255;
+  constexpr int kMaxSums = kMaxRR * (kMaxRR + 1) / 2 + kMaxRR * kMaxRR;
+  return 2 * (size_t)K * vb + part_bytes + (size_t)kMaxSums * 8;
+}
+
 namespace {
 
 struct DevMem {
@@ -634,7 +643,7 @@ int rayleigh_ritz(aed_handle* h, const TmatInfo& T1, int m1, const std::vector<d
   // the finished sums: np Gram entries, then (reused) the residuals
   constexpr int kMaxSums = kMaxRR * (kMaxRR + 1) / 2 + kMaxRR * kMaxRR;
   static_assert(kMaxSums >= kMaxRR, "residual sums fit the Gram buffer");
-  int rc = handle_workspace(h, 2, 2 * (size_t)K * vb + part_bytes + (size_t)kMaxSums * 8, &ws);
+  int rc = handle_workspace(h, 2, rr_workspace_bytes(D, K), &ws);
   if (rc) return rc;
   VecSet psi{}, img{};
   for (int k = 0; k < K; ++k) {

@@ -123,8 +123,9 @@ int aed_destroy(aed_handle* h);
  * reference's matrices are freed with their task. */
 int aed_empty_cache(int device);
 /* Allocate now the FP32 Lanczos basis store of a mixed-precision (AED_FP32)
- * spin-1/2 Sz-sector handle for `vectors` vectors; the store otherwise grows
- * chunk by chunk inside the solves that need it, and is kept until
+ * spin-1/2 Sz-sector handle for `vectors` vectors, and the workspace of its
+ * Rayleigh-Ritz step for the most Ritz vectors that step takes; both
+ * otherwise grow inside the solves that need them, and are kept until
  * aed_destroy.  A long-running caller sizes it once so that no solve pays for
  * a device allocation.  No reference counterpart: the reference keeps no basis. */
 int aed_reserve_basis(aed_handle* h, int32_t vectors);
